@@ -1,0 +1,365 @@
+"""Benchmark: staggered load increments per second of the 3D periodic voxel pore cell.
+
+Workload (the metric's single-GPU configuration): 64^3 periodic voxel H8 cell,
+edge 1 mm, one spherical pore of radius 0.2 at the centre with E x 1e-6,
+matrix E = 3 GPa, nu = 0.35, Gc = 0.5 N/mm, ell = 2 voxels, hybrid AT2 with
+kappa = 1e-6, spectral driver; uniaxial macro strain eps_zz ramped 0 -> 0.02 in
+50 increments.  A "step" is one staggered load increment (mechanics PCG,
+driving force + history, box-KKT damage solve, until the staggered change is
+below 1e-4, then the final mechanics re-solve).  Inputs are synthetic (the
+geometry above, built in memory).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun, one process per GPU) every rank runs its own replica of
+the cell: the workload does not shard (replicas only), the value is the total
+increments of all ranks over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "staggered steps/s, chosen vs plain FP64 on 1 B200 at ≤1e-6 rel err; HBM GB/s"
+UNIT = "staggered steps/s"
+N_CELL = 64
+INCREMENTS = 50
+# Mean per-increment iteration counts of this workload over increments 4..8
+# (the default timed window), measured with this repository's CUDA solver on a
+# B200; the CPU reference arm scales its timed per-iteration samples by them.
+REF_COUNTS = {"mech": 600.0, "pf": 60.0, "stag": 2.0}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload_config():
+    return {
+        "workload": "3D periodic voxel H8 pore cell 64^3 (r=0.2 L, E x 1e-6), AT2 spectral, eps_zz 0->0.02 in 50 "
+                    "increments; step = one staggered load increment",
+        "cells": 1, "voxels": N_CELL ** 3, "mechanics": "constrained Jacobi PCG rtol 1e-8",
+        "damage": "box-KKT active set + Dirichlet PCG", "form": "plain FP64",
+        "l2": "flushed (256 MB write) before every timed step", "parallelism": "replicas",
+    }
+
+
+def build_cell(device):
+    from phast_b200 import solid3d as s3
+    h = 1.0 / N_CELL
+    shape = (N_CELL, N_CELL, N_CELL)
+    phase = s3.sphere_pore_phase(shape, 0.2)
+    phases = [s3.PhaseMaterial("mi_matrix", 3000.0, 0.35, 0.5), s3.PhaseMaterial("pore", 3000.0 * 1e-6, 0.35, 0.5)]
+    load = s3.LoadCase.ramp("zz", 2, 0.02, INCREMENTS)
+    op = s3.PeriodicVoxelPhaseFieldOperator(s3.VoxelGrid(shape, (h, h, h)), phase, phases, 2 * h, 1e-6, load,
+                                            device=device)
+    return op, s3.StaggeredSolver(op)
+
+
+class Clocks:
+    """nvidia-smi sampler over the timed region (SM clock, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.remove(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def flush_l2(buf):
+    buf.add_(1)
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the numpy oracle timed on bounded samples of the same cell
+# ---------------------------------------------------------------------------
+
+def cpu_per_iteration_costs(threads_note=True):
+    """Seconds per mechanics PCG iteration, per damage PCG iteration and per staggered pass
+    of the oracle at full size (64^3); ~10-20 s of CPU work."""
+    from oracle import h8
+    shape, h = (N_CELL,) * 3, 1.0 / N_CELL
+    k, j, i = np.meshgrid(*(np.arange(N_CELL),) * 3, indexing="ij")
+    c = np.stack([(i + 0.5) / N_CELL - 0.5, (j + 0.5) / N_CELL - 0.5, (k + 0.5) / N_CELL - 0.5], -1)
+    slot = (np.linalg.norm(c, axis=-1) < 0.2).astype(np.int64).reshape(-1)
+    C0, l0, m0 = h8.isotropic_C(3000.0, 0.35)
+    C1, l1, m1 = h8.isotropic_C(3e-3, 0.35)
+    op = h8.VoxelOperator(shape, (h, h, h), slot, np.stack([C0, C1]), np.array([l0, l1]), np.array([m0, m1]),
+                          np.array([0.5, 0.5]), np.array([2, 0]), 2 * h, 1e-6, 0, 2, (0, 1, 3, 4, 5))
+    rng = np.random.default_rng(0)
+    d = rng.uniform(0, 0.5, op.n_red)
+    g = op.degradation(d)
+    x = rng.normal(size=op.n_mech) * 1e-4
+    H = rng.uniform(0, 1, (op.n_elements, 8))
+    dg = op.mech_diagonal(g)
+    free = ~op.fixed_mask()
+    n_it = 4
+    t0 = time.perf_counter()
+    _, its, _, _, _ = h8.pcg(lambda v: np.where(free, op.mech_action(v, g), 0.0), np.where(free, x, 0.0),
+                             np.where(free, dg, 1.0), rtol=1e-30, atol=1e-300, maxiter=n_it, check_every=n_it)
+    t_mech = (time.perf_counter() - t0) / n_it
+    s = op.damage_scale
+    n_it = 10
+    t0 = time.perf_counter()
+    h8.dirichlet_pcg(lambda v: s * op.damage_action(v, H), s * op.damage_rhs(H), s * op.damage_diagonal(H),
+                     np.zeros(op.n_red, bool), np.zeros(op.n_red), None, 1e-300, n_it)
+    t_pf = (time.perf_counter() - t0) / n_it
+    t0 = time.perf_counter()
+    op.degradation(d)
+    op.mech_diagonal(g)
+    op.driving_force(x)
+    op.damage_rhs(H)
+    op.damage_diagonal(H)
+    t_pass = time.perf_counter() - t0
+    return t_mech, t_pf, t_pass
+
+
+def cpu_step_estimate(counts):
+    t_mech, t_pf, t_pass = cpu_per_iteration_costs()
+    sec = counts["mech"] * t_mech + counts["pf"] * t_pf + (counts["stag"] + 1) * t_pass
+    sample = (f"numpy oracle on the full 64^3 cell: 4 mechanics PCG iterations ({t_mech:.3f} s each), 10 damage "
+              f"PCG iterations ({t_pf:.4f} s each), one staggered pass of diagonal/driving/rhs ({t_pass:.2f} s); "
+              f"scaled to one step with {counts['mech']:.0f} mechanics + {counts['pf']:.0f} damage iterations "
+              f"and {counts['stag']:.1f} staggered passes per increment")
+    return sec, sample
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args, rank, world, device):
+    from phast_b200 import _lib
+    op, solver = build_cell(device)
+    state = solver.initial_state()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)  # 256 MB > 126 MB L2
+    for _ in range(args.warmup):
+        state, _ = solver.advance(state, op.load.targets[state.increment])
+    torch.cuda.synchronize()
+    snap = {k: getattr(state, k).detach().cpu().pin_memory() for k in ("x", "d", "H")}
+    snap_meta = (state.step, state.macro_strain.copy(), state.macro_stress.copy(), state.increment)
+
+    # ---- device-resident timed region --------------------------------------------------
+    clocks = Clocks(torch.cuda.current_device())
+    lib = _lib.load()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    lib.phastb_launch_count_reset()
+    total_ms, counts = 0.0, []
+    for _ in range(args.steps):
+        flush_l2(flush)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        state, rec = solver.advance(state, op.load.targets[state.increment])
+        e1.record()
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        counts.append((rec.pcg_iters_mech, rec.pcg_iters_pf, rec.stagger_iters))
+    launches = lib.phastb_launch_count()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.barrier()
+    max_ms = float(t.item())
+    value = args.steps * world / (max_ms / 1e3)
+
+    # ---- end to end through the public API with host buffers ---------------------------
+    from phast_b200.solid3d import SolverState
+    pinned_out = {k: torch.empty_like(v).pin_memory() for k, v in snap.items()}
+    dev_in = {k: torch.empty(v.shape, dtype=v.dtype, device=device) for k, v in snap.items()}
+    h2d = sum(v.numel() * v.element_size() for v in snap.values())
+    st_meta = snap_meta
+    e2e_ms = 0.0
+    host_state = {k: v for k, v in snap.items()}
+    for _ in range(args.steps):
+        flush_l2(flush)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in dev_in:
+            dev_in[k].copy_(host_state[k], non_blocking=True)
+        s_in = SolverState(st_meta[0], dev_in["x"].clone(), dev_in["d"].clone(), dev_in["H"].clone(), st_meta[1],
+                           st_meta[2], st_meta[3])
+        s_out, _ = solver.advance(s_in, op.load.targets[s_in.increment])
+        for k in pinned_out:
+            pinned_out[k].copy_(getattr(s_out, k), non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+        host_state = {k: v.clone().pin_memory() for k, v in pinned_out.items()}
+        st_meta = (s_out.step, s_out.macro_strain, s_out.macro_stress, s_out.increment)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = args.steps * world / (float(te.item()) / 1e3)
+
+    # ---- dominant kernel: the elastic action (element kernel + node gather) ------------
+    x, d = state.x.contiguous(), state.d.contiguous()
+    for _ in range(3):
+        op.mech_action(x, d=d)
+    n_rep, ms = 20, 0.0
+    for _ in range(n_rep):
+        flush_l2(flush)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        op.mech_action(x, d=d)
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    apply_s = ms / n_rep / 1e3
+    alg_bytes = 7 * op.n_red * 8 + op.n_elements * 1  # read u~ 3n, d n; write 3n (FP64); slot id per voxel
+    peak, peak_src = peaks()
+    achieved = alg_bytes / apply_s / 1e9
+    traffic = profile_traffic()
+    mech = float(np.mean([c[0] for c in counts]))
+    pf = float(np.mean([c[1] for c in counts]))
+    stag = float(np.mean([c[2] for c in counts]))
+    dof_updates = (mech * op.n_mech + pf * op.n_red) * args.steps * world / (max_ms / 1e3)
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "config": workload_config(),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "h8 elastic action (element kernel + node gather), FP64",
+                     "algorithmic_bytes": alg_bytes, "launch_ms": apply_s * 1e3, "peak_source": peak_src},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "iterations_per_step": {"mech": mech, "pf": pf, "stagger": stag},
+        "dof_updates_per_s": dof_updates,
+    }
+    if world == 1 and rank == 0 and not args.no_cpu:
+        sec, sample = cpu_step_estimate({"mech": mech, "pf": pf, "stag": stag})
+        out["cpu_baseline"] = {"value": 1.0 / sec, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                               "sample": sample}
+    return out
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the elastic action from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "h8_mech_apply_64.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_apply:"):
+                    return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def run_reference(args, rank, world):
+    torch.set_num_threads(os.cpu_count() or 1)
+    times = []
+    sample = ""
+    for _ in range(args.warmup):
+        pass
+    for _ in range(max(1, min(args.steps, 2))):
+        sec, sample = cpu_step_estimate(REF_COUNTS)
+        times.append(sec)
+    sec = float(np.mean(times))
+    value = 1.0 / sec
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    if args.warmup + args.steps > INCREMENTS:
+        raise SystemExit(f"warmup + steps must not exceed the {INCREMENTS} increments of the load path")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, rank, world)), flush=True)
+        return
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=device)
+    try:
+        out = run_ours(args, rank, world, device)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+    finally:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,262 @@
+/*
+ * phastb.h -- C ABI of the B200 backend for PhAST's matrix-free phase-field
+ * hot path (structured Q4 grids in 2D, periodic voxel H8 cells in 3D).
+ *
+ * Conventions
+ *   - Every entry point returns an int status (PHASTB_OK on success) and never
+ *     throws or traps.  Device errors surface as PHASTB_ERR_CUDA.
+ *   - Pointers named d_* / arrays are DEVICE pointers unless stated otherwise;
+ *     they are caller-owned.  `stream` is a cudaStream_t (NULL = legacy stream).
+ *   - Field layouts follow PhAST: 2D u/v/a (N,2) node-major, d (N,), Gauss
+ *     fields (E,4); 3D x = [u~ (3 n_red), E (6)], d (n_red,), Gauss fields (E,8).
+ *     Node and element numbering are those of structured_q4_mesh and of
+ *     PeriodicVoxelMap (x fastest).
+ *   - `dtype` selects the storage/arithmetic type of the vectors: PHASTB_F64 or
+ *     PHASTB_F32.  Inner products, norms and reductions are always FP64.
+ *   - Scratch memory comes from a caller-provided workspace whose size is given
+ *     by the matching *_workspace_bytes function.
+ *
+ * Each declaration cites the PhAST function (src/phast/..., file:line) whose
+ * behaviour it reproduces.
+ */
+#ifndef PHASTB_H
+#define PHASTB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define PHASTB_OK 0
+#define PHASTB_ERR_ARG 1         /* bad shape/option (ValueError in PhAST)      */
+#define PHASTB_ERR_CUDA 2        /* CUDA runtime error                           */
+#define PHASTB_NONCONVERGED 3    /* iteration cap reached                        */
+#define PHASTB_DIVERGED 4        /* residual grew past the divergence guard      */
+#define PHASTB_BREAKDOWN 5       /* non-positive curvature / non-SPD             */
+#define PHASTB_NONFINITE 6       /* NaN/Inf met                                  */
+#define PHASTB_ERR_WORKSPACE 7   /* workspace too small                          */
+#define PHASTB_UNSUPPORTED 8     /* option not implemented (NotImplementedError) */
+
+#define PHASTB_F64 0
+#define PHASTB_F32 1
+
+/* energy splits of the 2D operators (fem_operators.py:283-560, 951-1161) */
+#define PHASTB_SPLIT_LINEAR 0          /* undegraded C eps (internal_force_linear) */
+#define PHASTB_SPLIT_ISOTROPIC 1
+#define PHASTB_SPLIT_AMOR 2
+#define PHASTB_SPLIT_SPECTRAL 3        /* strain-spectral, algebraic projector     */
+#define PHASTB_SPLIT_STAR_CONVEX 4
+#define PHASTB_SPLIT_SPECTRAL_STRESS 5
+
+/* --------------------------------------------------------------- 2D (Q4) */
+typedef struct {
+  int nx, ny;        /* elements along x and y (structured_q4_mesh, quad_elements.py:458) */
+  double hx, hy;     /* element edge lengths */
+} phastb_q4_grid;
+
+typedef struct {
+  double E, nu;
+  double lam;          /* Material.lam (plane-stress reduced when plane_stress) */
+  double mu;           /* Material.mu */
+  double kappa;        /* Material.kappa, the 3D bulk modulus */
+  double eta;          /* eta_residual of g(d) = (1-d)^2 (1-eta) + eta */
+  double spectral_eps; /* FEMOperators._spectral_eps */
+  int plane_stress;
+  int stress_split;    /* PHASTB_SPLIT_* of effective_stress_split() */
+  int psi_split;       /* PHASTB_SPLIT_* of energy_split (history driver) */
+} phastb_q4_material;
+
+/* Strain at the 2x2 Gauss points, three (E,4) arrays.
+ * FEMOperators._compute_strain_q4, core/fem_operators.py:244-254 */
+int phastb_q4_strain(const phastb_q4_grid* g, int dtype, const void* u, void* exx, void* eyy,
+                     void* gxy, void* stream);
+
+/* Degraded internal force f (N,2); d == NULL gives the undegraded linear force.
+ * FEMOperators.internal_force / internal_force_linear, fem_operators.py:598-612,655-659 */
+int phastb_q4_internal_force(const phastb_q4_grid* g, const phastb_q4_material* m, int dtype,
+                             const void* u, const void* d, void* f, void* stream);
+
+/* Jacobi diagonal (N,2) of K(d); d == NULL means g = 1.
+ * FEMOperators.stiffness_diagonal, fem_operators.py:1284-1320 */
+int phastb_q4_stiffness_diagonal(const phastb_q4_grid* g, const phastb_q4_material* m, int dtype,
+                                 const void* d, void* diag, void* stream);
+
+/* psi+ at Gauss points and the history max H_out = max(H_in, psi+), (E,4) each.
+ * Any of H_in/H_out/psi may be NULL (H_in NULL means H_in = 0).
+ * compute_psi_plus fem_operators.py:951-1161 + StaggeredSolver._H_update
+ * staggered_solver.py:804-845 (hard_max, h_update.py:47-49) */
+int phastb_q4_psi_history(const phastb_q4_grid* g, const phastb_q4_material* m, int dtype,
+                          const void* u, const void* H_in, void* H_out, void* psi, void* stream);
+
+/* AT2 damage operator y = Gc l0 K d + M(rho) d with Gauss reaction density
+ * rho_q = rd_scale * Hq + (rd_shift_e ? rd_shift_e[e] : rd_shift) and Laplacian weight
+ * (gcl0_e ? gcl0_e[e] : gcl0).  Always FP64.
+ * PhaseFieldDamageSolver._Ax_q4, solvers/damage_solver.py:1797-1838 */
+int phastb_q4_damage_apply(const phastb_q4_grid* g, const double* d, const double* Hq,
+                           double rd_scale, double rd_shift, const double* rd_shift_e, double gcl0,
+                           const double* gcl0_e, double* y, void* stream);
+
+/* Right-hand side b = sum_q N 2 H_q w and Jacobi inverse M_inv = 1/(diag + 1e-30).
+ * _prepare_cg_q4, damage_solver.py:2270-2301 */
+int phastb_q4_damage_prepare(const phastb_q4_grid* g, const double* Hq, double gc_over_l0,
+                             const double* gc_over_l0_e, double gcl0, const double* gcl0_e,
+                             double* b, double* m_inv, void* stream);
+
+/* Bound-projected PCG damage solve, d in [d_prev, 1] with optional pinned nodes.
+ * d_init NULL starts from d_prev.  fixed (N,) uint8 and fixed_vals may be NULL.
+ * info[0] = last_iter, info[1] = reason (0 converged, 1 max_iter, 2 non-SPD, 3 diverged).
+ * PhaseFieldDamageSolver._solve_projected_cg, damage_solver.py:3528-3775 */
+size_t phastb_q4_damage_solve_workspace_bytes(int n_nodes);
+int phastb_q4_damage_solve(const phastb_q4_grid* g, const double* Hq, double gc_over_l0,
+                           const double* gc_over_l0_e, double gcl0, const double* gcl0_e,
+                           const double* d_prev, const double* d_init, const uint8_t* fixed,
+                           const double* fixed_vals, double tol, int max_iter, int check_every,
+                           double* d_out, int* info, void* workspace, size_t workspace_bytes,
+                           void* stream);
+
+/* One central-difference step, fused: predictor, f_int(u_new, d), corrector,
+ * Dirichlet zeroing; optionally the history update H_out = max(H_in, psi+(u_new)).
+ * m_inv (N,) = 1/(rho M + 1e-30) per node; bc_mask (N,2) uint8.
+ * ExplicitDynamics.step, mechanics_solver.py:153-239 (+ step_compute_driving_force) */
+int phastb_q4_explicit_step(const phastb_q4_grid* g, const phastb_q4_material* m, int dtype,
+                            double dt, const void* m_inv, const void* u, const void* v,
+                            const void* a, const void* d, const void* f_ext, const uint8_t* bc_mask,
+                            const void* bc_vals, void* u_out, void* v_out, void* a_out,
+                            const void* H_in, void* H_out, void* stream);
+
+/* Energy sums (FP64): out[0] elastic, out[1] fracture surface term d^T M d,
+ * out[2] gradient term d^T K d, out[3] kinetic sum_i |v_i|^2 M_i (v may be NULL).
+ * compute_energy_components, fem_operators.py:1430-1496 (caller scales by Gc etc.) */
+int phastb_q4_energy_sums(const phastb_q4_grid* g, const phastb_q4_material* m, const double* u,
+                          const double* d, const double* v, double* out_host, void* workspace,
+                          size_t workspace_bytes, void* stream);
+
+/* Size of the small reduction workspace used by the *_sums / *_change entry points. */
+size_t phastb_reduce_workspace_bytes(void);
+
+/* Reaction sum_{i in nodes} f_int[i, comp] (- f_ext[i, comp]), FP64, host result.
+ * compute_reaction_force, fem_operators.py:1502-1530 */
+int phastb_q4_reaction(const phastb_q4_grid* g, const phastb_q4_material* m, const double* u,
+                       const double* d, const int64_t* nodes, int n_nodes_sel, int comp,
+                       const double* f_ext, double* out_host, void* workspace,
+                       size_t workspace_bytes, void* stream);
+size_t phastb_q4_reaction_workspace_bytes(int n_nodes);
+
+/* Quasi-static Newton with matrix-free CG on K(d) du = r (isotropic split).
+ * QuasiStaticSolver.solve / _cg_solve / _accept_newton_step,
+ * mechanics_solver.py:1597-1831, 1984-2043.  info[0] = Newton iterations,
+ * info[1] = converged, info[2] = total CG iterations. */
+size_t phastb_q4_qs_workspace_bytes(int n_nodes);
+int phastb_q4_qs_solve(const phastb_q4_grid* g, const phastb_q4_material* m, const double* d,
+                       const double* f_ext, const uint8_t* bc_mask, const double* bc_vals,
+                       double* u, double tol, double cg_tol, int cg_max_iter, int max_iter,
+                       int line_search, int ls_max_steps, double ls_min_alpha, double ls_c,
+                       int* info, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ----------------------------------------------------- 3D (periodic H8) */
+#define PHASTB_MAX_SLOTS 8
+#define PHASTB_DRIVER_NONE 0
+#define PHASTB_DRIVER_FULL 1
+#define PHASTB_DRIVER_SPECTRAL 2
+
+typedef struct {
+  int nx, ny, nz;          /* voxels per axis (VoxelGrid.shape) */
+  int px, py, pz;          /* periodic flags */
+  double hx, hy, hz;       /* voxel size */
+} phastb_voxel_grid;
+
+typedef struct {
+  int n_slots;                           /* material slots (<= PHASTB_MAX_SLOTS) */
+  int isotropic;                         /* every slot isotropic: C from lam, mu */
+  double C[PHASTB_MAX_SLOTS][36];        /* engineering-Voigt stiffness per slot */
+  double lam[PHASTB_MAX_SLOTS], mu[PHASTB_MAX_SLOTS], Gc[PHASTB_MAX_SLOTS];
+  int driver[PHASTB_MAX_SLOTS];          /* PHASTB_DRIVER_* */
+  double kappa;                          /* residual stiffness of g */
+  double ell;                            /* phase-field length */
+} phastb_voxel_material;
+
+/* Element scratch for the element->node gather: 24 values per element. */
+size_t phastb_h8_scratch_bytes(const phastb_voxel_grid* g, int dtype);
+
+/* g (E,8) = (1-kappa)(1-d_q)^2 + kappa.  operator.py:939-946, splits.py:56-59 */
+int phastb_h8_degradation(const phastb_voxel_grid* g, int dtype, const void* d, double kappa,
+                          void* g_out, void* stream);
+
+/* y = [P^T sum_q w B^T g C (B u~ + E), sum w g C eps]; gq (E,8) or, when NULL, g from
+ * d (n_red) (d NULL too: g = 1).  mask (n_mech,) uint8 zeroes fixed rows (NULL: none).
+ * mech_action / _stress_pass, solid3d/operator.py:1108-1194 */
+int phastb_h8_mech_apply(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                         int dtype, const void* x, const void* gq, const void* d, const uint8_t* mask,
+                         void* y, void* scratch, void* stream);
+
+/* Jacobi diagonal of A(g).  mech_diagonal, operator.py:1196-1254 */
+int phastb_h8_mech_diagonal(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                            const uint8_t* slot, int dtype, const void* gq, const void* d, void* diag,
+                            void* scratch, void* stream);
+
+/* r_E (6) and elastic energy, FP64 host results.  macro_stress/elastic_energy,
+ * operator.py:1303-1340 */
+int phastb_h8_stress_energy(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                            const uint8_t* slot, const double* x, const double* gq, const double* d,
+                            double* rE_host, double* energy_host, void* scratch, void* stream);
+
+/* Y (E,8) undamaged driving energy and H_out = max(H_prev, Y) (either output NULL).
+ * driving_force operator.py:1415-1444, spectral_tensile_energy splits.py:146-161,
+ * history max staggered.py:1302 */
+int phastb_h8_driving_history(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                              const uint8_t* slot, const double* x, const double* H_prev,
+                              double* Y, double* H_out, void* stream);
+
+/* scale * [Gc_e (M/ell + ell L) d + 2(1-kappa) sum_q w H_q N_q N_q^T d]; H NULL drops
+ * the history term.  damage_action, operator.py:1450-1466 */
+int phastb_h8_damage_apply(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                           const uint8_t* slot, const double* d, const double* H, double scale,
+                           double* y, void* scratch, void* stream);
+
+/* scale * rhs and scale * Jacobi diagonal.  damage_rhs/damage_diagonal, operator.py:1468-1493 */
+int phastb_h8_damage_rhs_diag(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                              const uint8_t* slot, const double* H, double scale, double* rhs,
+                              double* diag, void* scratch, void* stream);
+
+/* Constrained Jacobi-PCG mechanics solve at fixed damage (g from d, or gq).
+ * solve_constrained + pcg, solid3d/linalg.py:99-287.
+ * info[0] iterations, info[1] converged; rinfo[0] ||b_f||, rinfo[1] ||r||. */
+size_t phastb_h8_mech_solve_workspace_bytes(const phastb_voxel_grid* g, int dtype);
+int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                         const uint8_t* slot, const double* gq, const double* d,
+                         const uint8_t* fixed, const double* fixed_values, const double* x0,
+                         double rtol, double atol, int maxiter, int check_every, double* x_out,
+                         int* info, double* rinfo, void* workspace, size_t workspace_bytes,
+                         void* stream);
+
+/* Box-constrained damage solve lower <= d <= upper by the primal active-set method
+ * with a Dirichlet PCG per set (scale applied to the system).
+ * solve_h8_scalar_box_kkt + solve_h8_scalar_dirichlet_pcg, solvers/box_kkt_h8.py:256-778.
+ * info[0] total PCG iterations, info[1] active-set iterations, info[2] kkt_ok. */
+size_t phastb_h8_box_kkt_workspace_bytes(const phastb_voxel_grid* g);
+int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                             const uint8_t* slot, const double* H, double scale, const double* lower,
+                             double upper, const double* initial, double lin_tol, double kkt_tol,
+                             int max_lin, int max_active, double* d_out, int* info, void* workspace,
+                             size_t workspace_bytes, void* stream);
+
+/* Staggered change parts out[0..4] = ||du~||, ||u~||, max|dE|, max|E|, max|dd| (FP64, host).
+ * StaggeredSolver._change, solid3d/staggered.py:1097-1124 */
+int phastb_h8_stagger_change(int n_u, const double* x_new, const double* x_old, int n_d,
+                             const double* d_new, const double* d_old, double* out_host,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/* Library version string (host pointer). */
+const char* phastb_version(void);
+
+/* Number of kernel launches this library has issued in the process (host counter). */
+long long phastb_launch_count(void);
+void phastb_launch_count_reset(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PHASTB_H */

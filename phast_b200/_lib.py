@@ -1,0 +1,171 @@
+"""ctypes binding of the C ABI in ``include/phastb.h`` (``phast_b200/_lib/libphastb.so``).
+
+The library is the product: every operator and solver in this package calls it.
+There is no CPU or PyTorch fallback -- if the library is missing, loading raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libphastb.so")
+
+OK, ERR_ARG, ERR_CUDA, NONCONVERGED, DIVERGED, BREAKDOWN, NONFINITE, ERR_WORKSPACE, UNSUPPORTED = range(9)
+F64, F32 = 0, 1
+SPLITS = {"linear": 0, "isotropic": 1, "amor": 2, "spectral": 3, "star_convex": 4, "spectral_stress": 5}
+DRIVER_NONE, DRIVER_FULL, DRIVER_SPECTRAL = 0, 1, 2
+MAX_SLOTS = 8
+
+vp, ip, dp, sz = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_size_t
+
+
+class Q4Grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("hx", C.c_double), ("hy", C.c_double)]
+
+
+class Q4Material(C.Structure):
+    _fields_ = [("E", C.c_double), ("nu", C.c_double), ("lam", C.c_double), ("mu", C.c_double),
+                ("kappa", C.c_double), ("eta", C.c_double), ("spectral_eps", C.c_double),
+                ("plane_stress", C.c_int), ("stress_split", C.c_int), ("psi_split", C.c_int)]
+
+
+class VoxelGrid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("px", C.c_int), ("py", C.c_int),
+                ("pz", C.c_int), ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double)]
+
+
+class VoxelMaterial(C.Structure):
+    _fields_ = [("n_slots", C.c_int), ("isotropic", C.c_int), ("C", (C.c_double * 36) * MAX_SLOTS),
+                ("lam", C.c_double * MAX_SLOTS), ("mu", C.c_double * MAX_SLOTS), ("Gc", C.c_double * MAX_SLOTS),
+                ("driver", C.c_int * MAX_SLOTS), ("kappa", C.c_double), ("ell", C.c_double)]
+
+
+Q4G, Q4M, VG, VM = C.POINTER(Q4Grid), C.POINTER(Q4Material), C.POINTER(VoxelGrid), C.POINTER(VoxelMaterial)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "phastb_version": (C.c_char_p, []),
+    "phastb_launch_count": (C.c_longlong, []),
+    "phastb_launch_count_reset": (None, []),
+    "phastb_reduce_workspace_bytes": (sz, []),
+    "phastb_q4_strain": (C.c_int, [Q4G, C.c_int, vp, vp, vp, vp, vp]),
+    "phastb_q4_internal_force": (C.c_int, [Q4G, Q4M, C.c_int, vp, vp, vp, vp]),
+    "phastb_q4_stiffness_diagonal": (C.c_int, [Q4G, Q4M, C.c_int, vp, vp, vp]),
+    "phastb_q4_psi_history": (C.c_int, [Q4G, Q4M, C.c_int, vp, vp, vp, vp, vp]),
+    "phastb_q4_damage_apply": (C.c_int, [Q4G, vp, vp, C.c_double, C.c_double, vp, C.c_double, vp, vp, vp]),
+    "phastb_q4_damage_prepare": (C.c_int, [Q4G, vp, C.c_double, vp, C.c_double, vp, vp, vp, vp]),
+    "phastb_q4_damage_solve_workspace_bytes": (sz, [C.c_int]),
+    "phastb_q4_damage_solve": (C.c_int, [Q4G, vp, C.c_double, vp, C.c_double, vp, vp, vp, vp, vp, C.c_double,
+                                         C.c_int, C.c_int, vp, ip, vp, sz, vp]),
+    "phastb_q4_explicit_step": (C.c_int, [Q4G, Q4M, C.c_int, C.c_double, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                          vp, vp, vp, vp]),
+    "phastb_q4_energy_sums": (C.c_int, [Q4G, Q4M, vp, vp, vp, dp, vp, sz, vp]),
+    "phastb_q4_reaction_workspace_bytes": (sz, [C.c_int]),
+    "phastb_q4_reaction": (C.c_int, [Q4G, Q4M, vp, vp, vp, C.c_int, C.c_int, vp, dp, vp, sz, vp]),
+    "phastb_q4_qs_workspace_bytes": (sz, [C.c_int]),
+    "phastb_q4_qs_solve": (C.c_int, [Q4G, Q4M, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_int,
+                                     C.c_int, C.c_int, C.c_double, C.c_double, ip, vp, sz, vp]),
+    "phastb_h8_scratch_bytes": (sz, [VG, C.c_int]),
+    "phastb_h8_degradation": (C.c_int, [VG, C.c_int, vp, C.c_double, vp, vp]),
+    "phastb_h8_mech_apply": (C.c_int, [VG, VM, vp, C.c_int, vp, vp, vp, vp, vp, vp, vp]),
+    "phastb_h8_mech_diagonal": (C.c_int, [VG, VM, vp, C.c_int, vp, vp, vp, vp, vp]),
+    "phastb_h8_stress_energy": (C.c_int, [VG, VM, vp, vp, vp, vp, dp, dp, vp, vp]),
+    "phastb_h8_driving_history": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, vp]),
+    "phastb_h8_damage_apply": (C.c_int, [VG, VM, vp, vp, vp, C.c_double, vp, vp, vp]),
+    "phastb_h8_damage_rhs_diag": (C.c_int, [VG, VM, vp, vp, C.c_double, vp, vp, vp, vp]),
+    "phastb_h8_mech_solve_workspace_bytes": (sz, [VG, C.c_int]),
+    "phastb_h8_mech_solve": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_int,
+                                       vp, ip, dp, vp, sz, vp]),
+    "phastb_h8_box_kkt_workspace_bytes": (sz, [VG]),
+    "phastb_h8_damage_box_kkt": (C.c_int, [VG, VM, vp, vp, C.c_double, vp, C.c_double, vp, C.c_double, C.c_double,
+                                           C.c_int, C.c_int, vp, ip, vp, sz, vp]),
+    "phastb_h8_stagger_change": (C.c_int, [C.c_int, vp, vp, C.c_int, vp, vp, dp, vp, sz, vp]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load():
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"phast_b200 CUDA library not found at {LIB_PATH}; build it with "
+                    "`python -m phast_b200.build` (needs nvcc)")
+            lib = C.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+        return _lib
+
+
+class PhastbError(RuntimeError):
+    def __init__(self, fn, status):
+        super().__init__(f"{fn} failed with status {status}")
+        self.status = status
+
+
+def check(status, fn):
+    """Map a C-ABI status to PhAST's exception contract."""
+    if status == OK:
+        return
+    if status == ERR_ARG:
+        raise ValueError(f"{fn}: invalid argument")
+    if status == UNSUPPORTED:
+        raise NotImplementedError(f"{fn}: option not implemented by the B200 backend")
+    raise PhastbError(fn, status)
+
+
+def call(name, *args):
+    """Call an entry point and raise on any non-OK status."""
+    st = getattr(load(), name)(*args)
+    check(st, name)
+    return st
+
+
+def raw(name, *args):
+    """Call an entry point and return its status (solvers report convergence this way)."""
+    return getattr(load(), name)(*args)
+
+
+def ptr(t):
+    """Device pointer of a contiguous tensor (or None)."""
+    if t is None:
+        return None
+    if not t.is_contiguous():
+        raise ValueError("phast_b200 kernels need contiguous tensors")
+    if t.data_ptr() % 16:
+        raise ValueError("phast_b200 kernels need 16-byte aligned tensors (vectorised loads)")
+    return C.c_void_p(t.data_ptr())
+
+
+def stream(device=None):
+    return C.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def require_cuda(t, name="tensor"):
+    if not (isinstance(t, torch.Tensor) and t.is_cuda):
+        raise ValueError(f"{name} must be a CUDA tensor: the B200 backend has no CPU path")
+
+
+class Workspace:
+    """Grow-only device scratch buffer reused across calls (caller-owned memory for the C ABI)."""
+
+    def __init__(self, device):
+        self.device = torch.device(device)
+        self.buf = None
+
+    def get(self, nbytes):
+        nbytes = int(nbytes)
+        if self.buf is None or self.buf.numel() < nbytes:
+            self.buf = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=self.device)
+        return C.c_void_p(self.buf.data_ptr()), C.c_size_t(self.buf.numel())

@@ -1,0 +1,132 @@
+// Shared device helpers for the phase-field kernels (sm_100a).
+//
+// Reductions are deterministic: every reducing kernel writes one partial per
+// block, and the last block to finish (ticket counter) folds the partials in
+// a fixed order.  Grid sizes depend only on the problem size, so the same
+// inputs always give the same bits.  No floating-point atomics are used.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+
+#include "../../include/phastb.h"
+
+namespace phastb {
+
+constexpr int kThreads = 256;        // block size of every vector/reduction kernel
+constexpr int kMaxBlocks = 148 * 8;  // 8 resident blocks per SM on 148 SMs
+constexpr int kMaxPartials = kMaxBlocks;
+
+inline int grid_for(long long n, int threads = kThreads) {
+  long long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > kMaxBlocks) b = kMaxBlocks;
+  return static_cast<int>(b);
+}
+
+inline int grid_full(long long n, int threads = kThreads) {
+  long long b = (n + threads - 1) / threads;
+  return static_cast<int>(b < 1 ? 1 : b);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ int warp_or(int v) {
+  return __any_sync(0xffffffffu, v) ? 1 : 0;
+}
+
+// Sum over a block of kThreads threads; result valid in every thread.
+// `sh` must hold kThreads/32 doubles.
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double t = (l < (blockDim.x >> 5)) ? sh[l] : 0.0;
+  t = warp_sum(t);
+  return t;
+}
+
+__device__ __forceinline__ double block_min(double v, double* sh) {
+  v = warp_min(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double t = (l < (blockDim.x >> 5)) ? sh[l] : INFINITY;
+  t = warp_min(t);
+  return t;
+}
+
+__device__ __forceinline__ double block_max(double v, double* sh) { return -block_min(-v, sh); }
+
+__device__ __forceinline__ int block_or(int v, int* sh) {
+  v = warp_or(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  int t = (l < (blockDim.x >> 5)) ? sh[l] : 0;
+  return warp_or(t);
+}
+
+// Returns true in every thread of the last block to arrive.  The caller has
+// already written its per-block partials; the fence publishes them.
+__device__ __forceinline__ bool arrive_last(unsigned int* counter) {
+  __shared__ unsigned int s_ticket;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_ticket = atomicAdd(counter, 1u);
+  __syncthreads();
+  const bool last = (s_ticket == gridDim.x - 1);
+  if (last) __threadfence();
+  return last;
+}
+
+// Fold `n` partials (global) in a fixed order inside the last block.
+__device__ __forceinline__ double fold_sum(const double* part, int n, double* sh) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += __ldcg(part + i);
+  return block_sum(v, sh);
+}
+
+__device__ __forceinline__ double fold_min(const double* part, int n, double* sh) {
+  double v = INFINITY;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v = fmin(v, __ldcg(part + i));
+  return block_min(v, sh);
+}
+
+__device__ __forceinline__ double fold_max(const double* part, int n, double* sh) {
+  double v = -INFINITY;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v = fmax(v, __ldcg(part + i));
+  return block_max(v, sh);
+}
+
+__device__ __forceinline__ int fold_or(const int* part, int n, int* sh) {
+  int v = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v |= __ldcg(part + i);
+  return block_or(v, sh);
+}
+
+template <typename T> __device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
+
+// Host-side count of kernel launches issued by this library (every launch site
+// is wrapped as `{ note_launch(); kernel<<<...>>>(...); }`).
+void note_launch();
+
+inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? PHASTB_OK : PHASTB_ERR_CUDA; }
+
+inline int last_launch_status() { return cuda_status(cudaGetLastError()); }
+
+}  // namespace phastb

@@ -1,0 +1,116 @@
+// Device-resident Krylov engines.
+//
+// The iteration state (alpha, beta, residual norms, flags) lives in device
+// memory; every kernel reads it and turns into a no-op once the solve is
+// finished, so the host can launch a whole chunk of iterations without
+// looking at any scalar and synchronise only once per chunk.  Reductions are
+// the deterministic last-block folds of common.cuh.
+//
+//   Ppcg   - bound-projected PCG of PhaseFieldDamageSolver._solve_projected_cg
+//            (solvers/damage_solver.py:3528-3775)
+//   Pcg    - Jacobi PCG with device flags of solid3d/linalg.py:pcg (freeze on
+//            convergence, :99-220), of box_kkt_h8._pcg (:256-347, strict
+//            curvature checks) and the unpreconditioned CG of
+//            QuasiStaticSolver._cg_solve (mechanics_solver.py:1984-2043,
+//            convergence looked at every 50 iterations).
+#pragma once
+#include "reduce.cuh"
+
+namespace phastb {
+
+// A linear operator y = A x on device vectors.  `guard` (device int, may be
+// NULL) lets the operator skip work when the engine has finished.
+template <typename T>
+struct LinOp {
+  int (*apply)(const void* ctx, const T* x, T* y, const int* guard, cudaStream_t s);
+  const void* ctx;
+  int operator()(const T* x, T* y, const int* guard, cudaStream_t s) const { return apply(ctx, x, y, guard, s); }
+};
+
+// ---------------------------------------------------------------- PPCG
+
+struct PpcgState {
+  double rz, tol_sq, r0sq, alpha, beta;
+  int go;          // iterating
+  int go_resid;    // this iteration recomputes the true residual
+  int done, reason, iter, last_iter;
+  int branch;      // 0 full CG step, 1 capped step + restart
+  int reset_dir;
+  int max_iter, check_every;
+};
+
+struct PpcgWs {
+  double *r, *z, *p, *Ap, *Ad, *lb, *minv, *b;
+  uint8_t* act;
+  double* part;      // 4 * kMaxPartials
+  int* ipart;        // kMaxPartials
+  unsigned* counter; // 4 tickets
+  PpcgState* st;
+};
+
+size_t ppcg_ws_bytes(int n);
+PpcgWs ppcg_ws(void* base, int n);
+
+// Runs the solve; `d` holds the iterate (initialised from d_init or d_prev) and
+// receives the clamped result.  Returns a PHASTB status; info[0] last_iter,
+// info[1] reason.
+int ppcg_solve(const LinOp<double>& A, int n, const PpcgWs& w, const double* d_prev, const double* d_init,
+               const uint8_t* fixed, const double* vals, double tol, int max_iter, int check_every, double* d,
+               int* info, cudaStream_t s);
+
+// ---------------------------------------------------------------- PCG
+
+enum PcgMode { PCG_FREEZE = 0, PCG_STRICT = 1, PCG_PERIODIC = 2 };
+
+struct PcgState {
+  double rz, rr, rr0, thr_sq, alpha, beta;
+  int active;       // iterating (guard for the operator)
+  int breakdown, nonfinite;
+  int steps;        // iterations that moved the iterate
+  int iter;
+  int converged;
+};
+
+template <typename T>
+struct PcgWs {
+  T *r, *z, *p, *Ap;
+  double* part;
+  unsigned* counter;
+  PcgState* st;
+};
+
+template <typename T>
+size_t pcg_ws_bytes(int n);
+template <typename T>
+PcgWs<T> pcg_ws(void* base, int n);
+
+// Preconditioner z = M^{-1} r (NULL ctx: Jacobi with inv_diag, or identity
+// when inv_diag is NULL).
+template <typename T>
+struct Precond {
+  int (*apply)(const void* ctx, const T* r, T* z, const int* guard, cudaStream_t s);
+  const void* ctx;
+};
+
+// Solves A x = b from x (initial guess held in x, zero allowed).  The caller
+// has formed r = b - A x in w.r beforehand when `have_r` is set; otherwise the
+// engine forms it.  thr is the absolute residual threshold on ||r||.
+// iters/converged/breakdown/nonfinite are reported through `out`.
+struct PcgResult {
+  int iterations;
+  int converged;
+  int breakdown;
+  int nonfinite;
+  double rnorm;
+};
+
+template <typename T>
+int pcg_run(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T* inv_diag, const Precond<T>* M,
+            T* x, double thr, int maxiter, int check_every, PcgMode mode, double rr0_for_div, PcgResult* out,
+            cudaStream_t s);
+
+// Vector helpers used by the drivers.
+template <typename T>
+int vec_norm2(const T* x, int n, double* host, void* red_ws_base, cudaStream_t s);
+
+}  // namespace phastb

@@ -1,0 +1,646 @@
+// Periodic voxel H8 operators: degradation, elastic action and diagonal,
+// driving force + history, AT2 damage action / rhs / diagonal.
+// C ABI in include/phastb.h.
+#include "h8_kernels.cuh"
+#include "reduce.cuh"
+
+#include <cmath>
+
+namespace phastb {
+
+template <typename T>
+__device__ __forceinline__ T g_of(T kappa, T d) {
+  const T o = T(1) - d;
+  return (T(1) - kappa) * o * o + kappa;
+}
+
+__device__ __forceinline__ void elem_ijk(const VoxGeom& g, int e, int& ie, int& je, int& ke) {
+  ie = e % g.nx;
+  const int r = e / g.nx;
+  je = r % g.ny;
+  ke = r / g.ny;
+}
+
+// Gauss-point degradation factors of one element from gq (E,8), from nodal d or 1.
+template <typename T>
+__device__ __forceinline__ void load_g(const VoxGeom& g, const T* __restrict__ gq, const T* __restrict__ d,
+                                       T kappa, int e, const int* nd, T* gv) {
+  if (gq) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) gv[q] = __ldg(gq + 8 * (size_t)e + q);
+  } else if (d) {
+    T dd[8], dq[8];
+#pragma unroll
+    for (int L = 0; L < 8; ++L) dd[L] = __ldg(d + nd[L]);
+    interp_sf(dd, dq);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) gv[q] = g_of(kappa, dq[q]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) gv[q] = T(1);
+  }
+}
+
+// ------------------------------------------------------------ elastic action
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) h8_mech_elem_kernel(VoxGeom g, VoxMat<T> m,
+                                                                const uint8_t* __restrict__ slot,
+                                                                const T* __restrict__ x, const T* __restrict__ gq,
+                                                                const T* __restrict__ d, T* __restrict__ scratch,
+                                                                T* __restrict__ y, const uint8_t* __restrict__ mask,
+                                                                RedWs ws, const int* guard) {
+  if (guard && *guard == 0) return;
+  const T ihx = T(1.0 / g.hx), ihy = T(1.0 / g.hy), ihz = T(1.0 / g.hz), w = T(g.w);
+  const size_t E = (size_t)g.n_elem;
+  const T* Ex = x + 3 * (size_t)g.n_red;
+  const T E6[6] = {__ldg(Ex), __ldg(Ex + 1), __ldg(Ex + 2), __ldg(Ex + 3), __ldg(Ex + 4), __ldg(Ex + 5)};
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.n_elem; e += gridDim.x * blockDim.x) {
+    int ie, je, ke;
+    elem_ijk(g, e, ie, je, ke);
+    int nd[8];
+    vox_corners(g, ie, je, ke, nd);
+    T gv[8];
+    load_g(g, gq, d, m.kappa, e, nd, gv);
+    const int s = slot[e];
+    T D[3][3][2][2];  // [component][axis][..][..]
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      T u[8];
+#pragma unroll
+      for (int L = 0; L < 8; ++L) u[L] = __ldg(x + 3 * (size_t)nd[L] + c);
+      grad_sf(u, ihx, ihy, ihz, D[c][0], D[c][1], D[c][2]);
+    }
+    T P[3][3][2][2];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) P[c][a][i][j] = T(0);
+#pragma unroll
+    for (int qz = 0; qz < 2; ++qz)
+#pragma unroll
+      for (int qy = 0; qy < 2; ++qy)
+#pragma unroll
+        for (int qx = 0; qx < 2; ++qx) {
+          T ep[6];
+          ep[0] = D[0][0][qz][qy] + E6[0];
+          ep[1] = D[1][1][qz][qx] + E6[1];
+          ep[2] = D[2][2][qy][qx] + E6[2];
+          ep[3] = D[1][2][qy][qx] + D[2][1][qz][qx] + E6[3];
+          ep[4] = D[0][2][qy][qx] + D[2][0][qz][qy] + E6[4];
+          ep[5] = D[0][1][qz][qx] + D[1][0][qz][qy] + E6[5];
+          T sg[6];
+          voigt_stress(m, s, ep, sg);
+          const T gw = gv[qx + 2 * qy + 4 * qz] * w;
+#pragma unroll
+          for (int k = 0; k < 6; ++k) sg[k] *= gw;
+#pragma unroll
+          for (int k = 0; k < 6; ++k) {
+            acc[k] += double(sg[k]);
+            acc[6] += 0.5 * double(sg[k]) * double(ep[k]);
+          }
+          P[0][0][qz][qy] += sg[0];
+          P[0][1][qz][qx] += sg[5];
+          P[0][2][qy][qx] += sg[4];
+          P[1][0][qz][qy] += sg[5];
+          P[1][1][qz][qx] += sg[1];
+          P[1][2][qy][qx] += sg[3];
+          P[2][0][qz][qy] += sg[4];
+          P[2][1][qz][qx] += sg[3];
+          P[2][2][qy][qx] += sg[2];
+        }
+    if (scratch) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        T out[8];
+        grad_sf_t(P[c][0], P[c][1], P[c][2], ihx, ihy, ihz, out);
+#pragma unroll
+        for (int L = 0; L < 8; ++L) scratch[(size_t)(L * 3 + c) * E + e] = out[L];
+      }
+    }
+  }
+  __shared__ double sh[32];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+    const double sm = block_sum(acc[k], sh);
+    if (threadIdx.x == 0) ws.part[k * kMaxPartials + blockIdx.x] = sm;
+  }
+  if (arrive_last(ws.counter)) {
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+      const double t = fold_sum(ws.part + k * kMaxPartials, gridDim.x, sh);
+      if (threadIdx.x == 0) {
+        ws.out[k] = t;
+        if (y && k < 6) {
+          const size_t idx = 3 * (size_t)g.n_red + k;
+          y[idx] = (mask && mask[idx]) ? T(0) : T(t);
+        }
+      }
+    }
+    if (threadIdx.x == 0) *ws.counter = 0u;
+  }
+}
+
+// Deterministic element->node gather of NC components per node.
+template <typename T, int NC>
+__global__ void __launch_bounds__(kThreads) h8_gather_kernel(VoxGeom g, const T* __restrict__ scratch,
+                                                             T* __restrict__ y, const uint8_t* __restrict__ mask,
+                                                             const int* guard) {
+  if (guard && *guard == 0) return;
+  const size_t E = (size_t)g.n_elem;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < g.n_red; n += gridDim.x * blockDim.x) {
+    const int ir = n % g.rx;
+    const int rem = n / g.rx;
+    const int jr = rem % g.ry, kr = rem / g.ry;
+    T acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = T(0);
+#pragma unroll
+    for (int L = 0; L < 8; ++L) {
+      int ie = ir - (L & 1), je = jr - ((L >> 1) & 1), ke = kr - ((L >> 2) & 1);
+      if (g.px) { if (ie < 0) ie += g.nx; } else if (ie < 0 || ie >= g.nx) continue;
+      if (g.py) { if (je < 0) je += g.ny; } else if (je < 0 || je >= g.ny) continue;
+      if (g.pz) { if (ke < 0) ke += g.nz; } else if (ke < 0 || ke >= g.nz) continue;
+      const size_t e = (size_t)ie + (size_t)g.nx * ((size_t)je + (size_t)g.ny * ke);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[c] += __ldg(scratch + (size_t)(L * NC + c) * E + e);
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const size_t idx = (size_t)n * NC + c;
+      y[idx] = (mask && mask[idx]) ? T(0) : acc[c];
+    }
+  }
+}
+
+// ------------------------------------------------------------ elastic diagonal
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) h8_mdiag_elem_kernel(VoxGeom g, VoxMat<T> m,
+                                                                 const uint8_t* __restrict__ slot,
+                                                                 const T* __restrict__ gq, const T* __restrict__ d,
+                                                                 T* __restrict__ scratch, T* __restrict__ diag,
+                                                                 RedWs ws) {
+  const T ihx = T(1.0 / g.hx), ihy = T(1.0 / g.hy), ihz = T(1.0 / g.hz), w = T(g.w);
+  const size_t E = (size_t)g.n_elem;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.n_elem; e += gridDim.x * blockDim.x) {
+    int ie, je, ke;
+    elem_ijk(g, e, ie, je, ke);
+    int nd[8];
+    vox_corners(g, ie, je, ke, nd);
+    T gv[8];
+    load_g(g, gq, d, m.kappa, e, nd, gv);
+    const int s = slot[e];
+    T C[6][6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        const int a = i < j ? i : j, b = i < j ? j : i;
+        C[i][j] = m.C[s][a * 6 - a * (a - 1) / 2 + (b - a)];
+      }
+    T out[3][8];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int L = 0; L < 8; ++L) out[c][L] = T(0);
+    T gsum = 0;
+#pragma unroll 1
+    for (int q = 0; q < 8; ++q) {
+      const int qx = q & 1, qy = (q >> 1) & 1, qz = q >> 2;
+      const T gw = gv[q] * w;
+      gsum += gw;
+#pragma unroll
+      for (int L = 0; L < 8; ++L) {
+        const int ax = L & 1, ay = (L >> 1) & 1, az = L >> 2;
+        const T nx_ = (qx == ax) ? T(kC1) : T(kC2);
+        const T ny_ = (qy == ay) ? T(kC1) : T(kC2);
+        const T nz_ = (qz == az) ? T(kC1) : T(kC2);
+        const T gx = (ax ? ihx : -ihx) * ny_ * nz_;
+        const T gy = (ay ? ihy : -ihy) * nx_ * nz_;
+        const T gz = (az ? ihz : -ihz) * nx_ * ny_;
+        out[0][L] += gw * (C[0][0] * gx * gx + C[4][4] * gz * gz + C[5][5] * gy * gy +
+                           T(2) * (C[0][4] * gx * gz + C[0][5] * gx * gy + C[4][5] * gz * gy));
+        out[1][L] += gw * (C[1][1] * gy * gy + C[3][3] * gz * gz + C[5][5] * gx * gx +
+                           T(2) * (C[1][3] * gy * gz + C[1][5] * gy * gx + C[3][5] * gz * gx));
+        out[2][L] += gw * (C[2][2] * gz * gz + C[3][3] * gy * gy + C[4][4] * gx * gx +
+                           T(2) * (C[2][3] * gz * gy + C[2][4] * gz * gx + C[3][4] * gy * gx));
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc[k] += double(gsum) * double(C[k][k]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int L = 0; L < 8; ++L) scratch[(size_t)(L * 3 + c) * E + e] = out[c][L];
+  }
+  __shared__ double sh[32];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const double sm = block_sum(acc[k], sh);
+    if (threadIdx.x == 0) ws.part[k * kMaxPartials + blockIdx.x] = sm;
+  }
+  if (arrive_last(ws.counter)) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const double t = fold_sum(ws.part + k * kMaxPartials, gridDim.x, sh);
+      if (threadIdx.x == 0) diag[3 * (size_t)g.n_red + k] = T(t);
+    }
+    if (threadIdx.x == 0) *ws.counter = 0u;
+  }
+}
+
+// ------------------------------------------------------------ degradation
+
+template <typename T>
+__global__ void h8_degradation_kernel(VoxGeom g, const T* __restrict__ d, T kappa, T* __restrict__ gout) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.n_elem; e += gridDim.x * blockDim.x) {
+    int ie, je, ke;
+    elem_ijk(g, e, ie, je, ke);
+    int nd[8];
+    vox_corners(g, ie, je, ke, nd);
+    T gv[8];
+    load_g<T>(g, nullptr, d, kappa, e, nd, gv);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) gout[8 * (size_t)e + q] = gv[q];
+  }
+}
+
+// ------------------------------------------------------------ driving force
+
+// Ascending eigenvalues of a symmetric 3x3 tensor by the trigonometric
+// solution of the characteristic cubic (Smith 1961), as symmetric_eigvalsh_3x3
+// (solid3d/splits.py:93-125).
+__device__ __forceinline__ void eig3(double a11, double a22, double a33, double a12, double a13, double a23,
+                                     double* ev) {
+  const double q = (a11 + a22 + a33) / 3.0;
+  const double b11 = a11 - q, b22 = a22 - q, b33 = a33 - q;
+  const double p1 = a12 * a12 + a13 * a13 + a23 * a23;
+  const double p = sqrt((b11 * b11 + b22 * b22 + b33 * b33 + 2.0 * p1) / 6.0);
+  if (!(p > 2.2250738585072014e-308)) {
+    ev[0] = ev[1] = ev[2] = q;
+    return;
+  }
+  const double det = b11 * (b22 * b33 - a23 * a23) - a12 * (a12 * b33 - a23 * a13) + a13 * (a12 * a23 - b22 * a13);
+  double r = det / (2.0 * p * p * p);
+  r = fmin(fmax(r, -1.0), 1.0);
+  const double phi = acos(r) / 3.0;
+  const double big = q + 2.0 * p * cos(phi);
+  const double small = q + 2.0 * p * cos(phi + 2.0943951023931954923);  // 2 pi / 3
+  ev[0] = small;
+  ev[1] = 3.0 * q - big - small;
+  ev[2] = big;
+}
+
+__global__ void __launch_bounds__(kThreads) h8_driving_kernel(VoxGeom g, VoxMat<double> m,
+                                                              const uint8_t* __restrict__ slot,
+                                                              const double* __restrict__ x,
+                                                              const double* __restrict__ Hprev,
+                                                              double* __restrict__ Y, double* __restrict__ Hout) {
+  const double ihx = 1.0 / g.hx, ihy = 1.0 / g.hy, ihz = 1.0 / g.hz;
+  const double* Ex = x + 3 * (size_t)g.n_red;
+  const double E6[6] = {__ldg(Ex), __ldg(Ex + 1), __ldg(Ex + 2), __ldg(Ex + 3), __ldg(Ex + 4), __ldg(Ex + 5)};
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.n_elem; e += gridDim.x * blockDim.x) {
+    const int s = slot[e];
+    const int drv = m.driver[s];
+    double yq[8];
+    if (drv == PHASTB_DRIVER_NONE) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) yq[q] = 0.0;
+    } else {
+      int ie, je, ke;
+      elem_ijk(g, e, ie, je, ke);
+      int nd[8];
+      vox_corners(g, ie, je, ke, nd);
+      double D[3][3][2][2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double u[8];
+#pragma unroll
+        for (int L = 0; L < 8; ++L) u[L] = __ldg(x + 3 * (size_t)nd[L] + c);
+        grad_sf(u, ihx, ihy, ihz, D[c][0], D[c][1], D[c][2]);
+      }
+#pragma unroll
+      for (int qz = 0; qz < 2; ++qz)
+#pragma unroll
+        for (int qy = 0; qy < 2; ++qy)
+#pragma unroll
+          for (int qx = 0; qx < 2; ++qx) {
+            double ep[6];
+            ep[0] = D[0][0][qz][qy] + E6[0];
+            ep[1] = D[1][1][qz][qx] + E6[1];
+            ep[2] = D[2][2][qy][qx] + E6[2];
+            ep[3] = D[1][2][qy][qx] + D[2][1][qz][qx] + E6[3];
+            ep[4] = D[0][2][qy][qx] + D[2][0][qz][qy] + E6[4];
+            ep[5] = D[0][1][qz][qx] + D[1][0][qz][qy] + E6[5];
+            double val;
+            if (drv == PHASTB_DRIVER_FULL) {
+              double sg[6];
+              voigt_stress(m, s, ep, sg);
+              val = 0.0;
+#pragma unroll
+              for (int k = 0; k < 6; ++k) val += ep[k] * sg[k];
+              val *= 0.5;
+            } else {
+              double ev[3];
+              eig3(ep[0], ep[1], ep[2], 0.5 * ep[5], 0.5 * ep[4], 0.5 * ep[3], ev);
+              double trp = ep[0] + ep[1] + ep[2];
+              trp = trp > 0.0 ? trp : 0.0;
+              double sp = 0.0;
+#pragma unroll
+              for (int k = 0; k < 3; ++k) {
+                const double v = ev[k] > 0.0 ? ev[k] : 0.0;
+                sp += v * v;
+              }
+              val = 0.5 * m.lam[s] * trp * trp + m.mu[s] * sp;
+            }
+            yq[qx + 2 * qy + 4 * qz] = val;
+          }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const size_t k = 8 * (size_t)e + q;
+      if (Y) Y[k] = yq[q];
+      if (Hout) {
+        const double h = Hprev ? Hprev[k] : 0.0;
+        Hout[k] = yq[q] > h ? yq[q] : h;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ damage
+
+template <int MODE>  // 0 action, 1 rhs, 2 diagonal
+__global__ void __launch_bounds__(kThreads) h8_damage_elem_kernel(VoxGeom g, VoxMat<double> m,
+                                                                  const uint8_t* __restrict__ slot,
+                                                                  const double* __restrict__ d,
+                                                                  const double* __restrict__ H, double scale,
+                                                                  double kdiag, double* __restrict__ scratch,
+                                                                  const int* guard) {
+  if (guard && *guard == 0) return;
+  const double ihx = 1.0 / g.hx, ihy = 1.0 / g.hy, ihz = 1.0 / g.hz, w = g.w;
+  const double ch = 2.0 * (1.0 - m.kappa);
+  const double ell = m.ell;
+  const size_t E = (size_t)g.n_elem;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.n_elem; e += gridDim.x * blockDim.x) {
+    const double Gc = m.Gc[slot[e]];
+    double Hq[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) Hq[q] = H ? __ldg(H + 8 * (size_t)e + q) : 0.0;
+    double out[8];
+    if (MODE == 0) {
+      int ie, je, ke;
+      elem_ijk(g, e, ie, je, ke);
+      int nd[8];
+      vox_corners(g, ie, je, ke, nd);
+      double dd[8], dq[8];
+#pragma unroll
+      for (int L = 0; L < 8; ++L) dd[L] = __ldg(d + nd[L]);
+      interp_sf(dd, dq);
+      double mq[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) mq[q] = w * (Gc / ell + ch * Hq[q]) * dq[q];
+      interp_sf_t(mq, out);
+      double Dx[2][2], Dy[2][2], Dz[2][2];
+      grad_sf(dd, ihx, ihy, ihz, Dx, Dy, Dz);
+      const double k2 = 2.0 * w * Gc * ell;
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          Dx[i][j] *= k2;
+          Dy[i][j] *= k2;
+          Dz[i][j] *= k2;
+        }
+      double og[8];
+      grad_sf_t(Dx, Dy, Dz, ihx, ihy, ihz, og);
+#pragma unroll
+      for (int L = 0; L < 8; ++L) out[L] += og[L];
+    } else if (MODE == 1) {
+      double hq[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) hq[q] = ch * (Hq[q] * w);
+      interp_sf_t(hq, out);
+    } else {
+#pragma unroll
+      for (int L = 0; L < 8; ++L) {
+        double acc = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const double n = ((q & 1) == (L & 1) ? kC1 : kC2) * (((q >> 1) & 1) == ((L >> 1) & 1) ? kC1 : kC2) *
+                           ((q >> 2) == (L >> 2) ? kC1 : kC2);
+          acc += (Hq[q] * w) * (n * n);
+        }
+        out[L] = Gc * kdiag + ch * acc;
+      }
+    }
+#pragma unroll
+    for (int L = 0; L < 8; ++L) scratch[(size_t)L * E + e] = scale * out[L];
+  }
+}
+
+// ------------------------------------------------------------ host helpers
+
+bool valid_vox(const phastb_voxel_grid* g) {
+  return g && g->nx >= 1 && g->ny >= 1 && g->nz >= 1 && g->hx > 0 && g->hy > 0 && g->hz > 0 &&
+         (long long)(g->nx + 1) * (g->ny + 1) * (g->nz + 1) < (1LL << 31) / 24;
+}
+
+bool valid_mat(const phastb_voxel_material* m) {
+  return m && m->n_slots >= 1 && m->n_slots <= PHASTB_MAX_SLOTS && m->ell > 0;
+}
+
+size_t h8_scratch_bytes(const VoxGeom& v, int dtype) {
+  const size_t w = dtype == PHASTB_F32 ? 4 : 8;
+  return align_up(24 * w * (size_t)v.n_elem) + red_ws_bytes();
+}
+
+template <typename T>
+int h8_mech_apply_t(const VoxGeom& v, const VoxMat<T>& mm, const uint8_t* slot, const T* x, const T* gq,
+                    const T* d, const uint8_t* mask, T* y, void* scratch, const int* guard, cudaStream_t s) {
+  T* sc = static_cast<T*>(scratch);
+  RedWs ws = red_ws(static_cast<char*>(scratch) + align_up(24 * sizeof(T) * (size_t)v.n_elem));
+  { note_launch(); h8_mech_elem_kernel<T><<<grid_for(v.n_elem), kThreads, 0, s>>>(v, mm, slot, x, gq, d, sc, y, mask, ws, guard); }
+  { note_launch(); h8_gather_kernel<T, 3><<<grid_for(v.n_red), kThreads, 0, s>>>(v, sc, y, mask, guard); }
+  return last_launch_status();
+}
+
+template int h8_mech_apply_t<double>(const VoxGeom&, const VoxMat<double>&, const uint8_t*, const double*,
+                                     const double*, const double*, const uint8_t*, double*, void*, const int*,
+                                     cudaStream_t);
+template int h8_mech_apply_t<float>(const VoxGeom&, const VoxMat<float>&, const uint8_t*, const float*,
+                                    const float*, const float*, const uint8_t*, float*, void*, const int*,
+                                    cudaStream_t);
+
+template <typename T>
+int h8_mech_diag_t(const VoxGeom& v, const VoxMat<T>& mm, const uint8_t* slot, const T* gq, const T* d, T* diag,
+                   void* scratch, cudaStream_t s) {
+  T* sc = static_cast<T*>(scratch);
+  RedWs ws = red_ws(static_cast<char*>(scratch) + align_up(24 * sizeof(T) * (size_t)v.n_elem));
+  { note_launch(); h8_mdiag_elem_kernel<T><<<grid_for(v.n_elem), kThreads, 0, s>>>(v, mm, slot, gq, d, sc, diag, ws); }
+  { note_launch(); h8_gather_kernel<T, 3><<<grid_for(v.n_red), kThreads, 0, s>>>(v, sc, diag, nullptr, nullptr); }
+  return last_launch_status();
+}
+
+template int h8_mech_diag_t<double>(const VoxGeom&, const VoxMat<double>&, const uint8_t*, const double*,
+                                    const double*, double*, void*, cudaStream_t);
+template int h8_mech_diag_t<float>(const VoxGeom&, const VoxMat<float>&, const uint8_t*, const float*, const float*,
+                                   float*, void*, cudaStream_t);
+
+double damage_kdiag(const VoxGeom& v, double ell) {
+  // diag of M/ell + ell L for one corner (the same at every corner by symmetry)
+  const double c[2] = {kC1, kC2};
+  double acc = 0.0;
+  for (int q = 0; q < 8; ++q) {
+    const int qx = q & 1, qy = (q >> 1) & 1, qz = q >> 2;
+    const double nx = c[qx != 0], ny = c[qy != 0], nz = c[qz != 0];  // corner L = 0
+    const double n = nx * ny * nz;
+    const double gx = -ny * nz / v.hx, gy = -nx * nz / v.hy, gz = -nx * ny / v.hz;
+    acc += v.w * (n * n / ell + ell * (gx * gx + gy * gy + gz * gz));
+  }
+  return acc;
+}
+
+int h8_damage_launch(const VoxGeom& v, const VoxMat<double>& mm, const uint8_t* slot, int mode, const double* d,
+                     const double* H, double scale, double* y, const uint8_t* mask, void* scratch,
+                     const int* guard, cudaStream_t s) {
+  double* sc = static_cast<double*>(scratch);
+  const int G = grid_for(v.n_elem);
+  const double kd = damage_kdiag(v, double(mm.ell));
+  if (mode == 0)
+    { note_launch(); h8_damage_elem_kernel<0><<<G, kThreads, 0, s>>>(v, mm, slot, d, H, scale, kd, sc, guard); }
+  else if (mode == 1)
+    { note_launch(); h8_damage_elem_kernel<1><<<G, kThreads, 0, s>>>(v, mm, slot, d, H, scale, kd, sc, guard); }
+  else
+    { note_launch(); h8_damage_elem_kernel<2><<<G, kThreads, 0, s>>>(v, mm, slot, d, H, scale, kd, sc, guard); }
+  { note_launch(); h8_gather_kernel<double, 1><<<grid_for(v.n_red), kThreads, 0, s>>>(v, sc, y, mask, guard); }
+  return last_launch_status();
+}
+
+}  // namespace phastb
+
+using namespace phastb;
+
+extern "C" {
+
+size_t phastb_h8_scratch_bytes(const phastb_voxel_grid* g, int dtype) {
+  if (!valid_vox(g)) return 0;
+  return h8_scratch_bytes(make_vox_geom(*g), dtype);
+}
+
+int phastb_h8_degradation(const phastb_voxel_grid* g, int dtype, const void* d, double kappa, void* g_out,
+                          void* stream) {
+  if (!valid_vox(g) || !d || !g_out) return PHASTB_ERR_ARG;
+  const VoxGeom v = make_vox_geom(*g);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == PHASTB_F64)
+    { note_launch(); h8_degradation_kernel<double><<<grid_for(v.n_elem), kThreads, 0, s>>>(v, (const double*)d, kappa,
+                                                                         (double*)g_out); }
+  else if (dtype == PHASTB_F32)
+    { note_launch(); h8_degradation_kernel<float><<<grid_for(v.n_elem), kThreads, 0, s>>>(v, (const float*)d, (float)kappa,
+                                                                        (float*)g_out); }
+  else
+    return PHASTB_ERR_ARG;
+  return last_launch_status();
+}
+
+int phastb_h8_mech_apply(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot, int dtype,
+                         const void* x, const void* gq, const void* d, const uint8_t* mask, void* y, void* scratch,
+                         void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !x || !y || !scratch) return PHASTB_ERR_ARG;
+  const VoxGeom v = make_vox_geom(*g);
+  cudaStream_t s = (cudaStream_t)stream;
+  RedWs ws = red_ws(static_cast<char*>(scratch) +
+                    align_up((dtype == PHASTB_F32 ? 4 : 8) * 24 * (size_t)v.n_elem));
+  int st = red_ws_reset(ws, s);
+  if (st) return st;
+  if (dtype == PHASTB_F64)
+    return h8_mech_apply_t<double>(v, make_vox_mat<double>(*m), slot, (const double*)x, (const double*)gq,
+                                   (const double*)d, mask, (double*)y, scratch, nullptr, s);
+  if (dtype == PHASTB_F32)
+    return h8_mech_apply_t<float>(v, make_vox_mat<float>(*m), slot, (const float*)x, (const float*)gq,
+                                  (const float*)d, mask, (float*)y, scratch, nullptr, s);
+  return PHASTB_ERR_ARG;
+}
+
+int phastb_h8_mech_diagonal(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                            int dtype, const void* gq, const void* d, void* diag, void* scratch, void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !diag || !scratch) return PHASTB_ERR_ARG;
+  const VoxGeom v = make_vox_geom(*g);
+  cudaStream_t s = (cudaStream_t)stream;
+  RedWs ws = red_ws(static_cast<char*>(scratch) +
+                    align_up((dtype == PHASTB_F32 ? 4 : 8) * 24 * (size_t)v.n_elem));
+  int st = red_ws_reset(ws, s);
+  if (st) return st;
+  if (dtype == PHASTB_F64)
+    return h8_mech_diag_t<double>(v, make_vox_mat<double>(*m), slot, (const double*)gq, (const double*)d,
+                                  (double*)diag, scratch, s);
+  if (dtype == PHASTB_F32)
+    return h8_mech_diag_t<float>(v, make_vox_mat<float>(*m), slot, (const float*)gq, (const float*)d,
+                                 (float*)diag, scratch, s);
+  return PHASTB_ERR_ARG;
+}
+
+int phastb_h8_stress_energy(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                            const double* x, const double* gq, const double* d, double* rE_host,
+                            double* energy_host, void* scratch, void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !x || !scratch) return PHASTB_ERR_ARG;
+  const VoxGeom v = make_vox_geom(*g);
+  cudaStream_t s = (cudaStream_t)stream;
+  RedWs ws = red_ws(static_cast<char*>(scratch) + align_up(8 * 24 * (size_t)v.n_elem));
+  int st = red_ws_reset(ws, s);
+  if (st) return st;
+  { note_launch(); h8_mech_elem_kernel<double><<<grid_for(v.n_elem), kThreads, 0, s>>>(
+      v, make_vox_mat<double>(*m), slot, x, gq, d, nullptr, nullptr, nullptr, ws, nullptr); }
+  if ((st = last_launch_status())) return st;
+  double o[7];
+  if ((st = red_ws_fetch(ws, o, 7, s))) return st;
+  if (rE_host)
+    for (int k = 0; k < 6; ++k) rE_host[k] = o[k];
+  if (energy_host) *energy_host = o[6];
+  return PHASTB_OK;
+}
+
+int phastb_h8_driving_history(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                              const double* x, const double* H_prev, double* Y, double* H_out, void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !x || (!Y && !H_out)) return PHASTB_ERR_ARG;
+  const VoxGeom v = make_vox_geom(*g);
+  { note_launch(); h8_driving_kernel<<<grid_for(v.n_elem), kThreads, 0, (cudaStream_t)stream>>>(v, make_vox_mat<double>(*m), slot,
+                                                                               x, H_prev, Y, H_out); }
+  return last_launch_status();
+}
+
+int phastb_h8_damage_apply(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                           const double* d, const double* H, double scale, double* y, void* scratch, void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !d || !y || !scratch) return PHASTB_ERR_ARG;
+  return h8_damage_launch(make_vox_geom(*g), make_vox_mat<double>(*m), slot, 0, d, H, scale, y, nullptr, scratch,
+                          nullptr, (cudaStream_t)stream);
+}
+
+int phastb_h8_damage_rhs_diag(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                              const double* H, double scale, double* rhs, double* diag, void* scratch,
+                              void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !scratch) return PHASTB_ERR_ARG;
+  const VoxGeom v = make_vox_geom(*g);
+  const VoxMat<double> mm = make_vox_mat<double>(*m);
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = PHASTB_OK;
+  if (rhs) {
+    if (H)
+      st = h8_damage_launch(v, mm, slot, 1, nullptr, H, scale, rhs, nullptr, scratch, nullptr, s);
+    else
+      st = cuda_status(cudaMemsetAsync(rhs, 0, sizeof(double) * v.n_red, s));
+  }
+  if (st) return st;
+  if (diag) st = h8_damage_launch(v, mm, slot, 2, nullptr, H, scale, diag, nullptr, scratch, nullptr, s);
+  return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,62 @@
+// Deterministic multi-quantity reductions over a caller workspace.
+#pragma once
+#include "common.cuh"
+
+namespace phastb {
+
+constexpr int kRedMaxK = 16;
+
+inline size_t align_up(size_t b, size_t a = 256) { return (b + a - 1) / a * a; }
+
+struct RedWs {
+  double* part;       // kRedMaxK * kMaxPartials
+  unsigned* counter;  // ticket
+  double* out;        // kRedMaxK results
+};
+
+inline size_t red_ws_bytes() {
+  return align_up(sizeof(double) * kRedMaxK * kMaxPartials) + 256 + align_up(sizeof(double) * kRedMaxK);
+}
+
+inline RedWs red_ws(void* base) {
+  char* p = static_cast<char*>(base);
+  RedWs w;
+  w.part = reinterpret_cast<double*>(p);
+  p += align_up(sizeof(double) * kRedMaxK * kMaxPartials);
+  w.counter = reinterpret_cast<unsigned*>(p);
+  p += 256;
+  w.out = reinterpret_cast<double*>(p);
+  return w;
+}
+
+inline int red_ws_reset(const RedWs& w, cudaStream_t s) {
+  return cuda_status(cudaMemsetAsync(w.counter, 0, sizeof(unsigned), s));
+}
+
+inline int red_ws_fetch(const RedWs& w, double* host, int k, cudaStream_t s) {
+  cudaError_t e = cudaMemcpyAsync(host, w.out, sizeof(double) * k, cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return PHASTB_ERR_CUDA;
+  return cuda_status(cudaStreamSynchronize(s));
+}
+
+// Block-reduce K sums, publish partials, the last block folds them into out[]
+// and resets the ticket so the workspace can be reused by the next launch.
+template <int K>
+__device__ __forceinline__ void reduce_multi(double (&v)[K], RedWs ws) {
+  __shared__ double sh[32];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const double s = block_sum(v[k], sh);
+    if (threadIdx.x == 0) ws.part[k * kMaxPartials + blockIdx.x] = s;
+  }
+  if (arrive_last(ws.counter)) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const double t = fold_sum(ws.part + k * kMaxPartials, gridDim.x, sh);
+      if (threadIdx.x == 0) ws.out[k] = t;
+    }
+    if (threadIdx.x == 0) *ws.counter = 0u;
+  }
+}
+
+}  // namespace phastb

@@ -1,0 +1,217 @@
+// 2D solver drivers over the structured-Q4 operators: the bound-projected
+// PCG damage solve and the quasi-static Newton / matrix-free CG mechanics.
+#include "engine.cuh"
+#include "q4_kernels.cuh"
+
+#include <cmath>
+#include <vector>
+
+namespace phastb {
+
+int q4_damage_apply_launch(const phastb_q4_grid* g, const double* d, const double* Hq, double rs, double rsh,
+                           const double* rsh_e, double gcl0, const double* gcl0_e, double* y, const int* guard,
+                           cudaStream_t s);
+int q4_force_launch(const phastb_q4_grid* g, const phastb_q4_material* m, const double* u, const double* d,
+                    double* f, const uint8_t* mask, const int* guard, cudaStream_t s);
+
+struct Q4DamageCtx {
+  const phastb_q4_grid* g;
+  const double* Hq;
+  double rsh;
+  const double* rsh_e;
+  double gcl0;
+  const double* gcl0_e;
+};
+
+static int q4_damage_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
+  const Q4DamageCtx* k = static_cast<const Q4DamageCtx*>(c);
+  return q4_damage_apply_launch(k->g, x, k->Hq, 2.0, k->rsh, k->rsh_e, k->gcl0, k->gcl0_e, y, guard, s);
+}
+
+struct Q4ForceCtx {
+  const phastb_q4_grid* g;
+  const phastb_q4_material* m;
+  const double* d;
+  const uint8_t* mask;
+};
+
+static int q4_force_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
+  const Q4ForceCtx* k = static_cast<const Q4ForceCtx*>(c);
+  return q4_force_launch(k->g, k->m, x, k->d, y, k->mask, guard, s);
+}
+
+// residual r = (f_ext - f) * free, and u[bc] = bc_vals helpers
+__global__ void qs_residual_kernel(int n2, const double* __restrict__ fext, const double* __restrict__ f,
+                                   const uint8_t* __restrict__ bcm, double* __restrict__ r, RedWs ws) {
+  double acc[2] = {0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
+    const double v = bcm[i] ? 0.0 : (fext ? fext[i] : 0.0) - f[i];
+    r[i] = v;
+    acc[0] += v * v;
+    acc[1] += isfinite(v) ? 0.0 : 1.0;
+  }
+  reduce_multi<2>(acc, ws);
+}
+
+__global__ void qs_axpy_bc_kernel(int n2, const double* __restrict__ u, double alpha, const double* __restrict__ du,
+                                  const uint8_t* __restrict__ bcm, const double* __restrict__ bcv,
+                                  double* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x)
+    out[i] = bcm[i] ? bcv[i] : (du ? u[i] + alpha * du[i] : u[i]);
+}
+
+__global__ void copy_kernel(int n, const double* __restrict__ a, double* __restrict__ b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
+}
+
+__global__ void zero_kernel(int n, double* __restrict__ a) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = 0.0;
+}
+
+static bool valid_grid(const phastb_q4_grid* g) {
+  return g && g->nx >= 1 && g->ny >= 1 && g->hx > 0 && g->hy > 0 &&
+         (long long)(g->nx + 1) * (g->ny + 1) < (1LL << 30);
+}
+
+}  // namespace phastb
+
+using namespace phastb;
+
+extern "C" {
+
+size_t phastb_q4_damage_solve_workspace_bytes(int n_nodes) { return ppcg_ws_bytes(n_nodes); }
+
+int phastb_q4_damage_solve(const phastb_q4_grid* g, const double* Hq, double gc_over_l0, const double* gc_over_l0_e,
+                           double gcl0, const double* gcl0_e, const double* d_prev, const double* d_init,
+                           const uint8_t* fixed, const double* fixed_vals, double tol, int max_iter, int check_every,
+                           double* d_out, int* info, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!valid_grid(g) || !Hq || !d_prev || !d_out || max_iter < 0 || check_every < 1) return PHASTB_ERR_ARG;
+  if (fixed && !fixed_vals) return PHASTB_ERR_ARG;
+  const int n = (g->nx + 1) * (g->ny + 1);
+  if (!workspace || workspace_bytes < ppcg_ws_bytes(n)) return PHASTB_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  PpcgWs w = ppcg_ws(workspace, n);
+  int st = phastb_q4_damage_prepare(g, Hq, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e, w.b, w.minv, stream);
+  if (st) return st;
+  Q4DamageCtx ctx{g, Hq, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e};
+  LinOp<double> A{q4_damage_op, &ctx};
+  int inf[2] = {0, 0};
+  st = ppcg_solve(A, n, w, d_prev, d_init, fixed, fixed_vals, tol, max_iter, check_every, d_out, inf, s);
+  if (info) {
+    info[0] = inf[0];
+    info[1] = inf[1];
+  }
+  return st;
+}
+
+size_t phastb_q4_qs_workspace_bytes(int n_nodes) {
+  const int n2 = 2 * n_nodes;
+  return pcg_ws_bytes<double>(n2) + 4 * align_up(sizeof(double) * (size_t)n2) + red_ws_bytes();
+}
+
+int phastb_q4_qs_solve(const phastb_q4_grid* g, const phastb_q4_material* m, const double* d, const double* f_ext,
+                       const uint8_t* bc_mask, const double* bc_vals, double* u, double tol, double cg_tol,
+                       int cg_max_iter, int max_iter, int line_search, int ls_max_steps, double ls_min_alpha,
+                       double ls_c, int* info, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!valid_grid(g) || !m || !d || !bc_mask || !bc_vals || !u || cg_max_iter < 1 || max_iter < 0)
+    return PHASTB_ERR_ARG;
+  if (m->stress_split != PHASTB_SPLIT_ISOTROPIC && m->stress_split != PHASTB_SPLIT_LINEAR)
+    return PHASTB_UNSUPPORTED;  // split-aware tangents need the consistent-tangent kernel
+  const int nn = (g->nx + 1) * (g->ny + 1), n2 = 2 * nn;
+  if (!workspace || workspace_bytes < phastb_q4_qs_workspace_bytes(nn)) return PHASTB_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  char* p = static_cast<char*>(workspace);
+  PcgWs<double> w = pcg_ws<double>(p, n2);
+  p += pcg_ws_bytes<double>(n2);
+  const size_t v = align_up(sizeof(double) * (size_t)n2);
+  double* du = reinterpret_cast<double*>(p);
+  double* res = reinterpret_cast<double*>(p + v);
+  double* ut = reinterpret_cast<double*>(p + 2 * v);
+  double* ub = reinterpret_cast<double*>(p + 3 * v);
+  void* redbase = p + 4 * v;
+  RedWs rw = red_ws(redbase);
+  const int G = grid_for(n2);
+  int st;
+  if ((st = red_ws_reset(rw, s))) return st;
+
+  // u[bc] = bc_vals
+  { note_launch(); qs_axpy_bc_kernel<<<G, kThreads, 0, s>>>(n2, u, 0.0, nullptr, bc_mask, bc_vals, u); }
+  Q4ForceCtx kctx{g, m, d, bc_mask};
+  LinOp<double> K{q4_force_op, &kctx};
+
+  auto residual_norm = [&](const double* uu, double* r, double* nrm, bool* finite) -> int {
+    int e = q4_force_launch(g, m, uu, d, w.Ap, nullptr, nullptr, s);
+    if (e) return e;
+    { note_launch(); qs_residual_kernel<<<G, kThreads, 0, s>>>(n2, f_ext, w.Ap, bc_mask, r, rw); }
+    if ((e = last_launch_status())) return e;
+    double o[2];
+    if ((e = red_ws_fetch(rw, o, 2, s))) return e;
+    *nrm = std::sqrt(o[0]);
+    *finite = o[1] == 0.0 && std::isfinite(o[0]);
+    return PHASTB_OK;
+  };
+
+  int total_cg = 0;
+  for (int it = 0; it < max_iter; ++it) {
+    double rn;
+    bool fin;
+    if ((st = residual_norm(u, res, &rn, &fin))) return st;
+    if (!std::isnan(rn) && rn <= tol) {
+      if (info) { info[0] = it; info[1] = 1; info[2] = total_cg; }
+      return PHASTB_OK;
+    }
+    if (!fin) {
+      if (info) { info[0] = max_iter; info[1] = 0; info[2] = total_cg; }
+      return PHASTB_NONFINITE;
+    }
+    // du = CG(K(d) restricted to free dofs, res)
+    { note_launch(); zero_kernel<<<G, kThreads, 0, s>>>(n2, du); }
+    PcgResult pr{};
+    if ((st = pcg_run<double>(K, n2, w, res, nullptr, nullptr, du, cg_tol, cg_max_iter, 50, PCG_PERIODIC, 0.0,
+                              &pr, s)))
+      return st;
+    total_cg += pr.iterations;
+    if (pr.breakdown || pr.nonfinite) {
+      if (info) { info[0] = it + 1; info[1] = 0; info[2] = total_cg; }
+      return PHASTB_BREAKDOWN;
+    }
+    // accept the Newton step (_accept_newton_step)
+    if (!line_search) {
+      { note_launch(); qs_axpy_bc_kernel<<<G, kThreads, 0, s>>>(n2, u, 1.0, du, bc_mask, bc_vals, u); }
+      continue;
+    }
+    double alpha = 1.0, best = INFINITY;
+    bool have_best = false, accepted = false;
+    const double baseline = std::max(rn, 1e-30);
+    const int n_ls = std::max(1, ls_max_steps + 1);
+    for (int ls = 0; ls < n_ls; ++ls) {
+      { note_launch(); qs_axpy_bc_kernel<<<G, kThreads, 0, s>>>(n2, u, alpha, du, bc_mask, bc_vals, ut); }
+      double tn;
+      bool tf;
+      if ((st = residual_norm(ut, w.z, &tn, &tf))) return st;
+      if (tn < best) {
+        best = tn;
+        have_best = true;
+        { note_launch(); copy_kernel<<<G, kThreads, 0, s>>>(n2, ut, ub); }
+      }
+      if (tf && tn <= (1.0 - ls_c * alpha) * baseline) {
+        { note_launch(); copy_kernel<<<G, kThreads, 0, s>>>(n2, ut, u); }
+        accepted = true;
+        break;
+      }
+      alpha *= 0.5;
+      if (alpha < ls_min_alpha) break;
+    }
+    if (!accepted) {
+      if (have_best && best < baseline)
+        { note_launch(); copy_kernel<<<G, kThreads, 0, s>>>(n2, ub, u); }
+      else
+        { note_launch(); qs_axpy_bc_kernel<<<G, kThreads, 0, s>>>(n2, u, 1.0, du, bc_mask, bc_vals, u); }
+    }
+    if ((st = last_launch_status())) return st;
+  }
+  if (info) { info[0] = max_iter; info[1] = 0; info[2] = total_cg; }
+  return PHASTB_NONCONVERGED;
+}
+
+}  // extern "C"

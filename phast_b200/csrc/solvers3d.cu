@@ -1,0 +1,398 @@
+// 3D solver drivers over the periodic-voxel operators: constrained Jacobi-PCG
+// mechanics (solid3d/linalg.py), box-KKT damage (solvers/box_kkt_h8.py) and the
+// staggered-change measure (solid3d/staggered.py:1097-1124).
+#include "engine.cuh"
+#include "h8_kernels.cuh"
+
+#include <cmath>
+
+namespace phastb {
+
+bool valid_vox(const phastb_voxel_grid* g);
+bool valid_mat(const phastb_voxel_material* m);
+size_t h8_scratch_bytes(const VoxGeom& v, int dtype);
+template <typename T>
+int h8_mech_apply_t(const VoxGeom& v, const VoxMat<T>& mm, const uint8_t* slot, const T* x, const T* gq,
+                    const T* d, const uint8_t* mask, T* y, void* scratch, const int* guard, cudaStream_t s);
+template <typename T>
+int h8_mech_diag_t(const VoxGeom& v, const VoxMat<T>& mm, const uint8_t* slot, const T* gq, const T* d, T* diag,
+                   void* scratch, cudaStream_t s);
+int h8_damage_launch(const VoxGeom& v, const VoxMat<double>& mm, const uint8_t* slot, int mode, const double* d,
+                     const double* H, double scale, double* y, const uint8_t* mask, void* scratch,
+                     const int* guard, cudaStream_t s);
+
+struct MechCtx {
+  VoxGeom v;
+  VoxMat<double> m;
+  const uint8_t* slot;
+  const double* gq;
+  const double* d;
+  const uint8_t* mask;
+  void* scratch;
+};
+
+static int mech_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
+  const MechCtx* k = static_cast<const MechCtx*>(c);
+  return h8_mech_apply_t<double>(k->v, k->m, k->slot, x, k->gq, k->d, k->mask, y, k->scratch, guard, s);
+}
+
+struct DamageCtx {
+  VoxGeom v;
+  VoxMat<double> m;
+  const uint8_t* slot;
+  const double* H;
+  double scale;
+  const uint8_t* mask;
+  void* scratch;
+};
+
+static int damage_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
+  const DamageCtx* k = static_cast<const DamageCtx*>(c);
+  return h8_damage_launch(k->v, k->m, k->slot, 0, x, k->H, k->scale, y, k->mask, k->scratch, guard, s);
+}
+
+// xc = where(fixed, vals, 0); x0f = where(free, x0, 0); invd = 1/where(free, diag, 1)
+__global__ void constrained_setup_kernel(int n, const uint8_t* __restrict__ fixed, const double* __restrict__ vals,
+                                         const double* __restrict__ x0, double* __restrict__ xc,
+                                         double* __restrict__ x0f, double* __restrict__ diag_inv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const bool f = fixed[i];
+    xc[i] = f ? vals[i] : 0.0;
+    x0f[i] = f ? 0.0 : (x0 ? x0[i] : 0.0);
+    diag_inv[i] = 1.0 / (f ? 1.0 : diag_inv[i]);
+  }
+}
+
+// b_f = where(free, rhs - image, 0) with ||b_f||^2
+__global__ void __launch_bounds__(kThreads) constrained_rhs_kernel(int n, const uint8_t* __restrict__ fixed,
+                                                                   const double* __restrict__ rhs,
+                                                                   const double* __restrict__ image,
+                                                                   double* __restrict__ bf, RedWs ws) {
+  double acc[1] = {0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = fixed[i] ? 0.0 : (rhs ? rhs[i] : 0.0) - image[i];
+    bf[i] = v;
+    acc[0] += v * v;
+  }
+  reduce_multi<1>(acc, ws);
+}
+
+__global__ void where_kernel(int n, const uint8_t* __restrict__ fixed, const double* __restrict__ a,
+                             const double* __restrict__ b, double* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = fixed[i] ? b[i] : a[i];
+}
+
+// box-KKT helpers -----------------------------------------------------------
+
+// fixed = la | ua | peq; known = where(fixed, (ua ? upper : lower), 0);
+// x0f = where(free, initial, 0); invd = 1/where(free, diag, 1)
+__global__ void kkt_setup_kernel(int n, const uint8_t* __restrict__ la, const uint8_t* __restrict__ ua,
+                                 const double* __restrict__ lower, double upper, const double* __restrict__ initial,
+                                 const double* __restrict__ diag, uint8_t* __restrict__ fixed,
+                                 double* __restrict__ known, double* __restrict__ x0f,
+                                 double* __restrict__ invd) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const bool peq = lower[i] == upper;
+    const bool f = la[i] || ua[i] || peq;
+    fixed[i] = f;
+    known[i] = f ? (ua[i] ? upper : lower[i]) : 0.0;
+    x0f[i] = f ? 0.0 : (initial ? initial[i] : 0.0);
+    invd[i] = 1.0 / (f ? 1.0 : diag[i]);
+  }
+}
+
+// grad = A cand - rhs; add/release sets; la/ua updated in place; counts OR'd.
+__global__ void __launch_bounds__(kThreads) kkt_update_kernel(int n, const uint8_t* __restrict__ fixed,
+                                                              const double* __restrict__ cand,
+                                                              const double* __restrict__ Acand,
+                                                              const double* __restrict__ rhs,
+                                                              const double* __restrict__ lower, double upper,
+                                                              double kkt_tol, uint8_t* __restrict__ la,
+                                                              uint8_t* __restrict__ ua, double* __restrict__ grad,
+                                                              RedWs ws) {
+  double acc[1] = {0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double gr = Acand[i] - rhs[i];
+    grad[i] = gr;
+    const bool fr = !fixed[i];
+    const bool add_l = fr && (cand[i] < lower[i]);
+    const bool add_u = fr && (cand[i] > upper);
+    const bool rel_l = la[i] && (gr < -kkt_tol);
+    const bool rel_u = ua[i] && (gr > kkt_tol);
+    if (add_l || add_u || rel_l || rel_u) acc[0] += 1.0;
+    la[i] = (la[i] || add_l) && !rel_l;
+    ua[i] = (ua[i] || add_u) && !rel_u;
+  }
+  reduce_multi<1>(acc, ws);
+}
+
+// KKT audit (box_kkt_h8._kkt_diagnostics): returns violation count and maxima.
+__global__ void __launch_bounds__(kThreads) kkt_audit_kernel(int n, const double* __restrict__ sol,
+                                                             const double* __restrict__ grad,
+                                                             const double* __restrict__ lower, double upper,
+                                                             const uint8_t* __restrict__ la,
+                                                             const uint8_t* __restrict__ ua, double tol, RedWs ws) {
+  // acc: [violations count, max|free grad|, max|projected grad|, max|complementarity|]
+  double cnt = 0, fs = 0, pg = 0, cm = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double s = sol[i], g = grad[i], lo = lower[i];
+    const bool peq = lo == upper;
+    const bool l = la[i], u = ua[i];
+    const bool fixed = l || u || peq;
+    if (s < lo || s > upper) cnt += 1.0;
+    if (l && g < -tol) cnt += 1.0;
+    if (u && -g < -tol) cnt += 1.0;
+    if (!fixed) {
+      fs = fmax(fs, fabs(g));
+      pg = fmax(pg, fabs(g));
+    }
+    if (l) {
+      pg = fmax(pg, fabs(fmin(g, 0.0)));
+      cm = fmax(cm, fabs(fmax(g, 0.0) * (s - lo)));
+    }
+    if (u) {
+      pg = fmax(pg, fabs(fmax(g, 0.0)));
+      cm = fmax(cm, fabs(fmax(-g, 0.0) * (upper - s)));
+    }
+  }
+  __shared__ double sh[32];
+  double v = block_sum(cnt, sh);
+  if (threadIdx.x == 0) ws.part[blockIdx.x] = v;
+  double mx[3] = {fs, pg, cm};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    v = block_max(mx[k], sh);
+    if (threadIdx.x == 0) ws.part[(k + 1) * kMaxPartials + blockIdx.x] = v;
+  }
+  if (arrive_last(ws.counter)) {
+    const double c = fold_sum(ws.part, gridDim.x, sh);
+    if (threadIdx.x == 0) ws.out[0] = c;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double t = fold_max(ws.part + (k + 1) * kMaxPartials, gridDim.x, sh);
+      if (threadIdx.x == 0) ws.out[k + 1] = t;
+    }
+    if (threadIdx.x == 0) *ws.counter = 0u;
+  }
+}
+
+// staggered change parts: ||du||, ||u||, max|dE|, max|E|, max|dd| (staggered.py:1097-1124)
+__global__ void __launch_bounds__(kThreads) change_kernel(int nu, const double* __restrict__ xn,
+                                                          const double* __restrict__ xo, int nd,
+                                                          const double* __restrict__ dn,
+                                                          const double* __restrict__ dol, RedWs ws) {
+  double du = 0, un = 0, dd = 0, dE = 0, Ei = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nu; i += gridDim.x * blockDim.x) {
+    const double a = xn[i], b = a - xo[i];
+    du += b * b;
+    un += a * a;
+  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nd; i += gridDim.x * blockDim.x)
+    dd = fmax(dd, fabs(dn[i] - dol[i]));
+  if (blockIdx.x == 0 && threadIdx.x < 6) {
+    dE = fabs(xn[nu + threadIdx.x] - xo[nu + threadIdx.x]);
+    Ei = fabs(xn[nu + threadIdx.x]);
+  }
+  __shared__ double sh[32];
+  double v = block_sum(du, sh);
+  if (threadIdx.x == 0) ws.part[blockIdx.x] = v;
+  v = block_sum(un, sh);
+  if (threadIdx.x == 0) ws.part[kMaxPartials + blockIdx.x] = v;
+  double mx[3] = {dE, Ei, dd};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    v = block_max(mx[k], sh);
+    if (threadIdx.x == 0) ws.part[(k + 2) * kMaxPartials + blockIdx.x] = v;
+  }
+  if (arrive_last(ws.counter)) {
+    double t = fold_sum(ws.part, gridDim.x, sh);
+    if (threadIdx.x == 0) ws.out[0] = sqrt(t);
+    t = fold_sum(ws.part + kMaxPartials, gridDim.x, sh);
+    if (threadIdx.x == 0) ws.out[1] = sqrt(t);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      t = fold_max(ws.part + (k + 2) * kMaxPartials, gridDim.x, sh);
+      if (threadIdx.x == 0) ws.out[k + 2] = t;
+    }
+    if (threadIdx.x == 0) *ws.counter = 0u;
+  }
+}
+
+}  // namespace phastb
+
+using namespace phastb;
+
+extern "C" {
+
+size_t phastb_h8_mech_solve_workspace_bytes(const phastb_voxel_grid* g, int dtype) {
+  if (!valid_vox(g)) return 0;
+  const VoxGeom v = make_vox_geom(*g);
+  const int n = 3 * v.n_red + 6;
+  return pcg_ws_bytes<double>(n) + 3 * align_up(sizeof(double) * (size_t)n) + h8_scratch_bytes(v, PHASTB_F64) +
+         red_ws_bytes();
+}
+
+int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                         const double* gq, const double* d, const uint8_t* fixed, const double* fixed_values,
+                         const double* x0, double rtol, double atol, int maxiter, int check_every, double* x_out,
+                         int* info, double* rinfo, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !fixed || !fixed_values || !x_out || maxiter < 1 ||
+      check_every < 1 || !(rtol >= 0) || !(atol >= 0) || (rtol == 0 && atol == 0))
+    return PHASTB_ERR_ARG;
+  if (!workspace || workspace_bytes < phastb_h8_mech_solve_workspace_bytes(g, PHASTB_F64))
+    return PHASTB_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  const VoxGeom v = make_vox_geom(*g);
+  const VoxMat<double> mm = make_vox_mat<double>(*m);
+  const int n = 3 * v.n_red + 6;
+  char* p = static_cast<char*>(workspace);
+  PcgWs<double> w = pcg_ws<double>(p, n);
+  p += pcg_ws_bytes<double>(n);
+  const size_t vb = align_up(sizeof(double) * (size_t)n);
+  double* xc = reinterpret_cast<double*>(p);
+  double* bf = reinterpret_cast<double*>(p + vb);
+  double* invd = reinterpret_cast<double*>(p + 2 * vb);
+  void* scratch = p + 3 * vb;
+  void* redb = p + 3 * vb + h8_scratch_bytes(v, PHASTB_F64);
+  RedWs rw = red_ws(redb);
+  RedWs sw = red_ws(static_cast<char*>(scratch) + align_up(24 * sizeof(double) * (size_t)v.n_elem));
+  const int G = grid_for(n);
+  int st;
+  if ((st = red_ws_reset(rw, s))) return st;
+  if ((st = red_ws_reset(sw, s))) return st;
+  // diagonal of A(g) into invd, then the constrained setup
+  if ((st = h8_mech_diag_t<double>(v, mm, slot, gq, d, invd, scratch, s))) return st;
+  { note_launch(); constrained_setup_kernel<<<G, kThreads, 0, s>>>(n, fixed, fixed_values, x0, xc, x_out, invd); }
+  MechCtx full{v, mm, slot, gq, d, nullptr, scratch};
+  if ((st = mech_op(&full, xc, w.Ap, nullptr, s))) return st;
+  { note_launch(); constrained_rhs_kernel<<<G, kThreads, 0, s>>>(n, fixed, nullptr, w.Ap, bf, rw); }
+  if ((st = last_launch_status())) return st;
+  double bn2;
+  if ((st = red_ws_fetch(rw, &bn2, 1, s))) return st;
+  const double bn = std::sqrt(bn2);
+  if (rinfo) rinfo[0] = bn;
+  if (!std::isfinite(bn)) return PHASTB_NONFINITE;
+  if (bn == 0.0) {
+    { note_launch(); where_kernel<<<G, kThreads, 0, s>>>(n, fixed, x_out, xc, x_out); }
+    if (info) { info[0] = 0; info[1] = 1; }
+    if (rinfo) rinfo[1] = 0.0;
+    return last_launch_status();
+  }
+  const double thr = std::max(rtol * bn, atol);
+  MechCtx free_ctx{v, mm, slot, gq, d, fixed, scratch};
+  LinOp<double> A{mech_op, &free_ctx};
+  PcgResult pr{};
+  if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, x_out, thr, maxiter, check_every, PCG_FREEZE, 0.0, &pr, s)))
+    return st;
+  { note_launch(); where_kernel<<<G, kThreads, 0, s>>>(n, fixed, x_out, xc, x_out); }
+  if ((st = last_launch_status())) return st;
+  if (info) { info[0] = pr.iterations; info[1] = pr.converged; }
+  if (rinfo) rinfo[1] = pr.rnorm;
+  if (pr.nonfinite) return PHASTB_NONFINITE;
+  if (pr.breakdown) return PHASTB_BREAKDOWN;
+  return pr.converged ? PHASTB_OK : PHASTB_NONCONVERGED;
+}
+
+size_t phastb_h8_box_kkt_workspace_bytes(const phastb_voxel_grid* g) {
+  if (!valid_vox(g)) return 0;
+  const VoxGeom v = make_vox_geom(*g);
+  const int n = v.n_red;
+  return pcg_ws_bytes<double>(n) + 6 * align_up(sizeof(double) * (size_t)n) + 4 * align_up((size_t)n) +
+         h8_scratch_bytes(v, PHASTB_F64) + red_ws_bytes();
+}
+
+int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                             const double* H, double scale, const double* lower, double upper,
+                             const double* initial, double lin_tol, double kkt_tol, int max_lin, int max_active,
+                             double* d_out, int* info, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !lower || !d_out || max_lin < 1 || max_active < 1 ||
+      !(lin_tol > 0) || !(kkt_tol >= 0))
+    return PHASTB_ERR_ARG;
+  if (!workspace || workspace_bytes < phastb_h8_box_kkt_workspace_bytes(g)) return PHASTB_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  const VoxGeom v = make_vox_geom(*g);
+  const VoxMat<double> mm = make_vox_mat<double>(*m);
+  const int n = v.n_red;
+  char* p = static_cast<char*>(workspace);
+  PcgWs<double> w = pcg_ws<double>(p, n);
+  p += pcg_ws_bytes<double>(n);
+  const size_t vb = align_up(sizeof(double) * (size_t)n), ub = align_up((size_t)n);
+  double* rhs = reinterpret_cast<double*>(p);
+  double* diag = reinterpret_cast<double*>(p + vb);
+  double* invd = reinterpret_cast<double*>(p + 2 * vb);
+  double* known = reinterpret_cast<double*>(p + 3 * vb);
+  double* bf = reinterpret_cast<double*>(p + 4 * vb);
+  double* grad = reinterpret_cast<double*>(p + 5 * vb);
+  uint8_t* la = reinterpret_cast<uint8_t*>(p + 6 * vb);
+  uint8_t* ua = la + ub;
+  uint8_t* fixed = la + 2 * ub;
+  char* scratch = p + 6 * vb + 4 * ub;
+  RedWs rw = red_ws(scratch + h8_scratch_bytes(v, PHASTB_F64));
+  const int G = grid_for(n);
+  int st;
+  if ((st = red_ws_reset(rw, s))) return st;
+  if ((st = h8_damage_launch(v, mm, slot, 1, nullptr, H, scale, rhs, nullptr, scratch, nullptr, s))) return st;
+  if (!H && (st = cuda_status(cudaMemsetAsync(rhs, 0, sizeof(double) * n, s)))) return st;
+  if ((st = h8_damage_launch(v, mm, slot, 2, nullptr, H, scale, diag, nullptr, scratch, nullptr, s))) return st;
+  if ((st = cuda_status(cudaMemsetAsync(la, 0, 2 * ub, s)))) return st;
+  DamageCtx full{v, mm, slot, H, scale, nullptr, scratch};
+  int total = 0;
+  const double* cinit = initial;
+  for (int ai = 1; ai <= max_active; ++ai) {
+    { note_launch(); kkt_setup_kernel<<<G, kThreads, 0, s>>>(n, la, ua, lower, upper, cinit, diag, fixed, known, d_out, invd); }
+    // b_f = where(free, rhs - A known, 0)
+    if ((st = damage_op(&full, known, w.Ap, nullptr, s))) return st;
+    { note_launch(); constrained_rhs_kernel<<<G, kThreads, 0, s>>>(n, fixed, rhs, w.Ap, bf, rw); }
+    if ((st = last_launch_status())) return st;
+    // Dirichlet PCG on the free set: tolerance relative to max(||r0||, 1)
+    DamageCtx fctx{v, mm, slot, H, scale, fixed, scratch};
+    LinOp<double> A{damage_op, &fctx};
+    PcgResult pr{};
+    if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, d_out, -lin_tol, max_lin, 10, PCG_STRICT, 0.0, &pr,
+                              s)))
+      return st;
+    // candidate = where(fixed, known, x)
+    { note_launch(); where_kernel<<<G, kThreads, 0, s>>>(n, fixed, d_out, known, d_out); }
+    total += pr.iterations;
+    if (pr.nonfinite) return PHASTB_NONFINITE;
+    if (pr.breakdown) return PHASTB_BREAKDOWN;
+    // gradient, active-set change
+    if ((st = damage_op(&full, d_out, w.Ap, nullptr, s))) return st;
+    { note_launch(); kkt_update_kernel<<<G, kThreads, 0, s>>>(n, fixed, d_out, w.Ap, rhs, lower, upper, kkt_tol, la, ua, grad, rw); }
+    if ((st = last_launch_status())) return st;
+    double changes;
+    if ((st = red_ws_fetch(rw, &changes, 1, s))) return st;
+    if (info) { info[0] = total; info[1] = ai; info[2] = 0; }
+    if (!pr.converged) return PHASTB_NONCONVERGED;
+    if (changes == 0.0) {
+      { note_launch(); kkt_audit_kernel<<<G, kThreads, 0, s>>>(n, d_out, grad, lower, upper, la, ua, kkt_tol, rw); }
+      if ((st = last_launch_status())) return st;
+      double a[4];
+      if ((st = red_ws_fetch(rw, a, 4, s))) return st;
+      const int ok = a[0] == 0.0 && a[1] <= kkt_tol && a[2] <= kkt_tol && a[3] <= kkt_tol;
+      if (info) info[2] = ok;
+      return ok ? PHASTB_OK : PHASTB_NONCONVERGED;
+    }
+    // next set starts from this candidate (copy so the solve can overwrite d_out)
+    if ((st = cuda_status(cudaMemcpyAsync(grad, d_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, s)))) return st;
+    cinit = grad;
+  }
+  return PHASTB_NONCONVERGED;
+}
+
+int phastb_h8_stagger_change(int n_u, const double* x_new, const double* x_old, int n_d, const double* d_new,
+                             const double* d_old, double* out_host, void* workspace, size_t workspace_bytes,
+                             void* stream) {
+  if (!x_new || !x_old || !d_new || !d_old || !out_host || n_u < 0 || n_d < 0) return PHASTB_ERR_ARG;
+  if (!workspace || workspace_bytes < red_ws_bytes()) return PHASTB_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  RedWs rw = red_ws(workspace);
+  int st = red_ws_reset(rw, s);
+  if (st) return st;
+  { note_launch(); change_kernel<<<grid_for(std::max(n_u, n_d)), kThreads, 0, s>>>(n_u, x_new, x_old, n_d, d_new, d_old, rw); }
+  if ((st = last_launch_status())) return st;
+  return red_ws_fetch(rw, out_host, 5, s);
+}
+
+}  // extern "C"

@@ -1,0 +1,121 @@
+"""2D mechanics solvers behind PhAST's ``ExplicitDynamics`` / ``QuasiStaticSolver``.
+
+``ExplicitDynamics.step`` is one fused kernel (predictor, internal force of the
+predicted field, corrector, Dirichlet zeroing) -- mechanics_solver.py:86-239.
+``QuasiStaticSolver.solve`` is Newton with matrix-free CG on K(d) and the
+residual line search of ``_accept_newton_step`` -- mechanics_solver.py:1597-2043;
+the Newton loop, the CG iterations and the line search all run in
+``libphastb.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import torch
+
+from . import _lib
+from ._lib import call, ptr, raw, stream
+from .fem2d import _dtype_code, stress_split_of
+
+
+class ExplicitDynamics:
+    """Central difference with lumped mass (mechanics_solver.py:86-239)."""
+
+    def __init__(self, fem, dt=None, dt_safety=1.0, differentiable=False, damping_ratio_max=0.0):
+        if differentiable:
+            raise NotImplementedError("use phast_b200.adjoint for gradients through the explicit loop")
+        if damping_ratio_max and damping_ratio_max > 0.0:
+            raise NotImplementedError("Kelvin-Voigt damping is not implemented by the B200 backend")
+        self.fem = fem
+        self.differentiable = False
+        self.damping_ratio_max = 0.0
+        self.dt_cfl = fem.dt_cfl * dt_safety
+        self.dt = self.dt_cfl if dt is None else dt
+        self.last_iter = 1
+        self._minv = {}
+
+    def _m_inv(self, dtype):
+        if dtype not in self._minv:
+            mi = 1.0 / (self.fem.material.rho * self.fem.M_scalar + 1e-30)
+            self._minv[dtype] = mi.to(dtype).contiguous()
+        return self._minv[dtype]
+
+    def step_into(self, u, v, a, d, f_ext, bc_mask, bc_vals, u_out, v_out, a_out, H_in=None, H_out=None):
+        """One step written into caller buffers; optionally fuses H_out = max(H_in, psi+(u_new))."""
+        fem = self.fem
+        dt = u.dtype
+        mask = bc_mask if bc_mask.dtype == torch.uint8 else bc_mask.to(torch.uint8)
+        call("phastb_q4_explicit_step", fem.grid, fem.mat(dt), _dtype_code(u), float(self.dt), ptr(self._m_inv(dt)),
+             ptr(u), ptr(v), ptr(a), ptr(d.to(dt).contiguous()), ptr(f_ext.to(dt).contiguous()),
+             ptr(mask.contiguous()), ptr(bc_vals.to(dt).contiguous()), ptr(u_out), ptr(v_out), ptr(a_out),
+             ptr(H_in), ptr(H_out), stream())
+
+    def step(self, u, v, a, d, f_ext, bc_mask, bc_vals, rigid_connectors=None):
+        """Predictor + corrector; returns new (u, v, a) (mechanics_solver.py:204-239)."""
+        if rigid_connectors:
+            raise NotImplementedError("rigid connectors are not implemented by the B200 backend")
+        self.last_iter = 1
+        u_n, v_n, a_n = torch.empty_like(u), torch.empty_like(v), torch.empty_like(a)
+        self.step_into(u.contiguous(), v.contiguous(), a.contiguous(), d, f_ext, bc_mask, bc_vals, u_n, v_n, a_n)
+        return u_n, v_n, a_n
+
+    def predictor(self, u, v, a, bc_mask, bc_vals):
+        u_new = u + self.dt * v + 0.5 * self.dt * self.dt * a
+        return torch.where(bc_mask, bc_vals, u_new)
+
+
+class QuasiStaticSolver:
+    """Newton-Raphson with matrix-free CG (mechanics_solver.py:816-2043), isotropic split."""
+
+    def __init__(self, fem, tol=1e-6, max_iter=50, cg_tol=1e-8, cg_max_iter=5000, backend="auto",
+                 sparse_dof_threshold=200000, inner_solver=None, consistent_tangent=None, line_search=True,
+                 line_search_max_steps=8, line_search_min_alpha=1e-4, line_search_c=1e-4, tol_rel=None,
+                 plasticity_operator=None, cohesive_operator=None):
+        if plasticity_operator is not None or cohesive_operator is not None:
+            raise NotImplementedError("plasticity / cohesive mechanics are not implemented by the B200 backend")
+        if tol_rel is not None:
+            raise NotImplementedError("relative Newton tolerance is not implemented by the B200 backend")
+        split = stress_split_of(fem.material)
+        if split != "isotropic":
+            raise NotImplementedError(
+                f"quasi-static mechanics with the {split!r} split needs the consistent-tangent kernel, which is "
+                "not implemented; use energy_split='isotropic'")
+        self.fem = fem
+        self.tol = float(tol)
+        self.max_iter = int(max_iter)
+        self.cg_tol = float(cg_tol)
+        self.cg_max_iter = int(cg_max_iter)
+        self.backend = backend
+        self.line_search = bool(line_search)
+        self.line_search_max_steps = int(line_search_max_steps)
+        self.line_search_min_alpha = float(line_search_min_alpha)
+        self.line_search_c = float(line_search_c)
+        self.last_iter = 0
+        self.last_cg_iters = 0
+        self.last_backend = "cg"
+        self._ws = _lib.Workspace(fem.device)
+
+    def solve(self, d, f_ext, bc_mask, bc_vals, u_init=None, rigid_connectors=None):
+        """Equilibrium f_int(u, d) = f_ext; returns (u, converged, n_iter) (mechanics_solver.py:1597-1783)."""
+        if rigid_connectors:
+            raise NotImplementedError("rigid connectors are not implemented by the B200 backend")
+        fem = self.fem
+        n = fem.n_nodes
+        u = (torch.zeros(n, 2, dtype=torch.float64, device=fem.device) if u_init is None
+             else u_init.to(torch.float64).clone().contiguous())
+        dd = d.to(torch.float64).contiguous()
+        fe = None if f_ext is None else f_ext.to(torch.float64).contiguous()
+        mask = bc_mask.to(torch.uint8).contiguous()
+        vals = bc_vals.to(torch.float64).contiguous()
+        info = (C.c_int * 3)()
+        wp, wn = self._ws.get(_lib.load().phastb_q4_qs_workspace_bytes(n))
+        st = raw("phastb_q4_qs_solve", fem.grid, fem.mat(torch.float64), ptr(dd), ptr(fe), ptr(mask), ptr(vals),
+                 ptr(u), self.tol, self.cg_tol, self.cg_max_iter, self.max_iter, int(self.line_search),
+                 self.line_search_max_steps, self.line_search_min_alpha, self.line_search_c, info, wp, wn, stream())
+        if st not in (_lib.OK, _lib.NONCONVERGED, _lib.NONFINITE, _lib.BREAKDOWN):
+            _lib.check(st, "phastb_q4_qs_solve")
+        self.last_iter = int(info[0])
+        self.last_cg_iters = int(info[2])
+        converged = bool(info[1])
+        return u.to(d.dtype if d.dtype.is_floating_point else torch.float64), converged, int(info[0])

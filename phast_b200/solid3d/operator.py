@@ -1,0 +1,296 @@
+"""Periodic voxel H8 phase-field operator on the GPU.
+
+Mirrors ``phast.solid3d.operator.PeriodicVoxelPhaseFieldOperator`` (AT2 parts,
+src/phast/solid3d/operator.py:133-1544): the same reduced periodic numbering
+(periodic.py:61-113), the same 2x2x2 Gauss rule and Voigt order, the same
+``x = [u~ (3 n_red), E (6)]`` layout.  Each action is two launches of
+``libphastb.so`` (an element kernel and a deterministic node gather).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from .. import _lib
+from .._lib import call, ptr, stream
+from .model import isotropic_C
+
+PORE = "pore"
+
+
+def _driver_code(phase, split_isotropic):
+    """resolve_driver (solid3d/materials.py:454-471) for isotropic phases."""
+    if getattr(phase, "name", "") == PORE or getattr(phase, "driver", "spectral") == "none":
+        return _lib.DRIVER_NONE
+    return _lib.DRIVER_SPECTRAL if split_isotropic == "spectral" else _lib.DRIVER_FULL
+
+
+class PeriodicVoxelPhaseFieldOperator:
+    """Matrix-free mechanics and damage operators of one periodic voxel cell (AT2).
+
+    Parameters
+    ----------
+    grid : VoxelGrid-like (``shape``, ``h``, ``periodic``)
+    slot : (nz, ny, nx) or (E,) integer array of material slots
+    phases : list of phase materials, one per slot (``E``, ``nu``, ``Gc``, ``driver``, ``name``)
+    ell, kappa : phase-field length and residual stiffness
+    load : LoadCase-like (``controlled``, ``fixed_zero``)
+    pinned_node : reduced node whose fluctuation is fixed (default: first node touching no pore)
+    """
+
+    def __init__(self, grid, slot, phases, ell, kappa, load, *, split_isotropic="spectral", pinned_node=None,
+                 device="cuda"):
+        self.grid = grid
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise ValueError("the B200 backend needs a CUDA device")
+        nx, ny, nz = (int(v) for v in grid.shape)
+        hx, hy, hz = (float(v) for v in grid.h)
+        px, py, pz = (bool(v) for v in getattr(grid, "periodic", (True, True, True)))
+        self.shape = (nx, ny, nz)
+        self.h = (hx, hy, hz)
+        self.vgrid = _lib.VoxelGrid(nx, ny, nz, int(px), int(py), int(pz), hx, hy, hz)
+        self.reduced_shape = (nx if px else nx + 1, ny if py else ny + 1, nz if pz else nz + 1)
+        rx, ry, rz = self.reduced_shape
+        self.n_red = rx * ry * rz
+        self.n_mech = 3 * self.n_red + 6
+        self.n_elements = nx * ny * nz
+        self.volume = nx * ny * nz * hx * hy * hz
+        self.ell = float(ell)
+        self.kappa = float(kappa)
+        self.load = load
+        slot_np = np.asarray(slot).reshape(-1).astype(np.int64)
+        if slot_np.shape[0] != self.n_elements:
+            raise ValueError(f"slot must hold {self.n_elements} entries")
+        if len(phases) > _lib.MAX_SLOTS or slot_np.min() < 0 or slot_np.max() >= len(phases):
+            raise ValueError("bad material slots")
+        self.phases = list(phases)
+        self.slot_np = slot_np
+        self.slot = torch.as_tensor(slot_np.astype(np.uint8), device=self.device)
+        m = _lib.VoxelMaterial()
+        m.n_slots = len(phases)
+        m.isotropic = 1
+        self._lam, self._mu, self._Gc = [], [], []
+        for s, ph in enumerate(phases):
+            Cm, lam, mu = isotropic_C(float(ph.E), float(ph.nu))
+            for k in range(36):
+                m.C[s][k] = float(Cm.reshape(-1)[k])
+            m.lam[s], m.mu[s], m.Gc[s] = lam, mu, float(ph.Gc)
+            m.driver[s] = _driver_code(ph, split_isotropic)
+            self._lam.append(lam)
+            self._mu.append(mu)
+            self._Gc.append(float(ph.Gc))
+        m.kappa = self.kappa
+        m.ell = self.ell
+        self.mat = m
+        Ge = np.asarray(self._Gc)[slot_np]
+        if not np.all(np.isfinite(Ge)) or not np.all(Ge > 0):
+            raise ValueError("Gc must be finite and positive at every element")
+        self.damage_scale = self.ell / (float(Ge.min()) * hx * hy * hz)  # operator.py:238
+        if pinned_node is None:
+            pinned_node = self._choose_pinned_node()
+        self.pinned_node = int(pinned_node)
+        self._ws = _lib.Workspace(self.device)
+        self._scratch64 = None
+        self._scratch32 = None
+        self._red = _lib.Workspace(self.device)
+
+    # -- construction helpers -----------------------------------------------------------
+    def _choose_pinned_node(self):
+        """choose_pinned_node (periodic.py:224-249): first reduced node touching no pore voxel."""
+        pore_slots = [s for s, p in enumerate(self.phases) if getattr(p, "name", "") == PORE]
+        if not pore_slots:
+            return 0
+        nx, ny, nz = self.shape
+        rx, ry, rz = self.reduced_shape
+        px, py, pz = self.vgrid.px, self.vgrid.py, self.vgrid.pz
+        ke, je, ie = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        pore = np.isin(self.slot_np, pore_slots)
+        count = np.zeros(self.n_red, dtype=np.int64)
+        for L in range(8):
+            i = ie.reshape(-1) + (L & 1)
+            j = je.reshape(-1) + ((L >> 1) & 1)
+            k = ke.reshape(-1) + (L >> 2)
+            if px:
+                i = i % nx
+            if py:
+                j = j % ny
+            if pz:
+                k = k % nz
+            nodes = i + rx * (j + ry * k)
+            np.add.at(count, nodes[pore], 1)
+        return int(np.argmin(count))
+
+    def scratch(self, dtype=torch.float64):
+        code = _lib.F64 if dtype == torch.float64 else _lib.F32
+        nbytes = _lib.load().phastb_h8_scratch_bytes(self.vgrid, code)
+        attr = "_scratch64" if code == _lib.F64 else "_scratch32"
+        buf = getattr(self, attr)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            setattr(self, attr, buf)
+        return C.c_void_p(buf.data_ptr())
+
+    def _check(self, name, t, shape, dtype=None):
+        if not isinstance(t, torch.Tensor):
+            raise TypeError(f"{name} must be a torch.Tensor")
+        if tuple(t.shape) != shape:
+            raise ValueError(f"{name} must have shape {shape}, got {tuple(t.shape)}")
+        _lib.require_cuda(t, name)
+        if dtype is not None and t.dtype != dtype:
+            raise ValueError(f"{name} must be {dtype}")
+        return t.contiguous()
+
+    def _dt(self, t):
+        return _lib.F64 if t.dtype == torch.float64 else _lib.F32
+
+    # -- layout --------------------------------------------------------------------------
+    def split_mech(self, x):
+        n = 3 * self.n_red
+        return x[:n].reshape(self.n_red, 3), x[n:]
+
+    def pack_mech(self, u, E):
+        u = torch.as_tensor(u, dtype=torch.float64, device=self.device).reshape(-1)
+        E = torch.as_tensor(E, dtype=torch.float64, device=self.device).reshape(-1)
+        return torch.cat((u, E))
+
+    def mech_fixed_mask(self):
+        """Pinned-node dofs, the controlled and the fixed_zero E components (operator.py:905-915)."""
+        mask = torch.zeros(self.n_mech, dtype=torch.bool, device=self.device)
+        b = 3 * self.pinned_node
+        mask[b:b + 3] = True
+        off = 3 * self.n_red
+        mask[off + int(self.load.controlled)] = True
+        for c in self.load.fixed_zero:
+            mask[off + int(c)] = True
+        return mask
+
+    def mech_fixed_values(self, e_c):
+        vals = torch.zeros(self.n_mech, dtype=torch.float64, device=self.device)
+        vals[3 * self.n_red + int(self.load.controlled)] = float(e_c)
+        return vals
+
+    # -- mechanics -------------------------------------------------------------------------
+    def degradation(self, d):
+        """g (E, 8) = (1-kappa)(1-d_q)^2 + kappa (operator.py:939-946)."""
+        d = self._check("d", d, (self.n_red,))
+        g = torch.empty(self.n_elements, 8, dtype=d.dtype, device=self.device)
+        call("phastb_h8_degradation", self.vgrid, self._dt(d), ptr(d), self.kappa, ptr(g), stream())
+        return g
+
+    def mech_action(self, x, g=None, *, d=None, mask=None):
+        """A(g) x (operator.py:1171-1194); ``d`` instead of ``g`` fuses the degradation."""
+        x = self._check("x", x, (self.n_mech,))
+        gq = None if g is None else self._check("g", g, (self.n_elements, 8), x.dtype)
+        dd = None if d is None else self._check("d", d, (self.n_red,)).to(x.dtype)
+        mk = None if mask is None else mask.to(torch.uint8).contiguous()
+        y = torch.empty_like(x)
+        call("phastb_h8_mech_apply", self.vgrid, self.mat, ptr(self.slot), self._dt(x), ptr(x), ptr(gq), ptr(dd),
+             ptr(mk), ptr(y), self.scratch(x.dtype), stream())
+        return y
+
+    def mech_diagonal(self, g=None, *, d=None):
+        """Jacobi diagonal of A(g) (operator.py:1196-1254)."""
+        dtype = g.dtype if g is not None else (d.dtype if d is not None else torch.float64)
+        gq = None if g is None else self._check("g", g, (self.n_elements, 8), dtype)
+        dd = None if d is None else self._check("d", d, (self.n_red,), dtype)
+        y = torch.empty(self.n_mech, dtype=dtype, device=self.device)
+        call("phastb_h8_mech_diagonal", self.vgrid, self.mat, ptr(self.slot), self._dt(y), ptr(gq), ptr(dd), ptr(y),
+             self.scratch(dtype), stream())
+        return y
+
+    def _stress_energy(self, x, g=None, d=None):
+        x = self._check("x", x, (self.n_mech,), torch.float64)
+        gq = None if g is None else self._check("g", g, (self.n_elements, 8), torch.float64)
+        dd = None if d is None else self._check("d", d, (self.n_red,), torch.float64)
+        rE = (C.c_double * 6)()
+        en = C.c_double(0.0)
+        call("phastb_h8_stress_energy", self.vgrid, self.mat, ptr(self.slot), ptr(x), ptr(gq), ptr(dd), rE,
+             C.byref(en), self.scratch(torch.float64), stream())
+        return np.array(list(rE)), float(en.value)
+
+    def macro_stress(self, x, g=None, *, d=None):
+        """Sigma = r_E / V (operator.py:1303-1316)."""
+        rE, _ = self._stress_energy(x, g, d)
+        return torch.as_tensor(rE / self.volume, dtype=torch.float64, device=self.device)
+
+    def elastic_energy(self, x, g=None, *, d=None):
+        _, en = self._stress_energy(x, g, d)
+        return torch.tensor(en, dtype=torch.float64, device=self.device)
+
+    def hill_mandel(self, x, g=None):
+        rE, en = self._stress_energy(x, g)
+        E = self.split_mech(x)[1].detach().cpu().numpy()
+        mean = 2.0 * en / self.volume
+        macro = float(np.dot(rE / self.volume, E))
+        scale = max(abs(mean), abs(macro))
+        return {"mean_work": mean, "macro_work": macro, "relative": abs(mean - macro) / scale if scale > 0 else 0.0}
+
+    def driving_force(self, x):
+        """Undamaged driving energy Y (E, 8) (operator.py:1415-1444)."""
+        return self.driving_history(x, None, want_Y=True)[0]
+
+    def driving_history(self, x, H_prev, want_Y=False):
+        """(Y or None, H = max(H_prev, Y)) in one kernel."""
+        x = self._check("x", x, (self.n_mech,), torch.float64)
+        Hp = None if H_prev is None else self._check("H_prev", H_prev, (self.n_elements, 8), torch.float64)
+        Y = torch.empty(self.n_elements, 8, dtype=torch.float64, device=self.device) if want_Y else None
+        H = None if (H_prev is None and want_Y) else torch.empty(self.n_elements, 8, dtype=torch.float64,
+                                                                 device=self.device)
+        call("phastb_h8_driving_history", self.vgrid, self.mat, ptr(self.slot), ptr(x), ptr(Hp), ptr(Y), ptr(H),
+             stream())
+        return Y, H
+
+    # -- damage ----------------------------------------------------------------------------
+    def damage_action(self, d, H=None, *, scale=1.0):
+        """Unscaled damage operator (operator.py:1450-1466)."""
+        d = self._check("d", d, (self.n_red,), torch.float64)
+        Hq = None if H is None else self._check("H", H, (self.n_elements, 8), torch.float64)
+        y = torch.empty_like(d)
+        call("phastb_h8_damage_apply", self.vgrid, self.mat, ptr(self.slot), ptr(d), ptr(Hq), float(scale), ptr(y),
+             self.scratch(), stream())
+        return y
+
+    def damage_rhs(self, H, *, scale=1.0):
+        Hq = None if H is None else self._check("H", H, (self.n_elements, 8), torch.float64)
+        y = torch.empty(self.n_red, dtype=torch.float64, device=self.device)
+        call("phastb_h8_damage_rhs_diag", self.vgrid, self.mat, ptr(self.slot), ptr(Hq), float(scale), ptr(y), None,
+             self.scratch(), stream())
+        return y
+
+    def damage_diagonal(self, H=None, *, scale=1.0):
+        Hq = None if H is None else self._check("H", H, (self.n_elements, 8), torch.float64)
+        y = torch.empty(self.n_red, dtype=torch.float64, device=self.device)
+        call("phastb_h8_damage_rhs_diag", self.vgrid, self.mat, ptr(self.slot), ptr(Hq), float(scale), None, ptr(y),
+             self.scratch(), stream())
+        return y
+
+    def damage_system(self, H, scaled=True):
+        """The scaled damage system; solved by ``solve_h8_scalar_box_kkt`` (operator.py:1495-1509)."""
+        return H8DamageSystem(self, H, self.damage_scale if scaled else 1.0)
+
+
+class H8DamageSystem:
+    """``H8ScalarSPDSystem`` of one history field (box_kkt_h8.py:64-122), evaluated on the device."""
+
+    def __init__(self, op, H, scale):
+        self.op, self.H, self.scale = op, H, float(scale)
+
+    @property
+    def n_dofs(self):
+        return self.op.n_red
+
+    def apply(self, field):
+        return self.op.damage_action(field, self.H, scale=self.scale)
+
+    action = apply
+
+    @property
+    def rhs(self):
+        return self.op.damage_rhs(self.H, scale=self.scale)
+
+    @property
+    def diagonal(self):
+        return self.op.damage_diagonal(self.H, scale=self.scale)
