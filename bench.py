@@ -37,10 +37,10 @@ METRIC = "staggered steps/s, chosen vs plain FP64 on 1 B200 at ≤1e-6 rel err; 
 UNIT = "staggered steps/s"
 N_CELL = 64
 INCREMENTS = 50
-# Mean per-increment iteration counts of this workload over increments 4..8
+# Mean per-increment iteration counts of this workload over increments 4..5
 # (the default timed window), measured with this repository's CUDA solver on a
 # B200; the CPU reference arm scales its timed per-iteration samples by them.
-REF_COUNTS = {"mech": 600.0, "pf": 60.0, "stag": 2.0}
+REF_COUNTS = {"mech": 232.5, "pf": 83.0, "stag": 3.0}
 
 
 def peaks():
