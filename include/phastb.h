@@ -39,6 +39,7 @@ extern "C" {
 #define PHASTB_NONFINITE 6       /* NaN/Inf met                                  */
 #define PHASTB_ERR_WORKSPACE 7   /* workspace too small                          */
 #define PHASTB_UNSUPPORTED 8     /* option not implemented (NotImplementedError) */
+#define PHASTB_ERR_CAPACITY 9    /* problem larger than a fixed-capacity entry point allows */
 
 #define PHASTB_F64 0
 #define PHASTB_F32 1
@@ -191,6 +192,21 @@ int phastb_h8_degradation(const phastb_voxel_grid* g, int dtype, const void* d, 
 int phastb_h8_mech_apply(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
                          int dtype, const void* x, const void* gq, const void* d, const uint8_t* mask,
                          void* y, void* scratch, void* stream);
+
+/* Allocation-free variant of phastb_h8_mech_apply (same arguments, same result, no
+ * scratch argument).  It has no counterpart in the reference: it serves callers that
+ * cannot allocate device memory, such as a host runtime bound through a thin FFI with
+ * no device-memory API, or an application whose GPU memory belongs entirely to another
+ * allocator.  Its element scratch is a file-scope device array for at most
+ * PHASTB_NOALLOC_MAX_VOXELS voxels (about 6.4 MB), held on every GPU that loads the
+ * library until exit.  Larger grids return PHASTB_ERR_CAPACITY.  The first call on a
+ * device looks up the array's device address (make that first call before any stream
+ * capture); the device current at the call must own `stream`.  All calls share the one
+ * array, so calls that overlap on the GPU (other streams, other host threads) race. */
+#define PHASTB_NOALLOC_MAX_VOXELS 32768
+int phastb_h8_mech_apply_noalloc(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                                 const uint8_t* slot, int dtype, const void* x, const void* gq,
+                                 const void* d, const uint8_t* mask, void* y, void* stream);
 
 /* Jacobi diagonal of A(g).  mech_diagonal, operator.py:1196-1254 */
 int phastb_h8_mech_diagonal(const phastb_voxel_grid* g, const phastb_voxel_material* m,

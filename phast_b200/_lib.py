@@ -14,7 +14,7 @@ import torch
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libphastb.so")
 
-OK, ERR_ARG, ERR_CUDA, NONCONVERGED, DIVERGED, BREAKDOWN, NONFINITE, ERR_WORKSPACE, UNSUPPORTED = range(9)
+OK, ERR_ARG, ERR_CUDA, NONCONVERGED, DIVERGED, BREAKDOWN, NONFINITE, ERR_WORKSPACE, UNSUPPORTED, ERR_CAPACITY = range(10)
 F64, F32 = 0, 1
 SPLITS = {"linear": 0, "isotropic": 1, "amor": 2, "spectral": 3, "star_convex": 4, "spectral_stress": 5}
 DRIVER_NONE, DRIVER_FULL, DRIVER_SPECTRAL = 0, 1, 2
@@ -72,6 +72,7 @@ SIGNATURES = {
     "phastb_h8_scratch_bytes": (sz, [VG, C.c_int]),
     "phastb_h8_degradation": (C.c_int, [VG, C.c_int, vp, C.c_double, vp, vp]),
     "phastb_h8_mech_apply": (C.c_int, [VG, VM, vp, C.c_int, vp, vp, vp, vp, vp, vp, vp]),
+    "phastb_h8_mech_apply_noalloc": (C.c_int, [VG, VM, vp, C.c_int, vp, vp, vp, vp, vp, vp]),
     "phastb_h8_mech_diagonal": (C.c_int, [VG, VM, vp, C.c_int, vp, vp, vp, vp, vp]),
     "phastb_h8_stress_energy": (C.c_int, [VG, VM, vp, vp, vp, vp, dp, dp, vp, vp]),
     "phastb_h8_driving_history": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, vp]),

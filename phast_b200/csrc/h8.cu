@@ -5,6 +5,7 @@
 #include "reduce.cuh"
 
 #include <cmath>
+#include <mutex>
 
 namespace phastb {
 
@@ -644,3 +645,66 @@ int phastb_h8_damage_rhs_diag(const phastb_voxel_grid* g, const phastb_voxel_mat
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ allocation-free elastic action
+//
+// Some callers cannot allocate device memory at all: a host runtime bound
+// through a thin FFI with no device-memory API of its own, or an application
+// whose GPU memory is owned entirely by another framework's pool and must not
+// see allocations it does not control.  For them the elastic action has a
+// variant whose element scratch is a file-scope device array, sized for at most
+// PHASTB_NOALLOC_MAX_VOXELS voxels and resident on every GPU that loads this
+// library until the process exits.  All calls share that one array.
+
+namespace phastb {
+
+constexpr size_t ca256(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t kNoAllocBytes = ca256(24 * sizeof(double) * (size_t)PHASTB_NOALLOC_MAX_VOXELS) +
+                                 ca256(sizeof(double) * kRedMaxK * kMaxPartials) + 256 +
+                                 ca256(sizeof(double) * kRedMaxK);
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once per
+// device (the array's name is only a host-side handle, not a device address).
+static int noalloc_scratch(void** out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return PHASTB_ERR_CUDA;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return PHASTB_ERR_ARG;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PHASTB_ERR_CUDA;
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return PHASTB_OK;
+}
+
+}  // namespace phastb
+
+extern "C" int phastb_h8_mech_apply_noalloc(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                                            const uint8_t* slot, int dtype, const void* x, const void* gq,
+                                            const void* d, const uint8_t* mask, void* y, void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !x || !y) return PHASTB_ERR_ARG;
+  if (dtype != PHASTB_F64 && dtype != PHASTB_F32) return PHASTB_ERR_ARG;
+  const VoxGeom v = make_vox_geom(*g);
+  if (v.n_elem > PHASTB_NOALLOC_MAX_VOXELS) return PHASTB_ERR_CAPACITY;
+  void* scratch = nullptr;
+  int st = noalloc_scratch(&scratch);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  // The array keeps the previous call's contents: the reduction ticket must start at zero.
+  const size_t elem = dtype == PHASTB_F32 ? sizeof(float) : sizeof(double);
+  RedWs ws = red_ws(static_cast<char*>(scratch) + align_up(24 * elem * (size_t)v.n_elem));
+  if ((st = red_ws_reset(ws, s))) return st;
+  if (dtype == PHASTB_F64)
+    return h8_mech_apply_t<double>(v, make_vox_mat<double>(*m), slot, (const double*)x, (const double*)gq,
+                                   (const double*)d, mask, (double*)y, scratch, nullptr, s);
+  return h8_mech_apply_t<float>(v, make_vox_mat<float>(*m), slot, (const float*)x, (const float*)gq,
+                                (const float*)d, mask, (float*)y, scratch, nullptr, s);
+}
