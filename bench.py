@@ -62,10 +62,11 @@ def workload_config():
     }
 
 
-def build_cell(device):
+def build_cell(device, n=None):
     from phast_b200 import solid3d as s3
-    h = 1.0 / N_CELL
-    shape = (N_CELL, N_CELL, N_CELL)
+    n = N_CELL if n is None else n
+    h = 1.0 / n
+    shape = (n, n, n)
     phase = s3.sphere_pore_phase(shape, 0.2)
     phases = [s3.PhaseMaterial("mi_matrix", 3000.0, 0.35, 0.5), s3.PhaseMaterial("pore", 3000.0 * 1e-6, 0.35, 0.5)]
     load = s3.LoadCase.ramp("zz", 2, 0.02, INCREMENTS)
@@ -327,6 +328,30 @@ def run_reference(args, rank, world):
     }
 
 
+def run_kernel_only(args, device):
+    """Elastic-action launches only, on an N^3 cell (the profiling case for ncu)."""
+    op, _ = build_cell(device, args.cell)
+    rng = np.random.default_rng(0)
+    x = torch.as_tensor(rng.normal(size=op.n_mech) * 1e-3, device=device)
+    d = torch.as_tensor(rng.uniform(0, 1, size=op.n_red), device=device)
+    dt = torch.float32 if args.fp32 else torch.float64
+    x, d = x.to(dt), d.to(dt)
+    for _ in range(args.warmup):
+        op.mech_action(x, d=d)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        op.mech_action(x, d=d)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    w = 4 if args.fp32 else 8
+    alg = 7 * op.n_red * w + op.n_elements
+    print(json.dumps({"kernel": "h8 elastic action", "cell": args.cell, "dtype": str(dt), "ms_per_apply": ms,
+                      "algorithmic_GBps": alg / ms / 1e6}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -334,6 +359,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--kernel-only", action="store_true", help="time the elastic action alone (profiling case)")
+    ap.add_argument("--cell", type=int, default=N_CELL, help="cell edge in voxels for --kernel-only")
+    ap.add_argument("--fp32", action="store_true", help="FP32 storage/arithmetic for --kernel-only")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -348,6 +376,9 @@ def main():
         return
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
+    if args.kernel_only:
+        run_kernel_only(args, device)
+        return
     if world > 1:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
