@@ -56,8 +56,8 @@ def workload_config():
     return {
         "workload": "3D periodic voxel H8 pore cell 64^3 (r=0.2 L, E x 1e-6), AT2 spectral, eps_zz 0->0.02 in 50 "
                     "increments; step = one staggered load increment",
-        "cells": 1, "voxels": N_CELL ** 3, "mechanics": "constrained Jacobi PCG rtol 1e-8",
-        "damage": "box-KKT active set + Dirichlet PCG", "form": "plain FP64",
+        "cells": 1, "voxels": N_CELL ** 3, "mechanics": "constrained PCG, FP64 residual rtol 1e-8",
+        "damage": "box-KKT active set + Dirichlet PCG (FP64)", "form": "",
         "l2": "flushed (256 MB write) before every timed step", "parallelism": "replicas",
     }
 
@@ -184,27 +184,32 @@ def cpu_step_estimate(counts):
 # our arm
 # ---------------------------------------------------------------------------
 
-def run_ours(args, rank, world, device):
-    from phast_b200 import _lib
-    op, solver = build_cell(device)
-    state = solver.initial_state()
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)  # 256 MB > 126 MB L2
-    for _ in range(args.warmup):
-        state, _ = solver.advance(state, op.load.targets[state.increment])
-    torch.cuda.synchronize()
-    snap = {k: getattr(state, k).detach().cpu().pin_memory() for k in ("x", "d", "H")}
-    snap_meta = (state.step, state.macro_strain.copy(), state.macro_stress.copy(), state.increment)
+def forms():
+    from phast_b200.solid3d import MechForm
+    return {"plain": MechForm(), "gmg": MechForm(precond="gmg"), "mixed": MechForm(mixed=True),
+            "mixed-gmg": MechForm(precond="gmg", mixed=True)}
 
-    # ---- device-resident timed region --------------------------------------------------
-    clocks = Clocks(torch.cuda.current_device())
-    lib = _lib.load()
-    if world > 1:
-        torch.distributed.barrier()
+
+FORM_LABEL = {
+    "plain": "plain FP64: Jacobi PCG (PhAST's algorithm), FP64 box-KKT damage",
+    "gmg": "FP64 PCG with a 3-level voxel multigrid V-cycle (Chebyshev deg 2, coarse deg 8)",
+    "mixed": "FP32 Jacobi PCG (FP64 dots) under FP64 iterative refinement",
+    "mixed-gmg": "FP32 PCG with an FP32 3-level multigrid V-cycle (FP64 dots) under FP64 iterative refinement; "
+                 "FP64 box-KKT damage",
+}
+
+
+def run_steps(op, form, snap, meta, steps, flush, device, clocks=None):
+    """Timed staggered increments from a host snapshot; device time per step with CUDA events."""
+    from phast_b200.solid3d import SolverState, StaggeredSolver
+    solver = StaggeredSolver(op, form=form)
+    state = SolverState(meta[0], snap["x"].to(device), snap["d"].to(device), snap["H"].to(device), meta[1].copy(),
+                        meta[2].copy(), meta[3])
     torch.cuda.synchronize()
-    clocks.start()
-    lib.phastb_launch_count_reset()
+    if clocks is not None:
+        clocks.start()
     total_ms, counts = 0.0, []
-    for _ in range(args.steps):
+    for _ in range(steps):
         flush_l2(flush)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -213,9 +218,34 @@ def run_ours(args, rank, world, device):
         torch.cuda.synchronize()
         total_ms += e0.elapsed_time(e1)
         counts.append((rec.pcg_iters_mech, rec.pcg_iters_pf, rec.stagger_iters))
-    launches = lib.phastb_launch_count()
+    clk = clocks.stop() if clocks is not None else None
+    return total_ms, state, counts, clk
+
+
+def run_ours(args, rank, world, device):
+    from phast_b200 import _lib
+    from phast_b200.solid3d import SolverState, StaggeredSolver
+    fm = forms()
+    chosen = fm[args.form]
+    op, solver = build_cell(device)
+    state = solver.initial_state()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)  # 256 MB > 126 MB L2
+    for _ in range(args.warmup):  # warm-up increments with the plain FP64 form (same start for both forms)
+        state, _ = solver.advance(state, op.load.targets[state.increment])
     torch.cuda.synchronize()
-    clk = clocks.stop()
+    snap = {k: getattr(state, k).detach().cpu().pin_memory() for k in ("x", "d", "H")}
+    meta = (state.step, state.macro_strain.copy(), state.macro_stress.copy(), state.increment)
+    # one untimed increment of the chosen form warms its workspaces and kernels
+    run_steps(op, chosen, snap, meta, 1, flush, device)
+
+    # ---- chosen form, device-resident timed region -----------------------------------
+    lib = _lib.load()
+    if world > 1:
+        torch.distributed.barrier()
+    lib.phastb_launch_count_reset()
+    clocks = Clocks(torch.cuda.current_device())
+    total_ms, st_c, counts, clk = run_steps(op, chosen, snap, meta, args.steps, flush, device, clocks)
+    launches = lib.phastb_launch_count()
     t = torch.tensor([total_ms], dtype=torch.float64, device=device)
     if world > 1:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -223,23 +253,39 @@ def run_ours(args, rank, world, device):
     max_ms = float(t.item())
     value = args.steps * world / (max_ms / 1e3)
 
+    # ---- plain FP64 form on the same increments (the comparison of the metric) --------
+    plain_ms, st_p, counts_p, _ = run_steps(op, fm["plain"], snap, meta, args.steps, flush, device)
+    tp = torch.tensor([plain_ms], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(tp, op=torch.distributed.ReduceOp.MAX)
+    plain_value = args.steps * world / (float(tp.item()) / 1e3)
+
+    def relerr(a, b):
+        nb = float(torch.linalg.vector_norm(b))
+        return float(torch.linalg.vector_norm(a - b)) / (nb if nb > 0 else 1.0)
+
+    err = {"x": relerr(st_c.x, st_p.x), "d": relerr(st_c.d, st_p.d),
+           "macro_stress": float(np.linalg.norm(st_c.macro_stress - st_p.macro_stress) /
+                                 max(np.linalg.norm(st_p.macro_stress), 1e-300)),
+           "crack_support_equal": bool(torch.equal(st_c.d > 0.9, st_p.d > 0.9))}
+
     # ---- end to end through the public API with host buffers ---------------------------
-    from phast_b200.solid3d import SolverState
+    solver_c = StaggeredSolver(op, form=chosen)
     pinned_out = {k: torch.empty_like(v).pin_memory() for k, v in snap.items()}
     dev_in = {k: torch.empty(v.shape, dtype=v.dtype, device=device) for k, v in snap.items()}
     h2d = sum(v.numel() * v.element_size() for v in snap.values())
-    st_meta = snap_meta
+    st_meta = meta
     e2e_ms = 0.0
-    host_state = {k: v for k, v in snap.items()}
+    host_state = dict(snap)
     for _ in range(args.steps):
         flush_l2(flush)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for k in dev_in:
             dev_in[k].copy_(host_state[k], non_blocking=True)
-        s_in = SolverState(st_meta[0], dev_in["x"].clone(), dev_in["d"].clone(), dev_in["H"].clone(), st_meta[1],
-                           st_meta[2], st_meta[3])
-        s_out, _ = solver.advance(s_in, op.load.targets[s_in.increment])
+        s_in = SolverState(st_meta[0], dev_in["x"].clone(), dev_in["d"].clone(), dev_in["H"].clone(),
+                           st_meta[1].copy(), st_meta[2].copy(), st_meta[3])
+        s_out, _ = solver_c.advance(s_in, op.load.targets[s_in.increment])
         for k in pinned_out:
             pinned_out[k].copy_(getattr(s_out, k), non_blocking=True)
         e1.record()
@@ -253,7 +299,9 @@ def run_ours(args, rank, world, device):
     e2e_value = args.steps * world / (float(te.item()) / 1e3)
 
     # ---- dominant kernel: the elastic action (element kernel + node gather) ------------
-    x, d = state.x.contiguous(), state.d.contiguous()
+    mixed = chosen.mixed
+    kdt = torch.float32 if mixed else torch.float64
+    x, d = st_c.x.to(kdt).contiguous(), st_c.d.to(kdt).contiguous()
     for _ in range(3):
         op.mech_action(x, d=d)
     n_rep, ms = 20, 0.0
@@ -266,21 +314,28 @@ def run_ours(args, rank, world, device):
         torch.cuda.synchronize()
         ms += e0.elapsed_time(e1)
     apply_s = ms / n_rep / 1e3
-    alg_bytes = 7 * op.n_red * 8 + op.n_elements * 1  # read u~ 3n, d n; write 3n (FP64); slot id per voxel
+    wsz = 4 if mixed else 8
+    alg_bytes = 7 * op.n_red * wsz + op.n_elements * 1  # read u~ 3n, d n; write 3n; slot id per voxel
     peak, peak_src = peaks()
     achieved = alg_bytes / apply_s / 1e9
-    traffic = profile_traffic()
     mech = float(np.mean([c[0] for c in counts]))
     pf = float(np.mean([c[1] for c in counts]))
     stag = float(np.mean([c[2] for c in counts]))
+    mech_p = float(np.mean([c[0] for c in counts_p]))
     dof_updates = (mech * op.n_mech + pf * op.n_red) * args.steps * world / (max_ms / 1e3)
-
+    cfg = workload_config()
+    cfg["form"] = FORM_LABEL[args.form]
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic", "config": workload_config(),
+        "dtype": "f32 (f64 dots, f64 refinement)" if mixed else "f64", "data": "synthetic", "config": cfg,
+        "plain_fp64": {"value": plain_value, "unit": UNIT, "ms_per_step": float(tp.item()) / args.steps,
+                       "mech_iters_per_step": mech_p},
+        "speedup_vs_plain_fp64": value / plain_value,
+        "rel_err_vs_plain_fp64": err,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "h8 elastic action (element kernel + node gather), FP64",
+                     "traffic": profile_traffic(mixed),
+                     "kernel": f"h8 elastic action (element kernel + node gather), {'FP32' if mixed else 'FP64'}",
                      "algorithmic_bytes": alg_bytes, "launch_ms": apply_s * 1e3, "peak_source": peak_src},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
         "gpu_launches": int(launches),
@@ -289,20 +344,21 @@ def run_ours(args, rank, world, device):
         "dof_updates_per_s": dof_updates,
     }
     if world == 1 and rank == 0 and not args.no_cpu:
-        sec, sample = cpu_step_estimate({"mech": mech, "pf": pf, "stag": stag})
+        sec, sample = cpu_step_estimate({"mech": mech_p, "pf": pf, "stag": stag})
         out["cpu_baseline"] = {"value": 1.0 / sec, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                                "sample": sample}
     return out
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the elastic action from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "h8_mech_apply_64.txt")
+def profile_traffic(fp32):
+    """DRAM bytes per 64^3 launch of the elastic action from the committed ncu summary, if any."""
+    key = "traffic_bytes_per_apply_64_fp32:" if fp32 else "traffic_bytes_per_apply_64_fp64:"
     try:
-        with open(path) as f:
-            for line in f:
-                if line.startswith("traffic_bytes_per_apply:"):
-                    return float(line.split(":")[1])
+        for name in sorted(os.listdir(os.path.join(ROOT, "profiles"))):
+            with open(os.path.join(ROOT, "profiles", name)) as f:
+                for line in f:
+                    if line.startswith(key):
+                        return float(line.split(":")[1])
     except OSError:
         pass
     return None
@@ -359,6 +415,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--form", default="mixed-gmg", choices=["plain", "gmg", "mixed", "mixed-gmg"],
+                    help="mechanics form of the timed value (the plain FP64 form is timed beside it)")
     ap.add_argument("--kernel-only", action="store_true", help="time the elastic action alone (profiling case)")
     ap.add_argument("--cell", type=int, default=N_CELL, help="cell edge in voxels for --kernel-only")
     ap.add_argument("--fp32", action="store_true", help="FP32 storage/arithmetic for --kernel-only")

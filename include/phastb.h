@@ -248,6 +248,37 @@ int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material
                          int* info, double* rinfo, void* workspace, size_t workspace_bytes,
                          void* stream);
 
+/* Options of the extended mechanics solve. */
+typedef struct {
+  int precond;        /* 0 Jacobi (the reference's), 1 geometric multigrid V-cycle */
+  int mixed;          /* 0 FP64 PCG; 1 FP32 inner PCG (FP64 dot products) + FP64 iterative refinement */
+  int levels;         /* multigrid levels, 2 or 3 (grid edges divisible by 2^(levels-1)) */
+  int smooth_degree;  /* Chebyshev degree of the pre/post smoother */
+  int coarse_degree;  /* Chebyshev degree on the coarsest level */
+  int power_iters;    /* power iterations for lambda_max(D^-1 A) per level */
+  double lmax_safety; /* Chebyshev interval [lambda_max/30, lmax_safety * lambda_max] */
+  double inner_rtol;  /* mixed: relative residual reduction of each inner FP32 solve */
+  int max_refine;     /* mixed: most refinement steps */
+} phastb_mech_opts;
+
+/* Constrained mechanics solve A(g(d)) x = 0 with x = fixed_values on fixed, stopped on the
+ * FP64 residual ||r|| <= max(rtol ||b_f||, atol) like solve_constrained (linalg.py:223-287),
+ * with a multigrid preconditioner and/or FP32 inner solves under FP64 iterative refinement
+ * (after mixed_precision_cg.py:18-95).  The voxel multigrid has no counterpart in PhAST's 3D
+ * code (its 2D GMG/AMG semantics: multigrid.py:534-576, 996-1089).  info[0] iterations,
+ * info[1] converged; rinfo[0] ||b_f||, rinfo[1] final FP64 ||r||.  lmax_io (host, one value per
+ * multigrid level, may be NULL): when lmax_io[0] > 0 these lambda_max(D^-1 A) estimates are used,
+ * otherwise they are estimated by power iteration and written back, so a caller can reuse them
+ * across the solves of one load increment.  Returns 0 bytes for unsupported options (grid not
+ * divisible for the requested levels). */
+size_t phastb_h8_mech_solve_ex_workspace_bytes(const phastb_voxel_grid* g, const phastb_mech_opts* o);
+int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                            const uint8_t* slot, const double* d, const uint8_t* fixed,
+                            const double* fixed_values, const double* x0, double rtol, double atol,
+                            int maxiter, int check_every, const phastb_mech_opts* o, double* lmax_io,
+                            double* x_out, int* info, double* rinfo, void* workspace,
+                            size_t workspace_bytes, void* stream);
+
 /* Box-constrained damage solve lower <= d <= upper by the primal active-set method
  * with a Dirichlet PCG per set (scale applied to the system).
  * solve_h8_scalar_box_kkt + solve_h8_scalar_dirichlet_pcg, solvers/box_kkt_h8.py:256-778.

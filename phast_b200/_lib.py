@@ -44,7 +44,15 @@ class VoxelMaterial(C.Structure):
                 ("driver", C.c_int * MAX_SLOTS), ("kappa", C.c_double), ("ell", C.c_double)]
 
 
+class MechOpts(C.Structure):
+    _fields_ = [("precond", C.c_int), ("mixed", C.c_int), ("levels", C.c_int), ("smooth_degree", C.c_int),
+                ("coarse_degree", C.c_int), ("power_iters", C.c_int), ("lmax_safety", C.c_double),
+                ("inner_rtol", C.c_double),
+                ("max_refine", C.c_int)]
+
+
 Q4G, Q4M, VG, VM = C.POINTER(Q4Grid), C.POINTER(Q4Material), C.POINTER(VoxelGrid), C.POINTER(VoxelMaterial)
+MO = C.POINTER(MechOpts)
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -81,6 +89,9 @@ SIGNATURES = {
     "phastb_h8_mech_solve_workspace_bytes": (sz, [VG, C.c_int]),
     "phastb_h8_mech_solve": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_int,
                                        vp, ip, dp, vp, sz, vp]),
+    "phastb_h8_mech_solve_ex_workspace_bytes": (sz, [VG, MO]),
+    "phastb_h8_mech_solve_ex": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_int, MO,
+                                          dp, vp, ip, dp, vp, sz, vp]),
     "phastb_h8_box_kkt_workspace_bytes": (sz, [VG]),
     "phastb_h8_damage_box_kkt": (C.c_int, [VG, VM, vp, vp, C.c_double, vp, C.c_double, vp, C.c_double, C.c_double,
                                            C.c_int, C.c_int, vp, ip, vp, sz, vp]),

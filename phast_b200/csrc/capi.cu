@@ -5,7 +5,48 @@
 
 namespace phastb {
 static std::atomic<long long> g_launches{0};
-void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_launch(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+namespace {
+struct DevStreams {
+  cudaStream_t s = nullptr;
+  cudaEvent_t in = nullptr, out = nullptr;
+};
+constexpr int kMaxDev = 64;
+thread_local DevStreams t_streams[kMaxDev];
+}  // namespace
+
+ScopedStream::ScopedStream(cudaStream_t caller) : caller_(caller) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) {
+    st_ = PHASTB_ERR_CUDA;
+    s_ = caller;
+    return;
+  }
+  DevStreams& d = t_streams[dev];
+  if (!d.s) {
+    if (cudaStreamCreateWithFlags(&d.s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&d.in, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&d.out, cudaEventDisableTiming) != cudaSuccess) {
+      st_ = PHASTB_ERR_CUDA;
+      s_ = caller;
+      d.s = nullptr;
+      return;
+    }
+  }
+  s_ = d.s;
+  out_ = d.out;
+  if (cudaEventRecord(d.in, caller) != cudaSuccess || cudaStreamWaitEvent(s_, d.in, 0) != cudaSuccess)
+    st_ = PHASTB_ERR_CUDA;
+}
+
+ScopedStream::~ScopedStream() {
+  if (s_ != caller_ && out_) {
+    cudaEventRecord(out_, s_);
+    cudaStreamWaitEvent(caller_, out_, 0);
+  }
+}
 }  // namespace phastb
 
 extern "C" {

@@ -123,7 +123,25 @@ template <typename T> __device__ __forceinline__ T ld(const T* p) { return __ldg
 
 // Host-side count of kernel launches issued by this library (every launch site
 // is wrapped as `{ note_launch(); kernel<<<...>>>(...); }`).
-void note_launch();
+void note_launch(long long n = 1);
+long long launch_count();
+
+// Solver entry points run on a library-owned non-blocking stream (one per device
+// and host thread), ordered after the caller's stream on entry and before it on
+// exit.  Iteration chunks can then be captured in CUDA graphs, which the legacy
+// default stream does not allow.
+class ScopedStream {
+ public:
+  explicit ScopedStream(cudaStream_t caller);
+  ~ScopedStream();
+  cudaStream_t get() const { return s_; }
+  int status() const { return st_; }
+
+ private:
+  cudaStream_t caller_ = nullptr, s_ = nullptr;
+  cudaEvent_t out_ = nullptr;
+  int st_ = 0;
+};
 
 inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? PHASTB_OK : PHASTB_ERR_CUDA; }
 

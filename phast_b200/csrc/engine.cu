@@ -2,8 +2,68 @@
 #include "engine.cuh"
 
 #include <cmath>
+#include <list>
 
 namespace phastb {
+
+// ================================================================= graph cache
+
+namespace {
+struct GraphEntry {
+  int dev;
+  GraphKey key;
+  cudaGraphExec_t exec;
+  long long launches;
+};
+constexpr size_t kGraphCacheSize = 48;
+thread_local std::list<GraphEntry> t_graph_cache;
+}  // namespace
+
+cudaGraphExec_t graph_for(const GraphKey& key, cudaStream_t s, const std::function<int()>& body, long long* count) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  for (auto it = t_graph_cache.begin(); it != t_graph_cache.end(); ++it) {
+    if (it->dev == dev && it->key == key) {
+      t_graph_cache.splice(t_graph_cache.begin(), t_graph_cache, it);
+      *count = t_graph_cache.front().launches;
+      return t_graph_cache.front().exec;
+    }
+  }
+  const long long c0 = launch_count();
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  const int st = body();
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &g);
+  const long long n = launch_count() - c0;
+  note_launch(-n);  // captured, not executed
+  if (st != PHASTB_OK || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return nullptr;
+  }
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0ULL);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess || !exec) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  t_graph_cache.push_front(GraphEntry{dev, key, exec, n});
+  while (t_graph_cache.size() > kGraphCacheSize) {
+    cudaGraphExecDestroy(t_graph_cache.back().exec);
+    t_graph_cache.pop_back();
+  }
+  *count = n;
+  return exec;
+}
+
+static int launch_graph(cudaGraphExec_t g, long long count, cudaStream_t s) {
+  note_launch(count);
+  return cuda_status(cudaGraphLaunch(g, s));
+}
 
 // ======================================================================= PPCG
 
@@ -286,17 +346,36 @@ int ppcg_solve(const LinOp<double>& A, int n, const PpcgWs& w, const double* d_p
   int it = 0;
   const int* go = &w.st->go;
   const int* go_resid = &w.st->go_resid;
-  while (it < max_iter) {
-    const int chunk = std::min(check_every, max_iter - it);
-    for (int k = 0; k < chunk; ++k) {
-      if ((st = A(w.p, w.Ap, go, s))) return st;
+  auto iterate = [&](int k_iters) -> int {
+    int e;
+    for (int k = 0; k < k_iters; ++k) {
+      if ((e = A(w.p, w.Ap, go, s))) return e;
       { note_launch(); ppcg_dir_stats_kernel<<<G, kThreads, 0, s>>>(n, w, d); }
       { note_launch(); ppcg_update_kernel<<<G, kThreads, 0, s>>>(n, w, d); }
-      if ((st = A(d, w.Ad, go_resid, s))) return st;
+      if ((e = A(d, w.Ad, go_resid, s))) return e;
       { note_launch(); ppcg_resid_kernel<<<G, kThreads, 0, s>>>(n, w, d, fixed); }
       { note_launch(); ppcg_dir_kernel<<<G, kThreads, 0, s>>>(n, w); }
     }
-    if ((st = last_launch_status())) return st;
+    return last_launch_status();
+  };
+  GraphKey key;
+  key_val(key, A.apply);
+  key_add(key, A.ctx, A.ctx_bytes);
+  key_val(key, w);
+  key_val(key, d);
+  key_val(key, fixed);
+  key_val(key, n);
+  key_val(key, check_every);
+  long long glaunch = 0;
+  cudaGraphExec_t gexec =
+      max_iter >= check_every ? graph_for(key, s, [&] { return iterate(check_every); }, &glaunch) : nullptr;
+  while (it < max_iter) {
+    const int chunk = std::min(check_every, max_iter - it);
+    if (gexec && chunk == check_every) {
+      if ((st = launch_graph(gexec, glaunch, s))) return st;
+    } else if ((st = iterate(chunk))) {
+      return st;
+    }
     it += chunk;
     if ((st = cuda_status(cudaMemcpyAsync(&hs, w.st, sizeof(hs), cudaMemcpyDeviceToHost, s)))) return st;
     if ((st = cuda_status(cudaStreamSynchronize(s)))) return st;
@@ -570,19 +649,46 @@ int pcg_run(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T* in
     return PHASTB_OK;
   }
   int it = 0;
-  while (it < maxiter) {
-    const int chunk = std::min(check_every, maxiter - it);
-    for (int k = 0; k < chunk; ++k) {
-      if ((st = A(w.p, w.Ap, active, s))) return st;
+  auto iterate = [&](int k_iters) -> int {
+    int e;
+    for (int k = 0; k < k_iters; ++k) {
+      if ((e = A(w.p, w.Ap, active, s))) return e;
       { note_launch(); pcg_alpha_kernel<T><<<G, kThreads, 0, s>>>(n, w, mode); }
       { note_launch(); pcg_update_kernel<T><<<G, kThreads, 0, s>>>(n, w, x, inv_diag, custom, mode, check_every); }
       if (custom) {
-        if ((st = M->apply(M->ctx, w.r, w.z, active, s))) return st;
+        if ((e = M->apply(M->ctx, w.r, w.z, active, s))) return e;
         { note_launch(); pcg_rz_kernel<T><<<G, kThreads, 0, s>>>(n, w, 0, mode); }
       }
       { note_launch(); pcg_dir_kernel<T><<<G, kThreads, 0, s>>>(n, w); }
     }
-    if ((st = last_launch_status())) return st;
+    return last_launch_status();
+  };
+  GraphKey key;
+  key_val(key, A.apply);
+  key_add(key, A.ctx, A.ctx_bytes);
+  key_val(key, custom);
+  if (custom) {
+    key_val(key, M->apply);
+    key_add(key, M->ctx, M->ctx_bytes);
+  }
+  key_val(key, w);
+  key_val(key, x);
+  key_val(key, inv_diag);
+  key_val(key, n);
+  key_val(key, mode);
+  key_val(key, check_every);
+  const int size_t_ = sizeof(T);
+  key_val(key, size_t_);
+  long long glaunch = 0;
+  cudaGraphExec_t gexec =
+      maxiter >= check_every ? graph_for(key, s, [&] { return iterate(check_every); }, &glaunch) : nullptr;
+  while (it < maxiter) {
+    const int chunk = std::min(check_every, maxiter - it);
+    if (gexec && chunk == check_every) {
+      if ((st = launch_graph(gexec, glaunch, s))) return st;
+    } else if ((st = iterate(chunk))) {
+      return st;
+    }
     it += chunk;
     if ((st = cuda_status(cudaMemcpyAsync(&hs, w.st, sizeof(hs), cudaMemcpyDeviceToHost, s)))) return st;
     if ((st = cuda_status(cudaStreamSynchronize(s)))) return st;

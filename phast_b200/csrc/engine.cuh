@@ -16,6 +16,9 @@
 #pragma once
 #include "reduce.cuh"
 
+#include <functional>
+#include <vector>
+
 namespace phastb {
 
 // A linear operator y = A x on device vectors.  `guard` (device int, may be
@@ -24,6 +27,7 @@ template <typename T>
 struct LinOp {
   int (*apply)(const void* ctx, const T* x, T* y, const int* guard, cudaStream_t s);
   const void* ctx;
+  size_t ctx_bytes;  // size of *ctx: the bytes that identify a captured iteration graph
   int operator()(const T* x, T* y, const int* guard, cudaStream_t s) const { return apply(ctx, x, y, guard, s); }
 };
 
@@ -90,6 +94,7 @@ template <typename T>
 struct Precond {
   int (*apply)(const void* ctx, const T* r, T* z, const int* guard, cudaStream_t s);
   const void* ctx;
+  size_t ctx_bytes;
 };
 
 // Solves A x = b from x (initial guess held in x, zero allowed).  The caller
@@ -112,5 +117,20 @@ int pcg_run(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T* in
 // Vector helpers used by the drivers.
 template <typename T>
 int vec_norm2(const T* x, int n, double* host, void* red_ws_base, cudaStream_t s);
+
+// CUDA-graph cache of captured iteration chunks (per host thread and device).
+// `key` must hold every value the captured launches depend on.
+using GraphKey = std::vector<unsigned char>;
+inline void key_add(GraphKey& k, const void* p, size_t n) {
+  const unsigned char* c = static_cast<const unsigned char*>(p);
+  k.insert(k.end(), c, c + n);
+}
+template <typename V>
+inline void key_val(GraphKey& k, const V& v) {
+  key_add(k, &v, sizeof(V));
+}
+// Returns the executable graph of `body` (captured on s) or nullptr when the
+// stream cannot be captured; *count receives the kernel launches per replay.
+cudaGraphExec_t graph_for(const GraphKey& key, cudaStream_t s, const std::function<int()>& body, long long* count);
 
 }  // namespace phastb

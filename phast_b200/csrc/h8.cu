@@ -44,7 +44,7 @@ __device__ __forceinline__ void load_g(const VoxGeom& g, const T* __restrict__ g
 
 // ------------------------------------------------------------ elastic action
 
-template <typename T>
+template <typename T, bool ENERGY>
 __global__ void __launch_bounds__(kThreads) h8_mech_elem_kernel(VoxGeom g, VoxMat<T> m,
                                                                 const uint8_t* __restrict__ slot,
                                                                 const T* __restrict__ x, const T* __restrict__ gq,
@@ -100,10 +100,9 @@ __global__ void __launch_bounds__(kThreads) h8_mech_elem_kernel(VoxGeom g, VoxMa
           const T gw = gv[qx + 2 * qy + 4 * qz] * w;
 #pragma unroll
           for (int k = 0; k < 6; ++k) sg[k] *= gw;
+          if (ENERGY) {
 #pragma unroll
-          for (int k = 0; k < 6; ++k) {
-            acc[k] += double(sg[k]);
-            acc[6] += 0.5 * double(sg[k]) * double(ep[k]);
+            for (int k = 0; k < 6; ++k) acc[6] += 0.5 * double(sg[k]) * double(ep[k]);
           }
           P[0][0][qz][qy] += sg[0];
           P[0][1][qz][qx] += sg[5];
@@ -115,6 +114,18 @@ __global__ void __launch_bounds__(kThreads) h8_mech_elem_kernel(VoxGeom g, VoxMa
           P[2][1][qz][qx] += sg[3];
           P[2][2][qy][qx] += sg[2];
         }
+    // r_E = sum_q w g sigma: each stress component is summed by one P block
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        acc[0] += double(P[0][0][i][j]);
+        acc[1] += double(P[1][1][i][j]);
+        acc[2] += double(P[2][2][i][j]);
+        acc[3] += double(P[1][2][i][j]);
+        acc[4] += double(P[0][2][i][j]);
+        acc[5] += double(P[0][1][i][j]);
+      }
     if (scratch) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -126,14 +137,15 @@ __global__ void __launch_bounds__(kThreads) h8_mech_elem_kernel(VoxGeom g, VoxMa
     }
   }
   __shared__ double sh[32];
+  constexpr int NK = ENERGY ? 7 : 6;
 #pragma unroll
-  for (int k = 0; k < 7; ++k) {
+  for (int k = 0; k < NK; ++k) {
     const double sm = block_sum(acc[k], sh);
     if (threadIdx.x == 0) ws.part[k * kMaxPartials + blockIdx.x] = sm;
   }
   if (arrive_last(ws.counter)) {
 #pragma unroll
-    for (int k = 0; k < 7; ++k) {
+    for (int k = 0; k < NK; ++k) {
       const double t = fold_sum(ws.part + k * kMaxPartials, gridDim.x, sh);
       if (threadIdx.x == 0) {
         ws.out[k] = t;
@@ -468,7 +480,7 @@ int h8_mech_apply_t(const VoxGeom& v, const VoxMat<T>& mm, const uint8_t* slot, 
                     const T* d, const uint8_t* mask, T* y, void* scratch, const int* guard, cudaStream_t s) {
   T* sc = static_cast<T*>(scratch);
   RedWs ws = red_ws(static_cast<char*>(scratch) + align_up(24 * sizeof(T) * (size_t)v.n_elem));
-  { note_launch(); h8_mech_elem_kernel<T><<<grid_for(v.n_elem), kThreads, 0, s>>>(v, mm, slot, x, gq, d, sc, y, mask, ws, guard); }
+  { note_launch(); h8_mech_elem_kernel<T, false><<<grid_for(v.n_elem), kThreads, 0, s>>>(v, mm, slot, x, gq, d, sc, y, mask, ws, guard); }
   { note_launch(); h8_gather_kernel<T, 3><<<grid_for(v.n_red), kThreads, 0, s>>>(v, sc, y, mask, guard); }
   return last_launch_status();
 }
@@ -598,7 +610,7 @@ int phastb_h8_stress_energy(const phastb_voxel_grid* g, const phastb_voxel_mater
   RedWs ws = red_ws(static_cast<char*>(scratch) + align_up(8 * 24 * (size_t)v.n_elem));
   int st = red_ws_reset(ws, s);
   if (st) return st;
-  { note_launch(); h8_mech_elem_kernel<double><<<grid_for(v.n_elem), kThreads, 0, s>>>(
+  { note_launch(); h8_mech_elem_kernel<double, true><<<grid_for(v.n_elem), kThreads, 0, s>>>(
       v, make_vox_mat<double>(*m), slot, x, gq, d, nullptr, nullptr, nullptr, ws, nullptr); }
   if ((st = last_launch_status())) return st;
   double o[7];

@@ -26,11 +26,13 @@ struct VoxGeom {
   int nx, ny, nz, px, py, pz;
   int rx, ry, rz;  // reduced node counts per axis
   int n_red, n_elem;
+  int pad_;        // keeps the struct free of implicit padding (it is hashed as bytes)
   double hx, hy, hz, w;
 };
+static_assert(sizeof(VoxGeom) == 12 * sizeof(int) + 4 * sizeof(double), "VoxGeom has implicit padding");
 
 inline VoxGeom make_vox_geom(const phastb_voxel_grid& g) {
-  VoxGeom v;
+  VoxGeom v{};
   v.nx = g.nx; v.ny = g.ny; v.nz = g.nz;
   v.px = g.px != 0; v.py = g.py != 0; v.pz = g.pz != 0;
   v.rx = v.px ? g.nx : g.nx + 1;
@@ -49,8 +51,11 @@ struct VoxMat {
   T lam[PHASTB_MAX_SLOTS], mu[PHASTB_MAX_SLOTS], Gc[PHASTB_MAX_SLOTS];
   int driver[PHASTB_MAX_SLOTS];
   int iso;
+  int pad_;  // no implicit padding (hashed as bytes)
   T kappa, ell;
 };
+static_assert(sizeof(VoxMat<double>) == 8 * (PHASTB_MAX_SLOTS * 24 + 2) + 4 * (PHASTB_MAX_SLOTS + 2), "padding");
+static_assert(sizeof(VoxMat<float>) == 4 * (PHASTB_MAX_SLOTS * 24 + 2) + 4 * (PHASTB_MAX_SLOTS + 2), "padding");
 
 inline int tri_index(int i, int j) {  // i <= j
   return i * 6 - i * (i - 1) / 2 + (j - i);

@@ -1,6 +1,9 @@
 // 2D solver drivers over the structured-Q4 operators: the bound-projected
 // PCG damage solve and the quasi-static Newton / matrix-free CG mechanics.
 #include "engine.cuh"
+
+#include <cstddef>
+#include <cstring>
 #include "q4_kernels.cuh"
 
 #include <cmath>
@@ -15,7 +18,7 @@ int q4_force_launch(const phastb_q4_grid* g, const phastb_q4_material* m, const 
                     double* f, const uint8_t* mask, const int* guard, cudaStream_t s);
 
 struct Q4DamageCtx {
-  const phastb_q4_grid* g;
+  phastb_q4_grid g;
   const double* Hq;
   double rsh;
   const double* rsh_e;
@@ -25,19 +28,19 @@ struct Q4DamageCtx {
 
 static int q4_damage_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
   const Q4DamageCtx* k = static_cast<const Q4DamageCtx*>(c);
-  return q4_damage_apply_launch(k->g, x, k->Hq, 2.0, k->rsh, k->rsh_e, k->gcl0, k->gcl0_e, y, guard, s);
+  return q4_damage_apply_launch(&k->g, x, k->Hq, 2.0, k->rsh, k->rsh_e, k->gcl0, k->gcl0_e, y, guard, s);
 }
 
 struct Q4ForceCtx {
-  const phastb_q4_grid* g;
-  const phastb_q4_material* m;
+  phastb_q4_grid g;
+  phastb_q4_material m;
   const double* d;
   const uint8_t* mask;
 };
 
 static int q4_force_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
   const Q4ForceCtx* k = static_cast<const Q4ForceCtx*>(c);
-  return q4_force_launch(k->g, k->m, x, k->d, y, k->mask, guard, s);
+  return q4_force_launch(&k->g, &k->m, x, k->d, y, k->mask, guard, s);
 }
 
 // residual r = (f_ext - f) * free, and u[bc] = bc_vals helpers
@@ -89,12 +92,14 @@ int phastb_q4_damage_solve(const phastb_q4_grid* g, const double* Hq, double gc_
   if (fixed && !fixed_vals) return PHASTB_ERR_ARG;
   const int n = (g->nx + 1) * (g->ny + 1);
   if (!workspace || workspace_bytes < ppcg_ws_bytes(n)) return PHASTB_ERR_WORKSPACE;
-  cudaStream_t s = (cudaStream_t)stream;
+  ScopedStream scope((cudaStream_t)stream);
+  if (scope.status()) return scope.status();
+  cudaStream_t s = scope.get();
   PpcgWs w = ppcg_ws(workspace, n);
-  int st = phastb_q4_damage_prepare(g, Hq, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e, w.b, w.minv, stream);
+  int st = phastb_q4_damage_prepare(g, Hq, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e, w.b, w.minv, (void*)s);
   if (st) return st;
-  Q4DamageCtx ctx{g, Hq, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e};
-  LinOp<double> A{q4_damage_op, &ctx};
+  Q4DamageCtx ctx{*g, Hq, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e};
+  LinOp<double> A{q4_damage_op, &ctx, sizeof(ctx)};
   int inf[2] = {0, 0};
   st = ppcg_solve(A, n, w, d_prev, d_init, fixed, fixed_vals, tol, max_iter, check_every, d_out, inf, s);
   if (info) {
@@ -119,7 +124,9 @@ int phastb_q4_qs_solve(const phastb_q4_grid* g, const phastb_q4_material* m, con
     return PHASTB_UNSUPPORTED;  // split-aware tangents need the consistent-tangent kernel
   const int nn = (g->nx + 1) * (g->ny + 1), n2 = 2 * nn;
   if (!workspace || workspace_bytes < phastb_q4_qs_workspace_bytes(nn)) return PHASTB_ERR_WORKSPACE;
-  cudaStream_t s = (cudaStream_t)stream;
+  ScopedStream scope((cudaStream_t)stream);
+  if (scope.status()) return scope.status();
+  cudaStream_t s = scope.get();
   char* p = static_cast<char*>(workspace);
   PcgWs<double> w = pcg_ws<double>(p, n2);
   p += pcg_ws_bytes<double>(n2);
@@ -136,8 +143,15 @@ int phastb_q4_qs_solve(const phastb_q4_grid* g, const phastb_q4_material* m, con
 
   // u[bc] = bc_vals
   { note_launch(); qs_axpy_bc_kernel<<<G, kThreads, 0, s>>>(n2, u, 0.0, nullptr, bc_mask, bc_vals, u); }
-  Q4ForceCtx kctx{g, m, d, bc_mask};
-  LinOp<double> K{q4_force_op, &kctx};
+  // The context is hashed as bytes (graph cache): zero it, then copy the material's
+  // fields without its trailing padding.
+  Q4ForceCtx kctx;
+  std::memset(&kctx, 0, sizeof(kctx));
+  kctx.g = *g;
+  std::memcpy(&kctx.m, m, offsetof(phastb_q4_material, psi_split) + sizeof(int));
+  kctx.d = d;
+  kctx.mask = bc_mask;
+  LinOp<double> K{q4_force_op, &kctx, sizeof(kctx)};
 
   auto residual_norm = [&](const double* uu, double* r, double* nrm, bool* finite) -> int {
     int e = q4_force_launch(g, m, uu, d, w.Ap, nullptr, nullptr, s);

@@ -242,7 +242,9 @@ int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material
     return PHASTB_ERR_ARG;
   if (!workspace || workspace_bytes < phastb_h8_mech_solve_workspace_bytes(g, PHASTB_F64))
     return PHASTB_ERR_WORKSPACE;
-  cudaStream_t s = (cudaStream_t)stream;
+  ScopedStream scope((cudaStream_t)stream);
+  if (scope.status()) return scope.status();
+  cudaStream_t s = scope.get();
   const VoxGeom v = make_vox_geom(*g);
   const VoxMat<double> mm = make_vox_mat<double>(*m);
   const int n = 3 * v.n_red + 6;
@@ -281,7 +283,7 @@ int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material
   }
   const double thr = std::max(rtol * bn, atol);
   MechCtx free_ctx{v, mm, slot, gq, d, fixed, scratch};
-  LinOp<double> A{mech_op, &free_ctx};
+  LinOp<double> A{mech_op, &free_ctx, sizeof(free_ctx)};
   PcgResult pr{};
   if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, x_out, thr, maxiter, check_every, PCG_FREEZE, 0.0, &pr, s)))
     return st;
@@ -310,7 +312,9 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
       !(lin_tol > 0) || !(kkt_tol >= 0))
     return PHASTB_ERR_ARG;
   if (!workspace || workspace_bytes < phastb_h8_box_kkt_workspace_bytes(g)) return PHASTB_ERR_WORKSPACE;
-  cudaStream_t s = (cudaStream_t)stream;
+  ScopedStream scope((cudaStream_t)stream);
+  if (scope.status()) return scope.status();
+  cudaStream_t s = scope.get();
   const VoxGeom v = make_vox_geom(*g);
   const VoxMat<double> mm = make_vox_mat<double>(*m);
   const int n = v.n_red;
@@ -347,7 +351,7 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
     if ((st = last_launch_status())) return st;
     // Dirichlet PCG on the free set: tolerance relative to max(||r0||, 1)
     DamageCtx fctx{v, mm, slot, H, scale, fixed, scratch};
-    LinOp<double> A{damage_op, &fctx};
+    LinOp<double> A{damage_op, &fctx, sizeof(fctx)};
     PcgResult pr{};
     if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, d_out, -lin_tol, max_lin, 10, PCG_STRICT, 0.0, &pr,
                               s)))
@@ -386,7 +390,9 @@ int phastb_h8_stagger_change(int n_u, const double* x_new, const double* x_old, 
                              void* stream) {
   if (!x_new || !x_old || !d_new || !d_old || !out_host || n_u < 0 || n_d < 0) return PHASTB_ERR_ARG;
   if (!workspace || workspace_bytes < red_ws_bytes()) return PHASTB_ERR_WORKSPACE;
-  cudaStream_t s = (cudaStream_t)stream;
+  ScopedStream scope((cudaStream_t)stream);
+  if (scope.status()) return scope.status();
+  cudaStream_t s = scope.get();
   RedWs rw = red_ws(workspace);
   int st = red_ws_reset(rw, s);
   if (st) return st;

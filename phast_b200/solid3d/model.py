@@ -65,8 +65,6 @@ class LoadCase:
         comps = sorted([int(self.controlled), *self.free, *self.fixed_zero])
         if comps != list(range(6)):
             raise ValueError("{controlled}, free and fixed_zero must partition {0,...,5}")
-        if self.free:
-            raise NotImplementedError("free macro-stress components are not implemented by the B200 backend")
 
     @property
     def n_increments(self):

@@ -72,6 +72,73 @@ def solve_constrained(op, *, fixed_mask, fixed_values, g=None, d=None, x0=None, 
 
 
 @dataclass(frozen=True)
+class MechForm:
+    """How the mechanics system is solved.
+
+    ``precond``: ``'jacobi'`` (PhAST's solve_constrained) or ``'gmg'`` (3-level voxel multigrid,
+    Chebyshev smoothing).  ``mixed``: FP32 inner PCG with FP64 dot products under FP64 iterative
+    refinement (the stopping test is always the FP64 residual).
+    """
+    precond: str = "jacobi"
+    mixed: bool = False
+    levels: int = 3
+    smooth_degree: int = 2
+    coarse_degree: int = 8
+    power_iters: int = 30
+    lmax_safety: float = 1.2
+    inner_rtol: float = 1e-4
+    max_refine: int = 30
+
+    def struct(self):
+        o = _lib.MechOpts()
+        o.precond = 1 if self.precond == "gmg" else 0
+        o.mixed = int(bool(self.mixed))
+        o.levels, o.smooth_degree, o.coarse_degree = self.levels, self.smooth_degree, self.coarse_degree
+        o.power_iters, o.inner_rtol, o.max_refine = self.power_iters, self.inner_rtol, self.max_refine
+        o.lmax_safety = self.lmax_safety
+        return o
+
+
+PLAIN = MechForm()
+
+
+def solve_constrained_form(op, form, *, fixed_mask, fixed_values, d=None, x0=None, rtol=1e-8, atol=0.0,
+                           maxiter=5000, check_every=10, lmax_cache=None):
+    """Constrained mechanics solve with a :class:`MechForm` (multigrid and/or mixed precision).
+
+    ``lmax_cache`` (a ctypes array of 3 doubles, zero to estimate) carries the multigrid's
+    lambda_max estimates from one solve to the next.
+    """
+    if form.precond == "jacobi" and not form.mixed:
+        return solve_constrained(op, fixed_mask=fixed_mask, fixed_values=fixed_values, d=d, x0=x0, rtol=rtol,
+                                 atol=atol, maxiter=maxiter, check_every=check_every)
+    n = op.n_mech
+    opts = form.struct()
+    nbytes = _lib.load().phastb_h8_mech_solve_ex_workspace_bytes(op.vgrid, opts)
+    if nbytes == 0:
+        raise NotImplementedError(f"mechanics form {form} is not available for a {op.shape} grid "
+                                  "(multigrid needs edges divisible by 2^(levels-1))")
+    mask = fixed_mask.to(torch.uint8).contiguous()
+    vals = fixed_values.to(torch.float64).contiguous()
+    x0c = None if x0 is None else x0.to(torch.float64).contiguous()
+    dd = (torch.zeros(op.n_red, dtype=torch.float64, device=op.device) if d is None
+          else d.to(torch.float64).contiguous())
+    out = torch.empty(n, dtype=torch.float64, device=op.device)
+    info = (C.c_int * 2)()
+    rinfo = (C.c_double * 2)()
+    wp, wn = op._ws.get(nbytes)
+    st = raw("phastb_h8_mech_solve_ex", op.vgrid, op.mat, ptr(op.slot), ptr(dd), ptr(mask), ptr(vals), ptr(x0c),
+             float(rtol), float(atol), int(maxiter), int(check_every), opts, lmax_cache, ptr(out), info, rinfo, wp, wn,
+             stream())
+    if st in (_lib.BREAKDOWN, _lib.NONFINITE):
+        raise PCGBreakdownError(f"PCG breakdown (status {st})")
+    if st not in (_lib.OK, _lib.NONCONVERGED):
+        _lib.check(st, "phastb_h8_mech_solve_ex")
+    bn, rn = float(rinfo[0]), float(rinfo[1])
+    return out, PCGInfo(int(info[0]), bool(info[1]), bn, rn, rn / bn if bn > 0 else 0.0)
+
+
+@dataclass(frozen=True)
 class BoxKKTResult:
     solution: torch.Tensor
     total_pcg_iterations: int
@@ -142,9 +209,11 @@ class _AttemptFailure(RuntimeError):
 class StaggeredSolver:
     """Staggered alternate minimisation of the hybrid AT2 cell (solid3d/staggered.py)."""
 
-    def __init__(self, op, cfg=None):
+    def __init__(self, op, cfg=None, form=PLAIN):
         self.op = op
         self.cfg = cfg or SolverConfig()
+        self.form = form
+        self._lmax = (C.c_double * 3)()
         self.load = op.load
         self._c = int(op.load.controlled)
         self._n_u = 3 * op.n_red
@@ -175,9 +244,9 @@ class StaggeredSolver:
     def _mechanics(self, d, values, x0):
         cfg = self.cfg
         try:
-            x, info = solve_constrained(self.op, fixed_mask=self._mask, fixed_values=values, d=d, x0=x0,
-                                        rtol=cfg.pcg_rtol_mech, maxiter=cfg.pcg_maxit_mech,
-                                        check_every=cfg.check_every)
+            x, info = solve_constrained_form(self.op, self.form, fixed_mask=self._mask, fixed_values=values, d=d,
+                                             x0=x0, rtol=cfg.pcg_rtol_mech, maxiter=cfg.pcg_maxit_mech,
+                                             check_every=cfg.check_every, lmax_cache=self._lmax)
         except PCGBreakdownError as exc:
             raise _AttemptFailure(f"mechanics PCG breakdown: {exc}") from exc
         if not info.converged:
@@ -214,6 +283,7 @@ class StaggeredSolver:
             raise ValueError(f"target {target!r} equals the current controlled strain")
         increment = state.increment + 1 if increment is None else int(increment)
         t0 = perf_counter()
+        self._lmax[0] = 0.0  # fresh multigrid eigenvalue estimates for every increment
         try:
             return self._attempt(state, target, previous, increment, t0)
         except _AttemptFailure as exc:
