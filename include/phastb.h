@@ -208,6 +208,20 @@ int phastb_h8_mech_apply_noalloc(const phastb_voxel_grid* g, const phastb_voxel_
                                  const uint8_t* slot, int dtype, const void* x, const void* gq,
                                  const void* d, const uint8_t* mask, void* y, void* stream);
 
+/* Tile shape of the elastic action for a grid and word size (no reference counterpart: the
+ * reference action is a batched gather/matmul/scatter).  shape = {ox, oy, kz}: owned nodes per
+ * block in x and y and node layers per block in z; (ox+1)(oy+1) <= 256.  set = 0 reads the
+ * shape in use (the recorded one, else a heuristic), set = 1 records `shape` for this grid. */
+int phastb_h8_tile_shape(const phastb_voxel_grid* g, int dtype, int set, int* shape);
+
+/* Times the elastic action over candidate tile shapes on the caller's buffers (x, d, slot
+ * as for phastb_h8_mech_apply; y is overwritten), records the fastest for this grid and
+ * word size and returns it in shape[3] and its time per action in *ms.  Must not be called
+ * while `stream` is being captured.  scratch: phastb_h8_scratch_bytes. */
+int phastb_h8_autotune(const phastb_voxel_grid* g, const phastb_voxel_material* m, int dtype,
+                       const uint8_t* slot, const void* x, const void* d, void* y, void* scratch,
+                       size_t scratch_bytes, int* shape, float* ms, void* stream);
+
 /* Jacobi diagonal of A(g).  mech_diagonal, operator.py:1196-1254 */
 int phastb_h8_mech_diagonal(const phastb_voxel_grid* g, const phastb_voxel_material* m,
                             const uint8_t* slot, int dtype, const void* gq, const void* d, void* diag,

@@ -21,6 +21,7 @@ DRIVER_NONE, DRIVER_FULL, DRIVER_SPECTRAL = 0, 1, 2
 MAX_SLOTS = 8
 
 vp, ip, dp, sz = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_size_t
+fp = C.POINTER(C.c_float)
 
 
 class Q4Grid(C.Structure):
@@ -81,6 +82,8 @@ SIGNATURES = {
     "phastb_h8_degradation": (C.c_int, [VG, C.c_int, vp, C.c_double, vp, vp]),
     "phastb_h8_mech_apply": (C.c_int, [VG, VM, vp, C.c_int, vp, vp, vp, vp, vp, vp, vp]),
     "phastb_h8_mech_apply_noalloc": (C.c_int, [VG, VM, vp, C.c_int, vp, vp, vp, vp, vp, vp]),
+    "phastb_h8_tile_shape": (C.c_int, [VG, C.c_int, C.c_int, ip]),
+    "phastb_h8_autotune": (C.c_int, [VG, VM, C.c_int, vp, vp, vp, vp, vp, sz, ip, fp, vp]),
     "phastb_h8_mech_diagonal": (C.c_int, [VG, VM, vp, C.c_int, vp, vp, vp, vp, vp]),
     "phastb_h8_stress_energy": (C.c_int, [VG, VM, vp, vp, vp, vp, dp, dp, vp, vp]),
     "phastb_h8_driving_history": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, vp]),

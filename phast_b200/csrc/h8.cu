@@ -2,6 +2,7 @@
 // driving force + history, AT2 damage action / rhs / diagonal.
 // C ABI in include/phastb.h.
 #include "h8_kernels.cuh"
+#include "h8_tile.cuh"
 #include "reduce.cuh"
 
 #include <cmath>
@@ -478,11 +479,8 @@ size_t h8_scratch_bytes(const VoxGeom& v, int dtype) {
 template <typename T>
 int h8_mech_apply_t(const VoxGeom& v, const VoxMat<T>& mm, const uint8_t* slot, const T* x, const T* gq,
                     const T* d, const uint8_t* mask, T* y, void* scratch, const int* guard, cudaStream_t s) {
-  T* sc = static_cast<T*>(scratch);
   RedWs ws = red_ws(static_cast<char*>(scratch) + align_up(24 * sizeof(T) * (size_t)v.n_elem));
-  { note_launch(); h8_mech_elem_kernel<T, false><<<grid_for(v.n_elem), kThreads, 0, s>>>(v, mm, slot, x, gq, d, sc, y, mask, ws, guard); }
-  { note_launch(); h8_gather_kernel<T, 3><<<grid_for(v.n_red), kThreads, 0, s>>>(v, sc, y, mask, guard); }
-  return last_launch_status();
+  return h8_mech_tile_launch<T>(v, mm, slot, x, gq, d, mask, y, ws, guard, false, false, s);
 }
 
 template int h8_mech_apply_t<double>(const VoxGeom&, const VoxMat<double>&, const uint8_t*, const double*,

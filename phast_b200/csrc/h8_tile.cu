@@ -1,0 +1,683 @@
+// Tiled z-marching voxel H8 elastic action (see h8_tile.cuh).
+#include "h8_tile.cuh"
+
+#include <map>
+#include <mutex>
+#include <tuple>
+
+namespace phastb {
+
+namespace {
+
+// Index of a node coordinate along one axis after the periodic wrap; -1 when
+// the coordinate lies outside a non-periodic grid.  |c| stays within one
+// period because tiles are never wider than the grid.
+__device__ __forceinline__ int wrap_node(int c, int n, int r, int periodic) {
+  if (periodic) return c < 0 ? c + n : (c >= n ? c - n : c);
+  return (c >= 0 && c < r) ? c : -1;
+}
+
+__device__ __forceinline__ int wrap_elem(int c, int n, int periodic) {
+  if (periodic) return c < 0 ? c + n : (c >= n ? c - n : c);
+  return (c >= 0 && c < n) ? c : -1;
+}
+
+// Node layer kn of the brick with its one-node halo, (ox+2)(oy+2) nodes, is
+// staged in two steps so the global loads of layer k+2 are in flight while
+// layer k's elements are computed: stage_load reads a thread's (at most two)
+// nodes into registers, stage_store writes them to buf[4][nt] (fields ux, uy,
+// uz, d).  Nodes outside a non-periodic grid read as zero.
+template <typename T>
+struct Staged {
+  T v[2][4];
+};
+
+template <typename T>
+__device__ __forceinline__ void stage_load(const VoxGeom& g, const T* __restrict__ x, const T* __restrict__ d,
+                                           int i0, int j0, int kn, int ntx, int nt, Staged<T>& r) {
+  const int gk = wrap_node(kn, g.nz, g.rz, g.pz);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int t = threadIdx.x + h * blockDim.x;
+    T u0 = T(0), u1 = T(0), u2 = T(0), dd = T(0);
+    if (t < nt && gk >= 0) {
+      const int a = t % ntx, b = t / ntx;
+      const int gi = wrap_node(i0 - 1 + a, g.nx, g.rx, g.px);
+      const int gj = wrap_node(j0 - 1 + b, g.ny, g.ry, g.py);
+      if (gi >= 0 && gj >= 0) {
+        const size_t n = (size_t)gi + (size_t)g.rx * ((size_t)gj + (size_t)g.ry * gk);
+        u0 = __ldg(x + 3 * n);
+        u1 = __ldg(x + 3 * n + 1);
+        u2 = __ldg(x + 3 * n + 2);
+        if (d) dd = __ldg(d + n);
+      }
+    }
+    r.v[h][0] = u0;
+    r.v[h][1] = u1;
+    r.v[h][2] = u2;
+    r.v[h][3] = dd;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void stage_store(int nt, const Staged<T>& r, T* buf) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int t = threadIdx.x + h * blockDim.x;
+    if (t < nt) {
+      buf[t] = r.v[h][0];
+      buf[nt + t] = r.v[h][1];
+      buf[2 * nt + t] = r.v[h][2];
+      buf[3 * nt + t] = r.v[h][3];
+    }
+  }
+}
+
+// Gauss-point constants of the action: N1 weights with the 1/h of each axis
+// folded in (the last interpolation stage of a derivative applies them).
+template <typename T>
+struct TileK {
+  T c1, c2;              // N1 = [[c1, c2], [c2, c1]]
+  T x1, x2, y1, y2, z1, z2;  // c1/h, c2/h per axis
+  T ihx, ihy, ihz;
+};
+
+template <typename T>
+__device__ __forceinline__ void ip2(T a0, T a1, T c1, T c2, T& q0, T& q1) {
+  q0 = c1 * a0 + c2 * a1;
+  q1 = c2 * a0 + c1 * a1;
+}
+
+// Gradient of a trilinear field u[L] at the Gauss points: Dx[qz][qy],
+// Dy[qz][qx], Dz[qy][qx] (each independent of its own axis).
+template <typename T>
+__device__ __forceinline__ void grad_k(const T* u, const TileK<T>& k, T (&Dx)[2][2], T (&Dy)[2][2],
+                                       T (&Dz)[2][2]) {
+  {
+    T Y[2][2];  // [az][qy]
+#pragma unroll
+    for (int az = 0; az < 2; ++az)
+      ip2(u[1 + 4 * az] - u[4 * az], u[3 + 4 * az] - u[2 + 4 * az], k.c1, k.c2, Y[az][0], Y[az][1]);
+#pragma unroll
+    for (int qy = 0; qy < 2; ++qy) ip2(Y[0][qy], Y[1][qy], k.x1, k.x2, Dx[0][qy], Dx[1][qy]);
+  }
+  {
+    T Y[2][2];  // [az][qx]
+#pragma unroll
+    for (int az = 0; az < 2; ++az)
+      ip2(u[2 + 4 * az] - u[4 * az], u[3 + 4 * az] - u[1 + 4 * az], k.c1, k.c2, Y[az][0], Y[az][1]);
+#pragma unroll
+    for (int qx = 0; qx < 2; ++qx) ip2(Y[0][qx], Y[1][qx], k.y1, k.y2, Dy[0][qx], Dy[1][qx]);
+  }
+  {
+    T Y[2][2];  // [ay][qx]
+#pragma unroll
+    for (int ay = 0; ay < 2; ++ay)
+      ip2(u[4 + 2 * ay] - u[2 * ay], u[5 + 2 * ay] - u[1 + 2 * ay], k.c1, k.c2, Y[ay][0], Y[ay][1]);
+#pragma unroll
+    for (int qx = 0; qx < 2; ++qx) ip2(Y[0][qx], Y[1][qx], k.z1, k.z2, Dz[0][qx], Dz[1][qx]);
+  }
+}
+
+// Transposed gradient: out[L] = sum over the Gauss points of dN_L/dx_a times
+// the summed terms Px[qz][qy], Py[qz][qx], Pz[qy][qx].
+template <typename T>
+__device__ __forceinline__ void grad_k_t(const T (&Px)[2][2], const T (&Py)[2][2], const T (&Pz)[2][2],
+                                         const TileK<T>& k, T* out) {
+  T Ax[2][2], Ay[2][2], Az[2][2];
+  {
+    T Y[2][2];  // [az][qy]
+#pragma unroll
+    for (int qy = 0; qy < 2; ++qy) ip2(Px[0][qy], Px[1][qy], k.x1, k.x2, Y[0][qy], Y[1][qy]);
+#pragma unroll
+    for (int az = 0; az < 2; ++az) ip2(Y[az][0], Y[az][1], k.c1, k.c2, Ax[az][0], Ax[az][1]);  // [az][ay]
+  }
+  {
+    T Y[2][2];  // [az][qx]
+#pragma unroll
+    for (int qx = 0; qx < 2; ++qx) ip2(Py[0][qx], Py[1][qx], k.y1, k.y2, Y[0][qx], Y[1][qx]);
+#pragma unroll
+    for (int az = 0; az < 2; ++az) ip2(Y[az][0], Y[az][1], k.c1, k.c2, Ay[az][0], Ay[az][1]);  // [az][ax]
+  }
+  {
+    T Y[2][2];  // [ay][qx]
+#pragma unroll
+    for (int qx = 0; qx < 2; ++qx) ip2(Pz[0][qx], Pz[1][qx], k.z1, k.z2, Y[0][qx], Y[1][qx]);
+#pragma unroll
+    for (int ay = 0; ay < 2; ++ay) ip2(Y[ay][0], Y[ay][1], k.c1, k.c2, Az[ay][0], Az[ay][1]);  // [ay][ax]
+  }
+#pragma unroll
+  for (int L = 0; L < 8; ++L) {
+    const int ax = L & 1, ay = (L >> 1) & 1, az = L >> 2;
+    const T tx = ax ? Ax[az][ay] : -Ax[az][ay];
+    const T ty = ay ? Ay[az][ax] : -Ay[az][ax];
+    const T tz = az ? Az[ay][ax] : -Az[ay][ax];
+    out[L] = tx + ty + tz;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T g_deg(T kappa, T d) {
+  const T o = T(1) - d;
+  return (T(1) - kappa) * o * o + kappa;
+}
+
+}  // namespace
+
+template <typename T, bool ISO, bool ENERGY, bool DOT>
+__global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
+    h8_mech_tile_kernel(VoxGeom g, VoxMat<T> m, const uint8_t* __restrict__ slot, const T* __restrict__ x,
+                        const T* __restrict__ gq, const T* __restrict__ d, T* __restrict__ y,
+                        const uint8_t* __restrict__ mask, RedWs ws, const int* guard, TileShape ts,
+                        TileK<T> K8) {
+  if (guard && *guard == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ox = ts.ox, oy = ts.oy, kz = ts.kz;
+  const int ex = ox + 1, exy = ex * (oy + 1);
+  const int ntx = ox + 2, nt = ntx * (oy + 2);
+  T* nb = reinterpret_cast<T*>(smem_raw);  // [3 buffers][4 fields][nt]
+  T* FL = nb + 12 * nt;                    // [4 corners][3 comps][exy], lower face (oz = 0)
+  T* FU = FL + 12 * exy;                   // upper face (oz = 1)
+  const int tid = threadIdx.x;
+  const T w = T(g.w);
+  const T* Ex = x + 3 * (size_t)g.n_red;
+  const T E6[6] = {__ldg(Ex), __ldg(Ex + 1), __ldg(Ex + 2), __ldg(Ex + 3), __ldg(Ex + 4), __ldg(Ex + 5)};
+  const int tiles_x = (g.rx + ox - 1) / ox, tiles_y = (g.ry + oy - 1) / oy;
+  const int tiles_xy = tiles_x * tiles_y;
+  const int n_tiles = tiles_xy * ((g.rz + kz - 1) / kz);
+  // element / owned-node coordinates of this thread inside the tile
+  const int ea = tid % ex, eb = tid / ex;
+  const int ni = tid % ox, nj = tid / ox;
+  const bool is_elem = tid < exy, is_node = tid < ox * oy;
+  double accd[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  // material slot of this thread's element in layer ke (0 outside the grid)
+  auto elem_slot = [&](int i0, int j0, int ke) -> int {
+    if (!is_elem) return 0;
+    const int gi = wrap_elem(i0 - 1 + ea, g.nx, g.px);
+    const int gj = wrap_elem(j0 - 1 + eb, g.ny, g.py);
+    const int gk = wrap_elem(ke, g.nz, g.pz);
+    if (gi < 0 || gj < 0 || gk < 0) return 0;
+    return __ldg(slot + (size_t)gi + (size_t)g.nx * ((size_t)gj + (size_t)g.ny * gk));
+  };
+  // fixed-dof bits (one per component) of this thread's owned node in layer kn
+  auto node_mask = [&](int i0, int j0, int kn) -> int {
+    if (!mask || !is_node || kn >= g.rz) return 0;
+    const int gi = i0 + ni, gj = j0 + nj;
+    if (gi >= g.rx || gj >= g.ry) return 0;
+    const size_t n = (size_t)gi + (size_t)g.rx * ((size_t)gj + (size_t)g.ry * kn);
+    return (__ldg(mask + 3 * n) ? 1 : 0) | (__ldg(mask + 3 * n + 1) ? 2 : 0) | (__ldg(mask + 3 * n + 2) ? 4 : 0);
+  };
+
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int tz = tile / tiles_xy, txy = tile - tz * tiles_xy;
+    const int i0 = (txy % tiles_x) * ox, j0 = (txy / tiles_x) * oy;
+    const int k0 = tz * kz, k1 = min(k0 + kz, g.rz);
+    T tacc[8] = {T(0), T(0), T(0), T(0), T(0), T(0), T(0), T(0)};
+    T pend[3] = {T(0), T(0), T(0)};
+    Staged<T> pf;
+    stage_load(g, x, d, i0, j0, k0 - 1, ntx, nt, pf);
+    __syncthreads();  // the previous tile's last node phase is done with the buffers
+    stage_store(nt, pf, nb);
+    stage_load(g, x, d, i0, j0, k0, ntx, nt, pf);
+    int sl_next = elem_slot(i0, j0, k0 - 1);
+    int mk_next = node_mask(i0, j0, k0), mk_cur = 0;
+    const int K = k1 - k0;
+    for (int kk = 0; kk <= K; ++kk) {
+      const int ke = k0 - 1 + kk;  // element layer of this step
+      T* b0 = nb + 4 * nt * (kk % 3);
+      T* b1 = nb + 4 * nt * ((kk + 1) % 3);
+      stage_store(nt, pf, b1);  // node layer ke + 1
+      const int sl = sl_next;
+      if (kk < K) {
+        stage_load(g, x, d, i0, j0, ke + 2, ntx, nt, pf);
+        sl_next = elem_slot(i0, j0, ke + 1);
+      }
+      if (kk >= 1) {
+        mk_cur = mk_next;
+        if (kk < K) mk_next = node_mask(i0, j0, ke + 1);
+      }
+      __syncthreads();
+      // ---- element phase: one element of the (ox+1) x (oy+1) tile per thread
+      if (is_elem) {
+        const int gi = wrap_elem(i0 - 1 + ea, g.nx, g.px);
+        const int gj = wrap_elem(j0 - 1 + eb, g.ny, g.py);
+        const int gk = wrap_elem(ke, g.nz, g.pz);
+        T f[3][8];
+        if (gi >= 0 && gj >= 0 && gk >= 0) {
+          const size_t e = (size_t)gi + (size_t)g.nx * ((size_t)gj + (size_t)g.ny * gk);
+          const bool own = ea >= 1 && eb >= 1 && kk >= 1 && i0 - 1 + ea < g.rx && j0 - 1 + eb < g.ry;
+          T gv[8];
+          if (gq) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) gv[q] = __ldg(gq + 8 * e + q);
+          } else if (d) {
+            T dd[8], dq[8];
+#pragma unroll
+            for (int L = 0; L < 8; ++L) {
+              const T* bb = (L & 4) ? b1 : b0;
+              dd[L] = bb[3 * nt + (eb + ((L >> 1) & 1)) * ntx + ea + (L & 1)];
+            }
+            interp_sf(dd, dq);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) gv[q] = g_deg(m.kappa, dq[q]);
+          } else {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) gv[q] = T(1);
+          }
+          T D[3][3][2][2];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            T u[8];
+#pragma unroll
+            for (int L = 0; L < 8; ++L) {
+              const T* bb = (L & 4) ? b1 : b0;
+              u[L] = bb[c * nt + (eb + ((L >> 1) & 1)) * ntx + ea + (L & 1)];
+            }
+            grad_k(u, K8, D[c][0], D[c][1], D[c][2]);
+          }
+          // the macro strain enters each strain component once: fold it into
+          // the gradient term that component starts from
+#pragma unroll
+          for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+              D[0][0][i][j] += E6[0];
+              D[1][1][i][j] += E6[1];
+              D[2][2][i][j] += E6[2];
+              D[1][2][i][j] += E6[3];
+              D[0][2][i][j] += E6[4];
+              D[0][1][i][j] += E6[5];
+            }
+          T P[3][3][2][2];
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+              for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) P[c][a][i][j] = T(0);
+          // sigma_q * w * g_q at the eight Gauss points, summed into the P terms
+          auto qp_loop = [&](auto stress) {
+#pragma unroll
+            for (int qz = 0; qz < 2; ++qz)
+#pragma unroll
+              for (int qy = 0; qy < 2; ++qy)
+#pragma unroll
+                for (int qx = 0; qx < 2; ++qx) {
+                  T ep[6];
+                  ep[0] = D[0][0][qz][qy];
+                  ep[1] = D[1][1][qz][qx];
+                  ep[2] = D[2][2][qy][qx];
+                  ep[3] = D[1][2][qy][qx] + D[2][1][qz][qx];
+                  ep[4] = D[0][2][qy][qx] + D[2][0][qz][qy];
+                  ep[5] = D[0][1][qz][qx] + D[1][0][qz][qy];
+                  T sg[6];
+                  stress(ep, gv[qx + 2 * qy + 4 * qz], sg);
+                  if (ENERGY && own) {
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) tacc[kOutEnergy] += T(0.5) * sg[k] * ep[k];
+                  }
+                  P[0][0][qz][qy] += sg[0];
+                  P[0][1][qz][qx] += sg[5];
+                  P[0][2][qy][qx] += sg[4];
+                  P[1][0][qz][qy] += sg[5];
+                  P[1][1][qz][qx] += sg[1];
+                  P[1][2][qy][qx] += sg[3];
+                  P[2][0][qz][qy] += sg[4];
+                  P[2][1][qz][qx] += sg[3];
+                  P[2][2][qy][qx] += sg[2];
+                }
+          };
+          if constexpr (ISO) {
+            const T lw = m.lam[sl] * w, mw = m.mu[sl] * w;
+            qp_loop([&](const T* ep, T gg, T* sg) {
+              const T lg = lw * gg, mg = mw * gg, mg2 = mg + mg;
+              const T lt = lg * (ep[0] + ep[1] + ep[2]);
+              sg[0] = mg2 * ep[0] + lt;
+              sg[1] = mg2 * ep[1] + lt;
+              sg[2] = mg2 * ep[2] + lt;
+              sg[3] = mg * ep[3];
+              sg[4] = mg * ep[4];
+              sg[5] = mg * ep[5];
+            });
+          } else {
+            qp_loop([&](const T* ep, T gg, T* sg) {
+              voigt_stress(m, sl, ep, sg);
+              const T gw = gg * w;
+#pragma unroll
+              for (int k = 0; k < 6; ++k) sg[k] *= gw;
+            });
+          }
+          if (own) {
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+              for (int j = 0; j < 2; ++j) {
+                tacc[0] += P[0][0][i][j];
+                tacc[1] += P[1][1][i][j];
+                tacc[2] += P[2][2][i][j];
+                tacc[3] += P[1][2][i][j];
+                tacc[4] += P[0][2][i][j];
+                tacc[5] += P[0][1][i][j];
+              }
+          }
+#pragma unroll
+          for (int c = 0; c < 3; ++c) grad_k_t(P[c][0], P[c][1], P[c][2], K8, f[c]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int L = 0; L < 8; ++L) f[c][L] = T(0);
+        }
+#pragma unroll
+        for (int L = 0; L < 4; ++L)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            FL[(L * 3 + c) * exy + tid] = f[c][L];
+            FU[(L * 3 + c) * exy + tid] = f[c][L + 4];
+          }
+      }
+      __syncthreads();
+      // ---- node phase: node layer ke = lower faces of this layer + upper faces of the previous
+      if (is_node) {
+        const int e11 = (ni + 1) + ex * (nj + 1), e01 = ni + ex * (nj + 1);
+        const int e10 = (ni + 1) + ex * nj, e00 = ni + ex * nj;
+        T lo[3], up[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          lo[c] = FL[(0 * 3 + c) * exy + e11] + FL[(1 * 3 + c) * exy + e01] + FL[(2 * 3 + c) * exy + e10] +
+                  FL[(3 * 3 + c) * exy + e00];
+          up[c] = FU[(0 * 3 + c) * exy + e11] + FU[(1 * 3 + c) * exy + e01] + FU[(2 * 3 + c) * exy + e10] +
+                  FU[(3 * 3 + c) * exy + e00];
+        }
+        const int gi = i0 + ni, gj = j0 + nj;
+        if (kk >= 1 && gi < g.rx && gj < g.ry) {
+          const size_t n = (size_t)gi + (size_t)g.rx * ((size_t)gj + (size_t)g.ry * ke);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            T v = pend[c] + lo[c];
+            if (mk_cur & (1 << c)) v = T(0);
+            if (y) y[3 * n + c] = v;
+            if (DOT) tacc[kOutDot] += b0[c * nt + (nj + 1) * ntx + ni + 1] * v;
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) pend[c] = up[c];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) accd[k] += double(tacc[k]);
+  }
+
+  __shared__ double sh[32];
+  constexpr int NK = DOT ? 8 : (ENERGY ? 7 : 6);
+#pragma unroll
+  for (int k = 0; k < NK; ++k) {
+    const double sm = block_sum(accd[k], sh);
+    if (tid == 0) ws.part[k * kMaxPartials + blockIdx.x] = sm;
+  }
+  if (arrive_last(ws.counter)) {
+    double dot_e = 0.0;
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+      const double t = fold_sum(ws.part + k * kMaxPartials, gridDim.x, sh);
+      if (tid == 0) {
+        if (k < 6) {
+          ws.out[k] = t;
+          const size_t idx = 3 * (size_t)g.n_red + k;
+          const T v = (mask && mask[idx]) ? T(0) : T(t);
+          if (y) y[idx] = v;
+          dot_e += double(x[idx]) * double(v);
+        } else if (k == kOutEnergy) {
+          ws.out[k] = t;
+        } else {
+          ws.out[k] = t + dot_e;
+        }
+      }
+    }
+    if (tid == 0) *ws.counter = 0u;
+  }
+}
+
+// ------------------------------------------------------------------ host side
+
+namespace {
+
+std::mutex g_shape_mu;
+std::map<std::tuple<int, int, int, int, int, int, int>, TileShape> g_shapes;
+
+auto shape_key(const VoxGeom& g, int word) {
+  return std::make_tuple(g.rx, g.ry, g.rz, g.px, g.py, g.pz, word);
+}
+
+// Heuristic: among owned-node tiles of <= kTileMaxThreads element threads,
+// prefer shapes whose sides divide the grid (no ragged tiles) and the least
+// recomputed halo; then pick the z depth that still gives two blocks per SM.
+TileShape heuristic_shape(const VoxGeom& g, int word) {
+  static const int cand[][2] = {{16, 12}, {12, 16}, {14, 14}, {24, 8}, {16, 8}, {8, 16}, {20, 8}, {32, 4},
+                                {12, 12}, {10, 10}, {8, 8},   {6, 6},   {4, 4},  {2, 2},  {1, 1}};
+  TileShape best{1, 1, 1};
+  double best_cost = 1e300;
+  for (const auto& c : cand) {
+    TileShape t{std::min(c[0], g.rx), std::min(c[1], g.ry), 1};
+    if (!tile_ok(t)) continue;
+    const int tx = (g.rx + t.ox - 1) / t.ox, ty = (g.ry + t.oy - 1) / t.oy;
+    // element-thread slots launched per node layer / useful nodes per layer
+    const double cost = double(tx) * ty * tile_threads(t) / (double(g.rx) * g.ry);
+    if (cost < best_cost - 1e-9) {
+      best_cost = cost;
+      best = t;
+    }
+  }
+  const long long tiles_xy = (long long)((g.rx + best.ox - 1) / best.ox) * ((g.ry + best.oy - 1) / best.oy);
+  const long long want = 2LL * 148;
+  int kz = 16;
+  while (kz > 2 && tiles_xy * ((g.rz + kz - 1) / kz) < want) kz /= 2;
+  best.kz = std::min(kz, g.rz);
+  (void)word;
+  return best;
+}
+
+template <typename T, bool ISO, bool ENERGY, bool DOT>
+int launch_variant(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, const T* x, const T* gq, const T* d,
+                   const uint8_t* mask, T* y, RedWs ws, const int* guard, const TileShape& ts, cudaStream_t s) {
+  auto kern = h8_mech_tile_kernel<T, ISO, ENERGY, DOT>;
+  const size_t smem = tile_smem_bytes<T>(ts);
+  const int threads = tile_threads(ts);
+  static std::mutex mu;
+  static size_t smem_set = 0;
+  static std::map<std::pair<int, size_t>, int> occ;  // (threads, smem) -> resident blocks per SM
+  int per_sm = 1;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (smem > smem_set) {
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return PHASTB_ERR_CUDA;
+      }
+      smem_set = smem;
+    }
+    auto it = occ.find({threads, smem});
+    if (it == occ.end()) {
+      int b = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        b = 1;
+      }
+      it = occ.emplace(std::make_pair(threads, smem), b < 1 ? 1 : b).first;
+    }
+    per_sm = it->second;
+  }
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long n_tiles = (long long)((v.rx + ts.ox - 1) / ts.ox) * ((v.ry + ts.oy - 1) / ts.oy) *
+                            ((v.rz + ts.kz - 1) / ts.kz);
+  long long grid = std::min<long long>(n_tiles, (long long)per_sm * sms);
+  grid = std::min<long long>(grid, kMaxPartials);
+  TileK<T> k8;
+  k8.c1 = T(kC1);
+  k8.c2 = T(kC2);
+  k8.ihx = T(1.0 / v.hx);
+  k8.ihy = T(1.0 / v.hy);
+  k8.ihz = T(1.0 / v.hz);
+  k8.x1 = T(kC1 / v.hx);
+  k8.x2 = T(kC2 / v.hx);
+  k8.y1 = T(kC1 / v.hy);
+  k8.y2 = T(kC2 / v.hy);
+  k8.z1 = T(kC1 / v.hz);
+  k8.z2 = T(kC2 / v.hz);
+  { note_launch(); kern<<<(int)grid, threads, smem, s>>>(v, m, slot, x, gq, d, y, mask, ws, guard, ts, k8); }
+  return last_launch_status();
+}
+
+}  // namespace
+
+TileShape tile_shape_for(const VoxGeom& g, int word) {
+  {
+    std::lock_guard<std::mutex> lk(g_shape_mu);
+    auto it = g_shapes.find(shape_key(g, word));
+    if (it != g_shapes.end()) return it->second;
+  }
+  return heuristic_shape(g, word);
+}
+
+void tile_shape_record(const VoxGeom& g, int word, const TileShape& t) {
+  std::lock_guard<std::mutex> lk(g_shape_mu);
+  g_shapes[shape_key(g, word)] = t;
+}
+
+template <typename T>
+int h8_mech_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, const T* x, const T* gq,
+                        const T* d, const uint8_t* mask, T* y, RedWs ws, const int* guard, bool dot, bool energy,
+                        cudaStream_t s, const TileShape* force_shape) {
+  TileShape ts = force_shape ? *force_shape : tile_shape_for(v, (int)sizeof(T));
+  ts.ox = std::min(ts.ox, v.rx);
+  ts.oy = std::min(ts.oy, v.ry);
+  ts.kz = std::min(ts.kz, v.rz);
+  if (!tile_ok(ts)) return PHASTB_ERR_ARG;
+  if (m.iso) {
+    if (dot) return launch_variant<T, true, false, true>(v, m, slot, x, gq, d, mask, y, ws, guard, ts, s);
+    if (energy) return launch_variant<T, true, true, false>(v, m, slot, x, gq, d, mask, y, ws, guard, ts, s);
+    return launch_variant<T, true, false, false>(v, m, slot, x, gq, d, mask, y, ws, guard, ts, s);
+  }
+  if (dot) return launch_variant<T, false, false, true>(v, m, slot, x, gq, d, mask, y, ws, guard, ts, s);
+  if (energy) return launch_variant<T, false, true, false>(v, m, slot, x, gq, d, mask, y, ws, guard, ts, s);
+  return launch_variant<T, false, false, false>(v, m, slot, x, gq, d, mask, y, ws, guard, ts, s);
+}
+
+template int h8_mech_tile_launch<double>(const VoxGeom&, const VoxMat<double>&, const uint8_t*, const double*,
+                                         const double*, const double*, const uint8_t*, double*, RedWs, const int*,
+                                         bool, bool, cudaStream_t, const TileShape*);
+template int h8_mech_tile_launch<float>(const VoxGeom&, const VoxMat<float>&, const uint8_t*, const float*,
+                                        const float*, const float*, const uint8_t*, float*, RedWs, const int*, bool,
+                                        bool, cudaStream_t, const TileShape*);
+
+}  // namespace phastb
+
+// ------------------------------------------------------------------ autotuner
+
+namespace phastb {
+bool valid_vox(const phastb_voxel_grid* g);
+bool valid_mat(const phastb_voxel_material* m);
+
+namespace {
+
+template <typename T>
+int tune_t(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, const T* x, const T* d, T* y, RedWs ws,
+           cudaStream_t s, TileShape* best_out, float* best_ms) {
+  static const int cand[][2] = {{16, 12}, {12, 16}, {14, 14}, {24, 8}, {16, 8}, {8, 16}, {20, 8},
+                                {32, 4},  {12, 12}, {10, 10}, {8, 8},  {6, 6},  {4, 4}};
+  static const int kzs[] = {2, 4, 8, 16};
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return PHASTB_ERR_CUDA;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return PHASTB_ERR_CUDA;
+  }
+  int st = PHASTB_OK;
+  float best = 1e30f;
+  TileShape bs = heuristic_shape(v, (int)sizeof(T));
+  for (const auto& c : cand) {
+    for (int kz : kzs) {
+      TileShape t{std::min(c[0], v.rx), std::min(c[1], v.ry), std::min(kz, v.rz)};
+      if (!tile_ok(t)) continue;
+      for (int r = 0; r < 2 && !st; ++r)
+        st = h8_mech_tile_launch<T>(v, m, slot, x, nullptr, d, nullptr, y, ws, nullptr, false, false, s, &t);
+      if (st) break;
+      const int reps = 5;
+      cudaEventRecord(e0, s);
+      for (int r = 0; r < reps && !st; ++r)
+        st = h8_mech_tile_launch<T>(v, m, slot, x, nullptr, d, nullptr, y, ws, nullptr, false, false, s, &t);
+      cudaEventRecord(e1, s);
+      if (st || (st = cuda_status(cudaEventSynchronize(e1)))) break;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms /= reps;
+      if (ms < best) {
+        best = ms;
+        bs = t;
+      }
+    }
+    if (st) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) return st;
+  tile_shape_record(v, (int)sizeof(T), bs);
+  *best_out = bs;
+  *best_ms = best;
+  return PHASTB_OK;
+}
+
+}  // namespace
+}  // namespace phastb
+
+using namespace phastb;
+
+extern "C" {
+
+int phastb_h8_tile_shape(const phastb_voxel_grid* g, int dtype, int set, int* shape) {
+  if (!valid_vox(g) || !shape || (dtype != PHASTB_F32 && dtype != PHASTB_F64)) return PHASTB_ERR_ARG;
+  const VoxGeom v = make_vox_geom(*g);
+  const int word = dtype == PHASTB_F32 ? 4 : 8;
+  if (set) {
+    TileShape t{shape[0], shape[1], shape[2]};
+    if (!tile_ok(t)) return PHASTB_ERR_ARG;
+    tile_shape_record(v, word, t);
+    return PHASTB_OK;
+  }
+  const TileShape t = tile_shape_for(v, word);
+  shape[0] = std::min(t.ox, v.rx);
+  shape[1] = std::min(t.oy, v.ry);
+  shape[2] = std::min(t.kz, v.rz);
+  return PHASTB_OK;
+}
+
+int phastb_h8_autotune(const phastb_voxel_grid* g, const phastb_voxel_material* m, int dtype, const uint8_t* slot,
+                       const void* x, const void* d, void* y, void* scratch, size_t scratch_bytes, int* shape,
+                       float* ms, void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !x || !y || !shape || !ms) return PHASTB_ERR_ARG;
+  if (dtype != PHASTB_F32 && dtype != PHASTB_F64) return PHASTB_ERR_ARG;
+  if (!scratch || scratch_bytes < red_ws_bytes()) return PHASTB_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return PHASTB_ERR_ARG;
+  const VoxGeom v = make_vox_geom(*g);
+  RedWs ws = red_ws(scratch);
+  int st;
+  if ((st = red_ws_reset(ws, s))) return st;
+  TileShape t{};
+  if (dtype == PHASTB_F64)
+    st = tune_t<double>(v, make_vox_mat<double>(*m), slot, (const double*)x, (const double*)d, (double*)y, ws, s,
+                        &t, ms);
+  else
+    st = tune_t<float>(v, make_vox_mat<float>(*m), slot, (const float*)x, (const float*)d, (float*)y, ws, s, &t, ms);
+  if (st) return st;
+  shape[0] = t.ox;
+  shape[1] = t.oy;
+  shape[2] = t.kz;
+  return PHASTB_OK;
+}
+
+}  // extern "C"

@@ -191,6 +191,29 @@ class PeriodicVoxelPhaseFieldOperator:
              ptr(mk), ptr(y), self.scratch(x.dtype), stream())
         return y
 
+    def tile_shape(self, dtype=torch.float64, shape=None):
+        """Tile shape (ox, oy, kz) of the elastic-action kernel; ``shape`` records a new one."""
+        arr = (C.c_int * 3)(*(shape if shape is not None else (0, 0, 0)))
+        code = _lib.F32 if dtype == torch.float32 else _lib.F64
+        call("phastb_h8_tile_shape", self.vgrid, code, int(shape is not None), arr)
+        return tuple(arr)
+
+    def autotune(self, dtype=torch.float64, seed=0):
+        """Time the elastic action over the candidate tile shapes and keep the fastest for this grid.
+
+        Returns ``(shape, ms_per_action)``.
+        """
+        gen = torch.Generator(device="cpu").manual_seed(seed)
+        x = torch.rand(self.n_mech, generator=gen, dtype=torch.float64).to(self.device, dtype) * 1e-3
+        d = torch.rand(self.n_red, generator=gen, dtype=torch.float64).to(self.device, dtype) * 0.5
+        y = torch.empty_like(x)
+        shape = (C.c_int * 3)()
+        ms = C.c_float(0.0)
+        wn = _lib.load().phastb_h8_scratch_bytes(self.vgrid, self._dt(x))
+        call("phastb_h8_autotune", self.vgrid, self.mat, self._dt(x), ptr(self.slot), ptr(x), ptr(d), ptr(y),
+             self.scratch(dtype), wn, shape, C.byref(ms), stream())
+        return tuple(shape), float(ms.value)
+
     def mech_diagonal(self, g=None, *, d=None):
         """Jacobi diagonal of A(g) (operator.py:1196-1254)."""
         dtype = g.dtype if g is not None else (d.dtype if d is not None else torch.float64)
