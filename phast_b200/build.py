@@ -9,6 +9,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -39,15 +40,19 @@ def build(force=False, verbose=False):
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
     nvcc = nvcc_path()
-    objs = []
-    for src in SOURCES:
-        obj = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
+    objs = [os.path.join(OUT_DIR, src.replace(".cu", ".o")) for src in SOURCES]
+
+    def compile_one(src, obj):
         cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
                "-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+
+    # translation units compile independently; the largest dominates the wall time
+    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(compile_one, src, obj) for src, obj in zip(SOURCES, objs)]:
+            f.result()
     tmp = LIB + ".tmp"
     subprocess.run([nvcc, *ARCH, "-shared", "--cudart", "static", "-o", tmp, *objs], check=True)
     os.replace(tmp, LIB)

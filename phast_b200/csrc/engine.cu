@@ -597,6 +597,93 @@ __global__ void __launch_bounds__(kThreads) pcg_update_kernel(int n, PcgWs<T> w,
   }
 }
 
+// pcg_alpha_kernel + pcg_update_kernel in one launch, with p . Ap produced by the
+// operator (*pap).  Every block derives alpha from the same device scalars; the
+// last block does the state bookkeeping of both kernels.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) pcg_update_dot_kernel(int n, PcgWs<T> w, T* __restrict__ x,
+                                                                  const T* __restrict__ inv_diag, int custom_pre,
+                                                                  int mode, int check_every,
+                                                                  const double* __restrict__ pap) {
+  if (!w.st->active) return;
+  __shared__ double sh[32];
+  const double PAP = *pap;
+  bool ok;
+  double alpha;
+  if (mode == PCG_PERIODIC) {
+    ok = isfinite(PAP) && PAP > 1e-30;
+    alpha = w.st->rr / (PAP + 1e-30);
+  } else {
+    ok = isfinite(PAP) && PAP > 0.0;
+    alpha = w.st->rz / PAP;
+  }
+  const T a = T(alpha);
+  double rz = 0, rr = 0;
+  if (ok) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+      x[i] = x[i] + a * w.p[i];
+      const T r = w.r[i] - a * w.Ap[i];
+      w.r[i] = r;
+      rr += double(r) * double(r);
+      if (!custom_pre) {
+        const T z = inv_diag ? r * inv_diag[i] : r;
+        w.z[i] = z;
+        rz += double(r) * double(z);
+      }
+    }
+  }
+  double s = block_sum(rz, sh);
+  if (threadIdx.x == 0) w.part[blockIdx.x] = s;
+  s = block_sum(rr, sh);
+  if (threadIdx.x == 0) w.part[kMaxPartials + blockIdx.x] = s;
+  if (arrive_last(w.counter)) {
+    const double RZ = fold_sum(w.part, gridDim.x, sh);
+    const double RR = fold_sum(w.part + kMaxPartials, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+      PcgState& st = *w.st;
+      st.iter += 1;
+      if (!ok) {
+        if (mode == PCG_PERIODIC) {
+          st.breakdown = 1;
+        } else {
+          if (!isfinite(PAP)) st.nonfinite = 1;
+          if (!(PAP > 0.0)) st.breakdown = 1;
+        }
+        st.active = 0;
+      } else {
+        st.alpha = alpha;
+        if (mode != PCG_PERIODIC) st.steps += 1;
+        if (!isfinite(RR) || (!custom_pre && !isfinite(RZ))) st.nonfinite = 1;
+        if (mode == PCG_PERIODIC) {
+          st.beta = RR / (st.rr + 1e-30);
+          st.rr = RR;
+          st.rz = RR;
+          if (st.iter % check_every == 0) {
+            if (RR < st.thr_sq) {
+              st.converged = 1;
+              st.active = 0;
+            } else if (RR > 1e12 * st.rr0) {
+              st.active = 0;
+            }
+          }
+        } else {
+          st.rr = RR;
+          if (!(RR > st.thr_sq)) {
+            st.converged = 1;
+            st.active = 0;
+          } else if (!custom_pre) {
+            if (mode == PCG_STRICT && !(RZ > 0.0)) st.breakdown = 1;
+            st.beta = (mode == PCG_STRICT) ? RZ / st.rz : ((st.rz > 0.0) ? RZ / st.rz : 0.0);
+            st.rz = RZ;
+          }
+        }
+        if (st.breakdown || st.nonfinite) st.active = 0;
+      }
+      *w.counter = 0u;
+    }
+  }
+}
+
 template <typename T>
 __global__ void pcg_dir_kernel(int n, PcgWs<T> w) {
   if (!w.st->active) return;
@@ -652,9 +739,14 @@ int pcg_run(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T* in
   auto iterate = [&](int k_iters) -> int {
     int e;
     for (int k = 0; k < k_iters; ++k) {
-      if ((e = A(w.p, w.Ap, active, s))) return e;
-      { note_launch(); pcg_alpha_kernel<T><<<G, kThreads, 0, s>>>(n, w, mode); }
-      { note_launch(); pcg_update_kernel<T><<<G, kThreads, 0, s>>>(n, w, x, inv_diag, custom, mode, check_every); }
+      if (A.apply_dot) {
+        if ((e = A.apply_dot(A.ctx, w.p, w.Ap, active, s))) return e;
+        { note_launch(); pcg_update_dot_kernel<T><<<G, kThreads, 0, s>>>(n, w, x, inv_diag, custom, mode, check_every, A.dot_out); }
+      } else {
+        if ((e = A(w.p, w.Ap, active, s))) return e;
+        { note_launch(); pcg_alpha_kernel<T><<<G, kThreads, 0, s>>>(n, w, mode); }
+        { note_launch(); pcg_update_kernel<T><<<G, kThreads, 0, s>>>(n, w, x, inv_diag, custom, mode, check_every); }
+      }
       if (custom) {
         if ((e = M->apply(M->ctx, w.r, w.z, active, s))) return e;
         { note_launch(); pcg_rz_kernel<T><<<G, kThreads, 0, s>>>(n, w, 0, mode); }
@@ -665,6 +757,8 @@ int pcg_run(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T* in
   };
   GraphKey key;
   key_val(key, A.apply);
+  key_val(key, A.apply_dot);
+  key_val(key, A.dot_out);
   key_add(key, A.ctx, A.ctx_bytes);
   key_val(key, custom);
   if (custom) {

@@ -28,6 +28,10 @@ struct LinOp {
   int (*apply)(const void* ctx, const T* x, T* y, const int* guard, cudaStream_t s);
   const void* ctx;
   size_t ctx_bytes;  // size of *ctx: the bytes that identify a captured iteration graph
+  // Optional: the same action that also leaves x . y (FP64, device) at *dot_out,
+  // which lets CG skip its separate p . Ap reduction.
+  int (*apply_dot)(const void* ctx, const T* x, T* y, const int* guard, cudaStream_t s) = nullptr;
+  const double* dot_out = nullptr;
   int operator()(const T* x, T* y, const int* guard, cudaStream_t s) const { return apply(ctx, x, y, guard, s); }
 };
 

@@ -23,12 +23,19 @@
 //   Jacobi step (diagonal of the E block).
 #include "engine.cuh"
 #include "h8_kernels.cuh"
+#include "h8_tile.cuh"
+
+#include <utility>
 
 #include <cmath>
 #include <vector>
 
 namespace phastb {
 
+template <typename T>
+int h8_mech_apply_dot_t(const VoxGeom& v, const VoxMat<T>& mm, const uint8_t* slot, const T* x, const T* gq,
+                        const T* d, const uint8_t* mask, T* y, void* scratch, const int* guard, cudaStream_t s);
+const double* h8_apply_dot_slot(const VoxGeom& v, int word, void* scratch);
 template <typename T>
 int h8_mech_apply_t(const VoxGeom& v, const VoxMat<T>& mm, const uint8_t* slot, const T* x, const T* gq,
                     const T* d, const uint8_t* mask, T* y, void* scratch, const int* guard, cudaStream_t s);
@@ -364,6 +371,19 @@ __global__ void gmg_cheb_first(int n, const T* __restrict__ res, const T* __rest
   }
 }
 
+// First step from x = 0 reading b directly: res = b; d = invd * b / theta; x = d.
+template <typename T>
+__global__ void gmg_cheb_first_b(int n, const T* __restrict__ b, const T* __restrict__ invd, T inv_theta,
+                                 T* __restrict__ res, T* __restrict__ d, T* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const T bi = b[i];
+    res[i] = bi;
+    const T di = invd[i] * bi * inv_theta;
+    d[i] = di;
+    x[i] = di;
+  }
+}
+
 template <typename T>
 __global__ void gmg_cheb_step(int n, T* __restrict__ res, const T* __restrict__ Ad, const T* __restrict__ invd, T c1,
                               T c2, T* __restrict__ d, T* __restrict__ x) {
@@ -483,17 +503,43 @@ struct Gmg {
 };
 
 template <typename T>
-static int coarse_apply(const GmgLevel<T>& L, const T* x, T* y, void* scratch, cudaStream_t s) {
-  { note_launch(); gmg_coarse_elem<T, 0><<<grid_for(L.g.n_elem), kThreads, 0, s>>>(L.g, L.lam, L.mu, x, static_cast<T*>(scratch), nullptr); }
-  { note_launch(); gmg_gather3<T><<<grid_for(L.g.n_red), kThreads, 0, s>>>(L.g, static_cast<T*>(scratch), y, nullptr); }
-  return last_launch_status();
+static int coarse_apply(const Gmg<T>& M, const GmgLevel<T>& L, const T* x, T* y, cudaStream_t s) {
+  TileArgs<T> a = tile_args<T>(L.g, 1);
+  a.lam_q = L.lam;
+  a.mu_q = L.mu;
+  a.x = x;
+  a.y = y;
+  return h8_tile_launch<T>(a, M.mat, kCoefQP, kModeApply, s);
+}
+
+// One fused Chebyshev step on level l: res -= A din; dout = c1 din + c2 invd res; x += dout.
+template <typename T>
+static int level_cheb(const Gmg<T>& M, int l, const T* din, T* dout, double c1, double c2, cudaStream_t s) {
+  const GmgLevel<T>& L = M.lv[l];
+  TileArgs<T> a = tile_args<T>(L.g, l == 0 ? 0 : 1);
+  a.x = din;
+  a.res = L.res;
+  a.invd = L.invd;
+  a.xs = L.x;
+  a.d_out = dout;
+  a.c1 = c1;
+  a.c2 = c2;
+  if (l == 0) {
+    a.slot = M.slot;
+    a.d = M.dfield;
+    a.mask = M.mask;
+    return h8_tile_launch<T>(a, M.mat, M.mat.iso ? kCoefIso : kCoefAniso, kModeCheb, s);
+  }
+  a.lam_q = L.lam;
+  a.mu_q = L.mu;
+  return h8_tile_launch<T>(a, M.mat, kCoefQP, kModeCheb, s);
 }
 
 template <typename T>
 static int level_apply(const Gmg<T>& M, int l, const T* x, T* y, cudaStream_t s) {
   if (l == 0)
     return h8_mech_apply_t<T>(M.lv[0].g, M.mat, M.slot, x, nullptr, M.dfield, M.mask, y, M.scratch, nullptr, s);
-  return coarse_apply<T>(M.lv[l], x, y, M.scratch, s);
+  return coarse_apply<T>(M, M.lv[l], x, y, s);
 }
 
 template <typename T>
@@ -516,23 +562,24 @@ static int chebyshev(const Gmg<T>& M, int l, int deg, bool from_zero, bool need_
   const double bmax = M.safety * L.lmax, amin = L.lmax / 30.0;
   const double theta = 0.5 * (bmax + amin), delta = 0.5 * (bmax - amin), sigma = theta / delta;
   if (from_zero) {
-    if ((st = cuda_status(cudaMemcpyAsync(L.res, L.b, sizeof(T) * n, cudaMemcpyDeviceToDevice, s)))) return st;
+    { note_launch(); gmg_cheb_first_b<T><<<G, kThreads, 0, s>>>(n, L.b, L.invd, T(1.0 / theta), L.res, L.dvec, L.x); }
   } else {
     if ((st = level_apply(M, l, L.x, L.Ad, s))) return st;
     { note_launch(); gmg_residual<T><<<G, kThreads, 0, s>>>(n, L.b, L.Ad, L.res); }
+    { note_launch(); gmg_cheb_first<T><<<G, kThreads, 0, s>>>(n, L.res, L.invd, T(1.0 / theta), L.dvec, L.x, 1); }
   }
-  { note_launch(); gmg_cheb_first<T><<<G, kThreads, 0, s>>>(n, L.res, L.invd, T(1.0 / theta), L.dvec, L.x, from_zero ? 0 : 1); }
+  // later steps ping-pong the direction between dvec and Ad
+  T* cur = L.dvec;
+  T* oth = L.Ad;
   double rho_old = 1.0 / sigma;
   for (int k = 1; k < deg; ++k) {
-    if ((st = level_apply(M, l, L.dvec, L.Ad, s))) return st;
     const double rho = 1.0 / (2.0 * sigma - rho_old);
-    { note_launch(); gmg_cheb_step<T><<<G, kThreads, 0, s>>>(n, L.res, L.Ad, L.invd, T(rho * rho_old), T(2.0 * rho / delta), L.dvec, L.x); }
+    if ((st = level_cheb(M, l, cur, oth, rho * rho_old, 2.0 * rho / delta, s))) return st;
+    std::swap(cur, oth);
     rho_old = rho;
   }
-  if (need_res) {
-    if ((st = level_apply(M, l, L.dvec, L.Ad, s))) return st;
-    { note_launch(); gmg_sub_inplace<T><<<G, kThreads, 0, s>>>(n, L.res, L.Ad); }
-  }
+  // res -= A d (a step with zero coefficients leaves x unchanged)
+  if (need_res && (st = level_cheb(M, l, cur, oth, 0.0, 0.0, s))) return st;
   return last_launch_status();
 }
 
@@ -743,6 +790,12 @@ static int mech_op_t(const void* c, const T* x, T* y, const int* guard, cudaStre
   return h8_mech_apply_t<T>(k->v, k->m, k->slot, x, nullptr, k->d, k->mask, y, k->scratch, guard, s);
 }
 
+template <typename T>
+static int mech_op_dot_t(const void* c, const T* x, T* y, const int* guard, cudaStream_t s) {
+  const MechOpT<T>* k = static_cast<const MechOpT<T>*>(c);
+  return h8_mech_apply_dot_t<T>(k->v, k->m, k->slot, x, nullptr, k->d, k->mask, y, k->scratch, guard, s);
+}
+
 __global__ void ex_setup_kernel(int n, const uint8_t* __restrict__ fixed, const double* __restrict__ vals,
                                 const double* __restrict__ x0, double* __restrict__ xc, double* __restrict__ x0f) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -898,7 +951,8 @@ int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_mater
     return last_launch_status();
   }
   const double thr = std::max(rtol * bn, atol);
-  LinOp<double> A64{mech_op_t<double>, &freeop, sizeof(freeop)};
+  LinOp<double> A64{mech_op_t<double>, &freeop, sizeof(freeop), mech_op_dot_t<double>,
+                    h8_apply_dot_slot(v, 8, L.scratch64)};
   if (!o->mixed) {
     // FP64 PCG with the FP64 V-cycle (precond = 1) or Jacobi (0)
     PcgResult pr{};
@@ -939,7 +993,8 @@ int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_mater
     { note_launch(); ex_invert_f<<<G, kThreads, 0, s>>>(n, L.inv32, fixed, L.inv32); }
   }
   MechOpT<float> free32{v, m32, slot, L.d32, fixed, scratch32};
-  LinOp<float> A32{mech_op_t<float>, &free32, sizeof(free32)};
+  LinOp<float> A32{mech_op_t<float>, &free32, sizeof(free32), mech_op_dot_t<float>,
+                   h8_apply_dot_slot(v, 4, scratch32)};
   Precond<float> M32{gmg_precond_apply<float>, &L.g32, sizeof(L.g32)};
   int total = 0, converged = 0;
   double rn = bn;

@@ -483,6 +483,24 @@ int h8_mech_apply_t(const VoxGeom& v, const VoxMat<T>& mm, const uint8_t* slot, 
   return h8_mech_tile_launch<T>(v, mm, slot, x, gq, d, mask, y, ws, guard, false, false, s);
 }
 
+template <typename T>
+int h8_mech_apply_dot_t(const VoxGeom& v, const VoxMat<T>& mm, const uint8_t* slot, const T* x, const T* gq,
+                        const T* d, const uint8_t* mask, T* y, void* scratch, const int* guard, cudaStream_t s) {
+  RedWs ws = red_ws(static_cast<char*>(scratch) + align_up(24 * sizeof(T) * (size_t)v.n_elem));
+  return h8_mech_tile_launch<T>(v, mm, slot, x, gq, d, mask, y, ws, guard, true, false, s);
+}
+
+const double* h8_apply_dot_slot(const VoxGeom& v, int word, void* scratch) {
+  return red_ws(static_cast<char*>(scratch) + align_up(24 * (size_t)word * (size_t)v.n_elem)).out + kOutDot;
+}
+
+template int h8_mech_apply_dot_t<double>(const VoxGeom&, const VoxMat<double>&, const uint8_t*, const double*,
+                                         const double*, const double*, const uint8_t*, double*, void*, const int*,
+                                         cudaStream_t);
+template int h8_mech_apply_dot_t<float>(const VoxGeom&, const VoxMat<float>&, const uint8_t*, const float*,
+                                        const float*, const float*, const uint8_t*, float*, void*, const int*,
+                                        cudaStream_t);
+
 template int h8_mech_apply_t<double>(const VoxGeom&, const VoxMat<double>&, const uint8_t*, const double*,
                                      const double*, const double*, const uint8_t*, double*, void*, const int*,
                                      cudaStream_t);

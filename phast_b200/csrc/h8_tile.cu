@@ -1,9 +1,12 @@
 // Tiled z-marching voxel H8 elastic action (see h8_tile.cuh).
 #include "h8_tile.cuh"
 
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <vector>
 
 namespace phastb {
 
@@ -73,14 +76,6 @@ __device__ __forceinline__ void stage_store(int nt, const Staged<T>& r, T* buf) 
   }
 }
 
-// Gauss-point constants of the action: N1 weights with the 1/h of each axis
-// folded in (the last interpolation stage of a derivative applies them).
-template <typename T>
-struct TileK {
-  T c1, c2;              // N1 = [[c1, c2], [c2, c1]]
-  T x1, x2, y1, y2, z1, z2;  // c1/h, c2/h per axis
-  T ihx, ihy, ihz;
-};
 
 template <typename T>
 __device__ __forceinline__ void ip2(T a0, T a1, T c1, T c2, T& q0, T& q1) {
@@ -164,15 +159,26 @@ __device__ __forceinline__ T g_deg(T kappa, T d) {
 
 }  // namespace
 
-template <typename T, bool ISO, bool ENERGY, bool DOT>
+// One launch = every brick of the grid (persistent blocks).  COEF selects the
+// element coefficients (material slot + g(d), isotropic or general Voigt, or
+// per-Gauss-point moduli of a multigrid coarse level); MODE selects the node
+// epilogue: y = A x, y plus x . y, y plus the energy, or one Chebyshev
+// smoothing step on (res, d, x) driven by A d.
+template <typename T, int COEF, int MODE, int OX, int OY>
 __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
-    h8_mech_tile_kernel(VoxGeom g, VoxMat<T> m, const uint8_t* __restrict__ slot, const T* __restrict__ x,
-                        const T* __restrict__ gq, const T* __restrict__ d, T* __restrict__ y,
-                        const uint8_t* __restrict__ mask, RedWs ws, const int* guard, TileShape ts,
-                        TileK<T> K8) {
-  if (guard && *guard == 0) return;
+    h8_tile_kernel(TileArgs<T> a, VoxMat<T> m) {
+  if (a.guard && *a.guard == 0) return;
+  constexpr bool SLOT = COEF != kCoefQP;
+  constexpr bool DOT = MODE == kModeDot, ENERGY = MODE == kModeEnergy, CHEB = MODE == kModeCheb;
+  // E rows (macro strain) exist on the fine operator; a Chebyshev step leaves them alone (masked)
+  constexpr bool EROWS = SLOT && !CHEB;
+  constexpr bool RED = EROWS || DOT || ENERGY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int ox = ts.ox, oy = ts.oy, kz = ts.kz;
+  const VoxGeom& g = a.g;
+  const T* __restrict__ x = a.x;
+  const T* __restrict__ d = SLOT ? a.d : nullptr;
+  // OX, OY > 0: a compiled tile shape (constant shared-memory offsets)
+  const int ox = OX ? OX : a.ts.ox, oy = OY ? OY : a.ts.oy, kz = a.ts.kz;
   const int ex = ox + 1, exy = ex * (oy + 1);
   const int ntx = ox + 2, nt = ntx * (oy + 2);
   T* nb = reinterpret_cast<T*>(smem_raw);  // [3 buffers][4 fields][nt]
@@ -180,8 +186,13 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
   T* FU = FL + 12 * exy;                   // upper face (oz = 1)
   const int tid = threadIdx.x;
   const T w = T(g.w);
-  const T* Ex = x + 3 * (size_t)g.n_red;
-  const T E6[6] = {__ldg(Ex), __ldg(Ex + 1), __ldg(Ex + 2), __ldg(Ex + 3), __ldg(Ex + 4), __ldg(Ex + 5)};
+  const T c1 = T(a.c1), c2 = T(a.c2);
+  T E6[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+  if (EROWS) {  // a Chebyshev step smooths the nodal block only (E rows masked)
+    const T* Ex = x + 3 * (size_t)g.n_red;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) E6[k] = __ldg(Ex + k);
+  }
   const int tiles_x = (g.rx + ox - 1) / ox, tiles_y = (g.ry + oy - 1) / oy;
   const int tiles_xy = tiles_x * tiles_y;
   const int n_tiles = tiles_xy * ((g.rz + kz - 1) / kz);
@@ -192,20 +203,21 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
   double accd[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   // material slot of this thread's element in layer ke (0 outside the grid)
   auto elem_slot = [&](int i0, int j0, int ke) -> int {
-    if (!is_elem) return 0;
+    if (!SLOT || !is_elem) return 0;
     const int gi = wrap_elem(i0 - 1 + ea, g.nx, g.px);
     const int gj = wrap_elem(j0 - 1 + eb, g.ny, g.py);
     const int gk = wrap_elem(ke, g.nz, g.pz);
     if (gi < 0 || gj < 0 || gk < 0) return 0;
-    return __ldg(slot + (size_t)gi + (size_t)g.nx * ((size_t)gj + (size_t)g.ny * gk));
+    return __ldg(a.slot + (size_t)gi + (size_t)g.nx * ((size_t)gj + (size_t)g.ny * gk));
   };
   // fixed-dof bits (one per component) of this thread's owned node in layer kn
   auto node_mask = [&](int i0, int j0, int kn) -> int {
-    if (!mask || !is_node || kn >= g.rz) return 0;
+    if (!a.mask || !is_node || kn >= g.rz) return 0;
     const int gi = i0 + ni, gj = j0 + nj;
     if (gi >= g.rx || gj >= g.ry) return 0;
     const size_t n = (size_t)gi + (size_t)g.rx * ((size_t)gj + (size_t)g.ry * kn);
-    return (__ldg(mask + 3 * n) ? 1 : 0) | (__ldg(mask + 3 * n + 1) ? 2 : 0) | (__ldg(mask + 3 * n + 2) ? 4 : 0);
+    return (__ldg(a.mask + 3 * n) ? 1 : 0) | (__ldg(a.mask + 3 * n + 1) ? 2 : 0) |
+           (__ldg(a.mask + 3 * n + 2) ? 4 : 0);
   };
 
   for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
@@ -247,22 +259,24 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
           const size_t e = (size_t)gi + (size_t)g.nx * ((size_t)gj + (size_t)g.ny * gk);
           const bool own = ea >= 1 && eb >= 1 && kk >= 1 && i0 - 1 + ea < g.rx && j0 - 1 + eb < g.ry;
           T gv[8];
-          if (gq) {
+          if (SLOT) {
+            if (a.gq) {
 #pragma unroll
-            for (int q = 0; q < 8; ++q) gv[q] = __ldg(gq + 8 * e + q);
-          } else if (d) {
-            T dd[8], dq[8];
+              for (int q = 0; q < 8; ++q) gv[q] = __ldg(a.gq + 8 * e + q);
+            } else if (d) {
+              T dd[8], dq[8];
 #pragma unroll
-            for (int L = 0; L < 8; ++L) {
-              const T* bb = (L & 4) ? b1 : b0;
-              dd[L] = bb[3 * nt + (eb + ((L >> 1) & 1)) * ntx + ea + (L & 1)];
+              for (int L = 0; L < 8; ++L) {
+                const T* bb = (L & 4) ? b1 : b0;
+                dd[L] = bb[3 * nt + (eb + ((L >> 1) & 1)) * ntx + ea + (L & 1)];
+              }
+              interp_sf(dd, dq);
+#pragma unroll
+              for (int q = 0; q < 8; ++q) gv[q] = g_deg(m.kappa, dq[q]);
+            } else {
+#pragma unroll
+              for (int q = 0; q < 8; ++q) gv[q] = T(1);
             }
-            interp_sf(dd, dq);
-#pragma unroll
-            for (int q = 0; q < 8; ++q) gv[q] = g_deg(m.kappa, dq[q]);
-          } else {
-#pragma unroll
-            for (int q = 0; q < 8; ++q) gv[q] = T(1);
           }
           T D[3][3][2][2];
 #pragma unroll
@@ -273,31 +287,33 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
               const T* bb = (L & 4) ? b1 : b0;
               u[L] = bb[c * nt + (eb + ((L >> 1) & 1)) * ntx + ea + (L & 1)];
             }
-            grad_k(u, K8, D[c][0], D[c][1], D[c][2]);
+            grad_k(u, a.k, D[c][0], D[c][1], D[c][2]);
           }
-          // the macro strain enters each strain component once: fold it into
-          // the gradient term that component starts from
+          if (EROWS) {
+            // the macro strain enters each strain component once: fold it into
+            // the gradient term that component starts from
 #pragma unroll
-          for (int i = 0; i < 2; ++i)
+            for (int i = 0; i < 2; ++i)
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-              D[0][0][i][j] += E6[0];
-              D[1][1][i][j] += E6[1];
-              D[2][2][i][j] += E6[2];
-              D[1][2][i][j] += E6[3];
-              D[0][2][i][j] += E6[4];
-              D[0][1][i][j] += E6[5];
-            }
+              for (int j = 0; j < 2; ++j) {
+                D[0][0][i][j] += E6[0];
+                D[1][1][i][j] += E6[1];
+                D[2][2][i][j] += E6[2];
+                D[1][2][i][j] += E6[3];
+                D[0][2][i][j] += E6[4];
+                D[0][1][i][j] += E6[5];
+              }
+          }
           T P[3][3][2][2];
 #pragma unroll
           for (int c = 0; c < 3; ++c)
 #pragma unroll
-            for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
 #pragma unroll
               for (int i = 0; i < 2; ++i)
 #pragma unroll
-                for (int j = 0; j < 2; ++j) P[c][a][i][j] = T(0);
-          // sigma_q * w * g_q at the eight Gauss points, summed into the P terms
+                for (int j = 0; j < 2; ++j) P[c][b][i][j] = T(0);
+          // w * g_q * sigma_q at the eight Gauss points, summed into the P terms
           auto qp_loop = [&](auto stress) {
 #pragma unroll
             for (int qz = 0; qz < 2; ++qz)
@@ -313,7 +329,7 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
                   ep[4] = D[0][2][qy][qx] + D[2][0][qz][qy];
                   ep[5] = D[0][1][qz][qx] + D[1][0][qz][qy];
                   T sg[6];
-                  stress(ep, gv[qx + 2 * qy + 4 * qz], sg);
+                  stress(ep, qx + 2 * qy + 4 * qz, sg);
                   if (ENERGY && own) {
 #pragma unroll
                     for (int k = 0; k < 6; ++k) tacc[kOutEnergy] += T(0.5) * sg[k] * ep[k];
@@ -329,27 +345,32 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
                   P[2][2][qy][qx] += sg[2];
                 }
           };
-          if constexpr (ISO) {
+          auto iso_stress = [&](const T* ep, T lg, T mg, T* sg) {
+            const T mg2 = mg + mg;
+            const T lt = lg * (ep[0] + ep[1] + ep[2]);
+            sg[0] = mg2 * ep[0] + lt;
+            sg[1] = mg2 * ep[1] + lt;
+            sg[2] = mg2 * ep[2] + lt;
+            sg[3] = mg * ep[3];
+            sg[4] = mg * ep[4];
+            sg[5] = mg * ep[5];
+          };
+          if constexpr (COEF == kCoefIso) {
             const T lw = m.lam[sl] * w, mw = m.mu[sl] * w;
-            qp_loop([&](const T* ep, T gg, T* sg) {
-              const T lg = lw * gg, mg = mw * gg, mg2 = mg + mg;
-              const T lt = lg * (ep[0] + ep[1] + ep[2]);
-              sg[0] = mg2 * ep[0] + lt;
-              sg[1] = mg2 * ep[1] + lt;
-              sg[2] = mg2 * ep[2] + lt;
-              sg[3] = mg * ep[3];
-              sg[4] = mg * ep[4];
-              sg[5] = mg * ep[5];
-            });
-          } else {
-            qp_loop([&](const T* ep, T gg, T* sg) {
+            qp_loop([&](const T* ep, int q, T* sg) { iso_stress(ep, lw * gv[q], mw * gv[q], sg); });
+          } else if constexpr (COEF == kCoefAniso) {
+            qp_loop([&](const T* ep, int q, T* sg) {
               voigt_stress(m, sl, ep, sg);
-              const T gw = gg * w;
+              const T gw = gv[q] * w;
 #pragma unroll
               for (int k = 0; k < 6; ++k) sg[k] *= gw;
             });
+          } else {
+            const T* lq = a.lam_q + 8 * e;
+            const T* mq = a.mu_q + 8 * e;
+            qp_loop([&](const T* ep, int q, T* sg) { iso_stress(ep, __ldg(lq + q) * w, __ldg(mq + q) * w, sg); });
           }
-          if (own) {
+          if (EROWS && own) {
 #pragma unroll
             for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -363,7 +384,7 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
               }
           }
 #pragma unroll
-          for (int c = 0; c < 3; ++c) grad_k_t(P[c][0], P[c][1], P[c][2], K8, f[c]);
+          for (int c = 0; c < 3; ++c) grad_k_t(P[c][0], P[c][1], P[c][2], a.k, f[c]);
         } else {
 #pragma unroll
           for (int c = 0; c < 3; ++c)
@@ -398,45 +419,59 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
           for (int c = 0; c < 3; ++c) {
             T v = pend[c] + lo[c];
             if (mk_cur & (1 << c)) v = T(0);
-            if (y) y[3 * n + c] = v;
-            if (DOT) tacc[kOutDot] += b0[c * nt + (nj + 1) * ntx + ni + 1] * v;
+            const size_t i = 3 * n + c;
+            const T xin = b0[c * nt + (nj + 1) * ntx + ni + 1];
+            if (CHEB) {
+              const T r = a.res[i] - v;
+              a.res[i] = r;
+              const T dn = c1 * xin + c2 * __ldg(a.invd + i) * r;
+              a.d_out[i] = dn;
+              a.xs[i] += dn;
+            } else {
+              if (a.y) a.y[i] = v;
+              if (DOT) tacc[kOutDot] += xin * v;
+            }
           }
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) pend[c] = up[c];
       }
     }
+    if (RED) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) accd[k] += double(tacc[k]);
+      for (int k = 0; k < 8; ++k) accd[k] += double(tacc[k]);
+    }
   }
 
-  __shared__ double sh[32];
-  constexpr int NK = DOT ? 8 : (ENERGY ? 7 : 6);
-#pragma unroll
-  for (int k = 0; k < NK; ++k) {
-    const double sm = block_sum(accd[k], sh);
-    if (tid == 0) ws.part[k * kMaxPartials + blockIdx.x] = sm;
-  }
-  if (arrive_last(ws.counter)) {
-    double dot_e = 0.0;
+  if constexpr (RED) {
+    __shared__ double sh[32];
+    constexpr int NK = DOT ? 8 : (ENERGY ? 7 : 6);
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
-      const double t = fold_sum(ws.part + k * kMaxPartials, gridDim.x, sh);
-      if (tid == 0) {
-        if (k < 6) {
-          ws.out[k] = t;
-          const size_t idx = 3 * (size_t)g.n_red + k;
-          const T v = (mask && mask[idx]) ? T(0) : T(t);
-          if (y) y[idx] = v;
-          dot_e += double(x[idx]) * double(v);
-        } else if (k == kOutEnergy) {
-          ws.out[k] = t;
-        } else {
-          ws.out[k] = t + dot_e;
+      const double sm = block_sum(accd[k], sh);
+      if (tid == 0) a.ws.part[k * kMaxPartials + blockIdx.x] = sm;
+    }
+    if (arrive_last(a.ws.counter)) {
+      double dot_e = 0.0;
+#pragma unroll
+      for (int k = 0; k < NK; ++k) {
+        const double t = fold_sum(a.ws.part + k * kMaxPartials, gridDim.x, sh);
+        if (tid == 0) {
+          if (k < 6) {
+            a.ws.out[k] = t;
+            const size_t idx = 3 * (size_t)g.n_red + k;
+            const T v = (a.mask && a.mask[idx]) ? T(0) : T(t);
+            if (a.y) a.y[idx] = v;
+            dot_e += double(x[idx]) * double(v);
+          } else if (k == kOutEnergy) {
+            a.ws.out[k] = t;
+          } else {
+            a.ws.out[k] = t + dot_e;
+          }
         }
       }
+      if (tid == 0) *a.ws.counter = 0u;
     }
-    if (tid == 0) *ws.counter = 0u;
   }
 }
 
@@ -445,10 +480,10 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
 namespace {
 
 std::mutex g_shape_mu;
-std::map<std::tuple<int, int, int, int, int, int, int>, TileShape> g_shapes;
+std::map<std::tuple<int, int, int, int, int, int, int, int>, TileShape> g_shapes;
 
-auto shape_key(const VoxGeom& g, int word) {
-  return std::make_tuple(g.rx, g.ry, g.rz, g.px, g.py, g.pz, word);
+auto shape_key(const VoxGeom& g, int word, int cls) {
+  return std::make_tuple(g.rx, g.ry, g.rz, g.px, g.py, g.pz, word, cls);
 }
 
 // Heuristic: among owned-node tiles of <= kTileMaxThreads element threads,
@@ -479,12 +514,11 @@ TileShape heuristic_shape(const VoxGeom& g, int word) {
   return best;
 }
 
-template <typename T, bool ISO, bool ENERGY, bool DOT>
-int launch_variant(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, const T* x, const T* gq, const T* d,
-                   const uint8_t* mask, T* y, RedWs ws, const int* guard, const TileShape& ts, cudaStream_t s) {
-  auto kern = h8_mech_tile_kernel<T, ISO, ENERGY, DOT>;
-  const size_t smem = tile_smem_bytes<T>(ts);
-  const int threads = tile_threads(ts);
+template <typename T, int COEF, int MODE, int OX, int OY>
+int launch_variant(const TileArgs<T>& a, const VoxMat<T>& m, cudaStream_t s) {
+  auto kern = h8_tile_kernel<T, COEF, MODE, OX, OY>;
+  const size_t smem = tile_smem_bytes<T>(a.ts);
+  const int threads = tile_threads(a.ts);
   static std::mutex mu;
   static size_t smem_set = 0;
   static std::map<std::pair<int, size_t>, int> occ;  // (threads, smem) -> resident blocks per SM
@@ -511,61 +545,198 @@ int launch_variant(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, co
   }
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long n_tiles = (long long)((v.rx + ts.ox - 1) / ts.ox) * ((v.ry + ts.oy - 1) / ts.oy) *
-                            ((v.rz + ts.kz - 1) / ts.kz);
+  const VoxGeom& v = a.g;
+  const long long n_tiles = (long long)((v.rx + a.ts.ox - 1) / a.ts.ox) * ((v.ry + a.ts.oy - 1) / a.ts.oy) *
+                            ((v.rz + a.ts.kz - 1) / a.ts.kz);
   long long grid = std::min<long long>(n_tiles, (long long)per_sm * sms);
   grid = std::min<long long>(grid, kMaxPartials);
-  TileK<T> k8;
-  k8.c1 = T(kC1);
-  k8.c2 = T(kC2);
-  k8.ihx = T(1.0 / v.hx);
-  k8.ihy = T(1.0 / v.hy);
-  k8.ihz = T(1.0 / v.hz);
-  k8.x1 = T(kC1 / v.hx);
-  k8.x2 = T(kC2 / v.hx);
-  k8.y1 = T(kC1 / v.hy);
-  k8.y2 = T(kC2 / v.hy);
-  k8.z1 = T(kC1 / v.hz);
-  k8.z2 = T(kC2 / v.hz);
-  { note_launch(); kern<<<(int)grid, threads, smem, s>>>(v, m, slot, x, gq, d, y, mask, ws, guard, ts, k8); }
+  { note_launch(); kern<<<(int)grid, threads, smem, s>>>(a, m); }
   return last_launch_status();
 }
 
 }  // namespace
 
-TileShape tile_shape_for(const VoxGeom& g, int word) {
-  {
-    std::lock_guard<std::mutex> lk(g_shape_mu);
-    auto it = g_shapes.find(shape_key(g, word));
-    if (it != g_shapes.end()) return it->second;
-  }
+bool tile_shape_lookup(const VoxGeom& g, int word, int cls, TileShape* t) {
+  std::lock_guard<std::mutex> lk(g_shape_mu);
+  auto it = g_shapes.find(shape_key(g, word, cls));
+  if (it == g_shapes.end()) return false;
+  *t = it->second;
+  return true;
+}
+
+TileShape tile_shape_for(const VoxGeom& g, int word, int cls) {
+  TileShape t;
+  if (tile_shape_lookup(g, word, cls, &t)) return t;
   return heuristic_shape(g, word);
 }
 
-void tile_shape_record(const VoxGeom& g, int word, const TileShape& t) {
+void tile_shape_record(const VoxGeom& g, int word, int cls, const TileShape& t) {
   std::lock_guard<std::mutex> lk(g_shape_mu);
-  g_shapes[shape_key(g, word)] = t;
+  g_shapes[shape_key(g, word, cls)] = t;
+}
+
+namespace {
+
+bool autotune_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("PHASTB_AUTOTUNE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+TileShape clamp_shape(TileShape t, const VoxGeom& v) {
+  t.ox = std::min(t.ox, v.rx);
+  t.oy = std::min(t.oy, v.ry);
+  t.kz = std::min(t.kz, v.rz);
+  return t;
+}
+
+// The hot variants are also compiled for a few fixed tile shapes (every
+// shared-memory offset then becomes a constant); other shapes run the generic
+// kernel.
+template <typename T, int COEF, int MODE>
+int by_shape(const TileArgs<T>& a, const VoxMat<T>& m, cudaStream_t s) {
+  const int ox = a.ts.ox, oy = a.ts.oy;
+  if (ox == 16 && oy == 8) return launch_variant<T, COEF, MODE, 16, 8>(a, m, s);
+  if (ox == 32 && oy == 4) return launch_variant<T, COEF, MODE, 32, 4>(a, m, s);
+  if (ox == 8 && oy == 8) return launch_variant<T, COEF, MODE, 8, 8>(a, m, s);
+  if (ox == 8 && oy == 4) return launch_variant<T, COEF, MODE, 8, 4>(a, m, s);
+  if (ox == 4 && oy == 4) return launch_variant<T, COEF, MODE, 4, 4>(a, m, s);
+  return launch_variant<T, COEF, MODE, 0, 0>(a, m, s);
+}
+
+template <typename T>
+int dispatch(const TileArgs<T>& a, const VoxMat<T>& m, int coef, int mode, cudaStream_t s) {
+  switch (coef * 4 + mode) {
+    case kCoefIso * 4 + kModeApply: return by_shape<T, kCoefIso, kModeApply>(a, m, s);
+    case kCoefIso * 4 + kModeDot: return by_shape<T, kCoefIso, kModeDot>(a, m, s);
+    case kCoefIso * 4 + kModeEnergy: return launch_variant<T, kCoefIso, kModeEnergy, 0, 0>(a, m, s);
+    case kCoefIso * 4 + kModeCheb: return by_shape<T, kCoefIso, kModeCheb>(a, m, s);
+    case kCoefAniso * 4 + kModeApply: return launch_variant<T, kCoefAniso, kModeApply, 0, 0>(a, m, s);
+    case kCoefAniso * 4 + kModeDot: return launch_variant<T, kCoefAniso, kModeDot, 0, 0>(a, m, s);
+    case kCoefAniso * 4 + kModeEnergy: return launch_variant<T, kCoefAniso, kModeEnergy, 0, 0>(a, m, s);
+    case kCoefAniso * 4 + kModeCheb: return launch_variant<T, kCoefAniso, kModeCheb, 0, 0>(a, m, s);
+    case kCoefQP * 4 + kModeApply: return by_shape<T, kCoefQP, kModeApply>(a, m, s);
+    case kCoefQP * 4 + kModeCheb: return by_shape<T, kCoefQP, kModeCheb>(a, m, s);
+    default: return PHASTB_ERR_ARG;
+  }
+}
+
+// Times the (coef, mode) launch of `a` over the candidate shapes (a's outputs
+// are overwritten; modes that update their inputs in place are not timed).
+template <typename T>
+int tune_shape(TileArgs<T> a, const VoxMat<T>& m, int coef, int mode, cudaStream_t s, TileShape* best_out,
+               float* best_ms) {
+  static const int cand[][2] = {{16, 8}, {32, 4},  {8, 8},   {8, 4},   {4, 4},   {16, 12}, {12, 16},
+                                {14, 14}, {24, 8}, {20, 8}, {12, 12}, {10, 10}, {6, 6},   {2, 4}};
+  static const int kzs[] = {1, 2, 4, 8, 16};
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return PHASTB_ERR_CUDA;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return PHASTB_ERR_CUDA;
+  }
+  int st = PHASTB_OK;
+  float best = 1e30f;
+  TileShape bs = clamp_shape(heuristic_shape(a.g, (int)sizeof(T)), a.g);
+  std::vector<TileShape> seen;
+  for (const auto& c : cand) {
+    for (int kz : kzs) {
+      const TileShape t = clamp_shape(TileShape{c[0], c[1], kz}, a.g);
+      if (!tile_ok(t)) continue;
+      bool dup = false;
+      for (const auto& q : seen) dup |= (q.ox == t.ox && q.oy == t.oy && q.kz == t.kz);
+      if (dup) continue;
+      seen.push_back(t);
+      a.ts = t;
+      if ((st = dispatch<T>(a, m, coef, mode, s))) break;
+      const int reps = 3;
+      cudaEventRecord(e0, s);
+      for (int r = 0; r < reps && !st; ++r) st = dispatch<T>(a, m, coef, mode, s);
+      cudaEventRecord(e1, s);
+      if (st || (st = cuda_status(cudaEventSynchronize(e1)))) break;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms /= reps;
+      if (ms < best) {
+        best = ms;
+        bs = t;
+      }
+    }
+    if (st) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) return st;
+  *best_out = bs;
+  if (best_ms) *best_ms = best;
+  return PHASTB_OK;
+}
+
+}  // namespace
+
+template <typename T>
+TileArgs<T> tile_args(const VoxGeom& v, int cls) {
+  TileArgs<T> a;
+  std::memset(&a, 0, sizeof(a));
+  a.g = v;
+  a.ts = clamp_shape(tile_shape_for(v, (int)sizeof(T), cls), v);
+  a.k.c1 = T(kC1);
+  a.k.c2 = T(kC2);
+  a.k.x1 = T(kC1 / v.hx);
+  a.k.x2 = T(kC2 / v.hx);
+  a.k.y1 = T(kC1 / v.hy);
+  a.k.y2 = T(kC2 / v.hy);
+  a.k.z1 = T(kC1 / v.hz);
+  a.k.z2 = T(kC2 / v.hz);
+  return a;
+}
+
+template <typename T>
+int h8_tile_launch(const TileArgs<T>& a, const VoxMat<T>& m, int coef, int mode, cudaStream_t s, bool tune) {
+  if (!tile_ok(a.ts) || a.ts.ox > a.g.rx || a.ts.oy > a.g.ry || a.ts.kz > a.g.rz) return PHASTB_ERR_ARG;
+  const int cls = coef == kCoefQP ? 1 : 0;
+  TileShape known;
+  if (tune && autotune_enabled() && (mode == kModeApply || mode == kModeDot) && a.guard == nullptr &&
+      !tile_shape_lookup(a.g, (int)sizeof(T), cls, &known)) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+      TileShape best;
+      int st = tune_shape<T>(a, m, coef, mode, s, &best, nullptr);
+      if (st) return st;
+      tile_shape_record(a.g, (int)sizeof(T), cls, best);
+      TileArgs<T> b = a;
+      b.ts = best;
+      return dispatch<T>(b, m, coef, mode, s);
+    }
+    cudaGetLastError();
+  }
+  return dispatch<T>(a, m, coef, mode, s);
 }
 
 template <typename T>
 int h8_mech_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, const T* x, const T* gq,
                         const T* d, const uint8_t* mask, T* y, RedWs ws, const int* guard, bool dot, bool energy,
                         cudaStream_t s, const TileShape* force_shape) {
-  TileShape ts = force_shape ? *force_shape : tile_shape_for(v, (int)sizeof(T));
-  ts.ox = std::min(ts.ox, v.rx);
-  ts.oy = std::min(ts.oy, v.ry);
-  ts.kz = std::min(ts.kz, v.rz);
-  if (!tile_ok(ts)) return PHASTB_ERR_ARG;
-  if (m.iso) {
-    if (dot) return launch_variant<T, true, false, true>(v, m, slot, x, gq, d, mask, y, ws, guard, ts, s);
-    if (energy) return launch_variant<T, true, true, false>(v, m, slot, x, gq, d, mask, y, ws, guard, ts, s);
-    return launch_variant<T, true, false, false>(v, m, slot, x, gq, d, mask, y, ws, guard, ts, s);
-  }
-  if (dot) return launch_variant<T, false, false, true>(v, m, slot, x, gq, d, mask, y, ws, guard, ts, s);
-  if (energy) return launch_variant<T, false, true, false>(v, m, slot, x, gq, d, mask, y, ws, guard, ts, s);
-  return launch_variant<T, false, false, false>(v, m, slot, x, gq, d, mask, y, ws, guard, ts, s);
+  TileArgs<T> a = tile_args<T>(v, 0);
+  if (force_shape) a.ts = clamp_shape(*force_shape, v);
+  a.slot = slot;
+  a.gq = gq;
+  a.d = d;
+  a.x = x;
+  a.y = y;
+  a.mask = mask;
+  a.ws = ws;
+  a.guard = guard;
+  const int coef = m.iso ? kCoefIso : kCoefAniso;
+  return h8_tile_launch<T>(a, m, coef, dot ? kModeDot : (energy ? kModeEnergy : kModeApply), s, !force_shape);
 }
 
+template TileArgs<double> tile_args<double>(const VoxGeom&, int);
+template TileArgs<float> tile_args<float>(const VoxGeom&, int);
+template int h8_tile_launch<double>(const TileArgs<double>&, const VoxMat<double>&, int, int, cudaStream_t, bool);
+template int h8_tile_launch<float>(const TileArgs<float>&, const VoxMat<float>&, int, int, cudaStream_t, bool);
 template int h8_mech_tile_launch<double>(const VoxGeom&, const VoxMat<double>&, const uint8_t*, const double*,
                                          const double*, const double*, const uint8_t*, double*, RedWs, const int*,
                                          bool, bool, cudaStream_t, const TileShape*);
@@ -586,47 +757,15 @@ namespace {
 template <typename T>
 int tune_t(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, const T* x, const T* d, T* y, RedWs ws,
            cudaStream_t s, TileShape* best_out, float* best_ms) {
-  static const int cand[][2] = {{16, 12}, {12, 16}, {14, 14}, {24, 8}, {16, 8}, {8, 16}, {20, 8},
-                                {32, 4},  {12, 12}, {10, 10}, {8, 8},  {6, 6},  {4, 4}};
-  static const int kzs[] = {2, 4, 8, 16};
-  cudaEvent_t e0, e1;
-  if (cudaEventCreate(&e0) != cudaSuccess) return PHASTB_ERR_CUDA;
-  if (cudaEventCreate(&e1) != cudaSuccess) {
-    cudaEventDestroy(e0);
-    return PHASTB_ERR_CUDA;
-  }
-  int st = PHASTB_OK;
-  float best = 1e30f;
-  TileShape bs = heuristic_shape(v, (int)sizeof(T));
-  for (const auto& c : cand) {
-    for (int kz : kzs) {
-      TileShape t{std::min(c[0], v.rx), std::min(c[1], v.ry), std::min(kz, v.rz)};
-      if (!tile_ok(t)) continue;
-      for (int r = 0; r < 2 && !st; ++r)
-        st = h8_mech_tile_launch<T>(v, m, slot, x, nullptr, d, nullptr, y, ws, nullptr, false, false, s, &t);
-      if (st) break;
-      const int reps = 5;
-      cudaEventRecord(e0, s);
-      for (int r = 0; r < reps && !st; ++r)
-        st = h8_mech_tile_launch<T>(v, m, slot, x, nullptr, d, nullptr, y, ws, nullptr, false, false, s, &t);
-      cudaEventRecord(e1, s);
-      if (st || (st = cuda_status(cudaEventSynchronize(e1)))) break;
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      ms /= reps;
-      if (ms < best) {
-        best = ms;
-        bs = t;
-      }
-    }
-    if (st) break;
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  TileArgs<T> a = tile_args<T>(v, 0);
+  a.slot = slot;
+  a.d = d;
+  a.x = x;
+  a.y = y;
+  a.ws = ws;
+  int st = tune_shape<T>(a, m, m.iso ? kCoefIso : kCoefAniso, kModeApply, s, best_out, best_ms);
   if (st) return st;
-  tile_shape_record(v, (int)sizeof(T), bs);
-  *best_out = bs;
-  *best_ms = best;
+  tile_shape_record(v, (int)sizeof(T), 0, *best_out);
   return PHASTB_OK;
 }
 
@@ -644,10 +783,10 @@ int phastb_h8_tile_shape(const phastb_voxel_grid* g, int dtype, int set, int* sh
   if (set) {
     TileShape t{shape[0], shape[1], shape[2]};
     if (!tile_ok(t)) return PHASTB_ERR_ARG;
-    tile_shape_record(v, word, t);
+    tile_shape_record(v, word, 0, t);
     return PHASTB_OK;
   }
-  const TileShape t = tile_shape_for(v, word);
+  const TileShape t = tile_shape_for(v, word, 0);
   shape[0] = std::min(t.ox, v.rx);
   shape[1] = std::min(t.oy, v.ry);
   shape[2] = std::min(t.kz, v.rz);

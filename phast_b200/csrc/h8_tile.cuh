@@ -43,12 +43,52 @@ inline size_t tile_smem_bytes(const TileShape& t) {
 // Result slots of the apply's reduction workspace (ws.out).
 enum ApplyOut { kOutE = 0, kOutEnergy = 6, kOutDot = 7, kApplyOuts = 8 };
 
-// Tile shape used for a grid and word size: the autotuned choice when one was
-// recorded for this grid, otherwise a heuristic.
-TileShape tile_shape_for(const VoxGeom& g, int word);
+// Element coefficients: material slot with g(d) (isotropic / general Voigt), or
+// per-Gauss-point isotropic moduli (multigrid coarse levels, no macro strain).
+enum TileCoef { kCoefIso = 0, kCoefAniso = 1, kCoefQP = 2 };
+// Node epilogue: y = A x; y and x . y; y and the energy; one Chebyshev step.
+enum TileMode { kModeApply = 0, kModeDot = 1, kModeEnergy = 2, kModeCheb = 3 };
 
-// Records / forgets a tuned tile shape (host table, per process).
-void tile_shape_record(const VoxGeom& g, int word, const TileShape& t);
+// Gauss-point constants of the action: N1 weights with the 1/h of each axis
+// folded in (the last interpolation stage of a derivative applies them).
+template <typename T>
+struct TileK {
+  T c1, c2;                  // N1 = [[c1, c2], [c2, c1]]
+  T x1, x2, y1, y2, z1, z2;  // c1/h, c2/h per axis
+};
+
+template <typename T>
+struct TileArgs {
+  VoxGeom g;
+  TileShape ts;
+  int pad_;
+  const uint8_t* slot;  // kCoefIso / kCoefAniso
+  const T* gq;          // optional (E, 8) degradation; else g(d) from d, else 1
+  const T* d;
+  const T* lam_q;       // kCoefQP: (E, 8) moduli
+  const T* mu_q;
+  const T* x;
+  T* y;
+  const uint8_t* mask;
+  // kModeCheb: res -= A x;  d_out = c1 x + c2 invd res;  xs += d_out
+  T* res;
+  const T* invd;
+  T* xs;
+  T* d_out;
+  double c1, c2;
+  RedWs ws;
+  const int* guard;
+  TileK<T> k;
+};
+
+// Tile shape used for a grid, word size and coefficient class (0: material
+// slots, 1: per-Gauss-point moduli): the recorded (tuned or pinned) choice when
+// there is one, otherwise a heuristic.
+TileShape tile_shape_for(const VoxGeom& g, int word, int cls);
+bool tile_shape_lookup(const VoxGeom& g, int word, int cls, TileShape* t);
+
+// Records a tile shape (host table, per process).
+void tile_shape_record(const VoxGeom& g, int word, int cls, const TileShape& t);
 
 // y = A(d) x with fused g(d); optional x . y (DOT) and energy (ENERGY).  ws.out
 // receives the E-row sums (kOutE..), the energy and the dot.
@@ -56,5 +96,17 @@ template <typename T>
 int h8_mech_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, const T* x, const T* gq,
                         const T* d, const uint8_t* mask, T* y, RedWs ws, const int* guard, bool dot, bool energy,
                         cudaStream_t s, const TileShape* force_shape = nullptr);
+
+// Fills the geometry-derived members of a TileArgs (g, ts, k) for grid v and
+// coefficient class cls.
+template <typename T>
+TileArgs<T> tile_args(const VoxGeom& v, int cls);
+
+// Launches the tile kernel for (COEF, MODE) with prepared arguments.  With
+// `tune`, the first plain or dot launch for a grid with no recorded shape
+// (outside stream capture, unguarded) times the candidate shapes and records
+// the fastest; PHASTB_AUTOTUNE=0 in the environment keeps the heuristic.
+template <typename T>
+int h8_tile_launch(const TileArgs<T>& a, const VoxMat<T>& m, int coef, int mode, cudaStream_t s, bool tune = true);
 
 }  // namespace phastb

@@ -12,6 +12,10 @@ bool valid_vox(const phastb_voxel_grid* g);
 bool valid_mat(const phastb_voxel_material* m);
 size_t h8_scratch_bytes(const VoxGeom& v, int dtype);
 template <typename T>
+int h8_mech_apply_dot_t(const VoxGeom& v, const VoxMat<T>& mm, const uint8_t* slot, const T* x, const T* gq,
+                        const T* d, const uint8_t* mask, T* y, void* scratch, const int* guard, cudaStream_t s);
+const double* h8_apply_dot_slot(const VoxGeom& v, int word, void* scratch);
+template <typename T>
 int h8_mech_apply_t(const VoxGeom& v, const VoxMat<T>& mm, const uint8_t* slot, const T* x, const T* gq,
                     const T* d, const uint8_t* mask, T* y, void* scratch, const int* guard, cudaStream_t s);
 template <typename T>
@@ -34,6 +38,11 @@ struct MechCtx {
 static int mech_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
   const MechCtx* k = static_cast<const MechCtx*>(c);
   return h8_mech_apply_t<double>(k->v, k->m, k->slot, x, k->gq, k->d, k->mask, y, k->scratch, guard, s);
+}
+
+static int mech_op_dot(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
+  const MechCtx* k = static_cast<const MechCtx*>(c);
+  return h8_mech_apply_dot_t<double>(k->v, k->m, k->slot, x, k->gq, k->d, k->mask, y, k->scratch, guard, s);
 }
 
 struct DamageCtx {
@@ -283,7 +292,7 @@ int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material
   }
   const double thr = std::max(rtol * bn, atol);
   MechCtx free_ctx{v, mm, slot, gq, d, fixed, scratch};
-  LinOp<double> A{mech_op, &free_ctx, sizeof(free_ctx)};
+  LinOp<double> A{mech_op, &free_ctx, sizeof(free_ctx), mech_op_dot, h8_apply_dot_slot(v, 8, scratch)};
   PcgResult pr{};
   if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, x_out, thr, maxiter, check_every, PCG_FREEZE, 0.0, &pr, s)))
     return st;
