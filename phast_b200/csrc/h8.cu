@@ -490,6 +490,12 @@ int h8_mech_apply_dot_t(const VoxGeom& v, const VoxMat<T>& mm, const uint8_t* sl
   return h8_mech_tile_launch<T>(v, mm, slot, x, gq, d, mask, y, ws, guard, true, false, s);
 }
 
+// The reduction ticket inside an element scratch must start at zero: every
+// entry point that hands a caller workspace to the actions resets it once.
+int h8_scratch_reset(const VoxGeom& v, int word, void* scratch, cudaStream_t s) {
+  return red_ws_reset(red_ws(static_cast<char*>(scratch) + align_up(24 * (size_t)word * (size_t)v.n_elem)), s);
+}
+
 const double* h8_apply_dot_slot(const VoxGeom& v, int word, void* scratch) {
   return red_ws(static_cast<char*>(scratch) + align_up(24 * (size_t)word * (size_t)v.n_elem)).out + kOutDot;
 }
@@ -543,9 +549,11 @@ int h8_damage_launch(const VoxGeom& v, const VoxMat<double>& mm, const uint8_t* 
   double* sc = static_cast<double*>(scratch);
   const int G = grid_for(v.n_elem);
   const double kd = damage_kdiag(v, double(mm.ell));
-  if (mode == 0)
-    { note_launch(); h8_damage_elem_kernel<0><<<G, kThreads, 0, s>>>(v, mm, slot, d, H, scale, kd, sc, guard); }
-  else if (mode == 1)
+  if (mode == 0 || mode == 3) {
+    RedWs ws = red_ws(static_cast<char*>(scratch) + align_up(24 * sizeof(double) * (size_t)v.n_elem));
+    return h8_damage_tile_launch<double>(v, mm, slot, d, H, scale, mask, y, ws, guard, mode == 3, s);
+  }
+  if (mode == 1)
     { note_launch(); h8_damage_elem_kernel<1><<<G, kThreads, 0, s>>>(v, mm, slot, d, H, scale, kd, sc, guard); }
   else
     { note_launch(); h8_damage_elem_kernel<2><<<G, kThreads, 0, s>>>(v, mm, slot, d, H, scale, kd, sc, guard); }

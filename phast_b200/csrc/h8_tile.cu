@@ -475,6 +475,152 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
   }
 }
 
+// ------------------------------------------------------------------ damage action
+
+// Scalar AT2 damage action on the same brick schedule:
+//   y = scale * [Gc_e (M / ell + ell L) d + 2 (1 - kappa) sum_q w H_q N_q N_q^T d]
+// (the element arithmetic of h8_damage_elem_kernel), masked rows zero, and with
+// MODE == kModeDot also x . y into ws.out[kOutDot].
+template <typename T, int MODE, int OX, int OY>
+__global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_kernel(DTileArgs<T> a) {
+  if (a.guard && *a.guard == 0) return;
+  constexpr bool DOT = MODE == kModeDot;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const VoxGeom& g = a.g;
+  const int ox = OX ? OX : a.ts.ox, oy = OY ? OY : a.ts.oy, kz = a.ts.kz;
+  const int ex = ox + 1, exy = ex * (oy + 1);
+  const int ntx = ox + 2, nt = ntx * (oy + 2);
+  T* nb = reinterpret_cast<T*>(smem_raw);  // [3 buffers][nt]
+  T* FL = nb + 3 * nt;                     // [4 corners][exy]
+  T* FU = FL + 4 * exy;
+  const int tid = threadIdx.x;
+  const T w = T(g.w), ell = T(a.ell), ch = T(2.0 * (1.0 - a.kappa)), sc = T(a.scale);
+  const int tiles_x = (g.rx + ox - 1) / ox, tiles_y = (g.ry + oy - 1) / oy;
+  const int tiles_xy = tiles_x * tiles_y;
+  const int n_tiles = tiles_xy * ((g.rz + kz - 1) / kz);
+  const int ea = tid % ex, eb = tid / ex;
+  const int ni = tid % ox, nj = tid / ox;
+  const bool is_elem = tid < exy, is_node = tid < ox * oy;
+  double accd = 0.0;
+  auto stage1 = [&](int i0, int j0, int kn, T (&r)[2]) {
+    const int gk = wrap_node(kn, g.nz, g.rz, g.pz);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int t = tid + h * blockDim.x;
+      T v = T(0);
+      if (t < nt && gk >= 0) {
+        const int gi = wrap_node(i0 - 1 + t % ntx, g.nx, g.rx, g.px);
+        const int gj = wrap_node(j0 - 1 + t / ntx, g.ny, g.ry, g.py);
+        if (gi >= 0 && gj >= 0) v = __ldg(a.x + (size_t)gi + (size_t)g.rx * ((size_t)gj + (size_t)g.ry * gk));
+      }
+      r[h] = v;
+    }
+  };
+  auto store1 = [&](const T (&r)[2], T* buf) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int t = tid + h * blockDim.x;
+      if (t < nt) buf[t] = r[h];
+    }
+  };
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int tz = tile / tiles_xy, txy = tile - tz * tiles_xy;
+    const int i0 = (txy % tiles_x) * ox, j0 = (txy / tiles_x) * oy;
+    const int k0 = tz * kz, k1 = min(k0 + kz, g.rz);
+    T tdot = T(0), pend = T(0);
+    T pf[2];
+    stage1(i0, j0, k0 - 1, pf);
+    __syncthreads();
+    store1(pf, nb);
+    stage1(i0, j0, k0, pf);
+    const int K = k1 - k0;
+    for (int kk = 0; kk <= K; ++kk) {
+      const int ke = k0 - 1 + kk;
+      T* b0 = nb + nt * (kk % 3);
+      T* b1 = nb + nt * ((kk + 1) % 3);
+      store1(pf, b1);
+      if (kk < K) stage1(i0, j0, ke + 2, pf);
+      __syncthreads();
+      if (is_elem) {
+        const int gi = wrap_elem(i0 - 1 + ea, g.nx, g.px);
+        const int gj = wrap_elem(j0 - 1 + eb, g.ny, g.py);
+        const int gk = wrap_elem(ke, g.nz, g.pz);
+        T out[8];
+        if (gi >= 0 && gj >= 0 && gk >= 0) {
+          const size_t e = (size_t)gi + (size_t)g.nx * ((size_t)gj + (size_t)g.ny * gk);
+          const T Gc = a.Gc[__ldg(a.slot + e)];
+          T dd[8], dq[8];
+#pragma unroll
+          for (int L = 0; L < 8; ++L) {
+            const T* bb = (L & 4) ? b1 : b0;
+            dd[L] = bb[(eb + ((L >> 1) & 1)) * ntx + ea + (L & 1)];
+          }
+          interp_sf(dd, dq);
+          T mq[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const T Hq = a.H ? __ldg(a.H + 8 * e + q) : T(0);
+            mq[q] = w * (Gc / ell + ch * Hq) * dq[q];
+          }
+          interp_sf_t(mq, out);
+          T Dx[2][2], Dy[2][2], Dz[2][2];
+          grad_k(dd, a.k, Dx, Dy, Dz);
+          const T k2 = T(2) * w * Gc * ell;
+#pragma unroll
+          for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+              Dx[i][j] *= k2;
+              Dy[i][j] *= k2;
+              Dz[i][j] *= k2;
+            }
+          T og[8];
+          grad_k_t(Dx, Dy, Dz, a.k, og);
+#pragma unroll
+          for (int L = 0; L < 8; ++L) out[L] = sc * (out[L] + og[L]);
+        } else {
+#pragma unroll
+          for (int L = 0; L < 8; ++L) out[L] = T(0);
+        }
+#pragma unroll
+        for (int L = 0; L < 4; ++L) {
+          FL[L * exy + tid] = out[L];
+          FU[L * exy + tid] = out[L + 4];
+        }
+      }
+      __syncthreads();
+      if (is_node) {
+        const int e11 = (ni + 1) + ex * (nj + 1), e01 = ni + ex * (nj + 1);
+        const int e10 = (ni + 1) + ex * nj, e00 = ni + ex * nj;
+        const T lo = FL[0 * exy + e11] + FL[1 * exy + e01] + FL[2 * exy + e10] + FL[3 * exy + e00];
+        const T up = FU[0 * exy + e11] + FU[1 * exy + e01] + FU[2 * exy + e10] + FU[3 * exy + e00];
+        const int gi = i0 + ni, gj = j0 + nj;
+        if (kk >= 1 && gi < g.rx && gj < g.ry) {
+          const size_t n = (size_t)gi + (size_t)g.rx * ((size_t)gj + (size_t)g.ry * ke);
+          T v = pend + lo;
+          if (a.mask && __ldg(a.mask + n)) v = T(0);
+          a.y[n] = v;
+          if (DOT) tdot += b0[(nj + 1) * ntx + ni + 1] * v;
+        }
+        pend = up;
+      }
+    }
+    if (DOT) accd += double(tdot);
+  }
+  if constexpr (DOT) {
+    __shared__ double sh[32];
+    const double sm = block_sum(accd, sh);
+    if (tid == 0) a.ws.part[kOutDot * kMaxPartials + blockIdx.x] = sm;
+    if (arrive_last(a.ws.counter)) {
+      const double t = fold_sum(a.ws.part + kOutDot * kMaxPartials, gridDim.x, sh);
+      if (tid == 0) {
+        a.ws.out[kOutDot] = t;
+        *a.ws.counter = 0u;
+      }
+    }
+  }
+}
+
 // ------------------------------------------------------------------ host side
 
 namespace {
@@ -733,6 +879,121 @@ int h8_mech_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slo
   return h8_tile_launch<T>(a, m, coef, dot ? kModeDot : (energy ? kModeEnergy : kModeApply), s, !force_shape);
 }
 
+template <typename T, int MODE, int OX, int OY>
+int dlaunch_variant(const DTileArgs<T>& a, cudaStream_t s) {
+  auto kern = h8_dtile_kernel<T, MODE, OX, OY>;
+  const size_t nt = (size_t)(a.ts.ox + 2) * (a.ts.oy + 2), exy = (size_t)(a.ts.ox + 1) * (a.ts.oy + 1);
+  const size_t smem = sizeof(T) * (3 * nt + 8 * exy);
+  const int threads = tile_threads(a.ts);
+  static std::mutex mu;
+  static std::map<std::pair<int, size_t>, int> occ;
+  int per_sm = 1;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = occ.find({threads, smem});
+    if (it == occ.end()) {
+      int b = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        b = 1;
+      }
+      it = occ.emplace(std::make_pair(threads, smem), b < 1 ? 1 : b).first;
+    }
+    per_sm = it->second;
+  }
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const VoxGeom& v = a.g;
+  const long long n_tiles = (long long)((v.rx + a.ts.ox - 1) / a.ts.ox) * ((v.ry + a.ts.oy - 1) / a.ts.oy) *
+                            ((v.rz + a.ts.kz - 1) / a.ts.kz);
+  long long grid = std::min<long long>(n_tiles, (long long)per_sm * sms);
+  grid = std::min<long long>(grid, kMaxPartials);
+  { note_launch(); kern<<<(int)grid, threads, smem, s>>>(a); }
+  return last_launch_status();
+}
+
+template <typename T, int MODE>
+int dby_shape(const DTileArgs<T>& a, cudaStream_t s) {
+  const int ox = a.ts.ox, oy = a.ts.oy;
+  if (ox == 16 && oy == 8) return dlaunch_variant<T, MODE, 16, 8>(a, s);
+  if (ox == 32 && oy == 4) return dlaunch_variant<T, MODE, 32, 4>(a, s);
+  if (ox == 8 && oy == 8) return dlaunch_variant<T, MODE, 8, 8>(a, s);
+  return dlaunch_variant<T, MODE, 0, 0>(a, s);
+}
+
+template <typename T>
+int h8_damage_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, const T* x, const T* H,
+                          double scale, const uint8_t* mask, T* y, RedWs ws, const int* guard, bool dot,
+                          cudaStream_t s) {
+  DTileArgs<T> a;
+  std::memset(&a, 0, sizeof(a));
+  const TileArgs<T> base = tile_args<T>(v, 2);
+  a.g = v;
+  a.ts = base.ts;
+  a.k = base.k;
+  a.slot = slot;
+  for (int i = 0; i < PHASTB_MAX_SLOTS; ++i) a.Gc[i] = m.Gc[i];
+  a.kappa = double(m.kappa);
+  a.ell = double(m.ell);
+  a.scale = scale;
+  a.H = H;
+  a.x = x;
+  a.y = y;
+  a.mask = mask;
+  a.ws = ws;
+  a.guard = guard;
+  if (!tile_ok(a.ts)) return PHASTB_ERR_ARG;
+  auto run = [&](const DTileArgs<T>& b) { return dot ? dby_shape<T, kModeDot>(b, s) : dby_shape<T, kModeApply>(b, s); };
+  TileShape known;
+  if (autotune_enabled() && guard == nullptr && !tile_shape_lookup(v, (int)sizeof(T), 2, &known)) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+      // time the candidate shapes on this call's buffers (y is recomputed below)
+      static const int cand[][2] = {{16, 8}, {32, 4}, {8, 8}, {16, 12}, {14, 14}, {10, 10}, {8, 4}, {4, 4}};
+      static const int kzs[] = {2, 4, 8, 16};
+      cudaEvent_t e0, e1;
+      if (cudaEventCreate(&e0) != cudaSuccess) return PHASTB_ERR_CUDA;
+      if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return PHASTB_ERR_CUDA;
+      }
+      int st = PHASTB_OK;
+      float best = 1e30f;
+      TileShape bs = a.ts;
+      DTileArgs<T> b = a;
+      for (const auto& c : cand) {
+        for (int kz : kzs) {
+          b.ts = clamp_shape(TileShape{c[0], c[1], kz}, v);
+          if (!tile_ok(b.ts)) continue;
+          if ((st = run(b))) break;
+          cudaEventRecord(e0, s);
+          for (int r = 0; r < 3 && !st; ++r) st = run(b);
+          cudaEventRecord(e1, s);
+          if (st || (st = cuda_status(cudaEventSynchronize(e1)))) break;
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, e0, e1);
+          if (ms < best) {
+            best = ms;
+            bs = b.ts;
+          }
+        }
+        if (st) break;
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      if (st) return st;
+      tile_shape_record(v, (int)sizeof(T), 2, bs);
+      a.ts = bs;
+    } else {
+      cudaGetLastError();
+    }
+  }
+  return run(a);
+}
+
+template int h8_damage_tile_launch<double>(const VoxGeom&, const VoxMat<double>&, const uint8_t*, const double*,
+                                           const double*, double, const uint8_t*, double*, RedWs, const int*, bool,
+                                           cudaStream_t);
 template TileArgs<double> tile_args<double>(const VoxGeom&, int);
 template TileArgs<float> tile_args<float>(const VoxGeom&, int);
 template int h8_tile_launch<double>(const TileArgs<double>&, const VoxMat<double>&, int, int, cudaStream_t, bool);

@@ -90,6 +90,31 @@ bool tile_shape_lookup(const VoxGeom& g, int word, int cls, TileShape* t);
 // Records a tile shape (host table, per process).
 void tile_shape_record(const VoxGeom& g, int word, int cls, const TileShape& t);
 
+template <typename T>
+struct DTileArgs {
+  VoxGeom g;
+  TileShape ts;
+  int pad_;
+  const uint8_t* slot;
+  T Gc[PHASTB_MAX_SLOTS];
+  double kappa, ell, scale;
+  const T* H;  // (E, 8) history, may be null
+  const T* x;
+  T* y;
+  const uint8_t* mask;
+  RedWs ws;
+  const int* guard;
+  TileK<T> k;
+};
+
+// Damage action y = scale [Gc (M/ell + ell L) + 2 (1-kappa) H-mass] x on the
+// brick schedule (tile shapes of coefficient class 2), masked rows zero; with
+// `dot` also x . y at ws.out[kOutDot].
+template <typename T>
+int h8_damage_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, const T* x, const T* H,
+                          double scale, const uint8_t* mask, T* y, RedWs ws, const int* guard, bool dot,
+                          cudaStream_t s);
+
 // y = A(d) x with fused g(d); optional x . y (DOT) and energy (ENERGY).  ws.out
 // receives the E-row sums (kOutE..), the energy and the dot.
 template <typename T>

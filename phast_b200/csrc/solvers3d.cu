@@ -60,6 +60,12 @@ static int damage_op(const void* c, const double* x, double* y, const int* guard
   return h8_damage_launch(k->v, k->m, k->slot, 0, x, k->H, k->scale, y, k->mask, k->scratch, guard, s);
 }
 
+// the action plus x . y (mode 3 of h8_damage_launch)
+static int damage_op_dot(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
+  const DamageCtx* k = static_cast<const DamageCtx*>(c);
+  return h8_damage_launch(k->v, k->m, k->slot, 3, x, k->H, k->scale, y, k->mask, k->scratch, guard, s);
+}
+
 // xc = where(fixed, vals, 0); x0f = where(free, x0, 0); invd = 1/where(free, diag, 1)
 __global__ void constrained_setup_kernel(int n, const uint8_t* __restrict__ fixed, const double* __restrict__ vals,
                                          const double* __restrict__ x0, double* __restrict__ xc,
@@ -342,9 +348,12 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
   uint8_t* fixed = la + 2 * ub;
   char* scratch = p + 6 * vb + 4 * ub;
   RedWs rw = red_ws(scratch + h8_scratch_bytes(v, PHASTB_F64));
+  // the action's own reduction ticket (x . y of the fused CG) lives inside the scratch
+  RedWs aw = red_ws(scratch + align_up(24 * sizeof(double) * (size_t)v.n_elem));
   const int G = grid_for(n);
   int st;
   if ((st = red_ws_reset(rw, s))) return st;
+  if ((st = red_ws_reset(aw, s))) return st;
   if ((st = h8_damage_launch(v, mm, slot, 1, nullptr, H, scale, rhs, nullptr, scratch, nullptr, s))) return st;
   if (!H && (st = cuda_status(cudaMemsetAsync(rhs, 0, sizeof(double) * n, s)))) return st;
   if ((st = h8_damage_launch(v, mm, slot, 2, nullptr, H, scale, diag, nullptr, scratch, nullptr, s))) return st;
@@ -360,7 +369,7 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
     if ((st = last_launch_status())) return st;
     // Dirichlet PCG on the free set: tolerance relative to max(||r0||, 1)
     DamageCtx fctx{v, mm, slot, H, scale, fixed, scratch};
-    LinOp<double> A{damage_op, &fctx, sizeof(fctx)};
+    LinOp<double> A{damage_op, &fctx, sizeof(fctx), damage_op_dot, h8_apply_dot_slot(v, 8, scratch)};
     PcgResult pr{};
     if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, d_out, -lin_tol, max_lin, 10, PCG_STRICT, 0.0, &pr,
                               s)))

@@ -214,6 +214,7 @@ class StaggeredSolver:
         self.cfg = cfg or SolverConfig()
         self.form = form
         self._lmax = (C.c_double * 3)()
+        self.lmax_every = 10
         self.load = op.load
         self._c = int(op.load.controlled)
         self._n_u = 3 * op.n_red
@@ -283,7 +284,10 @@ class StaggeredSolver:
             raise ValueError(f"target {target!r} equals the current controlled strain")
         increment = state.increment + 1 if increment is None else int(increment)
         t0 = perf_counter()
-        self._lmax[0] = 0.0  # fresh multigrid eigenvalue estimates for every increment
+        # lambda_max of the Jacobi-scaled operator barely moves with the damage
+        # field; the multigrid re-estimates it every `lmax_every` increments
+        if (increment - 1) % self.lmax_every == 0:
+            self._lmax[0] = 0.0
         try:
             return self._attempt(state, target, previous, increment, t0)
         except _AttemptFailure as exc:
