@@ -36,6 +36,7 @@ sys.path.insert(0, ROOT)
 METRIC = "staggered steps/s, chosen vs plain FP64 on 1 B200 at ≤1e-6 rel err; HBM GB/s"
 UNIT = "staggered steps/s"
 N_CELL = 64
+N_LARGE = 192  # roofline cell: the action's working set (about 200 MB in FP32) exceeds the 126 MB L2
 INCREMENTS = 50
 # Mean per-increment iteration counts of this workload over increments 4..5
 # (the default timed window), measured with this repository's CUDA solver on a
@@ -302,22 +303,18 @@ def run_ours(args, rank, world, device):
     mixed = chosen.mixed
     kdt = torch.float32 if mixed else torch.float64
     x, d = st_c.x.to(kdt).contiguous(), st_c.d.to(kdt).contiguous()
-    for _ in range(3):
-        op.mech_action(x, d=d)
-    n_rep, ms = 20, 0.0
-    for _ in range(n_rep):
-        flush_l2(flush)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        op.mech_action(x, d=d)
-        e1.record()
-        torch.cuda.synchronize()
-        ms += e0.elapsed_time(e1)
-    apply_s = ms / n_rep / 1e3
+    apply_s = time_action(op, x, d, flush)
     wsz = 4 if mixed else 8
     alg_bytes = 7 * op.n_red * wsz + op.n_elements * 1  # read u~ 3n, d n; write 3n; slot id per voxel
     peak, peak_src = peaks()
     achieved = alg_bytes / apply_s / 1e9
+    # the same kernel on a cell whose working set exceeds L2 (HBM-bound regime)
+    big, _ = build_cell(device, N_LARGE)
+    xb = torch.as_tensor(np.random.default_rng(1).normal(size=big.n_mech) * 1e-3, device=device).to(kdt)
+    db = torch.as_tensor(np.random.default_rng(2).uniform(0, 0.9, size=big.n_red), device=device).to(kdt)
+    big_s = time_action(big, xb, db, flush)
+    big_bytes = 7 * big.n_red * wsz + big.n_elements
+    del big, xb, db
     mech = float(np.mean([c[0] for c in counts]))
     pf = float(np.mean([c[1] for c in counts]))
     stag = float(np.mean([c[2] for c in counts]))
@@ -335,8 +332,12 @@ def run_ours(args, rank, world, device):
         "rel_err_vs_plain_fp64": err,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": profile_traffic(mixed),
-                     "kernel": f"h8 elastic action (element kernel + node gather), {'FP32' if mixed else 'FP64'}",
+                     "kernel": f"h8 elastic action (tiled z-marching, fused g(d)), {'FP32' if mixed else 'FP64'}",
+                     "note": "64^3 working set is L2-resident; HBM fraction of the large cell in roofline_large",
                      "algorithmic_bytes": alg_bytes, "launch_ms": apply_s * 1e3, "peak_source": peak_src},
+        "roofline_large": {"bound": "hbm", "cell": f"{N_LARGE}^3", "achieved": big_bytes / big_s / 1e9, "peak": peak,
+                           "unit": "GB/s", "frac": big_bytes / big_s / 1e9 / peak, "algorithmic_bytes": big_bytes,
+                           "launch_ms": big_s * 1e3},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
         "gpu_launches": int(launches),
         "clocks": clk,
@@ -348,6 +349,25 @@ def run_ours(args, rank, world, device):
         out["cpu_baseline"] = {"value": 1.0 / sec, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                                "sample": sample}
     return out
+
+
+def time_action(op, x, d, flush, n_rep=20):
+    """Mean device time of one elastic action (CUDA events on the launching stream, L2 flushed before each)."""
+    dt = x.dtype
+    op.autotune(dt)
+    y = torch.empty_like(x)
+    for _ in range(3):
+        op.mech_action(x, d=d, out=y)
+    ms = 0.0
+    for _ in range(n_rep):
+        flush_l2(flush)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        op.mech_action(x, d=d, out=y)
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    return ms / n_rep / 1e3
 
 
 def profile_traffic(fp32):
@@ -392,6 +412,10 @@ def run_kernel_only(args, device):
     d = torch.as_tensor(rng.uniform(0, 1, size=op.n_red), device=device)
     dt = torch.float32 if args.fp32 else torch.float64
     x, d = x.to(dt), d.to(dt)
+    if args.tile:
+        op.tile_shape(dt, tuple(int(v) for v in args.tile.split(",")))  # pinned: no tuning launches
+    else:
+        op.autotune(dt)
     for _ in range(args.warmup):
         op.mech_action(x, d=d)
     torch.cuda.synchronize()
@@ -404,8 +428,8 @@ def run_kernel_only(args, device):
     ms = e0.elapsed_time(e1) / args.steps
     w = 4 if args.fp32 else 8
     alg = 7 * op.n_red * w + op.n_elements
-    print(json.dumps({"kernel": "h8 elastic action", "cell": args.cell, "dtype": str(dt), "ms_per_apply": ms,
-                      "algorithmic_GBps": alg / ms / 1e6}), flush=True)
+    print(json.dumps({"kernel": "h8 elastic action (tiled)", "cell": args.cell, "dtype": str(dt),
+                      "tile": op.tile_shape(dt), "ms_per_apply": ms, "algorithmic_GBps": alg / ms / 1e6}), flush=True)
 
 
 def main():
@@ -420,6 +444,7 @@ def main():
     ap.add_argument("--kernel-only", action="store_true", help="time the elastic action alone (profiling case)")
     ap.add_argument("--cell", type=int, default=N_CELL, help="cell edge in voxels for --kernel-only")
     ap.add_argument("--fp32", action="store_true", help="FP32 storage/arithmetic for --kernel-only")
+    ap.add_argument("--tile", default="", help="pin the tile shape ox,oy,kz for --kernel-only (else autotune)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

@@ -3,8 +3,8 @@
 Mirrors ``phast.solid3d.operator.PeriodicVoxelPhaseFieldOperator`` (AT2 parts,
 src/phast/solid3d/operator.py:133-1544): the same reduced periodic numbering
 (periodic.py:61-113), the same 2x2x2 Gauss rule and Voigt order, the same
-``x = [u~ (3 n_red), E (6)]`` layout.  Each action is two launches of
-``libphastb.so`` (an element kernel and a deterministic node gather).
+``x = [u~ (3 n_red), E (6)]`` layout.  The elastic and damage actions are
+one launch each of ``libphastb.so``'s tiled z-marching kernels.
 """
 from __future__ import annotations
 
@@ -180,13 +180,18 @@ class PeriodicVoxelPhaseFieldOperator:
         call("phastb_h8_degradation", self.vgrid, self._dt(d), ptr(d), self.kappa, ptr(g), stream())
         return g
 
-    def mech_action(self, x, g=None, *, d=None, mask=None):
+    def mech_action(self, x, g=None, *, d=None, mask=None, out=None):
         """A(g) x (operator.py:1171-1194); ``d`` instead of ``g`` fuses the degradation."""
         x = self._check("x", x, (self.n_mech,))
         gq = None if g is None else self._check("g", g, (self.n_elements, 8), x.dtype)
         dd = None if d is None else self._check("d", d, (self.n_red,)).to(x.dtype)
         mk = None if mask is None else mask.to(torch.uint8).contiguous()
-        y = torch.empty_like(x)
+        if out is None:
+            y = torch.empty_like(x)
+        else:
+            y = out
+            if y.shape != x.shape or y.dtype != x.dtype or not y.is_contiguous() or y.data_ptr() == x.data_ptr():
+                raise ValueError("out must be a distinct contiguous tensor like x")
         call("phastb_h8_mech_apply", self.vgrid, self.mat, ptr(self.slot), self._dt(x), ptr(x), ptr(gq), ptr(dd),
              ptr(mk), ptr(y), self.scratch(x.dtype), stream())
         return y
