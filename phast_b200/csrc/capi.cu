@@ -5,8 +5,13 @@
 
 namespace phastb {
 static std::atomic<long long> g_launches{0};
-void note_launch(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+static thread_local long long t_launches = 0;  // this host thread's launches (graph capture counts)
+void note_launch(long long n) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+  t_launches += n;
+}
 long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+long long thread_launch_count() { return t_launches; }
 
 namespace {
 struct DevStreams {

@@ -125,6 +125,7 @@ template <typename T> __device__ __forceinline__ T ld(const T* p) { return __ldg
 // is wrapped as `{ note_launch(); kernel<<<...>>>(...); }`).
 void note_launch(long long n = 1);
 long long launch_count();
+long long thread_launch_count();
 
 // Solver entry points run on a library-owned non-blocking stream (one per device
 // and host thread), ordered after the caller's stream on entry and before it on

@@ -29,7 +29,7 @@ cudaGraphExec_t graph_for(const GraphKey& key, cudaStream_t s, const std::functi
       return t_graph_cache.front().exec;
     }
   }
-  const long long c0 = launch_count();
+  const long long c0 = thread_launch_count();
   if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
     return nullptr;
@@ -37,7 +37,7 @@ cudaGraphExec_t graph_for(const GraphKey& key, cudaStream_t s, const std::functi
   const int st = body();
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(s, &g);
-  const long long n = launch_count() - c0;
+  const long long n = thread_launch_count() - c0;
   note_launch(-n);  // captured, not executed
   if (st != PHASTB_OK || e != cudaSuccess || !g) {
     if (g) cudaGraphDestroy(g);
