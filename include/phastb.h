@@ -118,6 +118,29 @@ int phastb_q4_damage_solve(const phastb_q4_grid* g, const double* Hq, double gc_
                            double* d_out, int* info, void* workspace, size_t workspace_bytes,
                            void* stream);
 
+/* Linear AT2 damage system A x = rhs (the operator of phastb_q4_damage_solve, no bounds) with
+ * the rows in `fixed` eliminated and held at fixed_vals (0 when fixed_vals is NULL); Jacobi PCG
+ * from x0 (NULL: zero) to ||r|| <= rtol ||rhs_free||.  This is the adjoint solve of the damage
+ * step: A is symmetric, so A^T lam = g is the same system.  info[0] iterations, info[1] 0 converged,
+ * 1 max_iter, 2 breakdown, 3 non-finite; rinfo[0] ||rhs_free||, rinfo[1] final ||r||.
+ * _pcg_solve_adjoint_system, solvers/damage_solver.py:423-480 */
+size_t phastb_q4_damage_linear_workspace_bytes(int n_nodes);
+int phastb_q4_damage_linear_solve(const phastb_q4_grid* g, const double* Hq, double gc_over_l0,
+                                  const double* gc_over_l0_e, double gcl0, const double* gcl0_e,
+                                  const double* rhs, const uint8_t* fixed, const double* fixed_vals,
+                                  const double* x0, double rtol, int max_iter, int check_every,
+                                  double* x_out, int* info, double* rinfo, void* workspace,
+                                  size_t workspace_bytes, void* stream);
+
+/* Adjoint sensitivities of the AT2 damage system for an adjoint field lam (N,) and damage d (N,),
+ * per element: lam_K_d_e = lam^T K_e d, lam_M_d_e = lam^T M_e d (Gauss-point sums),
+ * grad_gc_e = -(l0 lam_K_d_e + lam_M_d_e / l0), grad_H (E,4) = 2 w lam_q (1 - d_q).  Any output may
+ * be NULL.  _adjoint_quadratic_forms_perelem and _AdjointDamageSolveField.backward,
+ * solvers/damage_solver.py:284-331, 998-1016, written for the Q4 Gauss rule */
+int phastb_q4_damage_adjoint_grads(const phastb_q4_grid* g, const double* lam, const double* d, double l0,
+                                   double* grad_gc_e, double* grad_H, double* lam_K_d_e,
+                                   double* lam_M_d_e, void* stream);
+
 /* One central-difference step, fused: predictor, f_int(u_new, d), corrector,
  * Dirichlet zeroing; optionally the history update H_out = max(H_in, psi+(u_new)).
  * m_inv (N,) = 1/(rho M + 1e-30) per node; bc_mask (N,2) uint8.

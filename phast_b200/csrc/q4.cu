@@ -148,7 +148,8 @@ __global__ void __launch_bounds__(kThreads) q4_damage_apply_kernel(Q4Tab<double>
                                                                    const double* __restrict__ Hq, double rs,
                                                                    double rsh, const double* __restrict__ rsh_e,
                                                                    double gcl0, const double* __restrict__ gcl0_e,
-                                                                   double* __restrict__ y, const int* guard) {
+                                                                   double* __restrict__ y, const int* guard,
+                                                                   const uint8_t* __restrict__ mask) {
   if (guard && *guard == 0) return;
   const int nn = (t.nx + 1) * (t.ny + 1);
   const int node = blockIdx.x * blockDim.x + threadIdx.x;
@@ -188,7 +189,56 @@ __global__ void __launch_bounds__(kThreads) q4_damage_apply_kernel(Q4Tab<double>
       lap_acc += (gcl0_e ? __ldg(gcl0_e + e) : gcl0) * lap;
       mass_acc += mass;
     }
-  y[node] = lap_acc + mass_acc;
+  y[node] = (mask && mask[node]) ? 0.0 : lap_acc + mass_acc;
+}
+
+// Adjoint sensitivities of the AT2 damage system A(Gc, l0, H) d = b(H) for an
+// adjoint field lam (one thread per element):
+//   lKd_e = lam_e^T K_e d_e,  lMd_e = lam_e^T M_e d_e   (Gauss-point sums)
+//   dL/dGc_e   = -(l0 lKd_e + lMd_e / l0)
+//   dL/dH_{e,q} = 2 w lam_q (1 - d_q)   (db/dH minus dA/dH d at Gauss point q)
+__global__ void __launch_bounds__(kThreads) q4_damage_adjoint_kernel(Q4Tab<double> t, const double* __restrict__ lam,
+                                                                     const double* __restrict__ d, double l0,
+                                                                     double* __restrict__ g_gc,
+                                                                     double* __restrict__ g_h,
+                                                                     double* __restrict__ lkd,
+                                                                     double* __restrict__ lmd) {
+  const int ne = t.nx * t.ny;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const int ei = e % t.nx, ej = e / t.nx;
+  int n[4];
+  q4_corners(ei, ej, t.nx, n);
+  double la[4], dd[4];
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    la[b] = __ldg(lam + n[b]);
+    dd[b] = __ldg(d + n[b]);
+  }
+  double kd = 0, md = 0, gh[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    double lx = 0, ly = 0, lq = 0, dx = 0, dy = 0, dq = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      lx += t.gx[q][b] * la[b];
+      ly += t.gy[q][b] * la[b];
+      lq += t.N[q][b] * la[b];
+      dx += t.gx[q][b] * dd[b];
+      dy += t.gy[q][b] * dd[b];
+      dq += t.N[q][b] * dd[b];
+    }
+    kd += t.w * (lx * dx + ly * dy);
+    md += t.w * (lq * dq);
+    gh[q] = 2.0 * t.w * lq * (1.0 - dq);
+  }
+  if (lkd) lkd[e] = kd;
+  if (lmd) lmd[e] = md;
+  if (g_gc) g_gc[e] = -(l0 * kd + md / l0);
+  if (g_h) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) g_h[4 * (size_t)e + q] = gh[q];
+  }
 }
 
 __global__ void __launch_bounds__(kThreads) q4_damage_prepare_kernel(Q4Tab<double> t, const double* __restrict__ Hq,
@@ -390,10 +440,18 @@ static int launch_force(const phastb_q4_grid* g, const phastb_q4_material* m, co
 
 int q4_damage_apply_launch(const phastb_q4_grid* g, const double* d, const double* Hq, double rs, double rsh,
                            const double* rsh_e, double gcl0, const double* gcl0_e, double* y, const int* guard,
-                           cudaStream_t s) {
+                           cudaStream_t s, const uint8_t* mask) {
   const Q4Tab<double> t = make_q4_tab<double>(*g);
   const int nn = (g->nx + 1) * (g->ny + 1);
-  { note_launch(); q4_damage_apply_kernel<<<grid_full(nn), kThreads, 0, s>>>(t, d, Hq, rs, rsh, rsh_e, gcl0, gcl0_e, y, guard); }
+  { note_launch(); q4_damage_apply_kernel<<<grid_full(nn), kThreads, 0, s>>>(t, d, Hq, rs, rsh, rsh_e, gcl0, gcl0_e, y, guard, mask); }
+  return last_launch_status();
+}
+
+int q4_damage_adjoint_launch(const phastb_q4_grid* g, const double* lam, const double* d, double l0, double* g_gc,
+                             double* g_h, double* lkd, double* lmd, cudaStream_t s) {
+  const Q4Tab<double> t = make_q4_tab<double>(*g);
+  const int ne = g->nx * g->ny;
+  { note_launch(); q4_damage_adjoint_kernel<<<grid_full(ne), kThreads, 0, s>>>(t, lam, d, l0, g_gc, g_h, lkd, lmd); }
   return last_launch_status();
 }
 
@@ -478,7 +536,7 @@ int phastb_q4_damage_apply(const phastb_q4_grid* g, const double* d, const doubl
                            void* stream) {
   if (!valid_grid(g) || !d || !Hq || !y) return PHASTB_ERR_ARG;
   return q4_damage_apply_launch(g, d, Hq, rd_scale, rd_shift, rd_shift_e, gcl0, gcl0_e, y, nullptr,
-                                (cudaStream_t)stream);
+                                (cudaStream_t)stream, nullptr);
 }
 
 int phastb_q4_damage_prepare(const phastb_q4_grid* g, const double* Hq, double gc_over_l0,

@@ -13,7 +13,9 @@ namespace phastb {
 
 int q4_damage_apply_launch(const phastb_q4_grid* g, const double* d, const double* Hq, double rs, double rsh,
                            const double* rsh_e, double gcl0, const double* gcl0_e, double* y, const int* guard,
-                           cudaStream_t s);
+                           cudaStream_t s, const uint8_t* mask);
+int q4_damage_adjoint_launch(const phastb_q4_grid* g, const double* lam, const double* d, double l0, double* g_gc,
+                             double* g_h, double* lkd, double* lmd, cudaStream_t s);
 int q4_force_launch(const phastb_q4_grid* g, const phastb_q4_material* m, const double* u, const double* d,
                     double* f, const uint8_t* mask, const int* guard, cudaStream_t s);
 
@@ -24,11 +26,25 @@ struct Q4DamageCtx {
   const double* rsh_e;
   double gcl0;
   const double* gcl0_e;
+  const uint8_t* mask;  // rows held fixed (zero output), may be null
 };
 
 static int q4_damage_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
   const Q4DamageCtx* k = static_cast<const Q4DamageCtx*>(c);
-  return q4_damage_apply_launch(&k->g, x, k->Hq, 2.0, k->rsh, k->rsh_e, k->gcl0, k->gcl0_e, y, guard, s);
+  return q4_damage_apply_launch(&k->g, x, k->Hq, 2.0, k->rsh, k->rsh_e, k->gcl0, k->gcl0_e, y, guard, s, k->mask);
+}
+
+// Dirichlet-eliminated linear system set-up: bf = rhs on free rows (0 on fixed),
+// x = vals on fixed rows (x0 or 0 elsewhere), Jacobi inverse zero on fixed rows.
+__global__ void lin_setup_kernel(int n, const double* __restrict__ rhs, const uint8_t* __restrict__ fixed,
+                                 const double* __restrict__ vals, const double* __restrict__ x0,
+                                 double* __restrict__ bf, double* __restrict__ x, double* __restrict__ minv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const bool f = fixed && fixed[i];
+    bf[i] = f ? 0.0 : rhs[i];
+    x[i] = f ? (vals ? vals[i] : 0.0) : (x0 ? x0[i] : 0.0);
+    if (f) minv[i] = 0.0;
+  }
 }
 
 struct Q4ForceCtx {
@@ -98,7 +114,7 @@ int phastb_q4_damage_solve(const phastb_q4_grid* g, const double* Hq, double gc_
   PpcgWs w = ppcg_ws(workspace, n);
   int st = phastb_q4_damage_prepare(g, Hq, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e, w.b, w.minv, (void*)s);
   if (st) return st;
-  Q4DamageCtx ctx{*g, Hq, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e};
+  Q4DamageCtx ctx{*g, Hq, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e, nullptr};
   LinOp<double> A{q4_damage_op, &ctx, sizeof(ctx)};
   int inf[2] = {0, 0};
   st = ppcg_solve(A, n, w, d_prev, d_init, fixed, fixed_vals, tol, max_iter, check_every, d_out, inf, s);
@@ -107,6 +123,61 @@ int phastb_q4_damage_solve(const phastb_q4_grid* g, const double* Hq, double gc_
     info[1] = inf[1];
   }
   return st;
+}
+
+size_t phastb_q4_damage_linear_workspace_bytes(int n_nodes) {
+  return pcg_ws_bytes<double>(n_nodes) + 2 * align_up(sizeof(double) * (size_t)n_nodes) + red_ws_bytes();
+}
+
+int phastb_q4_damage_linear_solve(const phastb_q4_grid* g, const double* Hq, double gc_over_l0,
+                                  const double* gc_over_l0_e, double gcl0, const double* gcl0_e, const double* rhs,
+                                  const uint8_t* fixed, const double* fixed_vals, const double* x0, double rtol,
+                                  int max_iter, int check_every, double* x_out, int* info, double* rinfo,
+                                  void* workspace, size_t workspace_bytes, void* stream) {
+  if (!valid_grid(g) || !Hq || !rhs || !x_out || max_iter < 1 || check_every < 1 || !(rtol >= 0)) return PHASTB_ERR_ARG;
+  const int n = (g->nx + 1) * (g->ny + 1);
+  if (!workspace || workspace_bytes < phastb_q4_damage_linear_workspace_bytes(n)) return PHASTB_ERR_WORKSPACE;
+  ScopedStream scope((cudaStream_t)stream);
+  if (scope.status()) return scope.status();
+  cudaStream_t s = scope.get();
+  char* p = static_cast<char*>(workspace);
+  PcgWs<double> w = pcg_ws<double>(p, n);
+  p += pcg_ws_bytes<double>(n);
+  const size_t vb = align_up(sizeof(double) * (size_t)n);
+  double* bf = reinterpret_cast<double*>(p);
+  double* minv = reinterpret_cast<double*>(p + vb);
+  RedWs rw = red_ws(p + 2 * vb);
+  int st;
+  if ((st = red_ws_reset(rw, s))) return st;
+  // Jacobi inverse of the full operator (the b output of prepare is not needed)
+  if ((st = phastb_q4_damage_prepare(g, Hq, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e, w.z, minv, (void*)s))) return st;
+  { note_launch(); lin_setup_kernel<<<grid_for(n), kThreads, 0, s>>>(n, rhs, fixed, fixed_vals, x0, bf, x_out, minv); }
+  if ((st = last_launch_status())) return st;
+  double bn = 0.0;
+  if ((st = vec_norm2<double>(bf, n, &bn, p + 2 * vb, s))) return st;
+  if (rinfo) rinfo[0] = bn;
+  Q4DamageCtx ctx{*g, Hq, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e, fixed};
+  LinOp<double> A{q4_damage_op, &ctx, sizeof(ctx)};
+  PcgResult pr{};
+  if (bn == 0.0) {
+    pr.converged = 1;
+  } else if ((st = pcg_run<double>(A, n, w, bf, minv, nullptr, x_out, rtol * bn, max_iter, check_every, PCG_FREEZE,
+                                   0.0, &pr, s))) {
+    return st;
+  }
+  if (info) {
+    info[0] = pr.iterations;
+    info[1] = pr.converged ? 0 : (pr.breakdown ? 2 : (pr.nonfinite ? 3 : 1));
+  }
+  if (rinfo) rinfo[1] = pr.rnorm;
+  return cuda_status(cudaStreamSynchronize(s));
+}
+
+int phastb_q4_damage_adjoint_grads(const phastb_q4_grid* g, const double* lam, const double* d, double l0,
+                                   double* grad_gc_e, double* grad_H, double* lam_K_d_e, double* lam_M_d_e,
+                                   void* stream) {
+  if (!valid_grid(g) || !lam || !d || !(l0 > 0)) return PHASTB_ERR_ARG;
+  return q4_damage_adjoint_launch(g, lam, d, l0, grad_gc_e, grad_H, lam_K_d_e, lam_M_d_e, (cudaStream_t)stream);
 }
 
 size_t phastb_q4_qs_workspace_bytes(int n_nodes) {

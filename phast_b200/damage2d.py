@@ -96,34 +96,86 @@ class PhaseFieldDamageSolver:
     # -- solve ------------------------------------------------------------------
     def solve(self, H_input, d_prev, Gc=None, l0=None, Gc_field=None, pf_dirichlet_mask=None,
               pf_dirichlet_values=None, initial_guess=None):
-        """Projected-CG AT2 solve with d in [d_prev, 1] (damage_solver.py:2493-2640, 3528-3775)."""
-        self.n_solves += 1
-        for t in (Gc, l0, Gc_field):
-            if isinstance(t, torch.Tensor) and t.requires_grad:
-                raise NotImplementedError(
-                    "Differentiable native Q4 damage solves are not implemented yet. Use forward Q4 AT2 solves "
-                    "without gradient-tracked material overrides, or convert Q4 cells to T3 for adjoint damage "
-                    "workflows.")
-        if Gc is not None and Gc_field is not None:
-            raise ValueError("Pass either Gc (scalar) or Gc_field (per-element), not both.")
+        """Projected-CG AT2 solve with d in [d_prev, 1] (damage_solver.py:2493-2640, 3528-3775).
+
+        When autograd is on and H_input, d_prev, Gc, l0 or Gc_field requires a
+        gradient, the solve is differentiated by the adjoint method on the frozen
+        active set (``_Q4DamageAdjoint``); PhAST raises NotImplementedError for
+        differentiable Q4 solves (damage_solver.py:2550-2557) and differentiates
+        its T3 path the same way (damage_solver.py:483-1154).
+        """
+        tracked = [t for t in (H_input, d_prev, Gc, l0, Gc_field) if isinstance(t, torch.Tensor) and t.requires_grad]
+        if tracked and torch.is_grad_enabled():
+            if Gc is not None and Gc_field is not None:
+                raise ValueError("Pass either Gc (scalar) or Gc_field (per-element), not both.")
+            return _Q4DamageAdjoint.apply(self, H_input, d_prev, Gc, l0, Gc_field, pf_dirichlet_mask,
+                                          pf_dirichlet_values, initial_guess)
+        return self._solve_forward(H_input, d_prev, Gc, l0, Gc_field, pf_dirichlet_mask, pf_dirichlet_values,
+                                   initial_guess)
+
+    def _material(self, Gc=None, l0=None, Gc_field=None):
+        """(Gc l0, Gc / l0) scalars and per-element fields for the overrides."""
         Gc_s = self._Gc if Gc is None else float(Gc)
         l0_s = self._l0 if l0 is None else float(l0)
-        gcl0, gco = Gc_s * l0_s, Gc_s / l0_s
         gcl0_e = gco_e = None
         if Gc_field is not None:
-            gf = torch.as_tensor(Gc_field, dtype=torch.float64, device=self.fem.device).reshape(-1)
+            gf = torch.as_tensor(Gc_field, dtype=torch.float64, device=self.fem.device).detach().reshape(-1)
             if gf.numel() != self.fem.n_elems:
                 raise ValueError("Gc_field must have one value per element")
             gcl0_e = (gf * l0_s).contiguous()
             gco_e = (gf / l0_s).contiguous()
+        return Gc_s, l0_s, Gc_s * l0_s, Gc_s / l0_s, gcl0_e, gco_e
+
+    def _apply_full(self, H_input, x, Gc=None, l0=None, Gc_field=None):
+        """A x of the AT2 system (unmasked) with the given material overrides."""
+        _, _, gcl0, gco, gcl0_e, gco_e = self._material(Gc, l0, Gc_field)
+        Hq = self._normalize_q4_H(H_input.detach())
+        xx = x.detach().to(torch.float64).contiguous()
+        y = torch.empty_like(xx)
+        call("phastb_q4_damage_apply", self.fem.grid, ptr(xx), ptr(Hq), 2.0, gco, ptr(gco_e), gcl0, ptr(gcl0_e),
+             ptr(y), stream())
+        return y
+
+    def linear_solve(self, H_input, rhs, Gc=None, l0=None, Gc_field=None, fixed=None, fixed_values=None, x0=None,
+                     rtol=1e-11, max_iter=None):
+        """Solve the unbounded AT2 system A x = rhs with ``fixed`` rows held at ``fixed_values``.
+
+        The adjoint system of the damage step (A is symmetric); mirrors
+        _pcg_solve_adjoint_system (damage_solver.py:423-480).
+        """
+        _, _, gcl0, gco, gcl0_e, gco_e = self._material(Gc, l0, Gc_field)
+        Hq = self._normalize_q4_H(H_input.detach())
+        n = self.fem.n_nodes
+        r = rhs.detach().to(torch.float64).contiguous()
+        fx = None if fixed is None else fixed.to(torch.uint8).contiguous()
+        fv = None if fixed_values is None else fixed_values.detach().to(torch.float64).contiguous()
+        xi = None if x0 is None else x0.detach().to(torch.float64).contiguous()
+        out = torch.empty(n, dtype=torch.float64, device=r.device)
+        info = (C.c_int * 2)()
+        rinfo = (C.c_double * 2)()
+        wp, wn = self._ws.get(_lib.load().phastb_q4_damage_linear_workspace_bytes(n))
+        call("phastb_q4_damage_linear_solve", self.fem.grid, ptr(Hq), gco, ptr(gco_e), gcl0, ptr(gcl0_e), ptr(r),
+             ptr(fx), ptr(fv), ptr(xi), float(rtol), int(max_iter or max(self.max_iter, 1000)), self.check_every,
+             ptr(out), info, rinfo, wp, wn, stream())
+        self.last_linear_info = (int(info[0]), int(info[1]), float(rinfo[0]), float(rinfo[1]))
+        if info[1] not in (0, 1):
+            raise RuntimeError(f"adjoint damage PCG failed (reason {int(info[1])})")
+        return out
+
+    def _solve_forward(self, H_input, d_prev, Gc=None, l0=None, Gc_field=None, pf_dirichlet_mask=None,
+                       pf_dirichlet_values=None, initial_guess=None):
+        self.n_solves += 1
+        if Gc is not None and Gc_field is not None:
+            raise ValueError("Pass either Gc (scalar) or Gc_field (per-element), not both.")
+        _, _, gcl0, gco, gcl0_e, gco_e = self._material(Gc, l0, Gc_field)
         orig_dtype = d_prev.dtype
         if not torch.isfinite(d_prev).all():
             self.last_iter = 0
             self.last_converged = False
             return d_prev.clone()
-        Hq = self._normalize_q4_H(H_input)
-        dp = d_prev.to(torch.float64).contiguous()
-        di = None if initial_guess is None else initial_guess.to(torch.float64).contiguous()
+        Hq = self._normalize_q4_H(H_input.detach())
+        dp = d_prev.detach().to(torch.float64).contiguous()
+        di = None if initial_guess is None else initial_guess.detach().to(torch.float64).contiguous()
         fixed = vals = None
         if pf_dirichlet_mask is not None:
             m = pf_dirichlet_mask.to(device=dp.device, dtype=torch.bool)
@@ -146,3 +198,88 @@ class PhaseFieldDamageSolver:
         if info[1] == 3:
             print(f"  [PhaseFieldDamageSolver diverged at iter {self.last_iter}]", flush=True)
         return out.to(orig_dtype)
+
+
+def classify_active_set(d_new, d_prev, fixed=None, upper_bound=1.0, atol=1e-12):
+    """(lower, upper, fixed, interior) masks after projection onto [d_prev, 1].
+
+    classify_damage_active_set, damage_solver.py:70-106: the upper bound and
+    pinned nodes take precedence over the lower (irreversibility) bound.
+    """
+    upper = d_new >= (upper_bound - atol)
+    fx = torch.zeros_like(upper) if fixed is None else fixed.to(device=d_new.device, dtype=torch.bool)
+    lower = (d_new <= d_prev + atol) & ~upper & ~fx
+    upper = upper & ~fx
+    interior = ~(lower | upper | fx)
+    return lower, upper, fx, interior
+
+
+class _Q4DamageAdjoint(torch.autograd.Function):
+    """Implicit differentiation of the bound-projected AT2 solve on its frozen active set.
+
+    Forward: the device PPCG solve.  Backward: with the active set (bound-active
+    and pinned nodes) frozen, the solution satisfies A_FF d_F = b_F - A_FA d_A,
+    so for an upstream gradient g the adjoint lam solves A_FF lam_F = g_F
+    (lam_A = 0) -- one Jacobi PCG on the device -- and
+
+        dL/dGc_e     = -(l0 lam^T K_e d + lam^T M_e d / l0)
+        dL/dl0       = -sum_e (Gc_e lam^T K_e d - Gc_e / l0^2 lam^T M_e d)
+        dL/dH_{e,q}  = 2 w lam_q (1 - d_q)
+        dL/dd_prev   = g_i - (A lam)_i on the nodes i held at their lower bound
+
+    (the AT2 formulas of _AdjointDamageSolveScalar/_AdjointDamageSolveField,
+    damage_solver.py:483-1037, with the Q4 Gauss rule; where PhAST passes g
+    through to d_prev unchanged, the coupling of a held node to its free
+    neighbours, -(A lam)_i, is kept here, which is the exact derivative).
+    """
+
+    @staticmethod
+    def forward(ctx, solver, H_input, d_prev, Gc, l0, Gc_field, mask, values, initial_guess):
+        d = solver._solve_forward(H_input, d_prev, Gc, l0, Gc_field, mask, values, initial_guess)
+        ctx.solver = solver
+        ctx.h_shape = tuple(H_input.shape)
+        ctx.gc_scalar = isinstance(Gc, torch.Tensor)
+        ctx.l0_tensor = isinstance(l0, torch.Tensor)
+        ctx.has_field = Gc_field is not None
+        ctx.Gc = None if Gc is None else float(Gc)
+        ctx.l0 = None if l0 is None else float(l0)
+        m = None if mask is None else mask.to(device=d.device, dtype=torch.bool)
+        gf = None if Gc_field is None else torch.as_tensor(Gc_field, device=d.device).detach().to(torch.float64)
+        ctx.save_for_backward(H_input.detach(), d_prev.detach(), d.detach(),
+                              m if m is not None else torch.empty(0, dtype=torch.bool, device=d.device),
+                              gf if gf is not None else torch.empty(0, dtype=torch.float64, device=d.device))
+        return d
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        solver = ctx.solver
+        H, d_prev, d, m, gf = ctx.saved_tensors
+        mask = m if m.numel() else None
+        gfield = gf if gf.numel() else None
+        Gc_s, l0_s, *_ = solver._material(ctx.Gc, ctx.l0, gfield)
+        g = grad_out.detach().to(torch.float64)
+        lower, upper, fx, interior = classify_active_set(d.to(torch.float64), d_prev.to(torch.float64), mask)
+        frozen = ~interior
+        lam = solver.linear_solve(H, g * interior, Gc=ctx.Gc, l0=ctx.l0, Gc_field=gfield, fixed=frozen,
+                                  fixed_values=None, rtol=1e-11)
+        E = solver.fem.n_elems
+        dev = d.device
+        g_gc = torch.empty(E, dtype=torch.float64, device=dev)
+        g_h = torch.empty(E, 4, dtype=torch.float64, device=dev)
+        lkd = torch.empty(E, dtype=torch.float64, device=dev)
+        lmd = torch.empty(E, dtype=torch.float64, device=dev)
+        dd = d.to(torch.float64).contiguous()
+        call("phastb_q4_damage_adjoint_grads", solver.fem.grid, ptr(lam), ptr(dd), l0_s, ptr(g_gc), ptr(g_h), ptr(lkd),
+             ptr(lmd), stream())
+        grad_H = g_h if ctx.h_shape == (E, 4) else g_h.sum(1)
+        grad_H = grad_H.to(H.dtype).reshape(ctx.h_shape)
+        grad_dprev = torch.zeros_like(g)
+        if bool(lower.any()):
+            Alam = solver._apply_full(H, lam, ctx.Gc, ctx.l0, gfield)
+            grad_dprev = (g - Alam) * lower
+        grad_dprev = grad_dprev.to(d_prev.dtype)
+        gc_e = gfield if gfield is not None else torch.full((E,), Gc_s, dtype=torch.float64, device=dev)
+        grad_l0 = -(gc_e * lkd).sum() + (gc_e / l0_s ** 2 * lmd).sum()
+        grad_Gc = g_gc.sum() if ctx.gc_scalar else None
+        grad_field = g_gc if ctx.has_field else None
+        return (None, grad_H, grad_dprev, grad_Gc, grad_l0 if ctx.l0_tensor else None, grad_field, None, None, None)
