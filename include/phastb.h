@@ -151,6 +151,20 @@ int phastb_q4_explicit_step(const phastb_q4_grid* g, const phastb_q4_material* m
                             const void* bc_vals, void* u_out, void* v_out, void* a_out,
                             const void* H_in, void* H_out, void* stream);
 
+/* Reverse of one phastb_q4_explicit_step (FP64, stress splits linear in u at fixed d:
+ * isotropic or linear; others return PHASTB_UNSUPPORTED).  Given the adjoints ub, vb, ab of the
+ * step's outputs (u', v', a'), writes the adjoints of its inputs (u, v, a) to ub_out, vb_out,
+ * ab_out, adds the f_ext adjoint to fb_acc and, when db_acc is given, the adjoint of d to db_acc
+ * (u_new = the step's u').  The history update of the forward step is not differentiated.
+ * scratch: 4 N doubles.  No reference counterpart for Q4; the reference differentiates its explicit
+ * loop through torch autograd with chunked recomputation (ChunkedExplicitDynamicsAutograd,
+ * solvers/mechanics_solver.py:4057-4137). */
+int phastb_q4_explicit_adjoint_step(const phastb_q4_grid* g, const phastb_q4_material* m, double dt,
+                                    const double* m_inv, const double* d, const uint8_t* bc_mask,
+                                    const double* u_new, const double* ub, const double* vb,
+                                    const double* ab, double* ub_out, double* vb_out, double* ab_out,
+                                    double* fb_acc, double* db_acc, double* scratch, void* stream);
+
 /* Energy sums (FP64): out[0] elastic, out[1] fracture surface term d^T M d,
  * out[2] gradient term d^T K d, out[3] kinetic sum_i |v_i|^2 M_i (v may be NULL).
  * compute_energy_components, fem_operators.py:1430-1496 (caller scales by Gc etc.) */

@@ -74,6 +74,8 @@ SIGNATURES = {
     "phastb_q4_damage_linear_solve": (C.c_int, [Q4G, vp, C.c_double, vp, C.c_double, vp, vp, vp, vp, vp, C.c_double,
                                                 C.c_int, C.c_int, vp, ip, dp, vp, sz, vp]),
     "phastb_q4_damage_adjoint_grads": (C.c_int, [Q4G, vp, vp, C.c_double, vp, vp, vp, vp, vp]),
+    "phastb_q4_explicit_adjoint_step": (C.c_int, [Q4G, Q4M, C.c_double, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                                  vp, vp, vp]),
     "phastb_q4_explicit_step": (C.c_int, [Q4G, Q4M, C.c_int, C.c_double, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                           vp, vp, vp, vp]),
     "phastb_q4_energy_sums": (C.c_int, [Q4G, Q4M, vp, vp, vp, dp, vp, sz, vp]),

@@ -357,6 +357,92 @@ __global__ void __launch_bounds__(kThreads) q4_explicit_kernel(
   reinterpret_cast<typename Vec2<T>::type*>(ao)[node] = o;
 }
 
+// ---- reverse central-difference step (FP64), for splits whose stress is linear
+// in u at fixed d (isotropic, linear).  The forward step on free dofs F is
+//   u' = u + dt v + dt^2/2 a,  a' = Minv (f_ext - K(d) u'),  v' = v + dt/2 (a + a'),
+// and u' = bc, a' = v' = 0 on the Dirichlet dofs.  With output adjoints
+// (ub', vb', ab'):  s = F Minv (ab' + dt/2 vb');  t = ub' - K(d) s;
+//   ub = F t,  vb = F (vb' + dt t),  ab = F (dt/2 vb' + dt^2/2 t),  f_ext_b += s,
+//   d_b += -sum_q w g'(d_q) N_q eps(s)_q . C eps(u')_q.
+__global__ void __launch_bounds__(kThreads) q4_adj_s_kernel(int n2, double dt, const double* __restrict__ minv,
+                                                            const uint8_t* __restrict__ bcm,
+                                                            const double* __restrict__ vb,
+                                                            const double* __restrict__ ab, double* __restrict__ sv,
+                                                            double* __restrict__ fb) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
+    const double v = bcm[i] ? 0.0 : minv[i >> 1] * (ab[i] + 0.5 * dt * vb[i]);
+    sv[i] = v;
+    if (fb) fb[i] += v;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) q4_adj_combine_kernel(int n2, double dt, const uint8_t* __restrict__ bcm,
+                                                                  const double* __restrict__ ub,
+                                                                  const double* __restrict__ vb,
+                                                                  const double* __restrict__ Ks,
+                                                                  double* __restrict__ ub_out,
+                                                                  double* __restrict__ vb_out,
+                                                                  double* __restrict__ ab_out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
+    const bool f = bcm[i] != 0;
+    const double t = ub[i] - Ks[i], vbi = vb[i];
+    ub_out[i] = f ? 0.0 : t;
+    vb_out[i] = f ? 0.0 : vbi + dt * t;
+    ab_out[i] = f ? 0.0 : 0.5 * dt * vbi + 0.5 * dt * dt * t;
+  }
+}
+
+// d_b[node] += -sum over its elements and Gauss points of w g'(d_q) N_q[node] eps(s):C eps(u')
+__global__ void __launch_bounds__(kThreads) q4_adj_dgrad_kernel(Q4Tab<double> t, Mat2<double> m,
+                                                                const double* __restrict__ un,
+                                                                const double* __restrict__ sv,
+                                                                const double* __restrict__ d,
+                                                                double* __restrict__ db) {
+  const int nn = (t.nx + 1) * (t.ny + 1);
+  const int node = blockIdx.x * blockDim.x + threadIdx.x;
+  if (node >= nn) return;
+  const int i = node % (t.nx + 1), j = node / (t.nx + 1);
+  double acc = 0.0;
+#pragma unroll
+  for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+    for (int di = 0; di < 2; ++di) {
+      const int ei = i - 1 + di, ej = j - 1 + dj;
+      if (ei < 0 || ei >= t.nx || ej < 0 || ej >= t.ny) continue;
+      const int al = q4_local(1 - di, 1 - dj);
+      int n[4];
+      q4_corners(ei, ej, t.nx, n);
+      double ux[4], uy[4], sx[4], sy[4], dd[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        ux[b] = un[2 * n[b]];
+        uy[b] = un[2 * n[b] + 1];
+        sx[b] = sv[2 * n[b]];
+        sy[b] = sv[2 * n[b] + 1];
+        dd[b] = d[n[b]];
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double exx = 0, eyy = 0, gxy = 0, fxx = 0, fyy = 0, fxy = 0, dq = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          exx += t.gx[q][b] * ux[b];
+          eyy += t.gy[q][b] * uy[b];
+          gxy += t.gy[q][b] * ux[b] + t.gx[q][b] * uy[b];
+          fxx += t.gx[q][b] * sx[b];
+          fyy += t.gy[q][b] * sy[b];
+          fxy += t.gy[q][b] * sx[b] + t.gx[q][b] * sy[b];
+          dq += t.N[q][b] * dd[b];
+        }
+        double sxx, syy, sxy;
+        stress2(m, PHASTB_SPLIT_LINEAR, exx, eyy, gxy, 1.0, sxx, syy, sxy);
+        const double gp = -2.0 * (1.0 - dq) * (1.0 - m.eta);  // dg/dd
+        acc -= t.w * gp * t.N[q][al] * (fxx * sxx + fyy * syy + fxy * sxy);
+      }
+    }
+  db[node] += acc;
+}
+
 // Energy sums: elastic sum_q (g psi+ + psi-) w, d^T M d, d^T K d, sum |v|^2 M.
 __global__ void __launch_bounds__(kThreads) q4_energy_kernel(Q4Tab<double> t, Mat2<double> m,
                                                              const double* __restrict__ u,
@@ -571,6 +657,35 @@ int phastb_q4_explicit_step(const phastb_q4_grid* g, const phastb_q4_material* m
         (float*)u_out, (float*)v_out, (float*)a_out, (const float*)H_in, (float*)H_out); }
   else
     return PHASTB_ERR_ARG;
+  return last_launch_status();
+}
+
+int phastb_q4_explicit_adjoint_step(const phastb_q4_grid* g, const phastb_q4_material* m, double dt,
+                                    const double* m_inv, const double* d, const uint8_t* bc_mask,
+                                    const double* u_new, const double* ub, const double* vb, const double* ab,
+                                    double* ub_out, double* vb_out, double* ab_out, double* fb_acc, double* db_acc,
+                                    double* scratch, void* stream) {
+  if (!valid_grid(g) || !m || !m_inv || !d || !bc_mask || !ub || !vb || !ab || !ub_out || !vb_out || !ab_out ||
+      !scratch)
+    return PHASTB_ERR_ARG;
+  if (m->stress_split != PHASTB_SPLIT_ISOTROPIC && m->stress_split != PHASTB_SPLIT_LINEAR)
+    return PHASTB_UNSUPPORTED;  // the step is then nonlinear in u: its adjoint needs the split's tangent
+  if (db_acc && !u_new) return PHASTB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nn = (g->nx + 1) * (g->ny + 1), n2 = 2 * nn;
+  double* sv = scratch;
+  double* Ks = scratch + n2;
+  { note_launch(); q4_adj_s_kernel<<<grid_for(n2), kThreads, 0, s>>>(n2, dt, m_inv, bc_mask, vb, ab, sv, fb_acc); }
+  int st = last_launch_status();
+  if (st) return st;
+  if ((st = q4_force_launch(g, m, sv, d, Ks, nullptr, nullptr, s))) return st;
+  { note_launch(); q4_adj_combine_kernel<<<grid_for(n2), kThreads, 0, s>>>(n2, dt, bc_mask, ub, vb, Ks, ub_out, vb_out, ab_out); }
+  if ((st = last_launch_status())) return st;
+  if (db_acc && m->stress_split == PHASTB_SPLIT_ISOTROPIC) {
+    note_launch();
+    q4_adj_dgrad_kernel<<<grid_full(nn), kThreads, 0, s>>>(make_q4_tab<double>(*g), make_mat2<double>(*m), u_new, sv,
+                                                             d, db_acc);
+  }
   return last_launch_status();
 }
 

@@ -64,6 +64,41 @@ class ExplicitDynamics:
         u_new = u + self.dt * v + 0.5 * self.dt * self.dt * a
         return torch.where(bc_mask, bc_vals, u_new)
 
+    def rollout(self, u, v, a, d, f_ext, bc_mask, bc_vals, n_steps, checkpoint_every=10):
+        """``n_steps`` central-difference steps at fixed damage; returns the final (u, v, a).
+
+        Differentiable (FP64) with respect to u, v, a, f_ext and d when any of
+        them requires a gradient: the backward pass runs the hand-written reverse
+        step (phastb_q4_explicit_adjoint_step) and recomputes each segment of
+        ``checkpoint_every`` steps from its stored start state, so memory grows
+        with n_steps / checkpoint_every, not with n_steps (the chunked
+        recomputation of ChunkedExplicitDynamicsAutograd, mechanics_solver.py:4057-4137).
+        """
+        n_steps, k = int(n_steps), int(checkpoint_every)
+        if n_steps < 0 or k < 1:
+            raise ValueError("n_steps must be >= 0 and checkpoint_every >= 1")
+        tracked = any(isinstance(t, torch.Tensor) and t.requires_grad for t in (u, v, a, f_ext, d))
+        if tracked and torch.is_grad_enabled():
+            return _ExplicitRollout.apply(self, u, v, a, d, f_ext, bc_mask, bc_vals, n_steps, k)
+        with torch.no_grad():
+            return self._run(u.detach(), v.detach(), a.detach(), d.detach(), f_ext.detach(), bc_mask, bc_vals,
+                             n_steps)[0]
+
+    def _run(self, u, v, a, d, f_ext, bc_mask, bc_vals, n_steps, keep_every=0):
+        """Forward steps; with keep_every > 0 also the start states of the segments."""
+        u, v, a = u.contiguous().clone(), v.contiguous().clone(), a.contiguous().clone()
+        un, vn, an = torch.empty_like(u), torch.empty_like(v), torch.empty_like(a)
+        dd, ff = d.contiguous(), f_ext.contiguous()
+        kept = []
+        for s in range(n_steps):
+            if keep_every and s % keep_every == 0:
+                kept.append((u.clone(), v.clone(), a.clone()))
+            self.step_into(u, v, a, dd, ff, bc_mask, bc_vals, un, vn, an)
+            u, un = un, u
+            v, vn = vn, v
+            a, an = an, a
+        return (u, v, a), kept
+
 
 class QuasiStaticSolver:
     """Newton-Raphson with matrix-free CG (mechanics_solver.py:816-2043), isotropic split."""
@@ -119,3 +154,56 @@ class QuasiStaticSolver:
         self.last_cg_iters = int(info[2])
         converged = bool(info[1])
         return u.to(d.dtype if d.dtype.is_floating_point else torch.float64), converged, int(info[0])
+
+
+class _ExplicitRollout(torch.autograd.Function):
+    """Reverse-mode differentiation of n explicit steps with checkpoint-and-recompute."""
+
+    @staticmethod
+    def forward(ctx, dyn, u, v, a, d, f_ext, bc_mask, bc_vals, n_steps, k):
+        if u.dtype != torch.float64:
+            raise NotImplementedError("the differentiable explicit rollout runs in FP64")
+        with torch.no_grad():
+            (uN, vN, aN), kept = dyn._run(u.detach(), v.detach(), a.detach(), d.detach().to(u.dtype),
+                                           f_ext.detach().to(u.dtype), bc_mask, bc_vals, n_steps, keep_every=k)
+        ctx.dyn, ctx.n, ctx.k, ctx.kept = dyn, n_steps, k, kept
+        ctx.save_for_backward(d.detach().to(u.dtype).contiguous(), f_ext.detach().to(u.dtype).contiguous(),
+                              bc_mask, bc_vals)
+        ctx.d_dtype, ctx.f_dtype = d.dtype, f_ext.dtype
+        return uN, vN, aN
+
+    @staticmethod
+    def backward(ctx, gu, gv, ga):
+        dyn, n, k = ctx.dyn, ctx.n, ctx.k
+        d, f_ext, bc_mask, bc_vals = ctx.saved_tensors
+        fem = dyn.fem
+        mask = (bc_mask if bc_mask.dtype == torch.uint8 else bc_mask.to(torch.uint8)).contiguous()
+        z = lambda t: torch.zeros_like(f_ext) if t is None else t.detach().contiguous().to(torch.float64)
+        ub, vb, ab = z(gu), z(gv), z(ga)
+        fb = torch.zeros_like(f_ext)
+        db = torch.zeros(fem.n_nodes, dtype=torch.float64, device=f_ext.device)
+        nb = [torch.empty_like(ub) for _ in range(3)]
+        scratch = torch.empty(4 * fem.n_nodes, dtype=torch.float64, device=f_ext.device)
+        mat = fem.mat(torch.float64)
+        minv = dyn._m_inv(torch.float64)
+        n_seg = len(ctx.kept)
+        for seg in range(n_seg - 1, -1, -1):
+            s0, s1 = seg * k, min((seg + 1) * k, n)
+            # recompute the segment's states u_{s0+1} .. u_{s1} (the u' of each step)
+            u, v, a = (t.clone() for t in ctx.kept[seg])
+            outs = []
+            with torch.no_grad():
+                for _ in range(s1 - s0):
+                    un, vn, an = torch.empty_like(u), torch.empty_like(v), torch.empty_like(a)
+                    dyn.step_into(u, v, a, d, f_ext, bc_mask, bc_vals, un, vn, an)
+                    outs.append(un)
+                    u, v, a = un, vn, an
+            for j in range(s1 - s0 - 1, -1, -1):
+                call("phastb_q4_explicit_adjoint_step", fem.grid, mat, float(dyn.dt), ptr(minv), ptr(d), ptr(mask),
+                     ptr(outs[j]), ptr(ub), ptr(vb), ptr(ab), ptr(nb[0]), ptr(nb[1]), ptr(nb[2]), ptr(fb), ptr(db),
+                     ptr(scratch), stream())
+                ub, nb[0] = nb[0], ub
+                vb, nb[1] = nb[1], vb
+                ab, nb[2] = nb[2], ab
+        ctx.kept = None
+        return (None, ub, vb, ab, db.to(ctx.d_dtype), fb.to(ctx.f_dtype), None, None, None, None)

@@ -106,3 +106,59 @@ def test_linear_solve_is_the_adjoint_system():
         solver._Gc_l0_e = solver._Gc_over_l0_e = None
     r[fixed] = 0.0
     assert float(torch.linalg.vector_norm(r)) <= 1e-10 * float(torch.linalg.vector_norm(w))
+
+
+def explicit_setup(seed=3, nx=10, ny=8):
+    import phast_b200 as pb
+    sm = pb.structured_q4_mesh(1.0, 0.8, nx, ny)
+    mesh = pb.FEMMesh.from_tensors(sm.nodes, sm.quads, element_type="Q4", device="cuda")
+    mat = pb.Material(E=32000.0, nu=0.2, Gc=3e-3, l0=0.1, eta_residual=1e-8, energy_split="isotropic", rho=2.45e-9)
+    fem = pb.FEMOperators(mesh, mat)
+    dyn = pb.ExplicitDynamics(fem, dt_safety=0.5)
+    rng = np.random.default_rng(seed)
+    N = fem.n_nodes
+    t = lambda x: torch.as_tensor(x, device="cuda")
+    u0 = t(rng.normal(size=(N, 2)) * 1e-4)
+    v0 = t(rng.normal(size=(N, 2)) * 1e-2)
+    a0 = torch.zeros(N, 2, dtype=torch.float64, device="cuda")
+    d = t(rng.uniform(0.0, 0.6, N))
+    f = t(rng.normal(size=(N, 2)) * 1e-3)
+    bc = torch.zeros(N, 2, dtype=torch.bool, device="cuda")
+    bc[: nx + 1] = True  # bottom row clamped
+    bcv = torch.zeros(N, 2, dtype=torch.float64, device="cuda")
+    wu, wv = t(rng.normal(size=(N, 2))), t(rng.normal(size=(N, 2)))
+    return dyn, u0, v0, a0, d, f, bc, bcv, wu, wv, rng
+
+
+def test_explicit_rollout_adjoint_matches_central_differences():
+    dyn, u0, v0, a0, d, f, bc, bcv, wu, wv, rng = explicit_setup()
+    n = 25
+
+    def objective(u0_, v0_, d_, f_, k=10):
+        u, v, _ = dyn.rollout(u0_, v0_, a0, d_, f_, bc, bcv, n, checkpoint_every=k)
+        return (wu * u).sum() * 1e4 + (wv * v).sum()
+
+    grads = {}
+    for k in (10, 1, 25):
+        leaves = [x.clone().requires_grad_(True) for x in (u0, v0, d, f)]
+        objective(*leaves, k=k).backward()
+        grads[k] = [x.grad.clone() for x in leaves]
+    for k in (1, 25):  # the checkpoint interval changes the schedule, not the gradient
+        for g10, gk in zip(grads[10], grads[k]):
+            assert float((g10 - gk).abs().max()) <= 1e-12 * float(g10.abs().max()) + 1e-300
+    gu, gv, gd, gf = grads[10]
+    with torch.no_grad():
+        def fd(which, idx, eps):
+            args_p = [u0.clone(), v0.clone(), d.clone(), f.clone()]
+            args_m = [u0.clone(), v0.clone(), d.clone(), f.clone()]
+            args_p[which][idx] += eps
+            args_m[which][idx] -= eps
+            return float(objective(*args_p) - objective(*args_m)) / (2 * eps)
+        free = torch.nonzero(~bc[:, 0]).flatten().tolist()
+        for node in rng.choice(free, 4, replace=False):
+            for c in (0, 1):
+                assert rel_close(float(gf[node, c]), fd(3, (node, c), 1e-6), FD_TOL)
+                assert rel_close(float(gu[node, c]), fd(0, (node, c), 1e-8), FD_TOL)
+                assert rel_close(float(gv[node, c]), fd(1, (node, c), 1e-6), FD_TOL)
+        for node in rng.choice(free, 5, replace=False):
+            assert rel_close(float(gd[node]), fd(2, (int(node),), 1e-5), FD_TOL), (node, float(gd[node]))
