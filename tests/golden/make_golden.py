@@ -367,6 +367,63 @@ def h8_staggered_case():
     np.savez_compressed(os.path.join(HERE, "h8_staggered.npz"), **out)
 
 
+# ---------------------------------------------------------------------------
+# 2D T3 (unstructured triangles: a perturbed q4_to_triangles twin)
+# ---------------------------------------------------------------------------
+
+def t3_cases():
+    import torch
+    from phast.core.mesh import FEMMesh
+    from phast.core.quad_elements import q4_to_triangles, structured_q4_mesh
+    from phast.core.fem_operators import FEMOperators
+    from phast.physics.material import Material
+    from phast.solvers.damage_solver import PhaseFieldDamageSolver
+
+    rng = np.random.default_rng(4321)
+    sm = structured_q4_mesh(1.0, 0.8, 9, 7)
+    nodes = n(sm.nodes).copy()
+    # jitter interior nodes so the element geometry varies (an unstructured mesh)
+    inner = (nodes[:, 0] > 1e-9) & (nodes[:, 0] < 1.0 - 1e-9) & (nodes[:, 1] > 1e-9) & (nodes[:, 1] < 0.8 - 1e-9)
+    nodes[inner] += rng.uniform(-0.02, 0.02, size=(int(inner.sum()), 2))
+    tri = q4_to_triangles(sm.quads)
+    mesh = FEMMesh.from_tensors(t(nodes), tri, element_type="T3")
+    N, E = mesh.n_nodes, mesh.n_elems
+    u = rng.normal(size=(N, 2)) * 1e-3
+    d = rng.uniform(0, 1, size=N)
+    out = {"nodes": nodes, "tris": n(tri), "u": u, "d": d}
+    for split in ("isotropic", "amor", "spectral", "star_convex", "spectral_stress"):
+        for ps in (False, True):
+            if ps and split in ("spectral", "spectral_stress"):
+                continue
+            mat = Material(E=210000.0, nu=0.3, Gc=2.7, l0=0.05, eta_residual=1e-8, energy_split=split,
+                           plane_stress=ps, rho=2.45e-9)
+            fem = FEMOperators(mesh, mat)
+            key = f"{split}_{'ps' if ps else 'pe'}"
+            out[f"f_{key}"] = n(fem.internal_force(t(u), t(d)))
+            out[f"psi_{key}"] = n(fem.compute_psi_plus(t(u)))
+    mat = Material(E=210000.0, nu=0.3, Gc=2.7, l0=0.05, eta_residual=1e-8, energy_split="isotropic", rho=2.45e-9)
+    fem = FEMOperators(mesh, mat)
+    exx, eyy, gxy = fem.compute_strain(t(u))
+    out.update(exx=n(exx), eyy=n(eyy), gxy=n(gxy), areas=n(mesh.areas), grad_phi=n(mesh.grad_phi))
+    out["f_linear"] = n(fem.internal_force_linear(t(u)))
+    out["M_scalar"] = n(mesh.M_scalar)
+    # damage system (element H) and the projected solve
+    H = rng.uniform(0, 400.0, size=E)
+    d_prev = np.clip(rng.uniform(-0.3, 0.5, size=N), 0, 1)
+    out.update(H=H, d_prev=d_prev)
+    ds = PhaseFieldDamageSolver(fem, tol=1e-10, max_iter=3000, use_multigrid=False, bounds_method="projected_cg")
+    prep = ds._prepare_cg(t(H), t(d_prev))
+    x = rng.uniform(0, 1, size=N)
+    out["x"] = x
+    out["rc"] = n(prep[2])
+    out["Ax"] = n(ds._Ax(t(x), prep[2]))
+    out["b"] = n(prep[3])
+    out["M_inv"] = n(prep[4])
+    out["d_solve"] = n(ds.solve(t(H), t(d_prev)))
+    out["iters_solve"] = np.array([ds.last_iter])
+    np.savez_compressed(os.path.join(HERE, "t3_ops.npz"), **out)
+
+
 if __name__ == "__main__":
     _import_reference(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
     import torch
@@ -377,4 +434,5 @@ if __name__ == "__main__":
     q4_staggered_case()
     h8_cases()
     h8_staggered_case()
+    t3_cases()
     print("golden fixtures written to", HERE)

@@ -169,3 +169,31 @@ def test_h8_staggered_increments():
         assert rel(x, g["x"][k]) < 1e-7
         assert rel(d, g["d"][k]) < 1e-7 if np.linalg.norm(g["d"][k]) > 0 else np.allclose(d, 0, atol=1e-12)
         assert rel(sig, g["sigma"][k]) < 1e-7
+
+
+def test_t3_operators_damage_and_solve():
+    """Unstructured T3 oracle against the reference's triangle path (perturbed q4_to_triangles twin)."""
+    from oracle import solvers2d, t3
+    from oracle.q4 import Mat2D
+    g = golden("t3_ops")
+    geo = t3.geometry(g["nodes"], g["tris"])
+    assert rel(geo.grad, g["grad_phi"]) < 1e-14 and rel(geo.areas, g["areas"]) < 1e-14
+    assert rel(geo.M_scalar, g["M_scalar"]) < 1e-14
+    for split in ("isotropic", "amor", "spectral", "star_convex", "spectral_stress"):
+        for ps in (False, True):
+            if ps and split.startswith("spectral"):
+                continue
+            mat = Mat2D(E=210000.0, nu=0.3, Gc=2.7, l0=0.05, eta=1e-8, plane_stress=ps, split=split)
+            k = f"{split}_{'ps' if ps else 'pe'}"
+            assert rel(t3.internal_force(geo, mat, g["u"], g["d"]), g["f_" + k]) < 1e-13
+            assert rel(t3.psi(geo, mat, g["u"]), g["psi_" + k]) < 1e-13
+    rc, b, mi = t3.damage_prepare(geo, g["H"], 2.7 / 0.05, 2.7 * 0.05)
+    assert rel(rc, g["rc"]) < 1e-14 and rel(b, g["b"]) < 1e-14 and rel(mi, g["M_inv"]) < 1e-14
+    assert rel(t3.damage_apply(geo, g["x"], rc, 2.7 * 0.05), g["Ax"]) < 1e-14
+    d, it = solvers2d.projected_cg(lambda x: t3.damage_apply(geo, x, rc, 2.7 * 0.05), b, mi, g["d_prev"],
+                                   g["d_prev"], 1e-10, 3000)
+    assert rel(d, g["d_solve"]) < 1e-12 and it == int(g["iters_solve"][0])
+    colors = t3.color_elements(g["tris"], geo.n_nodes)
+    for c in range(colors.max() + 1):
+        nodes = g["tris"][colors == c].reshape(-1)
+        assert len(np.unique(nodes)) == len(nodes)  # one colour never touches a node twice
