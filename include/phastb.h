@@ -165,6 +165,50 @@ int phastb_q4_explicit_adjoint_step(const phastb_q4_grid* g, const phastb_q4_mat
                                     const double* ab, double* ub_out, double* vb_out, double* ab_out,
                                     double* fb_acc, double* db_acc, double* scratch, void* stream);
 
+/* ---- unstructured linear triangles (T3), FP64 ----------------------------------------------
+ * Greedily coloured elements: no two elements of one colour share a node, so each colour's
+ * elements scatter their nodal contributions without atomics (one launch per colour; the
+ * per-node summation order is fixed, hence deterministic results).  elem, order, grad, areas
+ * are device arrays; color_off is a HOST array of n_colors + 1 offsets into order, which the
+ * caller keeps unchanged for the lifetime of the mesh.  Geometry as FEMMesh (T3 branch,
+ * core/mesh.py:236-303): grad (E,3,2) P1 gradients, areas (E,). */
+typedef struct {
+  int n_nodes, n_elems, n_colors, reserved; /* reserved: 0 */
+  const int* elem;       /* (E,3) node ids */
+  const int* order;      /* (E,) element ids sorted by colour */
+  const int* color_off;  /* host, (n_colors+1) */
+  const double* grad;    /* (E,3,2) */
+  const double* areas;   /* (E,) */
+} phastb_t3_mesh;
+
+/* Internal force at the element centroid stress of the split (d NULL: undegraded linear).
+ * FEMOperators.internal_force / _assemble_force, core/fem_operators.py:598-680 */
+int phastb_t3_internal_force(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u,
+                             const double* d, double* f, void* stream);
+/* psi+ per element and H_out = max(H_in, psi+) (either output may be NULL).
+ * compute_psi_plus, fem_operators.py:951-1025 (T3 branch) + _H_update */
+int phastb_t3_psi_history(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u,
+                          const double* H_in, double* H_out, double* psi, void* stream);
+/* AT2 damage operator y = Gc l0 K d + consistent mass with rc_e = (2 H_e + Gc/l0) A_e / 12;
+ * per-element overrides gc_over_l0_e, gcl0_e may be NULL.  PhaseFieldDamageSolver._Ax,
+ * solvers/damage_solver.py:1702-1755 */
+int phastb_t3_damage_apply(const phastb_t3_mesh* mesh, const double* d, const double* H, double gc_over_l0,
+                           const double* gc_over_l0_e, double gcl0, const double* gcl0_e, double* y,
+                           void* stream);
+/* b = sum 2 H_e A_e / 3 and Jacobi M_inv = 1 / (diag + 1e-30), diag = Gc l0 A |grad phi|^2 + 2 rc_e.
+ * _prepare_cg + _compute_preconditioner, damage_solver.py:2095-2265 */
+int phastb_t3_damage_prepare(const phastb_t3_mesh* mesh, const double* H, double gc_over_l0,
+                             const double* gc_over_l0_e, double gcl0, const double* gcl0_e, double* b,
+                             double* m_inv, void* stream);
+/* Bound-projected PCG damage solve on T3 (as phastb_q4_damage_solve).
+ * _solve_projected_cg, damage_solver.py:3528-3775 */
+size_t phastb_t3_damage_solve_workspace_bytes(int n_nodes);
+int phastb_t3_damage_solve(const phastb_t3_mesh* mesh, const double* H, double gc_over_l0,
+                           const double* gc_over_l0_e, double gcl0, const double* gcl0_e,
+                           const double* d_prev, const double* d_init, const uint8_t* fixed,
+                           const double* fixed_vals, double tol, int max_iter, int check_every,
+                           double* d_out, int* info, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Energy sums (FP64): out[0] elastic, out[1] fracture surface term d^T M d,
  * out[2] gradient term d^T K d, out[3] kinetic sum_i |v_i|^2 M_i (v may be NULL).
  * compute_energy_components, fem_operators.py:1430-1496 (caller scales by Gc etc.) */

@@ -52,7 +52,14 @@ class MechOpts(C.Structure):
                 ("max_refine", C.c_int)]
 
 
+class T3Mesh(C.Structure):
+    _fields_ = [("n_nodes", C.c_int), ("n_elems", C.c_int), ("n_colors", C.c_int), ("reserved", C.c_int),
+                ("elem", C.c_void_p), ("order", C.c_void_p), ("color_off", C.POINTER(C.c_int)),
+                ("grad", C.c_void_p), ("areas", C.c_void_p)]
+
+
 Q4G, Q4M, VG, VM = C.POINTER(Q4Grid), C.POINTER(Q4Material), C.POINTER(VoxelGrid), C.POINTER(VoxelMaterial)
+T3M = C.POINTER(T3Mesh)
 MO = C.POINTER(MechOpts)
 
 # name -> (restype, argtypes)
@@ -76,6 +83,13 @@ SIGNATURES = {
     "phastb_q4_damage_adjoint_grads": (C.c_int, [Q4G, vp, vp, C.c_double, vp, vp, vp, vp, vp]),
     "phastb_q4_explicit_adjoint_step": (C.c_int, [Q4G, Q4M, C.c_double, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                                   vp, vp, vp]),
+    "phastb_t3_internal_force": (C.c_int, [T3M, Q4M, vp, vp, vp, vp]),
+    "phastb_t3_psi_history": (C.c_int, [T3M, Q4M, vp, vp, vp, vp, vp]),
+    "phastb_t3_damage_apply": (C.c_int, [T3M, vp, vp, C.c_double, vp, C.c_double, vp, vp, vp]),
+    "phastb_t3_damage_prepare": (C.c_int, [T3M, vp, C.c_double, vp, C.c_double, vp, vp, vp, vp]),
+    "phastb_t3_damage_solve_workspace_bytes": (C.c_size_t, [C.c_int]),
+    "phastb_t3_damage_solve": (C.c_int, [T3M, vp, C.c_double, vp, C.c_double, vp, vp, vp, vp, vp, C.c_double, C.c_int,
+                                         C.c_int, vp, ip, vp, sz, vp]),
     "phastb_q4_explicit_step": (C.c_int, [Q4G, Q4M, C.c_int, C.c_double, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                           vp, vp, vp, vp]),
     "phastb_q4_energy_sums": (C.c_int, [Q4G, Q4M, vp, vp, vp, dp, vp, sz, vp]),

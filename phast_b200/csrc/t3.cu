@@ -1,0 +1,275 @@
+// Unstructured linear-triangle (T3) operators with a coloured element scatter.
+//
+// The elements are greedily coloured on the host so that no two elements of
+// one colour share a node; each colour is one launch in which every element
+// adds its three nodal contributions with plain read-modify-writes -- no
+// atomics, and the per-node summation order (colour by colour) is fixed, so
+// results are deterministic.  One Gauss point per element (centroid), the
+// stress splits of q4_kernels.cuh, and the element-H AT2 damage system with
+// the consistent T3 mass.  C ABI in include/phastb.h.
+#include "engine.cuh"
+#include "q4_kernels.cuh"
+
+#include <cstring>
+
+namespace phastb {
+
+namespace {
+
+struct T3Dev {
+  const int* elem;     // (E, 3)
+  const int* order;    // (E,) element ids sorted by colour
+  const double* grad;  // (E, 3, 2)
+  const double* areas; // (E,)
+};
+
+inline T3Dev t3_dev(const phastb_t3_mesh& m) { return T3Dev{m.elem, m.order, m.grad, m.areas}; }
+
+__device__ __forceinline__ void t3_strain(const T3Dev& t, int e, const double* __restrict__ u, double& exx,
+                                          double& eyy, double& gxy, int* n, double (*gp)[2]) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    n[a] = __ldg(t.elem + 3 * e + a);
+    gp[a][0] = __ldg(t.grad + 6 * e + 2 * a);
+    gp[a][1] = __ldg(t.grad + 6 * e + 2 * a + 1);
+  }
+  exx = eyy = gxy = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double ux = __ldg(u + 2 * n[a]), uy = __ldg(u + 2 * n[a] + 1);
+    exx += gp[a][0] * ux;
+    eyy += gp[a][1] * uy;
+    gxy += gp[a][1] * ux + gp[a][0] * uy;
+  }
+}
+
+// f_a += A (sigma . grad phi_a) for the elements order[k0 .. k1) of one colour.
+__global__ void __launch_bounds__(kThreads) t3_force_colour(T3Dev t, Mat2<double> m, int split,
+                                                            const double* __restrict__ u,
+                                                            const double* __restrict__ d, double* f, int k0,
+                                                            int k1) {
+  const int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= k1) return;
+  const int e = __ldg(t.order + k);
+  int n[3];
+  double gp[3][2], exx, eyy, gxy;
+  t3_strain(t, e, u, exx, eyy, gxy, n, gp);
+  double sxx, syy, sxy;
+  if (d) {
+    const double de = (__ldg(d + n[0]) + __ldg(d + n[1]) + __ldg(d + n[2])) / 3.0;
+    stress2(m, split, exx, eyy, gxy, degr(m, de), sxx, syy, sxy);
+  } else {
+    stress2(m, PHASTB_SPLIT_LINEAR, exx, eyy, gxy, 1.0, sxx, syy, sxy);
+  }
+  const double A = __ldg(t.areas + e);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    f[2 * n[a]] += A * (sxx * gp[a][0] + sxy * gp[a][1]);
+    f[2 * n[a] + 1] += A * (sxy * gp[a][0] + syy * gp[a][1]);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) t3_psi_kernel(T3Dev t, Mat2<double> m, const double* __restrict__ u,
+                                                          const double* __restrict__ Hin, double* __restrict__ Hout,
+                                                          double* __restrict__ psi, int ne) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  int n[3];
+  double gp[3][2], exx, eyy, gxy;
+  t3_strain(t, e, u, exx, eyy, gxy, n, gp);
+  const double p = psi2(m, m.psplit, exx, eyy, gxy);
+  if (psi) psi[e] = p;
+  if (Hout) {
+    const double h = Hin ? Hin[e] : 0.0;
+    Hout[e] = p > h ? p : h;
+  }
+}
+
+// y_a += gcl0_e A (grad phi_a . grad d) + rc_e (d_a + d_sum),  rc_e = (2 H_e + gco_e) A / 12
+__global__ void __launch_bounds__(kThreads) t3_damage_colour(T3Dev t, const double* __restrict__ d,
+                                                             const double* __restrict__ H, double gco,
+                                                             const double* __restrict__ gco_e, double gcl0,
+                                                             const double* __restrict__ gcl0_e, double* y, int k0,
+                                                             int k1, const int* guard) {
+  if (guard && *guard == 0) return;
+  const int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= k1) return;
+  const int e = __ldg(t.order + k);
+  int n[3];
+  double gp[3][2], dd[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    n[a] = __ldg(t.elem + 3 * e + a);
+    gp[a][0] = __ldg(t.grad + 6 * e + 2 * a);
+    gp[a][1] = __ldg(t.grad + 6 * e + 2 * a + 1);
+    dd[a] = __ldg(d + n[a]);
+  }
+  const double A = __ldg(t.areas + e);
+  const double gx = gp[0][0] * dd[0] + gp[1][0] * dd[1] + gp[2][0] * dd[2];
+  const double gy = gp[0][1] * dd[0] + gp[1][1] * dd[1] + gp[2][1] * dd[2];
+  const double rc = (2.0 * (H ? __ldg(H + e) : 0.0) + (gco_e ? __ldg(gco_e + e) : gco)) * A / 12.0;
+  const double kl = gcl0_e ? __ldg(gcl0_e + e) : gcl0;
+  const double ds = dd[0] + dd[1] + dd[2];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) y[n[a]] += kl * (A * (gp[a][0] * gx + gp[a][1] * gy)) + rc * (dd[a] + ds);
+}
+
+// b_a += 2 H_e A / 3;  diag_a += gcl0_e A |grad phi_a|^2 + 2 rc_e
+__global__ void __launch_bounds__(kThreads) t3_prepare_colour(T3Dev t, const double* __restrict__ H, double gco,
+                                                              const double* __restrict__ gco_e, double gcl0,
+                                                              const double* __restrict__ gcl0_e, double* b,
+                                                              double* diag, int k0, int k1) {
+  const int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= k1) return;
+  const int e = __ldg(t.order + k);
+  const double A = __ldg(t.areas + e);
+  const double He = H ? __ldg(H + e) : 0.0;
+  const double rc = (2.0 * He + (gco_e ? __ldg(gco_e + e) : gco)) * A / 12.0;
+  const double kl = gcl0_e ? __ldg(gcl0_e + e) : gcl0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int n = __ldg(t.elem + 3 * e + a);
+    const double gx = __ldg(t.grad + 6 * e + 2 * a), gy = __ldg(t.grad + 6 * e + 2 * a + 1);
+    b[n] += 2.0 * He * A / 3.0;
+    diag[n] += kl * (A * (gx * gx + gy * gy)) + 2.0 * rc;
+  }
+}
+
+__global__ void t3_invert_kernel(int n, double* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = 1.0 / (x[i] + 1e-30);
+}
+
+bool valid_mesh(const phastb_t3_mesh* m) {
+  if (!m || m->n_nodes < 1 || m->n_elems < 1 || m->n_colors < 1 || !m->elem || !m->order || !m->color_off ||
+      !m->grad || !m->areas)
+    return false;
+  if (m->color_off[0] != 0 || m->color_off[m->n_colors] != m->n_elems) return false;
+  for (int c = 0; c < m->n_colors; ++c)
+    if (m->color_off[c + 1] < m->color_off[c]) return false;
+  return true;
+}
+
+int t3_damage_apply_launch(const phastb_t3_mesh& mesh, const double* d, const double* H, double gco,
+                           const double* gco_e, double gcl0, const double* gcl0_e, double* y, const int* guard,
+                           cudaStream_t s) {
+  int st = cuda_status(cudaMemsetAsync(y, 0, sizeof(double) * (size_t)mesh.n_nodes, s));
+  if (st) return st;
+  const T3Dev t = t3_dev(mesh);
+  for (int c = 0; c < mesh.n_colors; ++c) {
+    const int k0 = mesh.color_off[c], k1 = mesh.color_off[c + 1];
+    if (k1 <= k0) continue;
+    { note_launch(); t3_damage_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, d, H, gco, gco_e, gcl0, gcl0_e, y, k0, k1, guard); }
+  }
+  return last_launch_status();
+}
+
+// Damage operator context for the Krylov engines.  The mesh is held by value;
+// color_off points into caller memory that must outlive the solve.
+struct T3DamageCtx {
+  phastb_t3_mesh mesh;
+  const double* H;
+  double gco;
+  const double* gco_e;
+  double gcl0;
+  const double* gcl0_e;
+};
+
+int t3_damage_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
+  const T3DamageCtx* k = static_cast<const T3DamageCtx*>(c);
+  return t3_damage_apply_launch(k->mesh, x, k->H, k->gco, k->gco_e, k->gcl0, k->gcl0_e, y, guard, s);
+}
+
+}  // namespace
+
+}  // namespace phastb
+
+using namespace phastb;
+
+extern "C" {
+
+int phastb_t3_internal_force(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u,
+                             const double* d, double* f, void* stream) {
+  if (!valid_mesh(mesh) || !m || !u || !f) return PHASTB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = cuda_status(cudaMemsetAsync(f, 0, sizeof(double) * 2 * (size_t)mesh->n_nodes, s));
+  if (st) return st;
+  const T3Dev t = t3_dev(*mesh);
+  const Mat2<double> mm = make_mat2<double>(*m);
+  for (int c = 0; c < mesh->n_colors; ++c) {
+    const int k0 = mesh->color_off[c], k1 = mesh->color_off[c + 1];
+    if (k1 <= k0) continue;
+    { note_launch(); t3_force_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, mm, m->stress_split, u, d, f, k0, k1); }
+  }
+  return last_launch_status();
+}
+
+int phastb_t3_psi_history(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u,
+                          const double* H_in, double* H_out, double* psi, void* stream) {
+  if (!valid_mesh(mesh) || !m || !u || (!H_out && !psi)) return PHASTB_ERR_ARG;
+  const int ne = mesh->n_elems;
+  { note_launch(); t3_psi_kernel<<<grid_full(ne), kThreads, 0, (cudaStream_t)stream>>>(t3_dev(*mesh), make_mat2<double>(*m), u, H_in, H_out, psi, ne); }
+  return last_launch_status();
+}
+
+int phastb_t3_damage_apply(const phastb_t3_mesh* mesh, const double* d, const double* H, double gc_over_l0,
+                           const double* gc_over_l0_e, double gcl0, const double* gcl0_e, double* y, void* stream) {
+  if (!valid_mesh(mesh) || !d || !y) return PHASTB_ERR_ARG;
+  return t3_damage_apply_launch(*mesh, d, H, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e, y, nullptr,
+                                (cudaStream_t)stream);
+}
+
+int phastb_t3_damage_prepare(const phastb_t3_mesh* mesh, const double* H, double gc_over_l0,
+                             const double* gc_over_l0_e, double gcl0, const double* gcl0_e, double* b,
+                             double* m_inv, void* stream) {
+  if (!valid_mesh(mesh) || !b || !m_inv) return PHASTB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t nb = sizeof(double) * (size_t)mesh->n_nodes;
+  int st;
+  if ((st = cuda_status(cudaMemsetAsync(b, 0, nb, s)))) return st;
+  if ((st = cuda_status(cudaMemsetAsync(m_inv, 0, nb, s)))) return st;
+  const T3Dev t = t3_dev(*mesh);
+  for (int c = 0; c < mesh->n_colors; ++c) {
+    const int k0 = mesh->color_off[c], k1 = mesh->color_off[c + 1];
+    if (k1 <= k0) continue;
+    { note_launch(); t3_prepare_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, H, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e, b, m_inv, k0, k1); }
+  }
+  { note_launch(); t3_invert_kernel<<<grid_for(mesh->n_nodes), kThreads, 0, s>>>(mesh->n_nodes, m_inv); }
+  return last_launch_status();
+}
+
+size_t phastb_t3_damage_solve_workspace_bytes(int n_nodes) { return ppcg_ws_bytes(n_nodes); }
+
+int phastb_t3_damage_solve(const phastb_t3_mesh* mesh, const double* H, double gc_over_l0,
+                           const double* gc_over_l0_e, double gcl0, const double* gcl0_e, const double* d_prev,
+                           const double* d_init, const uint8_t* fixed, const double* fixed_vals, double tol,
+                           int max_iter, int check_every, double* d_out, int* info, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+  if (!valid_mesh(mesh) || !d_prev || !d_out || max_iter < 0 || check_every < 1) return PHASTB_ERR_ARG;
+  if (fixed && !fixed_vals) return PHASTB_ERR_ARG;
+  const int n = mesh->n_nodes;
+  if (!workspace || workspace_bytes < ppcg_ws_bytes(n)) return PHASTB_ERR_WORKSPACE;
+  ScopedStream scope((cudaStream_t)stream);
+  if (scope.status()) return scope.status();
+  cudaStream_t s = scope.get();
+  PpcgWs w = ppcg_ws(workspace, n);
+  int st = phastb_t3_damage_prepare(mesh, H, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e, w.b, w.minv, (void*)s);
+  if (st) return st;
+  T3DamageCtx ctx;
+  std::memset(&ctx, 0, sizeof(ctx));
+  ctx.mesh = *mesh;
+  ctx.H = H;
+  ctx.gco = gc_over_l0;
+  ctx.gco_e = gc_over_l0_e;
+  ctx.gcl0 = gcl0;
+  ctx.gcl0_e = gcl0_e;
+  LinOp<double> A{t3_damage_op, &ctx, sizeof(ctx)};
+  int inf[2] = {0, 0};
+  st = ppcg_solve(A, n, w, d_prev, d_init, fixed, fixed_vals, tol, max_iter, check_every, d_out, inf, s);
+  if (info) {
+    info[0] = inf[0];
+    info[1] = inf[1];
+  }
+  return st;
+}
+
+}  // extern "C"

@@ -17,7 +17,14 @@ from ._lib import call, ptr, raw, stream
 
 
 class PhaseFieldDamageSolver:
-    """GPU projected-CG AT2 damage solver for structured Q4 grids."""
+    """GPU projected-CG AT2 damage solver for structured Q4 grids (T3 meshes: ``phast_b200.t3``)."""
+
+    def __new__(cls, fem, *args, **kwargs):
+        from .t3 import T3DamageSolver, T3FEMOperators
+        if isinstance(fem, T3FEMOperators):
+            keep = {k: kwargs[k] for k in ("tol", "max_iter", "bounds_method") if k in kwargs}
+            return T3DamageSolver(fem, *args[:2], **keep)
+        return super().__new__(cls)
 
     def __init__(self, fem, tol=1e-5, max_iter=5000, ctx=None, use_multigrid=True, bounds_method="post_clamp",
                  preconditioner=None, nodal_H=False):

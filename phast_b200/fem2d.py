@@ -101,10 +101,10 @@ class FEMMesh:
     """Minimal ``FEMMesh.from_tensors`` (core/mesh.py:84-155) for Q4 grids on the GPU."""
 
     def __init__(self, nodes, elements, element_type="Q4", device=None, dtype=torch.float64, node_sets=None):
-        if element_type != "Q4":
-            raise NotImplementedError("the B200 backend implements structured Q4 meshes")
+        if element_type not in ("Q4", "T3"):
+            raise NotImplementedError("the B200 backend implements structured Q4 and unstructured T3 meshes")
         device = torch.device(device) if device is not None else torch.device("cuda")
-        self.element_type = "Q4"
+        self.element_type = element_type
         self.dtype = dtype
         self.device = device
         self.nodes = torch.as_tensor(nodes, dtype=dtype).to(device)
@@ -176,7 +176,17 @@ def _dtype_code(t):
 
 
 class FEMOperators:
-    """GPU ``FEMOperators`` for structured Q4 grids (core/fem_operators.py:35-1530)."""
+    """GPU ``FEMOperators`` for structured Q4 grids (core/fem_operators.py:35-1530).
+
+    A mesh whose ``element_type`` is ``'T3'`` gets the triangle operators of
+    ``phast_b200.t3`` instead.
+    """
+
+    def __new__(cls, mesh, material, ctx=None):
+        if getattr(mesh, "element_type", "Q4") == "T3":
+            from .t3 import T3FEMOperators
+            return T3FEMOperators(mesh, material)
+        return super().__new__(cls)
 
     def __init__(self, mesh, material, ctx=None):
         self.mesh = mesh

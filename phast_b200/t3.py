@@ -1,0 +1,208 @@
+"""Unstructured linear triangles (T3) behind PhAST's ``FEMOperators`` and
+``PhaseFieldDamageSolver`` interfaces.
+
+PhAST's default 2D element is the T3 (src/phast/core/mesh.py:236-303,
+core/fem_operators.py T3 branches, solvers/damage_solver.py element-H AT2 path).
+The geometry (P1 gradients, areas, lumped mass, incircle sizes) is computed once
+on the device; the elements are greedily coloured on the host so that the CUDA
+kernels scatter element contributions colour by colour without atomics.
+``FEMOperators`` / ``PhaseFieldDamageSolver`` construct these classes when the
+mesh's ``element_type`` is ``'T3'``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, ptr, raw, stream
+
+
+def color_elements(elements, n_nodes):
+    """Greedy first-fit colouring in element order: no colour touches a node twice."""
+    el = np.asarray(elements, dtype=np.int64)
+    used = np.zeros(n_nodes, dtype=np.uint64)
+    colors = np.empty(el.shape[0], dtype=np.int64)
+    for e in range(el.shape[0]):
+        a, b, c = el[e]
+        busy = int(used[a] | used[b] | used[c])
+        k = 0
+        while busy >> k & 1:
+            k += 1
+        if k >= 64:
+            raise RuntimeError("T3 colouring needs more than 64 colours")
+        colors[e] = k
+        bit = np.uint64(1 << k)
+        used[a] |= bit
+        used[b] |= bit
+        used[c] |= bit
+    return colors
+
+
+class T3FEMOperators:
+    """GPU operators of a T3 mesh (core/fem_operators.py, triangle branches)."""
+
+    def __init__(self, mesh, material):
+        from .fem2d import q4_material_struct
+        self.mesh = mesh
+        self.material = material
+        self.device = torch.device(getattr(mesh, "device", "cuda"))
+        if self.device.type != "cuda":
+            raise ValueError("the B200 backend needs the mesh on a CUDA device")
+        self.dtype = torch.float64
+        nodes = mesh.nodes.detach().to(self.device, torch.float64)
+        el = mesh.elements.detach().to(self.device, torch.long)
+        if el.ndim != 2 or el.shape[1] != 3:
+            raise ValueError("T3 connectivity must have shape (E, 3)")
+        self.n_nodes, self.n_elems = int(nodes.shape[0]), int(el.shape[0])
+        p0, p1, p2 = nodes[el[:, 0]], nodes[el[:, 1]], nodes[el[:, 2]]
+        v01, v02, v12 = p1 - p0, p2 - p0, p2 - p1
+        s2a = v01[:, 0] * v02[:, 1] - v01[:, 1] * v02[:, 0]
+        self.areas = (0.5 * s2a.abs()).contiguous()
+        sgn = torch.sign(s2a)
+        sgn[sgn == 0] = 1.0
+        inv = 1.0 / torch.where(s2a.abs() > 1e-10, s2a, sgn * 1e-10)  # mesh.py:252-258
+        g = torch.empty(self.n_elems, 3, 2, dtype=torch.float64, device=self.device)
+        g[:, 0, 0] = (p1[:, 1] - p2[:, 1]) * inv
+        g[:, 0, 1] = (p2[:, 0] - p1[:, 0]) * inv
+        g[:, 1, 0] = (p2[:, 1] - p0[:, 1]) * inv
+        g[:, 1, 1] = (p0[:, 0] - p2[:, 0]) * inv
+        g[:, 2, 0] = (p0[:, 1] - p1[:, 1]) * inv
+        g[:, 2, 1] = (p1[:, 0] - p0[:, 0]) * inv
+        self.grad_phi = g.contiguous()
+        perim = v01.norm(dim=1) + v12.norm(dim=1) + v02.norm(dim=1)
+        self.elem_h = 4.0 * self.areas / (perim + 1e-30)
+        self.h_min = float(self.elem_h.min())
+        self.M_scalar = torch.zeros(self.n_nodes, dtype=torch.float64, device=self.device)
+        self.M_scalar.scatter_add_(0, el.reshape(-1), (self.areas / 3.0).unsqueeze(1).expand(-1, 3).reshape(-1))
+        self.M_vec = material.rho * self.M_scalar.unsqueeze(1).expand(-1, 2).flatten()
+        self.M_vec_inv = 1.0 / (self.M_vec + 1e-30)
+        self.dt_cfl = self.h_min / material.c_p
+        self.diff_E_field = None
+        colors = color_elements(el.cpu().numpy(), self.n_nodes)
+        order = np.argsort(colors, kind="stable")
+        self.n_colors = int(colors.max()) + 1
+        off = np.searchsorted(colors[order], np.arange(self.n_colors + 1))
+        self._elem32 = el.to(torch.int32).contiguous()
+        self._order = torch.as_tensor(order.astype(np.int32), device=self.device)
+        self._color_off = (C.c_int * (self.n_colors + 1))(*[int(v) for v in off])
+        self.t3 = _lib.T3Mesh(self.n_nodes, self.n_elems, self.n_colors, 0, ptr(self._elem32), ptr(self._order),
+                              self._color_off, ptr(self.grad_phi), ptr(self.areas))
+        self._mat = q4_material_struct(material, torch.float64)
+
+    def mat(self, dtype=None):
+        return self._mat
+
+    def _nodal(self, t, comps, name):
+        shape = (self.n_nodes, comps) if comps > 1 else (self.n_nodes,)
+        if tuple(t.shape) != shape:
+            raise ValueError(f"{name} must have shape {shape}, got {tuple(t.shape)}")
+        _lib.require_cuda(t, name)
+        return t.to(torch.float64).contiguous()
+
+    def internal_force(self, u, d):
+        """f = sum_e A_e B_e^T sigma(u, d_e), d_e the element mean (fem_operators.py:598-680)."""
+        u = self._nodal(u, 2, "u")
+        dd = None if d is None else self._nodal(d, 1, "d")
+        f = torch.empty_like(u)
+        call("phastb_t3_internal_force", self.t3, self._mat, ptr(u), ptr(dd), ptr(f), stream())
+        return f
+
+    def internal_force_linear(self, u):
+        return self.internal_force(u, None)
+
+    def compute_psi_plus(self, u, strain=None, d=None):
+        """psi+ per element for the material's energy split (fem_operators.py:951-1025)."""
+        u = self._nodal(u, 2, "u")
+        psi = torch.empty(self.n_elems, dtype=torch.float64, device=self.device)
+        call("phastb_t3_psi_history", self.t3, self._mat, ptr(u), None, None, ptr(psi), stream())
+        return psi
+
+    def psi_history(self, u, H_in=None):
+        """H_out = max(H_in, psi+(u)) per element (StaggeredSolver._H_update)."""
+        u = self._nodal(u, 2, "u")
+        H = torch.empty(self.n_elems, dtype=torch.float64, device=self.device)
+        hin = None if H_in is None else H_in.to(torch.float64).contiguous()
+        call("phastb_t3_psi_history", self.t3, self._mat, ptr(u), ptr(hin), ptr(H), None, stream())
+        return H
+
+
+class T3DamageSolver:
+    """Bound-projected PCG AT2 damage solve on a T3 mesh (element H)."""
+
+    def __init__(self, fem, tol=1e-5, max_iter=5000, bounds_method="projected_cg"):
+        if bounds_method != "projected_cg":
+            raise NotImplementedError("the B200 backend implements bounds_method='projected_cg'")
+        mat = fem.material
+        if getattr(mat, "pf_model", "AT2") != "AT2":
+            raise NotImplementedError("T3 damage supports pf_model='AT2'")
+        self.fem = fem
+        self.material = mat
+        self.tol = float(tol)
+        self.max_iter = int(max_iter)
+        self._Gc, self._l0 = float(mat.Gc), float(mat.l0)
+        self.check_every = 10
+        self.last_iter = 0
+        self.last_converged = True
+        self.n_solves = 0
+        self._ws = _lib.Workspace(fem.device)
+
+    def _coeffs(self, Gc=None, l0=None, Gc_field=None):
+        Gc_s = self._Gc if Gc is None else float(Gc)
+        l0_s = self._l0 if l0 is None else float(l0)
+        gcl0_e = gco_e = None
+        if Gc_field is not None:
+            gf = torch.as_tensor(Gc_field, dtype=torch.float64, device=self.fem.device).reshape(-1)
+            if gf.numel() != self.fem.n_elems:
+                raise ValueError("Gc_field must have one value per element")
+            gcl0_e, gco_e = (gf * l0_s).contiguous(), (gf / l0_s).contiguous()
+        return Gc_s * l0_s, Gc_s / l0_s, gcl0_e, gco_e
+
+    def _Ax(self, d, reaction_H, Gc=None, l0=None, Gc_field=None):
+        """(Gc l0 K + M(rc)) d with rc_e = (2 H_e + Gc/l0) A_e / 12 (damage_solver.py:1702-1755)."""
+        gcl0, gco, gcl0_e, gco_e = self._coeffs(Gc, l0, Gc_field)
+        d = d.to(torch.float64).contiguous()
+        H = reaction_H.to(torch.float64).contiguous()
+        y = torch.empty_like(d)
+        call("phastb_t3_damage_apply", self.fem.t3, ptr(d), ptr(H), gco, ptr(gco_e), gcl0, ptr(gcl0_e), ptr(y),
+             stream())
+        return y
+
+    def prepare(self, H, Gc=None, l0=None, Gc_field=None):
+        gcl0, gco, gcl0_e, gco_e = self._coeffs(Gc, l0, Gc_field)
+        H = H.to(torch.float64).contiguous()
+        b = torch.empty(self.fem.n_nodes, dtype=torch.float64, device=H.device)
+        m = torch.empty_like(b)
+        call("phastb_t3_damage_prepare", self.fem.t3, ptr(H), gco, ptr(gco_e), gcl0, ptr(gcl0_e), ptr(b), ptr(m),
+             stream())
+        return b, m
+
+    def solve(self, H_input, d_prev, Gc=None, l0=None, Gc_field=None, pf_dirichlet_mask=None,
+              pf_dirichlet_values=None, initial_guess=None):
+        """d in [d_prev, 1] by projected CG (damage_solver.py:2493-2640, 3528-3775)."""
+        self.n_solves += 1
+        gcl0, gco, gcl0_e, gco_e = self._coeffs(Gc, l0, Gc_field)
+        H = H_input.detach().to(torch.float64).contiguous()
+        if tuple(H.shape) != (self.fem.n_elems,):
+            raise ValueError(f"T3 damage expects element H of shape ({self.fem.n_elems},)")
+        dp = d_prev.detach().to(torch.float64).contiguous()
+        di = None if initial_guess is None else initial_guess.detach().to(torch.float64).contiguous()
+        fixed = vals = None
+        if pf_dirichlet_mask is not None and bool(pf_dirichlet_mask.any()):
+            if pf_dirichlet_values is None:
+                raise ValueError("pf_dirichlet_values must be supplied with mask")
+            fixed = pf_dirichlet_mask.to(device=dp.device, dtype=torch.uint8).contiguous()
+            vals = pf_dirichlet_values.to(device=dp.device, dtype=torch.float64).contiguous()
+        n = self.fem.n_nodes
+        out = torch.empty(n, dtype=torch.float64, device=dp.device)
+        info = (C.c_int * 2)()
+        wp, wn = self._ws.get(_lib.load().phastb_t3_damage_solve_workspace_bytes(n))
+        st = raw("phastb_t3_damage_solve", self.fem.t3, ptr(H), gco, ptr(gco_e), gcl0, ptr(gcl0_e), ptr(dp),
+                 ptr(di), ptr(fixed), ptr(vals), self.tol, self.max_iter, self.check_every, ptr(out), info, wp, wn,
+                 stream())
+        _lib.check(st, "phastb_t3_damage_solve")
+        self.last_iter = int(info[0])
+        self.last_converged = info[1] == 0
+        return out.to(d_prev.dtype)
