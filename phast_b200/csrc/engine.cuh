@@ -77,6 +77,9 @@ struct PcgState {
   int steps;        // iterations that moved the iterate
   int iter;
   int converged;
+  double outer_rr;  // an enclosing refinement's residual norm^2, when one is checked at the start
+  int outer_done;   // ... and that residual already met its threshold: nothing was iterated
+  int trips;        // iterations run by the device-side loop (bounds it by max_iter)
 };
 
 template <typename T>
@@ -111,12 +114,29 @@ struct PcgResult {
   int breakdown;
   int nonfinite;
   double rnorm;
+  int outer_done;
+  double outer_rnorm;
+};
+
+// Stopping rule of a PCG solve, evaluated on the device at the start:
+// ||r|| <= max(abs, rel * max(||r0||, rel_floor)); with outer_rr set, the solve
+// first checks *outer_rr <= outer_thr^2 (an enclosing refinement's FP64
+// residual) and does nothing when it holds.
+struct PcgThreshold {
+  double abs = 0.0, rel = 0.0, rel_floor = 0.0;
+  const double* outer_rr = nullptr;
+  double outer_thr = 0.0;
 };
 
 template <typename T>
 int pcg_run(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T* inv_diag, const Precond<T>* M,
             T* x, double thr, int maxiter, int check_every, PcgMode mode, double rr0_for_div, PcgResult* out,
             cudaStream_t s);
+
+template <typename T>
+int pcg_run_thr(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T* inv_diag, const Precond<T>* M,
+                T* x, const PcgThreshold& thr, int maxiter, int check_every, PcgMode mode, PcgResult* out,
+                cudaStream_t s);
 
 // Vector helpers used by the drivers.
 template <typename T>
@@ -136,5 +156,12 @@ inline void key_val(GraphKey& k, const V& v) {
 // Returns the executable graph of `body` (captured on s) or nullptr when the
 // stream cannot be captured; *count receives the kernel launches per replay.
 cudaGraphExec_t graph_for(const GraphKey& key, cudaStream_t s, const std::function<int()>& body, long long* count);
+
+// A graph holding one conditional WHILE node: `body` (one solver iteration) then
+// a one-thread kernel that sets the loop condition to *active && ++*trips <
+// max_iter.  The whole solve is one graph launch; the trip counter bounds it.
+// nullptr when conditional nodes are unavailable.  *count: launches per trip.
+cudaGraphExec_t while_graph_for(const GraphKey& key, cudaStream_t s, const std::function<int()>& body,
+                                const int* active, int* trips, int max_iter, long long* count);
 
 }  // namespace phastb

@@ -25,6 +25,7 @@
 #include "h8_kernels.cuh"
 #include "h8_tile.cuh"
 
+#include <cstdlib>
 #include <utility>
 
 #include <cmath>
@@ -247,7 +248,8 @@ __device__ __forceinline__ int fine_of(int i, int n_f, int periodic, bool& ok) {
 // (rows held at zero are skipped).
 template <typename T>
 __global__ void gmg_restrict(VoxGeom f, VoxGeom c, const T* __restrict__ rf, const uint8_t* __restrict__ mask,
-                             T* __restrict__ rc) {
+                             T* __restrict__ rc, const int* guard) {
+  if (guard && *guard == 0) return;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < c.n_red; n += gridDim.x * blockDim.x) {
     const int I = n % c.rx;
     const int rem = n / c.rx;
@@ -287,7 +289,8 @@ __global__ void gmg_restrict(VoxGeom f, VoxGeom c, const T* __restrict__ rf, con
 // x_f += P x_c (trilinear), masked rows untouched.
 template <typename T>
 __global__ void gmg_prolong_add(VoxGeom f, VoxGeom c, const T* __restrict__ xc, const uint8_t* __restrict__ mask,
-                                T* __restrict__ xf) {
+                                T* __restrict__ xf, const int* guard) {
+  if (guard && *guard == 0) return;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < f.n_red; n += gridDim.x * blockDim.x) {
     const int i = n % f.rx;
     const int rem = n / f.rx;
@@ -339,7 +342,8 @@ __global__ void gmg_prolong_add(VoxGeom f, VoxGeom c, const T* __restrict__ xc, 
 
 // per-component mean removal of a (3 n) nodal vector (coarse periodic levels)
 template <typename T>
-__global__ void __launch_bounds__(kThreads) gmg_mean3(int n, const T* __restrict__ x, RedWs ws) {
+__global__ void __launch_bounds__(kThreads) gmg_mean3(int n, const T* __restrict__ x, RedWs ws, const int* guard) {
+  if (guard && *guard == 0) return;
   double acc[3] = {0, 0, 0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     acc[0] += double(x[3 * (size_t)i]);
@@ -350,7 +354,8 @@ __global__ void __launch_bounds__(kThreads) gmg_mean3(int n, const T* __restrict
 }
 
 template <typename T>
-__global__ void gmg_sub_mean3(int n, const double* __restrict__ sums, T* __restrict__ x) {
+__global__ void gmg_sub_mean3(int n, const double* __restrict__ sums, T* __restrict__ x, const int* guard) {
+  if (guard && *guard == 0) return;
   const double s0 = sums[0] / n, s1 = sums[1] / n, s2 = sums[2] / n;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     x[3 * (size_t)i] -= T(s0);
@@ -363,7 +368,8 @@ __global__ void gmg_sub_mean3(int n, const double* __restrict__ sums, T* __restr
 // Later steps: res -= Ad; d = c1 d + c2 invd res; x += d.
 template <typename T>
 __global__ void gmg_cheb_first(int n, const T* __restrict__ res, const T* __restrict__ invd, T inv_theta,
-                               T* __restrict__ d, T* __restrict__ x, int accumulate) {
+                               T* __restrict__ d, T* __restrict__ x, int accumulate, const int* guard) {
+  if (guard && *guard == 0) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const T di = invd[i] * res[i] * inv_theta;
     d[i] = di;
@@ -374,7 +380,8 @@ __global__ void gmg_cheb_first(int n, const T* __restrict__ res, const T* __rest
 // First step from x = 0 reading b directly: res = b; d = invd * b / theta; x = d.
 template <typename T>
 __global__ void gmg_cheb_first_b(int n, const T* __restrict__ b, const T* __restrict__ invd, T inv_theta,
-                                 T* __restrict__ res, T* __restrict__ d, T* __restrict__ x) {
+                                 T* __restrict__ res, T* __restrict__ d, T* __restrict__ x, const int* guard) {
+  if (guard && *guard == 0) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const T bi = b[i];
     res[i] = bi;
@@ -403,7 +410,8 @@ __global__ void gmg_sub_inplace(int n, T* __restrict__ res, const T* __restrict_
 
 // res = b - A x
 template <typename T>
-__global__ void gmg_residual(int n, const T* __restrict__ b, const T* __restrict__ Ax, T* __restrict__ res) {
+__global__ void gmg_residual(int n, const T* __restrict__ b, const T* __restrict__ Ax, T* __restrict__ res, const int* guard) {
+  if (guard && *guard == 0) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) res[i] = b[i] - Ax[i];
 }
 
@@ -461,7 +469,8 @@ __global__ void gmg_init_vec(int n, const uint8_t* __restrict__ mask, T* __restr
 // E block of the preconditioned vector: z_E = r_E / diag_E on free rows
 template <typename T>
 __global__ void gmg_eblock(int nu, const T* __restrict__ r, const T* __restrict__ diag,
-                           const uint8_t* __restrict__ mask, T* __restrict__ z) {
+                           const uint8_t* __restrict__ mask, T* __restrict__ z, const int* guard) {
+  if (guard && *guard == 0) return;
   const int k = threadIdx.x;
   if (k < 6) {
     const size_t i = (size_t)nu + k;
@@ -500,6 +509,7 @@ struct Gmg {
   double* rsum;          // device copy of reduction results used by kernels
   int deg, deg_coarse;
   double safety;         // Chebyshev interval [lmax/30, safety * lmax]
+  const int* guard;      // set per preconditioner call: the Krylov engine's "still iterating" flag
 };
 
 template <typename T>
@@ -509,6 +519,7 @@ static int coarse_apply(const Gmg<T>& M, const GmgLevel<T>& L, const T* x, T* y,
   a.mu_q = L.mu;
   a.x = x;
   a.y = y;
+  a.guard = M.guard;
   return h8_tile_launch<T>(a, M.mat, kCoefQP, kModeApply, s);
 }
 
@@ -524,6 +535,7 @@ static int level_cheb(const Gmg<T>& M, int l, const T* din, T* dout, double c1, 
   a.d_out = dout;
   a.c1 = c1;
   a.c2 = c2;
+  a.guard = M.guard;
   if (l == 0) {
     a.slot = M.slot;
     a.d = M.dfield;
@@ -538,7 +550,7 @@ static int level_cheb(const Gmg<T>& M, int l, const T* din, T* dout, double c1, 
 template <typename T>
 static int level_apply(const Gmg<T>& M, int l, const T* x, T* y, cudaStream_t s) {
   if (l == 0)
-    return h8_mech_apply_t<T>(M.lv[0].g, M.mat, M.slot, x, nullptr, M.dfield, M.mask, y, M.scratch, nullptr, s);
+    return h8_mech_apply_t<T>(M.lv[0].g, M.mat, M.slot, x, nullptr, M.dfield, M.mask, y, M.scratch, M.guard, s);
   return coarse_apply<T>(M, M.lv[l], x, y, s);
 }
 
@@ -547,8 +559,8 @@ static int remove_mean(const Gmg<T>& M, int l, T* x, cudaStream_t s) {
   const GmgLevel<T>& L = M.lv[l];
   if (!(L.g.px && L.g.py && L.g.pz)) return PHASTB_OK;
   const int nn = L.g.n_red;
-  { note_launch(); gmg_mean3<T><<<grid_for(nn), kThreads, 0, s>>>(nn, x, M.rw); }
-  { note_launch(); gmg_sub_mean3<T><<<grid_for(nn), kThreads, 0, s>>>(nn, M.rw.out, x); }
+  { note_launch(); gmg_mean3<T><<<grid_for(nn), kThreads, 0, s>>>(nn, x, M.rw, M.guard); }
+  { note_launch(); gmg_sub_mean3<T><<<grid_for(nn), kThreads, 0, s>>>(nn, M.rw.out, x, M.guard); }
   return last_launch_status();
 }
 
@@ -562,11 +574,11 @@ static int chebyshev(const Gmg<T>& M, int l, int deg, bool from_zero, bool need_
   const double bmax = M.safety * L.lmax, amin = L.lmax / 30.0;
   const double theta = 0.5 * (bmax + amin), delta = 0.5 * (bmax - amin), sigma = theta / delta;
   if (from_zero) {
-    { note_launch(); gmg_cheb_first_b<T><<<G, kThreads, 0, s>>>(n, L.b, L.invd, T(1.0 / theta), L.res, L.dvec, L.x); }
+    { note_launch(); gmg_cheb_first_b<T><<<G, kThreads, 0, s>>>(n, L.b, L.invd, T(1.0 / theta), L.res, L.dvec, L.x, M.guard); }
   } else {
     if ((st = level_apply(M, l, L.x, L.Ad, s))) return st;
-    { note_launch(); gmg_residual<T><<<G, kThreads, 0, s>>>(n, L.b, L.Ad, L.res); }
-    { note_launch(); gmg_cheb_first<T><<<G, kThreads, 0, s>>>(n, L.res, L.invd, T(1.0 / theta), L.dvec, L.x, 1); }
+    { note_launch(); gmg_residual<T><<<G, kThreads, 0, s>>>(n, L.b, L.Ad, L.res, M.guard); }
+    { note_launch(); gmg_cheb_first<T><<<G, kThreads, 0, s>>>(n, L.res, L.invd, T(1.0 / theta), L.dvec, L.x, 1, M.guard); }
   }
   // later steps ping-pong the direction between dvec and Ad
   T* cur = L.dvec;
@@ -594,9 +606,9 @@ static int vcycle(const Gmg<T>& M, int l, cudaStream_t s) {
   }
   if ((st = chebyshev(M, l, M.deg, true, true, s))) return st;
   const GmgLevel<T>& C = M.lv[l + 1];
-  { note_launch(); gmg_restrict<T><<<grid_for(C.g.n_red), kThreads, 0, s>>>(L.g, C.g, L.res, l == 0 ? M.mask : nullptr, C.b); }
+  { note_launch(); gmg_restrict<T><<<grid_for(C.g.n_red), kThreads, 0, s>>>(L.g, C.g, L.res, l == 0 ? M.mask : nullptr, C.b, M.guard); }
   if ((st = vcycle(M, l + 1, s))) return st;
-  { note_launch(); gmg_prolong_add<T><<<grid_for(L.g.n_red), kThreads, 0, s>>>(L.g, C.g, C.x, l == 0 ? M.mask : nullptr, L.x); }
+  { note_launch(); gmg_prolong_add<T><<<grid_for(L.g.n_red), kThreads, 0, s>>>(L.g, C.g, C.x, l == 0 ? M.mask : nullptr, L.x, M.guard); }
   if ((st = chebyshev(M, l, M.deg, false, false, s))) return st;
   if (l > 0 && (st = remove_mean(M, l, L.x, s))) return st;
   return last_launch_status();
@@ -744,21 +756,25 @@ static int gmg_setup(Gmg<T>& M, const VoxMat<T>& mat, const uint8_t* slot, const
 }
 
 template <typename T>
-__global__ void gmg_copy(int n, const T* __restrict__ a, T* __restrict__ b) {
+__global__ void gmg_copy(int n, const T* __restrict__ a, T* __restrict__ b, const int* guard) {
+  if (guard && *guard == 0) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
 }
 
 // z = M^-1 r: V-cycle on the fluctuation rows, Jacobi on the free E rows.
 template <typename T>
-static int gmg_precond_apply(const void* ctx, const T* r, T* z, const int*, cudaStream_t s) {
+static int gmg_precond_apply(const void* ctx, const T* r, T* z, const int* guard, cudaStream_t s) {
   const Gmg<T>& M = *static_cast<const Gmg<T>*>(ctx);
   const GmgLevel<T>& L = M.lv[0];
   const int n = L.n;
   int st;
-  { note_launch(); gmg_copy<T><<<grid_for(n), kThreads, 0, s>>>(n, r, L.b); }
-  if ((st = vcycle(M, 0, s))) return st;
-  { note_launch(); gmg_copy<T><<<grid_for(n), kThreads, 0, s>>>(n, L.x, z); }
-  { note_launch(); gmg_eblock<T><<<1, 32, 0, s>>>(3 * L.g.n_red, r, L.diag, M.fmask, z); }
+  // every V-cycle kernel turns into a no-op once the Krylov solve has converged
+  Gmg<T> Mg = M;
+  Mg.guard = guard;
+  { note_launch(); gmg_copy<T><<<grid_for(n), kThreads, 0, s>>>(n, r, L.b, guard); }
+  if ((st = vcycle(Mg, 0, s))) return st;
+  { note_launch(); gmg_copy<T><<<grid_for(n), kThreads, 0, s>>>(n, L.x, z, guard); }
+  { note_launch(); gmg_eblock<T><<<1, 32, 0, s>>>(3 * L.g.n_red, r, L.diag, M.fmask, z, guard); }
   return last_launch_status();
 }
 
@@ -773,6 +789,18 @@ namespace phastb {
 
 bool valid_vox(const phastb_voxel_grid* g);
 bool valid_mat(const phastb_voxel_material* m);
+
+// Multigrid-preconditioned PCG looks at its state every gmg_check() iterations
+// (one captured chunk); iterations past convergence cost only no-op launches.
+// PHASTB_GMG_CHECK overrides the default interval.
+static int gmg_check() {
+  static const int v = [] {
+    const char* e = std::getenv("PHASTB_GMG_CHECK");
+    const int k = e ? std::atoi(e) : 0;
+    return k >= 1 && k <= 64 ? k : 1;
+  }();
+  return v;
+}
 
 template <typename T>
 struct MechOpT {
@@ -838,6 +866,7 @@ struct ExLayout {
   PcgWs<double> w64;
   PcgWs<float> w32;
   double *xc, *bf, *r64;
+  double *d64, *x64;  // workspace copies of the damage field and the FP64 iterate (stable graph pointers)
   float *d32, *r32, *dx32, *inv32;
   void* scratch64;
   RedWs rw;
@@ -858,6 +887,8 @@ static ExLayout ex_layout(const VoxGeom& v, const phastb_mech_opts& o, char* bas
   L.xc = reinterpret_cast<double*>(take(sizeof(double) * n));
   L.bf = reinterpret_cast<double*>(take(sizeof(double) * n));
   L.r64 = reinterpret_cast<double*>(take(sizeof(double) * n));
+  L.d64 = reinterpret_cast<double*>(take(sizeof(double) * v.n_red));
+  L.x64 = reinterpret_cast<double*>(take(sizeof(double) * n));
   L.scratch64 = take(h8_scratch_bytes(v, PHASTB_F64));
   L.rw = red_ws(take(red_ws_bytes()));
   if (!o.mixed) {
@@ -933,8 +964,12 @@ int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_mater
   RedWs sw = red_ws(static_cast<char*>(L.scratch64) + h8_scratch_bytes(v, PHASTB_F64) - red_ws_bytes());
   if ((st = red_ws_reset(sw, s))) return st;
   { note_launch(); ex_setup_kernel<<<G, kThreads, 0, s>>>(n, fixed, fixed_values, x0, L.xc, x_out); }
-  MechOpT<double> full{v, m64, slot, d, nullptr, L.scratch64};
-  MechOpT<double> freeop{v, m64, slot, d, fixed, L.scratch64};
+  // captured PCG chunks read the damage field and the iterate from the workspace
+  if (d && (st = cuda_status(cudaMemcpyAsync(L.d64, d, sizeof(double) * v.n_red, cudaMemcpyDeviceToDevice, s))))
+    return st;
+  const double* dd = d ? L.d64 : nullptr;
+  MechOpT<double> full{v, m64, slot, dd, nullptr, L.scratch64};
+  MechOpT<double> freeop{v, m64, slot, dd, fixed, L.scratch64};
   if ((st = mech_op_t<double>(&full, L.xc, L.r64, nullptr, s))) return st;
   { note_launch(); ex_rhs_kernel<<<G, kThreads, 0, s>>>(n, fixed, nullptr, L.r64, L.bf, L.rw); }
   if ((st = last_launch_status())) return st;
@@ -957,19 +992,26 @@ int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_mater
     // FP64 PCG with the FP64 V-cycle (precond = 1) or Jacobi (0)
     PcgResult pr{};
     if (o->precond) {
-      if ((st = gmg_setup<double>(L.g64, m64, slot, d, fixed, o->smooth_degree, o->coarse_degree, o->power_iters,
+      if ((st = gmg_setup<double>(L.g64, m64, slot, dd, fixed, o->smooth_degree, o->coarse_degree, o->power_iters,
                                   o->lmax_safety, lmax_io, s)))
         return st;
       Precond<double> M{gmg_precond_apply<double>, &L.g64, sizeof(L.g64)};
-      if ((st = pcg_run<double>(A64, n, L.w64, L.bf, nullptr, &M, x_out, thr, maxiter, 1, PCG_FREEZE, 0.0, &pr, s)))
+      if ((st = cuda_status(cudaMemcpyAsync(L.x64, x_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, s))))
+        return st;
+      if ((st = pcg_run<double>(A64, n, L.w64, L.bf, nullptr, &M, L.x64, thr, maxiter, gmg_check(), PCG_FREEZE, 0.0,
+                                &pr, s)))
         return st;
     } else {
-      if ((st = h8_mech_diag_t<double>(v, m64, slot, nullptr, d, L.r64, L.scratch64, s))) return st;
+      if ((st = h8_mech_diag_t<double>(v, m64, slot, nullptr, dd, L.r64, L.scratch64, s))) return st;
       { note_launch(); gmg_invert<double><<<G, kThreads, 0, s>>>(n, L.r64, fixed, L.r64); }
-      if ((st = pcg_run<double>(A64, n, L.w64, L.bf, L.r64, nullptr, x_out, thr, maxiter, check_every, PCG_FREEZE,
+      if ((st = cuda_status(cudaMemcpyAsync(L.x64, x_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, s))))
+        return st;
+      if ((st = pcg_run<double>(A64, n, L.w64, L.bf, L.r64, nullptr, L.x64, thr, maxiter, check_every, PCG_FREEZE,
                                 0.0, &pr, s)))
         return st;
     }
+    if ((st = cuda_status(cudaMemcpyAsync(x_out, L.x64, sizeof(double) * n, cudaMemcpyDeviceToDevice, s))))
+      return st;
     { note_launch(); ex_where_kernel<<<G, kThreads, 0, s>>>(n, fixed, L.xc, x_out); }
     if ((st = last_launch_status())) return st;
     if (info) { info[0] = pr.iterations; info[1] = pr.converged; }
@@ -980,7 +1022,7 @@ int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_mater
   }
   // FP32 inner PCG (FP64 dot products) + FP64 iterative refinement
   const VoxMat<float> m32 = make_vox_mat<float>(*m);
-  { note_launch(); gmg_convert<double, float><<<grid_for(v.n_red), kThreads, 0, s>>>(v.n_red, d, L.d32); }
+  { note_launch(); gmg_convert<double, float><<<grid_for(v.n_red), kThreads, 0, s>>>(v.n_red, dd, L.d32); }
   void* scratch32 = L.g32.scratch;
   if (o->precond) {
     if ((st = gmg_setup<float>(L.g32, m32, slot, L.d32, fixed, o->smooth_degree, o->coarse_degree, o->power_iters,
@@ -999,26 +1041,30 @@ int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_mater
   int total = 0, converged = 0;
   double rn = bn;
   for (int k = 0; k < o->max_refine && total < maxiter; ++k) {
+    // FP64 residual; its norm is checked on the device by the inner solve's
+    // start (no host round trip): when it already meets thr the inner solve
+    // does nothing and reports outer_done
     if ((st = mech_op_t<double>(&freeop, x_out, L.r64, nullptr, s))) return st;
     { note_launch(); ex_rhs_kernel<<<G, kThreads, 0, s>>>(n, fixed, L.bf, L.r64, L.r64, L.rw); }
-    if ((st = last_launch_status())) return st;
-    double rr;
-    if ((st = red_ws_fetch(L.rw, &rr, 1, s))) return st;
-    rn = std::sqrt(rr);
-    if (!std::isfinite(rn)) return PHASTB_NONFINITE;
-    if (rn <= thr) {
-      converged = 1;
-      break;
-    }
     { note_launch(); gmg_convert<double, float><<<G, kThreads, 0, s>>>(n, L.r64, L.r32); }
     if ((st = cuda_status(cudaMemsetAsync(L.dx32, 0, sizeof(float) * n, s)))) return st;
     PcgResult pr{};
-    const double thr_in = std::max(o->inner_rtol * rn, 0.5 * thr);
-    if ((st = pcg_run<float>(A32, n, L.w32, L.r32, o->precond ? nullptr : L.inv32, o->precond ? &M32 : nullptr,
-                             L.dx32, thr_in, maxiter - total, o->precond ? 1 : check_every, PCG_FREEZE, 0.0, &pr, s)))
+    PcgThreshold tin;
+    tin.abs = 0.5 * thr;       // never resolve the correction far below the outer target
+    tin.rel = o->inner_rtol;   // relative to the FP32 right-hand side, i.e. the FP64 residual
+    tin.outer_rr = L.rw.out;
+    tin.outer_thr = thr;
+    if ((st = pcg_run_thr<float>(A32, n, L.w32, L.r32, o->precond ? nullptr : L.inv32, o->precond ? &M32 : nullptr,
+                                 L.dx32, tin, maxiter - total, o->precond ? gmg_check() : check_every, PCG_FREEZE, &pr,
+                                 s)))
       return st;
+    rn = pr.outer_rnorm;
+    if (pr.outer_done) {
+      converged = 1;
+      break;
+    }
+    if (!std::isfinite(rn) || pr.nonfinite) return PHASTB_NONFINITE;
     total += pr.iterations;
-    if (pr.nonfinite) return PHASTB_NONFINITE;
     if (pr.breakdown) return PHASTB_BREAKDOWN;
     { note_launch(); ex_add_kernel<<<G, kThreads, 0, s>>>(n, L.dx32, x_out); }
   }

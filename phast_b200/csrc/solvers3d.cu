@@ -245,7 +245,8 @@ size_t phastb_h8_mech_solve_workspace_bytes(const phastb_voxel_grid* g, int dtyp
   const VoxGeom v = make_vox_geom(*g);
   const int n = 3 * v.n_red + 6;
   return pcg_ws_bytes<double>(n) + 3 * align_up(sizeof(double) * (size_t)n) + h8_scratch_bytes(v, PHASTB_F64) +
-         red_ws_bytes();
+         red_ws_bytes() + align_up(sizeof(double) * (size_t)n) + align_up(sizeof(double) * (size_t)v.n_red) +
+         align_up(sizeof(double) * 8 * (size_t)v.n_elem);
 }
 
 int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
@@ -278,6 +279,19 @@ int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material
   int st;
   if ((st = red_ws_reset(rw, s))) return st;
   if ((st = red_ws_reset(sw, s))) return st;
+  // the captured PCG chunks read the iterate, d and g(d) from the workspace, so
+  // repeated solves replay one graph however the caller allocates its tensors
+  char* q = static_cast<char*>(redb) + red_ws_bytes();
+  double* xw = reinterpret_cast<double*>(q);
+  double* dw = reinterpret_cast<double*>(q + vb);
+  double* gw = reinterpret_cast<double*>(q + vb + align_up(sizeof(double) * (size_t)v.n_red));
+  if (d && (st = cuda_status(cudaMemcpyAsync(dw, d, sizeof(double) * v.n_red, cudaMemcpyDeviceToDevice, s))))
+    return st;
+  if (gq && (st = cuda_status(cudaMemcpyAsync(gw, gq, sizeof(double) * 8 * (size_t)v.n_elem,
+                                               cudaMemcpyDeviceToDevice, s))))
+    return st;
+  d = d ? dw : nullptr;
+  gq = gq ? gw : nullptr;
   // diagonal of A(g) into invd, then the constrained setup
   if ((st = h8_mech_diag_t<double>(v, mm, slot, gq, d, invd, scratch, s))) return st;
   { note_launch(); constrained_setup_kernel<<<G, kThreads, 0, s>>>(n, fixed, fixed_values, x0, xc, x_out, invd); }
@@ -300,9 +314,10 @@ int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material
   MechCtx free_ctx{v, mm, slot, gq, d, fixed, scratch};
   LinOp<double> A{mech_op, &free_ctx, sizeof(free_ctx), mech_op_dot, h8_apply_dot_slot(v, 8, scratch)};
   PcgResult pr{};
-  if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, x_out, thr, maxiter, check_every, PCG_FREEZE, 0.0, &pr, s)))
+  if ((st = cuda_status(cudaMemcpyAsync(xw, x_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, s)))) return st;
+  if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, xw, thr, maxiter, check_every, PCG_FREEZE, 0.0, &pr, s)))
     return st;
-  { note_launch(); where_kernel<<<G, kThreads, 0, s>>>(n, fixed, x_out, xc, x_out); }
+  { note_launch(); where_kernel<<<G, kThreads, 0, s>>>(n, fixed, xw, xc, x_out); }
   if ((st = last_launch_status())) return st;
   if (info) { info[0] = pr.iterations; info[1] = pr.converged; }
   if (rinfo) rinfo[1] = pr.rnorm;
@@ -316,7 +331,8 @@ size_t phastb_h8_box_kkt_workspace_bytes(const phastb_voxel_grid* g) {
   const VoxGeom v = make_vox_geom(*g);
   const int n = v.n_red;
   return pcg_ws_bytes<double>(n) + 6 * align_up(sizeof(double) * (size_t)n) + 4 * align_up((size_t)n) +
-         h8_scratch_bytes(v, PHASTB_F64) + red_ws_bytes();
+         h8_scratch_bytes(v, PHASTB_F64) + red_ws_bytes() + align_up(sizeof(double) * (size_t)n) +
+         align_up(sizeof(double) * 8 * (size_t)v.n_elem) + red_ws_bytes();
 }
 
 int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
@@ -350,57 +366,72 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
   RedWs rw = red_ws(scratch + h8_scratch_bytes(v, PHASTB_F64));
   // the action's own reduction ticket (x . y of the fused CG) lives inside the scratch
   RedWs aw = red_ws(scratch + align_up(24 * sizeof(double) * (size_t)v.n_elem));
+  // the iterate and the history live in the workspace, so the captured PCG
+  // chunks see the same pointers on every call (one graph per workspace)
+  char* q = scratch + h8_scratch_bytes(v, PHASTB_F64) + red_ws_bytes();
+  double* xd = reinterpret_cast<double*>(q);
+  double* Hw = H ? reinterpret_cast<double*>(q + vb) : nullptr;
+  // the KKT audit reduces into its own workspace so one host read serves both checks
+  RedWs kw = red_ws(q + vb + align_up(sizeof(double) * 8 * (size_t)v.n_elem));
   const int G = grid_for(n);
   int st;
   if ((st = red_ws_reset(rw, s))) return st;
   if ((st = red_ws_reset(aw, s))) return st;
-  if ((st = h8_damage_launch(v, mm, slot, 1, nullptr, H, scale, rhs, nullptr, scratch, nullptr, s))) return st;
+  if ((st = red_ws_reset(kw, s))) return st;
+  if (H && (st = cuda_status(cudaMemcpyAsync(Hw, H, sizeof(double) * 8 * (size_t)v.n_elem,
+                                              cudaMemcpyDeviceToDevice, s))))
+    return st;
+  auto finish = [&](int code) -> int {
+    const int e = cuda_status(cudaMemcpyAsync(d_out, xd, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    return e ? e : code;
+  };
+  if ((st = h8_damage_launch(v, mm, slot, 1, nullptr, Hw, scale, rhs, nullptr, scratch, nullptr, s))) return st;
   if (!H && (st = cuda_status(cudaMemsetAsync(rhs, 0, sizeof(double) * n, s)))) return st;
-  if ((st = h8_damage_launch(v, mm, slot, 2, nullptr, H, scale, diag, nullptr, scratch, nullptr, s))) return st;
+  if ((st = h8_damage_launch(v, mm, slot, 2, nullptr, Hw, scale, diag, nullptr, scratch, nullptr, s))) return st;
   if ((st = cuda_status(cudaMemsetAsync(la, 0, 2 * ub, s)))) return st;
-  DamageCtx full{v, mm, slot, H, scale, nullptr, scratch};
+  DamageCtx full{v, mm, slot, Hw, scale, nullptr, scratch};
   int total = 0;
   const double* cinit = initial;
   for (int ai = 1; ai <= max_active; ++ai) {
-    { note_launch(); kkt_setup_kernel<<<G, kThreads, 0, s>>>(n, la, ua, lower, upper, cinit, diag, fixed, known, d_out, invd); }
+    { note_launch(); kkt_setup_kernel<<<G, kThreads, 0, s>>>(n, la, ua, lower, upper, cinit, diag, fixed, known, xd, invd); }
     // b_f = where(free, rhs - A known, 0)
     if ((st = damage_op(&full, known, w.Ap, nullptr, s))) return st;
     { note_launch(); constrained_rhs_kernel<<<G, kThreads, 0, s>>>(n, fixed, rhs, w.Ap, bf, rw); }
     if ((st = last_launch_status())) return st;
     // Dirichlet PCG on the free set: tolerance relative to max(||r0||, 1)
-    DamageCtx fctx{v, mm, slot, H, scale, fixed, scratch};
+    DamageCtx fctx{v, mm, slot, Hw, scale, fixed, scratch};
     LinOp<double> A{damage_op, &fctx, sizeof(fctx), damage_op_dot, h8_apply_dot_slot(v, 8, scratch)};
     PcgResult pr{};
-    if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, d_out, -lin_tol, max_lin, 10, PCG_STRICT, 0.0, &pr,
-                              s)))
+    if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, xd, -lin_tol, max_lin, 10, PCG_STRICT, 0.0, &pr, s)))
       return st;
     // candidate = where(fixed, known, x)
-    { note_launch(); where_kernel<<<G, kThreads, 0, s>>>(n, fixed, d_out, known, d_out); }
+    { note_launch(); where_kernel<<<G, kThreads, 0, s>>>(n, fixed, xd, known, xd); }
     total += pr.iterations;
-    if (pr.nonfinite) return PHASTB_NONFINITE;
-    if (pr.breakdown) return PHASTB_BREAKDOWN;
+    if (pr.nonfinite) return finish(PHASTB_NONFINITE);
+    if (pr.breakdown) return finish(PHASTB_BREAKDOWN);
     // gradient, active-set change
-    if ((st = damage_op(&full, d_out, w.Ap, nullptr, s))) return st;
-    { note_launch(); kkt_update_kernel<<<G, kThreads, 0, s>>>(n, fixed, d_out, w.Ap, rhs, lower, upper, kkt_tol, la, ua, grad, rw); }
+    if ((st = damage_op(&full, xd, w.Ap, nullptr, s))) return st;
+    { note_launch(); kkt_update_kernel<<<G, kThreads, 0, s>>>(n, fixed, xd, w.Ap, rhs, lower, upper, kkt_tol, la, ua, grad, rw); }
+    // the audit of the updated sets is only read when nothing changed, but running
+    // it now lets one synchronisation fetch both results
+    { note_launch(); kkt_audit_kernel<<<G, kThreads, 0, s>>>(n, xd, grad, lower, upper, la, ua, kkt_tol, kw); }
     if ((st = last_launch_status())) return st;
-    double changes;
-    if ((st = red_ws_fetch(rw, &changes, 1, s))) return st;
+    double changes, a[4];
+    if ((st = cuda_status(cudaMemcpyAsync(&changes, rw.out, sizeof(double), cudaMemcpyDeviceToHost, s)))) return st;
+    if ((st = cuda_status(cudaMemcpyAsync(a, kw.out, sizeof(a), cudaMemcpyDeviceToHost, s)))) return st;
+    if ((st = cuda_status(cudaStreamSynchronize(s)))) return st;
     if (info) { info[0] = total; info[1] = ai; info[2] = 0; }
-    if (!pr.converged) return PHASTB_NONCONVERGED;
+    if (!pr.converged) return finish(PHASTB_NONCONVERGED);
     if (changes == 0.0) {
-      { note_launch(); kkt_audit_kernel<<<G, kThreads, 0, s>>>(n, d_out, grad, lower, upper, la, ua, kkt_tol, rw); }
-      if ((st = last_launch_status())) return st;
-      double a[4];
-      if ((st = red_ws_fetch(rw, a, 4, s))) return st;
       const int ok = a[0] == 0.0 && a[1] <= kkt_tol && a[2] <= kkt_tol && a[3] <= kkt_tol;
       if (info) info[2] = ok;
-      return ok ? PHASTB_OK : PHASTB_NONCONVERGED;
+      return finish(ok ? PHASTB_OK : PHASTB_NONCONVERGED);
     }
-    // next set starts from this candidate (copy so the solve can overwrite d_out)
-    if ((st = cuda_status(cudaMemcpyAsync(grad, d_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, s)))) return st;
+    // next set starts from this candidate (copy so the solve can overwrite the iterate)
+    if ((st = cuda_status(cudaMemcpyAsync(grad, xd, sizeof(double) * n, cudaMemcpyDeviceToDevice, s)))) return st;
     cinit = grad;
   }
-  return PHASTB_NONCONVERGED;
+  return finish(PHASTB_NONCONVERGED);
 }
 
 int phastb_h8_stagger_change(int n_u, const double* x_new, const double* x_old, int n_d, const double* d_new,

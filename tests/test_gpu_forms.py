@@ -100,3 +100,31 @@ def test_staggered_increments_forms_golden(name, kw):
         assert rel(state.x.cpu(), g["x"][k]) < 1e-6
         assert rel(state.d.cpu(), g["d"][k]) < 1e-6
         assert rel(state.macro_stress, g["sigma"][k]) < 1e-6
+
+
+def test_device_side_loop_matches_chunked_loop():
+    """PHASTB_DEVICE_LOOP=1 (conditional-WHILE graphs) gives the chunked loop's solution."""
+    import os
+    import subprocess
+    import sys
+    code = (
+        "import sys; sys.path.insert(0, 'tests'); sys.path.insert(0, '.');"
+        "import torch, numpy as np; from test_gpu_forms import cell, smooth_damage;"
+        "from phast_b200 import solid3d as s3;"
+        "op = cell(16); d = smooth_damage(op, 3); m, v = op.mech_fixed_mask(), op.mech_fixed_values(0.01);"
+        "x, i = s3.solve_constrained(op, fixed_mask=m, fixed_values=v, d=d, rtol=1e-10, maxiter=20000);"
+        "y, j = s3.solve_constrained_form(op, s3.MechForm(precond='gmg', mixed=True), fixed_mask=m, fixed_values=v,"
+        " d=d, rtol=1e-10, maxiter=20000);"
+        "np.save(sys.argv[1], np.stack([x.cpu().numpy(), y.cpu().numpy()]))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = {}
+    for flag in ("0", "1"):
+        path = os.path.join(root, "gpurun_out" if os.path.isdir(os.path.join(root, "gpurun_out")) else "",
+                            f"_loop_{flag}.npy")
+        env = dict(os.environ, PHASTB_DEVICE_LOOP=flag)
+        subprocess.run([sys.executable, "-c", code, path], check=True, cwd=root, env=env, timeout=600)
+        outs[flag] = np.load(path)
+        os.remove(path)
+    for k in range(2):
+        a, b = outs["0"][k], outs["1"][k]
+        assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(a)
