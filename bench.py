@@ -245,7 +245,10 @@ def run_ours(args, rank, world, device):
         torch.distributed.barrier()
     lib.phastb_launch_count_reset()
     clocks = Clocks(torch.cuda.current_device())
+    # brackets the timed steps for a profiler started with --profile-from-start off (no-op otherwise)
+    torch.cuda.profiler.start()
     total_ms, st_c, counts, clk = run_steps(op, chosen, snap, meta, args.steps, flush, device, clocks)
+    torch.cuda.profiler.stop()
     launches = lib.phastb_launch_count()
     t = torch.tensor([total_ms], dtype=torch.float64, device=device)
     if world > 1:

@@ -25,6 +25,63 @@ __device__ __forceinline__ int wrap_elem(int c, int n, int periodic) {
   return (c >= 0 && c < n) ? c : -1;
 }
 
+// Asynchronous global -> shared copies (cp.async, 16 bytes, L2 only).  A thread
+// stages the per-element arrays of the NEXT element layer into its own slot of
+// a two-buffer shared array and waits for its own group before reading it, so
+// no barrier is needed for these slots; both addresses must be 16-byte aligned.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+// One word (4 or 8 bytes, naturally aligned) with cp.async.
+template <typename T>
+__device__ __forceinline__ void cp_async_word(T* smem, const T* gmem) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "cp.async copies 4, 8 or 16 bytes");
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(sizeof(T)) : "memory");
+}
+__device__ __forceinline__ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Staged per-element arrays live chunk-major in shared memory: chunk c (16
+// bytes) of the element owned by thread t sits at base + (c * n + t) * 16, so a
+// warp reading one chunk touches consecutive 16-byte units (no bank conflicts).
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using type = float4;
+};
+template <>
+struct Vec16<double> {
+  using type = double2;
+};
+
+// Copies n_chunks 16-byte chunks of src into chunks c0.. of thread t's column.
+__device__ __forceinline__ void stage_chunks(unsigned char* base, int n, int t, int c0, const void* src,
+                                             int n_chunks) {
+  for (int c = 0; c < n_chunks; ++c)
+    cp_async16(base + ((size_t)(c0 + c) * n + t) * 16, static_cast<const unsigned char*>(src) + 16 * c);
+}
+
+// Reads W words of thread t's staged column (W * sizeof(T) a multiple of 16).
+template <typename T, int W>
+__device__ __forceinline__ void load_chunks(const unsigned char* base, int n, int t, T (&out)[W]) {
+  using V = typename Vec16<T>::type;
+  constexpr int per = 16 / sizeof(T);
+#pragma unroll
+  for (int c = 0; c < W / per; ++c) {
+    const V v = *reinterpret_cast<const V*>(base + ((size_t)c * n + t) * 16);
+    const T* pv = reinterpret_cast<const T*>(&v);
+#pragma unroll
+    for (int j = 0; j < per; ++j) out[c * per + j] = pv[j];
+  }
+}
+
 // Node layer kn of the brick with its one-node halo, (ox+2)(oy+2) nodes, is
 // staged in two steps so the global loads of layer k+2 are in flight while
 // layer k's elements are computed: stage_load reads a thread's (at most two)
@@ -184,6 +241,18 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
   T* nb = reinterpret_cast<T*>(smem_raw);  // [3 buffers][4 fields][nt]
   T* FL = nb + 12 * nt;                    // [4 corners][3 comps][exy], lower face (oz = 0)
   T* FU = FL + 12 * exy;                   // upper face (oz = 1)
+  // staged by cp.async, two buffers each: kCoefQP (lam_q, mu_q) of this thread's
+  // element one element layer ahead, chunk-major [2][chunks][exy]; kModeCheb
+  // (res, invd, xs) of this thread's owned node, [2][9][ox*oy], copied while the
+  // layer's elements are computed
+  constexpr bool STAGE = COEF == kCoefQP || CHEB;
+  constexpr int kQChunks = kStageQP * (int)sizeof(T) / 16;
+  size_t off_qp = 0, off_cheb = 0;
+  tile_layout<T>(ox, oy, COEF == kCoefQP, CHEB, &off_qp, &off_cheb);
+  unsigned char* QS = smem_raw + off_qp;
+  T* CS = reinterpret_cast<T*>(smem_raw + off_cheb);
+  const int oxy = ox * oy;
+  const bool q_async = COEF == kCoefQP && aligned16(a.lam_q) && aligned16(a.mu_q);
   const int tid = threadIdx.x;
   const T w = T(g.w);
   const T c1 = T(a.c1), c2 = T(a.c2);
@@ -219,6 +288,43 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
     return (__ldg(a.mask + 3 * n) ? 1 : 0) | (__ldg(a.mask + 3 * n + 1) ? 2 : 0) |
            (__ldg(a.mask + 3 * n + 2) ? 4 : 0);
   };
+  // Staging commit groups, in order: per step kk one Chebyshev group (node layer
+  // ke) then one moduli group (element layer ke + 1), each possibly empty, so the
+  // number of groups committed after any one of them is fixed.
+  // kCoefQP: copies element layer ke's (lam_q, mu_q) into buffer `buf`.
+  auto stage_qp = [&](int i0, int j0, int ke, int buf, bool live) {
+    if constexpr (STAGE) {
+      if (COEF == kCoefQP && live && q_async && is_elem) {
+        const int gi = wrap_elem(i0 - 1 + ea, g.nx, g.px);
+        const int gj = wrap_elem(j0 - 1 + eb, g.ny, g.py);
+        const int gk = wrap_elem(ke, g.nz, g.pz);
+        if (gi >= 0 && gj >= 0 && gk >= 0) {
+          const size_t e = (size_t)gi + (size_t)g.nx * ((size_t)gj + (size_t)g.ny * gk);
+          unsigned char* dst = QS + (size_t)buf * kQChunks * exy * 16;
+          stage_chunks(dst, exy, tid, 0, a.lam_q + 8 * e, kQChunks / 2);
+          stage_chunks(dst, exy, tid, kQChunks / 2, a.mu_q + 8 * e, kQChunks / 2);
+        }
+      }
+      cp_async_commit();
+    }
+  };
+  // kModeCheb: copies (res, invd, xs) of the owned node in node layer kn into buffer `buf`.
+  auto stage_cheb = [&](int i0, int j0, int kn, int buf, bool live) {
+    if constexpr (STAGE) {
+      const int gi = i0 + ni, gj = j0 + nj;
+      if (CHEB && live && is_node && gi < g.rx && gj < g.ry) {
+        const size_t n3 = 3 * ((size_t)gi + (size_t)g.rx * ((size_t)gj + (size_t)g.ry * kn));
+        T* dst = CS + (size_t)buf * 9 * oxy + tid;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          cp_async_word(dst + c * oxy, a.res + n3 + c);
+          cp_async_word(dst + (3 + c) * oxy, a.invd + n3 + c);
+          cp_async_word(dst + (6 + c) * oxy, a.xs + n3 + c);
+        }
+      }
+      cp_async_commit();
+    }
+  };
 
   for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const int tz = tile / tiles_xy, txy = tile - tz * tiles_xy;
@@ -232,6 +338,7 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
     stage_store(nt, pf, nb);
     stage_load(g, x, d, i0, j0, k0, ntx, nt, pf);
     int sl_next = elem_slot(i0, j0, k0 - 1);
+    stage_qp(i0, j0, k0 - 1, 0, true);
     int mk_next = node_mask(i0, j0, k0), mk_cur = 0;
     const int K = k1 - k0;
     for (int kk = 0; kk <= K; ++kk) {
@@ -243,6 +350,11 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
       if (kk < K) {
         stage_load(g, x, d, i0, j0, ke + 2, ntx, nt, pf);
         sl_next = elem_slot(i0, j0, ke + 1);
+      }
+      if constexpr (STAGE) {
+        stage_cheb(i0, j0, ke, kk & 1, kk >= 1);
+        stage_qp(i0, j0, ke + 1, (kk + 1) & 1, kk < K);
+        cp_async_wait<2>();  // this thread's moduli of element layer ke have landed
       }
       if (kk >= 1) {
         mk_cur = mk_next;
@@ -366,9 +478,17 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
               for (int k = 0; k < 6; ++k) sg[k] *= gw;
             });
           } else {
-            const T* lq = a.lam_q + 8 * e;
-            const T* mq = a.mu_q + 8 * e;
-            qp_loop([&](const T* ep, int q, T* sg) { iso_stress(ep, __ldg(lq + q) * w, __ldg(mq + q) * w, sg); });
+            T lm[kStageQP];  // lam_q[0..7], mu_q[0..7]
+            if (q_async) {
+              load_chunks<T, kStageQP>(QS + (size_t)(kk & 1) * kQChunks * exy * 16, exy, tid, lm);
+            } else {
+#pragma unroll
+              for (int q = 0; q < 8; ++q) {
+                lm[q] = __ldg(a.lam_q + 8 * e + q);
+                lm[8 + q] = __ldg(a.mu_q + 8 * e + q);
+              }
+            }
+            qp_loop([&](const T* ep, int q, T* sg) { iso_stress(ep, lm[q] * w, lm[8 + q] * w, sg); });
           }
           if (EROWS && own) {
 #pragma unroll
@@ -400,6 +520,7 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
           }
       }
       __syncthreads();
+      if constexpr (STAGE) cp_async_wait<1>();  // this thread's (res, invd, xs) of node layer ke
       // ---- node phase: node layer ke = lower faces of this layer + upper faces of the previous
       if (is_node) {
         const int e11 = (ni + 1) + ex * (nj + 1), e01 = ni + ex * (nj + 1);
@@ -422,11 +543,12 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
             const size_t i = 3 * n + c;
             const T xin = b0[c * nt + (nj + 1) * ntx + ni + 1];
             if (CHEB) {
-              const T r = a.res[i] - v;
+              const T* cs = CS + (size_t)(kk & 1) * 9 * oxy + tid;
+              const T r = cs[c * oxy] - v;
               a.res[i] = r;
-              const T dn = c1 * xin + c2 * __ldg(a.invd + i) * r;
+              const T dn = c1 * xin + c2 * cs[(3 + c) * oxy] * r;
               a.d_out[i] = dn;
-              a.xs[i] += dn;
+              a.xs[i] = cs[(6 + c) * oxy] + dn;
             } else {
               if (a.y) a.y[i] = v;
               if (DOT) tacc[kOutDot] += xin * v;
@@ -493,6 +615,9 @@ __global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_kernel(DTileArgs<
   T* nb = reinterpret_cast<T*>(smem_raw);  // [3 buffers][nt]
   T* FL = nb + 3 * nt;                     // [4 corners][exy]
   T* FU = FL + 4 * exy;
+  // H of this thread's element, staged one element layer ahead, chunk-major [2][chunks][exy]
+  constexpr int kHChunks = kStageH * (int)sizeof(T) / 16;
+  unsigned char* HS = smem_raw + tile_stage_offset<T>(nt, exy, 3, 8);
   const int tid = threadIdx.x;
   const T w = T(g.w), ell = T(a.ell), ch = T(2.0 * (1.0 - a.kappa)), sc = T(a.scale);
   const int tiles_x = (g.rx + ox - 1) / ox, tiles_y = (g.ry + oy - 1) / oy;
@@ -501,7 +626,25 @@ __global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_kernel(DTileArgs<
   const int ea = tid % ex, eb = tid / ex;
   const int ni = tid % ox, nj = tid / ox;
   const bool is_elem = tid < exy, is_node = tid < ox * oy;
+  const bool h_async = a.H != nullptr && aligned16(a.H);
   double accd = 0.0;
+  // issues the copy of element layer ke's H into buffer `buf` (one commit group
+  // per call, empty when there is nothing to copy) and returns its material slot
+  auto stage_elem = [&](int i0, int j0, int ke, int buf) -> int {
+    int sl = 0;
+    if (is_elem) {
+      const int gi = wrap_elem(i0 - 1 + ea, g.nx, g.px);
+      const int gj = wrap_elem(j0 - 1 + eb, g.ny, g.py);
+      const int gk = wrap_elem(ke, g.nz, g.pz);
+      if (gi >= 0 && gj >= 0 && gk >= 0) {
+        const size_t e = (size_t)gi + (size_t)g.nx * ((size_t)gj + (size_t)g.ny * gk);
+        sl = __ldg(a.slot + e);
+        if (h_async) stage_chunks(HS + (size_t)buf * kHChunks * exy * 16, exy, tid, 0, a.H + kStageH * e, kHChunks);
+      }
+    }
+    cp_async_commit();
+    return sl;
+  };
   auto stage1 = [&](int i0, int j0, int kn, T (&r)[2]) {
     const int gk = wrap_node(kn, g.nz, g.rz, g.pz);
 #pragma unroll
@@ -533,13 +676,21 @@ __global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_kernel(DTileArgs<
     __syncthreads();
     store1(pf, nb);
     stage1(i0, j0, k0, pf);
+    int sl_next = stage_elem(i0, j0, k0 - 1, 0);
     const int K = k1 - k0;
     for (int kk = 0; kk <= K; ++kk) {
       const int ke = k0 - 1 + kk;
       T* b0 = nb + nt * (kk % 3);
       T* b1 = nb + nt * ((kk + 1) % 3);
       store1(pf, b1);
-      if (kk < K) stage1(i0, j0, ke + 2, pf);
+      const int sl = sl_next;
+      if (kk < K) {
+        stage1(i0, j0, ke + 2, pf);
+        sl_next = stage_elem(i0, j0, ke + 1, (kk + 1) & 1);
+        cp_async_wait<1>();  // this thread's copy of layer ke has landed
+      } else {
+        cp_async_wait<0>();
+      }
       __syncthreads();
       if (is_elem) {
         const int gi = wrap_elem(i0 - 1 + ea, g.nx, g.px);
@@ -548,7 +699,7 @@ __global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_kernel(DTileArgs<
         T out[8];
         if (gi >= 0 && gj >= 0 && gk >= 0) {
           const size_t e = (size_t)gi + (size_t)g.nx * ((size_t)gj + (size_t)g.ny * gk);
-          const T Gc = a.Gc[__ldg(a.slot + e)];
+          const T Gc = a.Gc[sl];
           T dd[8], dq[8];
 #pragma unroll
           for (int L = 0; L < 8; ++L) {
@@ -556,12 +707,16 @@ __global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_kernel(DTileArgs<
             dd[L] = bb[(eb + ((L >> 1) & 1)) * ntx + ea + (L & 1)];
           }
           interp_sf(dd, dq);
+          T hq[kStageH];
+          if (h_async) {
+            load_chunks<T, kStageH>(HS + (size_t)(kk & 1) * kHChunks * exy * 16, exy, tid, hq);
+          } else {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) hq[q] = a.H ? __ldg(a.H + 8 * e + q) : T(0);
+          }
           T mq[8];
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const T Hq = a.H ? __ldg(a.H + 8 * e + q) : T(0);
-            mq[q] = w * (Gc / ell + ch * Hq) * dq[q];
-          }
+          for (int q = 0; q < 8; ++q) mq[q] = w * (Gc / ell + ch * hq[q]) * dq[q];
           interp_sf_t(mq, out);
           T Dx[2][2], Dy[2][2], Dz[2][2];
           grad_k(dd, a.k, Dx, Dy, Dz);
@@ -663,7 +818,8 @@ TileShape heuristic_shape(const VoxGeom& g, int word) {
 template <typename T, int COEF, int MODE, int OX, int OY>
 int launch_variant(const TileArgs<T>& a, const VoxMat<T>& m, cudaStream_t s) {
   auto kern = h8_tile_kernel<T, COEF, MODE, OX, OY>;
-  const size_t smem = tile_smem_bytes<T>(a.ts);
+  size_t off_qp = 0, off_cheb = 0;
+  const size_t smem = tile_layout<T>(a.ts.ox, a.ts.oy, COEF == kCoefQP, MODE == kModeCheb, &off_qp, &off_cheb);
   const int threads = tile_threads(a.ts);
   static std::mutex mu;
   static size_t smem_set = 0;
@@ -882,14 +1038,22 @@ int h8_mech_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slo
 template <typename T, int MODE, int OX, int OY>
 int dlaunch_variant(const DTileArgs<T>& a, cudaStream_t s) {
   auto kern = h8_dtile_kernel<T, MODE, OX, OY>;
-  const size_t nt = (size_t)(a.ts.ox + 2) * (a.ts.oy + 2), exy = (size_t)(a.ts.ox + 1) * (a.ts.oy + 1);
-  const size_t smem = sizeof(T) * (3 * nt + 8 * exy);
+  const int nt = (a.ts.ox + 2) * (a.ts.oy + 2), exy = (a.ts.ox + 1) * (a.ts.oy + 1);
+  const size_t smem = tile_stage_offset<T>(nt, exy, 3, 8) + sizeof(T) * 2 * kStageH * (size_t)exy;
   const int threads = tile_threads(a.ts);
   static std::mutex mu;
+  static size_t smem_set = 0;
   static std::map<std::pair<int, size_t>, int> occ;
   int per_sm = 1;
   {
     std::lock_guard<std::mutex> lk(mu);
+    if (smem > smem_set) {
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return PHASTB_ERR_CUDA;
+      }
+      smem_set = smem;
+    }
     auto it = occ.find({threads, smem});
     if (it == occ.end()) {
       int b = 0;

@@ -34,10 +34,31 @@ inline bool tile_ok(const TileShape& t) {
          (t.ox + 2) * (t.oy + 2) <= 2 * tile_threads(t);
 }
 
+// Byte offset, rounded up to 16, of the staged per-element arrays that follow
+// node_words * nt + face_words * exy words of node and face buffers.
 template <typename T>
-inline size_t tile_smem_bytes(const TileShape& t) {
-  const size_t nt = (size_t)(t.ox + 2) * (t.oy + 2), exy = (size_t)(t.ox + 1) * (t.oy + 1);
-  return sizeof(T) * (3 * 4 * nt + 2 * 12 * exy);
+__host__ __device__ inline size_t tile_stage_offset(int nt, int exy, int node_words, int face_words) {
+  return (sizeof(T) * ((size_t)node_words * nt + (size_t)face_words * exy) + 15) / 16 * 16;
+}
+
+// Words per element staged for the next element layer: (lam_q, mu_q) of the
+// per-Gauss-point coarse operators, H of the damage action.
+constexpr int kStageQP = 16, kStageH = 8;
+
+// Dynamic shared memory of h8_tile_kernel: node buffers [3][4][nt] and face
+// buffers [2][12][exy]; then, 16-byte aligned, with per-Gauss-point moduli two
+// element layers of staged (lam_q, mu_q), 16 words per element; then, for a
+// Chebyshev step, two layers of the owned nodes' staged (res, invd, xs) [2][9][ox*oy].
+// Returns the total bytes; *off_qp and *off_cheb receive the two offsets.
+template <typename T>
+__host__ __device__ inline size_t tile_layout(int ox, int oy, bool qp, bool cheb, size_t* off_qp, size_t* off_cheb) {
+  const int nt = (ox + 2) * (oy + 2), exy = (ox + 1) * (oy + 1);
+  size_t o = tile_stage_offset<T>(nt, exy, 12, 24);
+  *off_qp = o;
+  if (qp) o += sizeof(T) * 2 * kStageQP * (size_t)exy;
+  *off_cheb = o;
+  if (cheb) o += (sizeof(T) * 2 * 9 * (size_t)ox * oy + 15) / 16 * 16;
+  return o;
 }
 
 // Result slots of the apply's reduction workspace (ws.out).
