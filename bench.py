@@ -355,9 +355,8 @@ def run_ours(args, rank, world, device):
 
 
 def time_action(op, x, d, flush, n_rep=20):
-    """Mean device time of one elastic action (CUDA events on the launching stream, L2 flushed before each)."""
-    dt = x.dtype
-    op.autotune(dt)
+    """Mean device time of one elastic action (CUDA events on the launching stream, L2 flushed before each),
+    with the tile shape the solver uses for this grid."""
     y = torch.empty_like(x)
     for _ in range(3):
         op.mech_action(x, d=d, out=y)
@@ -416,9 +415,7 @@ def run_kernel_only(args, device):
     dt = torch.float32 if args.fp32 else torch.float64
     x, d = x.to(dt), d.to(dt)
     if args.tile:
-        op.tile_shape(dt, tuple(int(v) for v in args.tile.split(",")))  # pinned: no tuning launches
-    else:
-        op.autotune(dt)
+        op.tile_shape(dt, tuple(int(v) for v in args.tile.split(",")))  # pinned shape
     for _ in range(args.warmup):
         op.mech_action(x, d=d)
     torch.cuda.synchronize()
@@ -447,7 +444,7 @@ def main():
     ap.add_argument("--kernel-only", action="store_true", help="time the elastic action alone (profiling case)")
     ap.add_argument("--cell", type=int, default=N_CELL, help="cell edge in voxels for --kernel-only")
     ap.add_argument("--fp32", action="store_true", help="FP32 storage/arithmetic for --kernel-only")
-    ap.add_argument("--tile", default="", help="pin the tile shape ox,oy,kz for --kernel-only (else autotune)")
+    ap.add_argument("--tile", default="", help="pin the tile shape ox,oy,kz for --kernel-only (else the solver's shape)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

@@ -101,6 +101,37 @@ __device__ __forceinline__ double fold_sum(const double* part, int n, double* sh
   return block_sum(v, sh);
 }
 
+// K block sums at once: for each value the same summation tree as block_sum
+// (so the same bits), with two barriers in all instead of two per value.
+// `sh` must hold 32 * K doubles; every thread receives the K sums.
+template <int K>
+__device__ __forceinline__ void block_sum_multi(double (&v)[K], double* sh) {
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
+  __syncthreads();
+  if (l == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) sh[32 * k + w] = v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = warp_sum((l < (blockDim.x >> 5)) ? sh[32 * k + l] : 0.0);
+}
+
+// K folds of `n` partials each (value k at part + k * stride) in one pass: the
+// loads of all K are in flight together; per value the order of fold_sum.
+template <int K>
+__device__ __forceinline__ void fold_sum_multi(const double* part, int stride, int n, double (&out)[K], double* sh) {
+#pragma unroll
+  for (int k = 0; k < K; ++k) out[k] = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) out[k] += __ldcg(part + (size_t)k * stride + i);
+  }
+  block_sum_multi<K>(out, sh);
+}
+
 __device__ __forceinline__ double fold_min(const double* part, int n, double* sh) {
   double v = INFINITY;
   for (int i = threadIdx.x; i < n; i += blockDim.x) v = fmin(v, __ldcg(part + i));

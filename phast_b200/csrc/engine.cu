@@ -62,19 +62,19 @@ cudaGraphExec_t graph_for(const GraphKey& key, cudaStream_t s, const std::functi
 }
 
 __global__ void while_cond_kernel(cudaGraphConditionalHandle h, const int* __restrict__ active, int* trips,
-                                  int max_iter) {
+                                  const int* __restrict__ max_trips) {
   const int t = ++(*trips);
-  cudaGraphSetConditional(h, (*active && t < max_iter) ? 1u : 0u);
+  cudaGraphSetConditional(h, (*active && t < *max_trips) ? 1u : 0u);
 }
 
 cudaGraphExec_t while_graph_for(const GraphKey& key0, cudaStream_t s, const std::function<int()>& body,
-                                const int* active, int* trips, int max_iter, long long* count) {
+                                const int* active, int* trips, const int* max_trips, long long* count) {
   GraphKey key = key0;
   const char tag[] = "while";
   key_add(key, tag, sizeof(tag));
   key_val(key, active);
   key_val(key, trips);
-  key_val(key, max_iter);
+  key_val(key, max_trips);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
   for (auto it = t_graph_cache.begin(); it != t_graph_cache.end(); ++it) {
@@ -109,7 +109,7 @@ cudaGraphExec_t while_graph_for(const GraphKey& key0, cudaStream_t s, const std:
     return fail();
   const long long c0 = thread_launch_count();
   int st = body();
-  { note_launch(); while_cond_kernel<<<1, 1, 0, s>>>(h, active, trips, max_iter); }
+  { note_launch(); while_cond_kernel<<<1, 1, 0, s>>>(h, active, trips, max_trips); }
   if (!st) st = last_launch_status();
   cudaGraph_t captured = bodyg;
   const cudaError_t e = cudaStreamEndCapture(s, &captured);
@@ -197,7 +197,7 @@ __global__ void ppcg_setup_kernel(int n, const double* __restrict__ d_prev, cons
 __global__ void __launch_bounds__(kThreads) ppcg_init_kernel(int n, PpcgWs w, const double* __restrict__ d,
                                                              const uint8_t* __restrict__ fixed, double tol,
                                                              int max_iter, int check_every) {
-  __shared__ double sh[32];
+  __shared__ double sh[96];
   double rr = 0, bb = 0, rz = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const bool fx = fixed && fixed[i];
@@ -221,17 +221,16 @@ __global__ void __launch_bounds__(kThreads) ppcg_init_kernel(int n, PpcgWs w, co
     bb += bi * bi;
     rz += rf * z;
   }
-  double s;
-  s = block_sum(rr, sh);
-  if (threadIdx.x == 0) w.part[0 * kMaxPartials + blockIdx.x] = s;
-  s = block_sum(bb, sh);
-  if (threadIdx.x == 0) w.part[1 * kMaxPartials + blockIdx.x] = s;
-  s = block_sum(rz, sh);
-  if (threadIdx.x == 0) w.part[2 * kMaxPartials + blockIdx.x] = s;
+  double v3[3] = {rr, bb, rz};
+  block_sum_multi<3>(v3, sh);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) w.part[k * kMaxPartials + blockIdx.x] = v3[k];
+  }
   if (arrive_last(w.counter)) {
-    const double RR = fold_sum(w.part, gridDim.x, sh);
-    const double BB = fold_sum(w.part + kMaxPartials, gridDim.x, sh);
-    const double RZ = fold_sum(w.part + 2 * kMaxPartials, gridDim.x, sh);
+    double f3[3];
+    fold_sum_multi<3>(w.part, kMaxPartials, gridDim.x, f3, sh);
+    const double RR = f3[0], BB = f3[1], RZ = f3[2];
     if (threadIdx.x == 0) {
       PpcgState& st = *w.st;
       st.r0sq = RR;
@@ -256,7 +255,7 @@ __global__ void __launch_bounds__(kThreads) ppcg_init_kernel(int n, PpcgWs w, co
 
 __global__ void __launch_bounds__(kThreads) ppcg_dir_stats_kernel(int n, PpcgWs w, const double* __restrict__ d) {
   if (!w.st->go) return;
-  __shared__ double sh[32];
+  __shared__ double sh[96];
   double pap = 0, up = INFINITY, dn = INFINITY;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double p = w.p[i];
@@ -321,7 +320,7 @@ __global__ void ppcg_update_kernel(int n, PpcgWs w, double* __restrict__ d) {
 __global__ void __launch_bounds__(kThreads) ppcg_resid_kernel(int n, PpcgWs w, const double* __restrict__ d,
                                                               const uint8_t* __restrict__ fixed) {
   if (!w.st->go) return;
-  __shared__ double sh[32];
+  __shared__ double sh[96];
   __shared__ int ish[32];
   const bool need = w.st->go_resid != 0;
   double rfsq = 0, rzn = 0;
@@ -346,15 +345,18 @@ __global__ void __launch_bounds__(kThreads) ppcg_resid_kernel(int n, PpcgWs w, c
     rfsq += rf * rf;
     rzn += rf * z;
   }
-  double s = block_sum(rfsq, sh);
-  if (threadIdx.x == 0) w.part[blockIdx.x] = s;
-  s = block_sum(rzn, sh);
-  if (threadIdx.x == 0) w.part[kMaxPartials + blockIdx.x] = s;
+  double v2[2] = {rfsq, rzn};
+  block_sum_multi<2>(v2, sh);
+  if (threadIdx.x == 0) {
+    w.part[blockIdx.x] = v2[0];
+    w.part[kMaxPartials + blockIdx.x] = v2[1];
+  }
   const int c = block_or(chg, ish);
   if (threadIdx.x == 0) w.ipart[blockIdx.x] = c;
   if (arrive_last(w.counter)) {
-    const double RF = fold_sum(w.part, gridDim.x, sh);
-    const double RZ = fold_sum(w.part + kMaxPartials, gridDim.x, sh);
+    double f2[2];
+    fold_sum_multi<2>(w.part, kMaxPartials, gridDim.x, f2, sh);
+    const double RF = f2[0], RZ = f2[1];
     const int CH = fold_or(w.ipart, gridDim.x, ish);
     if (threadIdx.x == 0) {
       PpcgState& st = *w.st;
@@ -512,8 +514,8 @@ __global__ void __launch_bounds__(kThreads) pcg_start_kernel(int n, PcgWs<T> w, 
                                                              const T* __restrict__ inv_diag, int custom_pre,
                                                              double thr_sq, int mode, double thr_rel,
                                                              double rel_floor, const double* outer_rr,
-                                                             double outer_thr_sq) {
-  __shared__ double sh[32];
+                                                             double outer_thr_sq, int max_trips) {
+  __shared__ double sh[96];
   double rz = 0, rr = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const T r = b[i] - w.Ap[i];
@@ -526,13 +528,16 @@ __global__ void __launch_bounds__(kThreads) pcg_start_kernel(int n, PcgWs<T> w, 
       rz += double(r) * double(z);
     }
   }
-  double s = block_sum(rz, sh);
-  if (threadIdx.x == 0) w.part[blockIdx.x] = s;
-  s = block_sum(rr, sh);
-  if (threadIdx.x == 0) w.part[kMaxPartials + blockIdx.x] = s;
+  double v2[2] = {rz, rr};
+  block_sum_multi<2>(v2, sh);
+  if (threadIdx.x == 0) {
+    w.part[blockIdx.x] = v2[0];
+    w.part[kMaxPartials + blockIdx.x] = v2[1];
+  }
   if (arrive_last(w.counter)) {
-    const double RZ = fold_sum(w.part, gridDim.x, sh);
-    const double RR = fold_sum(w.part + kMaxPartials, gridDim.x, sh);
+    double f2[2];
+    fold_sum_multi<2>(w.part, kMaxPartials, gridDim.x, f2, sh);
+    const double RZ = f2[0], RR = f2[1];
     if (threadIdx.x == 0) {
       PcgState& st = *w.st;
       st.rz = RZ;
@@ -551,6 +556,7 @@ __global__ void __launch_bounds__(kThreads) pcg_start_kernel(int n, PcgWs<T> w, 
       st.active = 1;
       st.outer_done = 0;
       st.trips = 0;
+      st.max_trips = max_trips;
       st.outer_rr = 0.0;
       if (outer_rr) st.outer_rr = *outer_rr;
       // the checks the host used to make before the first iteration
@@ -576,7 +582,7 @@ __global__ void __launch_bounds__(kThreads) pcg_start_kernel(int n, PcgWs<T> w, 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) pcg_rz_kernel(int n, PcgWs<T> w, int start, int mode) {
   if (!w.st->active) return;
-  __shared__ double sh[32];
+  __shared__ double sh[96];
   double rz = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     rz += double(w.r[i]) * double(w.z[i]);
@@ -613,7 +619,7 @@ __global__ void pcg_copy_p_kernel(int n, PcgWs<T> w) {
 template <typename T>
 __global__ void __launch_bounds__(kThreads) pcg_alpha_kernel(int n, PcgWs<T> w, int mode) {
   if (!w.st->active) return;
-  __shared__ double sh[32];
+  __shared__ double sh[96];
   double pap = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     pap += double(w.p[i]) * double(w.Ap[i]);
@@ -652,7 +658,7 @@ __global__ void __launch_bounds__(kThreads) pcg_update_kernel(int n, PcgWs<T> w,
                                                               const T* __restrict__ inv_diag, int custom_pre,
                                                               int mode, int check_every) {
   if (!w.st->active) return;
-  __shared__ double sh[32];
+  __shared__ double sh[96];
   const T a = T(w.st->alpha);
   double rz = 0, rr = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -666,13 +672,16 @@ __global__ void __launch_bounds__(kThreads) pcg_update_kernel(int n, PcgWs<T> w,
       rz += double(r) * double(z);
     }
   }
-  double s = block_sum(rz, sh);
-  if (threadIdx.x == 0) w.part[blockIdx.x] = s;
-  s = block_sum(rr, sh);
-  if (threadIdx.x == 0) w.part[kMaxPartials + blockIdx.x] = s;
+  double v2[2] = {rz, rr};
+  block_sum_multi<2>(v2, sh);
+  if (threadIdx.x == 0) {
+    w.part[blockIdx.x] = v2[0];
+    w.part[kMaxPartials + blockIdx.x] = v2[1];
+  }
   if (arrive_last(w.counter)) {
-    const double RZ = fold_sum(w.part, gridDim.x, sh);
-    const double RR = fold_sum(w.part + kMaxPartials, gridDim.x, sh);
+    double f2[2];
+    fold_sum_multi<2>(w.part, kMaxPartials, gridDim.x, f2, sh);
+    const double RZ = f2[0], RR = f2[1];
     if (threadIdx.x == 0) {
       PcgState& st = *w.st;
       if (!isfinite(RR) || (!custom_pre && !isfinite(RZ))) st.nonfinite = 1;
@@ -714,7 +723,7 @@ __global__ void __launch_bounds__(kThreads) pcg_update_dot_kernel(int n, PcgWs<T
                                                                   int mode, int check_every,
                                                                   const double* __restrict__ pap) {
   if (!w.st->active) return;
-  __shared__ double sh[32];
+  __shared__ double sh[96];
   const double PAP = *pap;
   bool ok;
   double alpha;
@@ -740,13 +749,16 @@ __global__ void __launch_bounds__(kThreads) pcg_update_dot_kernel(int n, PcgWs<T
       }
     }
   }
-  double s = block_sum(rz, sh);
-  if (threadIdx.x == 0) w.part[blockIdx.x] = s;
-  s = block_sum(rr, sh);
-  if (threadIdx.x == 0) w.part[kMaxPartials + blockIdx.x] = s;
+  double v2[2] = {rz, rr};
+  block_sum_multi<2>(v2, sh);
+  if (threadIdx.x == 0) {
+    w.part[blockIdx.x] = v2[0];
+    w.part[kMaxPartials + blockIdx.x] = v2[1];
+  }
   if (arrive_last(w.counter)) {
-    const double RZ = fold_sum(w.part, gridDim.x, sh);
-    const double RR = fold_sum(w.part + kMaxPartials, gridDim.x, sh);
+    double f2[2];
+    fold_sum_multi<2>(w.part, kMaxPartials, gridDim.x, f2, sh);
+    const double RZ = f2[0], RR = f2[1];
     if (threadIdx.x == 0) {
       PcgState& st = *w.st;
       st.iter += 1;
@@ -826,7 +838,7 @@ int pcg_run_thr(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T
   // The start-of-solve decisions (relative threshold, already converged,
   // non-finite, non-positive curvature) are taken on the device: no host
   // round trip before the first chunk.
-  { note_launch(); pcg_start_kernel<T><<<G, kThreads, 0, s>>>(n, w, b, inv_diag, custom, thr.abs * thr.abs, mode, thr.rel, thr.rel_floor, thr.outer_rr, thr.outer_thr * thr.outer_thr); }
+  { note_launch(); pcg_start_kernel<T><<<G, kThreads, 0, s>>>(n, w, b, inv_diag, custom, thr.abs * thr.abs, mode, thr.rel, thr.rel_floor, thr.outer_rr, thr.outer_thr * thr.outer_thr, (maxiter + check_every - 1) / check_every); }
   if ((st = last_launch_status())) return st;
   const int* active = &w.st->active;
   if (custom) {
@@ -880,7 +892,7 @@ int pcg_run_thr(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T
   // check_every iterations with a host check after each.
   cudaGraphExec_t wexec = device_loop_enabled()
                               ? while_graph_for(key, s, [&] { return iterate(check_every); }, active,
-                                                &w.st->trips, (maxiter + check_every - 1) / check_every, &glaunch)
+                                                &w.st->trips, &w.st->max_trips, &glaunch)
                               : nullptr;
   if (wexec) {
     if ((st = cuda_status(cudaGraphLaunch(wexec, s)))) return st;

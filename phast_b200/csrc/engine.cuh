@@ -79,7 +79,8 @@ struct PcgState {
   int converged;
   double outer_rr;  // an enclosing refinement's residual norm^2, when one is checked at the start
   int outer_done;   // ... and that residual already met its threshold: nothing was iterated
-  int trips;        // iterations run by the device-side loop (bounds it by max_iter)
+  int trips;        // chunks run by the device-side loop ...
+  int max_trips;    // ... which stops after this many (set per solve, not baked into the graph)
 };
 
 template <typename T>
@@ -157,11 +158,12 @@ inline void key_val(GraphKey& k, const V& v) {
 // stream cannot be captured; *count receives the kernel launches per replay.
 cudaGraphExec_t graph_for(const GraphKey& key, cudaStream_t s, const std::function<int()>& body, long long* count);
 
-// A graph holding one conditional WHILE node: `body` (one solver iteration) then
-// a one-thread kernel that sets the loop condition to *active && ++*trips <
-// max_iter.  The whole solve is one graph launch; the trip counter bounds it.
+// A graph holding one conditional WHILE node: `body` (one chunk of solver
+// iterations) then a one-thread kernel that sets the loop condition to
+// *active && ++*trips < *max_trips.  The whole solve is one graph launch; the
+// trip limit is read from device memory, so one graph serves every limit.
 // nullptr when conditional nodes are unavailable.  *count: launches per trip.
 cudaGraphExec_t while_graph_for(const GraphKey& key, cudaStream_t s, const std::function<int()>& body,
-                                const int* active, int* trips, int max_iter, long long* count);
+                                const int* active, int* trips, const int* max_trips, long long* count);
 
 }  // namespace phastb

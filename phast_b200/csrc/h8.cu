@@ -137,26 +137,30 @@ __global__ void __launch_bounds__(kThreads) h8_mech_elem_kernel(VoxGeom g, VoxMa
       }
     }
   }
-  __shared__ double sh[32];
   constexpr int NK = ENERGY ? 7 : 6;
+  __shared__ double sh[32 * NK];
+  double v[NK];
 #pragma unroll
-  for (int k = 0; k < NK; ++k) {
-    const double sm = block_sum(acc[k], sh);
-    if (threadIdx.x == 0) ws.part[k * kMaxPartials + blockIdx.x] = sm;
+  for (int k = 0; k < NK; ++k) v[k] = acc[k];
+  block_sum_multi<NK>(v, sh);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NK; ++k) ws.part[k * kMaxPartials + blockIdx.x] = v[k];
   }
   if (arrive_last(ws.counter)) {
+    double f[NK];
+    fold_sum_multi<NK>(ws.part, kMaxPartials, gridDim.x, f, sh);
+    if (threadIdx.x == 0) {
 #pragma unroll
-    for (int k = 0; k < NK; ++k) {
-      const double t = fold_sum(ws.part + k * kMaxPartials, gridDim.x, sh);
-      if (threadIdx.x == 0) {
-        ws.out[k] = t;
+      for (int k = 0; k < NK; ++k) {
+        ws.out[k] = f[k];
         if (y && k < 6) {
           const size_t idx = 3 * (size_t)g.n_red + k;
-          y[idx] = (mask && mask[idx]) ? T(0) : T(t);
+          y[idx] = (mask && mask[idx]) ? T(0) : T(f[k]);
         }
       }
+      *ws.counter = 0u;
     }
-    if (threadIdx.x == 0) *ws.counter = 0u;
   }
 }
 
@@ -254,19 +258,23 @@ __global__ void __launch_bounds__(kThreads) h8_mdiag_elem_kernel(VoxGeom g, VoxM
 #pragma unroll
       for (int L = 0; L < 8; ++L) scratch[(size_t)(L * 3 + c) * E + e] = out[c][L];
   }
-  __shared__ double sh[32];
+  __shared__ double sh[32 * 6];
+  double v[6];
 #pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    const double sm = block_sum(acc[k], sh);
-    if (threadIdx.x == 0) ws.part[k * kMaxPartials + blockIdx.x] = sm;
+  for (int k = 0; k < 6; ++k) v[k] = acc[k];
+  block_sum_multi<6>(v, sh);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) ws.part[k * kMaxPartials + blockIdx.x] = v[k];
   }
   if (arrive_last(ws.counter)) {
+    double f[6];
+    fold_sum_multi<6>(ws.part, kMaxPartials, gridDim.x, f, sh);
+    if (threadIdx.x == 0) {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      const double t = fold_sum(ws.part + k * kMaxPartials, gridDim.x, sh);
-      if (threadIdx.x == 0) diag[3 * (size_t)g.n_red + k] = T(t);
+      for (int k = 0; k < 6; ++k) diag[3 * (size_t)g.n_red + k] = T(f[k]);
+      *ws.counter = 0u;
     }
-    if (threadIdx.x == 0) *ws.counter = 0u;
   }
 }
 

@@ -149,9 +149,10 @@ template <typename T>
 TileArgs<T> tile_args(const VoxGeom& v, int cls);
 
 // Launches the tile kernel for (COEF, MODE) with prepared arguments.  With
-// `tune`, the first plain or dot launch for a grid with no recorded shape
-// (outside stream capture, unguarded) times the candidate shapes and records
-// the fastest; PHASTB_AUTOTUNE=0 in the environment keeps the heuristic.
+// `tune` and PHASTB_AUTOTUNE=1 in the environment, the first plain or dot
+// launch for a grid with no recorded shape (outside stream capture, unguarded)
+// times the candidate shapes and records the fastest; otherwise the
+// deterministic heuristic shape is used.
 template <typename T>
 int h8_tile_launch(const TileArgs<T>& a, const VoxMat<T>& m, int coef, int mode, cudaStream_t s, bool tune = true);
 

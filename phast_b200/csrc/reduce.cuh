@@ -43,19 +43,20 @@ inline int red_ws_fetch(const RedWs& w, double* host, int k, cudaStream_t s) {
 // and resets the ticket so the workspace can be reused by the next launch.
 template <int K>
 __device__ __forceinline__ void reduce_multi(double (&v)[K], RedWs ws) {
-  __shared__ double sh[32];
+  __shared__ double sh[32 * K];
+  block_sum_multi<K>(v, sh);
+  if (threadIdx.x == 0) {
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    const double s = block_sum(v[k], sh);
-    if (threadIdx.x == 0) ws.part[k * kMaxPartials + blockIdx.x] = s;
+    for (int k = 0; k < K; ++k) ws.part[k * kMaxPartials + blockIdx.x] = v[k];
   }
   if (arrive_last(ws.counter)) {
+    double t[K];
+    fold_sum_multi<K>(ws.part, kMaxPartials, gridDim.x, t, sh);
+    if (threadIdx.x == 0) {
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const double t = fold_sum(ws.part + k * kMaxPartials, gridDim.x, sh);
-      if (threadIdx.x == 0) ws.out[k] = t;
+      for (int k = 0; k < K; ++k) ws.out[k] = t[k];
+      *ws.counter = 0u;
     }
-    if (threadIdx.x == 0) *ws.counter = 0u;
   }
 }
 

@@ -147,19 +147,30 @@ class BoxKKTResult:
 
 
 def solve_h8_scalar_box_kkt(system, *, lower_bound=0.0, upper_bound=1.0, initial=None, linear_tolerance=1e-10,
-                            kkt_tolerance=1e-9, max_linear_iterations=4000, max_active_set_iterations=64):
-    """Box-constrained scalar H8 solve (box_kkt_h8.py:603-778) of ``op.damage_system(H)``."""
+                            kkt_tolerance=1e-9, max_linear_iterations=4000, max_active_set_iterations=64,
+                            check_bounds=True):
+    """Box-constrained scalar H8 solve (box_kkt_h8.py:603-778) of ``op.damage_system(H)``.
+
+    ``check_bounds=False`` skips the ValueError checks of the bounds and the initial
+    guess (one device-to-host read) for callers whose inputs satisfy them by
+    construction.
+    """
     op = system.op
     n = op.n_red
     if not isinstance(upper_bound, (int, float)):
         raise NotImplementedError("the B200 box-KKT solve takes a scalar upper bound")
     lower = (torch.full((n,), float(lower_bound), dtype=torch.float64, device=op.device)
              if not isinstance(lower_bound, torch.Tensor) else lower_bound.to(torch.float64).contiguous())
-    if bool((lower > upper_bound).any()):
-        raise ValueError("lower_bound must not exceed upper_bound at any degree of freedom")
     init = None if initial is None else initial.to(torch.float64).contiguous()
-    if init is not None and (bool((init < lower).any()) or bool((init > upper_bound).any())):
-        raise ValueError("initial must already satisfy the requested box bounds; it is never clipped")
+    if check_bounds:
+        flags = [(lower > upper_bound).any()]
+        if init is not None:
+            flags.append(((init < lower) | (init > upper_bound)).any())
+        flags = torch.stack(flags).tolist()  # one read for both checks
+        if flags[0]:
+            raise ValueError("lower_bound must not exceed upper_bound at any degree of freedom")
+        if len(flags) > 1 and flags[1]:
+            raise ValueError("initial must already satisfy the requested box bounds; it is never clipped")
     H = None if system.H is None else system.H.to(torch.float64).contiguous()
     out = torch.empty(n, dtype=torch.float64, device=op.device)
     info = (C.c_int * 3)()
@@ -221,6 +232,7 @@ class StaggeredSolver:
         self._u_floor = min(op.h) * math.sqrt(self._n_u)
         self._mask = op.mech_fixed_mask()
         self._red = _lib.Workspace(op.device)
+        self._tail = torch.empty(7, dtype=torch.float64, pin_memory=True)
 
     def initial_state(self):
         op = self.op
@@ -262,11 +274,14 @@ class StaggeredSolver:
             raise _AttemptFailure("damage residual is not finite")
         tol = min(cfg.damage_linear_tol, 0.1 * cfg.damage_kkt_tol / max(r0, 1.0))
         tol = max(tol, 4.0 * float(np.finfo(np.float64).eps))
+        # the bounds hold by construction: lower is the accepted damage of the last
+        # increment (in [0, 1]) and initial is lower itself or a box-KKT solution
         try:
             res = solve_h8_scalar_box_kkt(system, lower_bound=lower, upper_bound=1.0, initial=initial,
                                           linear_tolerance=tol, kkt_tolerance=cfg.damage_kkt_tol,
                                           max_linear_iterations=cfg.damage_maxit,
-                                          max_active_set_iterations=cfg.damage_max_active_set)
+                                          max_active_set_iterations=cfg.damage_max_active_set,
+                                          check_bounds=False)
         except (H8ScalarBoxKKTConvergenceError, RuntimeError) as exc:
             raise _AttemptFailure(f"damage box-KKT solve failed: {exc}") from exc
         return res.solution, res.total_pcg_iterations, res.active_set_iterations, res.satisfies_kkt
@@ -326,13 +341,21 @@ class StaggeredSolver:
         else:
             x = x_old
         g = op.degradation(d)
-        sigma = op.macro_stress(x, g).cpu().numpy()
-        E = op.split_mech(x)[1].detach().cpu().numpy()
+        # E and max(d) travel in one copy that the stress reduction's read waits for
+        tail = torch.cat((op.split_mech(x)[1].detach(), d.max().reshape(1)))
+        self._tail.copy_(tail, non_blocking=True)
+        done = torch.cuda.Event()
+        done.record()
+        rE, _ = op._stress_energy(x, g)
+        done.synchronize()
+        sigma = rE / op.volume
+        E = self._tail[:6].numpy().copy()
+        d_max = float(self._tail[6])
         completes = 1 <= increment <= self.load.n_increments and target == self.load.targets[increment - 1]
         new_state = SolverState(state.step + 1, x, d, H, E.copy(), sigma,
                                 increment if completes else state.increment)
         rec = IncrementRecord(increment, target, tuple(float(v) for v in sigma), k, pm, pp, sets, bool(kkt),
-                              float(d.max()), perf_counter() - t0)
+                              d_max, perf_counter() - t0)
         return new_state, rec
 
     def run(self, max_increments=None, on_increment=None, start_state=None):
