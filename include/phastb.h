@@ -291,8 +291,9 @@ int phastb_h8_mech_apply_noalloc(const phastb_voxel_grid* g, const phastb_voxel_
 
 /* Tile shape of the elastic action for a grid and word size (no reference counterpart: the
  * reference action is a batched gather/matmul/scatter).  shape = {ox, oy, kz}: owned nodes per
- * block in x and y and node layers per block in z; (ox+1)(oy+1) <= 256.  set = 0 reads the
- * shape in use (the recorded one, else a heuristic), set = 1 records `shape` for this grid. */
+ * block in x and y and node layers per block in z; (ox+1)(oy+1) <= 256; kz = 0 lets each launch
+ * pick the depth from the kernel's occupancy.  set = 0 reads the shape in use (the recorded
+ * one, else a heuristic), set = 1 records `shape` for this grid. */
 int phastb_h8_tile_shape(const phastb_voxel_grid* g, int dtype, int set, int* shape);
 
 /* Times the elastic action over candidate tile shapes on the caller's buffers (x, d, slot

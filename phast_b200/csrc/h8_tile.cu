@@ -794,7 +794,7 @@ auto shape_key(const VoxGeom& g, int word, int cls) {
 
 // Heuristic: among owned-node tiles of <= kTileMaxThreads element threads,
 // prefer shapes whose sides divide the grid (no ragged tiles) and the least
-// recomputed halo; then pick the z depth that still gives two blocks per SM.
+// recomputed halo; the z depth is left to the launch (kz = 0, launch_kz).
 TileShape heuristic_shape(const VoxGeom& g, int word) {
   static const int cand[][2] = {{16, 12}, {12, 16}, {14, 14}, {24, 8}, {16, 8}, {8, 16}, {20, 8}, {32, 4},
                                 {12, 12}, {10, 10}, {8, 8},   {6, 6},   {4, 4},  {2, 2},  {1, 1}};
@@ -811,12 +811,28 @@ TileShape heuristic_shape(const VoxGeom& g, int word) {
       best = t;
     }
   }
-  const long long tiles_xy = (long long)((g.rx + best.ox - 1) / best.ox) * ((g.ry + best.oy - 1) / best.oy);
-  const long long want = 2LL * 148;
-  int kz = 16;
-  while (kz > 2 && tiles_xy * ((g.rz + kz - 1) / kz) < want) kz /= 2;
-  best.kz = std::min(kz, g.rz);
+  best.kz = 0;
   (void)word;
+  return best;
+}
+
+// Z depth of a tile whose shape leaves it to the launch (kz = 0), from the
+// number of blocks that can be resident at once (`capacity`): the fewest
+// rounds of resident blocks, each round costing one tile's kz + 1 element
+// layers plus its two-layer prologue.  A power-of-two depth leaves a second,
+// mostly idle round on e.g. 64^3 (512 tiles of kz = 4 for 444 resident blocks);
+// kz = 5 runs 416 tiles in one round.
+int launch_kz(long long tiles_xy, int rz, long long capacity) {
+  int best = 1;
+  double best_cost = 1e300;
+  for (int kz = 1; kz <= rz; ++kz) {
+    const long long tiles = tiles_xy * ((rz + kz - 1) / kz);
+    const double cost = double((tiles + capacity - 1) / capacity) * (kz + 2);
+    if (cost < best_cost - 1e-9) {
+      best_cost = cost;
+      best = kz;
+    }
+  }
   return best;
 }
 
@@ -853,11 +869,13 @@ int launch_variant(const TileArgs<T>& a, const VoxMat<T>& m, cudaStream_t s) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const VoxGeom& v = a.g;
-  const long long n_tiles = (long long)((v.rx + a.ts.ox - 1) / a.ts.ox) * ((v.ry + a.ts.oy - 1) / a.ts.oy) *
-                            ((v.rz + a.ts.kz - 1) / a.ts.kz);
-  long long grid = std::min<long long>(n_tiles, (long long)per_sm * sms);
-  grid = std::min<long long>(grid, kMaxPartials);
-  { note_launch(); kern<<<(int)grid, threads, smem, s>>>(a, m); }
+  const long long tiles_xy = (long long)((v.rx + a.ts.ox - 1) / a.ts.ox) * ((v.ry + a.ts.oy - 1) / a.ts.oy);
+  const long long cap = std::min<long long>((long long)per_sm * sms, kMaxPartials);
+  TileArgs<T> b = a;
+  if (b.ts.kz <= 0) b.ts.kz = launch_kz(tiles_xy, v.rz, cap);
+  const long long n_tiles = tiles_xy * ((v.rz + b.ts.kz - 1) / b.ts.kz);
+  const long long grid = std::min<long long>(n_tiles, cap);
+  { note_launch(); kern<<<(int)grid, threads, smem, s>>>(b, m); }
   return last_launch_status();
 }
 
@@ -942,7 +960,7 @@ int tune_shape(TileArgs<T> a, const VoxMat<T>& m, int coef, int mode, cudaStream
                float* best_ms) {
   static const int cand[][2] = {{16, 8}, {32, 4},  {8, 8},   {8, 4},   {4, 4},   {16, 12}, {12, 16},
                                 {14, 14}, {24, 8}, {20, 8}, {12, 12}, {10, 10}, {6, 6},   {2, 4}};
-  static const int kzs[] = {1, 2, 4, 8, 16};
+  static const int kzs[] = {0, 1, 2, 4, 8, 16};  // 0: chosen at launch
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess) return PHASTB_ERR_CUDA;
   if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -1078,11 +1096,13 @@ int dlaunch_variant(const DTileArgs<T>& a, cudaStream_t s) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const VoxGeom& v = a.g;
-  const long long n_tiles = (long long)((v.rx + a.ts.ox - 1) / a.ts.ox) * ((v.ry + a.ts.oy - 1) / a.ts.oy) *
-                            ((v.rz + a.ts.kz - 1) / a.ts.kz);
-  long long grid = std::min<long long>(n_tiles, (long long)per_sm * sms);
-  grid = std::min<long long>(grid, kMaxPartials);
-  { note_launch(); kern<<<(int)grid, threads, smem, s>>>(a); }
+  const long long tiles_xy = (long long)((v.rx + a.ts.ox - 1) / a.ts.ox) * ((v.ry + a.ts.oy - 1) / a.ts.oy);
+  const long long cap = std::min<long long>((long long)per_sm * sms, kMaxPartials);
+  DTileArgs<T> b = a;
+  if (b.ts.kz <= 0) b.ts.kz = launch_kz(tiles_xy, v.rz, cap);
+  const long long n_tiles = tiles_xy * ((v.rz + b.ts.kz - 1) / b.ts.kz);
+  const long long grid = std::min<long long>(n_tiles, cap);
+  { note_launch(); kern<<<(int)grid, threads, smem, s>>>(b); }
   return last_launch_status();
 }
 
@@ -1124,7 +1144,7 @@ int h8_damage_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* s
     if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
       // time the candidate shapes on this call's buffers (y is recomputed below)
       static const int cand[][2] = {{16, 8}, {32, 4}, {8, 8}, {16, 12}, {14, 14}, {10, 10}, {8, 4}, {4, 4}};
-      static const int kzs[] = {2, 4, 8, 16};
+      static const int kzs[] = {0, 2, 4, 8, 16};  // 0: chosen at launch
       cudaEvent_t e0, e1;
       if (cudaEventCreate(&e0) != cudaSuccess) return PHASTB_ERR_CUDA;
       if (cudaEventCreate(&e1) != cudaSuccess) {

@@ -28,9 +28,10 @@ constexpr int kTileMaxThreads = 256;
 
 inline int tile_threads(const TileShape& t) { return ((t.ox + 1) * (t.oy + 1) + 31) / 32 * 32; }
 
+// kz = 0: the launch picks the z depth from the kernel's occupancy.
 inline bool tile_ok(const TileShape& t) {
   // each thread stages at most two halo-tile nodes per layer
-  return t.ox >= 1 && t.oy >= 1 && t.kz >= 1 && tile_threads(t) <= kTileMaxThreads &&
+  return t.ox >= 1 && t.oy >= 1 && t.kz >= 0 && tile_threads(t) <= kTileMaxThreads &&
          (t.ox + 2) * (t.oy + 2) <= 2 * tile_threads(t);
 }
 

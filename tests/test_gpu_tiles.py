@@ -20,7 +20,7 @@ GRIDS = [
     ((9, 5, 4), (True, False, True)),
     ((17, 3, 2), (True, True, False)),
 ]
-SHAPES = [None, (16, 12, 16), (14, 14, 8), (24, 8, 4), (8, 8, 2), (4, 4, 4), (3, 2, 1), (1, 1, 1)]
+SHAPES = [None, (16, 12, 16), (14, 14, 8), (24, 8, 4), (8, 8, 2), (4, 4, 4), (3, 2, 1), (1, 1, 1), (16, 8, 0), (5, 3, 0)]
 
 
 def build(shape, periodic, seed):
@@ -66,7 +66,7 @@ def test_autotune_records_a_valid_shape():
     want = ref.mech_action(x, ref.degradation(d))
     for dt, tol in ((torch.float64, 1e-12), (torch.float32, 3e-5)):
         shape, ms = op.autotune(dt)
-        assert ms > 0 and all(v >= 1 for v in shape)
+        assert ms > 0 and shape[0] >= 1 and shape[1] >= 1 and shape[2] >= 0  # kz = 0: depth chosen per launch
         assert (shape[0] + 1) * (shape[1] + 1) <= 256
         assert op.tile_shape(dt) == shape
         got = op.mech_action(torch.as_tensor(x, device="cuda", dtype=dt),
