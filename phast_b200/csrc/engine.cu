@@ -557,6 +557,9 @@ __global__ void __launch_bounds__(kThreads) pcg_start_kernel(int n, PcgWs<T> w, 
       st.outer_done = 0;
       st.trips = 0;
       st.max_trips = max_trips;
+      st.bar_count = 0u;
+      st.bar_gen = 0u;
+      st.grid_error = 0;
       st.outer_rr = 0.0;
       if (outer_rr) st.outer_rr = *outer_rr;
       // the checks the host used to make before the first iteration
@@ -814,7 +817,8 @@ __global__ void pcg_dir_kernel(int n, PcgWs<T> w) {
 
 template <typename T>
 int pcg_run(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T* inv_diag, const Precond<T>* M, T* x,
-            double thr, int maxiter, int check_every, PcgMode mode, double, PcgResult* out, cudaStream_t s) {
+            double thr, int maxiter, int check_every, PcgMode mode, double, PcgResult* out, cudaStream_t s,
+            const PcgLoop* loop) {
   PcgThreshold t;
   if (thr >= 0.0) {
     t.abs = thr;
@@ -822,13 +826,13 @@ int pcg_run(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T* in
     t.rel = -thr;
     t.rel_floor = 1.0;
   }
-  return pcg_run_thr<T>(A, n, w, b, inv_diag, M, x, t, maxiter, check_every, mode, out, s);
+  return pcg_run_thr<T>(A, n, w, b, inv_diag, M, x, t, maxiter, check_every, mode, out, s, loop);
 }
 
 template <typename T>
 int pcg_run_thr(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T* inv_diag, const Precond<T>* M,
                 T* x, const PcgThreshold& thr, int maxiter, int check_every, PcgMode mode, PcgResult* out,
-                cudaStream_t s) {
+                cudaStream_t s, const PcgLoop* loop) {
   if (check_every < 1 || maxiter < 1) return PHASTB_ERR_ARG;
   const int G = grid_for(n);
   int st;
@@ -849,6 +853,18 @@ int pcg_run_thr(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T
   }
   PcgState hs{};
   int it = 0;
+  bool looped = false;
+  if (loop && !custom) {
+    const int ls = (*loop)(maxiter);
+    if (ls == PHASTB_OK) {
+      if ((st = cuda_status(cudaMemcpyAsync(&hs, w.st, sizeof(hs), cudaMemcpyDeviceToHost, s)))) return st;
+      if ((st = cuda_status(cudaStreamSynchronize(s)))) return st;
+      if (hs.grid_error) return PHASTB_ERR_CUDA;
+      looped = true;
+    } else if (ls != PHASTB_UNSUPPORTED) {
+      return ls;
+    }
+  }
   auto iterate = [&](int k_iters) -> int {
     int e;
     for (int k = 0; k < k_iters; ++k) {
@@ -890,11 +906,13 @@ int pcg_run_thr(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T
   // Preferred: the whole iteration loop on the device (one conditional-WHILE
   // graph, one host synchronisation per solve).  Otherwise chunks of
   // check_every iterations with a host check after each.
-  cudaGraphExec_t wexec = device_loop_enabled()
+  cudaGraphExec_t wexec = !looped && device_loop_enabled()
                               ? while_graph_for(key, s, [&] { return iterate(check_every); }, active,
                                                 &w.st->trips, &w.st->max_trips, &glaunch)
                               : nullptr;
-  if (wexec) {
+  if (looped) {
+    it = maxiter;
+  } else if (wexec) {
     if ((st = cuda_status(cudaGraphLaunch(wexec, s)))) return st;
     if ((st = cuda_status(cudaMemcpyAsync(&hs, w.st, sizeof(hs), cudaMemcpyDeviceToHost, s)))) return st;
     if ((st = cuda_status(cudaStreamSynchronize(s)))) return st;
@@ -932,16 +950,16 @@ template PcgWs<double> pcg_ws<double>(void*, int);
 template PcgWs<float> pcg_ws<float>(void*, int);
 template int pcg_run<double>(const LinOp<double>&, int, const PcgWs<double>&, const double*, const double*,
                              const Precond<double>*, double*, double, int, int, PcgMode, double, PcgResult*,
-                             cudaStream_t);
+                             cudaStream_t, const PcgLoop*);
 template int pcg_run<float>(const LinOp<float>&, int, const PcgWs<float>&, const float*, const float*,
                             const Precond<float>*, float*, double, int, int, PcgMode, double, PcgResult*,
-                            cudaStream_t);
+                            cudaStream_t, const PcgLoop*);
 template int pcg_run_thr<double>(const LinOp<double>&, int, const PcgWs<double>&, const double*, const double*,
                                  const Precond<double>*, double*, const PcgThreshold&, int, int, PcgMode, PcgResult*,
-                                 cudaStream_t);
+                                 cudaStream_t, const PcgLoop*);
 template int pcg_run_thr<float>(const LinOp<float>&, int, const PcgWs<float>&, const float*, const float*,
                                 const Precond<float>*, float*, const PcgThreshold&, int, int, PcgMode, PcgResult*,
-                                cudaStream_t);
+                                cudaStream_t, const PcgLoop*);
 
 // ================================================================ vector ops
 

@@ -81,6 +81,10 @@ struct PcgState {
   int outer_done;   // ... and that residual already met its threshold: nothing was iterated
   int trips;        // chunks run by the device-side loop ...
   int max_trips;    // ... which stops after this many (set per solve, not baked into the graph)
+  // grid barrier of a persistent iteration kernel (reset by the start kernel)
+  unsigned bar_count, bar_gen;
+  int grid_error;   // a barrier wait ran out: the persistent kernel stopped early
+  int pad_;
 };
 
 template <typename T>
@@ -129,15 +133,21 @@ struct PcgThreshold {
   double outer_thr = 0.0;
 };
 
+// The iterations of a Jacobi- or identity-preconditioned solve run by one
+// persistent launch: loop(maxiter) continues from the started state in the
+// workspace with the iteration semantics of the engine and returns a status;
+// PHASTB_UNSUPPORTED means it cannot run here and the engine iterates itself.
+using PcgLoop = std::function<int(int maxiter)>;
+
 template <typename T>
 int pcg_run(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T* inv_diag, const Precond<T>* M,
             T* x, double thr, int maxiter, int check_every, PcgMode mode, double rr0_for_div, PcgResult* out,
-            cudaStream_t s);
+            cudaStream_t s, const PcgLoop* loop = nullptr);
 
 template <typename T>
 int pcg_run_thr(const LinOp<T>& A, int n, const PcgWs<T>& w, const T* b, const T* inv_diag, const Precond<T>* M,
                 T* x, const PcgThreshold& thr, int maxiter, int check_every, PcgMode mode, PcgResult* out,
-                cudaStream_t s);
+                cudaStream_t s, const PcgLoop* loop = nullptr);
 
 // Vector helpers used by the drivers.
 template <typename T>

@@ -1,5 +1,6 @@
 // Tiled z-marching voxel H8 elastic action (see h8_tile.cuh).
 #include "h8_tile.cuh"
+#include "engine.cuh"
 
 #include <cstdlib>
 #include <cstring>
@@ -606,13 +607,13 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
 
 // Scalar AT2 damage action on the same brick schedule:
 //   y = scale * [Gc_e (M / ell + ell L) d + 2 (1 - kappa) sum_q w H_q N_q N_q^T d]
-// (the element arithmetic of h8_damage_elem_kernel), masked rows zero, and with
-// MODE == kModeDot also x . y into ws.out[kOutDot].
-template <typename T, int MODE, int OX, int OY>
-__global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_kernel(DTileArgs<T> a) {
-  if (a.guard && *a.guard == 0) return;
-  constexpr bool DOT = MODE == kModeDot;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+// (the element arithmetic of h8_damage_elem_kernel), masked rows zero.  One
+// pass covers every brick of this (persistent) block: node values come from
+// node_val(n), each owned node's result goes to on_owned(n, x_n, y_n), and the
+// return value is this thread's share of sum_n x_n y_n (with DOT).
+template <typename T, int OX, int OY, bool DOT, class NodeVal, class OnOwned>
+__device__ __forceinline__ double dtile_pass(const DTileArgs<T>& a, unsigned char* smem_raw, NodeVal node_val,
+                                             OnOwned on_owned) {
   const VoxGeom& g = a.g;
   const int ox = OX ? OX : a.ts.ox, oy = OY ? OY : a.ts.oy, kz = a.ts.kz;
   const int ex = ox + 1, exy = ex * (oy + 1);
@@ -659,7 +660,7 @@ __global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_kernel(DTileArgs<
       if (t < nt && gk >= 0) {
         const int gi = wrap_node(i0 - 1 + t % ntx, g.nx, g.rx, g.px);
         const int gj = wrap_node(j0 - 1 + t / ntx, g.ny, g.ry, g.py);
-        if (gi >= 0 && gj >= 0) v = __ldg(a.x + (size_t)gi + (size_t)g.rx * ((size_t)gj + (size_t)g.ry * gk));
+        if (gi >= 0 && gj >= 0) v = node_val((size_t)gi + (size_t)g.rx * ((size_t)gj + (size_t)g.ry * gk));
       }
       r[h] = v;
     }
@@ -759,25 +760,184 @@ __global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_kernel(DTileArgs<
           const size_t n = (size_t)gi + (size_t)g.rx * ((size_t)gj + (size_t)g.ry * ke);
           T v = pend + lo;
           if (a.mask && __ldg(a.mask + n)) v = T(0);
-          a.y[n] = v;
-          if (DOT) tdot += b0[(nj + 1) * ntx + ni + 1] * v;
+          const T xn = b0[(nj + 1) * ntx + ni + 1];
+          on_owned(n, xn, v);
+          if (DOT) tdot += xn * v;
         }
         pend = up;
       }
     }
     if (DOT) accd += double(tdot);
   }
+  return accd;
+}
+
+// The damage action as its own launch (MODE == kModeDot also x . y into ws.out[kOutDot]).
+template <typename T, int MODE, int OX, int OY>
+__global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_kernel(DTileArgs<T> a) {
+  if (a.guard && *a.guard == 0) return;
+  constexpr bool DOT = MODE == kModeDot;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const T* __restrict__ x = a.x;
+  T* __restrict__ y = a.y;
+  const double accd = dtile_pass<T, OX, OY, DOT>(
+      a, smem_raw, [&](size_t n) { return __ldg(x + n); }, [&](size_t n, T, T v) { y[n] = v; });
   if constexpr (DOT) {
     __shared__ double sh[32];
     const double sm = block_sum(accd, sh);
-    if (tid == 0) a.ws.part[kOutDot * kMaxPartials + blockIdx.x] = sm;
+    if (threadIdx.x == 0) a.ws.part[kOutDot * kMaxPartials + blockIdx.x] = sm;
     if (arrive_last(a.ws.counter)) {
       const double t = fold_sum(a.ws.part + kOutDot * kMaxPartials, gridDim.x, sh);
-      if (tid == 0) {
+      if (threadIdx.x == 0) {
         a.ws.out[kOutDot] = t;
         *a.ws.counter = 0u;
       }
     }
+  }
+}
+
+// ------------------------------------------------------- persistent damage PCG
+
+// Polls of one grid-barrier wait before it gives up (each poll sleeps ~64 ns,
+// so about two seconds; a normal wait is a few microseconds).
+constexpr unsigned kBarSpins = 1u << 25;
+
+// Grid-wide barrier of a cooperative launch (every block resident).  The last
+// block to arrive resets the count and advances the generation; the others
+// poll the generation.  A wait that runs out sets st->grid_error, and every
+// block that sees the error leaves the barrier with false, so the kernel ends
+// instead of hanging.  gen: this block's copy of the generation (thread 0).
+__device__ __forceinline__ bool grid_barrier(PcgState* st, unsigned& gen) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned g0 = gen;
+    __threadfence();
+    if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
+      atomicExch(&st->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&st->bar_gen, 1u);
+    } else {
+      unsigned spins = 0;
+      while (*reinterpret_cast<volatile unsigned*>(&st->bar_gen) == g0) {
+        if (++spins > kBarSpins || *reinterpret_cast<volatile int*>(&st->grid_error)) {
+          atomicExch(&st->grid_error, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    gen = g0 + 1;
+    s_ok = ok && !*reinterpret_cast<volatile int*>(&st->grid_error);
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <typename T>
+struct DamagePcgArgs {
+  int n, maxiter, mode, pad_;
+  T *r, *z, *p, *p_alt, *Ap, *x;
+  const T* inv_diag;
+  double* part;  // 3 * kMaxPartials
+  PcgState* st;
+};
+
+// Every iteration of a Jacobi-preconditioned CG on the damage operator in one
+// cooperative launch, continuing from the state left by pcg_start_kernel:
+//   A: p = z + beta p (formed while the bricks are staged; two direction
+//      buffers, so a neighbour's halo never sees a new value), Ap, p . Ap
+//   -- grid barrier --  alpha = rz / p.Ap  (every block folds the partials)
+//   B: x += alpha p, r -= alpha Ap, z = r / diag, r . z, r . r
+//   -- grid barrier --  beta, convergence: the state rules of
+//      pcg_update_dot_kernel, evaluated identically in every block.
+// Data written inside the launch is read through L2 (__ldcg).
+template <typename T, int OX, int OY>
+__global__ void __launch_bounds__(kTileMaxThreads, 2) h8_damage_pcg_kernel(DTileArgs<T> a, DamagePcgArgs<T> c) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double sh[64];
+  const int tid = threadIdx.x;
+  PcgState S = *c.st;
+  unsigned gen = S.bar_gen;
+  const T* p_src = c.p;
+  T* p_dst = c.p_alt;
+  const int n = c.n;
+  for (int it = 0; it < c.maxiter && S.active; ++it) {
+    const T beta = T(S.beta);
+    double pap = dtile_pass<T, OX, OY, true>(
+        a, smem_raw, [&](size_t i) { return __ldcg(c.z + i) + beta * __ldcg(p_src + i); },
+        [&](size_t i, T pn, T v) {
+          c.Ap[i] = v;
+          p_dst[i] = pn;
+        });
+    pap = block_sum(pap, sh);
+    if (tid == 0) c.part[blockIdx.x] = pap;
+    if (!grid_barrier(c.st, gen)) return;
+    const double PAP = fold_sum(c.part, gridDim.x, sh);
+    const bool ok = isfinite(PAP) && PAP > 0.0;
+    const double alpha = S.rz / PAP;
+    const T al = T(alpha);
+    double v2[2] = {0.0, 0.0};  // r . z, r . r
+    if (ok) {
+      for (int i = blockIdx.x * blockDim.x + tid; i < n; i += gridDim.x * blockDim.x) {
+        c.x[i] = c.x[i] + al * __ldcg(p_dst + i);
+        const T r = c.r[i] - al * __ldcg(c.Ap + i);
+        c.r[i] = r;
+        v2[1] += double(r) * double(r);
+        const T z = c.inv_diag ? r * __ldg(c.inv_diag + i) : r;
+        c.z[i] = z;
+        v2[0] += double(r) * double(z);
+      }
+    }
+    block_sum_multi<2>(v2, sh);
+    if (tid == 0) {
+      c.part[kMaxPartials + blockIdx.x] = v2[0];
+      c.part[2 * kMaxPartials + blockIdx.x] = v2[1];
+    }
+    if (!grid_barrier(c.st, gen)) return;
+    double f2[2];
+    fold_sum_multi<2>(c.part + kMaxPartials, kMaxPartials, gridDim.x, f2, sh);
+    const double RZ = f2[0], RR = f2[1];
+    // the state rules of pcg_update_dot_kernel (Jacobi / identity, not PCG_PERIODIC)
+    S.iter += 1;
+    if (!ok) {
+      if (!isfinite(PAP)) S.nonfinite = 1;
+      if (!(PAP > 0.0)) S.breakdown = 1;
+      S.active = 0;
+    } else {
+      S.alpha = alpha;
+      S.steps += 1;
+      if (!isfinite(RR) || !isfinite(RZ)) S.nonfinite = 1;
+      S.rr = RR;
+      if (!(RR > S.thr_sq)) {
+        S.converged = 1;
+        S.active = 0;
+      } else {
+        if (c.mode == PCG_STRICT && !(RZ > 0.0)) S.breakdown = 1;
+        S.beta = (c.mode == PCG_STRICT) ? RZ / S.rz : ((S.rz > 0.0) ? RZ / S.rz : 0.0);
+        S.rz = RZ;
+      }
+      if (S.breakdown || S.nonfinite) S.active = 0;
+    }
+    if (blockIdx.x == 0 && tid == 0) {
+      PcgState& o = *c.st;
+      o.rz = S.rz;
+      o.rr = S.rr;
+      o.alpha = S.alpha;
+      o.beta = S.beta;
+      o.active = S.active;
+      o.breakdown = S.breakdown;
+      o.nonfinite = S.nonfinite;
+      o.steps = S.steps;
+      o.iter = S.iter;
+      o.converged = S.converged;
+    }
+    const T* t = p_src;
+    p_src = p_dst;
+    p_dst = const_cast<T*>(t);
   }
 }
 
@@ -1115,6 +1275,71 @@ int dby_shape(const DTileArgs<T>& a, cudaStream_t s) {
   return dlaunch_variant<T, MODE, 0, 0>(a, s);
 }
 
+template <typename T, int OX, int OY>
+int dpcg_variant(const DTileArgs<T>& a0, const DamagePcgArgs<T>& c0, cudaStream_t s) {
+  auto kern = h8_damage_pcg_kernel<T, OX, OY>;
+  const int nt = (a0.ts.ox + 2) * (a0.ts.oy + 2), exy = (a0.ts.ox + 1) * (a0.ts.oy + 1);
+  const size_t smem = tile_stage_offset<T>(nt, exy, 3, 8) + sizeof(T) * 2 * kStageH * (size_t)exy;
+  const int threads = tile_threads(a0.ts);
+  static std::mutex mu;
+  static size_t smem_set = 0;
+  static std::map<std::pair<int, size_t>, int> occ;
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (smem > smem_set) {
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return PHASTB_UNSUPPORTED;
+      }
+      smem_set = smem;
+    }
+    auto it = occ.find({threads, smem});
+    if (it == occ.end()) {
+      int b = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        b = 0;
+      }
+      it = occ.emplace(std::make_pair(threads, smem), b).first;
+    }
+    per_sm = it->second;
+  }
+  int dev = 0, sms = 0, coop = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return PHASTB_UNSUPPORTED;
+  }
+  if (!coop || per_sm < 1 || sms < 1) return PHASTB_UNSUPPORTED;
+  const VoxGeom& v = a0.g;
+  const long long tiles_xy = (long long)((v.rx + a0.ts.ox - 1) / a0.ts.ox) * ((v.ry + a0.ts.oy - 1) / a0.ts.oy);
+  // every block must be resident at once (the grid barriers wait for all of them)
+  const long long cap = std::min<long long>((long long)per_sm * sms, kMaxPartials);
+  DTileArgs<T> a = a0;
+  if (a.ts.kz <= 0) a.ts.kz = launch_kz(tiles_xy, v.rz, cap);
+  const long long n_tiles = tiles_xy * ((v.rz + a.ts.kz - 1) / a.ts.kz);
+  const int grid = (int)std::min<long long>(n_tiles, cap);
+  DamagePcgArgs<T> c = c0;
+  void* args[] = {&a, &c};
+  if (cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(threads), args, smem, s) != cudaSuccess) {
+    cudaGetLastError();
+    return PHASTB_UNSUPPORTED;
+  }
+  note_launch();
+  return PHASTB_OK;
+}
+
+// PHASTB_PERSISTENT_PCG=0 runs the damage CG as separate launches per iteration.
+bool persistent_pcg_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("PHASTB_PERSISTENT_PCG");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 template <typename T>
 int h8_damage_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, const T* x, const T* H,
                           double scale, const uint8_t* mask, T* y, RedWs ws, const int* guard, bool dot,
@@ -1188,6 +1413,50 @@ int h8_damage_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* s
 template int h8_damage_tile_launch<double>(const VoxGeom&, const VoxMat<double>&, const uint8_t*, const double*,
                                            const double*, double, const uint8_t*, double*, RedWs, const int*, bool,
                                            cudaStream_t);
+
+template <typename T>
+int h8_damage_pcg_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, const T* H, double scale,
+                         const uint8_t* mask, const PcgWs<T>& w, T* p_alt, T* x, const T* inv_diag, int maxiter,
+                         int mode, cudaStream_t s) {
+  if (mode == PCG_PERIODIC || !persistent_pcg_enabled()) return PHASTB_UNSUPPORTED;
+  DTileArgs<T> a;
+  std::memset(&a, 0, sizeof(a));
+  const TileArgs<T> base = tile_args<T>(v, 2);
+  a.g = v;
+  a.ts = base.ts;
+  a.k = base.k;
+  a.slot = slot;
+  for (int i = 0; i < PHASTB_MAX_SLOTS; ++i) a.Gc[i] = m.Gc[i];
+  a.kappa = double(m.kappa);
+  a.ell = double(m.ell);
+  a.scale = scale;
+  a.H = H;
+  a.mask = mask;
+  if (!tile_ok(a.ts)) return PHASTB_ERR_ARG;
+  DamagePcgArgs<T> c;
+  std::memset(&c, 0, sizeof(c));
+  c.n = v.n_red;
+  c.maxiter = maxiter;
+  c.mode = mode;
+  c.r = w.r;
+  c.z = w.z;
+  c.p = w.p;
+  c.p_alt = p_alt;
+  c.Ap = w.Ap;
+  c.x = x;
+  c.inv_diag = inv_diag;
+  c.part = w.part;
+  c.st = w.st;
+  const int ox = a.ts.ox, oy = a.ts.oy;
+  if (ox == 16 && oy == 8) return dpcg_variant<T, 16, 8>(a, c, s);
+  if (ox == 32 && oy == 4) return dpcg_variant<T, 32, 4>(a, c, s);
+  if (ox == 8 && oy == 8) return dpcg_variant<T, 8, 8>(a, c, s);
+  return dpcg_variant<T, 0, 0>(a, c, s);
+}
+
+template int h8_damage_pcg_launch<double>(const VoxGeom&, const VoxMat<double>&, const uint8_t*, const double*,
+                                          double, const uint8_t*, const PcgWs<double>&, double*, double*,
+                                          const double*, int, int, cudaStream_t);
 template TileArgs<double> tile_args<double>(const VoxGeom&, int);
 template TileArgs<float> tile_args<float>(const VoxGeom&, int);
 template int h8_tile_launch<double>(const TileArgs<double>&, const VoxMat<double>&, int, int, cudaStream_t, bool);

@@ -137,6 +137,20 @@ int h8_damage_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* s
                           double scale, const uint8_t* mask, T* y, RedWs ws, const int* guard, bool dot,
                           cudaStream_t s);
 
+template <typename T>
+struct PcgWs;
+
+// Every iteration of a Jacobi-preconditioned (inv_diag) or unpreconditioned CG
+// on the masked damage operator in one cooperative launch, continuing from the
+// state that pcg_start_kernel left in w (engine.cuh's PcgLoop contract); p_alt
+// is a second direction buffer of n_red values.  PHASTB_UNSUPPORTED when the
+// device cannot run it (or PHASTB_PERSISTENT_PCG=0): the caller iterates with
+// separate launches instead.
+template <typename T>
+int h8_damage_pcg_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, const T* H, double scale,
+                         const uint8_t* mask, const PcgWs<T>& w, T* p_alt, T* x, const T* inv_diag, int maxiter,
+                         int mode, cudaStream_t s);
+
 // y = A(d) x with fused g(d); optional x . y (DOT) and energy (ENERGY).  ws.out
 // receives the E-row sums (kOutE..), the energy and the dot.
 template <typename T>

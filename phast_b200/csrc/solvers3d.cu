@@ -3,6 +3,7 @@
 // staggered-change measure (solid3d/staggered.py:1097-1124).
 #include "engine.cuh"
 #include "h8_kernels.cuh"
+#include "h8_tile.cuh"
 
 #include <cmath>
 
@@ -332,7 +333,7 @@ size_t phastb_h8_box_kkt_workspace_bytes(const phastb_voxel_grid* g) {
   const int n = v.n_red;
   return pcg_ws_bytes<double>(n) + 6 * align_up(sizeof(double) * (size_t)n) + 4 * align_up((size_t)n) +
          h8_scratch_bytes(v, PHASTB_F64) + red_ws_bytes() + align_up(sizeof(double) * (size_t)n) +
-         align_up(sizeof(double) * 8 * (size_t)v.n_elem) + red_ws_bytes();
+         align_up(sizeof(double) * 8 * (size_t)v.n_elem) + red_ws_bytes() + align_up(sizeof(double) * (size_t)n);
 }
 
 int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
@@ -373,6 +374,8 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
   double* Hw = H ? reinterpret_cast<double*>(q + vb) : nullptr;
   // the KKT audit reduces into its own workspace so one host read serves both checks
   RedWs kw = red_ws(q + vb + align_up(sizeof(double) * 8 * (size_t)v.n_elem));
+  // second CG direction buffer of the persistent damage PCG
+  double* p_alt = reinterpret_cast<double*>(q + vb + align_up(sizeof(double) * 8 * (size_t)v.n_elem) + red_ws_bytes());
   const int G = grid_for(n);
   int st;
   if ((st = red_ws_reset(rw, s))) return st;
@@ -402,7 +405,12 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
     DamageCtx fctx{v, mm, slot, Hw, scale, fixed, scratch};
     LinOp<double> A{damage_op, &fctx, sizeof(fctx), damage_op_dot, h8_apply_dot_slot(v, 8, scratch)};
     PcgResult pr{};
-    if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, xd, -lin_tol, max_lin, 10, PCG_STRICT, 0.0, &pr, s)))
+    // all iterations in one persistent launch where the device allows it
+    const PcgLoop loop = [&](int mi) {
+      return h8_damage_pcg_launch<double>(v, mm, slot, Hw, scale, fixed, w, p_alt, xd, invd, mi, PCG_STRICT, s);
+    };
+    if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, xd, -lin_tol, max_lin, 10, PCG_STRICT, 0.0, &pr, s,
+                              &loop)))
       return st;
     // candidate = where(fixed, known, x)
     { note_launch(); where_kernel<<<G, kThreads, 0, s>>>(n, fixed, xd, known, xd); }
