@@ -625,7 +625,7 @@ __device__ __forceinline__ double dtile_pass(const DTileArgs<T>& a, unsigned cha
   constexpr int kHChunks = kStageH * (int)sizeof(T) / 16;
   unsigned char* HS = smem_raw + tile_stage_offset<T>(nt, exy, 3, 8);
   const int tid = threadIdx.x;
-  const T w = T(g.w), ell = T(a.ell), ch = T(2.0 * (1.0 - a.kappa)), sc = T(a.scale);
+  const T w = T(g.w), ch = T(2.0 * (1.0 - a.kappa)), sc = T(a.scale);
   const int tiles_x = (g.rx + ox - 1) / ox, tiles_y = (g.ry + oy - 1) / oy;
   const int tiles_xy = tiles_x * tiles_y;
   const int n_tiles = tiles_xy * ((g.rz + kz - 1) / kz);
@@ -705,7 +705,7 @@ __device__ __forceinline__ double dtile_pass(const DTileArgs<T>& a, unsigned cha
         T out[8];
         if (gi >= 0 && gj >= 0 && gk >= 0) {
           const size_t e = (size_t)gi + (size_t)g.nx * ((size_t)gj + (size_t)g.ny * gk);
-          const T Gc = a.Gc[sl];
+          const T gc_ell = a.gc_ell[sl], k2 = a.gc_k2[sl];
           T dd[8], dq[8];
 #pragma unroll
           for (int L = 0; L < 8; ++L) {
@@ -722,11 +722,10 @@ __device__ __forceinline__ double dtile_pass(const DTileArgs<T>& a, unsigned cha
           }
           T mq[8];
 #pragma unroll
-          for (int q = 0; q < 8; ++q) mq[q] = w * (Gc / ell + ch * hq[q]) * dq[q];
+          for (int q = 0; q < 8; ++q) mq[q] = w * (gc_ell + ch * hq[q]) * dq[q];
           interp_sf_t(mq, out);
           T Dx[2][2], Dy[2][2], Dz[2][2];
           grad_k(dd, a.k, Dx, Dy, Dz);
-          const T k2 = T(2) * w * Gc * ell;
 #pragma unroll
           for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -770,6 +769,18 @@ __device__ __forceinline__ double dtile_pass(const DTileArgs<T>& a, unsigned cha
     if (DOT) accd += double(tdot);
   }
   return accd;
+}
+
+// Per-slot factors of the damage element, Gc / ell and 2 w Gc ell, formed once on
+// the host in the order the element arithmetic would form them (same bits).
+template <typename T>
+void damage_slot_coefs(DTileArgs<T>& a, const VoxMat<T>& m) {
+  const T w = T(a.g.w), ell = T(a.ell);
+  for (int i = 0; i < PHASTB_MAX_SLOTS; ++i) {
+    const T gc = m.Gc[i];
+    a.gc_ell[i] = gc / ell;
+    a.gc_k2[i] = T(2) * w * gc * ell;
+  }
 }
 
 // The damage action as its own launch (MODE == kModeDot also x . y into ws.out[kOutDot]).
@@ -1351,9 +1362,9 @@ int h8_damage_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* s
   a.ts = base.ts;
   a.k = base.k;
   a.slot = slot;
-  for (int i = 0; i < PHASTB_MAX_SLOTS; ++i) a.Gc[i] = m.Gc[i];
   a.kappa = double(m.kappa);
   a.ell = double(m.ell);
+  damage_slot_coefs(a, m);
   a.scale = scale;
   a.H = H;
   a.x = x;
@@ -1426,9 +1437,9 @@ int h8_damage_pcg_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* sl
   a.ts = base.ts;
   a.k = base.k;
   a.slot = slot;
-  for (int i = 0; i < PHASTB_MAX_SLOTS; ++i) a.Gc[i] = m.Gc[i];
   a.kappa = double(m.kappa);
   a.ell = double(m.ell);
+  damage_slot_coefs(a, m);
   a.scale = scale;
   a.H = H;
   a.mask = mask;

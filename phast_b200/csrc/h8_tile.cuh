@@ -118,7 +118,8 @@ struct DTileArgs {
   TileShape ts;
   int pad_;
   const uint8_t* slot;
-  T Gc[PHASTB_MAX_SLOTS];
+  T gc_ell[PHASTB_MAX_SLOTS];  // Gc / ell per material slot
+  T gc_k2[PHASTB_MAX_SLOTS];   // 2 w Gc ell per material slot
   double kappa, ell, scale;
   const T* H;  // (E, 8) history, may be null
   const T* x;
