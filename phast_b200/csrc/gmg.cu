@@ -286,11 +286,19 @@ __global__ void gmg_restrict(VoxGeom f, VoxGeom c, const T* __restrict__ rf, con
   }
 }
 
-// x_f += P x_c (trilinear), masked rows untouched.
+// x_f += P x_c (trilinear), masked rows untouched.  With csums, x_c still
+// carries its mean: each coarse value is read as x_c - csums[comp] / c.n_red
+// (what a separate subtraction pass would have stored, so the same bits).
 template <typename T>
 __global__ void gmg_prolong_add(VoxGeom f, VoxGeom c, const T* __restrict__ xc, const uint8_t* __restrict__ mask,
-                                T* __restrict__ xf, const int* guard) {
+                                T* __restrict__ xf, const double* __restrict__ csums, const int* guard) {
   if (guard && *guard == 0) return;
+  T m0 = T(0), m1 = T(0), m2 = T(0);
+  if (csums) {
+    m0 = T(csums[0] / c.n_red);
+    m1 = T(csums[1] / c.n_red);
+    m2 = T(csums[2] / c.n_red);
+  }
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < f.n_red; n += gridDim.x * blockDim.x) {
     const int i = n % f.rx;
     const int rem = n / f.rx;
@@ -328,9 +336,15 @@ __global__ void gmg_prolong_add(VoxGeom f, VoxGeom c, const T* __restrict__ xc, 
         for (int xx = 0; xx < cxn; ++xx) {
           const size_t cn = (size_t)I[xx] + (size_t)c.rx * ((size_t)J[yy] + (size_t)c.ry * K[z]);
           const T wgt = wx[xx] * wy[yy] * wz[z];
-          a0 += wgt * xc[3 * cn + 0];
-          a1 += wgt * xc[3 * cn + 1];
-          a2 += wgt * xc[3 * cn + 2];
+          T v0 = xc[3 * cn + 0], v1 = xc[3 * cn + 1], v2 = xc[3 * cn + 2];
+          if (csums) {
+            v0 -= m0;
+            v1 -= m1;
+            v2 -= m2;
+          }
+          a0 += wgt * v0;
+          a1 += wgt * v1;
+          a2 += wgt * v2;
         }
     if (!(mask && mask[3 * (size_t)n + 0])) xf[3 * (size_t)n + 0] += a0;
     if (!(mask && mask[3 * (size_t)n + 1])) xf[3 * (size_t)n + 1] += a1;
@@ -353,17 +367,6 @@ __global__ void __launch_bounds__(kThreads) gmg_mean3(int n, const T* __restrict
   reduce_multi<3>(acc, ws);
 }
 
-template <typename T>
-__global__ void gmg_sub_mean3(int n, const double* __restrict__ sums, T* __restrict__ x, const int* guard) {
-  if (guard && *guard == 0) return;
-  const double s0 = sums[0] / n, s1 = sums[1] / n, s2 = sums[2] / n;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    x[3 * (size_t)i] -= T(s0);
-    x[3 * (size_t)i + 1] -= T(s1);
-    x[3 * (size_t)i + 2] -= T(s2);
-  }
-}
-
 // Chebyshev step: first step from x = 0: d = invd * res / theta; x = d.
 // Later steps: res -= Ad; d = c1 d + c2 invd res; x += d.
 template <typename T>
@@ -378,12 +381,26 @@ __global__ void gmg_cheb_first(int n, const T* __restrict__ res, const T* __rest
 }
 
 // First step from x = 0 reading b directly: res = b; d = invd * b / theta; x = d.
+// With bsums, b (a coarse nodal vector, 3 values per node) still carries its
+// mean: b -= bsums[comp] / (n / 3) is applied here and stored back.
 template <typename T>
-__global__ void gmg_cheb_first_b(int n, const T* __restrict__ b, const T* __restrict__ invd, T inv_theta,
-                                 T* __restrict__ res, T* __restrict__ d, T* __restrict__ x, const int* guard) {
+__global__ void gmg_cheb_first_b(int n, T* __restrict__ b, const T* __restrict__ invd, T inv_theta,
+                                 T* __restrict__ res, T* __restrict__ d, T* __restrict__ x,
+                                 const double* __restrict__ bsums, const int* guard) {
   if (guard && *guard == 0) return;
+  T m[3] = {T(0), T(0), T(0)};
+  if (bsums) {
+    const int nn = n / 3;
+    m[0] = T(bsums[0] / nn);
+    m[1] = T(bsums[1] / nn);
+    m[2] = T(bsums[2] / nn);
+  }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const T bi = b[i];
+    T bi = b[i];
+    if (bsums) {
+      bi -= m[i % 3];
+      b[i] = bi;
+    }
     res[i] = bi;
     const T di = invd[i] * bi * inv_theta;
     d[i] = di;
@@ -554,27 +571,34 @@ static int level_apply(const Gmg<T>& M, int l, const T* x, T* y, cudaStream_t s)
   return coarse_apply<T>(M, M.lv[l], x, y, s);
 }
 
+// Mean removal on a fully periodic coarse level (its null space): sums the
+// three components of x into M.rw.out and sets *sums to them; the next kernel
+// that reads x subtracts sums / n_red (gmg_cheb_first_b, gmg_prolong_add), so
+// no separate subtraction pass is launched.  *sums = nullptr when the level
+// has no null space.  No other reduction into M.rw may run in between.
 template <typename T>
-static int remove_mean(const Gmg<T>& M, int l, T* x, cudaStream_t s) {
+static int pending_mean(const Gmg<T>& M, int l, const T* x, const double** sums, cudaStream_t s) {
   const GmgLevel<T>& L = M.lv[l];
+  *sums = nullptr;
   if (!(L.g.px && L.g.py && L.g.pz)) return PHASTB_OK;
   const int nn = L.g.n_red;
   { note_launch(); gmg_mean3<T><<<grid_for(nn), kThreads, 0, s>>>(nn, x, M.rw, M.guard); }
-  { note_launch(); gmg_sub_mean3<T><<<grid_for(nn), kThreads, 0, s>>>(nn, M.rw.out, x, M.guard); }
+  *sums = M.rw.out;
   return last_launch_status();
 }
 
 // Chebyshev smoothing of A x = b on level l; x starts at zero (from_zero) or at
 // its current value.  With need_res, L.res holds b - A x on exit.
 template <typename T>
-static int chebyshev(const Gmg<T>& M, int l, int deg, bool from_zero, bool need_res, cudaStream_t s) {
+static int chebyshev(const Gmg<T>& M, int l, int deg, bool from_zero, bool need_res, const double* bsums,
+                     cudaStream_t s) {
   const GmgLevel<T>& L = M.lv[l];
   const int n = L.n, G = grid_for(n);
   int st;
   const double bmax = M.safety * L.lmax, amin = L.lmax / 30.0;
   const double theta = 0.5 * (bmax + amin), delta = 0.5 * (bmax - amin), sigma = theta / delta;
   if (from_zero) {
-    { note_launch(); gmg_cheb_first_b<T><<<G, kThreads, 0, s>>>(n, L.b, L.invd, T(1.0 / theta), L.res, L.dvec, L.x, M.guard); }
+    { note_launch(); gmg_cheb_first_b<T><<<G, kThreads, 0, s>>>(n, L.b, L.invd, T(1.0 / theta), L.res, L.dvec, L.x, bsums, M.guard); }
   } else {
     if ((st = level_apply(M, l, L.x, L.Ad, s))) return st;
     { note_launch(); gmg_residual<T><<<G, kThreads, 0, s>>>(n, L.b, L.Ad, L.res, M.guard); }
@@ -595,22 +619,27 @@ static int chebyshev(const Gmg<T>& M, int l, int deg, bool from_zero, bool need_
   return last_launch_status();
 }
 
+// V-cycle from level l; on coarse levels the mean of the result L.x is left
+// pending (*xsums, see pending_mean) for the parent's prolongation.
 template <typename T>
-static int vcycle(const Gmg<T>& M, int l, cudaStream_t s) {
+static int vcycle(const Gmg<T>& M, int l, const double** xsums, cudaStream_t s) {
   const GmgLevel<T>& L = M.lv[l];
   int st;
-  if (l > 0 && (st = remove_mean(M, l, L.b, s))) return st;
+  const double* bsums = nullptr;
+  *xsums = nullptr;
+  if (l > 0 && (st = pending_mean(M, l, L.b, &bsums, s))) return st;
   if (l == M.nlev - 1) {
-    if ((st = chebyshev(M, l, M.deg_coarse, true, false, s))) return st;
-    return remove_mean(M, l, L.x, s);
+    if ((st = chebyshev(M, l, M.deg_coarse, true, false, bsums, s))) return st;
+    return pending_mean(M, l, L.x, xsums, s);
   }
-  if ((st = chebyshev(M, l, M.deg, true, true, s))) return st;
+  if ((st = chebyshev(M, l, M.deg, true, true, bsums, s))) return st;
   const GmgLevel<T>& C = M.lv[l + 1];
   { note_launch(); gmg_restrict<T><<<grid_for(C.g.n_red), kThreads, 0, s>>>(L.g, C.g, L.res, l == 0 ? M.mask : nullptr, C.b, M.guard); }
-  if ((st = vcycle(M, l + 1, s))) return st;
-  { note_launch(); gmg_prolong_add<T><<<grid_for(L.g.n_red), kThreads, 0, s>>>(L.g, C.g, C.x, l == 0 ? M.mask : nullptr, L.x, M.guard); }
-  if ((st = chebyshev(M, l, M.deg, false, false, s))) return st;
-  if (l > 0 && (st = remove_mean(M, l, L.x, s))) return st;
+  const double* csums = nullptr;
+  if ((st = vcycle(M, l + 1, &csums, s))) return st;
+  { note_launch(); gmg_prolong_add<T><<<grid_for(L.g.n_red), kThreads, 0, s>>>(L.g, C.g, C.x, l == 0 ? M.mask : nullptr, L.x, csums, M.guard); }
+  if ((st = chebyshev(M, l, M.deg, false, false, nullptr, s))) return st;
+  if (l > 0 && (st = pending_mean(M, l, L.x, xsums, s))) return st;
   return last_launch_status();
 }
 
@@ -755,25 +784,21 @@ static int gmg_setup(Gmg<T>& M, const VoxMat<T>& mat, const uint8_t* slot, const
   return PHASTB_OK;
 }
 
-template <typename T>
-__global__ void gmg_copy(int n, const T* __restrict__ a, T* __restrict__ b, const int* guard) {
-  if (guard && *guard == 0) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
-}
-
 // z = M^-1 r: V-cycle on the fluctuation rows, Jacobi on the free E rows.
 template <typename T>
 static int gmg_precond_apply(const void* ctx, const T* r, T* z, const int* guard, cudaStream_t s) {
   const Gmg<T>& M = *static_cast<const Gmg<T>*>(ctx);
   const GmgLevel<T>& L = M.lv[0];
-  const int n = L.n;
   int st;
   // every V-cycle kernel turns into a no-op once the Krylov solve has converged
   Gmg<T> Mg = M;
   Mg.guard = guard;
-  { note_launch(); gmg_copy<T><<<grid_for(n), kThreads, 0, s>>>(n, r, L.b, guard); }
-  if ((st = vcycle(Mg, 0, s))) return st;
-  { note_launch(); gmg_copy<T><<<grid_for(n), kThreads, 0, s>>>(n, L.x, z, guard); }
+  // the fine level reads its right-hand side from r (never written there: the
+  // fine level has no pending mean) and builds its iterate directly in z
+  Mg.lv[0].b = const_cast<T*>(r);
+  Mg.lv[0].x = z;
+  const double* xsums = nullptr;
+  if ((st = vcycle(Mg, 0, &xsums, s))) return st;
   { note_launch(); gmg_eblock<T><<<1, 32, 0, s>>>(3 * L.g.n_red, r, L.diag, M.fmask, z, guard); }
   return last_launch_status();
 }
