@@ -406,6 +406,39 @@ def run_reference(args, rank, world):
     }
 
 
+def run_damage_cg_only(args, device):
+    """Box-KKT damage solves only (the persistent damage CG), on an N^3 cell with a
+    seeded history field: the profiling case of h8_damage_pcg_kernel."""
+    from phast_b200 import solid3d as s3
+    op, _ = build_cell(device, args.cell)
+    gen = torch.Generator(device="cpu").manual_seed(0)
+    H = (torch.rand(op.n_elements, 8, generator=gen, dtype=torch.float64) * 50.0).to(device)
+    lower = torch.zeros(op.n_red, dtype=torch.float64, device=device)
+    system = op.damage_system(H)
+
+    def solve():
+        return s3.solve_h8_scalar_box_kkt(system, lower_bound=lower, upper_bound=1.0, initial=lower,
+                                          linear_tolerance=1e-10, kkt_tolerance=1e-8, check_bounds=False)
+    for _ in range(args.warmup):
+        res = solve()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        res = solve()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    its = res.total_pcg_iterations
+    # per CG iteration: z, p read and Ap, p written (action), x, p, r, Ap, 1/diag read and x, r, z
+    # written (update): 12 n words, plus the history (8 words) and slot byte of every element
+    alg = (12 * op.n_red + 8 * op.n_elements) * 8 + op.n_elements
+    print(json.dumps({"kernel": "persistent damage CG (box-KKT)", "cell": args.cell, "ms_per_solve": ms,
+                      "cg_iterations": its, "active_set_iterations": res.active_set_iterations,
+                      "us_per_cg_iteration": 1e3 * ms / max(its, 1),
+                      "algorithmic_GBps": alg * its / ms / 1e6}), flush=True)
+
+
 def run_kernel_only(args, device):
     """Elastic-action launches only, on an N^3 cell (the profiling case for ncu)."""
     op, _ = build_cell(device, args.cell)
@@ -444,6 +477,7 @@ def main():
     ap.add_argument("--kernel-only", action="store_true", help="time the elastic action alone (profiling case)")
     ap.add_argument("--cell", type=int, default=N_CELL, help="cell edge in voxels for --kernel-only")
     ap.add_argument("--fp32", action="store_true", help="FP32 storage/arithmetic for --kernel-only")
+    ap.add_argument("--damage-cg", action="store_true", help="with --kernel-only: time box-KKT damage solves instead")
     ap.add_argument("--tile", default="", help="pin the tile shape ox,oy,kz for --kernel-only (else the solver's shape)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -460,7 +494,10 @@ def main():
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
     if args.kernel_only:
-        run_kernel_only(args, device)
+        if args.damage_cg:
+            run_damage_cg_only(args, device)
+        else:
+            run_kernel_only(args, device)
         return
     if world > 1:
         import datetime
