@@ -367,16 +367,18 @@ __global__ void __launch_bounds__(kThreads) gmg_mean3(int n, const T* __restrict
   reduce_multi<3>(acc, ws);
 }
 
-// Chebyshev step: first step from x = 0: d = invd * res / theta; x = d.
-// Later steps: res -= Ad; d = c1 d + c2 invd res; x += d.
+// First Chebyshev step from the current x: res = b - Ax; d = invd * res / theta; x += d.
 template <typename T>
-__global__ void gmg_cheb_first(int n, const T* __restrict__ res, const T* __restrict__ invd, T inv_theta,
-                               T* __restrict__ d, T* __restrict__ x, int accumulate, const int* guard) {
+__global__ void gmg_cheb_first_res(int n, const T* __restrict__ b, const T* __restrict__ Ax,
+                                   const T* __restrict__ invd, T inv_theta, T* __restrict__ res, T* __restrict__ d,
+                                   T* __restrict__ x, const int* guard) {
   if (guard && *guard == 0) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const T di = invd[i] * res[i] * inv_theta;
+    const T r = b[i] - Ax[i];
+    res[i] = r;
+    const T di = invd[i] * r * inv_theta;
     d[i] = di;
-    x[i] = accumulate ? x[i] + di : di;
+    x[i] = x[i] + di;
   }
 }
 
@@ -426,12 +428,6 @@ __global__ void gmg_sub_inplace(int n, T* __restrict__ res, const T* __restrict_
 }
 
 // res = b - A x
-template <typename T>
-__global__ void gmg_residual(int n, const T* __restrict__ b, const T* __restrict__ Ax, T* __restrict__ res, const int* guard) {
-  if (guard && *guard == 0) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) res[i] = b[i] - Ax[i];
-}
-
 template <typename T>
 __global__ void gmg_invert(int n, const T* __restrict__ diag, const uint8_t* __restrict__ mask, T* __restrict__ inv) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -601,8 +597,7 @@ static int chebyshev(const Gmg<T>& M, int l, int deg, bool from_zero, bool need_
     { note_launch(); gmg_cheb_first_b<T><<<G, kThreads, 0, s>>>(n, L.b, L.invd, T(1.0 / theta), L.res, L.dvec, L.x, bsums, M.guard); }
   } else {
     if ((st = level_apply(M, l, L.x, L.Ad, s))) return st;
-    { note_launch(); gmg_residual<T><<<G, kThreads, 0, s>>>(n, L.b, L.Ad, L.res, M.guard); }
-    { note_launch(); gmg_cheb_first<T><<<G, kThreads, 0, s>>>(n, L.res, L.invd, T(1.0 / theta), L.dvec, L.x, 1, M.guard); }
+    { note_launch(); gmg_cheb_first_res<T><<<G, kThreads, 0, s>>>(n, L.b, L.Ad, L.invd, T(1.0 / theta), L.res, L.dvec, L.x, M.guard); }
   }
   // later steps ping-pong the direction between dvec and Ad
   T* cur = L.dvec;
