@@ -245,11 +245,14 @@ __device__ __forceinline__ int fine_of(int i, int n_f, int periodic, bool& ok) {
 }
 
 // r_c = R r_f = P^T r_f (full weighting).  The fine vector may carry a mask
-// (rows held at zero are skipped).
+// (rows held at zero are skipped).  With `sum_ws`, the kernel also sums the
+// three components of r_c into sum_ws.out (the coarse level's mean, in the
+// order and grouping of gmg_mean3 over the same grid, so the same bits).
 template <typename T>
 __global__ void gmg_restrict(VoxGeom f, VoxGeom c, const T* __restrict__ rf, const uint8_t* __restrict__ mask,
-                             T* __restrict__ rc, const int* guard) {
+                             T* __restrict__ rc, RedWs sum_ws, int want_sum, const int* guard) {
   if (guard && *guard == 0) return;
+  double acc[3] = {0, 0, 0};
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < c.n_red; n += gridDim.x * blockDim.x) {
     const int I = n % c.rx;
     const int rem = n / c.rx;
@@ -283,7 +286,11 @@ __global__ void gmg_restrict(VoxGeom f, VoxGeom c, const T* __restrict__ rf, con
     rc[3 * (size_t)n + 0] = a0;
     rc[3 * (size_t)n + 1] = a1;
     rc[3 * (size_t)n + 2] = a2;
+    acc[0] += double(a0);
+    acc[1] += double(a1);
+    acc[2] += double(a2);
   }
+  if (want_sum) reduce_multi<3>(acc, sum_ws);
 }
 
 // x_f += P x_c (trilinear), masked rows untouched.  With csums, x_c still
@@ -368,17 +375,24 @@ __global__ void __launch_bounds__(kThreads) gmg_mean3(int n, const T* __restrict
 }
 
 // First Chebyshev step from the current x: res = b - Ax; d = invd * res / theta; x += d.
+// With e_nu >= 0 (the fine level's last elementwise pass), the six E rows
+// i = e_nu.. of x instead receive the preconditioner's Jacobi step on the
+// macro-strain block, x_E = e_mask ? 0 : b_E / e_diag.
 template <typename T>
 __global__ void gmg_cheb_first_res(int n, const T* __restrict__ b, const T* __restrict__ Ax,
                                    const T* __restrict__ invd, T inv_theta, T* __restrict__ res, T* __restrict__ d,
-                                   T* __restrict__ x, const int* guard) {
+                                   T* __restrict__ x, int e_nu, const T* __restrict__ e_diag,
+                                   const uint8_t* __restrict__ e_mask, const int* guard) {
   if (guard && *guard == 0) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const T r = b[i] - Ax[i];
     res[i] = r;
     const T di = invd[i] * r * inv_theta;
     d[i] = di;
-    x[i] = x[i] + di;
+    if (e_nu >= 0 && i >= e_nu && i < e_nu + 6)
+      x[i] = e_mask[i] ? T(0) : b[i] / e_diag[i];
+    else
+      x[i] = x[i] + di;
   }
 }
 
@@ -480,17 +494,6 @@ __global__ void gmg_init_vec(int n, const uint8_t* __restrict__ mask, T* __restr
 }
 
 // E block of the preconditioned vector: z_E = r_E / diag_E on free rows
-template <typename T>
-__global__ void gmg_eblock(int nu, const T* __restrict__ r, const T* __restrict__ diag,
-                           const uint8_t* __restrict__ mask, T* __restrict__ z, const int* guard) {
-  if (guard && *guard == 0) return;
-  const int k = threadIdx.x;
-  if (k < 6) {
-    const size_t i = (size_t)nu + k;
-    z[i] = mask[i] ? T(0) : r[i] / diag[i];
-  }
-}
-
 template <typename Ts, typename Td>
 __global__ void gmg_convert(int n, const Ts* __restrict__ a, Td* __restrict__ b) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = Td(a[i]);
@@ -597,7 +600,10 @@ static int chebyshev(const Gmg<T>& M, int l, int deg, bool from_zero, bool need_
     { note_launch(); gmg_cheb_first_b<T><<<G, kThreads, 0, s>>>(n, L.b, L.invd, T(1.0 / theta), L.res, L.dvec, L.x, bsums, M.guard); }
   } else {
     if ((st = level_apply(M, l, L.x, L.Ad, s))) return st;
-    { note_launch(); gmg_cheb_first_res<T><<<G, kThreads, 0, s>>>(n, L.b, L.Ad, L.invd, T(1.0 / theta), L.res, L.dvec, L.x, M.guard); }
+    // on the fine level this is the last pass over the E rows of x: it also
+    // writes their Jacobi step (the V-cycle smooths the nodal block only)
+    const int e_nu = l == 0 ? 3 * L.g.n_red : -1;
+    { note_launch(); gmg_cheb_first_res<T><<<G, kThreads, 0, s>>>(n, L.b, L.Ad, L.invd, T(1.0 / theta), L.res, L.dvec, L.x, e_nu, L.diag, M.fmask, M.guard); }
   }
   // later steps ping-pong the direction between dvec and Ad
   T* cur = L.dvec;
@@ -614,24 +620,25 @@ static int chebyshev(const Gmg<T>& M, int l, int deg, bool from_zero, bool need_
   return last_launch_status();
 }
 
-// V-cycle from level l; on coarse levels the mean of the result L.x is left
-// pending (*xsums, see pending_mean) for the parent's prolongation.
+// V-cycle from level l.  bsums: the pending mean of L.b, summed by the
+// parent's restriction (nullptr on the fine level and on levels without a null
+// space); on coarse levels the mean of the result L.x is left pending
+// (*xsums, see pending_mean) for the parent's prolongation.
 template <typename T>
-static int vcycle(const Gmg<T>& M, int l, const double** xsums, cudaStream_t s) {
+static int vcycle(const Gmg<T>& M, int l, const double* bsums, const double** xsums, cudaStream_t s) {
   const GmgLevel<T>& L = M.lv[l];
   int st;
-  const double* bsums = nullptr;
   *xsums = nullptr;
-  if (l > 0 && (st = pending_mean(M, l, L.b, &bsums, s))) return st;
   if (l == M.nlev - 1) {
     if ((st = chebyshev(M, l, M.deg_coarse, true, false, bsums, s))) return st;
     return pending_mean(M, l, L.x, xsums, s);
   }
   if ((st = chebyshev(M, l, M.deg, true, true, bsums, s))) return st;
   const GmgLevel<T>& C = M.lv[l + 1];
-  { note_launch(); gmg_restrict<T><<<grid_for(C.g.n_red), kThreads, 0, s>>>(L.g, C.g, L.res, l == 0 ? M.mask : nullptr, C.b, M.guard); }
+  const int cper = C.g.px && C.g.py && C.g.pz;  // the coarse level has a null space: sum its mean
+  { note_launch(); gmg_restrict<T><<<grid_for(C.g.n_red), kThreads, 0, s>>>(L.g, C.g, L.res, l == 0 ? M.mask : nullptr, C.b, M.rw, cper, M.guard); }
   const double* csums = nullptr;
-  if ((st = vcycle(M, l + 1, &csums, s))) return st;
+  if ((st = vcycle(M, l + 1, cper ? M.rw.out : nullptr, &csums, s))) return st;
   { note_launch(); gmg_prolong_add<T><<<grid_for(L.g.n_red), kThreads, 0, s>>>(L.g, C.g, C.x, l == 0 ? M.mask : nullptr, L.x, csums, M.guard); }
   if ((st = chebyshev(M, l, M.deg, false, false, nullptr, s))) return st;
   if (l > 0 && (st = pending_mean(M, l, L.x, xsums, s))) return st;
@@ -783,7 +790,6 @@ static int gmg_setup(Gmg<T>& M, const VoxMat<T>& mat, const uint8_t* slot, const
 template <typename T>
 static int gmg_precond_apply(const void* ctx, const T* r, T* z, const int* guard, cudaStream_t s) {
   const Gmg<T>& M = *static_cast<const Gmg<T>*>(ctx);
-  const GmgLevel<T>& L = M.lv[0];
   int st;
   // every V-cycle kernel turns into a no-op once the Krylov solve has converged
   Gmg<T> Mg = M;
@@ -793,8 +799,8 @@ static int gmg_precond_apply(const void* ctx, const T* r, T* z, const int* guard
   Mg.lv[0].b = const_cast<T*>(r);
   Mg.lv[0].x = z;
   const double* xsums = nullptr;
-  if ((st = vcycle(Mg, 0, &xsums, s))) return st;
-  { note_launch(); gmg_eblock<T><<<1, 32, 0, s>>>(3 * L.g.n_red, r, L.diag, M.fmask, z, guard); }
+  // the fine level's post-smoothing also writes z's E rows (gmg_cheb_first_res)
+  if ((st = vcycle(Mg, 0, nullptr, &xsums, s))) return st;
   return last_launch_status();
 }
 
