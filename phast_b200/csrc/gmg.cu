@@ -563,10 +563,20 @@ static int level_cheb(const Gmg<T>& M, int l, const T* din, T* dout, double c1, 
   return h8_tile_launch<T>(a, M.mat, kCoefQP, kModeCheb, s);
 }
 
+// y = A x on level l.  The fine level's smoother masks the E rows, so its action
+// skips them (kModeNodal: no E-row sums, y_E = 0, as the masked full action gives).
 template <typename T>
 static int level_apply(const Gmg<T>& M, int l, const T* x, T* y, cudaStream_t s) {
-  if (l == 0)
-    return h8_mech_apply_t<T>(M.lv[0].g, M.mat, M.slot, x, nullptr, M.dfield, M.mask, y, M.scratch, M.guard, s);
+  if (l == 0) {
+    TileArgs<T> a = tile_args<T>(M.lv[0].g, 0);
+    a.slot = M.slot;
+    a.d = M.dfield;
+    a.x = x;
+    a.y = y;
+    a.mask = M.mask;
+    a.guard = M.guard;
+    return h8_tile_launch<T>(a, M.mat, M.mat.iso ? kCoefIso : kCoefAniso, kModeNodal, s);
+  }
   return coarse_apply<T>(M, M.lv[l], x, y, s);
 }
 

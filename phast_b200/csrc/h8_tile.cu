@@ -228,11 +228,14 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
   if (a.guard && *a.guard == 0) return;
   constexpr bool SLOT = COEF != kCoefQP;
   constexpr bool DOT = MODE == kModeDot, ENERGY = MODE == kModeEnergy, CHEB = MODE == kModeCheb;
-  // E rows (macro strain) exist on the fine operator; a Chebyshev step leaves them alone (masked)
-  constexpr bool EROWS = SLOT && !CHEB;
+  // E rows (macro strain) exist on the fine operator; a Chebyshev step and a
+  // nodal-block action leave them alone (masked)
+  constexpr bool NODAL = MODE == kModeNodal;
+  constexpr bool EROWS = SLOT && !CHEB && !NODAL;
   constexpr bool RED = EROWS || DOT || ENERGY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const VoxGeom& g = a.g;
+  if (NODAL && blockIdx.x == 0 && threadIdx.x < 6 && a.y) a.y[3 * (size_t)g.n_red + threadIdx.x] = T(0);
   const T* __restrict__ x = a.x;
   const T* __restrict__ d = SLOT ? a.d : nullptr;
   // OX, OY > 0: a compiled tile shape (constant shared-memory offsets)
@@ -1109,17 +1112,19 @@ int by_shape(const TileArgs<T>& a, const VoxMat<T>& m, cudaStream_t s) {
 
 template <typename T>
 int dispatch(const TileArgs<T>& a, const VoxMat<T>& m, int coef, int mode, cudaStream_t s) {
-  switch (coef * 4 + mode) {
-    case kCoefIso * 4 + kModeApply: return by_shape<T, kCoefIso, kModeApply>(a, m, s);
-    case kCoefIso * 4 + kModeDot: return by_shape<T, kCoefIso, kModeDot>(a, m, s);
-    case kCoefIso * 4 + kModeEnergy: return launch_variant<T, kCoefIso, kModeEnergy, 0, 0>(a, m, s);
-    case kCoefIso * 4 + kModeCheb: return by_shape<T, kCoefIso, kModeCheb>(a, m, s);
-    case kCoefAniso * 4 + kModeApply: return launch_variant<T, kCoefAniso, kModeApply, 0, 0>(a, m, s);
-    case kCoefAniso * 4 + kModeDot: return launch_variant<T, kCoefAniso, kModeDot, 0, 0>(a, m, s);
-    case kCoefAniso * 4 + kModeEnergy: return launch_variant<T, kCoefAniso, kModeEnergy, 0, 0>(a, m, s);
-    case kCoefAniso * 4 + kModeCheb: return launch_variant<T, kCoefAniso, kModeCheb, 0, 0>(a, m, s);
-    case kCoefQP * 4 + kModeApply: return by_shape<T, kCoefQP, kModeApply>(a, m, s);
-    case kCoefQP * 4 + kModeCheb: return by_shape<T, kCoefQP, kModeCheb>(a, m, s);
+  switch (coef * 8 + mode) {
+    case kCoefIso * 8 + kModeApply: return by_shape<T, kCoefIso, kModeApply>(a, m, s);
+    case kCoefIso * 8 + kModeDot: return by_shape<T, kCoefIso, kModeDot>(a, m, s);
+    case kCoefIso * 8 + kModeEnergy: return launch_variant<T, kCoefIso, kModeEnergy, 0, 0>(a, m, s);
+    case kCoefIso * 8 + kModeCheb: return by_shape<T, kCoefIso, kModeCheb>(a, m, s);
+    case kCoefIso * 8 + kModeNodal: return by_shape<T, kCoefIso, kModeNodal>(a, m, s);
+    case kCoefAniso * 8 + kModeApply: return launch_variant<T, kCoefAniso, kModeApply, 0, 0>(a, m, s);
+    case kCoefAniso * 8 + kModeDot: return launch_variant<T, kCoefAniso, kModeDot, 0, 0>(a, m, s);
+    case kCoefAniso * 8 + kModeEnergy: return launch_variant<T, kCoefAniso, kModeEnergy, 0, 0>(a, m, s);
+    case kCoefAniso * 8 + kModeCheb: return launch_variant<T, kCoefAniso, kModeCheb, 0, 0>(a, m, s);
+    case kCoefAniso * 8 + kModeNodal: return launch_variant<T, kCoefAniso, kModeNodal, 0, 0>(a, m, s);
+    case kCoefQP * 8 + kModeApply: return by_shape<T, kCoefQP, kModeApply>(a, m, s);
+    case kCoefQP * 8 + kModeCheb: return by_shape<T, kCoefQP, kModeCheb>(a, m, s);
     default: return PHASTB_ERR_ARG;
   }
 }

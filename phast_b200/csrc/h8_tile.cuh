@@ -68,8 +68,10 @@ enum ApplyOut { kOutE = 0, kOutEnergy = 6, kOutDot = 7, kApplyOuts = 8 };
 // Element coefficients: material slot with g(d) (isotropic / general Voigt), or
 // per-Gauss-point isotropic moduli (multigrid coarse levels, no macro strain).
 enum TileCoef { kCoefIso = 0, kCoefAniso = 1, kCoefQP = 2 };
-// Node epilogue: y = A x; y and x . y; y and the energy; one Chebyshev step.
-enum TileMode { kModeApply = 0, kModeDot = 1, kModeEnergy = 2, kModeCheb = 3 };
+// Node epilogue: y = A x; y and x . y; y and the energy; one Chebyshev step;
+// y = A x on the nodal block only (the macro-strain E rows of x are not read,
+// those of y are set to zero: a smoother's residual with the E rows masked).
+enum TileMode { kModeApply = 0, kModeDot = 1, kModeEnergy = 2, kModeCheb = 3, kModeNodal = 4 };
 
 // Gauss-point constants of the action: N1 weights with the 1/h of each axis
 // folded in (the last interpolation stage of a derivative applies them).
