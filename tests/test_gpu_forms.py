@@ -116,15 +116,15 @@ def test_device_side_loop_matches_chunked_loop():
         "y, j = s3.solve_constrained_form(op, s3.MechForm(precond='gmg', mixed=True), fixed_mask=m, fixed_values=v,"
         " d=d, rtol=1e-10, maxiter=20000);"
         "np.save(sys.argv[1], np.stack([x.cpu().numpy(), y.cpu().numpy()]))")
+    import tempfile
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     outs = {}
-    for flag in ("0", "1"):
-        path = os.path.join(root, "gpurun_out" if os.path.isdir(os.path.join(root, "gpurun_out")) else "",
-                            f"_loop_{flag}.npy")
-        env = dict(os.environ, PHASTB_DEVICE_LOOP=flag)
-        subprocess.run([sys.executable, "-c", code, path], check=True, cwd=root, env=env, timeout=600)
-        outs[flag] = np.load(path)
-        os.remove(path)
+    with tempfile.TemporaryDirectory() as tmp:
+        for flag in ("0", "1"):
+            path = os.path.join(tmp, f"loop_{flag}.npy")
+            env = dict(os.environ, PHASTB_DEVICE_LOOP=flag)
+            subprocess.run([sys.executable, "-c", code, path], check=True, cwd=root, env=env, timeout=600)
+            outs[flag] = np.load(path)
     for k in range(2):
         a, b = outs["0"][k], outs["1"][k]
         assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(a)
