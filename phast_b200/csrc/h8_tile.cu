@@ -1429,6 +1429,9 @@ int h8_damage_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* s
 template int h8_damage_tile_launch<double>(const VoxGeom&, const VoxMat<double>&, const uint8_t*, const double*,
                                            const double*, double, const uint8_t*, double*, RedWs, const int*, bool,
                                            cudaStream_t);
+template int h8_damage_tile_launch<float>(const VoxGeom&, const VoxMat<float>&, const uint8_t*, const float*,
+                                          const float*, double, const uint8_t*, float*, RedWs, const int*, bool,
+                                          cudaStream_t);
 
 template <typename T>
 int h8_damage_pcg_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slot, const T* H, double scale,
@@ -1473,6 +1476,9 @@ int h8_damage_pcg_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* sl
 template int h8_damage_pcg_launch<double>(const VoxGeom&, const VoxMat<double>&, const uint8_t*, const double*,
                                           double, const uint8_t*, const PcgWs<double>&, double*, double*,
                                           const double*, int, int, cudaStream_t);
+template int h8_damage_pcg_launch<float>(const VoxGeom&, const VoxMat<float>&, const uint8_t*, const float*,
+                                         double, const uint8_t*, const PcgWs<float>&, float*, float*, const float*,
+                                         int, int, cudaStream_t);
 template TileArgs<double> tile_args<double>(const VoxGeom&, int);
 template TileArgs<float> tile_args<float>(const VoxGeom&, int);
 template int h8_tile_launch<double>(const TileArgs<double>&, const VoxMat<double>&, int, int, cudaStream_t, bool);

@@ -67,6 +67,38 @@ static int damage_op_dot(const void* c, const double* x, double* y, const int* g
   return h8_damage_launch(k->v, k->m, k->slot, 3, x, k->H, k->scale, y, k->mask, k->scratch, guard, s);
 }
 
+// The damage action in FP32 (the inner solves of the mixed-precision box-KKT CG).
+struct DamageCtx32 {
+  VoxGeom v;
+  VoxMat<float> m;
+  const uint8_t* slot;
+  const float* H;
+  double scale;
+  const uint8_t* mask;
+  RedWs ws;
+};
+
+static int damage_op32(const void* c, const float* x, float* y, const int* guard, cudaStream_t s) {
+  const DamageCtx32* k = static_cast<const DamageCtx32*>(c);
+  return h8_damage_tile_launch<float>(k->v, k->m, k->slot, x, k->H, k->scale, k->mask, y, k->ws, guard, false, s);
+}
+
+static int damage_op_dot32(const void* c, const float* x, float* y, const int* guard, cudaStream_t s) {
+  const DamageCtx32* k = static_cast<const DamageCtx32*>(c);
+  return h8_damage_tile_launch<float>(k->v, k->m, k->slot, x, k->H, k->scale, k->mask, y, k->ws, guard, true, s);
+}
+
+// PHASTB_DAMAGE_MIXED=1: the box-KKT's Dirichlet CG runs in FP32 (FP64 dot
+// products) under FP64 iterative refinement on the true FP64 residual, to the
+// same FP64 threshold.
+static bool damage_mixed_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("PHASTB_DAMAGE_MIXED");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
 // xc = where(fixed, vals, 0); x0f = where(free, x0, 0); invd = 1/where(free, diag, 1)
 __global__ void constrained_setup_kernel(int n, const uint8_t* __restrict__ fixed, const double* __restrict__ vals,
                                          const double* __restrict__ x0, double* __restrict__ xc,
@@ -91,6 +123,15 @@ __global__ void __launch_bounds__(kThreads) constrained_rhs_kernel(int n, const 
     acc[0] += v * v;
   }
   reduce_multi<1>(acc, ws);
+}
+
+__global__ void to_f32_kernel(size_t n, const double* __restrict__ a, float* __restrict__ b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = float(a[i]);
+}
+
+__global__ void add_f32_kernel(int n, const float* __restrict__ dx, double* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] += double(dx[i]);
 }
 
 __global__ void where_kernel(int n, const uint8_t* __restrict__ fixed, const double* __restrict__ a,
@@ -333,7 +374,10 @@ size_t phastb_h8_box_kkt_workspace_bytes(const phastb_voxel_grid* g) {
   const int n = v.n_red;
   return pcg_ws_bytes<double>(n) + 6 * align_up(sizeof(double) * (size_t)n) + 4 * align_up((size_t)n) +
          h8_scratch_bytes(v, PHASTB_F64) + red_ws_bytes() + align_up(sizeof(double) * (size_t)n) +
-         align_up(sizeof(double) * 8 * (size_t)v.n_elem) + red_ws_bytes() + align_up(sizeof(double) * (size_t)n);
+         align_up(sizeof(double) * 8 * (size_t)v.n_elem) + red_ws_bytes() + align_up(sizeof(double) * (size_t)n) +
+         // FP32 inner solves: CG workspace, right-hand side, correction, 1/diag, second direction, H, dot
+         pcg_ws_bytes<float>(n) + 4 * align_up(sizeof(float) * (size_t)n) +
+         align_up(sizeof(float) * 8 * (size_t)v.n_elem) + red_ws_bytes();
 }
 
 int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
@@ -376,14 +420,33 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
   RedWs kw = red_ws(q + vb + align_up(sizeof(double) * 8 * (size_t)v.n_elem));
   // second CG direction buffer of the persistent damage PCG
   double* p_alt = reinterpret_cast<double*>(q + vb + align_up(sizeof(double) * 8 * (size_t)v.n_elem) + red_ws_bytes());
+  // FP32 buffers of the mixed-precision inner solves
+  char* q32 = reinterpret_cast<char*>(p_alt) + vb;
+  PcgWs<float> w32 = pcg_ws<float>(q32, n);
+  q32 += pcg_ws_bytes<float>(n);
+  const size_t fb = align_up(sizeof(float) * (size_t)n);
+  float* r32 = reinterpret_cast<float*>(q32);
+  float* dx32 = reinterpret_cast<float*>(q32 + fb);
+  float* invd32 = reinterpret_cast<float*>(q32 + 2 * fb);
+  float* palt32 = reinterpret_cast<float*>(q32 + 3 * fb);
+  float* H32 = H ? reinterpret_cast<float*>(q32 + 4 * fb) : nullptr;
+  RedWs dw32 = red_ws(q32 + 4 * fb + align_up(sizeof(float) * 8 * (size_t)v.n_elem));
+  const bool mixed = damage_mixed_enabled();
   const int G = grid_for(n);
   int st;
   if ((st = red_ws_reset(rw, s))) return st;
   if ((st = red_ws_reset(aw, s))) return st;
   if ((st = red_ws_reset(kw, s))) return st;
+  if (mixed && (st = red_ws_reset(dw32, s))) return st;
   if (H && (st = cuda_status(cudaMemcpyAsync(Hw, H, sizeof(double) * 8 * (size_t)v.n_elem,
                                               cudaMemcpyDeviceToDevice, s))))
     return st;
+  const VoxMat<float> m32 = make_vox_mat<float>(*m);
+  if (mixed && H) {
+    const size_t ne = 8 * (size_t)v.n_elem;
+    { note_launch(); to_f32_kernel<<<grid_for((long long)ne), kThreads, 0, s>>>(ne, Hw, H32); }
+    if ((st = last_launch_status())) return st;
+  }
   auto finish = [&](int code) -> int {
     const int e = cuda_status(cudaMemcpyAsync(d_out, xd, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     return e ? e : code;
@@ -405,13 +468,66 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
     DamageCtx fctx{v, mm, slot, Hw, scale, fixed, scratch};
     LinOp<double> A{damage_op, &fctx, sizeof(fctx), damage_op_dot, h8_apply_dot_slot(v, 8, scratch)};
     PcgResult pr{};
-    // all iterations in one persistent launch where the device allows it
-    const PcgLoop loop = [&](int mi) {
-      return h8_damage_pcg_launch<double>(v, mm, slot, Hw, scale, fixed, w, p_alt, xd, invd, mi, PCG_STRICT, s);
-    };
-    if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, xd, -lin_tol, max_lin, 10, PCG_STRICT, 0.0, &pr, s,
-                              &loop)))
-      return st;
+    if (!mixed) {
+      // all iterations in one persistent launch where the device allows it
+      const PcgLoop loop = [&](int mi) {
+        return h8_damage_pcg_launch<double>(v, mm, slot, Hw, scale, fixed, w, p_alt, xd, invd, mi, PCG_STRICT, s);
+      };
+      if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, xd, -lin_tol, max_lin, 10, PCG_STRICT, 0.0, &pr, s,
+                                &loop)))
+        return st;
+    } else {
+      // FP64 residual of the start iterate on the free set; the threshold is
+      // lin_tol * max(||r0||, 1) as in the FP64 solve
+      if ((st = damage_op(&fctx, xd, w.Ap, nullptr, s))) return st;
+      { note_launch(); constrained_rhs_kernel<<<G, kThreads, 0, s>>>(n, fixed, bf, w.Ap, w.r, rw); }
+      { note_launch(); to_f32_kernel<<<G, kThreads, 0, s>>>((size_t)n, invd, invd32); }
+      if ((st = last_launch_status())) return st;
+      double rr0;
+      if ((st = red_ws_fetch(rw, &rr0, 1, s))) return st;
+      const double thr = lin_tol * std::max(std::sqrt(rr0), 1.0);
+      DamageCtx32 c32{v, m32, slot, H32, scale, fixed, dw32};
+      LinOp<float> A32{damage_op32, &c32, sizeof(c32), damage_op_dot32, dw32.out + kOutDot};
+      const PcgLoop loop32 = [&](int mi) {
+        return h8_damage_pcg_launch<float>(v, m32, slot, H32, scale, fixed, w32, palt32, dx32, invd32, mi,
+                                           PCG_STRICT, s);
+      };
+      int inner = 0, conv = 0;
+      for (int k = 0; k < 30 && inner < max_lin; ++k) {
+        // correction equation in FP32; the start kernel checks the FP64 residual
+        // norm (rw.out) against thr first and does nothing once it holds
+        { note_launch(); to_f32_kernel<<<G, kThreads, 0, s>>>((size_t)n, w.r, r32); }
+        if ((st = cuda_status(cudaMemsetAsync(dx32, 0, sizeof(float) * n, s)))) return st;
+        PcgThreshold tin;
+        tin.abs = 0.5 * thr;
+        tin.rel = 1e-5;
+        tin.outer_rr = rw.out;
+        tin.outer_thr = thr;
+        PcgResult pi{};
+        if ((st = pcg_run_thr<float>(A32, n, w32, r32, invd32, nullptr, dx32, tin, max_lin - inner, 10, PCG_STRICT,
+                                     &pi, s, &loop32)))
+          return st;
+        if (pi.outer_done) {
+          conv = 1;
+          break;
+        }
+        inner += pi.iterations;
+        if (pi.nonfinite) pr.nonfinite = 1;
+        if (pi.breakdown) pr.breakdown = 1;
+        if (pr.nonfinite || pr.breakdown) break;
+        { note_launch(); add_f32_kernel<<<G, kThreads, 0, s>>>(n, dx32, xd); }
+        if ((st = damage_op(&fctx, xd, w.Ap, nullptr, s))) return st;
+        { note_launch(); constrained_rhs_kernel<<<G, kThreads, 0, s>>>(n, fixed, bf, w.Ap, w.r, rw); }
+        if ((st = last_launch_status())) return st;
+      }
+      if (!conv && !pr.nonfinite && !pr.breakdown) {
+        double rr;
+        if ((st = red_ws_fetch(rw, &rr, 1, s))) return st;
+        conv = std::sqrt(rr) <= thr;
+      }
+      pr.iterations = inner;
+      pr.converged = conv;
+    }
     // candidate = where(fixed, known, x)
     { note_launch(); where_kernel<<<G, kThreads, 0, s>>>(n, fixed, xd, known, xd); }
     total += pr.iterations;

@@ -81,6 +81,34 @@ def test_h8_box_kkt_golden():
     assert float((res.solution - lower).min()) >= 0.0 and float(res.solution.max()) <= 1.0
 
 
+def test_h8_box_kkt_mixed_precision_golden():
+    """PHASTB_DAMAGE_MIXED=1 (FP32 CG under FP64 refinement) meets the same FP64 threshold."""
+    import os
+    import subprocess
+    import sys
+    import tempfile
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import sys; sys.path.insert(0, 'tests'); sys.path.insert(0, '.'); import numpy as np;"
+        "from conftest import golden; from test_gpu_h8 import make_op, cuda; from phast_b200 import solid3d as s3;"
+        "g = golden('h8_ops'); op = make_op(g); lower = cuda(g['lower_kkt']);"
+        "res = s3.solve_h8_scalar_box_kkt(op.damage_system(cuda(g['H_kkt'])), lower_bound=lower, upper_bound=1.0,"
+        " initial=lower, linear_tolerance=1e-10, kkt_tolerance=1e-8, max_linear_iterations=4000,"
+        " max_active_set_iterations=64);"
+        "np.save(sys.argv[1], np.concatenate([res.solution.cpu().numpy(),"
+        " [float(res.satisfies_kkt), float(res.active_set_iterations)]]))")
+    g = golden("h8_ops")
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "kkt_mixed.npy")
+        subprocess.run([sys.executable, "-c", code, path], check=True, cwd=root,
+                       env=dict(os.environ, PHASTB_DAMAGE_MIXED="1"), timeout=600)
+        out = np.load(path)
+    d, ok, sets = out[:-2], out[-2], out[-1]
+    assert ok == 1.0 and int(sets) == int(g["kkt_sets"][0])
+    assert rel(d, g["d_kkt"]) < 1e-9
+    assert float((d - g["lower_kkt"]).min()) >= 0.0 and float(d.max()) <= 1.0
+
+
 def test_h8_staggered_increments_golden():
     from phast_b200 import solid3d as s3
     g = golden("h8_staggered")
