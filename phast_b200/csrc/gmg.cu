@@ -424,23 +424,6 @@ __global__ void gmg_cheb_first_b(int n, T* __restrict__ b, const T* __restrict__
   }
 }
 
-template <typename T>
-__global__ void gmg_cheb_step(int n, T* __restrict__ res, const T* __restrict__ Ad, const T* __restrict__ invd, T c1,
-                              T c2, T* __restrict__ d, T* __restrict__ x) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const T r = res[i] - Ad[i];
-    res[i] = r;
-    const T di = c1 * d[i] + c2 * invd[i] * r;
-    d[i] = di;
-    x[i] += di;
-  }
-}
-
-template <typename T>
-__global__ void gmg_sub_inplace(int n, T* __restrict__ res, const T* __restrict__ Ad) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) res[i] -= Ad[i];
-}
-
 // res = b - A x
 template <typename T>
 __global__ void gmg_invert(int n, const T* __restrict__ diag, const uint8_t* __restrict__ mask, T* __restrict__ inv) {
