@@ -38,10 +38,10 @@ UNIT = "staggered steps/s"
 N_CELL = 64
 N_LARGE = 192  # roofline cell: the action's working set (about 200 MB in FP32) exceeds the 126 MB L2
 INCREMENTS = 50
-# Mean per-increment iteration counts of this workload over increments 4..5
-# (the default timed window), measured with this repository's CUDA solver on a
-# B200; the CPU reference arm scales its timed per-iteration samples by them.
-REF_COUNTS = {"mech": 232.5, "pf": 83.0, "stag": 3.0}
+# Wall-clock budgets of the reference's whole increments: the reference arm's
+# timed region, and the CPU baseline sample inside our arm's run.
+REF_BUDGET_S = 150.0
+CPU_BASELINE_BUDGET_S = 30.0
 
 
 def peaks():
@@ -58,7 +58,8 @@ def workload_config():
         "workload": "3D periodic voxel H8 pore cell 64^3 (r=0.2 L, E x 1e-6), AT2 spectral, eps_zz 0->0.02 in 50 "
                     "increments; step = one staggered load increment",
         "cells": 1, "voxels": N_CELL ** 3, "mechanics": "constrained PCG, FP64 residual rtol 1e-8",
-        "damage": "box-KKT active set + Dirichlet PCG (FP64)", "form": "",
+        "damage": "box-KKT active set + Dirichlet PCG (FP64)",
+        "window": "load increments 1..K of the ramp from the initial state",
         "l2": "flushed (256 MB write) before every timed step", "parallelism": "replicas",
     }
 
@@ -68,11 +69,10 @@ def build_cell(device, n=None):
     n = N_CELL if n is None else n
     h = 1.0 / n
     shape = (n, n, n)
-    phase = s3.sphere_pore_phase(shape, 0.2)
-    phases = [s3.PhaseMaterial("mi_matrix", 3000.0, 0.35, 0.5), s3.PhaseMaterial("pore", 3000.0 * 1e-6, 0.35, 0.5)]
+    model = s3.sphere_pore_model(shape, 0.2, E=3000.0, nu=0.35, Gc=0.5, ell_voxels=2.0, pore_stiffness=1e-6)
     load = s3.LoadCase.ramp("zz", 2, 0.02, INCREMENTS)
-    op = s3.PeriodicVoxelPhaseFieldOperator(s3.VoxelGrid(shape, (h, h, h)), phase, phases, 2 * h, 1e-6, load,
-                                            device=device)
+    cfg = s3.SolverConfig(device=str(device), kappa=1e-6, energy_split_isotropic="spectral", damage_law="at2")
+    op = s3.PeriodicVoxelPhaseFieldOperator(model, load, cfg)
     return op, s3.StaggeredSolver(op)
 
 
@@ -93,10 +93,16 @@ class Clocks:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # the sampler needs a moment to start: wait (at most 2 s) for its first row, so that
+        # the samples cover the timed region that follows
+        t0 = time.time()
+        while time.time() - t0 < 2.0 and os.path.getsize(self.path) == 0:
+            time.sleep(0.01)
 
     def stop(self):
         if self.proc is None:
@@ -128,57 +134,107 @@ def flush_l2(buf):
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the numpy oracle timed on bounded samples of the same cell
+# The reference: PhAST's own CPU implementation of the path, installed under
+# baseline/_ref (the unmodified package), timed on whole load increments
 # ---------------------------------------------------------------------------
 
-def cpu_per_iteration_costs(threads_note=True):
-    """Seconds per mechanics PCG iteration, per damage PCG iteration and per staggered pass
-    of the oracle at full size (64^3); ~10-20 s of CPU work."""
-    from oracle import h8
-    shape, h = (N_CELL,) * 3, 1.0 / N_CELL
-    k, j, i = np.meshgrid(*(np.arange(N_CELL),) * 3, indexing="ij")
-    c = np.stack([(i + 0.5) / N_CELL - 0.5, (j + 0.5) / N_CELL - 0.5, (k + 0.5) / N_CELL - 0.5], -1)
-    slot = (np.linalg.norm(c, axis=-1) < 0.2).astype(np.int64).reshape(-1)
-    C0, l0, m0 = h8.isotropic_C(3000.0, 0.35)
-    C1, l1, m1 = h8.isotropic_C(3e-3, 0.35)
-    op = h8.VoxelOperator(shape, (h, h, h), slot, np.stack([C0, C1]), np.array([l0, l1]), np.array([m0, m1]),
-                          np.array([0.5, 0.5]), np.array([2, 0]), 2 * h, 1e-6, 0, 2, (0, 1, 3, 4, 5))
-    rng = np.random.default_rng(0)
-    d = rng.uniform(0, 0.5, op.n_red)
-    g = op.degradation(d)
-    x = rng.normal(size=op.n_mech) * 1e-4
-    H = rng.uniform(0, 1, (op.n_elements, 8))
-    dg = op.mech_diagonal(g)
-    free = ~op.fixed_mask()
-    n_it = 4
-    t0 = time.perf_counter()
-    _, its, _, _, _ = h8.pcg(lambda v: np.where(free, op.mech_action(v, g), 0.0), np.where(free, x, 0.0),
-                             np.where(free, dg, 1.0), rtol=1e-30, atol=1e-300, maxiter=n_it, check_every=n_it)
-    t_mech = (time.perf_counter() - t0) / n_it
-    s = op.damage_scale
-    n_it = 10
-    t0 = time.perf_counter()
-    h8.dirichlet_pcg(lambda v: s * op.damage_action(v, H), s * op.damage_rhs(H), s * op.damage_diagonal(H),
-                     np.zeros(op.n_red, bool), np.zeros(op.n_red), None, 1e-300, n_it)
-    t_pf = (time.perf_counter() - t0) / n_it
-    t0 = time.perf_counter()
-    op.degradation(d)
-    op.mech_diagonal(g)
-    op.driving_force(x)
-    op.damage_rhs(H)
-    op.damage_diagonal(H)
-    t_pass = time.perf_counter() - t0
-    return t_mech, t_pf, t_pass
+REF_DIR = os.path.join(ROOT, "baseline", "_ref")
+# I/O-only dependencies of the reference package that the solver path never calls
+# (mesh files, HDF5/zarr result files, plots); they are not installed here.
+REF_STUBS = ("meshio", "gmsh", "h5py", "zarr", "numcodecs", "matplotlib", "mpl_toolkits")
 
 
-def cpu_step_estimate(counts):
-    t_mech, t_pf, t_pass = cpu_per_iteration_costs()
-    sec = counts["mech"] * t_mech + counts["pf"] * t_pf + (counts["stag"] + 1) * t_pass
-    sample = (f"numpy oracle on the full 64^3 cell: 4 mechanics PCG iterations ({t_mech:.3f} s each), 10 damage "
-              f"PCG iterations ({t_pf:.4f} s each), one staggered pass of diagonal/driving/rhs ({t_pass:.2f} s); "
-              f"scaled to one step with {counts['mech']:.0f} mechanics + {counts['pf']:.0f} damage iterations "
-              f"and {counts['stag']:.1f} staggered passes per increment")
-    return sec, sample
+def import_reference():
+    """Import ``phast`` from baseline/_ref with permissive stubs for its I/O-only modules."""
+    import importlib.abc
+    import importlib.machinery
+    from unittest import mock
+
+    if not os.path.isdir(os.path.join(REF_DIR, "phast")):
+        raise ImportError(f"the reference is not installed under {os.path.relpath(REF_DIR, ROOT)}")
+
+    class _Stubs(importlib.abc.MetaPathFinder, importlib.abc.Loader):
+        def find_spec(self, name, path=None, target=None):
+            if name.split(".")[0] in REF_STUBS:
+                return importlib.machinery.ModuleSpec(name, self, is_package=True)
+            return None
+
+        def create_module(self, spec):
+            m = mock.MagicMock(name=spec.name)
+            m.__path__ = []
+            m.__spec__ = spec
+            return m
+
+        def exec_module(self, module):
+            pass
+
+    sys.meta_path.insert(0, _Stubs())
+    sys.path.insert(0, REF_DIR)
+    import phast  # noqa: F401
+    return phast
+
+
+def reference_solver():
+    """The bench cell built with the reference's own classes (phast.solid3d)."""
+    from phast.solid3d.model import (PHASE_ID, LoadCase, MaterialTable, PhaseMaterial, SolverConfig, VoxelGrid,
+                                     VoxelModel)
+    from phast.solid3d.operator import PeriodicVoxelPhaseFieldOperator
+    from phast.solid3d.staggered import StaggeredSolver
+    n = N_CELL
+    h = 1.0 / n
+    k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    c = np.stack([(i + 0.5) / n - 0.5, (j + 0.5) / n - 0.5, (k + 0.5) / n - 0.5], -1)
+    phase = np.full((n, n, n), PHASE_ID["mi_matrix"], dtype=np.uint8)
+    phase[np.linalg.norm(c, axis=-1) < 0.2] = PHASE_ID["pore"]
+    phases = {"mi_matrix": PhaseMaterial(name="mi_matrix", kind="isotropic", Gc=0.5, driver="spectral", E=3000.0,
+                                         nu=0.35),
+              "pore": PhaseMaterial(name="pore", kind="isotropic", Gc=0.5, driver="spectral", E=3000.0 * 1e-6,
+                                    nu=0.35)}
+    tangent = np.zeros((n, n, n, 3))
+    tangent[..., 2] = 1.0
+    model = VoxelModel(grid=VoxelGrid(shape=(n, n, n), h=(h, h, h)), phase_id=phase, tangent=tangent,
+                       materials=MaterialTable(phases=phases, length_scale=2 * h, scale="micro"))
+    targets = tuple(0.02 * k / INCREMENTS for k in range(1, INCREMENTS + 1))
+    load = LoadCase(name="zz", controlled=2, targets=targets, free=(), fixed_zero=(0, 1, 3, 4, 5))
+    cfg = SolverConfig(device="cpu", kappa=1e-6, energy_split_isotropic="spectral", damage_law="at2")
+    op = PeriodicVoxelPhaseFieldOperator(model, load, cfg)
+    return op, StaggeredSolver(op)
+
+
+def time_reference(max_increments, budget_s, warmup=0):
+    """Whole staggered increments of the reference on the host cores, from the initial state.
+
+    Runs ``warmup`` untimed elastic actions, then increments 1, 2, ... until
+    ``max_increments`` are done or the next one would end past ``budget_s``
+    (at least one).  Returns (seconds per increment, threads, records).
+    """
+    import torch as th
+    import_reference()
+    threads = os.cpu_count() or 1
+    th.set_num_threads(threads)
+    op, solver = reference_solver()
+    state = solver.initial_state()
+    for _ in range(warmup):
+        op.mech_action(state.x)
+    secs, recs = [], []
+    for k in range(max_increments):
+        t0 = time.perf_counter()
+        state, rec = solver.advance(state, op.load.targets[k])
+        secs.append(time.perf_counter() - t0)
+        recs.append(rec)
+        if sum(secs) + secs[-1] > budget_s:
+            break
+    return secs, th.get_num_threads(), recs
+
+
+def reference_sample_note(secs, recs, threads):
+    its = ", ".join(f"{r.stagger_iters}/{r.pcg_iters_mech}/{r.pcg_iters_pf}" for r in recs)
+    return (f"PhAST {PHAST_VERSION} phast.solid3d.StaggeredSolver.advance (FP64, torch CPU, {threads} threads) on the "
+            f"same 64^3 cell: increments 1-{len(secs)} of the load path from the initial state, whole increments "
+            f"timed ({', '.join(f'{s:.1f}' for s in secs)} s; staggered/mechanics PCG/damage PCG iterations {its})")
+
+
+PHAST_VERSION = "0.18.0"
 
 
 # ---------------------------------------------------------------------------
@@ -200,12 +256,11 @@ FORM_LABEL = {
 }
 
 
-def run_steps(op, form, snap, meta, steps, flush, device, clocks=None):
-    """Timed staggered increments from a host snapshot; device time per step with CUDA events."""
-    from phast_b200.solid3d import SolverState, StaggeredSolver
+def run_steps(op, form, steps, flush, clocks=None):
+    """Timed staggered increments 1..steps from the initial state; device time per step with CUDA events."""
+    from phast_b200.solid3d import StaggeredSolver
     solver = StaggeredSolver(op, form=form)
-    state = SolverState(meta[0], snap["x"].to(device), snap["d"].to(device), snap["H"].to(device), meta[1].copy(),
-                        meta[2].copy(), meta[3])
+    state = solver.initial_state()
     torch.cuda.synchronize()
     if clocks is not None:
         clocks.start()
@@ -229,15 +284,15 @@ def run_ours(args, rank, world, device):
     fm = forms()
     chosen = fm[args.form]
     op, solver = build_cell(device)
-    state = solver.initial_state()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)  # 256 MB > 126 MB L2
-    for _ in range(args.warmup):  # warm-up increments with the plain FP64 form (same start for both forms)
+    # warm-up: W increments of the plain FP64 form and one of the chosen form, each from the
+    # initial state (workspaces, graphs and kernels); the timed runs start from the initial
+    # state again, so every arm times load increments 1..K of the same path
+    state = solver.initial_state()
+    for _ in range(args.warmup):
         state, _ = solver.advance(state, op.load.targets[state.increment])
     torch.cuda.synchronize()
-    snap = {k: getattr(state, k).detach().cpu().pin_memory() for k in ("x", "d", "H")}
-    meta = (state.step, state.macro_strain.copy(), state.macro_stress.copy(), state.increment)
-    # one untimed increment of the chosen form warms its workspaces and kernels
-    run_steps(op, chosen, snap, meta, 1, flush, device)
+    run_steps(op, chosen, 1, flush)
 
     # ---- chosen form, device-resident timed region -----------------------------------
     lib = _lib.load()
@@ -247,7 +302,7 @@ def run_ours(args, rank, world, device):
     clocks = Clocks(torch.cuda.current_device())
     # brackets the timed steps for a profiler started with --profile-from-start off (no-op otherwise)
     torch.cuda.profiler.start()
-    total_ms, st_c, counts, clk = run_steps(op, chosen, snap, meta, args.steps, flush, device, clocks)
+    total_ms, st_c, counts, clk = run_steps(op, chosen, args.steps, flush, clocks)
     torch.cuda.profiler.stop()
     launches = lib.phastb_launch_count()
     t = torch.tensor([total_ms], dtype=torch.float64, device=device)
@@ -258,7 +313,7 @@ def run_ours(args, rank, world, device):
     value = args.steps * world / (max_ms / 1e3)
 
     # ---- plain FP64 form on the same increments (the comparison of the metric) --------
-    plain_ms, st_p, counts_p, _ = run_steps(op, fm["plain"], snap, meta, args.steps, flush, device)
+    plain_ms, st_p, counts_p, _ = run_steps(op, fm["plain"], args.steps, flush)
     tp = torch.tensor([plain_ms], dtype=torch.float64, device=device)
     if world > 1:
         torch.distributed.all_reduce(tp, op=torch.distributed.ReduceOp.MAX)
@@ -269,26 +324,29 @@ def run_ours(args, rank, world, device):
         return float(torch.linalg.vector_norm(a - b)) / (nb if nb > 0 else 1.0)
 
     err = {"x": relerr(st_c.x, st_p.x), "d": relerr(st_c.d, st_p.d),
-           "macro_stress": float(np.linalg.norm(st_c.macro_stress - st_p.macro_stress) /
-                                 max(np.linalg.norm(st_p.macro_stress), 1e-300)),
+           "macro_stress": float(np.linalg.norm((st_c.macro_stress - st_p.macro_stress).numpy()) /
+                                 max(float(np.linalg.norm(st_p.macro_stress.numpy())), 1e-300)),
            "crack_support_equal": bool(torch.equal(st_c.d > 0.9, st_p.d > 0.9))}
 
     # ---- end to end through the public API with host buffers ---------------------------
+    # every step copies the state in from pinned host memory, advances one increment and
+    # copies the new state out (x, d, H; the lower bound d_prev_step is the incoming d)
     solver_c = StaggeredSolver(op, form=chosen)
-    pinned_out = {k: torch.empty_like(v).pin_memory() for k, v in snap.items()}
-    dev_in = {k: torch.empty(v.shape, dtype=v.dtype, device=device) for k, v in snap.items()}
-    h2d = sum(v.numel() * v.element_size() for v in snap.values())
-    st_meta = meta
+    init = solver_c.initial_state()
+    host_state = {k: getattr(init, k).detach().cpu().pin_memory() for k in ("x", "d", "H")}
+    pinned_out = {k: torch.empty_like(v).pin_memory() for k, v in host_state.items()}
+    dev_in = {k: torch.empty(v.shape, dtype=v.dtype, device=device) for k, v in host_state.items()}
+    h2d = sum(v.numel() * v.element_size() for v in host_state.values())
+    meta = (init.step, init.macro_strain, init.macro_stress, init.external_work, init.increment)
     e2e_ms = 0.0
-    host_state = dict(snap)
     for _ in range(args.steps):
         flush_l2(flush)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for k in dev_in:
             dev_in[k].copy_(host_state[k], non_blocking=True)
-        s_in = SolverState(st_meta[0], dev_in["x"].clone(), dev_in["d"].clone(), dev_in["H"].clone(),
-                           st_meta[1].copy(), st_meta[2].copy(), st_meta[3])
+        s_in = SolverState(meta[0], dev_in["x"].clone(), dev_in["d"].clone(), dev_in["H"].clone(), meta[1].clone(),
+                           meta[2].clone(), meta[3], dev_in["d"].clone(), meta[4])
         s_out, _ = solver_c.advance(s_in, op.load.targets[s_in.increment])
         for k in pinned_out:
             pinned_out[k].copy_(getattr(s_out, k), non_blocking=True)
@@ -296,7 +354,7 @@ def run_ours(args, rank, world, device):
         torch.cuda.synchronize()
         e2e_ms += e0.elapsed_time(e1)
         host_state = {k: v.clone().pin_memory() for k, v in pinned_out.items()}
-        st_meta = (s_out.step, s_out.macro_strain, s_out.macro_stress, s_out.increment)
+        meta = (s_out.step, s_out.macro_strain, s_out.macro_stress, s_out.external_work, s_out.increment)
     te = torch.tensor([e2e_ms], dtype=torch.float64, device=device)
     if world > 1:
         torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
@@ -324,11 +382,11 @@ def run_ours(args, rank, world, device):
     mech_p = float(np.mean([c[0] for c in counts_p]))
     dof_updates = (mech * op.n_mech + pf * op.n_red) * args.steps * world / (max_ms / 1e3)
     cfg = workload_config()
-    cfg["form"] = FORM_LABEL[args.form]
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 (f64 dots, f64 refinement)" if mixed else "f64", "data": "synthetic", "config": cfg,
+        "form": FORM_LABEL[args.form],
         "plain_fp64": {"value": plain_value, "unit": UNIT, "ms_per_step": float(tp.item()) / args.steps,
                        "mech_iters_per_step": mech_p},
         "speedup_vs_plain_fp64": value / plain_value,
@@ -348,9 +406,13 @@ def run_ours(args, rank, world, device):
         "dof_updates_per_s": dof_updates,
     }
     if world == 1 and rank == 0 and not args.no_cpu:
-        sec, sample = cpu_step_estimate({"mech": mech_p, "pf": pf, "stag": stag})
-        out["cpu_baseline"] = {"value": 1.0 / sec, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                               "sample": sample}
+        try:
+            secs, threads, recs = time_reference(args.steps, CPU_BASELINE_BUDGET_S)
+            out["cpu_baseline"] = {"value": len(secs) / sum(secs), "unit": UNIT, "cores": threads,
+                                   "kind": "reference", "sample": reference_sample_note(secs, recs, threads)}
+        except ImportError as exc:
+            out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                   "sample": f"unavailable: {exc}"}
     return out
 
 
@@ -387,22 +449,24 @@ def profile_traffic(fp32):
 
 
 def run_reference(args, rank, world):
-    torch.set_num_threads(os.cpu_count() or 1)
-    times = []
-    sample = ""
-    for _ in range(args.warmup):
-        pass
-    for _ in range(max(1, min(args.steps, 2))):
-        sec, sample = cpu_step_estimate(REF_COUNTS)
-        times.append(sec)
-    sec = float(np.mean(times))
-    value = 1.0 / sec
+    """PhAST's own solver on the host cores: whole increments 1..m (m <= K within the budget)."""
+    try:
+        secs, threads, recs = time_reference(args.steps, REF_BUDGET_S, warmup=args.warmup)
+    except ImportError as exc:
+        return {"impl": "reference", "unavailable": str(exc)}
+    total = sum(secs)
+    value = len(secs) / total
+    cfg = workload_config()
+    sample = reference_sample_note(secs, recs, threads)
     return {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": workload_config(), "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": sample},
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": len(secs),
+        "warmup": args.warmup, "ms_per_step": total * 1e3 / len(secs), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+        "impl": "reference", "form": "PhAST's own solver: FP64 Jacobi PCG mechanics, FP64 box-KKT damage (torch CPU)",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "timed_increments": {"requested": args.steps, "timed": len(secs), "budget_s": REF_BUDGET_S,
+                             "seconds": secs},
     }
 
 
@@ -482,8 +546,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
-    if args.warmup + args.steps > INCREMENTS:
-        raise SystemExit(f"warmup + steps must not exceed the {INCREMENTS} increments of the load path")
+    if args.steps > INCREMENTS or args.warmup > INCREMENTS:
+        raise SystemExit(f"steps and warmup must not exceed the {INCREMENTS} increments of the load path")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -280,10 +280,16 @@ int phastb_h8_mech_apply(const phastb_voxel_grid* g, const phastb_voxel_material
  * no device-memory API, or an application whose GPU memory belongs entirely to another
  * allocator.  Its element scratch is a file-scope device array for at most
  * PHASTB_NOALLOC_MAX_VOXELS voxels (about 6.4 MB), held on every GPU that loads the
- * library until exit.  Larger grids return PHASTB_ERR_CAPACITY.  The first call on a
- * device looks up the array's device address (make that first call before any stream
- * capture); the device current at the call must own `stream`.  All calls share the one
- * array, so calls that overlap on the GPU (other streams, other host threads) race. */
+ * library until exit.  Larger grids return PHASTB_ERR_CAPACITY.  The array holds the
+ * same workspace layout as the caller workspace of phastb_h8_mech_apply: a region of 24
+ * words per voxel followed by the reduction block of the macro-stress rows; the tiled
+ * action writes only the reduction block, whose offset grows with the grid, and that
+ * layout is what bounds the voxel count.  The first call on a device looks up the
+ * array's device address and keeps it for the process (make that first call before any
+ * stream capture; a device reset, cudaDeviceReset, in the same process is not supported
+ * afterwards, because the kept address may no longer be the array's).  The device current
+ * at the call must own `stream`.  All calls share the one array, so calls that overlap on
+ * the GPU (other streams, other host threads) race. */
 #define PHASTB_NOALLOC_MAX_VOXELS 32768
 int phastb_h8_mech_apply_noalloc(const phastb_voxel_grid* g, const phastb_voxel_material* m,
                                  const uint8_t* slot, int dtype, const void* x, const void* gq,
@@ -391,6 +397,38 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
 int phastb_h8_stagger_change(int n_u, const double* x_new, const double* x_old, int n_d,
                              const double* d_new, const double* d_old, double* out_host,
                              void* workspace, size_t workspace_bytes, void* stream);
+
+/* Scalars of an accepted increment, FP64, one host read (out_host[PHASTB_RECORD_WORDS]):
+ * [0:6] E (the macro unknowns of x), [6:12] r_E = sum w g sigma with g = g(d) (macro stress
+ * times volume), [12] elastic energy 0.5 x.A(g) x, [13:13+PHASTB_MAX_SLOTS] fracture energy
+ * by material slot, [21] its local part Gc/(2 ell) d.M d, [22] its gradient part
+ * Gc ell/2 d.L d, [23] sum of the element-mean damage (mean of the 8 corners), [24] number
+ * of elements whose mean damage >= threshold, [25] max H (0 when H is NULL), [26] max d.
+ * x NULL skips the mechanics part ([0:13] are then 0).
+ * The record of StaggeredSolver._attempt, solid3d/staggered.py:1436-1499, with
+ * macro_stress / elastic_energy (operator.py:1303-1340) and fracture_energy
+ * (operator.py:1511-1545). */
+#define PHASTB_RECORD_WORDS 27
+size_t phastb_h8_record_workspace_bytes(const phastb_voxel_grid* g);
+int phastb_h8_increment_record(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                               const uint8_t* slot, const double* x, const double* d, const double* H,
+                               double threshold, double* out_host, void* workspace,
+                               size_t workspace_bytes, void* stream);
+
+/* ||rhs - A d|| of the (scaled) damage system of history H, FP64, host result: the
+ * residual that sets the linear tolerance of the damage solve.
+ * StaggeredSolver._damage, solid3d/staggered.py:766-770 */
+size_t phastb_h8_damage_residual_workspace_bytes(const phastb_voxel_grid* g);
+int phastb_h8_damage_residual_norm(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                                   const uint8_t* slot, const double* H, double scale, const double* d,
+                                   double* norm_host, void* workspace, size_t workspace_bytes,
+                                   void* stream);
+
+/* out = factor * x, then out[index] = value (index < 0: none); n FP64 entries.  The
+ * staggered predictor x * (target / previous) with E[c] = target,
+ * StaggeredSolver._predictor, solid3d/staggered.py:1207-1213 */
+int phastb_scale_set(int n, const double* x, double factor, int index, double value, double* out,
+                     void* stream);
 
 /* Library version string (host pointer). */
 const char* phastb_version(void);

@@ -119,7 +119,13 @@ SIGNATURES = {
     "phastb_h8_damage_box_kkt": (C.c_int, [VG, VM, vp, vp, C.c_double, vp, C.c_double, vp, C.c_double, C.c_double,
                                            C.c_int, C.c_int, vp, ip, vp, sz, vp]),
     "phastb_h8_stagger_change": (C.c_int, [C.c_int, vp, vp, C.c_int, vp, vp, dp, vp, sz, vp]),
+    "phastb_h8_record_workspace_bytes": (sz, [VG]),
+    "phastb_h8_increment_record": (C.c_int, [VG, VM, vp, vp, vp, vp, C.c_double, dp, vp, sz, vp]),
+    "phastb_h8_damage_residual_workspace_bytes": (sz, [VG]),
+    "phastb_h8_damage_residual_norm": (C.c_int, [VG, VM, vp, vp, C.c_double, vp, dp, vp, sz, vp]),
+    "phastb_scale_set": (C.c_int, [C.c_int, vp, C.c_double, C.c_int, C.c_double, vp, vp]),
 }
+RECORD_WORDS = 27
 
 _lock = threading.Lock()
 _lib = None

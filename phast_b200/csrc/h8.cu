@@ -690,6 +690,205 @@ int phastb_h8_damage_rhs_diag(const phastb_voxel_grid* g, const phastb_voxel_mat
 
 }  // extern "C"
 
+// ------------------------------------------------------------ accepted-increment record
+
+namespace phastb {
+
+// Sums of the record kernel: fracture energy by material slot, its local and
+// gradient parts, the sum of element-mean damage and the damaged-element count.
+constexpr int kRecSums = PHASTB_MAX_SLOTS + 4;
+constexpr int kRecMax = 2;  // max H, max d
+
+// Per element (solid3d/operator.py:1511-1545, staggered.py:1440-1455):
+//   local    = Gc / (2 ell) d_e^T M d_e,  M = sum_q w N_q N_q^T
+//   gradient = Gc ell / 2 d_e^T L d_e,    L = sum_q w grad N_q . grad N_q
+// (by sum factorisation: d at the Gauss points and its face-difference gradients),
+// the element-mean damage of the 8 corners, and the maxima of H and d.
+__global__ void __launch_bounds__(kThreads) h8_record_kernel(VoxGeom g, VoxMat<double> m,
+                                                             const uint8_t* __restrict__ slot,
+                                                             const double* __restrict__ d,
+                                                             const double* __restrict__ H, double threshold,
+                                                             RedWs ws) {
+  const double ihx = 1.0 / g.hx, ihy = 1.0 / g.hy, ihz = 1.0 / g.hz, w = g.w, ell = m.ell;
+  double acc[kRecSums];
+#pragma unroll
+  for (int k = 0; k < kRecSums; ++k) acc[k] = 0.0;
+  double mxH = -INFINITY, mxd = -INFINITY;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.n_elem; e += gridDim.x * blockDim.x) {
+    int ie, je, ke;
+    elem_ijk(g, e, ie, je, ke);
+    int nd[8];
+    vox_corners(g, ie, je, ke, nd);
+    double dd[8], dq[8];
+#pragma unroll
+    for (int L = 0; L < 8; ++L) dd[L] = __ldg(d + nd[L]);
+    interp_sf(dd, dq);
+    double mloc = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) mloc += dq[q] * dq[q];
+    double Dx[2][2], Dy[2][2], Dz[2][2];
+    grad_sf(dd, ihx, ihy, ihz, Dx, Dy, Dz);
+    double gl = 0.0;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) gl += Dx[i][j] * Dx[i][j] + Dy[i][j] * Dy[i][j] + Dz[i][j] * Dz[i][j];
+    // each face-difference gradient value holds at the two Gauss points along its own axis
+    const int s = slot[e];
+    const double Gc = m.Gc[s];
+    const double local = Gc / (2.0 * ell) * (w * mloc);
+    const double grad = 0.5 * Gc * ell * (2.0 * w * gl);
+#pragma unroll
+    for (int k = 0; k < PHASTB_MAX_SLOTS; ++k) acc[k] += (k == s) ? local + grad : 0.0;
+    acc[PHASTB_MAX_SLOTS] += local;
+    acc[PHASTB_MAX_SLOTS + 1] += grad;
+    double dbar = 0.0;
+#pragma unroll
+    for (int L = 0; L < 8; ++L) {
+      dbar += dd[L];
+      mxd = fmax(mxd, dd[L]);
+    }
+    dbar *= 0.125;
+    acc[PHASTB_MAX_SLOTS + 2] += dbar;
+    acc[PHASTB_MAX_SLOTS + 3] += dbar >= threshold ? 1.0 : 0.0;
+    if (H) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) mxH = fmax(mxH, __ldg(H + 8 * (size_t)e + q));
+    }
+  }
+  __shared__ double sh[32 * kRecSums];
+  block_sum_multi<kRecSums>(acc, sh);
+  const double bH = block_max(mxH, sh);
+  const double bd = block_max(mxd, sh);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < kRecSums; ++k) ws.part[k * kMaxPartials + blockIdx.x] = acc[k];
+    ws.part[kRecSums * kMaxPartials + blockIdx.x] = bH;
+    ws.part[(kRecSums + 1) * kMaxPartials + blockIdx.x] = bd;
+  }
+  if (arrive_last(ws.counter)) {
+    double f[kRecSums];
+    fold_sum_multi<kRecSums>(ws.part, kMaxPartials, gridDim.x, f, sh);
+    const double fH = fold_max(ws.part + kRecSums * kMaxPartials, gridDim.x, sh);
+    const double fd = fold_max(ws.part + (kRecSums + 1) * kMaxPartials, gridDim.x, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < kRecSums; ++k) ws.out[k] = f[k];
+      ws.out[kRecSums] = H ? fH : 0.0;
+      ws.out[kRecSums + 1] = fd;
+      *ws.counter = 0u;
+    }
+  }
+}
+static_assert(kRecSums + kRecMax <= kRedMaxK, "record reduction exceeds the reduction workspace");
+
+// ||a - b||^2 over n entries (deterministic partials and fold).
+__global__ void __launch_bounds__(kThreads) diff_norm2_kernel(int n, const double* __restrict__ a,
+                                                              const double* __restrict__ b, RedWs ws) {
+  double v[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double r = a[i] - b[i];
+    v[0] += r * r;
+  }
+  reduce_multi<1>(v, ws);
+}
+
+// out = factor * x with out[idx] = value (idx < 0: no override).
+__global__ void scale_set_kernel(int n, const double* __restrict__ x, double factor, int idx, double value,
+                                 double* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = i == idx ? value : factor * x[i];
+}
+
+}  // namespace phastb
+
+extern "C" {
+
+size_t phastb_h8_record_workspace_bytes(const phastb_voxel_grid* g) {
+  if (!valid_vox(g)) return 0;
+  return 2 * red_ws_bytes();
+}
+
+int phastb_h8_increment_record(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                               const double* x, const double* d, const double* H, double threshold,
+                               double* out_host, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !d || !out_host) return PHASTB_ERR_ARG;
+  if (!workspace || workspace_bytes < phastb_h8_record_workspace_bytes(g)) return PHASTB_ERR_WORKSPACE;
+  const VoxGeom v = make_vox_geom(*g);
+  cudaStream_t s = (cudaStream_t)stream;
+  RedWs ws_s = red_ws(workspace);
+  RedWs ws_d = red_ws(static_cast<char*>(workspace) + red_ws_bytes());
+  int st;
+  if ((st = red_ws_reset(ws_s, s)) || (st = red_ws_reset(ws_d, s))) return st;
+  if (x) {
+    { note_launch(); h8_mech_elem_kernel<double, true><<<grid_for(v.n_elem), kThreads, 0, s>>>(
+        v, make_vox_mat<double>(*m), slot, x, nullptr, d, nullptr, nullptr, nullptr, ws_s, nullptr); }
+    if ((st = last_launch_status())) return st;
+  }
+  { note_launch(); h8_record_kernel<<<grid_for(v.n_elem), kThreads, 0, s>>>(v, make_vox_mat<double>(*m), slot, d, H,
+                                                                             threshold, ws_d); }
+  if ((st = last_launch_status())) return st;
+  if (x) {
+    if ((st = cuda_status(cudaMemcpyAsync(out_host, x + 3 * (size_t)v.n_red, 6 * sizeof(double),
+                                          cudaMemcpyDeviceToHost, s))))
+      return st;
+    if ((st = cuda_status(cudaMemcpyAsync(out_host + 6, ws_s.out, 7 * sizeof(double), cudaMemcpyDeviceToHost, s))))
+      return st;
+  } else {
+    for (int k = 0; k < 13; ++k) out_host[k] = 0.0;
+  }
+  if ((st = cuda_status(cudaMemcpyAsync(out_host + 13, ws_d.out, (kRecSums + kRecMax) * sizeof(double),
+                                        cudaMemcpyDeviceToHost, s))))
+    return st;
+  return cuda_status(cudaStreamSynchronize(s));
+}
+
+size_t phastb_h8_damage_residual_workspace_bytes(const phastb_voxel_grid* g) {
+  if (!valid_vox(g)) return 0;
+  const VoxGeom v = make_vox_geom(*g);
+  return h8_scratch_bytes(v, PHASTB_F64) + 2 * align_up(sizeof(double) * (size_t)v.n_red) + red_ws_bytes();
+}
+
+int phastb_h8_damage_residual_norm(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                                   const double* H, double scale, const double* d, double* norm_host,
+                                   void* workspace, size_t workspace_bytes, void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !d || !norm_host) return PHASTB_ERR_ARG;
+  if (!workspace || workspace_bytes < phastb_h8_damage_residual_workspace_bytes(g)) return PHASTB_ERR_WORKSPACE;
+  const VoxGeom v = make_vox_geom(*g);
+  const VoxMat<double> mm = make_vox_mat<double>(*m);
+  cudaStream_t s = (cudaStream_t)stream;
+  char* p = static_cast<char*>(workspace);
+  void* scratch = p;
+  p += h8_scratch_bytes(v, PHASTB_F64);
+  double* rhs = reinterpret_cast<double*>(p);
+  double* Ad = reinterpret_cast<double*>(p + align_up(sizeof(double) * (size_t)v.n_red));
+  RedWs ws = red_ws(p + 2 * align_up(sizeof(double) * (size_t)v.n_red));
+  int st;
+  if ((st = red_ws_reset(ws, s))) return st;
+  if (H) {
+    if ((st = h8_damage_launch(v, mm, slot, 1, nullptr, H, scale, rhs, nullptr, scratch, nullptr, s))) return st;
+  } else if ((st = cuda_status(cudaMemsetAsync(rhs, 0, sizeof(double) * v.n_red, s)))) {
+    return st;
+  }
+  if ((st = h8_damage_launch(v, mm, slot, 0, d, H, scale, Ad, nullptr, scratch, nullptr, s))) return st;
+  { note_launch(); diff_norm2_kernel<<<grid_for(v.n_red), kThreads, 0, s>>>(v.n_red, rhs, Ad, ws); }
+  if ((st = last_launch_status())) return st;
+  double r2 = 0.0;
+  if ((st = red_ws_fetch(ws, &r2, 1, s))) return st;
+  *norm_host = sqrt(r2);
+  return PHASTB_OK;
+}
+
+int phastb_scale_set(int n, const double* x, double factor, int index, double value, double* out, void* stream) {
+  if (n < 0 || (n > 0 && (!x || !out)) || index >= n) return PHASTB_ERR_ARG;
+  if (n == 0) return PHASTB_OK;
+  { note_launch(); scale_set_kernel<<<grid_for(n), kThreads, 0, (cudaStream_t)stream>>>(n, x, factor, index, value,
+                                                                                         out); }
+  return last_launch_status();
+}
+
+}  // extern "C"
+
 // ------------------------------------------------------------ allocation-free elastic action
 //
 // Some callers cannot allocate device memory at all: a host runtime bound

@@ -90,9 +90,9 @@ class PhaseFieldDamageSolver:
              self._Gc_l0, ptr(self._Gc_l0_e), ptr(b), ptr(m_inv), stream())
         return b, m_inv
 
-    def compute_residual(self, H, d):
+    def compute_residual(self, H_input, d):
         """A d - b of the AT2 system (damage_solver.py:1988-2093, Q4 AT2 branch)."""
-        Hq = self._normalize_q4_H(H)
+        Hq = self._normalize_q4_H(H_input)
         b, _ = self._prepare(Hq)
         y = torch.empty_like(b)
         dd = d.to(torch.float64).contiguous()

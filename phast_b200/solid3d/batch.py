@@ -24,9 +24,9 @@ MATRIX, INCLUSION, INTERFACE = 0, 1, 2
 #: matrix, particle ('fibre') and interface shell ('bn_band') phases of the
 #: particle-in-cube batch: E (MPa), nu, Gc (N/mm).  The shell carries 0.3 x the
 #: matrix Gc and the matrix stiffness; the particle keeps the matrix Gc.
-BATCH_PHASES = (PhaseMaterial("mi_matrix", 3000.0, 0.3, 0.5),
-                PhaseMaterial("fibre", 70000.0, 0.3, 0.5),
-                PhaseMaterial("bn_band", 3000.0, 0.3, 0.15))
+BATCH_PHASES = (PhaseMaterial("mi_matrix", "isotropic", 0.5, "spectral", 3000.0, 0.3),
+                PhaseMaterial("fibre", "isotropic", 0.5, "spectral", 70000.0, 0.3),
+                PhaseMaterial("bn_band", "isotropic", 0.15, "spectral", 3000.0, 0.3))
 
 
 @dataclass
@@ -130,7 +130,8 @@ def build_operator(cell, load, device="cuda", phases=BATCH_PHASES, kappa=1e-6):
     from .operator import PeriodicVoxelPhaseFieldOperator
     h = 1.0 / cell.n
     grid = VoxelGrid((cell.n, cell.n, cell.n), (h, h, h))
-    return PeriodicVoxelPhaseFieldOperator(grid, cell.phase, list(phases), 2 * h, kappa, load, device=device)
+    return PeriodicVoxelPhaseFieldOperator.from_slots(grid, cell.phase, list(phases), 2 * h, kappa, load,
+                                                      device=device)
 
 
 @dataclass
@@ -153,7 +154,7 @@ def _run_one(cell, increments, device, form, cfg):
     load = batch_load()
     t0 = time.perf_counter()
     op = build_operator(cell, load, device=device)
-    solver = StaggeredSolver(op, cfg or SolverConfig(), form or PLAIN)
+    solver = StaggeredSolver(op, cfg=cfg or SolverConfig(kappa=op.kappa), form=form or PLAIN)
     state = solver.initial_state()
     sig, pm, pp = [], 0, 0
     for _ in range(min(increments, load.n_increments)):

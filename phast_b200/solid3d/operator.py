@@ -15,7 +15,7 @@ import torch
 
 from .. import _lib
 from .._lib import call, ptr, stream
-from .model import isotropic_C
+from .model import SolverConfig, build_element_arrays, isotropic_C, unsupported_options
 
 PORE = "pore"
 
@@ -30,22 +30,60 @@ def _driver_code(phase, split_isotropic):
 class PeriodicVoxelPhaseFieldOperator:
     """Matrix-free mechanics and damage operators of one periodic voxel cell (AT2).
 
-    Parameters
-    ----------
-    grid : VoxelGrid-like (``shape``, ``h``, ``periodic``)
-    slot : (nz, ny, nx) or (E,) integer array of material slots
-    phases : list of phase materials, one per slot (``E``, ``nu``, ``Gc``, ``driver``, ``name``)
-    ell, kappa : phase-field length and residual stiffness
-    load : LoadCase-like (``controlled``, ``fixed_zero``)
-    pinned_node : reduced node whose fluctuation is fixed (default: first node touching no pore)
+    ``PeriodicVoxelPhaseFieldOperator(model, load, cfg, *, materials=None, pinned_node=None,
+    pfczm_strengths=None)`` as PhAST's constructor (operator.py:172-320): ``model`` a
+    ``VoxelModel`` (grid, phase ids, material table with the length scale ``ell``), ``load``
+    a ``LoadCase``, ``cfg`` a ``SolverConfig`` (``kappa``, ``energy_split_isotropic``,
+    ``device``), ``materials`` the ``build_element_arrays`` result (built from ``model`` and
+    ``cfg`` when omitted), ``pinned_node`` the reduced node whose fluctuation is fixed
+    (default: the first node touching no pore voxel, periodic.py:224-249).  The reference's
+    data classes are accepted as well as this package's.  Options the GPU kernels do not
+    run (see ``model.unsupported_options``) raise ``NotImplementedError``.
     """
 
-    def __init__(self, grid, slot, phases, ell, kappa, load, *, split_isotropic="spectral", pinned_node=None,
-                 device="cuda"):
+    def __init__(self, model, load, cfg, *, materials=None, pinned_node=None, pfczm_strengths=None):
+        bad = unsupported_options(cfg)
+        if bad:
+            raise NotImplementedError(f"the B200 backend does not run {', '.join(bad)}")
+        if pfczm_strengths is not None:
+            raise ValueError("pfczm_strengths applies to damage_law 'pfczm' only")
+        model.validate()
+        if materials is None:
+            materials = build_element_arrays(model, cfg)
+        if int(materials.stiffness_index.shape[0]) != int(model.grid.n_elements):
+            raise ValueError(f"materials describe {int(materials.stiffness_index.shape[0])} elements, the grid has "
+                             f"{model.grid.n_elements}")
+        present = model.phases_present()
+        phases = [model.materials.phases[name] for name in present]
+        framed = [p.name for p in phases if getattr(p, "kind", "isotropic") != "isotropic"]
+        if framed:
+            raise NotImplementedError(f"smeared-laminate phases {framed} are not supported by the GPU backend")
+        slot = materials.stiffness_index.detach().to("cpu").numpy().astype(np.int64)
+        self.model = model
+        self.cfg = cfg
+        self.mat_arrays = materials
+        self._setup(model.grid, slot, phases, float(model.materials.length_scale), float(cfg.kappa), load,
+                    cfg.energy_split_isotropic, pinned_node, materials.stiffness_index.device)
+
+    @classmethod
+    def from_slots(cls, grid, slot, phases, ell, kappa, load, *, split_isotropic="spectral", pinned_node=None,
+                   device="cuda"):
+        """An operator from per-voxel material slots: ``slot`` (nz, ny, nx) or (E,) indexes ``phases``
+        (objects with ``name``, ``E``, ``nu``, ``Gc``, ``driver``); ``ell`` and ``kappa`` given directly."""
+        self = cls.__new__(cls)
+        self.model = None
+        self.cfg = SolverConfig(device=str(device), kappa=float(kappa), energy_split_isotropic=split_isotropic)
+        self.mat_arrays = None
+        self._setup(grid, np.asarray(slot).reshape(-1).astype(np.int64), list(phases), float(ell), float(kappa),
+                    load, split_isotropic, pinned_node, device)
+        return self
+
+    def _setup(self, grid, slot_np, phases, ell, kappa, load, split_isotropic, pinned_node, device):
         self.grid = grid
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise ValueError("the B200 backend needs a CUDA device")
+        self.dtype = torch.float64
         nx, ny, nz = (int(v) for v in grid.shape)
         hx, hy, hz = (float(v) for v in grid.h)
         px, py, pz = (bool(v) for v in getattr(grid, "periodic", (True, True, True)))
@@ -61,7 +99,6 @@ class PeriodicVoxelPhaseFieldOperator:
         self.ell = float(ell)
         self.kappa = float(kappa)
         self.load = load
-        slot_np = np.asarray(slot).reshape(-1).astype(np.int64)
         if slot_np.shape[0] != self.n_elements:
             raise ValueError(f"slot must hold {self.n_elements} entries")
         if len(phases) > _lib.MAX_SLOTS or slot_np.min() < 0 or slot_np.max() >= len(phases):
@@ -96,6 +133,8 @@ class PeriodicVoxelPhaseFieldOperator:
         self._scratch64 = None
         self._scratch32 = None
         self._red = _lib.Workspace(self.device)
+        self._rec = _lib.Workspace(self.device)
+        self._resid = _lib.Workspace(self.device)
 
     # -- construction helpers -----------------------------------------------------------
     def _choose_pinned_node(self):
@@ -180,8 +219,15 @@ class PeriodicVoxelPhaseFieldOperator:
         call("phastb_h8_degradation", self.vgrid, self._dt(d), ptr(d), self.kappa, ptr(g), stream())
         return g
 
-    def mech_action(self, x, g=None, *, d=None, mask=None, out=None):
-        """A(g) x (operator.py:1171-1194); ``d`` instead of ``g`` fuses the degradation."""
+    @staticmethod
+    def _no_closure(opening=None, closure=None):
+        if opening is not None or closure is not None:
+            raise NotImplementedError("interface opening and crack closure are not supported by the GPU backend")
+
+    def mech_action(self, x, g=None, *, opening=None, closure=None, d=None, mask=None, out=None):
+        """A(g) x (operator.py:1171-1194); ``g=None`` means undamaged.  ``d`` instead of ``g`` fuses
+        the degradation into the action; ``mask`` zeroes rows; ``out`` receives the result."""
+        self._no_closure(opening, closure)
         x = self._check("x", x, (self.n_mech,))
         gq = None if g is None else self._check("g", g, (self.n_elements, 8), x.dtype)
         dd = None if d is None else self._check("d", d, (self.n_red,)).to(x.dtype)
@@ -195,6 +241,10 @@ class PeriodicVoxelPhaseFieldOperator:
         call("phastb_h8_mech_apply", self.vgrid, self.mat, ptr(self.slot), self._dt(x), ptr(x), ptr(gq), ptr(dd),
              ptr(mk), ptr(y), self.scratch(x.dtype), stream())
         return y
+
+    def mech_operator(self, g=None, *, d=None):
+        """The action ``v -> A(g) v`` as a callable that ``solve_constrained`` recognises."""
+        return MechOperator(self, g, d)
 
     def tile_shape(self, dtype=torch.float64, shape=None):
         """Tile shape (ox, oy, kz) of the elastic-action kernel; ``shape`` records a new one."""
@@ -219,8 +269,9 @@ class PeriodicVoxelPhaseFieldOperator:
              self.scratch(dtype), wn, shape, C.byref(ms), stream())
         return tuple(shape), float(ms.value)
 
-    def mech_diagonal(self, g=None, *, d=None):
+    def mech_diagonal(self, g=None, *, opening=None, closure=None, d=None):
         """Jacobi diagonal of A(g) (operator.py:1196-1254)."""
+        self._no_closure(opening, closure)
         dtype = g.dtype if g is not None else (d.dtype if d is not None else torch.float64)
         gq = None if g is None else self._check("g", g, (self.n_elements, 8), dtype)
         dd = None if d is None else self._check("d", d, (self.n_red,), dtype)
@@ -239,16 +290,28 @@ class PeriodicVoxelPhaseFieldOperator:
              C.byref(en), self.scratch(torch.float64), stream())
         return np.array(list(rE)), float(en.value)
 
-    def macro_stress(self, x, g=None, *, d=None):
+    def macro_stress(self, x, g=None, *, opening=None, closure=None, d=None):
         """Sigma = r_E / V (operator.py:1303-1316)."""
+        self._no_closure(opening, closure)
         rE, _ = self._stress_energy(x, g, d)
         return torch.as_tensor(rE / self.volume, dtype=torch.float64, device=self.device)
 
-    def elastic_energy(self, x, g=None, *, d=None):
+    def elastic_energy(self, x, g=None, *, opening=None, closure=None, d=None):
+        """0.5 x . A(g) x in mJ, a 0-dim tensor (operator.py:1318-1340)."""
+        self._no_closure(opening, closure)
         _, en = self._stress_energy(x, g, d)
         return torch.tensor(en, dtype=torch.float64, device=self.device)
 
-    def hill_mandel(self, x, g=None):
+    def mean_strain(self, x):
+        """Volume-average total strain <eps> (6,) (operator.py:1342-1389): E on a triply periodic cell."""
+        if not all(bool(p) for p in getattr(self.grid, "periodic", (True, True, True))):
+            raise NotImplementedError("mean_strain of a cell with free faces is not supported by the GPU backend")
+        x = self._check("x", x, (self.n_mech,))
+        return self.split_mech(x)[1].clone()
+
+    def hill_mandel(self, x, g=None, *, closure=None):
+        """``mean_work = 2 E_el / V``, ``macro_work = Sigma . E`` and their relative gap (operator.py:1390-1413)."""
+        self._no_closure(None, closure)
         rE, en = self._stress_energy(x, g)
         E = self.split_mech(x)[1].detach().cpu().numpy()
         mean = 2.0 * en / self.volume
@@ -295,9 +358,58 @@ class PeriodicVoxelPhaseFieldOperator:
              self.scratch(), stream())
         return y
 
-    def damage_system(self, H, scaled=True):
+    def fracture_energy(self, d):
+        """Fracture energy in mJ (operator.py:1511-1545): per element Gc/(2 ell) d.M d ('local') plus
+        Gc ell/2 d.L d ('gradient'), and 'by_phase' over the present phases (pores included)."""
+        out = self.increment_record(None, d, None, 1.0)
+        return {"total": out["local"] + out["gradient"], "local": out["local"], "gradient": out["gradient"],
+                "by_phase": out["by_phase"]}
+
+    def increment_record(self, x, d, H, threshold):
+        """All scalars of an accepted increment in one kernel pair and one host read (``x`` may be None):
+        E, r_E, elastic energy, fracture energy (total, parts, by phase), element-mean damage sum,
+        damaged-element count, max H and max d."""
+        d = self._check("d", d, (self.n_red,), torch.float64)
+        xx = None if x is None else self._check("x", x, (self.n_mech,), torch.float64)
+        Hq = None if H is None else self._check("H", H, (self.n_elements, 8), torch.float64)
+        out = (C.c_double * _lib.RECORD_WORDS)()
+        wp, wn = self._rec.get(_lib.load().phastb_h8_record_workspace_bytes(self.vgrid))
+        call("phastb_h8_increment_record", self.vgrid, self.mat, ptr(self.slot), ptr(xx), ptr(d), ptr(Hq),
+             float(threshold), out, wp, wn, stream())
+        v = list(out)
+        S = _lib.MAX_SLOTS
+        return {"E": np.array(v[0:6]), "rE": np.array(v[6:12]), "energy": v[12],
+                "by_phase": {p.name: v[13 + s] for s, p in enumerate(self.phases)},
+                "local": v[13 + S], "gradient": v[14 + S], "sum_element_d": v[15 + S], "damaged": v[16 + S],
+                "max_H": v[17 + S], "max_d": v[18 + S]}
+
+    def damage_residual_norm(self, H, d):
+        """||rhs - A d|| of the scaled damage system of history ``H`` (staggered.py:766-770)."""
+        d = self._check("d", d, (self.n_red,), torch.float64)
+        Hq = None if H is None else self._check("H", H, (self.n_elements, 8), torch.float64)
+        r = C.c_double(0.0)
+        wp, wn = self._resid.get(_lib.load().phastb_h8_damage_residual_workspace_bytes(self.vgrid))
+        call("phastb_h8_damage_residual_norm", self.vgrid, self.mat, ptr(self.slot), ptr(Hq), self.damage_scale,
+             ptr(d), C.byref(r), wp, wn, stream())
+        return float(r.value)
+
+    def damage_system(self, H, *, scaled=True):
         """The scaled damage system; solved by ``solve_h8_scalar_box_kkt`` (operator.py:1495-1509)."""
         return H8DamageSystem(self, H, self.damage_scale if scaled else 1.0)
+
+
+class MechOperator:
+    """``v -> A(g) v`` of one operator and degradation (``g`` (E, 8) or the damage ``d``), as a callable.
+
+    ``solve_constrained`` runs its whole solve as one fused C-ABI call when given this
+    object (or the bound ``op.mech_action``) instead of an arbitrary function.
+    """
+
+    def __init__(self, op, g=None, d=None):
+        self.op, self.g, self.d = op, g, d
+
+    def __call__(self, v):
+        return self.op.mech_action(v, self.g, d=self.d)
 
 
 class H8DamageSystem:

@@ -1,7 +1,8 @@
 """3D solvers and the staggered increment on the GPU.
 
-* ``solve_constrained`` -- Jacobi PCG with device flags on the free set
-  (solid3d/linalg.py:99-287); the whole solve is one C-ABI call.
+* ``pcg`` / ``solve_constrained`` -- Jacobi PCG with device flags on the free set
+  (solid3d/linalg.py:99-287), the reference's signatures; with this backend's
+  elastic action the whole constrained solve is one C-ABI call.
 * ``solve_h8_scalar_box_kkt`` -- primal active-set box-KKT damage solve with a
   Dirichlet PCG per set and the KKT audit (solvers/box_kkt_h8.py:256-778).
 * ``StaggeredSolver`` -- alternate minimisation of one load increment with
@@ -10,8 +11,9 @@
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 import math
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 from time import perf_counter
 
 import numpy as np
@@ -19,27 +21,62 @@ import torch
 
 from .. import _lib
 from .._lib import ptr, raw, stream
-from .model import SolverConfig
+from .model import unsupported_options
 
 
 class PCGBreakdownError(RuntimeError):
-    """Non-positive curvature, non-positive diagonal or non-finite values (linalg.py:41-44)."""
+    """Non-positive curvature, non-positive diagonal or non-finite values (linalg.py:41-42)."""
+
+
+class PCGConvergenceError(RuntimeError):
+    """Raised by callers that require convergence when PCG runs out of iterations (linalg.py:45-50)."""
+
+    def __init__(self, message, info):
+        super().__init__(message)
+        self.info = info
+
+
+@dataclass(frozen=True)
+class BoxKKTFailureEvidence:
+    """What a failed box-KKT solve had done (box_kkt_h8.py:226-234)."""
+    reason: str
+    active_set_iterations: int
+    total_pcg_iterations: int
 
 
 class H8ScalarBoxKKTConvergenceError(RuntimeError):
     """The active set did not stabilise or a PCG did not converge (box_kkt_h8.py:239-253)."""
 
+    def __init__(self, reason, *, last_solution=None, last_linear_solve=None, evidence=None):
+        super().__init__(reason)
+        self.last_solution = last_solution
+        self.last_linear_solve = last_linear_solve
+        self.evidence = evidence
+
 
 class StaggerConvergenceError(RuntimeError):
-    """A failed increment; carries the last accepted state (staggered.py:221-263)."""
+    """A load (sub-)increment could not be solved (solid3d/staggered.py:221-263).
 
-    def __init__(self, message, state=None):
+    ``state`` is the last accepted state, ``target`` the controlled strain of the failed
+    attempt, ``increment`` the 1-based load-case increment, ``cutbacks`` the halving depth,
+    ``reason`` why the last attempt failed, ``attempts`` the attempts made for the increment
+    and ``records`` the records accepted before the failure.
+    """
+
+    def __init__(self, message, *, state, target, increment, cutbacks, reason, attempts=1, records=()):
         super().__init__(message)
         self.state = state
+        self.target = float(target)
+        self.increment = int(increment)
+        self.cutbacks = int(cutbacks)
+        self.reason = str(reason)
+        self.attempts = int(attempts)
+        self.records = tuple(records)
 
 
 @dataclass(frozen=True)
 class PCGInfo:
+    """Outcome of one PCG solve (linalg.py:53-68)."""
     iterations: int
     converged: bool
     rhs_norm: float
@@ -47,9 +84,166 @@ class PCGInfo:
     relative_residual: float
 
 
-def solve_constrained(op, *, fixed_mask, fixed_values, g=None, d=None, x0=None, rtol=1e-8, atol=0.0, maxiter=5000,
-                      check_every=10):
-    """``A(g) x = 0`` with ``x = fixed_values`` on ``fixed_mask`` by projected Jacobi PCG (linalg.py:223-287)."""
+def _fused_target(action):
+    """(op, g, d) when ``action`` is this backend's elastic action, else None.
+
+    Recognised: the bound method ``op.mech_action`` (undamaged) and the callable of
+    ``op.mech_operator(g, d=...)``.
+    """
+    from .operator import MechOperator, PeriodicVoxelPhaseFieldOperator
+    if isinstance(action, MechOperator):
+        return action.op, action.g, action.d
+    if getattr(action, "__func__", None) is PeriodicVoxelPhaseFieldOperator.mech_action and \
+            isinstance(getattr(action, "__self__", None), PeriodicVoxelPhaseFieldOperator):
+        return action.__self__, None, None
+    return None
+
+
+def _check_settings(rtol, atol, maxiter, check_every):
+    rtol, atol = float(rtol), float(atol)
+    if not math.isfinite(rtol) or rtol < 0.0 or not math.isfinite(atol) or atol < 0.0:
+        raise ValueError("rtol and atol must be finite and non-negative")
+    if rtol == 0.0 and atol == 0.0:
+        raise ValueError("rtol and atol must not both be zero")
+    for name, value in (("maxiter", maxiter), ("check_every", check_every)):
+        if isinstance(value, bool) or int(value) != value or int(value) < 1:
+            raise ValueError(f"{name} must be an integer >= 1, got {value!r}")
+
+
+def _vec(name, v, like=None):
+    if not isinstance(v, torch.Tensor):
+        raise TypeError(f"{name} must be a torch.Tensor")
+    if v.ndim != 1:
+        raise ValueError(f"{name} must be one-dimensional, got shape {tuple(v.shape)}")
+    if v.dtype != torch.float64:
+        raise TypeError(f"{name} must be float64, got {v.dtype}")
+    if like is not None and (v.shape != like.shape or v.device != like.device):
+        raise ValueError(f"{name} must have shape {tuple(like.shape)} on {like.device}")
+    return v
+
+
+def pcg(action, rhs, *, diag, x0=None, rtol=1.0e-8, atol=0.0, maxiter=5000, check_every=10):
+    """Jacobi PCG for ``A x = rhs`` with an arbitrary matrix-free ``action`` (linalg.py:99-220).
+
+    Stops when ``||r|| <= max(rtol ||b||, atol)``; the convergence and breakdown flags stay
+    on the device and are read every ``check_every`` iterations.  Returns ``(x, PCGInfo)``;
+    ``info.converged`` is False when ``maxiter`` is reached; breakdown raises
+    :class:`PCGBreakdownError`.  The action is the caller's own code, so this loop drives it
+    from the host with device vector updates; the staggered solver never takes this route
+    (its solves are single fused C-ABI calls).
+    """
+    _check_settings(rtol, atol, maxiter, check_every)
+    _vec("rhs", rhs)
+    _vec("diag", diag, rhs)
+    if x0 is not None:
+        _vec("x0", x0, rhs)
+    head = torch.stack((torch.linalg.vector_norm(rhs), torch.isfinite(rhs).all().double(),
+                        (diag > 0).all().double(), torch.isfinite(diag).all().double())).tolist()
+    b_norm = head[0]
+    if head[1] < 1 or not math.isfinite(b_norm):
+        raise PCGBreakdownError("PCG right-hand side contains a non-finite value")
+    if head[3] < 1:
+        raise PCGBreakdownError("PCG diagonal contains a non-finite value")
+    if head[2] < 1:
+        raise PCGBreakdownError("PCG diagonal has a non-positive entry (non-positive curvature)")
+    if b_norm == 0.0:
+        return torch.zeros_like(rhs), PCGInfo(0, True, 0.0, 0.0, 0.0)
+    tol = max(rtol * b_norm, atol)
+    if x0 is None:
+        x, r, r_norm = torch.zeros_like(rhs), rhs.clone(), b_norm
+    else:
+        x = x0.clone()
+        r = rhs - _vec("action(x0)", action(x), rhs)
+        r_norm = float(torch.linalg.vector_norm(r))
+        if not math.isfinite(r_norm):
+            raise PCGBreakdownError("PCG initial residual is not finite")
+    if r_norm <= tol:
+        return x, PCGInfo(0, True, b_norm, r_norm, r_norm / b_norm)
+    inv = 1.0 / diag
+    z = r * inv
+    p = z.clone()
+    rz = torch.dot(r, z)
+    tol2 = torch.tensor(tol * tol, dtype=torch.float64, device=rhs.device)
+    running = torch.ones((), dtype=torch.bool, device=rhs.device)
+    bad_curv = torch.zeros_like(running)
+    bad_val = torch.zeros_like(running)
+    steps = torch.zeros((), dtype=torch.float64, device=rhs.device)
+    rr = torch.dot(r, r)
+    for it in range(1, int(maxiter) + 1):
+        Ap = action(p)
+        pAp = torch.dot(p, Ap)
+        curv = pAp > 0
+        bad_curv |= running & ~curv
+        bad_val |= ~torch.isfinite(pAp)
+        take = running & curv
+        alpha = torch.where(take, rz / torch.where(curv, pAp, torch.ones_like(pAp)), torch.zeros_like(pAp))
+        x += alpha * p
+        r -= alpha * Ap
+        steps += take.double()
+        z = r * inv
+        rz_next = torch.dot(r, z)
+        rr = torch.dot(r, r)
+        bad_val |= ~(torch.isfinite(rz_next) & torch.isfinite(rr))
+        running &= rr > tol2
+        beta = torch.where(running & (rz > 0), rz_next / torch.where(rz > 0, rz, torch.ones_like(rz)),
+                           torch.zeros_like(rz))
+        p = z + beta * p
+        rz = rz_next
+        if it % int(check_every) == 0 or it == int(maxiter):
+            f = torch.stack((bad_val.double(), bad_curv.double(), running.double(), rr, steps)).tolist()
+            if f[0] > 0:
+                raise PCGBreakdownError(f"PCG produced a non-finite value by iteration {it}")
+            if f[1] > 0:
+                raise PCGBreakdownError(f"PCG met non-positive curvature p.A p <= 0 by iteration {it}; "
+                                        "the operator is not positive definite on the free set")
+            r_norm = math.sqrt(f[3])
+            if f[2] < 1:
+                return x, PCGInfo(int(f[4]), True, b_norm, r_norm, r_norm / b_norm)
+    return x, PCGInfo(int(maxiter), False, b_norm, r_norm, r_norm / b_norm)
+
+
+def solve_constrained(action, *, diag, fixed_mask, fixed_values, rhs=None, x0=None, rtol=1.0e-8, atol=0.0,
+                      maxiter=5000, check_every=10):
+    """``A x = rhs`` with ``x = fixed_values`` on ``fixed_mask`` by projected Jacobi PCG (linalg.py:223-287).
+
+    When ``action`` is this backend's elastic action (``op.mech_action`` or
+    ``op.mech_operator(g, d=...)``) and ``rhs`` is None, the whole solve is one fused C-ABI
+    call with the convergence flags on the device; any other action runs :func:`pcg` on the
+    free set.  ``diag`` is the Jacobi diagonal (the fused solve forms its own, which is the
+    same diagonal of the same operator).  Returns ``(x, PCGInfo)`` with
+    ``x[fixed] == fixed_values[fixed]`` exactly.
+    """
+    _vec("fixed_values", fixed_values)
+    n = fixed_values.shape[0]
+    if not isinstance(fixed_mask, torch.Tensor) or fixed_mask.dtype != torch.bool:
+        raise TypeError("fixed_mask must be a torch.bool tensor")
+    if fixed_mask.shape != (n,) or fixed_mask.device != fixed_values.device:
+        raise ValueError(f"fixed_mask must have shape ({n},) on {fixed_values.device}")
+    _vec("diag", diag, fixed_values)
+    if rhs is not None:
+        _vec("rhs", rhs, fixed_values)
+    if x0 is not None:
+        _vec("x0", x0, fixed_values)
+    _check_settings(rtol, atol, maxiter, check_every)
+    target = _fused_target(action)
+    if target is not None and rhs is None:
+        op, g, d = target
+        return _solve_fused(op, fixed_mask=fixed_mask, fixed_values=fixed_values, g=g, d=d, x0=x0, rtol=rtol,
+                            atol=atol, maxiter=maxiter, check_every=check_every)
+    free = ~fixed_mask
+    zero = torch.zeros_like(fixed_values)
+    x_c = torch.where(fixed_mask, fixed_values, zero)
+    image = _vec("action(x_c)", action(x_c), fixed_values)
+    b_f = torch.where(free, -image if rhs is None else rhs - image, zero)
+    y, info = pcg(lambda v: torch.where(free, action(v), zero), b_f, diag=torch.where(free, diag, torch.ones_like(diag)),
+                  x0=None if x0 is None else torch.where(free, x0, zero), rtol=rtol, atol=atol, maxiter=maxiter,
+                  check_every=check_every)
+    return torch.where(free, y, x_c), info
+
+
+def _solve_fused(op, *, fixed_mask, fixed_values, g=None, d=None, x0=None, rtol=1e-8, atol=0.0, maxiter=5000,
+                 check_every=10):
+    """The constrained Jacobi PCG of the elastic action as one C-ABI call (FP64)."""
     n = op.n_mech
     mask = fixed_mask.to(torch.uint8).contiguous()
     vals = fixed_values.to(torch.float64).contiguous()
@@ -110,8 +304,8 @@ def solve_constrained_form(op, form, *, fixed_mask, fixed_values, d=None, x0=Non
     lambda_max estimates from one solve to the next.
     """
     if form.precond == "jacobi" and not form.mixed:
-        return solve_constrained(op, fixed_mask=fixed_mask, fixed_values=fixed_values, d=d, x0=x0, rtol=rtol,
-                                 atol=atol, maxiter=maxiter, check_every=check_every)
+        return _solve_fused(op, fixed_mask=fixed_mask, fixed_values=fixed_values, d=d, x0=x0, rtol=rtol,
+                            atol=atol, maxiter=maxiter, check_every=check_every)
     n = op.n_mech
     opts = form.struct()
     nbytes = _lib.load().phastb_h8_mech_solve_ex_workspace_bytes(op.vgrid, opts)
@@ -139,11 +333,23 @@ def solve_constrained_form(op, form, *, fixed_mask, fixed_values, d=None, x0=Non
 
 
 @dataclass(frozen=True)
+class KKTDiagnostics:
+    """The verdict of the KKT audit of a box-KKT solve (box_kkt_h8.py:165-191, ``satisfies_kkt``)."""
+    satisfies_kkt: bool
+
+
+@dataclass(frozen=True)
 class BoxKKTResult:
+    """A converged box-KKT damage field (box_kkt_h8.py:208-223): ``solution``, the iteration counts
+    and the audit verdict (``satisfies_kkt``, also as ``kkt.satisfies_kkt``)."""
     solution: torch.Tensor
     total_pcg_iterations: int
     active_set_iterations: int
     satisfies_kkt: bool
+
+    @property
+    def kkt(self):
+        return KKTDiagnostics(self.satisfies_kkt)
 
 
 def solve_h8_scalar_box_kkt(system, *, lower_bound=0.0, upper_bound=1.0, initial=None, linear_tolerance=1e-10,
@@ -181,64 +387,171 @@ def solve_h8_scalar_box_kkt(system, *, lower_bound=0.0, upper_bound=1.0, initial
     if st in (_lib.BREAKDOWN, _lib.NONFINITE):
         raise RuntimeError(f"PCG operator is not positive definite on the free space (status {st})")
     if st == _lib.NONCONVERGED:
-        raise H8ScalarBoxKKTConvergenceError(
-            f"H8 scalar box-KKT failed after {info[1]} active-set iterations ({info[0]} PCG iterations)")
+        reason = f"H8 scalar box-KKT failed after {info[1]} active-set iterations ({info[0]} PCG iterations)"
+        raise H8ScalarBoxKKTConvergenceError(reason, last_solution=out,
+                                             evidence=BoxKKTFailureEvidence(reason, int(info[1]), int(info[0])))
     _lib.check(st, "phastb_h8_damage_box_kkt")
     return BoxKKTResult(out, int(info[0]), int(info[1]), bool(info[2]))
 
 
-@dataclass
+@dataclass(eq=False)
 class SolverState:
-    """Accepted state of the staggered solver (staggered.py:167-218)."""
+    """Accepted solution after ``step`` solves (solid3d/staggered.py:166-218).
+
+    ``x = [u~, E]``, ``d`` the reduced nodal damage and ``H`` the (E, 8) history on the
+    device; ``macro_strain`` and ``macro_stress`` (6,) float64 tensors held on the host
+    (the solver reads them every increment); ``external_work`` in mJ; ``d_prev_step`` the
+    lower bound that produced ``d``; ``increment`` the load-case increments completed.
+    """
     step: int
     x: torch.Tensor
     d: torch.Tensor
     H: torch.Tensor
-    macro_strain: np.ndarray
-    macro_stress: np.ndarray
-    increment: int
+    macro_strain: torch.Tensor
+    macro_stress: torch.Tensor
+    external_work: float
+    d_prev_step: torch.Tensor
+    increment: int = 0
+
+    def clone(self):
+        return SolverState(int(self.step), self.x.clone(), self.d.clone(), self.H.clone(), self.macro_strain.clone(),
+                           self.macro_stress.clone(), float(self.external_work), self.d_prev_step.clone(),
+                           int(self.increment))
+
+    def to(self, device):
+        return SolverState(int(self.step), self.x.to(device), self.d.to(device), self.H.to(device),
+                           self.macro_strain.clone(), self.macro_stress.clone(), float(self.external_work),
+                           self.d_prev_step.to(device), int(self.increment))
 
 
-@dataclass
+@dataclass(frozen=True)
 class IncrementRecord:
-    increment: int
-    target: float
-    macro_stress: tuple
-    stagger_iters: int
-    pcg_iters_mech: int
-    pcg_iters_pf: int
-    active_set_iters: int
-    kkt_ok: bool
-    max_damage: float
-    wall_s: float
+    """Scalar record of one accepted load increment (solid3d/model.py:1234-1300), same fields.
+
+    ``mech_s``, ``damage_s`` and ``history_s`` stay 0: the solver enqueues its device work
+    asynchronously and does not stop to time the phases; ``wall_s`` is the increment's time.
+    """
+    step: int
+    increment: int = 0
+    load_factor: float = 0.0
+    macro_strain: tuple = (0.0,) * 6
+    macro_stress: tuple = (0.0,) * 6
+    applied_disp: float = 0.0
+    reaction_force: float = 0.0
+    elastic: float = 0.0
+    fracture: float = 0.0
+    fracture_by_phase: dict = field(default_factory=dict)
+    external: float = 0.0
+    balance_residual: float = 0.0
+    balance_residual_rel: float = 0.0
+    max_damage: float = 0.0
+    mean_damage: float = 0.0
+    damaged_volume_fraction: float = 0.0
+    max_H: float = 0.0
+    stagger_iters: int = 0
+    pcg_iters_mech: int = 0
+    pcg_iters_pf: int = 0
+    active_set_iters: int = 0
+    cutbacks: int = 0
+    converged: bool = True
+    kkt_ok: bool = True
+    stagger_change: float = 0.0
+    mech_relative_residual: float = 0.0
+    hill_mandel_rel: float = 0.0
+    wall_s: float = 0.0
+    mech_s: float = 0.0
+    damage_s: float = 0.0
+    history_s: float = 0.0
+    mean_strain: tuple | None = None
+    anderson_accepted: int | None = None
+    anderson_rejected: int | None = None
+    closure_solves: int | None = None
+    min_normal_strain: float | None = None
+    min_principal_strain: float | None = None
+    min_det_F: float | None = None
+    newton_iters_pf: int | None = None
 
 
-class _AttemptFailure(RuntimeError):
-    pass
+class _AttemptFailure(Exception):
+    """One attempt failed for a numerical reason (cut back or raise)."""
+
+
+_TINY = 1.0e-300
+_MIN_LINEAR_TOLERANCE = 4.0 * float(np.finfo(np.float64).eps)
 
 
 class StaggeredSolver:
-    """Staggered alternate minimisation of the hybrid AT2 cell (solid3d/staggered.py)."""
+    """Staggered hybrid AT2 solver of one periodic cell under mixed macro control (solid3d/staggered.py:391-1627).
 
-    def __init__(self, op, cfg=None, form=PLAIN):
+    ``StaggeredSolver(op, load=None, cfg=None, *, form=PLAIN)``: ``load`` and ``cfg`` default to
+    the operator's; ``form`` selects how the mechanics systems are solved (``MechForm``: the
+    reference's Jacobi PCG in FP64 by default, or multigrid and/or FP32 under FP64 refinement
+    to the same FP64 stopping rule).  Attributes ``op, load, cfg, last_state, n_attempts,
+    n_failed_attempts`` as the reference.
+    """
+
+    def __init__(self, op, load=None, cfg=None, *, form=PLAIN):
+        from .operator import PeriodicVoxelPhaseFieldOperator
+        if not isinstance(op, PeriodicVoxelPhaseFieldOperator):
+            raise TypeError("op must be a PeriodicVoxelPhaseFieldOperator")
+        load = op.load if load is None else load
+        cfg = op.cfg if cfg is None else cfg
+        if (int(load.controlled), set(load.free), set(load.fixed_zero)) != \
+                (int(op.load.controlled), set(op.load.free), set(op.load.fixed_zero)):
+            raise ValueError("load must control, free and fix the same components as op.load")
+        for key in ("kappa", "energy_split_isotropic", "energy_split_band", "band_stress", "dtype", "crack_closure",
+                    "damage_law"):
+            if getattr(cfg, key, None) != getattr(op.cfg, key, None):
+                raise ValueError(f"cfg.{key} must match the operator's ({getattr(op.cfg, key, None)!r})")
+        bad = unsupported_options(cfg)
+        if bad:
+            raise NotImplementedError(f"the B200 backend does not run {', '.join(bad)}")
         self.op = op
-        self.cfg = cfg or SolverConfig()
+        self.load = load
+        self.cfg = cfg
         self.form = form
+        self.device = op.device
+        self.dtype = torch.float64
+        self.last_state = None
+        self.n_attempts = 0
+        self.n_failed_attempts = 0
         self._lmax = (C.c_double * 3)()
         self.lmax_every = 10
-        self.load = op.load
-        self._c = int(op.load.controlled)
+        self._c = int(load.controlled)
         self._n_u = 3 * op.n_red
+        self._max_abs_target = max(abs(float(t)) for t in load.targets)
         self._u_floor = min(op.h) * math.sqrt(self._n_u)
         self._mask = op.mech_fixed_mask()
         self._red = _lib.Workspace(op.device)
-        self._tail = torch.empty(7, dtype=torch.float64, pin_memory=True)
+        lengths = tuple(n * h for n, h in zip(op.shape, op.h))
+        axis = self._c if self._c < 3 else 0
+        others = tuple(lengths[a] for a in range(3) if a != axis)
+        self._load_axis, self._load_length, self._face = axis, lengths[axis], others[0] * others[1]
 
+    # -- states ----------------------------------------------------------------------------
     def initial_state(self):
+        """Undamaged, unloaded state at step 0."""
         op = self.op
-        z = lambda *s: torch.zeros(*s, dtype=torch.float64, device=op.device)
-        return SolverState(0, z(op.n_mech), z(op.n_red), z(op.n_elements, 8), np.zeros(6), np.zeros(6), 0)
+        z = lambda *s: torch.zeros(*s, dtype=torch.float64, device=op.device)  # noqa: E731
+        host = lambda: torch.zeros(6, dtype=torch.float64)  # noqa: E731
+        return SolverState(0, z(op.n_mech), z(op.n_red), z(op.n_elements, 8), host(), host(), 0.0, z(op.n_red), 0)
 
+    def initial_record(self):
+        """The step-0 zero row (every present phase listed with zero fracture energy)."""
+        return IncrementRecord(step=0, fracture_by_phase={p.name: 0.0 for p in self.op.phases})
+
+    def _check_state(self, state):
+        if not isinstance(state, SolverState):
+            raise TypeError("state must be a SolverState")
+        op = self.op
+        for name, shape in (("x", (op.n_mech,)), ("d", (op.n_red,)), ("H", (op.n_elements, 8)),
+                            ("d_prev_step", (op.n_red,))):
+            t = getattr(state, name)
+            if not isinstance(t, torch.Tensor) or tuple(t.shape) != shape or t.dtype != torch.float64 or \
+                    t.device != op.device:
+                raise ValueError(f"state.{name} must be a float64 {shape} tensor on {op.device}")
+
+    # -- pieces of one staggered iteration --------------------------------------------------
     def _change(self, x_new, x_old, d_new, d_old, step_size):
         """max(du_rel, dE_rel, dd_inf) (staggered.py:1097-1124)."""
         out = (C.c_double * 5)()
@@ -267,105 +580,204 @@ class StaggeredSolver:
         return x, info
 
     def _damage(self, H, lower, initial):
+        """(d, PCG iterations, active-set iterations, kkt_ok) of the box-KKT damage solve (staggered.py:753-800)."""
         cfg, op = self.cfg, self.op
-        system = op.damage_system(H)
-        r0 = float(torch.linalg.vector_norm(system.rhs - system.apply(initial)))
+        r0 = op.damage_residual_norm(H, initial)
         if not math.isfinite(r0):
             raise _AttemptFailure("damage residual is not finite")
-        tol = min(cfg.damage_linear_tol, 0.1 * cfg.damage_kkt_tol / max(r0, 1.0))
-        tol = max(tol, 4.0 * float(np.finfo(np.float64).eps))
+        # the PCG stops at tol * max(||r0||, 1) while the KKT audit is absolute
+        tol = max(min(cfg.damage_linear_tol, 0.1 * cfg.damage_kkt_tol / max(r0, 1.0)), _MIN_LINEAR_TOLERANCE)
         # the bounds hold by construction: lower is the accepted damage of the last
         # increment (in [0, 1]) and initial is lower itself or a box-KKT solution
         try:
-            res = solve_h8_scalar_box_kkt(system, lower_bound=lower, upper_bound=1.0, initial=initial,
+            res = solve_h8_scalar_box_kkt(op.damage_system(H), lower_bound=lower, upper_bound=1.0, initial=initial,
                                           linear_tolerance=tol, kkt_tolerance=cfg.damage_kkt_tol,
                                           max_linear_iterations=cfg.damage_maxit,
                                           max_active_set_iterations=cfg.damage_max_active_set,
                                           check_bounds=False)
-        except (H8ScalarBoxKKTConvergenceError, RuntimeError) as exc:
+        except H8ScalarBoxKKTConvergenceError as exc:
             raise _AttemptFailure(f"damage box-KKT solve failed: {exc}") from exc
+        except RuntimeError as exc:
+            raise _AttemptFailure(f"damage PCG breakdown: {exc}") from exc
         return res.solution, res.total_pcg_iterations, res.active_set_iterations, res.satisfies_kkt
 
     def _predictor(self, state, previous, target):
-        x = state.x * (target / previous) if previous != 0.0 else torch.zeros_like(state.x)
-        x[self._n_u + self._c] = target
+        """x * (target / previous) with E[c] = target; zero start from an unloaded state (staggered.py:1207-1213)."""
+        x = torch.empty_like(state.x)
+        _lib.call("phastb_scale_set", self.op.n_mech, ptr(state.x), target / previous if previous != 0.0 else 0.0,
+                  self._n_u + self._c, float(target), ptr(x), stream())
         return x
 
-    def advance(self, state, target, *, increment=None):
-        """One increment to E_c = target (staggered.py:1215-1257); raises StaggerConvergenceError."""
+    # -- one attempt -------------------------------------------------------------------------
+    def advance(self, state, target, *, increment=None, cutbacks=0):
+        """Solve one (sub-)increment from ``state`` to ``E_c = target``, a single attempt (staggered.py:1215-1257).
+
+        Raises :class:`StaggerConvergenceError` (no cutback) on failure.
+        """
+        self._check_state(state)
         target = float(target)
+        if not math.isfinite(target):
+            raise ValueError(f"target must be finite, got {target!r}")
         previous = float(state.macro_strain[self._c])
         if target == previous:
             raise ValueError(f"target {target!r} equals the current controlled strain")
         increment = state.increment + 1 if increment is None else int(increment)
+        self.n_attempts += 1
         t0 = perf_counter()
         # lambda_max of the Jacobi-scaled operator barely moves with the damage
         # field; the multigrid re-estimates it every `lmax_every` increments
-        if (increment - 1) % self.lmax_every == 0:
+        if (increment - 1) % self.lmax_every == 0 and cutbacks == 0:
             self._lmax[0] = 0.0
         try:
-            return self._attempt(state, target, previous, increment, t0)
+            new_state, record = self._attempt(state, target, previous, increment, int(cutbacks), t0)
         except _AttemptFailure as exc:
-            raise StaggerConvergenceError(f"increment {increment} to E[{self._c}] = {target:.6e} failed: {exc}",
-                                          state) from exc
+            self.n_failed_attempts += 1
+            raise StaggerConvergenceError(
+                f"increment {increment} (cutback level {cutbacks}) to E[{self._c}] = {target:.6e} failed: {exc}",
+                state=state, target=target, increment=increment, cutbacks=int(cutbacks), reason=str(exc)) from exc
+        self.last_state = new_state
+        return new_state, record
 
-    def _attempt(self, state, target, previous, increment, t0):
+    def _attempt(self, state, target, previous, increment, cutbacks, t0):
         op, cfg = self.op, self.cfg
         values = op.mech_fixed_values(target)
-        step = abs(target - previous)
+        step_size = abs(target - previous)
         x_old = self._predictor(state, previous, target)
         d_old = state.d.clone()
         lower = state.d
         pm = pp = sets = 0
         kkt = True
         H = state.H
+        change = math.inf
         converged = False
+        info = None
         for k in range(1, cfg.max_stagger + 1):
             x_new, info = self._mechanics(d_old, values, x_old)
             pm += info.iterations
-            _, H = op.driving_history(x_new, state.H)
+            H = op.driving_history(x_new, state.H if cfg.history == "max" else None)[1]
             d_new, its, s, kkt = self._damage(H, lower, d_old)
             pp += its
             sets += s
-            change = self._change(x_new, x_old, d_new, d_old, step)
+            change = self._change(x_new, x_old, d_new, d_old, step_size)
             x_old, d_old = x_new, d_new
             if change <= cfg.stagger_tol and k >= cfg.min_stagger:
                 converged = True
                 break
         if not converged:
-            raise _AttemptFailure(f"staggered iteration did not converge in {cfg.max_stagger} iterations")
+            raise _AttemptFailure(f"staggered iteration did not converge in {cfg.max_stagger} iterations "
+                                  f"(change {change:.3e} > stagger_tol {cfg.stagger_tol:.3e})")
         d = d_old
         if cfg.final_mechanics_resolve:
             x, info = self._mechanics(d, values, x_old)
             pm += info.iterations
         else:
             x = x_old
-        g = op.degradation(d)
-        # E and max(d) travel in one copy that the stress reduction's read waits for
-        tail = torch.cat((op.split_mech(x)[1].detach(), d.max().reshape(1)))
-        self._tail.copy_(tail, non_blocking=True)
-        done = torch.cuda.Event()
-        done.record()
-        rE, _ = op._stress_energy(x, g)
-        done.synchronize()
-        sigma = rE / op.volume
-        E = self._tail[:6].numpy().copy()
-        d_max = float(self._tail[6])
+        # every scalar of the record in one kernel pair and one host read
+        rec = op.increment_record(x, d, H, cfg.damaged_threshold)
+        E = rec["E"]
+        sigma = rec["rE"] / op.volume
+        elastic = rec["energy"]
+        fracture = rec["local"] + rec["gradient"]
+        scalars = np.concatenate([E, sigma, [elastic, fracture, rec["max_d"], rec["max_H"]]])
+        if not np.isfinite(scalars).all():
+            raise _AttemptFailure("accepted state has non-finite stress, strain or energy")
+        mean_work = 2.0 * elastic / op.volume
+        macro_work = float(np.dot(sigma, E))
+        scale = max(abs(mean_work), abs(macro_work))
+        hill_rel = abs(mean_work - macro_work) / scale if scale > 0 else 0.0
+        c = self._c
+        external = state.external_work + op.volume * 0.5 * (sigma[c] + float(state.macro_stress[c])) * \
+            (target - previous)
+        residual = external - (elastic + fracture)
         completes = 1 <= increment <= self.load.n_increments and target == self.load.targets[increment - 1]
-        new_state = SolverState(state.step + 1, x, d, H, E.copy(), sigma,
-                                increment if completes else state.increment)
-        rec = IncrementRecord(increment, target, tuple(float(v) for v in sigma), k, pm, pp, sets, bool(kkt),
-                              d_max, perf_counter() - t0)
-        return new_state, rec
+        new_state = SolverState(state.step + 1, x, d, H, torch.as_tensor(E.copy()), torch.as_tensor(sigma.copy()),
+                                float(external), state.d, increment if completes else state.increment)
+        macro_strain = tuple(float(v) for v in E)
+        macro_stress = tuple(float(v) for v in sigma)
+        record = IncrementRecord(
+            step=new_state.step, increment=increment, load_factor=target / self._max_abs_target,
+            macro_strain=macro_strain, macro_stress=macro_stress,
+            applied_disp=macro_strain[self._load_axis] * self._load_length,
+            reaction_force=macro_stress[self._load_axis] * self._face, elastic=float(elastic),
+            fracture=float(fracture), fracture_by_phase=dict(rec["by_phase"]), external=float(external),
+            balance_residual=float(residual), balance_residual_rel=float(residual / max(abs(external), _TINY)),
+            max_damage=float(rec["max_d"]), mean_damage=float(rec["sum_element_d"] / op.n_elements),
+            damaged_volume_fraction=float(rec["damaged"] / op.n_elements), max_H=float(rec["max_H"]),
+            stagger_iters=k, pcg_iters_mech=pm, pcg_iters_pf=pp, active_set_iters=sets, cutbacks=int(cutbacks),
+            converged=True, kkt_ok=bool(kkt), stagger_change=float(change),
+            mech_relative_residual=float(info.relative_residual), hill_mandel_rel=float(hill_rel),
+            wall_s=perf_counter() - t0, mean_strain=macro_strain)
+        return new_state, record
 
-    def run(self, max_increments=None, on_increment=None, start_state=None):
-        state = self.initial_state() if start_state is None else start_state
-        n = self.load.n_increments if max_increments is None else min(self.load.n_increments, int(max_increments))
-        records = []
-        while state.increment < n:
-            target = self.load.targets[state.increment]
-            state, rec = self.advance(state, target)
-            records.append(rec)
+    # -- increments with cutback, and the load path -------------------------------------------
+    def advance_increment(self, state, target, *, increment=None, on_increment=None):
+        """One load-case increment with recursive half-step cutback (staggered.py:1523-1582).
+
+        A failed attempt with ``on_stagger_failure='cutback'`` splits the remaining
+        interval into two halves, each solved the same way, down to ``max_cutbacks``
+        levels; deeper failures (or any failure with ``'raise'``) raise
+        :class:`StaggerConvergenceError` with the last accepted state and the sub-steps
+        accepted so far.  ``on_increment(state, record)`` follows every accepted sub-step.
+        Returns ``(state, records)``.
+        """
+        increment = state.increment + 1 if increment is None else int(increment)
+        target = float(target)
+        accepted, latest, attempts = [], [state], [0]
+
+        def solve(current, end, depth):
+            attempts[0] += 1
+            try:
+                new_state, record = self.advance(current, end, increment=increment, cutbacks=depth)
+            except StaggerConvergenceError as exc:
+                if self.cfg.on_stagger_failure == "raise" or depth >= self.cfg.max_cutbacks:
+                    raise StaggerConvergenceError(
+                        f"increment {increment} to E[{self._c}] = {target:.6e} failed at cutback level {depth} "
+                        f"(max_cutbacks={self.cfg.max_cutbacks}, on_stagger_failure="
+                        f"{self.cfg.on_stagger_failure!r}): {exc.reason}",
+                        state=latest[0], target=end, increment=increment, cutbacks=depth, reason=exc.reason,
+                        attempts=attempts[0], records=tuple(accepted)) from exc
+                middle = 0.5 * (float(current.macro_strain[self._c]) + end)
+                current = solve(current, middle, depth + 1)
+                return solve(current, end, depth + 1)
+            accepted.append(record)
+            latest[0] = new_state
             if on_increment is not None:
-                on_increment(state, rec)
-        return state, records
+                on_increment(new_state, record)
+            return new_state
+
+        final = solve(state, target, 0)
+        if final.increment != increment:
+            final = dataclasses.replace(final, increment=increment)
+            self.last_state = final
+        return final, accepted
+
+    def run(self, *, start_state=None, max_increments=None, on_increment=None):
+        """Follow the load path from ``start_state`` (default the initial state), solving increments
+        ``start_state.increment + 1, ...`` (at most ``max_increments``); returns every accepted record
+        in order, the final state is ``last_state`` (staggered.py:1584-1636)."""
+        state = self.initial_state() if start_state is None else start_state
+        self._check_state(state)
+        self.last_state = state
+        first = int(state.increment)
+        last = self.load.n_increments
+        if max_increments is not None:
+            if isinstance(max_increments, bool) or int(max_increments) != max_increments or max_increments < 0:
+                raise ValueError(f"max_increments must be an integer >= 0, got {max_increments!r}")
+            last = min(last, first + int(max_increments))
+        records = []
+
+        def accepted(new_state, record):
+            records.append(record)
+            if on_increment is not None:
+                on_increment(new_state, record)
+
+        for index in range(first, last):
+            try:
+                state, _ = self.advance_increment(state, self.load.targets[index], increment=index + 1,
+                                                  on_increment=accepted)
+            except StaggerConvergenceError as exc:
+                exc.records = tuple(records)
+                self.last_state = exc.state
+                raise
+        self.last_state = state
+        return records

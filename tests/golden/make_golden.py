@@ -1,8 +1,9 @@
 """Generate golden vectors by running the PhAST reference implementation.
 
-Run in a container where the reference sources are present::
+Run in a container where the reference sources are present, passing the
+reference's ``src`` directory::
 
-    python tests/golden/make_golden.py /root/reference/src
+    python tests/golden/make_golden.py <path-to-reference-src>
 
 The reference is pure Python/PyTorch.  Its I/O-only dependencies (meshio,
 gmsh, h5py, zarr, numcodecs, matplotlib) are not needed on the hot path; they
@@ -425,7 +426,9 @@ def t3_cases():
 
 
 if __name__ == "__main__":
-    _import_reference(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) < 2:
+        raise SystemExit(__doc__)
+    _import_reference(sys.argv[1])
     import torch
     torch.set_num_threads(8)
     q4_cases()

@@ -29,9 +29,9 @@ def build(shape, periodic, seed):
     nx, ny, nz = shape
     h = (1.0 / nx, 1.1 / ny, 0.9 / nz)
     slot = rng.integers(0, 2, nx * ny * nz)
-    phases = [s3.PhaseMaterial("mi_matrix", 3000.0, 0.35, 0.5), s3.PhaseMaterial("fibre", 70000.0, 0.3, 0.4)]
+    phases = [s3.PhaseMaterial("mi_matrix", "isotropic", 0.5, "spectral", 3000.0, 0.35), s3.PhaseMaterial("fibre", "isotropic", 0.4, "spectral", 70000.0, 0.3)]
     load = s3.LoadCase("zz", 2, (0.01,), (), (0, 1, 3, 4, 5))
-    op = s3.PeriodicVoxelPhaseFieldOperator(s3.VoxelGrid(shape, h, periodic=periodic), slot, phases, 0.1, 1e-6,
+    op = s3.PeriodicVoxelPhaseFieldOperator.from_slots(s3.VoxelGrid(shape, h, periodic=periodic), slot, phases, 0.1, 1e-6,
                                             load, pinned_node=0)
     Cs, lams, mus = zip(*(isotropic_C(p.E, p.nu) for p in phases))
     ref = VoxelOperator(shape, h, slot, np.stack(Cs), np.array(lams), np.array(mus), np.array([0.5, 0.4]),

@@ -5,9 +5,10 @@ memory themselves (a host runtime bound through a thin FFI without a device
 allocator, or an application whose GPU memory is owned by another framework's
 pool).  It keeps its element scratch in a fixed device array inside the library,
 so these tests check that it gives the same result as the regular entry point
-``phastb_h8_mech_apply`` (which takes a caller workspace) on two calls in a row
--- the second call must not see anything left over from the first -- and that
-it refuses grids larger than its fixed capacity.  This file is collected last.
+``phastb_h8_mech_apply`` (which takes a caller workspace) and as the numpy
+oracle of the reference's ``mech_action`` on two calls in a row -- the second
+call must not see anything left over from the first -- and that it refuses
+grids larger than its fixed capacity.  This file is collected last.
 """
 import ctypes as C
 
@@ -23,10 +24,10 @@ TOL = 1e-12  # the FP64 tolerance of the other operator parity tests
 def _cell(shape):
     from phast_b200 import solid3d as s3
     h = 1.0 / shape[2]
-    phase = s3.sphere_pore_phase(shape, 0.25)
-    phases = [s3.PhaseMaterial("mi_matrix", 3000.0, 0.35, 0.5), s3.PhaseMaterial("pore", 3e-3, 0.35, 0.5)]
+    phase = s3.sphere_pore_phase(shape, 0.25, 0, 1)
+    phases = [s3.PhaseMaterial("mi_matrix", "isotropic", 0.5, "spectral", 3000.0, 0.35), s3.PhaseMaterial("pore", "isotropic", 0.5, "spectral", 3e-3, 0.35)]
     load = s3.LoadCase.ramp("zz", 2, 0.02, 50)
-    return s3.PeriodicVoxelPhaseFieldOperator(s3.VoxelGrid(shape, (h, h, h)), phase, phases, 2 * h, 1e-6, load)
+    return s3.PeriodicVoxelPhaseFieldOperator.from_slots(s3.VoxelGrid(shape, (h, h, h)), phase, phases, 2 * h, 1e-6, load)
 
 
 def _noalloc(op, x, d, mask=None):
@@ -61,6 +62,27 @@ def test_noalloc_matches_regular_entry_point_on_two_calls():
         refm = op.mech_action(x, d=d, mask=mask)
         assert _rel(ym, refm) < TOL
         assert bool((ym[mask.bool()] == 0).all())
+
+
+def _oracle_op(op):
+    from oracle import h8
+    C = [h8.isotropic_C(float(p.E), float(p.nu)) for p in op.phases]
+    drivers = np.array([0 if p.name == "pore" else 2 for p in op.phases])
+    return h8.VoxelOperator(op.shape, op.h, op.slot_np, np.stack([c[0] for c in C]), np.array([c[1] for c in C]),
+                            np.array([c[2] for c in C]), np.array([float(p.Gc) for p in op.phases]), drivers,
+                            op.ell, op.kappa, op.pinned_node, int(op.load.controlled), tuple(op.load.fixed_zero))
+
+
+def test_noalloc_matches_oracle_on_two_calls():
+    op = _cell((12, 10, 9))
+    ref = _oracle_op(op)
+    rng = np.random.default_rng(13)
+    for _ in range(2):  # two calls in a row, different inputs
+        x = rng.normal(size=op.n_mech) * 1e-3
+        d = rng.uniform(0, 1, size=op.n_red)
+        y = _noalloc(op, torch.as_tensor(x, device="cuda"), torch.as_tensor(d, device="cuda"))
+        want = ref.mech_action(x, ref.degradation(d))
+        assert float(np.linalg.norm(y.cpu().numpy() - want) / np.linalg.norm(want)) < TOL
 
 
 def test_noalloc_float32_matches_regular_entry_point():
