@@ -150,6 +150,8 @@ def import_reference():
     import importlib.machinery
     from unittest import mock
 
+    if "phast" in sys.modules:
+        return sys.modules["phast"]
     if not os.path.isdir(os.path.join(REF_DIR, "phast")):
         raise ImportError(f"the reference is not installed under {os.path.relpath(REF_DIR, ROOT)}")
 
@@ -235,6 +237,166 @@ def reference_sample_note(secs, recs, threads):
 
 
 PHAST_VERSION = "0.18.0"
+
+
+# ---------------------------------------------------------------------------
+# the 2D configurations: quasi-static SENT 200 x 200 (cfg0) and explicit crack
+# branching 400 x 160 (cfg2), each beside the reference's own CPU time
+# ---------------------------------------------------------------------------
+
+CFG0 = dict(nx=200, ny=200, width=1.0, height=1.0, crack_y=0.5, crack_x=0.5, bc=True,
+            mat=dict(E=210000.0, nu=0.3, Gc=2.7, l0=0.01, eta_residual=1e-8, energy_split="isotropic", rho=7.8e-9),
+            cfg=dict(solver_type="quasi_static", backend="cg", static_tol=1e-10, damage_tol=1e-10,
+                     bounds_method="projected_cg", use_multigrid=False, stagger_tol=1e-6, max_stagger=500))
+CFG2 = dict(nx=400, ny=160, width=100.0, height=40.0, crack_y=20.0, crack_x=50.0, bc=False,
+            mat=dict(E=32000.0, nu=0.2, Gc=3e-3, l0=0.5, rho=2.45e-9, eta_residual=1e-8, energy_split="spectral"),
+            cfg=dict(solver_type="explicit", dt_safety=0.5, damage_every=1, damage_tol=1e-10,
+                     bounds_method="projected_cg", use_multigrid=False))
+CFG0_STEPS, CFG2_STEPS, CFG2_REF_STEPS = 3, 200, 10
+
+
+def sent_problem(pkg, spec, device=None, dtype=None):
+    """The structured-Q4 SENT setup of ``spec`` built with package ``pkg`` (this one or the reference):
+    bottom fixed and top loaded (cfg0) or free edges with a +-1 MPa edge traction on f_ext (cfg2), the
+    crack as phase-field Dirichlet d = 1 on the node line."""
+    kw = {} if device is None else {"device": device}
+    if pkg.__name__ == "phast":
+        from phast.core.mesh import FEMMesh
+        from phast.core.quad_elements import structured_q4_mesh
+        from phast.physics.boundary_conditions import BoundaryConditions
+        from phast.physics.material import Material
+        from phast.solvers.staggered_solver import SolverConfig, StaggeredSolver
+    else:
+        FEMMesh, structured_q4_mesh, BoundaryConditions = pkg.FEMMesh, pkg.structured_q4_mesh, pkg.BoundaryConditions
+        Material, SolverConfig, StaggeredSolver = pkg.Material, pkg.SolverConfig, pkg.StaggeredSolver
+    sm = structured_q4_mesh(spec["width"], spec["height"], spec["nx"], spec["ny"])
+    mesh = FEMMesh.from_tensors(sm.nodes, sm.quads, element_type="Q4", **kw)
+    bcs = BoundaryConditions(mesh.n_nodes, **kw)
+    if spec["bc"]:
+        bcs.fix(sm.node_sets["bottom"], 0)
+        bcs.fix(sm.node_sets["bottom"], 1)
+        bcs.add(sm.node_sets["top"], 1, 1.0)
+    nodes = sm.nodes.cpu().numpy()
+    notch = np.nonzero((np.abs(nodes[:, 1] - spec["crack_y"]) < 1e-9 * spec["height"]) &
+                       (nodes[:, 0] < spec["crack_x"]))[0]
+    bcs.add_pf_dirichlet(torch.as_tensor(notch), 1.0)
+    cfg = dict(spec["cfg"])
+    if dtype is not None:
+        cfg["dtype"] = dtype
+    s = StaggeredSolver(mesh, Material(**spec["mat"]), bcs, SolverConfig(**cfg))
+    pf_mask, pf_vals = bcs.get_pf_dirichlet_mask_values()
+    s.d = torch.where(pf_mask, pf_vals.to(s.d.device), s.d)
+    if not spec["bc"]:
+        f_ext = np.zeros((mesh.n_nodes, 2))
+        hx = spec["width"] / spec["nx"]
+        for name, sign in (("top", 1.0), ("bottom", -1.0)):
+            ns = sm.node_sets[name].cpu().numpy()
+            ns = ns[np.argsort(nodes[ns, 0])]
+            w = np.full(len(ns), hx)
+            w[0] = w[-1] = hx / 2
+            f_ext[ns, 1] = sign * w
+        s.f_ext = torch.as_tensor(f_ext, dtype=s.u.dtype, device=s.u.device)
+    return s, sm, bcs
+
+
+def _time_2d(s, bcs, steps, load=None, flush=None):
+    """Device time of ``steps`` staggered steps (CUDA events per step); damage PCG iterations."""
+    ms, pf, stag = 0.0, 0, 0
+    for k in range(steps):
+        if load is not None:
+            bcs.load_factor = load(k + 1)
+        if flush is not None:
+            flush_l2(flush)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s.step_full()
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        pf += s.damage_solver.last_iter
+        stag += s._last_stagger_iter
+    return ms, pf, stag
+
+
+def _time_reference_2d(spec, steps, load=None):
+    import_reference()
+    import phast
+    torch.set_num_threads(os.cpu_count() or 1)
+    s, sm, bcs = sent_problem(phast, spec)
+    secs = []
+    for k in range(steps):
+        if load is not None:
+            bcs.load_factor = load(k + 1)
+        t0 = time.perf_counter()
+        s.step_full()
+        secs.append(time.perf_counter() - t0)
+    return secs, torch.get_num_threads()
+
+
+def run_2d_configs(device, flush, with_cpu):
+    """Bench lines of cfg0 and cfg2 (steps/s, DOF-updates/s, achieved GB/s of the algorithmic bytes)."""
+    import phast_b200 as pb
+    out = {}
+    peak, _ = peaks()
+    # cfg0: every load step is a full staggered solve (Newton-CG mechanics, projected-CG damage), FP64
+    load0 = lambda k: 0.007 * k / 100  # noqa: E731
+    s, sm, bcs = sent_problem(pb, CFG0, device=device)
+    _time_2d(s, bcs, 1, load0)  # warm-up step (workspaces), then the timed window from the start
+    s, sm, bcs = sent_problem(pb, CFG0, device=device)
+    ms, pf, stag = _time_2d(s, bcs, CFG0_STEPS, load0, flush)
+    N, E = s.fem.n_nodes, s.fem.n_elems
+    line = {"workload": "2D quasi-static SENT, Q4 200x200, isotropic split, CG and projected-CG tol 1e-10; "
+                        f"load steps 1..{CFG0_STEPS} of 100", "dtype": "f64",
+            "value": CFG0_STEPS / (ms / 1e3), "unit": "staggered steps/s", "ms_per_step": ms / CFG0_STEPS,
+            "stagger_iters_per_step": stag / CFG0_STEPS, "damage_pcg_iters_per_step": pf / CFG0_STEPS}
+    if with_cpu:
+        try:
+            secs, threads = _time_reference_2d(CFG0, 1, load0)
+            line["cpu_baseline"] = {"value": 1.0 / secs[0], "unit": "staggered steps/s", "cores": threads,
+                                    "kind": "reference",
+                                    "sample": f"PhAST {PHAST_VERSION} StaggeredSolver.step_full, load step 1 "
+                                              f"({secs[0]:.1f} s)"}
+        except ImportError as exc:
+            line["cpu_baseline"] = {"value": None, "sample": f"unavailable: {exc}"}
+    out["cfg0"] = line
+    # cfg2: explicit steps, FP32 fields and kernels (the configuration's form) beside plain FP64
+    res = {}
+    for name, dt in (("fp32", torch.float32), ("fp64", torch.float64)):
+        s, sm, bcs = sent_problem(pb, CFG2, device=device, dtype=dt)
+        _time_2d(s, bcs, 5)
+        s, sm, bcs = sent_problem(pb, CFG2, device=device, dtype=dt)
+        ms, pf, _ = _time_2d(s, bcs, CFG2_STEPS)
+        res[name] = (ms, pf, s)
+    (ms32, pf32, s32), (ms64, pf64, s64) = res["fp32"], res["fp64"]
+    N, E = s32.fem.n_nodes, s32.fem.n_elems
+    # explicit step (read u, v, a, f_ext, M^-1, d; write u, v, a; H read + write) and one projected-CG
+    # iteration of the damage solve (FP64) per damage PCG iteration
+    bytes32 = CFG2_STEPS * ((16 * N + 8 * E) * 4) + pf32 * (8 * N + 4 * E) * 8
+    bytes64 = CFG2_STEPS * ((16 * N + 8 * E) * 8) + pf64 * (8 * N + 4 * E) * 8
+    rel = lambda a, b: float(torch.linalg.vector_norm(a.double() - b.double()) / torch.linalg.vector_norm(b.double()))  # noqa: E731
+    line = {"workload": f"2D explicit crack branching, Q4 400x160, spectral split, damage solve every step; "
+                        f"steps 1..{CFG2_STEPS}", "dtype": "f32 fields/kernels, f64 damage solve",
+            "value": CFG2_STEPS / (ms32 / 1e3), "unit": "time steps/s", "ms_per_step": ms32 / CFG2_STEPS,
+            "dof_updates_per_s": (2 * N * CFG2_STEPS + N * pf32) / (ms32 / 1e3),
+            "achieved_GBps": bytes32 / (ms32 / 1e3) / 1e9, "hbm_frac": bytes32 / (ms32 / 1e3) / 1e9 / peak,
+            "l2": "working set (about 10 MB) is L2-resident",
+            "plain_fp64": {"value": CFG2_STEPS / (ms64 / 1e3), "ms_per_step": ms64 / CFG2_STEPS,
+                           "achieved_GBps": bytes64 / (ms64 / 1e3) / 1e9},
+            "speedup_vs_plain_fp64": ms64 / ms32,
+            "rel_err_fp32_vs_fp64": {"u": rel(s32.u, s64.u), "v": rel(s32.v, s64.v), "d": rel(s32.d, s64.d),
+                                     "crack_support_equal": bool(torch.equal(s32.d > 0.9, s64.d > 0.9))},
+            "damage_pcg_iters_per_step": pf32 / CFG2_STEPS}
+    if with_cpu:
+        try:
+            secs, threads = _time_reference_2d(CFG2, CFG2_REF_STEPS)
+            line["cpu_baseline"] = {"value": len(secs) / sum(secs), "unit": "time steps/s", "cores": threads,
+                                    "kind": "reference",
+                                    "sample": f"PhAST {PHAST_VERSION} StaggeredSolver.step_full (FP64), steps "
+                                              f"1..{len(secs)} ({sum(secs):.1f} s)"}
+        except ImportError as exc:
+            line["cpu_baseline"] = {"value": None, "sample": f"unavailable: {exc}"}
+    out["cfg2"] = line
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -405,6 +567,8 @@ def run_ours(args, rank, world, device):
         "iterations_per_step": {"mech": mech, "pf": pf, "stagger": stag},
         "dof_updates_per_s": dof_updates,
     }
+    if not args.no_2d:
+        out["configs"] = run_2d_configs(device, flush, world == 1 and rank == 0 and not args.no_cpu)
     if world == 1 and rank == 0 and not args.no_cpu:
         try:
             secs, threads, recs = time_reference(args.steps, CPU_BASELINE_BUDGET_S)
@@ -536,6 +700,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-2d", action="store_true", help="skip the 2D configuration lines (cfg0, cfg2)")
     ap.add_argument("--form", default="mixed-gmg", choices=["plain", "gmg", "mixed", "mixed-gmg"],
                     help="mechanics form of the timed value (the plain FP64 form is timed beside it)")
     ap.add_argument("--kernel-only", action="store_true", help="time the elastic action alone (profiling case)")

@@ -45,10 +45,15 @@ class ExplicitDynamics:
         """One step written into caller buffers; optionally fuses H_out = max(H_in, psi+(u_new))."""
         fem = self.fem
         dt = u.dtype
-        mask = bc_mask if bc_mask.dtype == torch.uint8 else bc_mask.to(torch.uint8)
+        # converted copies are held in locals until the launch is enqueued: a temporary whose
+        # last reference dies inside the argument list goes back to the caching allocator,
+        # which may hand its block to the next conversion before the kernel reads it
+        mask = (bc_mask if bc_mask.dtype == torch.uint8 else bc_mask.to(torch.uint8)).contiguous()
+        d_k = d.to(dt).contiguous()
+        f_k = f_ext.to(dt).contiguous()
+        vals_k = bc_vals.to(dt).contiguous()
         call("phastb_q4_explicit_step", fem.grid, fem.mat(dt), _dtype_code(u), float(self.dt), ptr(self._m_inv(dt)),
-             ptr(u), ptr(v), ptr(a), ptr(d.to(dt).contiguous()), ptr(f_ext.to(dt).contiguous()),
-             ptr(mask.contiguous()), ptr(bc_vals.to(dt).contiguous()), ptr(u_out), ptr(v_out), ptr(a_out),
+             ptr(u), ptr(v), ptr(a), ptr(d_k), ptr(f_k), ptr(mask), ptr(vals_k), ptr(u_out), ptr(v_out), ptr(a_out),
              ptr(H_in), ptr(H_out), stream())
 
     def step(self, u, v, a, d, f_ext, bc_mask, bc_vals, rigid_connectors=None):

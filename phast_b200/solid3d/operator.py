@@ -83,6 +83,8 @@ class PeriodicVoxelPhaseFieldOperator:
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise ValueError("the B200 backend needs a CUDA device")
+        if self.device.index is None:  # tensors made on "cuda" report the current device's index
+            self.device = torch.device("cuda", torch.cuda.current_device())
         self.dtype = torch.float64
         nx, ny, nz = (int(v) for v in grid.shape)
         hx, hy, hz = (float(v) for v in grid.h)

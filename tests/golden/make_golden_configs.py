@@ -10,10 +10,12 @@ reference's own solver classes on the full-size seeded inputs of one
 configuration for a short window and stores the fields at the end of the
 window plus per-step scalars:
 
-* ``cfg0_sent200.npz``: 2D quasi-static single-edge-notched tension, structured
-  Q4 200 x 200, isotropic split, CG tol 1e-10, projected-CG tol 1e-10; load
+* ``cfg0_sent200.npz`` / ``cfg0_sent200_tight.npz``: 2D quasi-static
+  single-edge-notched tension, structured Q4 200 x 200, isotropic split; load
   steps 1-3 of the 100-step ramp to 0.007 mm
-  (``phast.solvers.staggered_solver.StaggeredSolver.step_full``).
+  (``phast.solvers.staggered_solver.StaggeredSolver.step_full``), once with the
+  configuration's CG and projected-CG tolerances of 1e-10 and once with both at
+  1e-12.
 * ``cfg1_pore64.npz`` / ``cfg1_pore64_tight.npz``: 3D periodic 64^3 pore cell,
   AT2 spectral, eps_zz ramp to 0.02 in 50 increments; increments 1-3
   (``phast.solid3d.staggered.StaggeredSolver.advance``), once at PhAST's
@@ -71,10 +73,11 @@ def _sent_q4(nx, ny, width, height, mat_kwargs, cfg_kwargs, crack_y, crack_x_max
     return s, sm, bcs, notch, top, bot
 
 
-def cfg0():
+def _cfg0(tight):
     """200 x 200 SENT, load steps 1-3 of 100 (top uy = 0.007 k / 100)."""
     mat = dict(E=210000.0, nu=0.3, Gc=2.7, l0=0.01, eta_residual=1e-8, energy_split="isotropic", rho=7.8e-9)
-    cfg = dict(solver_type="quasi_static", backend="cg", static_tol=1e-10, damage_tol=1e-10,
+    tol = 1e-12 if tight else 1e-10
+    cfg = dict(solver_type="quasi_static", backend="cg", static_tol=tol, damage_tol=tol,
                bounds_method="projected_cg", use_multigrid=False, stagger_tol=1e-6, max_stagger=500)
     s, sm, bcs, notch, top, bot = _sent_q4(200, 200, 1.0, 1.0, mat, cfg, 0.5, 0.5, True)
     out = {"nx": 200, "ny": 200, "notch": notch, "steps": np.arange(1, 4)}
@@ -90,8 +93,16 @@ def cfg0():
         stag.append(s._last_stagger_iter)
         print(f"cfg0 step {k}: {secs[-1]:.1f} s, stagger {stag[-1]}, reaction {rf[-1]:.9e}", flush=True)
     out.update(u=np.stack(us), d=np.stack(ds), H=n(s.H_elem), rf=np.array(rf), stag=np.array(stag),
-               ref_seconds=np.array(secs))
-    np.savez_compressed(os.path.join(HERE, "cfg0_sent200.npz"), **out)
+               ref_seconds=np.array(secs), tol=np.array([tol]))
+    np.savez_compressed(os.path.join(HERE, "cfg0_sent200_tight.npz" if tight else "cfg0_sent200.npz"), **out)
+
+
+def cfg0():
+    _cfg0(False)
+
+
+def cfg0_tight():
+    _cfg0(True)
 
 
 def _cfg1(tight):
@@ -175,7 +186,7 @@ def cfg2():
     np.savez_compressed(os.path.join(HERE, "cfg2_branch400.npz"), **out)
 
 
-CASES = {"cfg0": cfg0, "cfg1": cfg1, "cfg1_tight": cfg1_tight, "cfg2": cfg2}
+CASES = {"cfg0": cfg0, "cfg0_tight": cfg0_tight, "cfg1": cfg1, "cfg1_tight": cfg1_tight, "cfg2": cfg2}
 
 if __name__ == "__main__":
     if len(sys.argv) < 2:

@@ -112,10 +112,15 @@ def _sent(nx, ny, width, height, mat_kw, cfg_kw, crack_y, crack_x, bc):
     return s, sm, bcs, notch
 
 
-def test_cfg0_sent200_plain_fp64():
-    g = golden("cfg0_sent200")
+@pytest.mark.parametrize("tight", [False, True])
+def test_cfg0_sent200_plain_fp64(tight):
+    """At the configuration's tolerances (mechanics CG and damage projected CG at 1e-10) the
+    fields agree to the size of that tolerance; with both sides at 1e-12 they agree to 1e-10."""
+    g = golden("cfg0_sent200_tight" if tight else "cfg0_sent200")
+    tol = float(g["tol"][0]) if "tol" in g else 1e-10
+    field_tol = 1e-10 if tight else 1e-9
     mat = dict(E=210000.0, nu=0.3, Gc=2.7, l0=0.01, eta_residual=1e-8, energy_split="isotropic", rho=7.8e-9)
-    cfg = dict(solver_type="quasi_static", backend="cg", static_tol=1e-10, damage_tol=1e-10,
+    cfg = dict(solver_type="quasi_static", backend="cg", static_tol=tol, damage_tol=tol,
                bounds_method="projected_cg", use_multigrid=False, stagger_tol=1e-6, max_stagger=500)
     s, sm, bcs, notch = _sent(200, 200, 1.0, 1.0, mat, cfg, 0.5, 0.5, True)
     assert np.array_equal(notch, g["notch"])
@@ -125,11 +130,12 @@ def test_cfg0_sent200_plain_fp64():
         assert s._last_stagger_iter == int(g["stag"][k])
         eu, ed = rel(s.u.cpu(), g["u"][k]), rel(s.d.cpu(), g["d"][k])
         rf = s.fem.compute_reaction_force(s.u, s.d, sm.node_sets["top"], component=1)
-        print(f"cfg0 step {k + 1}: rel-L2 u {eu:.3e}, d {ed:.3e}, reaction {abs(rf - g['rf'][k]) / abs(g['rf'][k]):.3e}")
-        assert eu < 1e-10 and ed < 1e-10
+        print(f"cfg0 (tol {tol:g}) step {k + 1}: rel-L2 u {eu:.3e}, d {ed:.3e}, "
+              f"reaction {abs(rf - g['rf'][k]) / abs(g['rf'][k]):.3e}")
+        assert eu < field_tol and ed < field_tol
         assert abs(rf - g["rf"][k]) <= 1e-8 * abs(g["rf"][k])
         assert np.array_equal(s.d.cpu().numpy() > 0.9, g["d"][k] > 0.9)
-    assert rel(s.H_elem.cpu(), g["H"]) < 1e-10
+    assert rel(s.H_elem.cpu(), g["H"]) < field_tol
 
 
 def _branch(dtype):

@@ -162,3 +162,29 @@ def test_q4_staggered_explicit_golden():
         assert rel(s.d.cpu(), g["ex_d"][k]) < 1e-10
         assert rel(s.H_elem.cpu(), g["ex_H"][k]) < 1e-10
     assert rel(s.v.cpu(), g["ex_v"]) < 1e-10 and rel(s.a.cpu(), g["ex_a"]) < 1e-10
+
+
+def test_fp32_explicit_rollout_is_reproducible():
+    """The FP32 explicit step converts d, f_ext and the BC values to FP32 before its launch; two
+    rollouts from the same state must give the same bits (a conversion freed before the kernel
+    read it once let the allocator hand its block to the next conversion)."""
+    g = golden("q4_staggered")
+    runs = []
+    for _ in range(2):
+        import phast_b200 as pb
+        nx = int(g["nx"])
+        sm = pb.structured_q4_mesh(1.0, 1.0, nx, nx)
+        mesh = pb.FEMMesh.from_tensors(sm.nodes, sm.quads, element_type="Q4", device="cuda")
+        bcs = pb.BoundaryConditions(mesh.n_nodes, device="cuda")
+        bcs.add_pf_dirichlet(torch.as_tensor(g["notch"]), 1.0)
+        mat = pb.Material(E=32000.0, nu=0.2, Gc=3e-3, l0=0.15, rho=2.45e-9, eta_residual=1e-8,
+                          energy_split="spectral")
+        cfg = pb.SolverConfig(solver_type="explicit", dt_safety=0.5, damage_every=1, damage_tol=1e-10,
+                              bounds_method="projected_cg", use_multigrid=False, dtype=torch.float32)
+        s = pb.StaggeredSolver(mesh, mat, bcs, cfg)
+        s._apply_pf_dirichlet()
+        s.f_ext = torch.as_tensor(g["ex_f_ext"]).cuda().float()
+        for _ in range(30):
+            s.step_full()
+        runs.append((s.u.clone(), s.d.clone()))
+    assert torch.equal(runs[0][0], runs[1][0]) and torch.equal(runs[0][1], runs[1][1])
