@@ -430,6 +430,21 @@ int phastb_h8_damage_residual_norm(const phastb_voxel_grid* g, const phastb_voxe
 int phastb_scale_set(int n, const double* x, double factor, int index, double value, double* out,
                      void* stream);
 
+/* 1 when the elastic action on this grid and word size stages its node layers with TMA tensor
+ * copies (rx a multiple of 16 bytes' worth of words, the driver's tensor-map encoder present,
+ * PHASTB_TMA not 0), 0 when it stages them through registers, -1 on bad arguments.  No reference
+ * counterpart: it reports how this backend's kernel loads the operator's halo tiles. */
+int phastb_h8_tma_staging(const phastb_voxel_grid* g, int dtype);
+
+/* Self-test of the bounded grid barrier that the persistent damage CG uses (no counterpart in
+ * the reference).  A cooperative launch of `blocks` blocks passes two barriers; block
+ * `skip_block` (< 0: none) never arrives, so the other blocks' first wait runs out after
+ * limit_s seconds (at most 10) of GPU time and the kernel ends with the error flag set.
+ * Returns PHASTB_ERR_CUDA with *grid_error_host = 1 in that case, PHASTB_OK with 0 otherwise;
+ * *passed_host counts the blocks that passed both barriers. */
+int phastb_test_grid_barrier(int blocks, int skip_block, double limit_s, int* grid_error_host,
+                             int* passed_host);
+
 /* Library version string (host pointer). */
 const char* phastb_version(void);
 

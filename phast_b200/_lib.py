@@ -124,6 +124,8 @@ SIGNATURES = {
     "phastb_h8_damage_residual_workspace_bytes": (sz, [VG]),
     "phastb_h8_damage_residual_norm": (C.c_int, [VG, VM, vp, vp, C.c_double, vp, dp, vp, sz, vp]),
     "phastb_scale_set": (C.c_int, [C.c_int, vp, C.c_double, C.c_int, C.c_double, vp, vp]),
+    "phastb_test_grid_barrier": (C.c_int, [C.c_int, C.c_int, C.c_double, ip, ip]),
+    "phastb_h8_tma_staging": (C.c_int, [VG, C.c_int]),
 }
 RECORD_WORDS = 27
 

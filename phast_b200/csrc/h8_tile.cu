@@ -1,5 +1,7 @@
 // Tiled z-marching voxel H8 elastic action (see h8_tile.cuh).
 #include "h8_tile.cuh"
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include "engine.cuh"
 
 #include <cstdlib>
@@ -48,6 +50,58 @@ __device__ __forceinline__ void cp_async_word(T* smem, const T* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(sizeof(T)) : "memory");
 }
 __device__ __forceinline__ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// ---- TMA staging of node layers (cp.async.bulk.tensor, completion on an mbarrier)
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Orders this thread's earlier generic-proxy accesses of shared memory (reads of
+// a buffer, stores of patched halo values) before async-proxy (TMA) writes.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// 3D tiled copy global -> this CTA's shared memory (no multicast); the innermost
+// coordinate c0 times the element size must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+          "r"(smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+// A TMA completion wait gives up after kTmaLimitNs of global time (a normal wait
+// is well under a microsecond); the caller then marks its output non-finite.
+constexpr unsigned long long kTmaLimitNs = 1000000000ull;
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  const unsigned long long t0 = global_ns();
+  for (unsigned i = 0; i < (1u << 26); ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63u) == 63u && global_ns() - t0 > kTmaLimitNs) return false;
+  }
+  return false;
+}
+__device__ __forceinline__ int floor_mult(int v, int m) { return (v >= 0 ? v / m : -((-v + m - 1) / m)) * m; }
 
 // Staged per-element arrays live chunk-major in shared memory: chunk c (16
 // bytes) of the element owned by thread t sits at base + (c * n + t) * 16, so a
@@ -223,9 +277,15 @@ __device__ __forceinline__ T g_deg(T kappa, T d) {
 // per-Gauss-point moduli of a multigrid coarse level); MODE selects the node
 // epilogue: y = A x, y plus x . y, y plus the energy, or one Chebyshev
 // smoothing step on (res, d, x) driven by A d.
-template <typename T, int COEF, int MODE, int OX, int OY>
+// TMA: the node layers are staged by tensor-map copies (tmx: u~ as a (3 rx,
+// ry, rz) array, tmd: d as (rx, ry, rz)) issued by one thread and completed on an
+// mbarrier per layer buffer; halo nodes that wrap around a periodic edge read
+// the zero fill and are patched by per-thread loads.  Otherwise every thread
+// stages its (at most two) halo-tile nodes through registers.
+template <typename T, int COEF, int MODE, int OX, int OY, bool TMA>
 __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
-    h8_tile_kernel(TileArgs<T> a, VoxMat<T> m) {
+    h8_tile_kernel(TileArgs<T> a, VoxMat<T> m, const __grid_constant__ CUtensorMap tmx,
+                   const __grid_constant__ CUtensorMap tmd) {
   if (a.guard && *a.guard == 0) return;
   constexpr bool SLOT = COEF != kCoefQP;
   constexpr bool DOT = MODE == kModeDot, ENERGY = MODE == kModeEnergy, CHEB = MODE == kModeCheb;
@@ -243,19 +303,43 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
   const int ox = OX ? OX : a.ts.ox, oy = OY ? OY : a.ts.oy, kz = a.ts.kz;
   const int ex = ox + 1, exy = ex * (oy + 1);
   const int ntx = ox + 2, nt = ntx * (oy + 2);
-  T* nb = reinterpret_cast<T*>(smem_raw);  // [3 buffers][4 fields][nt]
-  T* FL = nb + 12 * nt;                    // [4 corners][3 comps][exy], lower face (oz = 0)
-  T* FU = FL + 12 * exy;                   // upper face (oz = 1)
+  // TMA: shared memory from a 128-byte boundary; u~ layer buffers of W words per
+  // halo row, d layer buffers of Wd words, each started from a 16-byte aligned column
+  unsigned char* sbase =
+      TMA ? reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127))
+          : smem_raw;
+  const int W = tma_wx<T>(ox), Wd = tma_wd<T>(ox);
+  const size_t xbb = tma_xbytes<T>(ox, oy), dbb = tma_dbytes<T>(ox, oy);
+  T* nb = reinterpret_cast<T*>(sbase);  // [3 buffers][4 fields][nt] (without TMA)
+  size_t off_face = 0, off_qp = 0, off_cheb = 0;
+  if (TMA) {
+    tile_layout_tma<T>(ox, oy, COEF == kCoefQP, CHEB, &off_face, &off_qp, &off_cheb);
+  } else {
+    tile_layout<T>(ox, oy, COEF == kCoefQP, CHEB, &off_qp, &off_cheb);
+    off_face = sizeof(T) * 12 * (size_t)nt;
+  }
+  T* FL = reinterpret_cast<T*>(sbase + off_face);  // [4 corners][3 comps][exy], lower face (oz = 0)
+  T* FU = FL + 12 * exy;                           // upper face (oz = 1)
   // staged by cp.async, two buffers each: kCoefQP (lam_q, mu_q) of this thread's
   // element one element layer ahead, chunk-major [2][chunks][exy]; kModeCheb
   // (res, invd, xs) of this thread's owned node, [2][9][ox*oy], copied while the
   // layer's elements are computed
   constexpr bool STAGE = COEF == kCoefQP || CHEB;
   constexpr int kQChunks = kStageQP * (int)sizeof(T) / 16;
-  size_t off_qp = 0, off_cheb = 0;
-  tile_layout<T>(ox, oy, COEF == kCoefQP, CHEB, &off_qp, &off_cheb);
-  unsigned char* QS = smem_raw + off_qp;
-  T* CS = reinterpret_cast<T*>(smem_raw + off_cheb);
+  unsigned char* QS = sbase + off_qp;
+  T* CS = reinterpret_cast<T*>(sbase + off_cheb);
+  __shared__ __align__(8) unsigned long long s_mbar[3];
+  unsigned mphase = 0;  // bit b: parity of the next completion of buffer b's barrier
+  bool tma_fault = false;
+  const bool use_d = SLOT && d != nullptr && a.gq == nullptr;
+  const unsigned tma_tx = (unsigned)(sizeof(T) * (size_t)W * (oy + 2) + (use_d ? sizeof(T) * (size_t)Wd * (oy + 2) : 0));
+  if (TMA) {
+    if (threadIdx.x == 0) {
+      for (int b = 0; b < 3; ++b) mbar_init(&s_mbar[b], 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+  }
   const int oxy = ox * oy;
   const bool q_async = COEF == kCoefQP && aligned16(a.lam_q) && aligned16(a.mu_q);
   const int tid = threadIdx.x;
@@ -274,6 +358,76 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
   const int ea = tid % ex, eb = tid / ex;
   const int ni = tid % ox, nj = tid / ox;
   const bool is_elem = tid < exy, is_node = tid < ox * oy;
+  constexpr int kA = 16 / (int)sizeof(T);  // words per 16 bytes
+  int xr = 0, dr = 0, xs0 = 0, ds0 = 0;    // TMA: row start columns and remainders of the current tile
+  // node value of component c (3: d) at halo-tile position (row, col) of layer buffer `buf`
+  auto nval = [&](int buf, int c, int row, int col) -> T {
+    if constexpr (TMA) {
+      if (c < 3) return reinterpret_cast<const T*>(sbase + (size_t)buf * xbb)[row * W + xr + 3 * col + c];
+      return reinterpret_cast<const T*>(sbase + 3 * xbb + (size_t)buf * dbb)[row * Wd + dr + col];
+    } else {
+      return nb[4 * nt * buf + c * nt + row * ntx + col];
+    }
+  };
+  // TMA: thread 0 issues the copies of node layer kn into buffer b
+  auto tma_issue = [&](int i0, int j0, int kn, int b) {
+    if constexpr (TMA) {
+      if (threadIdx.x == 0) {
+        const int gz = g.pz ? wrap_node(kn, g.nz, g.rz, 1) : kn;  // out of range: the zero fill
+        fence_proxy_async();
+        mbar_expect_tx(&s_mbar[b], tma_tx);
+        tma_load_3d(sbase + (size_t)b * xbb, &tmx, xs0, j0 - 1, gz, &s_mbar[b]);
+        if (use_d) tma_load_3d(sbase + 3 * xbb + (size_t)b * dbb, &tmd, ds0, j0 - 1, gz, &s_mbar[b]);
+      }
+    }
+  };
+  // TMA: halo nodes of layer kn that wrap around a periodic edge (the copy read the zero fill there)
+  auto wrap_load = [&](int i0, int j0, int kn, Staged<T>& r, unsigned& on) {
+    on = 0;
+    if constexpr (TMA) {
+      const int gk = wrap_node(kn, g.nz, g.rz, g.pz);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int t = threadIdx.x + h * blockDim.x;
+        if (t < nt && gk >= 0) {
+          const int ri = i0 - 1 + t % ntx, rj = j0 - 1 + t / ntx;
+          const bool wx = g.px && (ri < 0 || ri >= g.rx), wy = g.py && (rj < 0 || rj >= g.ry);
+          if (wx || wy) {
+            const int gi = wrap_node(ri, g.nx, g.rx, g.px), gj = wrap_node(rj, g.ny, g.ry, g.py);
+            if (gi >= 0 && gj >= 0) {
+              const size_t n = (size_t)gi + (size_t)g.rx * ((size_t)gj + (size_t)g.ry * gk);
+              r.v[h][0] = __ldg(x + 3 * n);
+              r.v[h][1] = __ldg(x + 3 * n + 1);
+              r.v[h][2] = __ldg(x + 3 * n + 2);
+              r.v[h][3] = use_d ? __ldg(d + n) : T(0);
+              on |= 1u << h;
+            }
+          }
+        }
+      }
+    }
+  };
+  auto wrap_store = [&](const Staged<T>& r, unsigned on, int b) {
+    if constexpr (TMA) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (on & (1u << h)) {
+          const int t = threadIdx.x + h * blockDim.x, col = t % ntx, row = t / ntx;
+          T* xbuf = reinterpret_cast<T*>(sbase + (size_t)b * xbb);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) xbuf[row * W + xr + 3 * col + c] = r.v[h][c];
+          if (use_d) reinterpret_cast<T*>(sbase + 3 * xbb + (size_t)b * dbb)[row * Wd + dr + col] = r.v[h][3];
+        }
+      }
+    }
+  };
+  // TMA: waits (bounded) for buffer b's copies of its current fill
+  auto tma_wait = [&](int b) {
+    if constexpr (TMA) {
+      if (!mbar_wait(&s_mbar[b], (mphase >> b) & 1u)) tma_fault = true;
+      mphase ^= 1u << b;
+    }
+  };
   double accd[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   // material slot of this thread's element in layer ke (0 outside the grid)
   auto elem_slot = [&](int i0, int j0, int ke) -> int {
@@ -338,22 +492,45 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
     T tacc[8] = {T(0), T(0), T(0), T(0), T(0), T(0), T(0), T(0)};
     T pend[3] = {T(0), T(0), T(0)};
     Staged<T> pf;
-    stage_load(g, x, d, i0, j0, k0 - 1, ntx, nt, pf);
-    __syncthreads();  // the previous tile's last node phase is done with the buffers
-    stage_store(nt, pf, nb);
-    stage_load(g, x, d, i0, j0, k0, ntx, nt, pf);
+    unsigned pf_on = 0;
+    if constexpr (TMA) {
+      xs0 = floor_mult(3 * (i0 - 1), kA);
+      xr = 3 * (i0 - 1) - xs0;
+      ds0 = floor_mult(i0 - 1, kA);
+      dr = (i0 - 1) - ds0;
+      fence_proxy_async();
+      __syncthreads();  // the previous tile's last node phase is done with the buffers
+      tma_issue(i0, j0, k0 - 1, 0);
+      tma_issue(i0, j0, k0, 1);
+      wrap_load(i0, j0, k0 - 1, pf, pf_on);
+      tma_wait(0);
+      wrap_store(pf, pf_on, 0);
+      wrap_load(i0, j0, k0, pf, pf_on);
+    } else {
+      stage_load(g, x, d, i0, j0, k0 - 1, ntx, nt, pf);
+      __syncthreads();  // the previous tile's last node phase is done with the buffers
+      stage_store(nt, pf, nb);
+      stage_load(g, x, d, i0, j0, k0, ntx, nt, pf);
+    }
     int sl_next = elem_slot(i0, j0, k0 - 1);
     stage_qp(i0, j0, k0 - 1, 0, true);
     int mk_next = node_mask(i0, j0, k0), mk_cur = 0;
     const int K = k1 - k0;
     for (int kk = 0; kk <= K; ++kk) {
       const int ke = k0 - 1 + kk;  // element layer of this step
-      T* b0 = nb + 4 * nt * (kk % 3);
-      T* b1 = nb + 4 * nt * ((kk + 1) % 3);
-      stage_store(nt, pf, b1);  // node layer ke + 1
+      const int ib0 = kk % 3, ib1 = (kk + 1) % 3;
+      if constexpr (TMA) {
+        tma_wait(ib1);  // node layer ke + 1
+        wrap_store(pf, pf_on, ib1);
+      } else {
+        stage_store(nt, pf, nb + 4 * nt * ib1);  // node layer ke + 1
+      }
       const int sl = sl_next;
       if (kk < K) {
-        stage_load(g, x, d, i0, j0, ke + 2, ntx, nt, pf);
+        if constexpr (TMA)
+          wrap_load(i0, j0, ke + 2, pf, pf_on);
+        else
+          stage_load(g, x, d, i0, j0, ke + 2, ntx, nt, pf);
         sl_next = elem_slot(i0, j0, ke + 1);
       }
       if constexpr (STAGE) {
@@ -365,7 +542,10 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
         mk_cur = mk_next;
         if (kk < K) mk_next = node_mask(i0, j0, ke + 1);
       }
+      if constexpr (TMA) fence_proxy_async();  // this thread's reads and patches before the next copies
       __syncthreads();
+      // every thread is done with buffer (kk + 2) % 3 (node layer ke - 1): refill it with layer ke + 2
+      if (kk < K) tma_issue(i0, j0, ke + 2, (kk + 2) % 3);
       // ---- element phase: one element of the (ox+1) x (oy+1) tile per thread
       if (is_elem) {
         const int gi = wrap_elem(i0 - 1 + ea, g.nx, g.px);
@@ -383,10 +563,7 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
             } else if (d) {
               T dd[8], dq[8];
 #pragma unroll
-              for (int L = 0; L < 8; ++L) {
-                const T* bb = (L & 4) ? b1 : b0;
-                dd[L] = bb[3 * nt + (eb + ((L >> 1) & 1)) * ntx + ea + (L & 1)];
-              }
+              for (int L = 0; L < 8; ++L) dd[L] = nval((L & 4) ? ib1 : ib0, 3, eb + ((L >> 1) & 1), ea + (L & 1));
               interp_sf(dd, dq);
 #pragma unroll
               for (int q = 0; q < 8; ++q) gv[q] = g_deg(m.kappa, dq[q]);
@@ -400,10 +577,7 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
           for (int c = 0; c < 3; ++c) {
             T u[8];
 #pragma unroll
-            for (int L = 0; L < 8; ++L) {
-              const T* bb = (L & 4) ? b1 : b0;
-              u[L] = bb[c * nt + (eb + ((L >> 1) & 1)) * ntx + ea + (L & 1)];
-            }
+            for (int L = 0; L < 8; ++L) u[L] = nval((L & 4) ? ib1 : ib0, c, eb + ((L >> 1) & 1), ea + (L & 1));
             grad_k(u, a.k, D[c][0], D[c][1], D[c][2]);
           }
           if (EROWS) {
@@ -546,7 +720,7 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
             T v = pend[c] + lo[c];
             if (mk_cur & (1 << c)) v = T(0);
             const size_t i = 3 * n + c;
-            const T xin = b0[c * nt + (nj + 1) * ntx + ni + 1];
+            const T xin = nval(ib0, c, nj + 1, ni + 1);
             if (CHEB) {
               const T* cs = CS + (size_t)(kk & 1) * 9 * oxy + tid;
               const T r = cs[c * oxy] - v;
@@ -568,6 +742,15 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
 #pragma unroll
       for (int k = 0; k < 8; ++k) accd[k] += double(tacc[k]);
     }
+  }
+  if (TMA && tma_fault) {
+    // a layer copy did not complete in time: the result is unusable, so make it non-finite
+    // (every solver reports PHASTB_NONFINITE for it) instead of returning wrong numbers
+    const T bad = T(NAN);
+    if (a.y) a.y[0] = bad;
+    if (CHEB && a.res) a.res[0] = bad;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) accd[k] = NAN;
   }
 
   if constexpr (RED) {
@@ -815,16 +998,20 @@ __global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_kernel(DTileArgs<
 
 // ------------------------------------------------------- persistent damage PCG
 
-// Polls of one grid-barrier wait before it gives up (each poll sleeps ~64 ns,
-// so about two seconds; a normal wait is a few microseconds).
-constexpr unsigned kBarSpins = 1u << 25;
+// A grid-barrier wait gives up after kBarLimitNs of the GPU's global timer (a
+// normal wait is a few microseconds); kBarSpins polls of ~64 ns sleep bound it
+// a second time, should the timer not advance.
+constexpr unsigned long long kBarLimitNs = 2000000000ull;
+constexpr unsigned kBarSpins = 1u << 26;
 
 // Grid-wide barrier of a cooperative launch (every block resident).  The last
 // block to arrive resets the count and advances the generation; the others
-// poll the generation.  A wait that runs out sets st->grid_error, and every
-// block that sees the error leaves the barrier with false, so the kernel ends
-// instead of hanging.  gen: this block's copy of the generation (thread 0).
-__device__ __forceinline__ bool grid_barrier(PcgState* st, unsigned& gen) {
+// poll the generation.  A wait that runs out (limit_ns of global time) sets
+// st->grid_error, and every block that sees the error leaves the barrier with
+// false, so the kernel ends instead of hanging.  gen: this block's copy of the
+// generation (thread 0).
+__device__ __forceinline__ bool grid_barrier(PcgState* st, unsigned& gen,
+                                             unsigned long long limit_ns = kBarLimitNs) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -836,9 +1023,11 @@ __device__ __forceinline__ bool grid_barrier(PcgState* st, unsigned& gen) {
       __threadfence();
       atomicAdd(&st->bar_gen, 1u);
     } else {
+      const unsigned long long t0 = global_ns();
       unsigned spins = 0;
       while (*reinterpret_cast<volatile unsigned*>(&st->bar_gen) == g0) {
-        if (++spins > kBarSpins || *reinterpret_cast<volatile int*>(&st->grid_error)) {
+        if (++spins > kBarSpins || global_ns() - t0 > limit_ns ||
+            *reinterpret_cast<volatile int*>(&st->grid_error)) {
           atomicExch(&st->grid_error, 1);
           ok = 0;
           break;
@@ -852,6 +1041,17 @@ __device__ __forceinline__ bool grid_barrier(PcgState* st, unsigned& gen) {
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+// Self-test of the barrier's bounded wait: every block but `skip` arrives twice;
+// with skip >= 0 the first wait of the others runs out after limit_ns and the
+// kernel ends with st->grid_error set.
+__global__ void grid_barrier_test_kernel(PcgState* st, int skip, unsigned long long limit_ns, int* passed) {
+  if ((int)blockIdx.x == skip) return;
+  unsigned gen = 0;
+  if (!grid_barrier(st, gen, limit_ns)) return;
+  if (!grid_barrier(st, gen, limit_ns)) return;
+  if (threadIdx.x == 0) atomicAdd(passed, 1);
 }
 
 template <typename T>
@@ -1013,11 +1213,77 @@ int launch_kz(long long tiles_xy, int rz, long long capacity) {
   return best;
 }
 
-template <typename T, int COEF, int MODE, int OX, int OY>
-int launch_variant(const TileArgs<T>& a, const VoxMat<T>& m, cudaStream_t s) {
-  auto kern = h8_tile_kernel<T, COEF, MODE, OX, OY>;
-  size_t off_qp = 0, off_cheb = 0;
-  const size_t smem = tile_layout<T>(a.ts.ox, a.ts.oy, COEF == kCoefQP, MODE == kModeCheb, &off_qp, &off_cheb);
+// TMA staging of the elastic action's node layers (PHASTB_TMA=1 turns it on).
+bool tma_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("PHASTB_TMA");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// Tensor maps of u~ (a (3 rx, ry, rz) array) and d ((rx, ry, rz)) for the TMA
+// staging of a launch; false (stage through registers instead) when TMA is off,
+// the row strides are not multiples of 16 bytes (rx a multiple of 16 / sizeof(T)),
+// a buffer is not 16-byte aligned, or the driver refuses a map.
+template <typename T>
+bool tile_tensor_maps(const TileArgs<T>& a, CUtensorMap* mx, CUtensorMap* md) {
+  std::memset(mx, 0, sizeof(*mx));
+  std::memset(md, 0, sizeof(*md));
+  if (!tma_enabled()) return false;
+  const VoxGeom& v = a.g;
+  const int A = 16 / (int)sizeof(T);
+  if (v.rx % A != 0) return false;
+  if ((reinterpret_cast<uintptr_t>(a.x) & 15u) || (a.d && (reinterpret_cast<uintptr_t>(a.d) & 15u))) return false;
+  const int W = tma_wx<T>(a.ts.ox), Wd = tma_wd<T>(a.ts.ox), rows = a.ts.oy + 2;
+  if (W > 256 || Wd > 256 || rows > 256) return false;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  const cuuint32_t es[3] = {1, 1, 1};
+  {
+    const cuuint64_t dims[3] = {3ull * (cuuint64_t)v.rx, (cuuint64_t)v.ry, (cuuint64_t)v.rz};
+    const cuuint64_t strides[2] = {3ull * v.rx * sizeof(T), 3ull * v.rx * v.ry * sizeof(T)};
+    const cuuint32_t box[3] = {(cuuint32_t)W, (cuuint32_t)rows, 1};
+    if (enc(mx, dt, 3, const_cast<T*>(a.x), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  if (a.d) {
+    const cuuint64_t dims[3] = {(cuuint64_t)v.rx, (cuuint64_t)v.ry, (cuuint64_t)v.rz};
+    const cuuint64_t strides[2] = {(cuuint64_t)v.rx * sizeof(T), (cuuint64_t)v.rx * v.ry * sizeof(T)};
+    const cuuint32_t box[3] = {(cuuint32_t)Wd, (cuuint32_t)rows, 1};
+    if (enc(md, dt, 3, const_cast<T*>(a.d), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  return true;
+}
+
+template <typename T, int COEF, int MODE, int OX, int OY, bool TMA>
+int launch_variant_t(const TileArgs<T>& a, const VoxMat<T>& m, cudaStream_t s, const CUtensorMap& mx,
+                     const CUtensorMap& md) {
+  auto kern = h8_tile_kernel<T, COEF, MODE, OX, OY, TMA>;
+  size_t off_face = 0, off_qp = 0, off_cheb = 0;
+  const size_t smem = TMA ? tile_layout_tma<T>(a.ts.ox, a.ts.oy, COEF == kCoefQP, MODE == kModeCheb, &off_face,
+                                               &off_qp, &off_cheb)
+                          : tile_layout<T>(a.ts.ox, a.ts.oy, COEF == kCoefQP, MODE == kModeCheb, &off_qp, &off_cheb);
   const int threads = tile_threads(a.ts);
   static std::mutex mu;
   static size_t smem_set = 0;
@@ -1052,8 +1318,16 @@ int launch_variant(const TileArgs<T>& a, const VoxMat<T>& m, cudaStream_t s) {
   if (b.ts.kz <= 0) b.ts.kz = launch_kz(tiles_xy, v.rz, cap);
   const long long n_tiles = tiles_xy * ((v.rz + b.ts.kz - 1) / b.ts.kz);
   const long long grid = std::min<long long>(n_tiles, cap);
-  { note_launch(); kern<<<(int)grid, threads, smem, s>>>(b, m); }
+  { note_launch(); kern<<<(int)grid, threads, smem, s>>>(b, m, mx, md); }
   return last_launch_status();
+}
+
+template <typename T, int COEF, int MODE, int OX, int OY>
+int launch_variant(const TileArgs<T>& a, const VoxMat<T>& m, cudaStream_t s) {
+  CUtensorMap mx, md;
+  const bool tma = tile_tensor_maps<T>(a, &mx, &md);
+  return tma ? launch_variant_t<T, COEF, MODE, OX, OY, true>(a, m, s, mx, md)
+             : launch_variant_t<T, COEF, MODE, OX, OY, false>(a, m, s, mx, md);
 }
 
 }  // namespace
@@ -1656,3 +1930,48 @@ int phastb_h8_autotune(const phastb_voxel_grid* g, const phastb_voxel_material* 
 }
 
 }  // extern "C"
+
+extern "C" int phastb_test_grid_barrier(int blocks, int skip_block, double limit_s, int* grid_error_host,
+                                        int* passed_host) {
+  using namespace phastb;
+  if (blocks < 1 || blocks > 64 || skip_block >= blocks || !(limit_s > 0) || limit_s > 10.0 || !grid_error_host ||
+      !passed_host)
+    return PHASTB_ERR_ARG;
+  int dev = 0, coop = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
+    return PHASTB_UNSUPPORTED;
+  PcgState* st = nullptr;
+  int* passed = nullptr;
+  if (cudaMalloc(&st, sizeof(PcgState)) != cudaSuccess) return PHASTB_ERR_CUDA;
+  if (cudaMalloc(&passed, sizeof(int)) != cudaSuccess) {
+    cudaFree(st);
+    return PHASTB_ERR_CUDA;
+  }
+  int status = cuda_status(cudaMemset(st, 0, sizeof(PcgState)));
+  if (!status) status = cuda_status(cudaMemset(passed, 0, sizeof(int)));
+  unsigned long long limit_ns = (unsigned long long)(limit_s * 1e9);
+  void* args[] = {&st, &skip_block, &limit_ns, &passed};
+  if (!status) {
+    note_launch();
+    status = cuda_status(cudaLaunchCooperativeKernel((const void*)grid_barrier_test_kernel, dim3(blocks), dim3(32),
+                                                     args, 0, nullptr));
+  }
+  if (!status) status = cuda_status(cudaDeviceSynchronize());
+  PcgState hs{};
+  if (!status) status = cuda_status(cudaMemcpy(&hs, st, sizeof(PcgState), cudaMemcpyDeviceToHost));
+  if (!status) status = cuda_status(cudaMemcpy(passed_host, passed, sizeof(int), cudaMemcpyDeviceToHost));
+  cudaFree(st);
+  cudaFree(passed);
+  if (status) return status;
+  *grid_error_host = hs.grid_error;
+  return hs.grid_error ? PHASTB_ERR_CUDA : PHASTB_OK;
+}
+
+extern "C" int phastb_h8_tma_staging(const phastb_voxel_grid* g, int dtype) {
+  using namespace phastb;
+  if (!valid_vox(g) || (dtype != PHASTB_F64 && dtype != PHASTB_F32)) return -1;
+  const VoxGeom v = make_vox_geom(*g);
+  const int A = dtype == PHASTB_F32 ? 4 : 2;
+  return (tma_enabled() && v.rx % A == 0 && tensor_map_encoder() != nullptr) ? 1 : 0;
+}

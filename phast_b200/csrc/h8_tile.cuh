@@ -62,6 +62,52 @@ __host__ __device__ inline size_t tile_layout(int ox, int oy, bool qp, bool cheb
   return o;
 }
 
+// TMA staging of the node layers (h8_tile_kernel with TMA): per node layer one
+// buffer of the halo tile's oy + 2 rows for u~ (3 components interleaved per
+// node) and one for d, each row W (or Wd) words long.  A tiled copy must start
+// on a 16-byte boundary, so the row's first word is the node column i0 - 1
+// rounded down to a multiple of A = 16 / sizeof(T) words and the kernel indexes
+// from the remainder (at most A - 1 words).  Three layers are in flight; every
+// buffer starts on a 128-byte boundary of the (realigned) dynamic shared memory.
+template <typename T>
+__host__ __device__ inline int tma_wx(int ox) {
+  const int A = 16 / (int)sizeof(T);
+  return (3 * (ox + 2) + A - 1 + A - 1) / A * A;
+}
+template <typename T>
+__host__ __device__ inline int tma_wd(int ox) {
+  const int A = 16 / (int)sizeof(T);
+  return ((ox + 2) + A - 1 + A - 1) / A * A;
+}
+__host__ __device__ inline size_t align128(size_t b) { return (b + 127) / 128 * 128; }
+template <typename T>
+__host__ __device__ inline size_t tma_xbytes(int ox, int oy) {
+  return align128(sizeof(T) * (size_t)tma_wx<T>(ox) * (oy + 2));
+}
+template <typename T>
+__host__ __device__ inline size_t tma_dbytes(int ox, int oy) {
+  return align128(sizeof(T) * (size_t)tma_wd<T>(ox) * (oy + 2));
+}
+
+// Dynamic shared memory of the TMA variant, relative to the 128-byte aligned
+// base: [3 u~ layer buffers][3 d layer buffers][face buffers [2][12][exy]], then
+// the staged per-element arrays and Chebyshev node data as in tile_layout.
+// Returns the bytes to request (128 bytes of slack for the realignment).
+template <typename T>
+__host__ __device__ inline size_t tile_layout_tma(int ox, int oy, bool qp, bool cheb, size_t* off_face, size_t* off_qp,
+                                                  size_t* off_cheb) {
+  const int exy = (ox + 1) * (oy + 1);
+  size_t o = 3 * (tma_xbytes<T>(ox, oy) + tma_dbytes<T>(ox, oy));
+  *off_face = o;
+  o += sizeof(T) * 24 * (size_t)exy;
+  o = (o + 15) / 16 * 16;
+  *off_qp = o;
+  if (qp) o += sizeof(T) * 2 * kStageQP * (size_t)exy;
+  *off_cheb = o;
+  if (cheb) o += (sizeof(T) * 2 * 9 * (size_t)ox * oy + 15) / 16 * 16;
+  return o + 128;
+}
+
 // Result slots of the apply's reduction workspace (ws.out).
 enum ApplyOut { kOutE = 0, kOutEnergy = 6, kOutDot = 7, kApplyOuts = 8 };
 
