@@ -405,16 +405,18 @@ def run_2d_configs(device, flush, with_cpu):
 
 def forms():
     from phast_b200.solid3d import MechForm
+    # the chosen form's V-cycle (one Chebyshev step per smoothing on the fine and middle levels,
+    # degree 6 on the coarsest) and inner tolerance came from a sweep on increments 1-20 of this cell
     return {"plain": MechForm(), "gmg": MechForm(precond="gmg"), "mixed": MechForm(mixed=True),
-            "mixed-gmg": MechForm(precond="gmg", mixed=True)}
+            "mixed-gmg": MechForm(precond="gmg", mixed=True, smooth_degree=1, coarse_degree=6, inner_rtol=1e-5)}
 
 
 FORM_LABEL = {
     "plain": "plain FP64: Jacobi PCG (PhAST's algorithm), FP64 box-KKT damage",
     "gmg": "FP64 PCG with a 3-level voxel multigrid V-cycle (Chebyshev deg 2, coarse deg 8)",
     "mixed": "FP32 Jacobi PCG (FP64 dots) under FP64 iterative refinement",
-    "mixed-gmg": "FP32 PCG with an FP32 3-level multigrid V-cycle (FP64 dots) under FP64 iterative refinement; "
-                 "FP64 box-KKT damage",
+    "mixed-gmg": "FP32 PCG with an FP32 3-level multigrid V-cycle (Chebyshev degree 1 / coarse 6; FP64 dots) under "
+                 "FP64 iterative refinement; FP64 box-KKT damage",
 }
 
 

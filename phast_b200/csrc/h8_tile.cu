@@ -94,6 +94,7 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
 // is well under a microsecond); the caller then marks its output non-finite.
 constexpr unsigned long long kTmaLimitNs = 1000000000ull;
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;  // the usual case: the copy landed during the last layer
   const unsigned long long t0 = global_ns();
   for (unsigned i = 0; i < (1u << 26); ++i) {
     if (mbar_try_wait(bar, parity)) return true;
@@ -419,6 +420,8 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
           if (use_d) reinterpret_cast<T*>(sbase + 3 * xbb + (size_t)b * dbb)[row * Wd + dr + col] = r.v[h][3];
         }
       }
+      // these generic-proxy writes must be ordered before the tensor copy that later refills the buffer
+      if (on) fence_proxy_async();
     }
   };
   // TMA: waits (bounded) for buffer b's copies of its current fill
@@ -498,7 +501,6 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
       xr = 3 * (i0 - 1) - xs0;
       ds0 = floor_mult(i0 - 1, kA);
       dr = (i0 - 1) - ds0;
-      fence_proxy_async();
       __syncthreads();  // the previous tile's last node phase is done with the buffers
       tma_issue(i0, j0, k0 - 1, 0);
       tma_issue(i0, j0, k0, 1);
@@ -542,7 +544,6 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
         mk_cur = mk_next;
         if (kk < K) mk_next = node_mask(i0, j0, ke + 1);
       }
-      if constexpr (TMA) fence_proxy_async();  // this thread's reads and patches before the next copies
       __syncthreads();
       // every thread is done with buffer (kk + 2) % 3 (node layer ke - 1): refill it with layer ke + 2
       if (kk < K) tma_issue(i0, j0, ke + 2, (kk + 2) % 3);
