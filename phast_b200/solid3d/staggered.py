@@ -245,7 +245,7 @@ def _solve_fused(op, *, fixed_mask, fixed_values, g=None, d=None, x0=None, rtol=
                  check_every=10):
     """The constrained Jacobi PCG of the elastic action as one C-ABI call (FP64)."""
     n = op.n_mech
-    mask = fixed_mask.to(torch.uint8).contiguous()
+    mask = fixed_mask if fixed_mask.dtype == torch.uint8 else fixed_mask.to(torch.uint8).contiguous()
     vals = fixed_values.to(torch.float64).contiguous()
     x0c = None if x0 is None else x0.to(torch.float64).contiguous()
     gq = None if g is None else g.to(torch.float64).contiguous()
@@ -312,7 +312,7 @@ def solve_constrained_form(op, form, *, fixed_mask, fixed_values, d=None, x0=Non
     if nbytes == 0:
         raise NotImplementedError(f"mechanics form {form} is not available for a {op.shape} grid "
                                   "(multigrid needs edges divisible by 2^(levels-1))")
-    mask = fixed_mask.to(torch.uint8).contiguous()
+    mask = fixed_mask if fixed_mask.dtype == torch.uint8 else fixed_mask.to(torch.uint8).contiguous()
     vals = fixed_values.to(torch.float64).contiguous()
     x0c = None if x0 is None else x0.to(torch.float64).contiguous()
     dd = (torch.zeros(op.n_red, dtype=torch.float64, device=op.device) if d is None
@@ -522,6 +522,8 @@ class StaggeredSolver:
         self._max_abs_target = max(abs(float(t)) for t in load.targets)
         self._u_floor = min(op.h) * math.sqrt(self._n_u)
         self._mask = op.mech_fixed_mask()
+        self._mask_u8 = self._mask.to(torch.uint8).contiguous()
+        self._zeros = torch.zeros(op.n_mech, dtype=torch.float64, device=op.device)
         self._red = _lib.Workspace(op.device)
         lengths = tuple(n * h for n, h in zip(op.shape, op.h))
         axis = self._c if self._c < 3 else 0
@@ -570,7 +572,7 @@ class StaggeredSolver:
     def _mechanics(self, d, values, x0):
         cfg = self.cfg
         try:
-            x, info = solve_constrained_form(self.op, self.form, fixed_mask=self._mask, fixed_values=values, d=d,
+            x, info = solve_constrained_form(self.op, self.form, fixed_mask=self._mask_u8, fixed_values=values, d=d,
                                              x0=x0, rtol=cfg.pcg_rtol_mech, maxiter=cfg.pcg_maxit_mech,
                                              check_every=cfg.check_every, lmax_cache=self._lmax)
         except PCGBreakdownError as exc:
@@ -640,7 +642,10 @@ class StaggeredSolver:
 
     def _attempt(self, state, target, previous, increment, cutbacks, t0):
         op, cfg = self.op, self.cfg
-        values = op.mech_fixed_values(target)
+        # mech_fixed_values(target) as one kernel: zero except E[controlled] = target
+        values = torch.empty(op.n_mech, dtype=torch.float64, device=op.device)
+        _lib.call("phastb_scale_set", op.n_mech, ptr(self._zeros), 0.0, self._n_u + self._c, float(target), ptr(values),
+                  stream())
         step_size = abs(target - previous)
         x_old = self._predictor(state, previous, target)
         d_old = state.d.clone()
