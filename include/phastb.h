@@ -80,6 +80,19 @@ int phastb_q4_strain(const phastb_q4_grid* g, int dtype, const void* u, void* ex
 int phastb_q4_internal_force(const phastb_q4_grid* g, const phastb_q4_material* m, int dtype,
                              const void* u, const void* d, void* f, void* stream);
 
+/* Transposed Gauss-point energy gradient f (N,2) = sum_q wq[e][q] B_q^T sigma0(u)_q of the
+ * undegraded energy psi0 (isotropic split only, FP64): the adjoint of the history update
+ * H = max(H_prev, psi+(u)) where psi+ won.  compute_psi_plus (isotropic),
+ * core/fem_operators.py:951-990 */
+int phastb_q4_psi_grad_t(const phastb_q4_grid* g, const phastb_q4_material* m, const double* u,
+                         const double* wq, double* f, void* stream);
+
+/* out (N,) = d/dd [z . f_int(u, d)] = sum_q w g'(d_q) N_q eps(z)_q . sigma0(u)_q (isotropic split,
+ * FP64): the damage derivative of the degraded internal force, contracted with z.
+ * internal_force, core/fem_operators.py:598-699; degradation, physics/material.py:497-529 */
+int phastb_q4_force_dd_t(const phastb_q4_grid* g, const phastb_q4_material* m, const double* u,
+                         const double* z, const double* d, double* out, void* stream);
+
 /* Jacobi diagonal (N,2) of K(d); d == NULL means g = 1.
  * FEMOperators.stiffness_diagonal, fem_operators.py:1284-1320 */
 int phastb_q4_stiffness_diagonal(const phastb_q4_grid* g, const phastb_q4_material* m, int dtype,

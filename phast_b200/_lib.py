@@ -71,6 +71,8 @@ SIGNATURES = {
     "phastb_q4_strain": (C.c_int, [Q4G, C.c_int, vp, vp, vp, vp, vp]),
     "phastb_q4_internal_force": (C.c_int, [Q4G, Q4M, C.c_int, vp, vp, vp, vp]),
     "phastb_q4_stiffness_diagonal": (C.c_int, [Q4G, Q4M, C.c_int, vp, vp, vp]),
+    "phastb_q4_psi_grad_t": (C.c_int, [Q4G, Q4M, vp, vp, vp, vp]),
+    "phastb_q4_force_dd_t": (C.c_int, [Q4G, Q4M, vp, vp, vp, vp, vp]),
     "phastb_q4_psi_history": (C.c_int, [Q4G, Q4M, C.c_int, vp, vp, vp, vp, vp]),
     "phastb_q4_damage_apply": (C.c_int, [Q4G, vp, vp, C.c_double, C.c_double, vp, C.c_double, vp, vp, vp]),
     "phastb_q4_damage_prepare": (C.c_int, [Q4G, vp, C.c_double, vp, C.c_double, vp, vp, vp, vp]),

@@ -64,6 +64,104 @@ __global__ void __launch_bounds__(kThreads) q4_force_kernel(Q4Tab<T> t, Mat2<T> 
   reinterpret_cast<typename Vec2<T>::type*>(f)[node] = out;
 }
 
+// Transposed Gauss-point energy gradient of the undegraded (isotropic) energy:
+//   f_n = sum_{e in n} sum_q wq[e][q] B_q^T sigma0(u)_q,   sigma0 = d psi0 / d eps,
+// i.e. (d psi0_q / d u)^T wq: the adjoint of the history update H = max(H_prev, psi0(u))
+// on the Gauss points where psi0 won (compute_psi_plus, fem_operators.py:951-990).
+__global__ void __launch_bounds__(kThreads) q4_psi_grad_t_kernel(Q4Tab<double> t, Mat2<double> m,
+                                                                  const double* __restrict__ u,
+                                                                  const double* __restrict__ wq,
+                                                                  double* __restrict__ f) {
+  const int nn = (t.nx + 1) * (t.ny + 1);
+  const int node = blockIdx.x * blockDim.x + threadIdx.x;
+  if (node >= nn) return;
+  const int i = node % (t.nx + 1), j = node / (t.nx + 1);
+  double fx = 0, fy = 0;
+#pragma unroll
+  for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+    for (int di = 0; di < 2; ++di) {
+      const int ei = i - 1 + di, ej = j - 1 + dj;
+      if (ei < 0 || ei >= t.nx || ej < 0 || ej >= t.ny) continue;
+      const int a = q4_local(1 - di, 1 - dj);
+      const int e = ej * t.nx + ei;
+      int n[4];
+      q4_corners(ei, ej, t.nx, n);
+      double ux[4], uy[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) load2(u, n[b], ux[b], uy[b]);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double exx = 0, eyy = 0, gxy = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          exx += t.gx[q][b] * ux[b];
+          eyy += t.gy[q][b] * uy[b];
+          gxy += t.gy[q][b] * ux[b] + t.gx[q][b] * uy[b];
+        }
+        double sxx, syy, sxy;
+        stress2(m, PHASTB_SPLIT_LINEAR, exx, eyy, gxy, 1.0, sxx, syy, sxy);
+        const double wv = __ldg(wq + 4 * (size_t)e + q);
+        fx += (t.gx[q][a] * sxx + t.gy[q][a] * sxy) * wv;
+        fy += (t.gy[q][a] * syy + t.gx[q][a] * sxy) * wv;
+      }
+    }
+  f[2 * (size_t)node] = fx;
+  f[2 * (size_t)node + 1] = fy;
+}
+
+// Derivative of z . f_int(u, d) with respect to the nodal damage, isotropic split:
+//   out_n = sum_{e in n} sum_q w g'(d_q) N_q(n) eps(z)_q . sigma0(u)_q,
+// g(d) = (1-d)^2 (1-eta) + eta (internal_force, fem_operators.py:598-699; degradation,
+// physics/material.py:497-529).
+__global__ void __launch_bounds__(kThreads) q4_force_dd_t_kernel(Q4Tab<double> t, Mat2<double> m,
+                                                                  const double* __restrict__ u,
+                                                                  const double* __restrict__ z,
+                                                                  const double* __restrict__ d,
+                                                                  double* __restrict__ out) {
+  const int nn = (t.nx + 1) * (t.ny + 1);
+  const int node = blockIdx.x * blockDim.x + threadIdx.x;
+  if (node >= nn) return;
+  const int i = node % (t.nx + 1), j = node / (t.nx + 1);
+  double acc = 0;
+#pragma unroll
+  for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+    for (int di = 0; di < 2; ++di) {
+      const int ei = i - 1 + di, ej = j - 1 + dj;
+      if (ei < 0 || ei >= t.nx || ej < 0 || ej >= t.ny) continue;
+      const int a = q4_local(1 - di, 1 - dj);
+      int n[4];
+      q4_corners(ei, ej, t.nx, n);
+      double ux[4], uy[4], zx[4], zy[4], dd[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        load2(u, n[b], ux[b], uy[b]);
+        load2(z, n[b], zx[b], zy[b]);
+        dd[b] = __ldg(d + n[b]);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double exx = 0, eyy = 0, gxy = 0, zxx = 0, zyy = 0, zxy = 0, dq = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          exx += t.gx[q][b] * ux[b];
+          eyy += t.gy[q][b] * uy[b];
+          gxy += t.gy[q][b] * ux[b] + t.gx[q][b] * uy[b];
+          zxx += t.gx[q][b] * zx[b];
+          zyy += t.gy[q][b] * zy[b];
+          zxy += t.gy[q][b] * zx[b] + t.gx[q][b] * zy[b];
+          dq += t.N[q][b] * dd[b];
+        }
+        double sxx, syy, sxy;
+        stress2(m, PHASTB_SPLIT_LINEAR, exx, eyy, gxy, 1.0, sxx, syy, sxy);
+        const double dg = -2.0 * (1.0 - dq) * (1.0 - m.eta);
+        acc += t.w * dg * t.N[q][a] * (zxx * sxx + zyy * syy + zxy * sxy);
+      }
+    }
+  out[node] = acc;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads) q4_kdiag_kernel(Q4Tab<T> t, Mat2<T> m, const T* __restrict__ d,
                                                             T* __restrict__ diag) {
@@ -580,6 +678,26 @@ int phastb_q4_internal_force(const phastb_q4_grid* g, const phastb_q4_material* 
   if (dtype == PHASTB_F64) return launch_force<double>(g, m, u, d, f, (cudaStream_t)stream);
   if (dtype == PHASTB_F32) return launch_force<float>(g, m, u, d, f, (cudaStream_t)stream);
   return PHASTB_ERR_ARG;
+}
+
+int phastb_q4_psi_grad_t(const phastb_q4_grid* g, const phastb_q4_material* m, const double* u, const double* wq,
+                         double* f, void* stream) {
+  if (!valid_grid(g) || !m || !u || !wq || !f) return PHASTB_ERR_ARG;
+  if (m->psi_split != PHASTB_SPLIT_ISOTROPIC && m->psi_split != PHASTB_SPLIT_LINEAR) return PHASTB_UNSUPPORTED;
+  const int nn = (g->nx + 1) * (g->ny + 1);
+  { note_launch(); q4_psi_grad_t_kernel<<<grid_full(nn), kThreads, 0, (cudaStream_t)stream>>>(
+      make_q4_tab<double>(*g), make_mat2<double>(*m), u, wq, f); }
+  return last_launch_status();
+}
+
+int phastb_q4_force_dd_t(const phastb_q4_grid* g, const phastb_q4_material* m, const double* u, const double* z,
+                         const double* d, double* out, void* stream) {
+  if (!valid_grid(g) || !m || !u || !z || !d || !out) return PHASTB_ERR_ARG;
+  if (m->stress_split != PHASTB_SPLIT_ISOTROPIC && m->stress_split != PHASTB_SPLIT_LINEAR) return PHASTB_UNSUPPORTED;
+  const int nn = (g->nx + 1) * (g->ny + 1);
+  { note_launch(); q4_force_dd_t_kernel<<<grid_full(nn), kThreads, 0, (cudaStream_t)stream>>>(
+      make_q4_tab<double>(*g), make_mat2<double>(*m), u, z, d, out); }
+  return last_launch_status();
 }
 
 int phastb_q4_stiffness_diagonal(const phastb_q4_grid* g, const phastb_q4_material* m, int dtype, const void* d,

@@ -138,6 +138,8 @@ class StaggeredSolver:
         self._step_count = 0
         self._explicit_step_count = 0
         self._last_stagger_iter = 0
+        # when a list, every quasi-static staggered pass appends its iterate (u, d, H) to it
+        self.stagger_trace = None
 
     # -- pieces ------------------------------------------------------------------
     def _pf(self):
@@ -170,7 +172,9 @@ class StaggeredSolver:
         pf_mask, pf_vals = self._pf()
         d_prev_arg = d_prev_step if d_prev_step is not None else self.d
         init = self.d if d_prev_step is not None else None
-        self.d = self.damage_solver.solve(self.H_elem, d_prev_arg, pf_dirichlet_mask=pf_mask,
+        # a per-element Gc field set as diff_Gc_field (staggered_solver.py:904-936)
+        gc_field = getattr(self, "diff_Gc_field", None)
+        self.d = self.damage_solver.solve(self.H_elem, d_prev_arg, Gc_field=gc_field, pf_dirichlet_mask=pf_mask,
                                           pf_dirichlet_values=pf_vals, initial_guess=init)
         self._apply_pf_dirichlet()
 
@@ -205,6 +209,8 @@ class StaggeredSolver:
             self.step_mechanics()
             self.step_compute_driving_force()
             self.step_solve_damage(d_prev_step=d_prev_step)
+            if self.stagger_trace is not None:
+                self.stagger_trace.append((self.u.clone(), self.d.clone(), self.H_elem.clone()))
             if need:
                 d_change = float(torch.linalg.vector_norm(self.d - d_old) / (torch.linalg.vector_norm(self.d) + 1e-30))
                 u_change = float(torch.linalg.vector_norm(self.u - u_old) / (torch.linalg.vector_norm(self.u) + 1e-30))
