@@ -222,6 +222,41 @@ int phastb_t3_damage_solve(const phastb_t3_mesh* mesh, const double* H, double g
                            const double* fixed_vals, double tol, int max_iter, int check_every,
                            double* d_out, int* info, void* workspace, size_t workspace_bytes, void* stream);
 
+/* T3 adjoint pieces (isotropic split, FP64), the element analogues of the Q4 entries:
+ * f (N,2) = sum_e w[e] B_e^T sigma0(u)_e, the transpose of u -> psi+_e where w is the history
+ * gradient on the elements where psi+ won (compute_psi_plus, fem_operators.py:951-990);
+ * out (N,) = d/dd [z . f_int(u, d)] = sum_e A_e g'(d_e) / 3 eps(z)_e . sigma0(u)_e with d_e the
+ * element mean (internal_force, fem_operators.py:598-680). */
+int phastb_t3_psi_grad_t(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u,
+                         const double* w, double* f, void* stream);
+int phastb_t3_force_dd_t(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u,
+                         const double* z, const double* d, double* out, void* stream);
+/* Per-element adjoint quadratic forms of the T3 AT2 system for an adjoint lam and damage d:
+ * lam_K_d_e = A (grad lam . grad d), lam_M_d_e = A/12 (sum lam sum d + lam . d),
+ * grad_gc_e = -(l0 lam_K_d_e + lam_M_d_e / l0), grad_H_e = 2 A sum_a lam_a (1/3 - (d_a + sum d)/12);
+ * any output may be NULL.  _adjoint_quadratic_forms_perelem and the history pullback of
+ * _AdjointDamageSolveField, solvers/damage_solver.py:284-336, 1017-1027 */
+int phastb_t3_damage_adjoint_grads(const phastb_t3_mesh* mesh, const double* lam, const double* d, double l0,
+                                   double* grad_gc_e, double* grad_H, double* lam_K_d_e, double* lam_M_d_e,
+                                   void* stream);
+/* Dirichlet-eliminated linear AT2 solve A x = rhs on T3 (as phastb_q4_damage_linear_solve):
+ * the adjoint system of the damage step.  _pcg_solve_adjoint_system, damage_solver.py:423-480 */
+size_t phastb_t3_damage_linear_workspace_bytes(int n_nodes);
+int phastb_t3_damage_linear_solve(const phastb_t3_mesh* mesh, const double* H, double gc_over_l0,
+                                  const double* gc_over_l0_e, double gcl0, const double* gcl0_e, const double* rhs,
+                                  const uint8_t* fixed, const double* fixed_vals, const double* x0, double rtol,
+                                  int max_iter, int check_every, double* x_out, int* info, double* rinfo,
+                                  void* workspace, size_t workspace_bytes, void* stream);
+/* Quasi-static Newton with matrix-free CG on a T3 mesh (as phastb_q4_qs_solve; isotropic split;
+ * the stiffness action is the coloured internal-force scatter).  QuasiStaticSolver.solve,
+ * mechanics_solver.py:1597-1831 */
+size_t phastb_t3_qs_workspace_bytes(int n_nodes);
+int phastb_t3_qs_solve(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* d,
+                       const double* f_ext, const uint8_t* bc_mask, const double* bc_vals, double* u, double tol,
+                       double cg_tol, int cg_max_iter, int max_iter, int line_search, int ls_max_steps,
+                       double ls_min_alpha, double ls_c, int* info, void* workspace, size_t workspace_bytes,
+                       void* stream);
+
 /* Energy sums (FP64): out[0] elastic, out[1] fracture surface term d^T M d,
  * out[2] gradient term d^T K d, out[3] kinetic sum_i |v_i|^2 M_i (v may be NULL).
  * compute_energy_components, fem_operators.py:1430-1496 (caller scales by Gc etc.) */

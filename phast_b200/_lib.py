@@ -92,6 +92,15 @@ SIGNATURES = {
     "phastb_t3_damage_solve_workspace_bytes": (C.c_size_t, [C.c_int]),
     "phastb_t3_damage_solve": (C.c_int, [T3M, vp, C.c_double, vp, C.c_double, vp, vp, vp, vp, vp, C.c_double, C.c_int,
                                          C.c_int, vp, ip, vp, sz, vp]),
+    "phastb_t3_psi_grad_t": (C.c_int, [T3M, Q4M, vp, vp, vp, vp]),
+    "phastb_t3_force_dd_t": (C.c_int, [T3M, Q4M, vp, vp, vp, vp, vp]),
+    "phastb_t3_damage_adjoint_grads": (C.c_int, [T3M, vp, vp, C.c_double, vp, vp, vp, vp, vp]),
+    "phastb_t3_damage_linear_workspace_bytes": (C.c_size_t, [C.c_int]),
+    "phastb_t3_damage_linear_solve": (C.c_int, [T3M, vp, C.c_double, vp, C.c_double, vp, vp, vp, vp, vp, C.c_double,
+                                                C.c_int, C.c_int, vp, ip, dp, vp, sz, vp]),
+    "phastb_t3_qs_workspace_bytes": (sz, [C.c_int]),
+    "phastb_t3_qs_solve": (C.c_int, [T3M, Q4M, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_int,
+                                     C.c_int, C.c_int, C.c_double, C.c_double, ip, vp, sz, vp]),
     "phastb_q4_explicit_step": (C.c_int, [Q4G, Q4M, C.c_int, C.c_double, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                           vp, vp, vp, vp]),
     "phastb_q4_energy_sums": (C.c_int, [Q4G, Q4M, vp, vp, vp, dp, vp, sz, vp]),

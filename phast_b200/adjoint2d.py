@@ -1,5 +1,5 @@
 """Gradient of the peak reaction force of a quasi-static staggered run with respect to a
-per-element Gc field (Q4, isotropic split, AT2), by a hand-written reverse pass.
+per-element Gc field (Q4 or T3, isotropic split, AT2), by a hand-written reverse pass.
 
 The forward run is PhAST's quasi-static staggered scheme as this package executes it
 (``StaggeredSolver.step_full``, staggered_solver.py:1103-1344): at every load step each
@@ -16,26 +16,29 @@ PhAST's autograd would differentiate through its own unrolled loop
 _AdjointDamageSolveField for the damage, damage_solver.py:866-1037) -- with:
 
 * the damage solve on its frozen active set: lam solves A_FF lam_F = g_F (one device
-  PCG), giving the Gc-field, history and lower-bound gradients
-  (``PhaseFieldDamageSolver`` adjoint kernels);
+  PCG), giving the Gc-field, history and lower-bound gradients (the damage solver's
+  ``linear_solve`` and ``adjoint_grads``);
 * the history max: the gradient of H_j goes to psi0(u_j) on the Gauss points where psi0
-  won and to H_{j-1} elsewhere; (d psi0/du)^T w is ``phastb_q4_psi_grad_t``;
-* the mechanics solve: U^T w = -(d (K(d) u)/dd)^T z with K_ff z = w_f, one quasi-static
-  solve with K(d) and ``phastb_q4_force_dd_t``.
+  won and to H_{j-1} elsewhere; (d psi0/du)^T w is the operators' ``psi_grad_t``;
+* the mechanics solve: U^T w = -(d (K(d) u)/dd)^T z with K_ff z = w_f, one stiffness
+  solve (``QuasiStaticSolver.solve_stiffness``) and the operators' ``force_dd_t``.
+
+Where no damage node sits on a bound other than the pinned (phase-field Dirichlet) ones,
+the frozen-active-set derivative and PhAST's solve-then-clamp adjoint
+(``_masked_adjoint_inputs`` / ``_pcg_solve_adjoint_system``, damage_solver.py:400-480) are
+the same quantity; with bound-active nodes this module gives the exact derivative of the
+projected solve (the held nodes' coupling -(A lam)_i to the lower bound included).
 
 Memory: states are checkpointed every ``checkpoint_every`` load steps in the forward run;
 the reverse pass recomputes one segment at a time, recording every staggered pass of it.
 """
 from __future__ import annotations
 
-import ctypes as C
 from dataclasses import dataclass, field
 
 import numpy as np
 import torch
 
-from . import _lib
-from ._lib import call, ptr, raw, stream
 from .damage2d import classify_active_set
 from .fem2d import stress_split_of
 
@@ -53,7 +56,7 @@ class PeakReactionGradient:
     """dJ/dGc_e for J = max_k R_k over ``n_steps`` load steps of a quasi-static ``StaggeredSolver``.
 
     ``solver``: a ``phast_b200.StaggeredSolver`` with ``solver_type='quasi_static'`` on a
-    structured Q4 mesh with the isotropic split; its ``bcs`` prescribe the top displacement
+    structured Q4 or a T3 mesh with the isotropic split; its ``bcs`` prescribe the top displacement
     through ``load_factor``.  ``load(k)`` gives the load factor of step k (1-based);
     ``top`` the node ids of the loaded edge.  The solver's state is reset to its current
     values (u, d, H) at every ``forward`` call.
@@ -76,9 +79,7 @@ class PeakReactionGradient:
         self.rtol = float(adjoint_rtol)
         self.start = (solver.u.clone(), solver.d.clone(), solver.H_elem.clone())
         bc_mask, _ = solver.bcs.get_masks_and_values()
-        self.free = (~bc_mask.to(fem.device)).to(torch.float64)
-        self.bc_u8 = bc_mask.to(device=fem.device, dtype=torch.uint8).contiguous()
-        self.zero_bc = torch.zeros(fem.n_nodes, 2, dtype=torch.float64, device=fem.device)
+        self.bc_mask = bc_mask.to(fem.device)
         self.e_top = torch.zeros(fem.n_nodes, 2, dtype=torch.float64, device=fem.device)
         self.e_top[self.top, 1] = 1.0
         pf_mask, _ = (solver.bcs.get_pf_dirichlet_mask_values() if getattr(solver.bcs, "pf_dirichlet_bcs", None)
@@ -114,55 +115,19 @@ class PeakReactionGradient:
         return np.array(R)
 
     # -- reverse pieces ----------------------------------------------------------------------
-    def _psi_t(self, u, wq):
-        f = torch.empty(self.fem.n_nodes, 2, dtype=torch.float64, device=u.device)
-        call("phastb_q4_psi_grad_t", self.fem.grid, self.fem.mat(torch.float64), ptr(u.contiguous()),
-             ptr(wq.contiguous()), ptr(f), stream())
-        return f
-
-    def _force_dd_t(self, u, z, d):
-        out = torch.empty(self.fem.n_nodes, dtype=torch.float64, device=u.device)
-        call("phastb_q4_force_dd_t", self.fem.grid, self.fem.mat(torch.float64), ptr(u.contiguous()),
-             ptr(z.contiguous()), ptr(d.contiguous()), ptr(out), stream())
-        return out
-
     def _U_t(self, u, d, w):
-        """U^T w: -(d(K(d) u)/dd)^T z with K_ff z = w_f (z = 0 on prescribed dofs).
-
-        The stiffness solve is the quasi-static Newton-CG entry with zero prescribed values
-        (one CG solve plus refinement steps: the problem is linear) to a residual of
-        ``adjoint_rtol`` relative to w_f."""
-        wf = (w * self.free).contiguous()
-        nrm = float(torch.linalg.vector_norm(wf))
-        if nrm == 0.0:
+        """U^T w: -(d(K(d) u)/dd)^T z with K_ff z = w_f (z = 0 on prescribed dofs)."""
+        z = self.s.mechanics.solve_stiffness(d, w, self.bc_mask, rtol=self.rtol)
+        if not bool(torch.any(z != 0)):
             return torch.zeros(self.fem.n_nodes, dtype=torch.float64, device=u.device)
-        fem, qs = self.fem, self.s.mechanics
-        z = torch.zeros_like(wf)
-        dd = d.to(torch.float64).contiguous()
-        info = (C.c_int * 3)()
-        wp, wn = qs._ws.get(_lib.load().phastb_q4_qs_workspace_bytes(fem.n_nodes))
-        st = raw("phastb_q4_qs_solve", fem.grid, fem.mat(torch.float64), ptr(dd), ptr(wf), ptr(self.bc_u8),
-                 ptr(self.zero_bc), ptr(z), self.rtol * nrm, 1e-10, qs.cg_max_iter, 30, 0, 0, 1e-4, 1e-4, info,
-                 wp, wn, stream())
-        if st != _lib.OK or not info[1]:
-            raise RuntimeError(f"adjoint stiffness solve did not converge (status {st}, {info[0]} refinements)")
-        return -self._force_dd_t(u, z, d)
+        return -self.fem.force_dd_t(u, z, d)
 
     def _damage_vjp(self, H, d_start, d, g, Gc_field):
-        """(dJ/dH (E,4), dJ/dd_start (N,), dJ/dGc (E,)) of d = D(H, d_start, Gc) for the output gradient g."""
+        """(dJ/dH, dJ/dd_start (N,), dJ/dGc (E,)) of d = D(H, d_start, Gc) for the output gradient g."""
         ds = self.s.damage_solver
         lower, upper, fx, interior = classify_active_set(d, d_start, self.pf_mask)
         lam = ds.linear_solve(H, g * interior, Gc_field=Gc_field, fixed=~interior, rtol=self.rtol)
-        E = self.fem.n_elems
-        dev = d.device
-        g_gc = torch.empty(E, dtype=torch.float64, device=dev)
-        g_h = torch.empty(E, 4, dtype=torch.float64, device=dev)
-        lkd = torch.empty(E, dtype=torch.float64, device=dev)
-        lmd = torch.empty(E, dtype=torch.float64, device=dev)
-        dd = d.contiguous()
-        call("phastb_q4_damage_adjoint_grads", self.fem.grid, ptr(lam), ptr(dd), ds._material(None, None, Gc_field)[1],
-             ptr(g_gc), ptr(g_h),
-             ptr(lkd), ptr(lmd), stream())
+        g_gc, g_h = ds.adjoint_grads(lam, d, Gc_field=Gc_field)
         g_start = torch.zeros_like(g)
         if bool(lower.any()):
             g_start = (g - ds._apply_full(H, lam, Gc_field=Gc_field)) * lower
@@ -186,7 +151,7 @@ class PeakReactionGradient:
             # H_j = max(H_{j-1}, psi0(u_j))
             psi = self.fem.compute_psi_plus(u_j)
             won = (psi > H_prev_pass).to(torch.float64)
-            g_u = g_u + self._psi_t(u_j, won * g_H)
+            g_u = g_u + self.fem.psi_grad_t(u_j, won * g_H)
             g_H = (1.0 - won) * g_H
             # u_j = U(d_{j-1})
             g_d = self._U_t(u_j, d_prev_pass, g_u)
@@ -203,7 +168,7 @@ class PeakReactionGradient:
         grad = torch.zeros(self.fem.n_elems, dtype=torch.float64, device=self.fem.device)
         N = self.fem.n_nodes
         g_d = torch.zeros(N, dtype=torch.float64, device=grad.device)
-        g_H = torch.zeros(self.fem.n_elems, 4, dtype=torch.float64, device=grad.device)
+        g_H = torch.zeros_like(self.start[2], dtype=torch.float64)
         passes_per_step = {}
         seg_end = kstar
         while seg_end >= 1:
@@ -221,7 +186,7 @@ class PeakReactionGradient:
                 if k == kstar:
                     # R = e_top . K(d) u: dR/du = K(d) e_top, dR/dd = d(e_top . K(d) u)/dd
                     g_u = self.fem.internal_force(self.e_top, d_k).to(torch.float64)
-                    g_d = g_d + self._force_dd_t(u_k, self.e_top, d_k)
+                    g_d = g_d + self.fem.force_dd_t(u_k, self.e_top, d_k)
                 passes_per_step[k] = len(traces[k])
                 g_d, g_H = self._step_reverse(states[k - 1], traces[k], g_u, g_d, g_H, Gc_field, grad)
             seg_end = seg_start

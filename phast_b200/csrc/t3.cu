@@ -47,7 +47,8 @@ __device__ __forceinline__ void t3_strain(const T3Dev& t, int e, const double* _
 __global__ void __launch_bounds__(kThreads) t3_force_colour(T3Dev t, Mat2<double> m, int split,
                                                             const double* __restrict__ u,
                                                             const double* __restrict__ d, double* f, int k0,
-                                                            int k1) {
+                                                            int k1, const int* guard) {
+  if (guard && *guard == 0) return;
   const int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= k1) return;
   const int e = __ldg(t.order + k);
@@ -139,7 +140,113 @@ __global__ void t3_invert_kernel(int n, double* __restrict__ x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = 1.0 / (x[i] + 1e-30);
 }
 
-bool valid_mesh(const phastb_t3_mesh* m) {
+__global__ void t3_zero_kernel(int n, double* __restrict__ y, const int* guard) {
+  if (guard && *guard == 0) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = 0.0;
+}
+
+// y[i] = 0 on the rows a mask holds fixed (Dirichlet-eliminated operators of the Krylov engines)
+__global__ void t3_mask_rows_kernel(int n, const uint8_t* __restrict__ mask, double* __restrict__ y,
+                                    const int* guard) {
+  if (guard && *guard == 0) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (mask[i]) y[i] = 0.0;
+}
+
+// f_a += w_e B_a^T sigma0(u_e): the transpose of u -> psi_e (isotropic split, full energy
+// 0.5 eps : C : eps at the centroid), weighted per element.
+__global__ void __launch_bounds__(kThreads) t3_psi_grad_t_colour(T3Dev t, Mat2<double> m,
+                                                                 const double* __restrict__ u,
+                                                                 const double* __restrict__ w, double* f, int k0,
+                                                                 int k1) {
+  const int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= k1) return;
+  const int e = __ldg(t.order + k);
+  int n[3];
+  double gp[3][2], exx, eyy, gxy;
+  t3_strain(t, e, u, exx, eyy, gxy, n, gp);
+  double sxx, syy, sxy;
+  stress2(m, PHASTB_SPLIT_LINEAR, exx, eyy, gxy, 1.0, sxx, syy, sxy);
+  const double we = __ldg(w + e);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    f[2 * n[a]] += we * (sxx * gp[a][0] + sxy * gp[a][1]);
+    f[2 * n[a] + 1] += we * (sxy * gp[a][0] + syy * gp[a][1]);
+  }
+}
+
+// out_a += A_e g'(d_e) / 3 eps(z_e) . sigma0(u_e): the derivative of z . f_int(u, d) with
+// respect to the nodal damage, d_e the element mean, g(d) = (1-d)^2 (1-eta) + eta.
+__global__ void __launch_bounds__(kThreads) t3_force_dd_t_colour(T3Dev t, Mat2<double> m,
+                                                                 const double* __restrict__ u,
+                                                                 const double* __restrict__ z,
+                                                                 const double* __restrict__ d, double* out, int k0,
+                                                                 int k1) {
+  const int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= k1) return;
+  const int e = __ldg(t.order + k);
+  int n[3];
+  double gp[3][2], exx, eyy, gxy;
+  t3_strain(t, e, u, exx, eyy, gxy, n, gp);
+  double zxx = 0, zyy = 0, zxy = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double zx = __ldg(z + 2 * n[a]), zy = __ldg(z + 2 * n[a] + 1);
+    zxx += gp[a][0] * zx;
+    zyy += gp[a][1] * zy;
+    zxy += gp[a][1] * zx + gp[a][0] * zy;
+  }
+  double sxx, syy, sxy;
+  stress2(m, PHASTB_SPLIT_LINEAR, exx, eyy, gxy, 1.0, sxx, syy, sxy);
+  const double de = (__ldg(d + n[0]) + __ldg(d + n[1]) + __ldg(d + n[2])) / 3.0;
+  const double dg = -2.0 * (1.0 - de) * (1.0 - m.eta);
+  const double v = __ldg(t.areas + e) * dg * (zxx * sxx + zyy * syy + zxy * sxy) / 3.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) out[n[a]] += v;
+}
+
+// Per-element adjoint quadratic forms of the AT2 system and the Gc-field / history gradients:
+//   lkd_e = A (grad lam . grad d),  lmd_e = A/12 (sum lam sum d + lam . d),
+//   dJ/dGc_e = -(l0 lkd_e + lmd_e / l0),  dJ/dH_e = 2 A sum_a lam_a (1/3 - (d_a + sum d) / 12)
+// (_adjoint_quadratic_forms_perelem and the history pullback, damage_solver.py:284-336, 1017-1027).
+__global__ void __launch_bounds__(kThreads) t3_damage_adjoint_kernel(T3Dev t, const double* __restrict__ lam,
+                                                                     const double* __restrict__ d, double l0,
+                                                                     double* __restrict__ g_gc,
+                                                                     double* __restrict__ g_h,
+                                                                     double* __restrict__ lkd,
+                                                                     double* __restrict__ lmd, int ne) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  double l[3], dd[3], glx = 0, gly = 0, gdx = 0, gdy = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int n = __ldg(t.elem + 3 * e + a);
+    const double gx = __ldg(t.grad + 6 * e + 2 * a), gy = __ldg(t.grad + 6 * e + 2 * a + 1);
+    l[a] = __ldg(lam + n);
+    dd[a] = __ldg(d + n);
+    glx += gx * l[a];
+    gly += gy * l[a];
+    gdx += gx * dd[a];
+    gdy += gy * dd[a];
+  }
+  const double A = __ldg(t.areas + e);
+  const double ls = l[0] + l[1] + l[2], ds = dd[0] + dd[1] + dd[2];
+  const double kd = A * (glx * gdx + gly * gdy);
+  const double md = A / 12.0 * (ls * ds + l[0] * dd[0] + l[1] * dd[1] + l[2] * dd[2]);
+  if (g_gc) g_gc[e] = -(l0 * kd + md / l0);
+  if (g_h) {
+    double acc = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) acc += l[a] * (1.0 / 3.0 - (dd[a] + ds) / 12.0);
+    g_h[e] = 2.0 * A * acc;
+  }
+  if (lkd) lkd[e] = kd;
+  if (lmd) lmd[e] = md;
+}
+
+}  // namespace
+
+bool t3_valid_mesh(const phastb_t3_mesh* m) {
   if (!m || m->n_nodes < 1 || m->n_elems < 1 || m->n_colors < 1 || !m->elem || !m->order || !m->color_off ||
       !m->grad || !m->areas)
     return false;
@@ -149,9 +256,10 @@ bool valid_mesh(const phastb_t3_mesh* m) {
   return true;
 }
 
+// y = A(H, Gc) d of the AT2 system; rows that ``mask`` holds fixed give 0.
 int t3_damage_apply_launch(const phastb_t3_mesh& mesh, const double* d, const double* H, double gco,
                            const double* gco_e, double gcl0, const double* gcl0_e, double* y, const int* guard,
-                           cudaStream_t s) {
+                           cudaStream_t s, const uint8_t* mask) {
   int st = cuda_status(cudaMemsetAsync(y, 0, sizeof(double) * (size_t)mesh.n_nodes, s));
   if (st) return st;
   const T3Dev t = t3_dev(mesh);
@@ -160,8 +268,27 @@ int t3_damage_apply_launch(const phastb_t3_mesh& mesh, const double* d, const do
     if (k1 <= k0) continue;
     { note_launch(); t3_damage_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, d, H, gco, gco_e, gcl0, gcl0_e, y, k0, k1, guard); }
   }
+  if (mask) { note_launch(); t3_mask_rows_kernel<<<grid_for(mesh.n_nodes), kThreads, 0, s>>>(mesh.n_nodes, mask, y, guard); }
   return last_launch_status();
 }
+
+// f = f_int(u, d) (d NULL: undegraded linear); rows that ``mask`` holds fixed (2 per node) give 0.
+int t3_force_launch(const phastb_t3_mesh& mesh, const phastb_q4_material& m, const double* u, const double* d,
+                    double* f, const uint8_t* mask, const int* guard, cudaStream_t s) {
+  const int n2 = 2 * mesh.n_nodes;
+  { note_launch(); t3_zero_kernel<<<grid_for(n2), kThreads, 0, s>>>(n2, f, guard); }
+  const T3Dev t = t3_dev(mesh);
+  const Mat2<double> mm = make_mat2<double>(m);
+  for (int c = 0; c < mesh.n_colors; ++c) {
+    const int k0 = mesh.color_off[c], k1 = mesh.color_off[c + 1];
+    if (k1 <= k0) continue;
+    { note_launch(); t3_force_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, mm, m.stress_split, u, d, f, k0, k1, guard); }
+  }
+  if (mask) { note_launch(); t3_mask_rows_kernel<<<grid_for(n2), kThreads, 0, s>>>(n2, mask, f, guard); }
+  return last_launch_status();
+}
+
+namespace {
 
 // Damage operator context for the Krylov engines.  The mesh is held by value;
 // color_off points into caller memory that must outlive the solve.
@@ -176,7 +303,7 @@ struct T3DamageCtx {
 
 int t3_damage_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
   const T3DamageCtx* k = static_cast<const T3DamageCtx*>(c);
-  return t3_damage_apply_launch(k->mesh, x, k->H, k->gco, k->gco_e, k->gcl0, k->gcl0_e, y, guard, s);
+  return t3_damage_apply_launch(k->mesh, x, k->H, k->gco, k->gco_e, k->gcl0, k->gcl0_e, y, guard, s, nullptr);
 }
 
 }  // namespace
@@ -189,23 +316,13 @@ extern "C" {
 
 int phastb_t3_internal_force(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u,
                              const double* d, double* f, void* stream) {
-  if (!valid_mesh(mesh) || !m || !u || !f) return PHASTB_ERR_ARG;
-  cudaStream_t s = (cudaStream_t)stream;
-  int st = cuda_status(cudaMemsetAsync(f, 0, sizeof(double) * 2 * (size_t)mesh->n_nodes, s));
-  if (st) return st;
-  const T3Dev t = t3_dev(*mesh);
-  const Mat2<double> mm = make_mat2<double>(*m);
-  for (int c = 0; c < mesh->n_colors; ++c) {
-    const int k0 = mesh->color_off[c], k1 = mesh->color_off[c + 1];
-    if (k1 <= k0) continue;
-    { note_launch(); t3_force_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, mm, m->stress_split, u, d, f, k0, k1); }
-  }
-  return last_launch_status();
+  if (!t3_valid_mesh(mesh) || !m || !u || !f) return PHASTB_ERR_ARG;
+  return t3_force_launch(*mesh, *m, u, d, f, nullptr, nullptr, (cudaStream_t)stream);
 }
 
 int phastb_t3_psi_history(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u,
                           const double* H_in, double* H_out, double* psi, void* stream) {
-  if (!valid_mesh(mesh) || !m || !u || (!H_out && !psi)) return PHASTB_ERR_ARG;
+  if (!t3_valid_mesh(mesh) || !m || !u || (!H_out && !psi)) return PHASTB_ERR_ARG;
   const int ne = mesh->n_elems;
   { note_launch(); t3_psi_kernel<<<grid_full(ne), kThreads, 0, (cudaStream_t)stream>>>(t3_dev(*mesh), make_mat2<double>(*m), u, H_in, H_out, psi, ne); }
   return last_launch_status();
@@ -213,15 +330,15 @@ int phastb_t3_psi_history(const phastb_t3_mesh* mesh, const phastb_q4_material* 
 
 int phastb_t3_damage_apply(const phastb_t3_mesh* mesh, const double* d, const double* H, double gc_over_l0,
                            const double* gc_over_l0_e, double gcl0, const double* gcl0_e, double* y, void* stream) {
-  if (!valid_mesh(mesh) || !d || !y) return PHASTB_ERR_ARG;
+  if (!t3_valid_mesh(mesh) || !d || !y) return PHASTB_ERR_ARG;
   return t3_damage_apply_launch(*mesh, d, H, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e, y, nullptr,
-                                (cudaStream_t)stream);
+                                (cudaStream_t)stream, nullptr);
 }
 
 int phastb_t3_damage_prepare(const phastb_t3_mesh* mesh, const double* H, double gc_over_l0,
                              const double* gc_over_l0_e, double gcl0, const double* gcl0_e, double* b,
                              double* m_inv, void* stream) {
-  if (!valid_mesh(mesh) || !b || !m_inv) return PHASTB_ERR_ARG;
+  if (!t3_valid_mesh(mesh) || !b || !m_inv) return PHASTB_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   const size_t nb = sizeof(double) * (size_t)mesh->n_nodes;
   int st;
@@ -244,7 +361,7 @@ int phastb_t3_damage_solve(const phastb_t3_mesh* mesh, const double* H, double g
                            const double* d_init, const uint8_t* fixed, const double* fixed_vals, double tol,
                            int max_iter, int check_every, double* d_out, int* info, void* workspace,
                            size_t workspace_bytes, void* stream) {
-  if (!valid_mesh(mesh) || !d_prev || !d_out || max_iter < 0 || check_every < 1) return PHASTB_ERR_ARG;
+  if (!t3_valid_mesh(mesh) || !d_prev || !d_out || max_iter < 0 || check_every < 1) return PHASTB_ERR_ARG;
   if (fixed && !fixed_vals) return PHASTB_ERR_ARG;
   const int n = mesh->n_nodes;
   if (!workspace || workspace_bytes < ppcg_ws_bytes(n)) return PHASTB_ERR_WORKSPACE;
@@ -270,6 +387,50 @@ int phastb_t3_damage_solve(const phastb_t3_mesh* mesh, const double* H, double g
     info[1] = inf[1];
   }
   return st;
+}
+
+int phastb_t3_psi_grad_t(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u,
+                         const double* w, double* f, void* stream) {
+  if (!t3_valid_mesh(mesh) || !m || !u || !w || !f) return PHASTB_ERR_ARG;
+  if (m->psi_split != PHASTB_SPLIT_ISOTROPIC && m->psi_split != PHASTB_SPLIT_LINEAR) return PHASTB_UNSUPPORTED;
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = cuda_status(cudaMemsetAsync(f, 0, sizeof(double) * 2 * (size_t)mesh->n_nodes, s));
+  if (st) return st;
+  const T3Dev t = t3_dev(*mesh);
+  const Mat2<double> mm = make_mat2<double>(*m);
+  for (int c = 0; c < mesh->n_colors; ++c) {
+    const int k0 = mesh->color_off[c], k1 = mesh->color_off[c + 1];
+    if (k1 <= k0) continue;
+    { note_launch(); t3_psi_grad_t_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, mm, u, w, f, k0, k1); }
+  }
+  return last_launch_status();
+}
+
+int phastb_t3_force_dd_t(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u, const double* z,
+                         const double* d, double* out, void* stream) {
+  if (!t3_valid_mesh(mesh) || !m || !u || !z || !d || !out) return PHASTB_ERR_ARG;
+  if (m->stress_split != PHASTB_SPLIT_ISOTROPIC && m->stress_split != PHASTB_SPLIT_LINEAR) return PHASTB_UNSUPPORTED;
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = cuda_status(cudaMemsetAsync(out, 0, sizeof(double) * (size_t)mesh->n_nodes, s));
+  if (st) return st;
+  const T3Dev t = t3_dev(*mesh);
+  const Mat2<double> mm = make_mat2<double>(*m);
+  for (int c = 0; c < mesh->n_colors; ++c) {
+    const int k0 = mesh->color_off[c], k1 = mesh->color_off[c + 1];
+    if (k1 <= k0) continue;
+    { note_launch(); t3_force_dd_t_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, mm, u, z, d, out, k0, k1); }
+  }
+  return last_launch_status();
+}
+
+int phastb_t3_damage_adjoint_grads(const phastb_t3_mesh* mesh, const double* lam, const double* d, double l0,
+                                   double* grad_gc_e, double* grad_H, double* lam_K_d_e, double* lam_M_d_e,
+                                   void* stream) {
+  if (!t3_valid_mesh(mesh) || !lam || !d || !(l0 > 0)) return PHASTB_ERR_ARG;
+  const int ne = mesh->n_elems;
+  { note_launch(); t3_damage_adjoint_kernel<<<grid_full(ne), kThreads, 0, (cudaStream_t)stream>>>(
+      t3_dev(*mesh), lam, d, l0, grad_gc_e, grad_H, lam_K_d_e, lam_M_d_e, ne); }
+  return last_launch_status();
 }
 
 }  // extern "C"

@@ -169,6 +169,18 @@ class PhaseFieldDamageSolver:
             raise RuntimeError(f"adjoint damage PCG failed (reason {int(info[1])})")
         return out
 
+    def adjoint_grads(self, lam, d, Gc_field=None, l0=None):
+        """(dJ/dGc_e (E,), dJ/dH (E, 4)) for the adjoint ``lam`` of the damage solve at ``d``."""
+        _, l0_s, *_ = self._material(None, l0, Gc_field)
+        E, dev = self.fem.n_elems, d.device
+        g_gc = torch.empty(E, dtype=torch.float64, device=dev)
+        g_h = torch.empty(E, 4, dtype=torch.float64, device=dev)
+        lam = lam.to(torch.float64).contiguous()
+        d = d.to(torch.float64).contiguous()
+        call("phastb_q4_damage_adjoint_grads", self.fem.grid, ptr(lam), ptr(d), l0_s, ptr(g_gc), ptr(g_h), None, None,
+             stream())
+        return g_gc, g_h
+
     def _solve_forward(self, H_input, d_prev, Gc=None, l0=None, Gc_field=None, pf_dirichlet_mask=None,
                        pf_dirichlet_values=None, initial_guess=None):
         self.n_solves += 1

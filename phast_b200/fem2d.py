@@ -282,6 +282,24 @@ class FEMOperators:
              None, stream())
         return H_out
 
+    # -- adjoint pieces (isotropic split) -------------------------------------------
+    def psi_grad_t(self, u, wq):
+        """sum_{e,q} wq[e,q] (d psi+_{e,q} / du): the transpose of the Gauss-point energy map, (N, 2)."""
+        u = self._check_nodal(u, 2, "u").double()
+        wq = wq.to(torch.float64).contiguous()
+        f = torch.empty_like(u)
+        call("phastb_q4_psi_grad_t", self.grid, self.mat(torch.float64), ptr(u), ptr(wq), ptr(f), stream())
+        return f
+
+    def force_dd_t(self, u, z, d):
+        """d/dd [z . f_int(u, d)], (N,)."""
+        u = self._check_nodal(u, 2, "u").double()
+        z = self._check_nodal(z, 2, "z").double()
+        d = self._check_nodal(d, 1, "d").double()
+        out = torch.empty_like(d)
+        call("phastb_q4_force_dd_t", self.grid, self.mat(torch.float64), ptr(u), ptr(z), ptr(d), ptr(out), stream())
+        return out
+
     def laplacian_matvec(self, d):
         """K_lap d (fem_operators.py:1253-1266)."""
         d = self._check_nodal(d, 1, "d").double()

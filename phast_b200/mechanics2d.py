@@ -136,6 +136,25 @@ class QuasiStaticSolver:
         self.last_backend = "cg"
         self._ws = _lib.Workspace(fem.device)
 
+    def _newton(self, d, f_ext, mask_u8, bc_vals, u, tol, cg_tol, max_iter, line_search):
+        """One device Newton-CG solve into ``u`` (FP64, contiguous); returns (status, info)."""
+        fem = self.fem
+        t3 = getattr(fem, "t3", None)
+        n = fem.n_nodes
+        info = (C.c_int * 3)()
+        lib = _lib.load()
+        if t3 is not None:
+            name, geo, wb = "phastb_t3_qs_solve", t3, lib.phastb_t3_qs_workspace_bytes(n)
+        else:
+            name, geo, wb = "phastb_q4_qs_solve", fem.grid, lib.phastb_q4_qs_workspace_bytes(n)
+        wp, wn = self._ws.get(wb)
+        st = raw(name, geo, fem.mat(torch.float64), ptr(d), ptr(f_ext), ptr(mask_u8), ptr(bc_vals), ptr(u), float(tol),
+                 float(cg_tol), self.cg_max_iter, int(max_iter), int(line_search), self.line_search_max_steps,
+                 self.line_search_min_alpha, self.line_search_c, info, wp, wn, stream())
+        if st not in (_lib.OK, _lib.NONCONVERGED, _lib.NONFINITE, _lib.BREAKDOWN):
+            _lib.check(st, name)
+        return st, info
+
     def solve(self, d, f_ext, bc_mask, bc_vals, u_init=None, rigid_connectors=None):
         """Equilibrium f_int(u, d) = f_ext; returns (u, converged, n_iter) (mechanics_solver.py:1597-1783)."""
         if rigid_connectors:
@@ -148,17 +167,28 @@ class QuasiStaticSolver:
         fe = None if f_ext is None else f_ext.to(torch.float64).contiguous()
         mask = bc_mask.to(torch.uint8).contiguous()
         vals = bc_vals.to(torch.float64).contiguous()
-        info = (C.c_int * 3)()
-        wp, wn = self._ws.get(_lib.load().phastb_q4_qs_workspace_bytes(n))
-        st = raw("phastb_q4_qs_solve", fem.grid, fem.mat(torch.float64), ptr(dd), ptr(fe), ptr(mask), ptr(vals),
-                 ptr(u), self.tol, self.cg_tol, self.cg_max_iter, self.max_iter, int(self.line_search),
-                 self.line_search_max_steps, self.line_search_min_alpha, self.line_search_c, info, wp, wn, stream())
-        if st not in (_lib.OK, _lib.NONCONVERGED, _lib.NONFINITE, _lib.BREAKDOWN):
-            _lib.check(st, "phastb_q4_qs_solve")
+        _, info = self._newton(dd, fe, mask, vals, u, self.tol, self.cg_tol, self.max_iter, self.line_search)
         self.last_iter = int(info[0])
         self.last_cg_iters = int(info[2])
         converged = bool(info[1])
         return u.to(d.dtype if d.dtype.is_floating_point else torch.float64), converged, int(info[0])
+
+    def solve_stiffness(self, d, rhs, bc_mask, rtol=1e-12, max_refine=30):
+        """z with K(d)_ff z_f = rhs_f and z = 0 on prescribed dofs, to a residual of ``rtol``
+        relative to |rhs_f| (the Newton entry with zero prescribed values and no line search:
+        one CG solve plus refinement steps).  The adjoint of the equilibrium solve."""
+        mask = bc_mask.to(device=self.fem.device, dtype=torch.uint8).contiguous()
+        r = rhs.to(torch.float64) * (mask == 0).to(torch.float64)
+        r = r.contiguous()
+        z = torch.zeros_like(r)
+        nrm = float(torch.linalg.vector_norm(r))
+        if nrm == 0.0:
+            return z
+        dd = d.to(torch.float64).contiguous()
+        st, info = self._newton(dd, r, mask, torch.zeros_like(r), z, rtol * nrm, 1e-10, max_refine, False)
+        if st != _lib.OK or not info[1]:
+            raise RuntimeError(f"stiffness solve did not converge (status {st}, {int(info[0])} refinements)")
+        return z
 
 
 class _ExplicitRollout(torch.autograd.Function):

@@ -130,11 +130,13 @@ class StaggeredSolver:
             raise NotImplementedError(f"solver_type {cfg.solver_type!r} is not implemented by the B200 backend")
         N, E = fem.n_nodes, fem.n_elems
         z = lambda *s: torch.zeros(*s, dtype=self.dtype, device=self.device)
+        # history per Gauss point: four per Q4 element, one per T3 element
+        hq = (E,) if getattr(fem, "t3", None) is not None else (E, 4)
         self.u, self.v, self.a = z(N, 2), z(N, 2), z(N, 2)
         self.d = torch.zeros(N, dtype=torch.float64, device=self.device)
-        self.H_elem = z(E, 4)
+        self.H_elem = z(*hq)
         self.f_ext = z(N, 2)
-        self._nxt = [z(N, 2), z(N, 2), z(N, 2), z(E, 4)]
+        self._nxt = [z(N, 2), z(N, 2), z(N, 2), z(*hq)]
         self._step_count = 0
         self._explicit_step_count = 0
         self._last_stagger_iter = 0

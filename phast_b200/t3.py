@@ -120,13 +120,38 @@ class T3FEMOperators:
         call("phastb_t3_psi_history", self.t3, self._mat, ptr(u), None, None, ptr(psi), stream())
         return psi
 
-    def psi_history(self, u, H_in=None):
+    def psi_history(self, u, H_in=None, H_out=None):
         """H_out = max(H_in, psi+(u)) per element (StaggeredSolver._H_update)."""
         u = self._nodal(u, 2, "u")
-        H = torch.empty(self.n_elems, dtype=torch.float64, device=self.device)
+        H = torch.empty(self.n_elems, dtype=torch.float64, device=self.device) if H_out is None else H_out
         hin = None if H_in is None else H_in.to(torch.float64).contiguous()
         call("phastb_t3_psi_history", self.t3, self._mat, ptr(u), ptr(hin), ptr(H), None, stream())
         return H
+
+    def compute_reaction_force(self, u, d, node_indices, component=1, f_ext=None):
+        """Sum of f_int (- f_ext) over nodes (fem_operators.py:1502-1530); returns a float."""
+        f = self.internal_force(u, d)
+        idx = torch.as_tensor(node_indices, dtype=torch.long).to(self.device)
+        r = f[idx, component].sum()
+        if f_ext is not None:
+            r = r - f_ext.to(torch.float64)[idx, component].sum()
+        return float(r)
+
+    # -- adjoint pieces (isotropic split) -------------------------------------------
+    def psi_grad_t(self, u, w):
+        """sum_e w_e (d psi+_e / du): the transpose of the element energy map, (N, 2)."""
+        u = self._nodal(u, 2, "u")
+        w = w.to(torch.float64).contiguous()
+        f = torch.empty_like(u)
+        call("phastb_t3_psi_grad_t", self.t3, self._mat, ptr(u), ptr(w), ptr(f), stream())
+        return f
+
+    def force_dd_t(self, u, z, d):
+        """d/dd [z . f_int(u, d)], (N,)."""
+        u, z, d = self._nodal(u, 2, "u"), self._nodal(z, 2, "z"), self._nodal(d, 1, "d")
+        out = torch.empty_like(d)
+        call("phastb_t3_force_dd_t", self.t3, self._mat, ptr(u), ptr(z), ptr(d), ptr(out), stream())
+        return out
 
 
 class T3DamageSolver:
@@ -169,6 +194,45 @@ class T3DamageSolver:
         call("phastb_t3_damage_apply", self.fem.t3, ptr(d), ptr(H), gco, ptr(gco_e), gcl0, ptr(gcl0_e), ptr(y),
              stream())
         return y
+
+    def _apply_full(self, H_input, x, Gc=None, l0=None, Gc_field=None):
+        """A x of the AT2 system (unmasked) with the given material overrides."""
+        return self._Ax(x.detach(), H_input.detach(), Gc, l0, Gc_field)
+
+    def linear_solve(self, H_input, rhs, Gc=None, l0=None, Gc_field=None, fixed=None, fixed_values=None, x0=None,
+                     rtol=1e-11, max_iter=None):
+        """Solve the unbounded AT2 system A x = rhs with ``fixed`` rows held at ``fixed_values``
+        (_pcg_solve_adjoint_system, damage_solver.py:423-480)."""
+        gcl0, gco, gcl0_e, gco_e = self._coeffs(Gc, l0, Gc_field)
+        H = H_input.detach().to(torch.float64).contiguous()
+        n = self.fem.n_nodes
+        r = rhs.detach().to(torch.float64).contiguous()
+        fx = None if fixed is None else fixed.to(torch.uint8).contiguous()
+        fv = None if fixed_values is None else fixed_values.detach().to(torch.float64).contiguous()
+        xi = None if x0 is None else x0.detach().to(torch.float64).contiguous()
+        out = torch.empty(n, dtype=torch.float64, device=r.device)
+        info = (C.c_int * 2)()
+        rinfo = (C.c_double * 2)()
+        wp, wn = self._ws.get(_lib.load().phastb_t3_damage_linear_workspace_bytes(n))
+        call("phastb_t3_damage_linear_solve", self.fem.t3, ptr(H), gco, ptr(gco_e), gcl0, ptr(gcl0_e), ptr(r),
+             ptr(fx), ptr(fv), ptr(xi), float(rtol), int(max_iter or max(self.max_iter, 1000)), self.check_every,
+             ptr(out), info, rinfo, wp, wn, stream())
+        self.last_linear_info = (int(info[0]), int(info[1]), float(rinfo[0]), float(rinfo[1]))
+        if info[1] not in (0, 1):
+            raise RuntimeError(f"adjoint damage PCG failed (reason {int(info[1])})")
+        return out
+
+    def adjoint_grads(self, lam, d, Gc_field=None, l0=None):
+        """(dJ/dGc_e (E,), dJ/dH_e (E,)) for the adjoint ``lam`` of the damage solve at ``d``."""
+        l0_s = self._l0 if l0 is None else float(l0)
+        E, dev = self.fem.n_elems, d.device
+        g_gc = torch.empty(E, dtype=torch.float64, device=dev)
+        g_h = torch.empty(E, dtype=torch.float64, device=dev)
+        lam = lam.to(torch.float64).contiguous()
+        d = d.to(torch.float64).contiguous()
+        call("phastb_t3_damage_adjoint_grads", self.fem.t3, ptr(lam), ptr(d), l0_s, ptr(g_gc), ptr(g_h), None, None,
+             stream())
+        return g_gc, g_h
 
     def prepare(self, H, Gc=None, l0=None, Gc_field=None):
         gcl0, gco, gcl0_e, gco_e = self._coeffs(Gc, l0, Gc_field)
