@@ -399,6 +399,99 @@ def run_2d_configs(device, flush, with_cpu):
     return out
 
 
+CFG3_INCREMENTS = 2
+
+
+def run_cfg3(device, flush, n_cells=128, increments=CFG3_INCREMENTS, per_cell=True):
+    """Bench line of cfg3: the seeded particle-in-cube batch advanced as one packed batch
+    (every cell in one launch per operator apply and per Krylov vector step), load
+    increments 1..K of every cell from the initial state, beside the same cells advanced one
+    at a time by the single-cell solver with the same algorithm."""
+    from phast_b200.solid3d import batch as bt
+    from phast_b200.solid3d.model import SolverConfig
+    from phast_b200.solid3d.staggered import MechForm, StaggeredSolver
+    peak, _ = peaks()
+    cells = bt.particle_cells(seed=0, n_cells=n_cells)
+    load = bt.batch_load()
+    ops = [bt.build_operator(c, load, device=device) for c in cells]
+    B = bt.PackedCellBatch(ops, brick=(16, 8, 8))
+    cfg = SolverConfig(kappa=ops[0].kappa)
+    solver = bt.BatchStaggeredSolver(B, load, cfg, mixed=True)
+    # warm-up increment (workspaces, captured graphs), then the timed window from the initial state
+    solver.advance(solver.initial_state(), load.targets[0])
+    torch.cuda.synchronize()
+    state = solver.initial_state()
+    total_ms, recs = 0.0, []
+    for k in range(increments):
+        flush_l2(flush)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        state, r = solver.advance(state, load.targets[k])
+        e1.record()
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        recs.append(r)
+    voxels = sum(op.n_elements for op in ops)
+    mech_its = sum(r.pcg_iters_mech for rr in recs for r in rr)
+    pf_its = sum(r.pcg_iters_pf for rr in recs for r in rr)
+    dof_updates = sum((r.pcg_iters_mech * op.n_mech + r.pcg_iters_pf * op.n_red) for rr in recs
+                      for r, op in zip(rr, ops))
+    # the batched FP32 elastic action alone (the dominant kernel of the batch), L2 flushed
+    x32 = state.x.float().contiguous()
+    d32 = state.d.float().contiguous()
+    for _ in range(3):
+        B.mech_apply(x32, d32)
+    act_ms = 0.0
+    for _ in range(10):
+        flush_l2(flush)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        B.mech_apply(x32, d32)
+        e1.record()
+        torch.cuda.synchronize()
+        act_ms += e0.elapsed_time(e1) / 10
+    act_bytes = sum(7 * op.n_red * 4 + op.n_elements for op in ops)
+    line = {"workload": f"{n_cells} seeded periodic particle-in-cube cells (edge N in {{32,40,48,56,64}}, "
+                        f"{voxels} voxels in all), eps_xx ramp 0 -> 0.015 over 40 steps; increments 1..{increments} "
+                        "of every cell as one packed batch: FP32 Jacobi PCG (FP64 dots) under FP64 refinement, "
+                        "FP64 box-KKT damage",
+            "dtype": "f32 mechanics (f64 dots, f64 refinement), f64 damage",
+            "value": n_cells * increments / (total_ms / 1e3), "unit": "cell increments/s",
+            "ms_per_batch_increment": total_ms / increments,
+            "dof_updates_per_s": dof_updates / (total_ms / 1e3),
+            "mech_iters_per_cell_increment": mech_its / (n_cells * increments),
+            "damage_pcg_iters_per_cell_increment": pf_its / (n_cells * increments),
+            "batched_action": {"kernel": "h8_tile_batch_kernel<float> (every cell in one launch)",
+                               "launch_ms": act_ms, "algorithmic_bytes": act_bytes,
+                               "achieved_GBps": act_bytes / (act_ms / 1e3) / 1e9,
+                               "hbm_frac": act_bytes / (act_ms / 1e3) / 1e9 / peak,
+                               "l2": "working set beyond the 126 MB L2"}}
+    if per_cell:
+        # the same cells one at a time (single-cell solver, same algorithm: FP32 Jacobi PCG under refinement)
+        form = MechForm(mixed=True)
+        one_ms, worst = 0.0, 0.0
+        for c, op in enumerate(ops):
+            sv = StaggeredSolver(op, cfg=cfg, form=form)
+            st1 = sv.initial_state()
+            sv.advance(st1, load.targets[0])  # warm-up of this cell's workspaces
+            st1 = sv.initial_state()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for k in range(increments):
+                st1, r1 = sv.advance(st1, load.targets[k])
+            e1.record()
+            torch.cuda.synchronize()
+            one_ms += e0.elapsed_time(e1)
+            a, b = np.asarray(recs[-1][c].macro_stress), np.asarray(r1.macro_stress)
+            worst = max(worst, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
+        line["one_cell_at_a_time"] = {"value": n_cells * increments / (one_ms / 1e3), "unit": "cell increments/s",
+                                      "ms_per_batch_increment": one_ms / increments}
+        line["speedup_vs_one_cell_at_a_time"] = one_ms / total_ms
+        line["rel_err_macro_stress_vs_one_cell_at_a_time"] = worst
+    return line
+
+
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
@@ -571,6 +664,8 @@ def run_ours(args, rank, world, device):
     }
     if not args.no_2d:
         out["configs"] = run_2d_configs(device, flush, world == 1 and rank == 0 and not args.no_cpu)
+    if args.cfg3_cells > 0:
+        out.setdefault("configs", {})["cfg3"] = run_cfg3(device, flush, n_cells=args.cfg3_cells)
     if world == 1 and rank == 0 and not args.no_cpu:
         try:
             secs, threads, recs = time_reference(args.steps, CPU_BASELINE_BUDGET_S)
@@ -710,6 +805,8 @@ def main():
     ap.add_argument("--fp32", action="store_true", help="FP32 storage/arithmetic for --kernel-only")
     ap.add_argument("--damage-cg", action="store_true", help="with --kernel-only: time box-KKT damage solves instead")
     ap.add_argument("--tile", default="", help="pin the tile shape ox,oy,kz for --kernel-only (else the solver's shape)")
+    ap.add_argument("--cfg3-cells", type=int, default=128, help="cells of the packed-batch line (0: skip it)")
+    ap.add_argument("--cfg3-only", action="store_true", help="print the packed-batch line alone")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -724,6 +821,10 @@ def main():
         return
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
+    if args.cfg3_only:
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
+        print(json.dumps(run_cfg3(device, flush, n_cells=args.cfg3_cells)), flush=True)
+        return
     if args.kernel_only:
         if args.damage_cg:
             run_damage_cg_only(args, device)

@@ -493,6 +493,79 @@ int phastb_h8_tma_staging(const phastb_voxel_grid* g, int dtype);
 int phastb_test_grid_barrier(int blocks, int skip_block, double limit_s, int* grid_error_host,
                              int* passed_host);
 
+/* ---- Packed batches of periodic voxel cells --------------------------------------------
+ * PhAST runs one cell per Problem.run (solid3d/api.py:191-233); these entry points advance
+ * many cells of different sizes together.  A batch plan fixes the cells' grids, phase-field
+ * lengths and damage-system scales (operator.py:238) and the packed layout: cell c's reduced
+ * nodes, mechanics unknowns [u~ (3 n_red), E (6)] and elements follow those of cells
+ * 0..c-1.  Each Krylov iteration is one launch per operator apply and per vector step over
+ * every cell (one block per brick of a cell, one per chunk of a cell's vector), with every
+ * cell's solver state and stopping rule on the device, as the single-cell solves above. */
+typedef struct phastb_batch phastb_batch;
+
+/* Host plan of n_cells cells (NULL on bad arguments): bricks of ox x oy nodes (16 x 8 or
+ * 8 x 8) and kz node layers, at most 1184 bricks per cell.  ell and dscale: per cell. */
+phastb_batch* phastb_batch_create(int n_cells, const phastb_voxel_grid* grids, const double* ell,
+                                  const double* dscale, int ox, int oy, int kz);
+void phastb_batch_destroy(phastb_batch* batch);
+
+/* out[0..6] = packed nodes, mechanics unknowns, elements, brick blocks, bytes of the device
+ * tables (phastb_batch_bind), mechanics chunks, node chunks; then per cell c
+ * out[7 + 3c .. 9 + 3c] = its node, mechanics and element offsets. */
+int phastb_batch_sizes(const phastb_batch* batch, long long* out);
+
+/* Copies the plan's tables into the caller's device buffer (out[4] bytes), which must stay
+ * allocated while the plan is used; synchronises `stream`. */
+int phastb_batch_bind(phastb_batch* batch, void* tables, size_t bytes, void* stream);
+
+/* Batched elastic action y = A(d) x of every cell (mech_action, operator.py:1108-1194);
+ * rE_out (host, 6 per cell, may be NULL) receives each cell's macro-stress row sums. */
+size_t phastb_batch_apply_workspace_bytes(const phastb_batch* batch);
+int phastb_batch_mech_apply(const phastb_batch* batch, const phastb_voxel_material* m, const uint8_t* slot,
+                            int dtype, const void* x, const void* d, const uint8_t* mask, void* y,
+                            double* rE_out, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Batched damage action of every cell, scaled by each cell's dscale when `scaled`
+ * (damage_action, operator.py:1450-1466). */
+int phastb_batch_damage_apply(const phastb_batch* batch, const phastb_voxel_material* m, const uint8_t* slot,
+                              const double* d, const double* H, int scaled, const uint8_t* mask, double* y,
+                              void* workspace, size_t workspace_bytes, void* stream);
+
+/* Constrained mechanics solve of every cell (solve_constrained, solid3d/linalg.py:223-287):
+ * Jacobi PCG in FP64 (mixed = 0) or FP32 inner PCG with FP64 dot products under FP64
+ * iterative refinement (mixed = 1, after mixed_precision_cg.py:18-95), each cell stopped on
+ * its FP64 residual ||r|| <= max(rtol ||b_f||, atol).  info[2c] iterations, info[2c+1]
+ * converged; rinfo[2c] ||b_f||, rinfo[2c+1] final ||r||.  live_host (host, one int per cell,
+ * NULL: every cell) selects the cells solved; the others keep x0 in x_out.  Returns the first
+ * failing cell's status (PHASTB_OK when every cell converged). */
+size_t phastb_batch_mech_solve_workspace_bytes(const phastb_batch* batch, int mixed);
+int phastb_batch_mech_solve(const phastb_batch* batch, const phastb_voxel_material* m, const uint8_t* slot,
+                            const double* d, const uint8_t* fixed, const double* fixed_values, const double* x0,
+                            double rtol, double atol, int maxiter, int check_every, int mixed, double inner_rtol,
+                            int max_refine, const int* live_host, double* x_out, int* info, double* rinfo,
+                            void* workspace, size_t workspace_bytes, void* stream);
+
+/* Box-constrained damage solve of every cell's scaled system (solve_h8_scalar_box_kkt,
+ * solvers/box_kkt_h8.py:256-778).  tol_rule = 1 sets each cell's linear tolerance as the
+ * staggered solver does, max(min(lin_tol, 0.1 kkt_tol / max(r0, 1)), min_tol) with r0 the
+ * residual of `initial` (StaggeredSolver._damage, solid3d/staggered.py:753-800); 0 uses
+ * lin_tol.  info[4c..4c+3] = PCG iterations, active-set iterations, kkt_ok, status;
+ * rinfo[2c], rinfo[2c+1] = r0 and the tolerance used (rinfo may be NULL).  live_host as for
+ * phastb_batch_mech_solve; cells not solved return `initial` in d_out. */
+size_t phastb_batch_box_kkt_workspace_bytes(const phastb_batch* batch);
+int phastb_batch_damage_box_kkt(const phastb_batch* batch, const phastb_voxel_material* m, const uint8_t* slot,
+                                const double* H, const double* lower, double upper, const double* initial,
+                                double lin_tol, double kkt_tol, double min_tol, int tol_rule, int max_lin,
+                                int max_active, const int* live_host, double* d_out, int* info, double* rinfo,
+                                void* workspace, size_t workspace_bytes, void* stream);
+
+/* Staggered change parts of every cell, out_host[5c..5c+4] = ||du~||, ||u~||, max|dE|,
+ * max|E|, max|dd| (StaggeredSolver._change, solid3d/staggered.py:1097-1124). */
+size_t phastb_batch_change_workspace_bytes(const phastb_batch* batch);
+int phastb_batch_stagger_change(const phastb_batch* batch, const double* x_new, const double* x_old,
+                                const double* d_new, const double* d_old, double* out_host, void* workspace,
+                                size_t workspace_bytes, void* stream);
+
 /* Library version string (host pointer). */
 const char* phastb_version(void);
 

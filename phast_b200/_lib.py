@@ -137,6 +137,21 @@ SIGNATURES = {
     "phastb_scale_set": (C.c_int, [C.c_int, vp, C.c_double, C.c_int, C.c_double, vp, vp]),
     "phastb_test_grid_barrier": (C.c_int, [C.c_int, C.c_int, C.c_double, ip, ip]),
     "phastb_h8_tma_staging": (C.c_int, [VG, C.c_int]),
+    "phastb_batch_create": (vp, [C.c_int, VG, dp, dp, C.c_int, C.c_int, C.c_int]),
+    "phastb_batch_destroy": (None, [vp]),
+    "phastb_batch_sizes": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
+    "phastb_batch_bind": (C.c_int, [vp, vp, sz, vp]),
+    "phastb_batch_apply_workspace_bytes": (sz, [vp]),
+    "phastb_batch_mech_apply": (C.c_int, [vp, VM, vp, C.c_int, vp, vp, vp, vp, dp, vp, sz, vp]),
+    "phastb_batch_damage_apply": (C.c_int, [vp, VM, vp, vp, vp, C.c_int, vp, vp, vp, sz, vp]),
+    "phastb_batch_mech_solve_workspace_bytes": (sz, [vp, C.c_int]),
+    "phastb_batch_mech_solve": (C.c_int, [vp, VM, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_int,
+                                          C.c_int, C.c_double, C.c_int, ip, vp, ip, dp, vp, sz, vp]),
+    "phastb_batch_box_kkt_workspace_bytes": (sz, [vp]),
+    "phastb_batch_damage_box_kkt": (C.c_int, [vp, VM, vp, vp, vp, C.c_double, vp, C.c_double, C.c_double,
+                                              C.c_double, C.c_int, C.c_int, C.c_int, ip, vp, ip, dp, vp, sz, vp]),
+    "phastb_batch_change_workspace_bytes": (sz, [vp]),
+    "phastb_batch_stagger_change": (C.c_int, [vp, vp, vp, vp, vp, dp, vp, sz, vp]),
 }
 RECORD_WORDS = 27
 

@@ -94,6 +94,19 @@ __device__ __forceinline__ bool arrive_last(unsigned int* counter) {
   return last;
 }
 
+// arrive_last for a group of `count` blocks sharing one ticket (the blocks of
+// one cell in a batched launch).
+__device__ __forceinline__ bool arrive_last_n(unsigned int* counter, int count) {
+  __shared__ unsigned int s_ticket_n;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_ticket_n = atomicAdd(counter, 1u);
+  __syncthreads();
+  const bool last = (s_ticket_n == (unsigned)count - 1u);
+  if (last) __threadfence();
+  return last;
+}
+
 // Fold `n` partials (global) in a fixed order inside the last block.
 __device__ __forceinline__ double fold_sum(const double* part, int n, double* sh) {
   double v = 0.0;

@@ -283,10 +283,11 @@ __device__ __forceinline__ T g_deg(T kappa, T d) {
 // mbarrier per layer buffer; halo nodes that wrap around a periodic edge read
 // the zero fill and are patched by per-thread loads.  Otherwise every thread
 // stages its (at most two) halo-tile nodes through registers.
+// The action over the bricks vb, vb + vgrid, ... of one grid: a plain launch runs it with
+// its block index and grid size, a batched launch with the block's virtual index inside its cell.
 template <typename T, int COEF, int MODE, int OX, int OY, bool TMA>
-__global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
-    h8_tile_kernel(TileArgs<T> a, VoxMat<T> m, const __grid_constant__ CUtensorMap tmx,
-                   const __grid_constant__ CUtensorMap tmd) {
+__device__ __forceinline__ void tile_body(const TileArgs<T>& a, const VoxMat<T>& m, const CUtensorMap* tmx,
+                                          const CUtensorMap* tmd, const int vb, const int vgrid) {
   if (a.guard && *a.guard == 0) return;
   constexpr bool SLOT = COEF != kCoefQP;
   constexpr bool DOT = MODE == kModeDot, ENERGY = MODE == kModeEnergy, CHEB = MODE == kModeCheb;
@@ -297,7 +298,7 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
   constexpr bool RED = EROWS || DOT || ENERGY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const VoxGeom& g = a.g;
-  if (NODAL && blockIdx.x == 0 && threadIdx.x < 6 && a.y) a.y[3 * (size_t)g.n_red + threadIdx.x] = T(0);
+  if (NODAL && vb == 0 && threadIdx.x < 6 && a.y) a.y[3 * (size_t)g.n_red + threadIdx.x] = T(0);
   const T* __restrict__ x = a.x;
   const T* __restrict__ d = SLOT ? a.d : nullptr;
   // OX, OY > 0: a compiled tile shape (constant shared-memory offsets)
@@ -377,8 +378,8 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
         const int gz = g.pz ? wrap_node(kn, g.nz, g.rz, 1) : kn;  // out of range: the zero fill
         fence_proxy_async();
         mbar_expect_tx(&s_mbar[b], tma_tx);
-        tma_load_3d(sbase + (size_t)b * xbb, &tmx, xs0, j0 - 1, gz, &s_mbar[b]);
-        if (use_d) tma_load_3d(sbase + 3 * xbb + (size_t)b * dbb, &tmd, ds0, j0 - 1, gz, &s_mbar[b]);
+        tma_load_3d(sbase + (size_t)b * xbb, tmx, xs0, j0 - 1, gz, &s_mbar[b]);
+        if (use_d) tma_load_3d(sbase + 3 * xbb + (size_t)b * dbb, tmd, ds0, j0 - 1, gz, &s_mbar[b]);
       }
     }
   };
@@ -488,7 +489,7 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
     }
   };
 
-  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+  for (int tile = vb; tile < n_tiles; tile += vgrid) {
     const int tz = tile / tiles_xy, txy = tile - tz * tiles_xy;
     const int i0 = (txy % tiles_x) * ox, j0 = (txy / tiles_x) * oy;
     const int k0 = tz * kz, k1 = min(k0 + kz, g.rz);
@@ -763,11 +764,11 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
     block_sum_multi<NK>(v, sh);
     if (tid == 0) {
 #pragma unroll
-      for (int k = 0; k < NK; ++k) a.ws.part[k * kMaxPartials + blockIdx.x] = v[k];
+      for (int k = 0; k < NK; ++k) a.ws.part[k * kMaxPartials + vb] = v[k];
     }
-    if (arrive_last(a.ws.counter)) {
+    if (arrive_last_n(a.ws.counter, vgrid)) {
       double f[NK];
-      fold_sum_multi<NK>(a.ws.part, kMaxPartials, gridDim.x, f, sh);
+      fold_sum_multi<NK>(a.ws.part, kMaxPartials, vgrid, f, sh);
       if (tid == 0) {
         double dot_e = 0.0;
 #pragma unroll
@@ -791,6 +792,13 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
   }
 }
 
+template <typename T, int COEF, int MODE, int OX, int OY, bool TMA>
+__global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
+    h8_tile_kernel(TileArgs<T> a, VoxMat<T> m, const __grid_constant__ CUtensorMap tmx,
+                   const __grid_constant__ CUtensorMap tmd) {
+  tile_body<T, COEF, MODE, OX, OY, TMA>(a, m, &tmx, &tmd, blockIdx.x, gridDim.x);
+}
+
 #include "h8_tile2.cuh"
 
 // ------------------------------------------------------------------ damage action
@@ -803,7 +811,7 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
 // return value is this thread's share of sum_n x_n y_n (with DOT).
 template <typename T, int OX, int OY, bool DOT, class NodeVal, class OnOwned>
 __device__ __forceinline__ double dtile_pass(const DTileArgs<T>& a, unsigned char* smem_raw, NodeVal node_val,
-                                             OnOwned on_owned) {
+                                             OnOwned on_owned, const int vb, const int vgrid) {
   const VoxGeom& g = a.g;
   const int ox = OX ? OX : a.ts.ox, oy = OY ? OY : a.ts.oy, kz = a.ts.kz;
   const int ex = ox + 1, exy = ex * (oy + 1);
@@ -862,7 +870,7 @@ __device__ __forceinline__ double dtile_pass(const DTileArgs<T>& a, unsigned cha
       if (t < nt) buf[t] = r[h];
     }
   };
-  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+  for (int tile = vb; tile < n_tiles; tile += vgrid) {
     const int tz = tile / tiles_xy, txy = tile - tz * tiles_xy;
     const int i0 = (txy % tiles_x) * ox, j0 = (txy / tiles_x) * oy;
     const int k0 = tz * kz, k1 = min(k0 + kz, g.rz);
@@ -975,26 +983,31 @@ void damage_slot_coefs(DTileArgs<T>& a, const VoxMat<T>& m) {
 
 // The damage action as its own launch (MODE == kModeDot also x . y into ws.out[kOutDot]).
 template <typename T, int MODE, int OX, int OY>
-__global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_kernel(DTileArgs<T> a) {
+__device__ __forceinline__ void dtile_body(const DTileArgs<T>& a, const int vb, const int vgrid) {
   if (a.guard && *a.guard == 0) return;
   constexpr bool DOT = MODE == kModeDot;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const T* __restrict__ x = a.x;
   T* __restrict__ y = a.y;
   const double accd = dtile_pass<T, OX, OY, DOT>(
-      a, smem_raw, [&](size_t n) { return __ldg(x + n); }, [&](size_t n, T, T v) { y[n] = v; });
+      a, smem_raw, [&](size_t n) { return __ldg(x + n); }, [&](size_t n, T, T v) { y[n] = v; }, vb, vgrid);
   if constexpr (DOT) {
     __shared__ double sh[32];
     const double sm = block_sum(accd, sh);
-    if (threadIdx.x == 0) a.ws.part[kOutDot * kMaxPartials + blockIdx.x] = sm;
-    if (arrive_last(a.ws.counter)) {
-      const double t = fold_sum(a.ws.part + kOutDot * kMaxPartials, gridDim.x, sh);
+    if (threadIdx.x == 0) a.ws.part[kOutDot * kMaxPartials + vb] = sm;
+    if (arrive_last_n(a.ws.counter, vgrid)) {
+      const double t = fold_sum(a.ws.part + kOutDot * kMaxPartials, vgrid, sh);
       if (threadIdx.x == 0) {
         a.ws.out[kOutDot] = t;
         *a.ws.counter = 0u;
       }
     }
   }
+}
+
+template <typename T, int MODE, int OX, int OY>
+__global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_kernel(DTileArgs<T> a) {
+  dtile_body<T, MODE, OX, OY>(a, blockIdx.x, gridDim.x);
 }
 
 // ------------------------------------------------------- persistent damage PCG
@@ -1090,7 +1103,8 @@ __global__ void __launch_bounds__(kTileMaxThreads, 2) h8_damage_pcg_kernel(DTile
         [&](size_t i, T pn, T v) {
           c.Ap[i] = v;
           p_dst[i] = pn;
-        });
+        },
+        blockIdx.x, gridDim.x);
     pap = block_sum(pap, sh);
     if (tid == 0) c.part[blockIdx.x] = pap;
     if (!grid_barrier(c.st, gen)) return;
@@ -1844,6 +1858,159 @@ template int h8_damage_pcg_launch<double>(const VoxGeom&, const VoxMat<double>&,
 template int h8_damage_pcg_launch<float>(const VoxGeom&, const VoxMat<float>&, const uint8_t*, const float*,
                                          double, const uint8_t*, const PcgWs<float>&, float*, float*, const float*,
                                          int, int, cudaStream_t);
+// ------------------------------------------------------------ packed cell batches
+
+template <typename T>
+__device__ __forceinline__ TileK<T> batch_k(const BatchCell& c) {
+  if constexpr (sizeof(T) == 4)
+    return c.kf;
+  else
+    return c.kd;
+}
+
+// One brick of one cell per block: the block builds its cell's arguments in shared
+// memory and runs the single-grid tile body with its brick index inside the cell.
+template <typename T, int MODE, int OX, int OY>
+__global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
+    h8_tile_batch_kernel(TileBatchArgs<T> b, VoxMat<T> m) {
+  __shared__ TileArgs<T> sa;
+  const int2 wk = b.work[blockIdx.x];
+  const BatchCell& c = b.cells[wk.x];
+  if (threadIdx.x == 0) {
+    TileArgs<T> a;
+    a.g = c.g;
+    a.ts = c.ts;
+    a.pad_ = 0;
+    a.slot = b.slot + c.elem_off;
+    a.gq = nullptr;
+    a.d = b.d ? b.d + c.node_off : nullptr;
+    a.lam_q = nullptr;
+    a.mu_q = nullptr;
+    a.x = b.x + c.mech_off;
+    a.y = b.y ? b.y + c.mech_off : nullptr;
+    a.mask = b.mask ? b.mask + c.mech_off : nullptr;
+    a.res = nullptr;
+    a.invd = nullptr;
+    a.xs = nullptr;
+    a.d_out = nullptr;
+    a.c1 = 0.0;
+    a.c2 = 0.0;
+    a.ws = red_ws(b.ws + (size_t)wk.x * red_ws_bytes());
+    a.guard = b.guard ? b.guard + (size_t)wk.x * b.guard_stride : nullptr;
+    a.k = batch_k<T>(c);
+    sa = a;
+  }
+  __syncthreads();
+  tile_body<T, kCoefIso, MODE, OX, OY, false>(sa, m, nullptr, nullptr, wk.y, c.nvb);
+}
+
+template <typename T, int MODE, int OX, int OY>
+__global__ void __launch_bounds__(kTileMaxThreads, 2) h8_dtile_batch_kernel(TileBatchArgs<T> b, VoxMat<T> m) {
+  __shared__ DTileArgs<T> sa;
+  const int2 wk = b.work[blockIdx.x];
+  const BatchCell& c = b.cells[wk.x];
+  if (threadIdx.x == 0) {
+    DTileArgs<T> a;
+    a.g = c.g;
+    a.ts = c.ts;
+    a.pad_ = 0;
+    a.slot = b.slot + c.elem_off;
+    // per-slot factors in the order of damage_slot_coefs (same bits as a single-cell launch)
+    const T w = T(c.g.w), ell = T(c.ell);
+    for (int i = 0; i < PHASTB_MAX_SLOTS; ++i) {
+      const T gc = m.Gc[i];
+      a.gc_ell[i] = gc / ell;
+      a.gc_k2[i] = T(2) * w * gc * ell;
+    }
+    a.kappa = b.kappa;
+    a.ell = c.ell;
+    a.scale = b.dscale ? c.dscale : 1.0;
+    a.H = b.H ? b.H + 8 * c.elem_off : nullptr;
+    a.x = b.x + c.node_off;
+    a.y = b.y + c.node_off;
+    a.mask = b.mask ? b.mask + c.node_off : nullptr;
+    a.ws = red_ws(b.ws + (size_t)wk.x * red_ws_bytes());
+    a.guard = b.guard ? b.guard + (size_t)wk.x * b.guard_stride : nullptr;
+    a.k = batch_k<T>(c);
+    sa = a;
+  }
+  __syncthreads();
+  dtile_body<T, MODE, OX, OY>(sa, wk.y, c.nvb);
+}
+
+namespace {
+
+template <class K>
+int batch_smem_attr(K kern, size_t smem) {
+  static std::mutex mu;
+  static std::map<const void*, size_t> set;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = set.find((const void*)kern);
+  if (it != set.end() && it->second >= smem) return PHASTB_OK;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    cudaGetLastError();
+    return PHASTB_ERR_CUDA;
+  }
+  set[(const void*)kern] = smem;
+  return PHASTB_OK;
+}
+
+template <typename T, int MODE, int OX, int OY>
+int tile_batch_variant(const TileBatchArgs<T>& b, const VoxMat<T>& m, cudaStream_t s) {
+  auto kern = h8_tile_batch_kernel<T, MODE, OX, OY>;
+  size_t oq = 0, oc = 0;
+  const size_t smem = tile_layout<T>(OX, OY, false, false, &oq, &oc);
+  int st = batch_smem_attr(kern, smem);
+  if (st) return st;
+  const int threads = ((OX + 1) * (OY + 1) + 31) / 32 * 32;
+  { note_launch(); kern<<<b.n_blocks, threads, smem, s>>>(b, m); }
+  return last_launch_status();
+}
+
+template <typename T, int MODE, int OX, int OY>
+int dtile_batch_variant(const TileBatchArgs<T>& b, const VoxMat<T>& m, cudaStream_t s) {
+  auto kern = h8_dtile_batch_kernel<T, MODE, OX, OY>;
+  const int nt = (OX + 2) * (OY + 2), exy = (OX + 1) * (OY + 1);
+  const size_t smem = tile_stage_offset<T>(nt, exy, 3, 8) + sizeof(T) * 2 * kStageH * (size_t)exy;
+  int st = batch_smem_attr(kern, smem);
+  if (st) return st;
+  const int threads = ((OX + 1) * (OY + 1) + 31) / 32 * 32;
+  { note_launch(); kern<<<b.n_blocks, threads, smem, s>>>(b, m); }
+  return last_launch_status();
+}
+
+}  // namespace
+
+template <typename T>
+int h8_tile_batch_launch(const TileBatchArgs<T>& b, const VoxMat<T>& m, int mode, int ox, int oy, cudaStream_t s) {
+  if (!m.iso) return PHASTB_UNSUPPORTED;
+  if (b.n_blocks < 1) return PHASTB_OK;
+  const bool dot = mode == kModeDot;
+  if (mode != kModeApply && !dot) return PHASTB_ERR_ARG;
+  if (ox == 16 && oy == 8)
+    return dot ? tile_batch_variant<T, kModeDot, 16, 8>(b, m, s) : tile_batch_variant<T, kModeApply, 16, 8>(b, m, s);
+  if (ox == 8 && oy == 8)
+    return dot ? tile_batch_variant<T, kModeDot, 8, 8>(b, m, s) : tile_batch_variant<T, kModeApply, 8, 8>(b, m, s);
+  return PHASTB_ERR_ARG;
+}
+
+template <typename T>
+int h8_dtile_batch_launch(const TileBatchArgs<T>& b, const VoxMat<T>& m, bool dot, int ox, int oy, cudaStream_t s) {
+  if (b.n_blocks < 1) return PHASTB_OK;
+  if (ox == 16 && oy == 8)
+    return dot ? dtile_batch_variant<T, kModeDot, 16, 8>(b, m, s) : dtile_batch_variant<T, kModeApply, 16, 8>(b, m, s);
+  if (ox == 8 && oy == 8)
+    return dot ? dtile_batch_variant<T, kModeDot, 8, 8>(b, m, s) : dtile_batch_variant<T, kModeApply, 8, 8>(b, m, s);
+  return PHASTB_ERR_ARG;
+}
+
+template int h8_tile_batch_launch<double>(const TileBatchArgs<double>&, const VoxMat<double>&, int, int, int,
+                                          cudaStream_t);
+template int h8_tile_batch_launch<float>(const TileBatchArgs<float>&, const VoxMat<float>&, int, int, int,
+                                         cudaStream_t);
+template int h8_dtile_batch_launch<double>(const TileBatchArgs<double>&, const VoxMat<double>&, bool, int, int,
+                                           cudaStream_t);
+
 template TileArgs<double> tile_args<double>(const VoxGeom&, int);
 template TileArgs<float> tile_args<float>(const VoxGeom&, int);
 template int h8_tile_launch<double>(const TileArgs<double>&, const VoxMat<double>&, int, int, cudaStream_t, bool);

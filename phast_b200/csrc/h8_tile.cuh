@@ -212,6 +212,58 @@ int h8_mech_tile_launch(const VoxGeom& v, const VoxMat<T>& m, const uint8_t* slo
 template <typename T>
 TileArgs<T> tile_args(const VoxGeom& v, int cls);
 
+// ------------------------------------------------------------ packed cell batches
+//
+// Many periodic cells of different sizes in one launch: every block runs one
+// brick of one cell (the same tile body as a single-grid launch, with the
+// brick's index inside its cell), and each cell's reductions go to its own
+// workspace with its own ticket, folded by the cell's last block.
+
+// One cell of a packed batch: its grid, its brick schedule (the batch's ox x oy
+// bricks, kz node layers deep, nvb bricks), the offsets of its data in the
+// packed arrays (reduced nodes; mechanics unknowns, 3 n_red + 6 per cell;
+// elements) and its phase-field length and damage-system scale.
+struct BatchCell {
+  VoxGeom g;
+  TileShape ts;
+  int nvb;
+  long long node_off, mech_off, elem_off;
+  double ell, dscale;
+  TileK<float> kf;
+  TileK<double> kd;
+};
+
+// A batched launch over the packed arrays.  Per block work[b] = (cell, brick);
+// cell c's reductions use the workspace at ws + c * red_ws_bytes(); its guard
+// word (an engine's `active` flag; null: none) is guard[c * guard_stride].
+template <typename T>
+struct TileBatchArgs {
+  const BatchCell* cells;
+  const int2* work;
+  int n_blocks;
+  int guard_stride;
+  const uint8_t* slot;  // elements
+  const T* d;           // nodes (null: g = 1)
+  const T* H;           // damage action: (E, 8) per element (null: no history term)
+  const T* x;           // elastic action: mechanics vector; damage action: nodes
+  T* y;
+  const uint8_t* mask;  // like x (null: none)
+  char* ws;
+  const int* guard;
+  double kappa;         // damage action
+  int dscale;           // damage action: 1 scales it by each cell's damage-system scale
+  int pad_;
+};
+
+// y = A(d) x on every cell of the batch (MODE kModeApply or kModeDot: also
+// x . y per cell at ws_c.out[kOutDot]; the E-row sums at ws_c.out[0..5]).
+template <typename T>
+int h8_tile_batch_launch(const TileBatchArgs<T>& b, const VoxMat<T>& m, int mode, int ox, int oy, cudaStream_t s);
+
+// The damage action of every cell (dot: x . y per cell at ws_c.out[kOutDot]).
+template <typename T>
+int h8_dtile_batch_launch(const TileBatchArgs<T>& b, const VoxMat<T>& m, bool dot, int ox, int oy, cudaStream_t s);
+
 // Launches the tile kernel for (COEF, MODE) with prepared arguments.  With
 // `tune` and PHASTB_AUTOTUNE=1 in the environment, the first plain or dot
 // launch for a grid with no recorded shape (outside stream capture, unguarded)

@@ -6,7 +6,7 @@ namespace phastb {
 
 constexpr int kRedMaxK = 16;
 
-inline size_t align_up(size_t b, size_t a = 256) { return (b + a - 1) / a * a; }
+__host__ __device__ inline size_t align_up(size_t b, size_t a = 256) { return (b + a - 1) / a * a; }
 
 struct RedWs {
   double* part;       // kRedMaxK * kMaxPartials
@@ -14,11 +14,11 @@ struct RedWs {
   double* out;        // kRedMaxK results
 };
 
-inline size_t red_ws_bytes() {
+__host__ __device__ inline size_t red_ws_bytes() {
   return align_up(sizeof(double) * kRedMaxK * kMaxPartials) + 256 + align_up(sizeof(double) * kRedMaxK);
 }
 
-inline RedWs red_ws(void* base) {
+__host__ __device__ inline RedWs red_ws(void* base) {
   char* p = static_cast<char*>(base);
   RedWs w;
   w.part = reinterpret_cast<double*>(p);

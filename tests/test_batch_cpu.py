@@ -84,3 +84,36 @@ def test_gather_records_two_ranks_gloo():
     assert [r[0] for r in res] == list(range(n_cells))
     for idx, n, s, rank in res:
         assert n == cells[idx].n and s == float(cells[idx].phase.sum()) and rank == owner[idx]
+
+
+def test_packed_batch_plan_without_gpu():
+    """The host plan of a packed batch: packed offsets per cell, brick counts, and refusals."""
+    import ctypes as C
+
+    from phast_b200 import _lib
+    lib = _lib.load()
+    shapes = [(32, 32, 32), (40, 40, 40), (16, 24, 8)]
+    grids = (_lib.VoxelGrid * 3)(*[_lib.VoxelGrid(nx, ny, nz, 1, 1, 1, 1.0 / nx, 1.0 / ny, 1.0 / nz)
+                                   for nx, ny, nz in shapes])
+    ell = (C.c_double * 3)(0.1, 0.05, 0.2)
+    ds = (C.c_double * 3)(1.0, 2.0, 3.0)
+    h = lib.phastb_batch_create(3, grids, ell, ds, 8, 8, 4)
+    assert h
+    try:
+        out = (C.c_longlong * (7 + 9))()
+        assert lib.phastb_batch_sizes(C.c_void_p(h), out) == 0
+        n_red = [nx * ny * nz for nx, ny, nz in shapes]
+        assert out[0] == sum(n_red) and out[1] == sum(3 * n + 6 for n in n_red) and out[2] == sum(n_red)
+        bricks = sum(-(-nx // 8) * -(-ny // 8) * -(-nz // 4) for nx, ny, nz in shapes)
+        assert out[3] == bricks
+        offs = [tuple(out[7 + 3 * c:10 + 3 * c]) for c in range(3)]
+        assert offs[0] == (0, 0, 0)
+        assert offs[1] == (n_red[0], 3 * n_red[0] + 6, n_red[0])
+        assert offs[2] == (n_red[0] + n_red[1], 3 * (n_red[0] + n_red[1]) + 12, n_red[0] + n_red[1])
+    finally:
+        lib.phastb_batch_destroy(C.c_void_p(h))
+    # an unsupported brick shape, a brick deeper than a cell, a non-positive scale: no plan
+    assert not lib.phastb_batch_create(3, grids, ell, ds, 32, 4, 4)
+    assert not lib.phastb_batch_create(3, grids, ell, ds, 8, 8, 16)
+    bad = (C.c_double * 3)(1.0, 0.0, 3.0)
+    assert not lib.phastb_batch_create(3, grids, ell, bad, 8, 8, 4)
