@@ -400,6 +400,107 @@ def run_2d_configs(device, flush, with_cpu):
 
 
 CFG3_INCREMENTS = 2
+CFG4 = dict(CFG0, nx=256, ny=256)
+CFG4_STEPS, CFG4_TOTAL, CFG4_CHECKPOINT = 10, 50, 10
+
+
+def lognormal_gc(nx, ny, mean=2.7, cov=0.2, corr=4.0, seed=0):
+    """Seeded lognormal per-element Gc field (element e = j nx + i): a Gaussian field with a
+    squared-exponential correlation of length ``corr`` elements (white noise filtered in Fourier
+    space), mapped to the lognormal with the given mean and coefficient of variation."""
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((ny, nx))
+    kx, ky = np.fft.fftfreq(nx), np.fft.fftfreq(ny)
+    spec = np.exp(-2.0 * np.pi ** 2 * corr ** 2 * (kx[None, :] ** 2 + ky[:, None] ** 2))
+    g = np.real(np.fft.ifft2(np.fft.fft2(w) * np.sqrt(spec)))
+    g = (g - g.mean()) / g.std()
+    s2 = np.log1p(cov ** 2)
+    return np.exp(np.log(mean) - 0.5 * s2 + np.sqrt(s2) * g).reshape(-1)
+
+
+def run_cfg4(device, steps=CFG4_STEPS):
+    """Bench line of cfg4: d(peak reaction)/d(Gc field) of the 256 x 256 SENT run through the
+    hand-written reverse pass (checkpoint every 10 load steps), on load steps 1..steps of 50."""
+    import phast_b200 as pb
+    from phast_b200.adjoint2d import PeakReactionGradient
+    load = lambda k: 0.007 * k / CFG4_TOTAL  # noqa: E731
+    gc = torch.as_tensor(lognormal_gc(CFG4["nx"], CFG4["ny"]), device=device)
+    # warm-up on two steps (workspaces), then the timed forward and gradient from the initial state
+    s, sm, bcs = sent_problem(pb, CFG4, device=device)
+    # adjoint stiffness and damage solves to 1e-8 relative: the cracked 256 x 256 stiffness (residual
+    # stiffness 1e-8 on the notch) does not reach 1e-10 within the stiffness solve's refinement budget
+    rtol = 1e-8
+    PeakReactionGradient(s, sm.node_sets["top"], load, 2, checkpoint_every=CFG4_CHECKPOINT,
+                         adjoint_rtol=rtol).gradient(gc)
+    s, sm, bcs = sent_problem(pb, CFG4, device=device)
+    pr = PeakReactionGradient(s, sm.node_sets["top"], load, steps, checkpoint_every=CFG4_CHECKPOINT,
+                              adjoint_rtol=rtol)
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    pr.forward(gc)
+    e1.record()
+    res = pr.gradient(gc)
+    e2.record()
+    torch.cuda.synchronize()
+    fwd_ms, grad_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    g = res.grad
+    return {"workload": f"2D quasi-static SENT, Q4 256x256, isotropic split, lognormal Gc field (mean 2.7, CoV 0.2, "
+                        f"correlation 4 elements, seed 0); d(peak reaction)/d(Gc) over load steps 1..{steps} of "
+                        f"{CFG4_TOTAL}, checkpoint every {CFG4_CHECKPOINT}",
+            "dtype": "f64 (forward and adjoint)", "adjoint_rtol": rtol, "value": steps / (grad_ms / 1e3),
+            "unit": "load steps/s (forward with checkpoints + reverse pass)", "gradient_ms": grad_ms,
+            "forward_only_ms": fwd_ms, "gradient_over_forward": grad_ms / fwd_ms,
+            "objective": float(res.objective), "peak_step": int(res.peak_step),
+            "staggered_passes": [int(v) for v in res.passes][:steps],
+            "grad_norm": float(torch.linalg.vector_norm(g)), "grad_finite": bool(torch.isfinite(g).all()),
+            "check": "central differences (1e-4 relative) and PhAST's autograd gradient in tests/test_gpu_adjoint_qs.py"}
+
+
+def run_cfg3_action(device, flush, n_cells=16, brick=(16, 8, 8)):
+    """Profiling case of the packed batch: the batched FP32 elastic action of the seeded cells alone,
+    beside the same cells' single-cell actions (device time per launch, L2 flushed before each)."""
+    from phast_b200.solid3d import batch as bt
+    cells = bt.particle_cells(seed=0, n_cells=n_cells)
+    load = bt.batch_load()
+    ops = [bt.build_operator(c, load, device=device) for c in cells]
+    B = bt.PackedCellBatch(ops, brick=brick)
+    rng = np.random.default_rng(1)
+    x = torch.as_tensor(rng.normal(size=B.n_mech) * 1e-3, device=device).float()
+    d = torch.as_tensor(rng.uniform(0, 0.9, size=B.n_nodes), device=device).float()
+
+    def timed(fn, n=5):
+        for _ in range(3):
+            fn()
+        ms = 0.0
+        for _ in range(n):
+            flush_l2(flush)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1) / n
+        return ms
+
+    yb = torch.empty_like(x)
+    batched = timed(lambda: B.mech_apply(x, d, out=yb, macro_rows=False))
+    xs = [B.mech_view(x, c).clone() for c in range(n_cells)]
+    dsv = [B.node_view(d, c).clone() for c in range(n_cells)]
+    ys = [torch.empty_like(v) for v in xs]
+
+    def singles():
+        for op, xv, dv, yv in zip(ops, xs, dsv, ys):
+            op.mech_action(xv, d=dv, out=yv)
+
+    single = timed(singles)
+    peak, _ = peaks()
+    nbytes = sum(7 * op.n_red * 4 + op.n_elements for op in ops)
+    return {"workload": f"batched FP32 elastic action of {n_cells} particle-in-cube cells "
+                        f"({sum(op.n_elements for op in ops)} voxels), bricks {brick}",
+            "batched_ms": batched, "one_launch_per_cell_ms": single, "algorithmic_bytes": nbytes,
+            "batched_GBps": nbytes / (batched / 1e3) / 1e9, "hbm_frac": nbytes / (batched / 1e3) / 1e9 / peak,
+            "blocks": B.n_blocks}
 
 
 def run_cfg3(device, flush, n_cells=128, increments=CFG3_INCREMENTS, per_cell=True):
@@ -439,14 +540,15 @@ def run_cfg3(device, flush, n_cells=128, increments=CFG3_INCREMENTS, per_cell=Tr
     # the batched FP32 elastic action alone (the dominant kernel of the batch), L2 flushed
     x32 = state.x.float().contiguous()
     d32 = state.d.float().contiguous()
+    y32 = torch.empty_like(x32)
     for _ in range(3):
-        B.mech_apply(x32, d32)
+        B.mech_apply(x32, d32, out=y32, macro_rows=False)
     act_ms = 0.0
     for _ in range(10):
         flush_l2(flush)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        B.mech_apply(x32, d32)
+        B.mech_apply(x32, d32, out=y32, macro_rows=False)
         e1.record()
         torch.cuda.synchronize()
         act_ms += e0.elapsed_time(e1) / 10
@@ -664,8 +766,18 @@ def run_ours(args, rank, world, device):
     }
     if not args.no_2d:
         out["configs"] = run_2d_configs(device, flush, world == 1 and rank == 0 and not args.no_cpu)
+    # the packed-batch (cfg3) and gradient (cfg4) lines; a failure there is reported in its line
+    # and does not cost the headline
     if args.cfg3_cells > 0:
-        out.setdefault("configs", {})["cfg3"] = run_cfg3(device, flush, n_cells=args.cfg3_cells)
+        try:
+            out.setdefault("configs", {})["cfg3"] = run_cfg3(device, flush, n_cells=args.cfg3_cells)
+        except Exception as exc:  # noqa: BLE001
+            out.setdefault("configs", {})["cfg3"] = {"error": f"{type(exc).__name__}: {exc}"}
+    if not args.no_2d:
+        try:
+            out.setdefault("configs", {})["cfg4"] = run_cfg4(device)
+        except Exception as exc:  # noqa: BLE001
+            out.setdefault("configs", {})["cfg4"] = {"error": f"{type(exc).__name__}: {exc}"}
     if world == 1 and rank == 0 and not args.no_cpu:
         try:
             secs, threads, recs = time_reference(args.steps, CPU_BASELINE_BUDGET_S)
@@ -807,6 +919,9 @@ def main():
     ap.add_argument("--tile", default="", help="pin the tile shape ox,oy,kz for --kernel-only (else the solver's shape)")
     ap.add_argument("--cfg3-cells", type=int, default=128, help="cells of the packed-batch line (0: skip it)")
     ap.add_argument("--cfg3-only", action="store_true", help="print the packed-batch line alone")
+    ap.add_argument("--cfg3-action", action="store_true", help="time the packed batch's elastic action alone")
+    ap.add_argument("--cfg4-only", action="store_true", help="print the gradient line (cfg4) alone")
+    ap.add_argument("--brick", default="16,8,8", help="brick ox,oy,kz of --cfg3-action")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -821,6 +936,14 @@ def main():
         return
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
+    if args.cfg4_only:
+        print(json.dumps(run_cfg4(device)), flush=True)
+        return
+    if args.cfg3_action:
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
+        brick = tuple(int(v) for v in args.brick.split(","))
+        print(json.dumps(run_cfg3_action(device, flush, n_cells=args.cfg3_cells, brick=brick)), flush=True)
+        return
     if args.cfg3_only:
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
         print(json.dumps(run_cfg3(device, flush, n_cells=args.cfg3_cells)), flush=True)

@@ -194,6 +194,14 @@ typedef struct {
   const double* areas;   /* (E,) */
 } phastb_t3_mesh;
 
+/* Host check of a T3 colouring before it is used (all HOST arrays): node ids in range,
+ * `order` a permutation of the elements, colour offsets from 0 to n_elems, and no node shared
+ * by two elements of one colour.  PHASTB_ERR_ARG otherwise.  The element kernels trust the
+ * colouring (a conflict would race); the reference assembles with scatter-adds and has no
+ * colouring, so this check has no counterpart there. */
+int phastb_t3_check_mesh(int n_nodes, int n_elems, const int* elem, const int* order, int n_colors,
+                         const int* color_off);
+
 /* Internal force at the element centroid stress of the split (d NULL: undegraded linear).
  * FEMOperators.internal_force / _assemble_force, core/fem_operators.py:598-680 */
 int phastb_t3_internal_force(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u,
@@ -558,6 +566,12 @@ int phastb_batch_damage_box_kkt(const phastb_batch* batch, const phastb_voxel_ma
                                 double lin_tol, double kkt_tol, double min_tol, int tol_rule, int max_lin,
                                 int max_active, const int* live_host, double* d_out, int* info, double* rinfo,
                                 void* workspace, size_t workspace_bytes, void* stream);
+
+/* Predictor of the next increment of every cell: x_out = factor * x with each cell's
+ * E[component] = value, and values_out (may be NULL) = 0 except each cell's E[component] =
+ * value (StaggeredSolver._predictor and mech_fixed_values, solid3d/staggered.py:1207-1213). */
+int phastb_batch_predictor(const phastb_batch* batch, const double* x, double factor, int component,
+                           double value, double* x_out, double* values_out, void* stream);
 
 /* Staggered change parts of every cell, out_host[5c..5c+4] = ||du~||, ||u~||, max|dE|,
  * max|E|, max|dd| (StaggeredSolver._change, solid3d/staggered.py:1097-1124). */

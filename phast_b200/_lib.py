@@ -150,6 +150,8 @@ SIGNATURES = {
     "phastb_batch_box_kkt_workspace_bytes": (sz, [vp]),
     "phastb_batch_damage_box_kkt": (C.c_int, [vp, VM, vp, vp, vp, C.c_double, vp, C.c_double, C.c_double,
                                               C.c_double, C.c_int, C.c_int, C.c_int, ip, vp, ip, dp, vp, sz, vp]),
+    "phastb_batch_predictor": (C.c_int, [vp, vp, C.c_double, C.c_int, C.c_double, vp, vp, vp]),
+    "phastb_t3_check_mesh": (C.c_int, [C.c_int, C.c_int, ip, ip, C.c_int, ip]),
     "phastb_batch_change_workspace_bytes": (sz, [vp]),
     "phastb_batch_stagger_change": (C.c_int, [vp, vp, vp, vp, vp, dp, vp, sz, vp]),
 }

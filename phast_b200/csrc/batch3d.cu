@@ -659,6 +659,20 @@ __global__ void __launch_bounds__(kThreads) bpcg_start_rel_kernel(BVec V, BPcg<T
   });
 }
 
+// x_out = factor x with each cell's E[comp] = value; values_out = 0 except there
+__global__ void b_predictor_kernel(BVec V, const BatchCell* cells, const double* __restrict__ x, double factor,
+                                   int comp, double value, double* __restrict__ x_out,
+                                   double* __restrict__ values_out) {
+  const BChunk ck = V.chunks[blockIdx.x];
+  const BatchCell& cl = cells[ck.cell];
+  const long long ctrl = cl.mech_off + 3LL * cl.g.n_red + comp;
+  for (int i = ck.begin + threadIdx.x; i < ck.end; i += blockDim.x) {
+    const bool c = i == ctrl;
+    x_out[i] = c ? value : factor * x[i];
+    if (values_out) values_out[i] = c ? value : 0.0;
+  }
+}
+
 // staggered change parts per cell: out[5c..5c+4] = ||du~||, ||u~||, max|dE|, max|E|, max|dd|
 __global__ void __launch_bounds__(kThreads) b_change_mech_kernel(BVec V, const BatchCell* cells,
                                                                  const double* __restrict__ xn,
@@ -1431,6 +1445,14 @@ int phastb_batch_damage_box_kkt(const phastb_batch* B, const phastb_voxel_materi
     if (code != PHASTB_OK && worst == PHASTB_OK) worst = code;
   }
   return worst;
+}
+
+int phastb_batch_predictor(const phastb_batch* B, const double* x, double factor, int component, double value,
+                           double* x_out, double* values_out, void* stream) {
+  if (!batch_ready(B) || !x || !x_out || component < 0 || component > 5) return PHASTB_ERR_ARG;
+  const BVec V = mech_vec(B);
+  { note_launch(); b_predictor_kernel<<<V.n_chunks, kThreads, 0, (cudaStream_t)stream>>>(V, B->d_cells, x, factor, component, value, x_out, values_out); }
+  return last_launch_status();
 }
 
 size_t phastb_batch_change_workspace_bytes(const phastb_batch* B) {

@@ -8,6 +8,8 @@
 // stress splits of q4_kernels.cuh, and the element-H AT2 damage system with
 // the consistent T3 mass.  C ABI in include/phastb.h.
 #include "engine.cuh"
+
+#include <vector>
 #include "q4_kernels.cuh"
 
 #include <cstring>
@@ -256,6 +258,36 @@ bool t3_valid_mesh(const phastb_t3_mesh* m) {
   return true;
 }
 
+// Host check of a colouring (host arrays): node ids in range, `order` a permutation of the
+// elements, colour offsets non-decreasing from 0 to n_elems, and no node touched twice by
+// the elements of one colour (the condition of the atomic-free scatter).
+int t3_check_mesh_host(int n_nodes, int n_elems, const int* elem, const int* order, int n_colors,
+                       const int* color_off) {
+  if (n_nodes < 1 || n_elems < 1 || n_colors < 1 || !elem || !order || !color_off) return PHASTB_ERR_ARG;
+  if (color_off[0] != 0 || color_off[n_colors] != n_elems) return PHASTB_ERR_ARG;
+  for (int c = 0; c < n_colors; ++c)
+    if (color_off[c + 1] < color_off[c]) return PHASTB_ERR_ARG;
+  for (long long i = 0; i < 3LL * n_elems; ++i)
+    if (elem[i] < 0 || elem[i] >= n_nodes) return PHASTB_ERR_ARG;
+  std::vector<int> seen_elem(n_elems, 0), last(n_nodes, -1);
+  for (int i = 0; i < n_elems; ++i) {
+    const int e = order[i];
+    if (e < 0 || e >= n_elems || seen_elem[e]) return PHASTB_ERR_ARG;
+    seen_elem[e] = 1;
+  }
+  for (int c = 0; c < n_colors; ++c) {
+    for (int i = color_off[c]; i < color_off[c + 1]; ++i) {
+      const int e = order[i];
+      for (int k = 0; k < 3; ++k) {
+        const int v = elem[3 * (size_t)e + k];
+        if (last[v] == c) return PHASTB_ERR_ARG;  // two elements of colour c share node v
+        last[v] = c;
+      }
+    }
+  }
+  return PHASTB_OK;
+}
+
 // y = A(H, Gc) d of the AT2 system; rows that ``mask`` holds fixed give 0.
 int t3_damage_apply_launch(const phastb_t3_mesh& mesh, const double* d, const double* H, double gco,
                            const double* gco_e, double gcl0, const double* gcl0_e, double* y, const int* guard,
@@ -318,6 +350,11 @@ int phastb_t3_internal_force(const phastb_t3_mesh* mesh, const phastb_q4_materia
                              const double* d, double* f, void* stream) {
   if (!t3_valid_mesh(mesh) || !m || !u || !f) return PHASTB_ERR_ARG;
   return t3_force_launch(*mesh, *m, u, d, f, nullptr, nullptr, (cudaStream_t)stream);
+}
+
+int phastb_t3_check_mesh(int n_nodes, int n_elems, const int* elem, const int* order, int n_colors,
+                         const int* color_off) {
+  return t3_check_mesh_host(n_nodes, n_elems, elem, order, n_colors, color_off);
 }
 
 int phastb_t3_psi_history(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u,

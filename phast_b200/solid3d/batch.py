@@ -330,21 +330,23 @@ class PackedCellBatch:
         return t[self.elem_off[c]:self.elem_off[c] + self.ops[c].n_elements]
 
     # -- batched operators and solves --------------------------------------------------------
-    def mech_apply(self, x, d=None, *, mask=None):
-        """y = A(d) x of every cell in one launch (FP64 or FP32, like ``x``); returns (y, rE (C, 6))."""
+    def mech_apply(self, x, d=None, *, mask=None, out=None, macro_rows=True):
+        """y = A(d) x of every cell in one launch (FP64 or FP32, like ``x``); returns (y, rE (C, 6)),
+        rE the per-cell macro-stress row sums (None with ``macro_rows=False``, which skips their
+        host read).  ``out`` receives y."""
         import ctypes as C
 
         import numpy as np
         import torch
 
         from .. import _lib
-        y = torch.empty_like(x)
-        rE = (C.c_double * (6 * self.n_cells))()
+        y = torch.empty_like(x) if out is None else out
+        rE = (C.c_double * (6 * self.n_cells))() if macro_rows else None
         dt = _lib.F64 if x.dtype == torch.float64 else _lib.F32
         wp, wn = self.workspace("apply", self._lib.phastb_batch_apply_workspace_bytes(self._h))
         _lib.call("phastb_batch_mech_apply", self._h, self.mat, _lib.ptr(self.slot), dt, _lib.ptr(x), _lib.ptr(d),
                   _lib.ptr(mask), _lib.ptr(y), rE, wp, wn, _lib.stream(self.device))
-        return y, np.array(rE[:]).reshape(self.n_cells, 6)
+        return y, (np.array(rE[:]).reshape(self.n_cells, 6) if macro_rows else None)
 
     def damage_apply(self, d, H=None, *, scaled=True, mask=None):
         """The damage action of every cell in one launch (each scaled by its damage-system scale)."""
@@ -460,9 +462,6 @@ class BatchStaggeredSolver:
         self.max_refine = int(max_refine)
         self._c = int(load.controlled)
         C_ = batch.n_cells
-        self._ctrl = torch.tensor([batch.mech_off[c] + 3 * batch.ops[c].n_red + self._c for c in range(C_)],
-                                  dtype=torch.long, device=batch.device)
-        self._zeros = torch.zeros(batch.n_mech, dtype=torch.float64, device=batch.device)
         self._max_abs_target = max(abs(float(t)) for t in load.targets)
         self._u_floor = np.array([min(op.h) * math.sqrt(3 * op.n_red) for op in batch.ops])
         self.n_attempts = 0
@@ -501,8 +500,10 @@ class BatchStaggeredSolver:
         """
         import torch
 
-        from .staggered import _MIN_LINEAR_TOLERANCE, IncrementRecord, StaggerConvergenceError
         from time import perf_counter
+
+        from .. import _lib
+        from .staggered import _MIN_LINEAR_TOLERANCE, IncrementRecord, StaggerConvergenceError
         b, cfg = self.batch, self.cfg
         C_ = b.n_cells
         t0 = perf_counter()
@@ -512,10 +513,10 @@ class BatchStaggeredSolver:
             raise ValueError(f"target {target!r} equals the current controlled strain")
         increment = state.increment + 1
         self.n_attempts += 1
-        values = self._zeros.clone()
-        values.index_fill_(0, self._ctrl, target)
-        x_old = state.x * (target / previous if previous != 0.0 else 0.0)
-        x_old.index_fill_(0, self._ctrl, target)
+        values = torch.empty(b.n_mech, dtype=torch.float64, device=b.device)
+        x_old = torch.empty_like(values)
+        _lib.call("phastb_batch_predictor", b._h, _lib.ptr(state.x), target / previous if previous != 0.0 else 0.0,
+                  self._c, target, _lib.ptr(x_old), _lib.ptr(values), _lib.stream(b.device))
         d_old = state.d.clone()
         lower = state.d
         H = state.H.clone()

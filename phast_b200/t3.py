@@ -88,6 +88,12 @@ class T3FEMOperators:
         self._elem32 = el.to(torch.int32).contiguous()
         self._order = torch.as_tensor(order.astype(np.int32), device=self.device)
         self._color_off = (C.c_int * (self.n_colors + 1))(*[int(v) for v in off])
+        # the colour kernels trust the colouring: check it once, on the host, before any launch
+        el_h = np.ascontiguousarray(el.cpu().numpy().astype(np.int32))
+        ord_h = np.ascontiguousarray(order.astype(np.int32))
+        IP = C.POINTER(C.c_int)
+        _lib.call("phastb_t3_check_mesh", self.n_nodes, self.n_elems, el_h.ctypes.data_as(IP),
+                  ord_h.ctypes.data_as(IP), self.n_colors, self._color_off)
         self.t3 = _lib.T3Mesh(self.n_nodes, self.n_elems, self.n_colors, 0, ptr(self._elem32), ptr(self._order),
                               self._color_off, ptr(self.grad_phi), ptr(self.areas))
         self._mat = q4_material_struct(material, torch.float64)

@@ -47,3 +47,39 @@ def test_colouring_is_deterministic_and_handles_shuffled_order():
     a, b = color_elements(el, nn), color_elements(el, nn)
     assert np.array_equal(a, b)
     check_colouring(el[perm], nn, color_elements(el[perm], nn))
+
+
+def test_c_abi_rejects_bad_colourings_without_gpu():
+    """phastb_t3_check_mesh accepts the package's colouring and refuses out-of-range node ids,
+    a non-permutation and two elements of one colour sharing a node."""
+    import ctypes as C
+
+    from phast_b200 import _lib
+    from phast_b200.t3 import color_elements
+    nx, ny = 6, 5
+    quads = np.array([[j * (nx + 1) + i, j * (nx + 1) + i + 1, (j + 1) * (nx + 1) + i + 1, (j + 1) * (nx + 1) + i]
+                      for j in range(ny) for i in range(nx)])
+    tri = np.concatenate([quads[:, [0, 1, 2]], quads[:, [0, 2, 3]]]).astype(np.int32)
+    n_nodes = (nx + 1) * (ny + 1)
+    colors = color_elements(tri, n_nodes)
+    order = np.argsort(colors, kind="stable").astype(np.int32)
+    nc = int(colors.max()) + 1
+    off = np.searchsorted(colors[order], np.arange(nc + 1))
+    lib = _lib.load()
+    IP = C.POINTER(C.c_int)
+
+    def check(elem, ordr, offs, n=n_nodes):
+        e = np.ascontiguousarray(elem.astype(np.int32))
+        o = np.ascontiguousarray(ordr.astype(np.int32))
+        f = (C.c_int * len(offs))(*[int(v) for v in offs])
+        return lib.phastb_t3_check_mesh(n, len(e), e.ctypes.data_as(IP), o.ctypes.data_as(IP), len(offs) - 1, f)
+
+    assert check(tri, order, off) == _lib.OK
+    bad = tri.copy()
+    bad[3, 1] = n_nodes  # node id out of range
+    assert check(bad, order, off) == _lib.ERR_ARG
+    dup = order.copy()
+    dup[1] = dup[0]  # not a permutation
+    assert check(tri, dup, off) == _lib.ERR_ARG
+    one = np.array([0, len(tri)])  # every element in one colour: neighbours share nodes
+    assert check(tri, order, one) == _lib.ERR_ARG
