@@ -283,7 +283,16 @@ int phastb_q4_reaction(const phastb_q4_grid* g, const phastb_q4_material* m, con
                        size_t workspace_bytes, void* stream);
 size_t phastb_q4_reaction_workspace_bytes(int n_nodes);
 
-/* Quasi-static Newton with matrix-free CG on K(d) du = r (isotropic split).
+/* Consistent tangent action y = d f_int(u, d)/du [du] of the material's stress split at the
+ * state u (FP64; d NULL: g = 1): the directional derivative of internal_force that
+ * QuasiStaticSolver takes by autograd JVP for the spectral, Amor and star-convex splits,
+ * mechanics_solver.py:1705-1733, 2000-2012.  For the linear splits it equals the force of du;
+ * for the stress-spectral split it returns the force of du (the reference's linearisation). */
+int phastb_q4_tangent_apply(const phastb_q4_grid* g, const phastb_q4_material* m, const double* u,
+                            const double* du, const double* d, double* y, void* stream);
+
+/* Quasi-static Newton with matrix-free CG on K du = r, K the consistent tangent at the
+ * iterate for the spectral, Amor and star-convex splits and K(d) itself for the linear ones.
  * QuasiStaticSolver.solve / _cg_solve / _accept_newton_step,
  * mechanics_solver.py:1597-1831, 1984-2043.  info[0] = Newton iterations,
  * info[1] = converged, info[2] = total CG iterations. */

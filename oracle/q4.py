@@ -142,6 +142,78 @@ def _ezz(mat, tr2):
     return -mat.nu / (1.0 - mat.nu) * tr2 if mat.plane_stress else 0.0 * tr2
 
 
+class Dual:
+    """A value and its directional derivative (forward-mode differentiation of the stress
+    formulas below): the JVP QuasiStaticSolver takes of internal_force with autograd
+    (mechanics_solver.py:1705-1733, 2000-2012), restated for the oracle."""
+
+    __array_ufunc__ = None  # numpy arrays defer to the reflected operators below
+
+    def __init__(self, v, d):
+        self.v, self.d = np.asarray(v, dtype=float), np.asarray(d, dtype=float)
+
+    @staticmethod
+    def _split(o):
+        return (o.v, o.d) if isinstance(o, Dual) else (o, 0.0)
+
+    def __add__(self, o):
+        ov, od = Dual._split(o)
+        return Dual(self.v + ov, self.d + od)
+
+    __radd__ = __add__
+
+    def __sub__(self, o):
+        ov, od = Dual._split(o)
+        return Dual(self.v - ov, self.d - od)
+
+    def __rsub__(self, o):
+        ov, od = Dual._split(o)
+        return Dual(ov - self.v, od - self.d)
+
+    def __neg__(self):
+        return Dual(-self.v, -self.d)
+
+    def __mul__(self, o):
+        ov, od = Dual._split(o)
+        return Dual(self.v * ov, self.d * ov + self.v * od)
+
+    __rmul__ = __mul__
+
+    def __truediv__(self, o):
+        ov, od = Dual._split(o)
+        return Dual(self.v / ov, (self.d * ov - self.v * od) / (ov * ov))
+
+    def __rtruediv__(self, o):
+        ov, od = Dual._split(o)
+        return Dual(ov / self.v, (od * self.v - ov * self.d) / (self.v * self.v))
+
+
+def _value(x):
+    return x.v if isinstance(x, Dual) else x
+
+
+def _pos(x):
+    """max(x, 0); its derivative is taken as 1 where x >= 0 (the JVP of clamp(min=0))."""
+    if isinstance(x, Dual):
+        return Dual(np.maximum(x.v, 0.0), np.where(x.v >= 0, x.d, 0.0))
+    return np.maximum(x, 0.0)
+
+
+def _sqrt(x):
+    if isinstance(x, Dual):
+        r = np.sqrt(x.v)
+        return Dual(r, x.d / (2.0 * r))
+    return np.sqrt(x)
+
+
+def _where(c, a, b):
+    if isinstance(a, Dual) or isinstance(b, Dual):
+        av, ad = Dual._split(a)
+        bv, bd = Dual._split(b)
+        return Dual(np.where(c, av, bv), np.where(c, ad, bd))
+    return np.where(c, a, b)
+
+
 def stress_split(mat: Mat2D, split, exx, eyy, gxy, g):
     """compute_stress_* (fem_operators.py:283-560) for one split."""
     lam, mu, kap = mat.lam, mat.mu, mat.kappa
@@ -152,7 +224,7 @@ def stress_split(mat: Mat2D, split, exx, eyy, gxy, g):
     if split == "amor":
         tr2 = exx + eyy
         tr = tr2 + _ezz(mat, tr2)
-        trp = np.maximum(tr, 0.0)
+        trp = _pos(tr)
         trm = tr - trp
         return (g * (kap * trp + 2 * mu * (exx - tr / 3.0)) + kap * trm,
                 g * (kap * trp + 2 * mu * (eyy - tr / 3.0)) + kap * trm,
@@ -161,7 +233,7 @@ def stress_split(mat: Mat2D, split, exx, eyy, gxy, g):
         exy = gxy / 2.0
         trace = exx + eyy
         hd = (exx - eyy) / 2.0
-        delta = np.sqrt(hd ** 2 + exy ** 2 + mat.spectral_eps)
+        delta = _sqrt(hd * hd + exy * exy + mat.spectral_eps)
         e1 = trace / 2.0 + delta
         e2 = trace / 2.0 - delta
         inv2d = 1.0 / (2.0 * delta + 1e-30)
@@ -169,8 +241,8 @@ def stress_split(mat: Mat2D, split, exx, eyy, gxy, g):
         pyy = (-hd + delta) * inv2d
         pxy = exy * inv2d
         if split == "spectral":
-            e1p, e2p = np.maximum(e1, 0), np.maximum(e2, 0)
-            trp = np.maximum(trace, 0)
+            e1p, e2p = _pos(e1), _pos(e2)
+            trp = _pos(trace)
             trm = trace - trp
             xxp = e1p * pxx + e2p * (1 - pxx)
             yyp = e1p * pyy + e2p * (1 - pyy)
@@ -180,7 +252,7 @@ def stress_split(mat: Mat2D, split, exx, eyy, gxy, g):
                     g * (2 * mu * xyp) + 2 * mu * (exy - xyp))
         s1 = lam * trace + 2 * mu * e1
         s2 = lam * trace + 2 * mu * e2
-        s1p, s2p = np.maximum(s1, 0), np.maximum(s2, 0)
+        s1p, s2p = _pos(s1), _pos(s2)
         s1m, s2m = s1 - s1p, s2 - s2p
         return (g * (s1p * pxx + s2p * (1 - pxx)) + (s1m * pxx + s2m * (1 - pxx)),
                 g * (s1p * pyy + s2p * (1 - pyy)) + (s1m * pyy + s2m * (1 - pyy)),
@@ -188,14 +260,14 @@ def stress_split(mat: Mat2D, split, exx, eyy, gxy, g):
     if split == "star_convex":
         tr2 = exx + eyy
         tr = tr2 + _ezz(mat, tr2)
-        t = tr >= 0
+        t = _value(tr) >= 0
         sxx_t = g * ((lam + 2 * mu) * exx + lam * eyy)
         syy_t = g * (lam * exx + (lam + 2 * mu) * eyy)
         sxy_t = g * (mu * gxy)
         sxx_c = g * 2 * mu * (exx - tr / 3.0) + kap * tr
         syy_c = g * 2 * mu * (eyy - tr / 3.0) + kap * tr
         sxy_c = g * mu * gxy
-        return np.where(t, sxx_t, sxx_c), np.where(t, syy_t, syy_c), np.where(t, sxy_t, sxy_c)
+        return _where(t, sxx_t, sxx_c), _where(t, syy_t, syy_c), _where(t, sxy_t, sxy_c)
     raise ValueError(split)
 
 
@@ -257,6 +329,18 @@ def internal_force(geo, mat: Mat2D, u, d):
         g = mat.degradation(d_at_qp(geo, d))
         s = stress_split(mat, mat.stress_split or mat.split, exx, eyy, gxy, g)
     return assemble_force(geo, *s)
+
+
+def tangent_action(geo, mat: Mat2D, u, du, d):
+    """d internal_force(u, d)/du [du]: the JVP QuasiStaticSolver uses as its CG operator for the
+    spectral, Amor and star-convex splits (mechanics_solver.py:1705-1733, 2000-2012), by
+    forward-mode differentiation of stress_split at the strain of u with g(d) fixed."""
+    exx, eyy, gxy = strain(geo, u)
+    dxx, dyy, dxy = strain(geo, du)
+    g = mat.degradation(d_at_qp(geo, d))
+    split = mat.stress_split or mat.split
+    s = stress_split(mat, split, Dual(exx, dxx), Dual(eyy, dyy), Dual(gxy, dxy), g)
+    return assemble_force(geo, *(x.d if isinstance(x, Dual) else 0.0 * exx for x in s))
 
 
 def stiffness_diagonal(geo, mat: Mat2D, d=None):

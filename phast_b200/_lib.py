@@ -103,6 +103,7 @@ SIGNATURES = {
                                      C.c_int, C.c_int, C.c_double, C.c_double, ip, vp, sz, vp]),
     "phastb_q4_explicit_step": (C.c_int, [Q4G, Q4M, C.c_int, C.c_double, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                           vp, vp, vp, vp]),
+    "phastb_q4_tangent_apply": (C.c_int, [Q4G, Q4M, vp, vp, vp, vp, vp]),
     "phastb_q4_energy_sums": (C.c_int, [Q4G, Q4M, vp, vp, vp, dp, vp, sz, vp]),
     "phastb_q4_reaction_workspace_bytes": (sz, [C.c_int]),
     "phastb_q4_reaction": (C.c_int, [Q4G, Q4M, vp, vp, vp, C.c_int, C.c_int, vp, dp, vp, sz, vp]),

@@ -64,6 +64,66 @@ __global__ void __launch_bounds__(kThreads) q4_force_kernel(Q4Tab<T> t, Mat2<T> 
   reinterpret_cast<typename Vec2<T>::type*>(f)[node] = out;
 }
 
+// Consistent tangent action y = d f_int(u, d)/du [du] (node-centric gather like
+// q4_force_kernel): at every Gauss point the split's stress derivative at the strain of
+// u, applied to the strain of du, with g(d) fixed.  Masked rows give zero.
+__global__ void __launch_bounds__(kThreads) q4_tangent_kernel(Q4Tab<double> t, Mat2<double> m, int split,
+                                                              const double* __restrict__ u,
+                                                              const double* __restrict__ du,
+                                                              const double* __restrict__ d,
+                                                              double* __restrict__ f,
+                                                              const uint8_t* __restrict__ mask,
+                                                              const int* guard) {
+  if (guard && *guard == 0) return;
+  const int nn = (t.nx + 1) * (t.ny + 1);
+  const int node = blockIdx.x * blockDim.x + threadIdx.x;
+  if (node >= nn) return;
+  const int i = node % (t.nx + 1), j = node / (t.nx + 1);
+  double fx = 0, fy = 0;
+#pragma unroll
+  for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+    for (int di = 0; di < 2; ++di) {
+      const int ei = i - 1 + di, ej = j - 1 + dj;
+      if (ei < 0 || ei >= t.nx || ej < 0 || ej >= t.ny) continue;
+      const int a = q4_local(1 - di, 1 - dj);
+      int n[4];
+      q4_corners(ei, ej, t.nx, n);
+      double ux[4], uy[4], vx[4], vy[4], dd[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        load2(u, n[b], ux[b], uy[b]);
+        load2(du, n[b], vx[b], vy[b]);
+        dd[b] = d ? ld(d + n[b]) : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double exx = 0, eyy = 0, gxy = 0, vxx = 0, vyy = 0, vxy = 0, dq = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          exx += t.gx[q][b] * ux[b];
+          eyy += t.gy[q][b] * uy[b];
+          gxy += t.gy[q][b] * ux[b] + t.gx[q][b] * uy[b];
+          vxx += t.gx[q][b] * vx[b];
+          vyy += t.gy[q][b] * vy[b];
+          vxy += t.gy[q][b] * vx[b] + t.gx[q][b] * vy[b];
+          dq += t.N[q][b] * dd[b];
+        }
+        const double g = d ? degr(m, dq) : 1.0;
+        double sxx, syy, sxy;
+        dstress2(m, split, exx, eyy, gxy, vxx, vyy, vxy, g, sxx, syy, sxy);
+        fx += (t.gx[q][a] * sxx + t.gy[q][a] * sxy) * t.w;
+        fy += (t.gy[q][a] * syy + t.gx[q][a] * sxy) * t.w;
+      }
+    }
+  if (mask) {
+    const uchar2 mk = __ldg(reinterpret_cast<const uchar2*>(mask) + node);
+    if (mk.x) fx = 0.0;
+    if (mk.y) fy = 0.0;
+  }
+  reinterpret_cast<double2*>(f)[node] = make_double2(fx, fy);
+}
+
 // Transposed Gauss-point energy gradient of the undegraded (isotropic) energy:
 //   f_n = sum_{e in n} sum_q wq[e][q] B_q^T sigma0(u)_q,   sigma0 = d psi0 / d eps,
 // i.e. (d psi0_q / d u)^T wq: the adjoint of the history update H = max(H_prev, psi0(u))
@@ -644,6 +704,15 @@ int q4_force_launch(const phastb_q4_grid* g, const phastb_q4_material* m, const 
   return launch_force<double>(g, m, u, d, f, s, mask, guard);
 }
 
+int q4_tangent_launch(const phastb_q4_grid* g, const phastb_q4_material* m, const double* u, const double* du,
+                      const double* d, double* f, const uint8_t* mask, const int* guard, cudaStream_t s) {
+  const Q4Tab<double> t = make_q4_tab<double>(*g);
+  const Mat2<double> mm = make_mat2<double>(*m);
+  const int nn = (g->nx + 1) * (g->ny + 1);
+  { note_launch(); q4_tangent_kernel<<<grid_full(nn), kThreads, 0, s>>>(t, mm, m->stress_split, u, du, d, f, mask, guard); }
+  return last_launch_status();
+}
+
 }  // namespace phastb
 
 using namespace phastb;
@@ -678,6 +747,12 @@ int phastb_q4_internal_force(const phastb_q4_grid* g, const phastb_q4_material* 
   if (dtype == PHASTB_F64) return launch_force<double>(g, m, u, d, f, (cudaStream_t)stream);
   if (dtype == PHASTB_F32) return launch_force<float>(g, m, u, d, f, (cudaStream_t)stream);
   return PHASTB_ERR_ARG;
+}
+
+int phastb_q4_tangent_apply(const phastb_q4_grid* g, const phastb_q4_material* m, const double* u,
+                            const double* du, const double* d, double* y, void* stream) {
+  if (!valid_grid(g) || !m || !u || !du || !y) return PHASTB_ERR_ARG;
+  return q4_tangent_launch(g, m, u, du, d, y, nullptr, nullptr, (cudaStream_t)stream);
 }
 
 int phastb_q4_psi_grad_t(const phastb_q4_grid* g, const phastb_q4_material* m, const double* u, const double* wq,

@@ -139,6 +139,73 @@ __device__ __forceinline__ void stress2(const Mat2<T>& m, int split, T exx, T ey
   }
 }
 
+// Consistent tangent of stress2: the directional derivative d sigma(eps)[d eps] of the
+// split stress at the strain (exx, eyy, gxy), at fixed degradation g.  This is the action
+// QuasiStaticSolver takes by an autograd JVP of internal_force for the spectral, Amor and
+// star-convex splits (mechanics_solver.py:1705-1733, 2000-2012); it differentiates the same
+// algebra as stress2 (projectors included), with the derivative of a positive part
+// max(x, 0) taken as 1 where x >= 0, as the JVP of clamp(min=0) does.  Linear and isotropic
+// stresses are their own tangent; the stress-spectral split has no entry here (the reference
+// linearises it by evaluating the stress at the increment, which stress2 already does).
+template <typename T>
+__device__ __forceinline__ void dstress2(const Mat2<T>& m, int split, T exx, T eyy, T gxy, T dexx, T deyy, T dgxy,
+                                         T g, T& dsxx, T& dsyy, T& dsxy) {
+  const T lam = m.lam, mu = m.mu;
+  switch (split) {
+    case PHASTB_SPLIT_AMOR:
+    case PHASTB_SPLIT_STAR_CONVEX: {
+      const T tr2 = exx + eyy;
+      const T tr = tr2 + ezz_of(m, tr2);
+      const T dtr2 = dexx + deyy;
+      const T dtr = dtr2 + ezz_of(m, dtr2);
+      const bool pos = tr >= T(0);
+      if (split == PHASTB_SPLIT_AMOR) {
+        const T dtrp = pos ? dtr : T(0), dtrm = dtr - dtrp;
+        dsxx = g * (m.kap * dtrp + 2 * mu * (dexx - dtr / T(3))) + m.kap * dtrm;
+        dsyy = g * (m.kap * dtrp + 2 * mu * (deyy - dtr / T(3))) + m.kap * dtrm;
+        dsxy = g * mu * dgxy;
+      } else if (pos) {
+        dsxx = g * ((lam + 2 * mu) * dexx + lam * deyy);
+        dsyy = g * (lam * dexx + (lam + 2 * mu) * deyy);
+        dsxy = g * (mu * dgxy);
+      } else {
+        dsxx = g * 2 * mu * (dexx - dtr / T(3)) + m.kap * dtr;
+        dsyy = g * 2 * mu * (deyy - dtr / T(3)) + m.kap * dtr;
+        dsxy = g * mu * dgxy;
+      }
+      return;
+    }
+    case PHASTB_SPLIT_SPECTRAL: {
+      const T exy = gxy / T(2), dexy = dgxy / T(2);
+      const T trace = exx + eyy, dtrace = dexx + deyy;
+      const T hd = (exx - eyy) / T(2), dhd = (dexx - deyy) / T(2);
+      const T delta = sqrt(hd * hd + exy * exy + m.seps);
+      const T ddelta = (hd * dhd + exy * dexy) / delta;
+      const T e1 = trace / T(2) + delta, e2 = trace / T(2) - delta;
+      const T de1 = dtrace / T(2) + ddelta, de2 = dtrace / T(2) - ddelta;
+      const T e1p = e1 > T(0) ? e1 : T(0), e2p = e2 > T(0) ? e2 : T(0);
+      const T de1p = e1 >= T(0) ? de1 : T(0), de2p = e2 >= T(0) ? de2 : T(0);
+      const T dtrp = trace >= T(0) ? dtrace : T(0), dtrm = dtrace - dtrp;
+      const T inv2d = T(1) / (T(2) * delta + T(1e-30));
+      const T dinv2d = -T(2) * ddelta * inv2d * inv2d;
+      const T pxx = (hd + delta) * inv2d, pyy = (-hd + delta) * inv2d, pxy = exy * inv2d;
+      const T dpxx = (dhd + ddelta) * inv2d + (hd + delta) * dinv2d;
+      const T dpyy = (-dhd + ddelta) * inv2d + (-hd + delta) * dinv2d;
+      const T dpxy = dexy * inv2d + exy * dinv2d;
+      const T dxxp = de1p * pxx + e1p * dpxx + de2p * (T(1) - pxx) - e2p * dpxx;
+      const T dyyp = de1p * pyy + e1p * dpyy + de2p * (T(1) - pyy) - e2p * dpyy;
+      const T dxyp = (de1p - de2p) * pxy + (e1p - e2p) * dpxy;
+      dsxx = g * (lam * dtrp + 2 * mu * dxxp) + (lam * dtrm + 2 * mu * (dexx - dxxp));
+      dsyy = g * (lam * dtrp + 2 * mu * dyyp) + (lam * dtrm + 2 * mu * (deyy - dyyp));
+      dsxy = g * (2 * mu * dxyp) + 2 * mu * (dexy - dxyp);
+      return;
+    }
+    default:  // linear in eps: the tangent is the stress of the increment
+      stress2(m, split, dexx, deyy, dgxy, g, dsxx, dsyy, dsxy);
+      return;
+  }
+}
+
 // Tensile energy psi+ of one split (fem_operators.py:974-1161).
 template <typename T>
 __device__ __forceinline__ T psi2(const Mat2<T>& m, int split, T exx, T eyy, T gxy) {

@@ -59,6 +59,24 @@ static int q4_force_op(const void* c, const double* x, double* y, const int* gua
   return q4_force_launch(&k->g, &k->m, x, k->d, y, k->mask, guard, s);
 }
 
+int q4_tangent_launch(const phastb_q4_grid* g, const phastb_q4_material* m, const double* u, const double* du,
+                      const double* d, double* f, const uint8_t* mask, const int* guard, cudaStream_t s);
+
+// The consistent tangent at the Newton iterate `u` (read at every apply, so one
+// context serves every Newton step of a solve).
+struct Q4TangentCtx {
+  phastb_q4_grid g;
+  phastb_q4_material m;
+  const double* d;
+  const uint8_t* mask;
+  const double* u;
+};
+
+static int q4_tangent_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
+  const Q4TangentCtx* k = static_cast<const Q4TangentCtx*>(c);
+  return q4_tangent_launch(&k->g, &k->m, k->u, x, k->d, y, k->mask, guard, s);
+}
+
 // residual r = (f_ext - f) * free, and u[bc] = bc_vals helpers
 __global__ void qs_residual_kernel(int n2, const double* __restrict__ fext, const double* __restrict__ f,
                                    const uint8_t* __restrict__ bcm, double* __restrict__ r, RedWs ws) {
@@ -337,8 +355,6 @@ int phastb_q4_qs_solve(const phastb_q4_grid* g, const phastb_q4_material* m, con
                        double ls_c, int* info, void* workspace, size_t workspace_bytes, void* stream) {
   if (!valid_grid(g) || !m || !d || !bc_mask || !bc_vals || !u || cg_max_iter < 1 || max_iter < 0)
     return PHASTB_ERR_ARG;
-  if (m->stress_split != PHASTB_SPLIT_ISOTROPIC && m->stress_split != PHASTB_SPLIT_LINEAR)
-    return PHASTB_UNSUPPORTED;  // split-aware tangents need the consistent-tangent kernel
   const int nn = (g->nx + 1) * (g->ny + 1), n2 = 2 * nn;
   if (!workspace || workspace_bytes < phastb_q4_qs_workspace_bytes(nn)) return PHASTB_ERR_WORKSPACE;
   ScopedStream scope((cudaStream_t)stream);
@@ -351,7 +367,21 @@ int phastb_q4_qs_solve(const phastb_q4_grid* g, const phastb_q4_material* m, con
   std::memcpy(&kctx.m, m, offsetof(phastb_q4_material, psi_split) + sizeof(int));
   kctx.d = d;
   kctx.mask = bc_mask;
-  LinOp<double> K{q4_force_op, &kctx, sizeof(kctx)};
+  // Splits whose stress is not linear in the strain take the consistent tangent at the
+  // iterate, as the reference's autograd JVP does for the spectral, Amor and star-convex
+  // splits (mechanics_solver.py:1705-1733); linear stresses and the stress-spectral split
+  // (which the reference linearises by evaluating the force at the increment) use the force.
+  const int sp = m->stress_split;
+  const bool tangent = sp == PHASTB_SPLIT_AMOR || sp == PHASTB_SPLIT_SPECTRAL || sp == PHASTB_SPLIT_STAR_CONVEX;
+  Q4TangentCtx tctx;
+  std::memset(&tctx, 0, sizeof(tctx));
+  tctx.g = *g;
+  std::memcpy(&tctx.m, m, offsetof(phastb_q4_material, psi_split) + sizeof(int));
+  tctx.d = d;
+  tctx.mask = bc_mask;
+  tctx.u = u;
+  LinOp<double> K = tangent ? LinOp<double>{q4_tangent_op, &tctx, sizeof(tctx)}
+                            : LinOp<double>{q4_force_op, &kctx, sizeof(kctx)};
   return qs_newton(n2, K, q4_force_eval, &kctx, f_ext, bc_mask, bc_vals, u, tol, cg_tol, cg_max_iter, max_iter,
                    line_search, ls_max_steps, ls_min_alpha, ls_c, info, workspace, scope.get());
 }

@@ -106,7 +106,12 @@ class ExplicitDynamics:
 
 
 class QuasiStaticSolver:
-    """Newton-Raphson with matrix-free CG (mechanics_solver.py:816-2043), isotropic split."""
+    """Newton-Raphson with matrix-free CG (mechanics_solver.py:816-2043).
+
+    The CG operator is the consistent tangent at the Newton iterate for the spectral, Amor
+    and star-convex splits (the reference's autograd JVP, mechanics_solver.py:1705-1733) and
+    the degraded stiffness for the linear ones, both one kernel per CG step.
+    """
 
     def __init__(self, fem, tol=1e-6, max_iter=50, cg_tol=1e-8, cg_max_iter=5000, backend="auto",
                  sparse_dof_threshold=200000, inner_solver=None, consistent_tangent=None, line_search=True,
@@ -117,10 +122,13 @@ class QuasiStaticSolver:
         if tol_rel is not None:
             raise NotImplementedError("relative Newton tolerance is not implemented by the B200 backend")
         split = stress_split_of(fem.material)
-        if split != "isotropic":
+        if split != "isotropic" and getattr(fem, "t3", None) is not None:
             raise NotImplementedError(
-                f"quasi-static mechanics with the {split!r} split needs the consistent-tangent kernel, which is "
-                "not implemented; use energy_split='isotropic'")
+                f"quasi-static mechanics on T3 meshes with the {split!r} split is not implemented by the B200 "
+                "backend (the consistent-tangent kernel is structured-Q4); use energy_split='isotropic'")
+        if consistent_tangent is False and split in ("spectral", "amor", "star_convex"):
+            raise NotImplementedError("the secant (frozen-state) linearisation is not implemented by the B200 "
+                                      "backend; the consistent tangent is used")
         self.fem = fem
         self.tol = float(tol)
         self.max_iter = int(max_iter)

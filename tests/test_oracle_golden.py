@@ -197,3 +197,17 @@ def test_t3_operators_damage_and_solve():
     for c in range(colors.max() + 1):
         nodes = g["tris"][colors == c].reshape(-1)
         assert len(np.unique(nodes)) == len(nodes)  # one colour never touches a node twice
+
+
+@pytest.mark.parametrize("key,split,ps", [("tan_spectral", "spectral", False), ("tan_amor", "amor", False),
+                                          ("tan_star_convex", "star_convex", False), ("tan_amor_ps", "amor", True)])
+def test_q4_tangent_oracle_matches_reference_jvp(key, split, ps):
+    """The oracle's forward-mode tangent equals the reference's autograd JVP of internal_force."""
+    from oracle import q4
+    g = golden("q4_qs_splits")
+    nodes, el = q4.structured_mesh(float(g["tan_w"][0]), float(g["tan_h"][0]), int(g["tan_nx"][0]),
+                                   int(g["tan_ny"][0]))
+    geo = q4.geometry(nodes, el)
+    m = q4.Mat2D(E=210000.0, nu=0.3, Gc=2.7, l0=0.05, split=split, plane_stress=ps)
+    assert rel(q4.internal_force(geo, m, g["tan_u"], g["tan_d"]), g[key + "_f"]) < 1e-12
+    assert rel(q4.tangent_action(geo, m, g["tan_u"], g["tan_du"], g["tan_d"]), g[key]) < 1e-12
