@@ -144,7 +144,7 @@ class QuasiStaticSolver:
         self.last_backend = "cg"
         self._ws = _lib.Workspace(fem.device)
 
-    def _newton(self, d, f_ext, mask_u8, bc_vals, u, tol, cg_tol, max_iter, line_search):
+    def _newton(self, d, f_ext, mask_u8, bc_vals, u, tol, cg_tol, max_iter, line_search, cg_max_iter=None):
         """One device Newton-CG solve into ``u`` (FP64, contiguous); returns (status, info)."""
         fem = self.fem
         t3 = getattr(fem, "t3", None)
@@ -157,7 +157,7 @@ class QuasiStaticSolver:
             name, geo, wb = "phastb_q4_qs_solve", fem.grid, lib.phastb_q4_qs_workspace_bytes(n)
         wp, wn = self._ws.get(wb)
         st = raw(name, geo, fem.mat(torch.float64), ptr(d), ptr(f_ext), ptr(mask_u8), ptr(bc_vals), ptr(u), float(tol),
-                 float(cg_tol), self.cg_max_iter, int(max_iter), int(line_search), self.line_search_max_steps,
+                 float(cg_tol), int(cg_max_iter or self.cg_max_iter), int(max_iter), int(line_search), self.line_search_max_steps,
                  self.line_search_min_alpha, self.line_search_c, info, wp, wn, stream())
         if st not in (_lib.OK, _lib.NONCONVERGED, _lib.NONFINITE, _lib.BREAKDOWN):
             _lib.check(st, name)
@@ -193,7 +193,11 @@ class QuasiStaticSolver:
         if nrm == 0.0:
             return z
         dd = d.to(torch.float64).contiguous()
-        st, info = self._newton(dd, r, mask, torch.zeros_like(r), z, rtol * nrm, 1e-10, max_refine, False)
+        # one long CG per refinement: restarting a short CG discards its Krylov space, and the
+        # adjoint right-hand side (concentrated on the loaded edge) needs many iterations on
+        # large cracked meshes
+        st, info = self._newton(dd, r, mask, torch.zeros_like(r), z, rtol * nrm, 1e-10, max_refine, False,
+                                cg_max_iter=max(self.cg_max_iter, 200000))
         if st != _lib.OK or not info[1]:
             raise RuntimeError(f"stiffness solve did not converge (status {st}, {int(info[0])} refinements)")
         return z
