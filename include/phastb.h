@@ -194,6 +194,34 @@ typedef struct {
   const double* areas;   /* (E,) */
 } phastb_t3_mesh;
 
+/* A T3 damage model beyond element-history AT2 (PhaseFieldDamageSolver, damage_solver.py:1316-1340):
+ * AT1 (element history): gcl0 = 3 Gc l0 / 4, gc_over_l0 = 0, source = 3 Gc / (8 l0) subtracted from
+ * the reaction 2 H on the right-hand side; AT2 with nodal history (nodal_h = 1, H of length
+ * n_nodes, triple-product reaction mass, damage_solver.py:1840-1912, 2303-2348; the reference
+ * supports nodal history with AT2 only, so source must be 0).  The *_e arrays (may be NULL)
+ * override the scalars per element. */
+typedef struct {
+  int nodal_h, reserved;   /* reserved: 0 */
+  double gcl0, gc_over_l0, source;
+  const double* gcl0_e;
+  const double* gc_over_l0_e;
+  const double* source_e;
+} phastb_t3_damage_model;
+
+/* y = A d of the model's damage system.  _Ax / _Ax_nodal, damage_solver.py:1702-1912 */
+int phastb_t3_damage_apply_ex(const phastb_t3_mesh* mesh, const phastb_t3_damage_model* model, const double* d,
+                              const double* H, double* y, void* stream);
+/* b and M_inv = 1/(diag + 1e-30) of the model.  _prepare_cg / _prepare_cg_nodal,
+ * damage_solver.py:2040-2348 */
+int phastb_t3_damage_prepare_ex(const phastb_t3_mesh* mesh, const phastb_t3_damage_model* model, const double* H,
+                                double* b, double* m_inv, void* stream);
+/* Bound-projected PCG solve of the model's system (as phastb_t3_damage_solve; workspace
+ * phastb_t3_damage_solve_workspace_bytes).  _solve_projected_cg, damage_solver.py:3528-3775 */
+int phastb_t3_damage_solve_ex(const phastb_t3_mesh* mesh, const phastb_t3_damage_model* model, const double* H,
+                              const double* d_prev, const double* d_init, const uint8_t* fixed,
+                              const double* fixed_vals, double tol, int max_iter, int check_every, double* d_out,
+                              int* info, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Host check of a T3 colouring before it is used (all HOST arrays): node ids in range,
  * `order` a permutation of the elements, colour offsets from 0 to n_elems, and no node shared
  * by two elements of one colour.  PHASTB_ERR_ARG otherwise.  The element kernels trust the

@@ -122,6 +122,50 @@ def damage_prepare(geo, H, gc_over_l0, gc_l0):
     return rc, b, 1.0 / (dg + 1e-30)
 
 
+def damage_prepare_at1(geo, H, gc, l0, source=None):
+    """AT1 with element history (damage_solver.py:1325-1329, 2060-2080): the AT2 system with
+    Gc l0 -> 3 Gc l0 / 4, no Gc/l0 reaction, right-hand side (2 H_e - S) A_e / 3 with the source
+    S = 3 Gc / (8 l0).  Returns (rc, b, M_inv, gc_l0)."""
+    src = 3.0 * gc / (8.0 * l0) if source is None else source
+    gc_l0 = 0.75 * gc * l0
+    rc, b, mi = damage_prepare(geo, H, 0.0, gc_l0)
+    np.add.at(b, geo.elements.reshape(-1), np.repeat(-src * geo.areas / 3.0, 3))
+    return rc, b, mi, gc_l0
+
+
+def damage_apply_nodal(geo, d, Hn, gc_over_l0, gc_l0):
+    """_Ax_nodal (damage_solver.py:1840-1912): Gc l0 K d + the reaction mass of 2 H with H
+    interpolated from the nodes (triple products A/10, A/30, A/60) + Gc/l0 M d."""
+    de = d[geo.elements]
+    he = np.asarray(Hn)[geo.elements]
+    gp = geo.grad
+    gx = (gp[:, :, 0] * de).sum(1)
+    gy = (gp[:, :, 1] * de).sum(1)
+    lap = geo.areas[:, None] * (gp[:, :, 0] * gx[:, None] + gp[:, :, 1] * gy[:, None])
+    sh, sd, hd = he.sum(1), de.sum(1), (he * de).sum(1)
+    mh = (geo.areas / 30.0)[:, None] * ((2.0 * he + sh[:, None]) * de + (he + sh[:, None]) * sd[:, None] +
+                                        hd[:, None])
+    mg = (gc_over_l0 * geo.areas / 12.0)[:, None] * (de + sd[:, None])
+    y = np.zeros(geo.n_nodes)
+    np.add.at(y, geo.elements.reshape(-1), (gc_l0 * lap + mh + mg).reshape(-1))
+    return y
+
+
+def damage_prepare_nodal(geo, Hn, gc_over_l0, gc_l0):
+    """_prepare_cg_nodal (damage_solver.py:2303-2348): b_a = A/6 (H_a + S_H) and the Jacobi inverse
+    of Gc l0 diag_lap + (2 H_a + S_H) A/15 + Gc/l0 A/6."""
+    he = np.asarray(Hn)[geo.elements]
+    sh = he.sum(1)
+    b = np.zeros(geo.n_nodes)
+    np.add.at(b, geo.elements.reshape(-1), ((geo.areas / 6.0)[:, None] * (he + sh[:, None])).reshape(-1))
+    gp = geo.grad
+    diag_lap = geo.areas[:, None] * (gp[:, :, 0] ** 2 + gp[:, :, 1] ** 2)
+    md = (geo.areas / 15.0)[:, None] * (2.0 * he + sh[:, None]) + (gc_over_l0 * geo.areas / 6.0)[:, None]
+    dg = np.zeros(geo.n_nodes)
+    np.add.at(dg, geo.elements.reshape(-1), (gc_l0 * diag_lap + md).reshape(-1))
+    return b, 1.0 / (dg + 1e-30)
+
+
 def color_elements(elements, n_nodes):
     """Greedy colouring: no two elements of one colour share a node (first-fit, element order)."""
     el = np.asarray(elements, dtype=np.int64)

@@ -58,7 +58,14 @@ class T3Mesh(C.Structure):
                 ("grad", C.c_void_p), ("areas", C.c_void_p)]
 
 
+class T3DamageModel(C.Structure):
+    _fields_ = [("nodal_h", C.c_int), ("reserved", C.c_int), ("gcl0", C.c_double), ("gc_over_l0", C.c_double),
+                ("source", C.c_double), ("gcl0_e", C.c_void_p), ("gc_over_l0_e", C.c_void_p),
+                ("source_e", C.c_void_p)]
+
+
 Q4G, Q4M, VG, VM = C.POINTER(Q4Grid), C.POINTER(Q4Material), C.POINTER(VoxelGrid), C.POINTER(VoxelMaterial)
+T3DM = C.POINTER(T3DamageModel)
 T3M = C.POINTER(T3Mesh)
 MO = C.POINTER(MechOpts)
 
@@ -152,6 +159,10 @@ SIGNATURES = {
     "phastb_batch_damage_box_kkt": (C.c_int, [vp, VM, vp, vp, vp, C.c_double, vp, C.c_double, C.c_double,
                                               C.c_double, C.c_int, C.c_int, C.c_int, ip, vp, ip, dp, vp, sz, vp]),
     "phastb_batch_predictor": (C.c_int, [vp, vp, C.c_double, C.c_int, C.c_double, vp, vp, vp]),
+    "phastb_t3_damage_apply_ex": (C.c_int, [T3M, T3DM, vp, vp, vp, vp]),
+    "phastb_t3_damage_prepare_ex": (C.c_int, [T3M, T3DM, vp, vp, vp, vp]),
+    "phastb_t3_damage_solve_ex": (C.c_int, [T3M, T3DM, vp, vp, vp, vp, vp, C.c_double, C.c_int, C.c_int, vp, ip,
+                                            vp, sz, vp]),
     "phastb_t3_check_mesh": (C.c_int, [C.c_int, C.c_int, ip, ip, C.c_int, ip]),
     "phastb_batch_change_workspace_bytes": (sz, [vp]),
     "phastb_batch_stagger_change": (C.c_int, [vp, vp, vp, vp, vp, dp, vp, sz, vp]),

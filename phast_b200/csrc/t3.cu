@@ -117,10 +117,12 @@ __global__ void __launch_bounds__(kThreads) t3_damage_colour(T3Dev t, const doub
   for (int a = 0; a < 3; ++a) y[n[a]] += kl * (A * (gp[a][0] * gx + gp[a][1] * gy)) + rc * (dd[a] + ds);
 }
 
-// b_a += 2 H_e A / 3;  diag_a += gcl0_e A |grad phi_a|^2 + 2 rc_e
+// b_a += (2 H_e - src_e) A / 3;  diag_a += gcl0_e A |grad phi_a|^2 + 2 rc_e  (src: the AT1 source
+// 3 Gc / (8 l0), zero for AT2; damage_solver.py:2060-2080)
 __global__ void __launch_bounds__(kThreads) t3_prepare_colour(T3Dev t, const double* __restrict__ H, double gco,
                                                               const double* __restrict__ gco_e, double gcl0,
-                                                              const double* __restrict__ gcl0_e, double* b,
+                                                              const double* __restrict__ gcl0_e, double src,
+                                                              const double* __restrict__ src_e, double* b,
                                                               double* diag, int k0, int k1) {
   const int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= k1) return;
@@ -133,8 +135,74 @@ __global__ void __launch_bounds__(kThreads) t3_prepare_colour(T3Dev t, const dou
   for (int a = 0; a < 3; ++a) {
     const int n = __ldg(t.elem + 3 * e + a);
     const double gx = __ldg(t.grad + 6 * e + 2 * a), gy = __ldg(t.grad + 6 * e + 2 * a + 1);
-    b[n] += 2.0 * He * A / 3.0;
+    b[n] += (2.0 * He - (src_e ? __ldg(src_e + e) : src)) * A / 3.0;
     diag[n] += kl * (A * (gx * gx + gy * gy)) + 2.0 * rc;
+  }
+}
+
+// Nodal history (PhaseFieldX convention, damage_solver.py:1840-1912): the reaction mass is
+// int 2 H N_a N_b with H interpolated from the nodes, i.e. with the triple products
+// int N_i N_j N_k = A/10, A/30, A/60 (all, two, no indices equal):
+//   y_a += kl A grad phi_a . grad d + A/30 [(2 H_a + S_H) d_a + (H_a + S_H) S_d + H.d]
+//          + gco A/12 (d_a + S_d),   S_H, S_d, H.d the element sums.
+__global__ void __launch_bounds__(kThreads) t3_damage_nodal_colour(T3Dev t, const double* __restrict__ d,
+                                                                   const double* __restrict__ Hn, double gco,
+                                                                   const double* __restrict__ gco_e, double gcl0,
+                                                                   const double* __restrict__ gcl0_e, double* y,
+                                                                   int k0, int k1, const int* guard) {
+  if (guard && *guard == 0) return;
+  const int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= k1) return;
+  const int e = __ldg(t.order + k);
+  int n[3];
+  double gp[3][2], dd[3], hh[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    n[a] = __ldg(t.elem + 3 * e + a);
+    gp[a][0] = __ldg(t.grad + 6 * e + 2 * a);
+    gp[a][1] = __ldg(t.grad + 6 * e + 2 * a + 1);
+    dd[a] = __ldg(d + n[a]);
+    hh[a] = Hn ? __ldg(Hn + n[a]) : 0.0;
+  }
+  const double A = __ldg(t.areas + e);
+  const double gx = gp[0][0] * dd[0] + gp[1][0] * dd[1] + gp[2][0] * dd[2];
+  const double gy = gp[0][1] * dd[0] + gp[1][1] * dd[1] + gp[2][1] * dd[2];
+  const double kl = gcl0_e ? __ldg(gcl0_e + e) : gcl0;
+  const double rg = (gco_e ? __ldg(gco_e + e) : gco) * A / 12.0;
+  const double sh = hh[0] + hh[1] + hh[2], sd = dd[0] + dd[1] + dd[2];
+  const double hd = hh[0] * dd[0] + hh[1] * dd[1] + hh[2] * dd[2];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double mh = A / 30.0 * ((2.0 * hh[a] + sh) * dd[a] + (hh[a] + sh) * sd + hd);
+    y[n[a]] += kl * (A * (gp[a][0] * gx + gp[a][1] * gy)) + (mh + rg * (dd[a] + sd));
+  }
+}
+
+// Nodal history: b_a += A/6 (H_a + S_H);  diag_a += kl A |grad phi_a|^2 + (2 H_a + S_H) A/15 + gco A/6
+// (_prepare_cg_nodal, damage_solver.py:2303-2348)
+__global__ void __launch_bounds__(kThreads) t3_prepare_nodal_colour(T3Dev t, const double* __restrict__ Hn,
+                                                                    double gco, const double* __restrict__ gco_e,
+                                                                    double gcl0, const double* __restrict__ gcl0_e,
+                                                                    double* b, double* diag, int k0, int k1) {
+  const int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= k1) return;
+  const int e = __ldg(t.order + k);
+  const double A = __ldg(t.areas + e);
+  const double kl = gcl0_e ? __ldg(gcl0_e + e) : gcl0;
+  const double go = gco_e ? __ldg(gco_e + e) : gco;
+  int n[3];
+  double hh[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    n[a] = __ldg(t.elem + 3 * e + a);
+    hh[a] = Hn ? __ldg(Hn + n[a]) : 0.0;
+  }
+  const double sh = hh[0] + hh[1] + hh[2];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double gx = __ldg(t.grad + 6 * e + 2 * a), gy = __ldg(t.grad + 6 * e + 2 * a + 1);
+    b[n[a]] += A / 6.0 * (hh[a] + sh);
+    diag[n[a]] += kl * (A * (gx * gx + gy * gy)) + ((2.0 * hh[a] + sh) * A / 15.0 + go * A / 6.0);
   }
 }
 
@@ -304,6 +372,24 @@ int t3_damage_apply_launch(const phastb_t3_mesh& mesh, const double* d, const do
   return last_launch_status();
 }
 
+// y = A d of a damage model (element or nodal history, AT2 or AT1 coefficients); masked rows 0.
+int t3_damage_model_launch(const phastb_t3_mesh& mesh, const phastb_t3_damage_model& md, const double* d,
+                           const double* H, double* y, const int* guard, cudaStream_t s, const uint8_t* mask) {
+  if (!md.nodal_h)
+    return t3_damage_apply_launch(mesh, d, H, md.gc_over_l0, md.gc_over_l0_e, md.gcl0, md.gcl0_e, y, guard, s,
+                                  mask);
+  int st = cuda_status(cudaMemsetAsync(y, 0, sizeof(double) * (size_t)mesh.n_nodes, s));
+  if (st) return st;
+  const T3Dev t = t3_dev(mesh);
+  for (int c = 0; c < mesh.n_colors; ++c) {
+    const int k0 = mesh.color_off[c], k1 = mesh.color_off[c + 1];
+    if (k1 <= k0) continue;
+    { note_launch(); t3_damage_nodal_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, d, H, md.gc_over_l0, md.gc_over_l0_e, md.gcl0, md.gcl0_e, y, k0, k1, guard); }
+  }
+  if (mask) { note_launch(); t3_mask_rows_kernel<<<grid_for(mesh.n_nodes), kThreads, 0, s>>>(mesh.n_nodes, mask, y, guard); }
+  return last_launch_status();
+}
+
 // f = f_int(u, d) (d NULL: undegraded linear); rows that ``mask`` holds fixed (2 per node) give 0.
 int t3_force_launch(const phastb_t3_mesh& mesh, const phastb_q4_material& m, const double* u, const double* d,
                     double* f, const uint8_t* mask, const int* guard, cudaStream_t s) {
@@ -336,6 +422,23 @@ struct T3DamageCtx {
 int t3_damage_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
   const T3DamageCtx* k = static_cast<const T3DamageCtx*>(c);
   return t3_damage_apply_launch(k->mesh, x, k->H, k->gco, k->gco_e, k->gcl0, k->gcl0_e, y, guard, s, nullptr);
+}
+
+// A damage model's operator for the Krylov engines (hashed as bytes: zeroed before filling).
+struct T3ModelCtx {
+  phastb_t3_mesh mesh;
+  phastb_t3_damage_model model;
+  const double* H;
+};
+
+int t3_model_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
+  const T3ModelCtx* k = static_cast<const T3ModelCtx*>(c);
+  return t3_damage_model_launch(k->mesh, k->model, x, k->H, y, guard, s, nullptr);
+}
+
+bool valid_model(const phastb_t3_damage_model* m) {
+  return m && (m->nodal_h == 0 || m->nodal_h == 1) && !(m->nodal_h && (m->source != 0.0 || m->source_e)) &&
+         m->reserved == 0;
 }
 
 }  // namespace
@@ -385,7 +488,7 @@ int phastb_t3_damage_prepare(const phastb_t3_mesh* mesh, const double* H, double
   for (int c = 0; c < mesh->n_colors; ++c) {
     const int k0 = mesh->color_off[c], k1 = mesh->color_off[c + 1];
     if (k1 <= k0) continue;
-    { note_launch(); t3_prepare_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, H, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e, b, m_inv, k0, k1); }
+    { note_launch(); t3_prepare_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, H, gc_over_l0, gc_over_l0_e, gcl0, gcl0_e, 0.0, nullptr, b, m_inv, k0, k1); }
   }
   { note_launch(); t3_invert_kernel<<<grid_for(mesh->n_nodes), kThreads, 0, s>>>(mesh->n_nodes, m_inv); }
   return last_launch_status();
@@ -417,6 +520,64 @@ int phastb_t3_damage_solve(const phastb_t3_mesh* mesh, const double* H, double g
   ctx.gcl0 = gcl0;
   ctx.gcl0_e = gcl0_e;
   LinOp<double> A{t3_damage_op, &ctx, sizeof(ctx)};
+  int inf[2] = {0, 0};
+  st = ppcg_solve(A, n, w, d_prev, d_init, fixed, fixed_vals, tol, max_iter, check_every, d_out, inf, s);
+  if (info) {
+    info[0] = inf[0];
+    info[1] = inf[1];
+  }
+  return st;
+}
+
+int phastb_t3_damage_apply_ex(const phastb_t3_mesh* mesh, const phastb_t3_damage_model* model, const double* d,
+                              const double* H, double* y, void* stream) {
+  if (!t3_valid_mesh(mesh) || !valid_model(model) || !d || !y) return PHASTB_ERR_ARG;
+  return t3_damage_model_launch(*mesh, *model, d, H, y, nullptr, (cudaStream_t)stream, nullptr);
+}
+
+int phastb_t3_damage_prepare_ex(const phastb_t3_mesh* mesh, const phastb_t3_damage_model* model, const double* H,
+                                double* b, double* m_inv, void* stream) {
+  if (!t3_valid_mesh(mesh) || !valid_model(model) || !b || !m_inv) return PHASTB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t nb = sizeof(double) * (size_t)mesh->n_nodes;
+  int st;
+  if ((st = cuda_status(cudaMemsetAsync(b, 0, nb, s)))) return st;
+  if ((st = cuda_status(cudaMemsetAsync(m_inv, 0, nb, s)))) return st;
+  const T3Dev t = t3_dev(*mesh);
+  const phastb_t3_damage_model& md = *model;
+  for (int c = 0; c < mesh->n_colors; ++c) {
+    const int k0 = mesh->color_off[c], k1 = mesh->color_off[c + 1];
+    if (k1 <= k0) continue;
+    if (md.nodal_h)
+      { note_launch(); t3_prepare_nodal_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, H, md.gc_over_l0, md.gc_over_l0_e, md.gcl0, md.gcl0_e, b, m_inv, k0, k1); }
+    else
+      { note_launch(); t3_prepare_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, H, md.gc_over_l0, md.gc_over_l0_e, md.gcl0, md.gcl0_e, md.source, md.source_e, b, m_inv, k0, k1); }
+  }
+  { note_launch(); t3_invert_kernel<<<grid_for(mesh->n_nodes), kThreads, 0, s>>>(mesh->n_nodes, m_inv); }
+  return last_launch_status();
+}
+
+int phastb_t3_damage_solve_ex(const phastb_t3_mesh* mesh, const phastb_t3_damage_model* model, const double* H,
+                              const double* d_prev, const double* d_init, const uint8_t* fixed,
+                              const double* fixed_vals, double tol, int max_iter, int check_every, double* d_out,
+                              int* info, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!t3_valid_mesh(mesh) || !valid_model(model) || !d_prev || !d_out || max_iter < 0 || check_every < 1)
+    return PHASTB_ERR_ARG;
+  if (fixed && !fixed_vals) return PHASTB_ERR_ARG;
+  const int n = mesh->n_nodes;
+  if (!workspace || workspace_bytes < ppcg_ws_bytes(n)) return PHASTB_ERR_WORKSPACE;
+  ScopedStream scope((cudaStream_t)stream);
+  if (scope.status()) return scope.status();
+  cudaStream_t s = scope.get();
+  PpcgWs w = ppcg_ws(workspace, n);
+  int st = phastb_t3_damage_prepare_ex(mesh, model, H, w.b, w.minv, (void*)s);
+  if (st) return st;
+  T3ModelCtx ctx;
+  std::memset(&ctx, 0, sizeof(ctx));
+  ctx.mesh = *mesh;
+  ctx.model = *model;
+  ctx.H = H;
+  LinOp<double> A{t3_model_op, &ctx, sizeof(ctx)};
   int inf[2] = {0, 0};
   st = ppcg_solve(A, n, w, d_prev, d_init, fixed, fixed_vals, tol, max_iter, check_every, d_out, inf, s);
   if (info) {

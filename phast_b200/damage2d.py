@@ -22,7 +22,7 @@ class PhaseFieldDamageSolver:
     def __new__(cls, fem, *args, **kwargs):
         from .t3 import T3DamageSolver, T3FEMOperators
         if isinstance(fem, T3FEMOperators):
-            keep = {k: kwargs[k] for k in ("tol", "max_iter", "bounds_method") if k in kwargs}
+            keep = {k: kwargs[k] for k in ("tol", "max_iter", "bounds_method", "nodal_H") if k in kwargs}
             return T3DamageSolver(fem, *args[:2], **keep)
         return super().__new__(cls)
 

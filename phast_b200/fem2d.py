@@ -32,6 +32,7 @@ class Material:
     eta_residual: float = 1e-7
     energy_split: str = "amor"
     pf_model: str = "AT2"
+    at1_threshold: object = "auto"
     gamma_correction: bool = False
     degradation_type: str = "standard"
     stress_degradation: str = "split"
@@ -47,6 +48,16 @@ class Material:
     @property
     def mu(self):
         return self.E / (2 * (1 + self.nu))
+
+    @property
+    def at1_source(self):
+        """The AT1 source S_H of the damage right-hand side 2H - S_H: 3 Gc / (8 l0) unless
+        ``at1_threshold`` overrides it; 0 for AT2 (material.py:259-271)."""
+        if self.pf_model != "AT1":
+            return 0.0
+        if isinstance(self.at1_threshold, str) and self.at1_threshold == "auto":
+            return 3.0 * self.Gc / (8.0 * self.l0)
+        return float(self.at1_threshold)
 
     @property
     def kappa(self):

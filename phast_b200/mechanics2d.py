@@ -196,8 +196,10 @@ class QuasiStaticSolver:
         # one long CG per refinement: restarting a short CG discards its Krylov space, and the
         # adjoint right-hand side (concentrated on the loaded edge) needs many iterations on
         # large cracked meshes
-        st, info = self._newton(dd, r, mask, torch.zeros_like(r), z, rtol * nrm, 1e-10, max_refine, False,
-                                cg_max_iter=max(self.cg_max_iter, 200000))
+        # the inner CG's absolute threshold sits below the target, so a right-hand side much
+        # smaller than one (a reaction gradient) still converges in a refinement or two
+        st, info = self._newton(dd, r, mask, torch.zeros_like(r), z, rtol * nrm, min(1e-10, 0.5 * rtol * nrm),
+                                max_refine, False, cg_max_iter=max(self.cg_max_iter, 200000))
         if st != _lib.OK or not info[1]:
             raise RuntimeError(f"stiffness solve did not converge (status {st}, {int(info[0])} refinements)")
         return z

@@ -161,14 +161,21 @@ class T3FEMOperators:
 
 
 class T3DamageSolver:
-    """Bound-projected PCG AT2 damage solve on a T3 mesh (element H)."""
+    """Bound-projected PCG damage solve on a T3 mesh: AT2 with element or nodal history
+    (``nodal_H``), AT1 with element history (the combinations the reference supports,
+    damage_solver.py:1225-1236)."""
 
-    def __init__(self, fem, tol=1e-5, max_iter=5000, bounds_method="projected_cg"):
+    def __init__(self, fem, tol=1e-5, max_iter=5000, bounds_method="projected_cg", nodal_H=False):
         if bounds_method != "projected_cg":
             raise NotImplementedError("the B200 backend implements bounds_method='projected_cg'")
         mat = fem.material
-        if getattr(mat, "pf_model", "AT2") != "AT2":
-            raise NotImplementedError("T3 damage supports pf_model='AT2'")
+        self._pf_model = str(getattr(mat, "pf_model", "AT2")).upper()
+        if self._pf_model not in ("AT2", "AT1"):
+            raise NotImplementedError("T3 damage supports pf_model='AT2' and 'AT1'")
+        if nodal_H and self._pf_model != "AT2":
+            raise NotImplementedError(f"pf_model={self._pf_model!r} with nodal_H=True is not implemented "
+                                      "(the nodal-history system is AT2's)")
+        self.nodal_H = bool(nodal_H)
         self.fem = fem
         self.material = mat
         self.tol = float(tol)
@@ -181,6 +188,9 @@ class T3DamageSolver:
         self._ws = _lib.Workspace(fem.device)
 
     def _coeffs(self, Gc=None, l0=None, Gc_field=None):
+        if self._pf_model != "AT2" or self.nodal_H:
+            if Gc is not None or l0 is not None or Gc_field is not None:
+                raise NotImplementedError("material overrides are implemented for element-history AT2")
         Gc_s = self._Gc if Gc is None else float(Gc)
         l0_s = self._l0 if l0 is None else float(l0)
         gcl0_e = gco_e = None
@@ -191,12 +201,38 @@ class T3DamageSolver:
             gcl0_e, gco_e = (gf * l0_s).contiguous(), (gf / l0_s).contiguous()
         return Gc_s * l0_s, Gc_s / l0_s, gcl0_e, gco_e
 
+    def _model(self):
+        """The C-ABI model of AT1 or nodal-history AT2 (damage_solver.py:1316-1340), else None."""
+        if self._pf_model == "AT2" and not self.nodal_H:
+            return None
+        m = _lib.T3DamageModel()
+        m.nodal_h = int(self.nodal_H)
+        if self._pf_model == "AT1":
+            m.gcl0, m.gc_over_l0 = 0.75 * self._Gc * self._l0, 0.0
+            m.source = float(self.material.at1_source) if hasattr(self.material, "at1_source") else \
+                3.0 * self._Gc / (8.0 * self._l0)
+        else:
+            m.gcl0, m.gc_over_l0, m.source = self._Gc * self._l0, self._Gc / self._l0, 0.0
+        return m
+
+    def _history(self, H):
+        H = H.detach().to(torch.float64).contiguous()
+        want = (self.fem.n_nodes,) if self.nodal_H else (self.fem.n_elems,)
+        if tuple(H.shape) != want:
+            raise ValueError(f"T3 damage expects {'nodal' if self.nodal_H else 'element'} H of shape {want}")
+        return H
+
     def _Ax(self, d, reaction_H, Gc=None, l0=None, Gc_field=None):
         """(Gc l0 K + M(rc)) d with rc_e = (2 H_e + Gc/l0) A_e / 12 (damage_solver.py:1702-1755)."""
         gcl0, gco, gcl0_e, gco_e = self._coeffs(Gc, l0, Gc_field)
         d = d.to(torch.float64).contiguous()
         H = reaction_H.to(torch.float64).contiguous()
         y = torch.empty_like(d)
+        model = self._model()
+        if model is not None:
+            call("phastb_t3_damage_apply_ex", self.fem.t3, C.byref(model), ptr(d), ptr(self._history(H)), ptr(y),
+                 stream())
+            return y
         call("phastb_t3_damage_apply", self.fem.t3, ptr(d), ptr(H), gco, ptr(gco_e), gcl0, ptr(gcl0_e), ptr(y),
              stream())
         return y
@@ -209,6 +245,8 @@ class T3DamageSolver:
                      rtol=1e-11, max_iter=None):
         """Solve the unbounded AT2 system A x = rhs with ``fixed`` rows held at ``fixed_values``
         (_pcg_solve_adjoint_system, damage_solver.py:423-480)."""
+        if self._model() is not None:
+            raise NotImplementedError("the damage adjoint is implemented for element-history AT2")
         gcl0, gco, gcl0_e, gco_e = self._coeffs(Gc, l0, Gc_field)
         H = H_input.detach().to(torch.float64).contiguous()
         n = self.fem.n_nodes
@@ -230,6 +268,8 @@ class T3DamageSolver:
 
     def adjoint_grads(self, lam, d, Gc_field=None, l0=None):
         """(dJ/dGc_e (E,), dJ/dH_e (E,)) for the adjoint ``lam`` of the damage solve at ``d``."""
+        if self._model() is not None:
+            raise NotImplementedError("the damage adjoint is implemented for element-history AT2")
         l0_s = self._l0 if l0 is None else float(l0)
         E, dev = self.fem.n_elems, d.device
         g_gc = torch.empty(E, dtype=torch.float64, device=dev)
@@ -245,6 +285,11 @@ class T3DamageSolver:
         H = H.to(torch.float64).contiguous()
         b = torch.empty(self.fem.n_nodes, dtype=torch.float64, device=H.device)
         m = torch.empty_like(b)
+        model = self._model()
+        if model is not None:
+            call("phastb_t3_damage_prepare_ex", self.fem.t3, C.byref(model), ptr(self._history(H)), ptr(b), ptr(m),
+                 stream())
+            return b, m
         call("phastb_t3_damage_prepare", self.fem.t3, ptr(H), gco, ptr(gco_e), gcl0, ptr(gcl0_e), ptr(b), ptr(m),
              stream())
         return b, m
@@ -254,9 +299,7 @@ class T3DamageSolver:
         """d in [d_prev, 1] by projected CG (damage_solver.py:2493-2640, 3528-3775)."""
         self.n_solves += 1
         gcl0, gco, gcl0_e, gco_e = self._coeffs(Gc, l0, Gc_field)
-        H = H_input.detach().to(torch.float64).contiguous()
-        if tuple(H.shape) != (self.fem.n_elems,):
-            raise ValueError(f"T3 damage expects element H of shape ({self.fem.n_elems},)")
+        H = self._history(H_input)
         dp = d_prev.detach().to(torch.float64).contiguous()
         di = None if initial_guess is None else initial_guess.detach().to(torch.float64).contiguous()
         fixed = vals = None
@@ -269,10 +312,16 @@ class T3DamageSolver:
         out = torch.empty(n, dtype=torch.float64, device=dp.device)
         info = (C.c_int * 2)()
         wp, wn = self._ws.get(_lib.load().phastb_t3_damage_solve_workspace_bytes(n))
-        st = raw("phastb_t3_damage_solve", self.fem.t3, ptr(H), gco, ptr(gco_e), gcl0, ptr(gcl0_e), ptr(dp),
-                 ptr(di), ptr(fixed), ptr(vals), self.tol, self.max_iter, self.check_every, ptr(out), info, wp, wn,
-                 stream())
-        _lib.check(st, "phastb_t3_damage_solve")
+        model = self._model()
+        if model is not None:
+            st = raw("phastb_t3_damage_solve_ex", self.fem.t3, C.byref(model), ptr(H), ptr(dp), ptr(di), ptr(fixed),
+                     ptr(vals), self.tol, self.max_iter, self.check_every, ptr(out), info, wp, wn, stream())
+            _lib.check(st, "phastb_t3_damage_solve_ex")
+        else:
+            st = raw("phastb_t3_damage_solve", self.fem.t3, ptr(H), gco, ptr(gco_e), gcl0, ptr(gcl0_e), ptr(dp),
+                     ptr(di), ptr(fixed), ptr(vals), self.tol, self.max_iter, self.check_every, ptr(out), info, wp,
+                     wn, stream())
+            _lib.check(st, "phastb_t3_damage_solve")
         self.last_iter = int(info[0])
         self.last_converged = info[1] == 0
         return out.to(d_prev.dtype)

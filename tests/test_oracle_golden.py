@@ -211,3 +211,22 @@ def test_q4_tangent_oracle_matches_reference_jvp(key, split, ps):
     m = q4.Mat2D(E=210000.0, nu=0.3, Gc=2.7, l0=0.05, split=split, plane_stress=ps)
     assert rel(q4.internal_force(geo, m, g["tan_u"], g["tan_d"]), g[key + "_f"]) < 1e-12
     assert rel(q4.tangent_action(geo, m, g["tan_u"], g["tan_du"], g["tan_d"]), g[key]) < 1e-12
+
+
+def test_t3_at1_and_nodal_history_oracle():
+    """AT1 (element history) and AT2 with nodal history on the T3 twin against the reference."""
+    from oracle import solvers2d, t3
+    g = golden("t3_models")
+    geo = t3.geometry(g["nodes"], g["tris"])
+    rc, b, mi, gl = t3.damage_prepare_at1(geo, g["at1_H"], 2.7, 0.05)
+    assert rel(b, g["at1_b"]) < 1e-13 and rel(mi, g["at1_M_inv"]) < 1e-13
+    assert rel(t3.damage_apply(geo, g["x"], rc, gl), g["at1_Ax"]) < 1e-13
+    d, it = solvers2d.projected_cg(lambda x: t3.damage_apply(geo, x, rc, gl), b, mi, g["d_prev"], g["d_prev"],
+                                   1e-10, 3000)
+    assert rel(d, g["at1_d_solve"]) < 1e-12 and it == int(g["at1_iters"][0])
+    bn, mn = t3.damage_prepare_nodal(geo, g["nodal_H"], 2.7 / 0.05, 2.7 * 0.05)
+    assert rel(bn, g["nodal_b"]) < 1e-13 and rel(mn, g["nodal_M_inv"]) < 1e-13
+    act = lambda x: t3.damage_apply_nodal(geo, x, g["nodal_H"], 2.7 / 0.05, 2.7 * 0.05)  # noqa: E731
+    assert rel(act(g["x"]), g["nodal_Ax"]) < 1e-13
+    d, it = solvers2d.projected_cg(act, bn, mn, g["d_prev"], g["d_prev"], 1e-10, 3000)
+    assert rel(d, g["nodal_d_solve"]) < 1e-12 and it == int(g["nodal_iters"][0])
