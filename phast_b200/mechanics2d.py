@@ -193,16 +193,17 @@ class QuasiStaticSolver:
         if nrm == 0.0:
             return z
         dd = d.to(torch.float64).contiguous()
-        # one long CG per refinement: restarting a short CG discards its Krylov space, and the
-        # adjoint right-hand side (concentrated on the loaded edge) needs many iterations on
-        # large cracked meshes
-        # the inner CG's absolute threshold sits below the target, so a right-hand side much
-        # smaller than one (a reaction gradient) still converges in a refinement or two
-        st, info = self._newton(dd, r, mask, torch.zeros_like(r), z, rtol * nrm, min(1e-10, 0.5 * rtol * nrm),
-                                max_refine, False, cg_max_iter=max(self.cg_max_iter, 200000))
+        # The system is linear: solve for the unit-norm right-hand side and scale back, so the
+        # CG thresholds and curvature guards see numbers of order one whatever the size of rhs
+        # (a reaction gradient is small); the inner CG's threshold sits below the target, and one
+        # long CG per refinement keeps its Krylov space (a restarted short CG stalls on large
+        # cracked meshes).
+        r = (r / nrm).contiguous()
+        st, info = self._newton(dd, r, mask, torch.zeros_like(r), z, rtol, min(1e-10, 0.5 * rtol), max_refine, False,
+                                cg_max_iter=max(self.cg_max_iter, 200000))
         if st != _lib.OK or not info[1]:
             raise RuntimeError(f"stiffness solve did not converge (status {st}, {int(info[0])} refinements)")
-        return z
+        return z * nrm
 
 
 class _ExplicitRollout(torch.autograd.Function):
