@@ -503,24 +503,14 @@ def run_cfg3_action(device, flush, n_cells=16, brick=(16, 8, 8)):
             "blocks": B.n_blocks}
 
 
-def run_cfg3(device, flush, n_cells=128, increments=CFG3_INCREMENTS, per_cell=True):
-    """Bench line of cfg3: the seeded particle-in-cube batch advanced as one packed batch
-    (every cell in one launch per operator apply and per Krylov vector step), load
-    increments 1..K of every cell from the initial state, beside the same cells advanced one
-    at a time by the single-cell solver with the same algorithm."""
+def _batch_increments(B, load, cfg, flush, increments, mixed, form):
+    """Timed load increments 1..K of every cell of a packed batch, after one warm-up increment from a
+    separate initial state; returns (ms, records per increment)."""
     from phast_b200.solid3d import batch as bt
-    from phast_b200.solid3d.model import SolverConfig
-    from phast_b200.solid3d.staggered import MechForm, StaggeredSolver
-    peak, _ = peaks()
-    cells = bt.particle_cells(seed=0, n_cells=n_cells)
-    load = bt.batch_load()
-    ops = [bt.build_operator(c, load, device=device) for c in cells]
-    B = bt.PackedCellBatch(ops, brick=(16, 8, 8))
-    cfg = SolverConfig(kappa=ops[0].kappa)
-    solver = bt.BatchStaggeredSolver(B, load, cfg, mixed=True)
-    # warm-up increment (workspaces, captured graphs), then the timed window from the initial state
+    solver = bt.BatchStaggeredSolver(B, load, cfg, mixed=mixed, form=form)
     solver.advance(solver.initial_state(), load.targets[0])
     torch.cuda.synchronize()
+    solver = bt.BatchStaggeredSolver(B, load, cfg, mixed=mixed, form=form)
     state = solver.initial_state()
     total_ms, recs = 0.0, []
     for k in range(increments):
@@ -532,6 +522,49 @@ def run_cfg3(device, flush, n_cells=128, increments=CFG3_INCREMENTS, per_cell=Tr
         torch.cuda.synchronize()
         total_ms += e0.elapsed_time(e1)
         recs.append(r)
+    return total_ms, recs, state
+
+
+def _one_cell_at_a_time(ops, load, cfg, form, increments):
+    """The same increments with the single-cell solver, one cell after the other (each cell warmed up
+    on its own first increment); returns (ms, last record per cell)."""
+    from phast_b200.solid3d.staggered import StaggeredSolver
+    ms, last = 0.0, []
+    for op in ops:
+        sv = StaggeredSolver(op, cfg=cfg, form=form)
+        sv.advance(sv.initial_state(), load.targets[0])
+        sv = StaggeredSolver(op, cfg=cfg, form=form)
+        st1 = sv.initial_state()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(increments):
+            st1, r1 = sv.advance(st1, load.targets[k])
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        last.append(r1)
+    return ms, last
+
+
+def run_cfg3(device, flush, n_cells=128, increments=CFG3_INCREMENTS, per_cell=True):
+    """Bench line of cfg3: the seeded particle-in-cube batch advanced as one packed batch (every
+    cell in one launch per operator apply, per multigrid step and per Krylov vector step), load
+    increments 1..K of every cell from the initial state; beside the batch with Jacobi PCG and
+    the same cells advanced one at a time by the single-cell solver (same multigrid form, and the
+    plain FP64 form)."""
+    from phast_b200.solid3d import batch as bt
+    from phast_b200.solid3d.model import SolverConfig
+    from phast_b200.solid3d.staggered import PLAIN
+    peak, _ = peaks()
+    cells = bt.particle_cells(seed=0, n_cells=n_cells)
+    load = bt.batch_load()
+    ops = [bt.build_operator(c, load, device=device) for c in cells]
+    B = bt.PackedCellBatch(ops, brick=(16, 8, 8))
+    cfg = SolverConfig(kappa=ops[0].kappa)
+    gmg = forms()["mixed-gmg"]
+    total_ms, recs, state = _batch_increments(B, load, cfg, flush, increments, True, gmg)
+    jac_ms, jac_recs, _ = _batch_increments(B, load, cfg, flush, increments, True, None)
     voxels = sum(op.n_elements for op in ops)
     mech_its = sum(r.pcg_iters_mech for rr in recs for r in rr)
     pf_its = sum(r.pcg_iters_pf for rr in recs for r in rr)
@@ -553,44 +586,44 @@ def run_cfg3(device, flush, n_cells=128, increments=CFG3_INCREMENTS, per_cell=Tr
         torch.cuda.synchronize()
         act_ms += e0.elapsed_time(e1) / 10
     act_bytes = sum(7 * op.n_red * 4 + op.n_elements for op in ops)
+    rate = lambda ms: n_cells * increments / (ms / 1e3)  # noqa: E731
+
+    def worst_err(a_recs, b_recs):
+        w = 0.0
+        for a, b in zip(a_recs, b_recs):
+            a, b = np.asarray(a.macro_stress), np.asarray(b.macro_stress)
+            w = max(w, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
+        return w
+
     line = {"workload": f"{n_cells} seeded periodic particle-in-cube cells (edge N in {{32,40,48,56,64}}, "
                         f"{voxels} voxels in all), eps_xx ramp 0 -> 0.015 over 40 steps; increments 1..{increments} "
-                        "of every cell as one packed batch: FP32 Jacobi PCG (FP64 dots) under FP64 refinement, "
-                        "FP64 box-KKT damage",
+                        "of every cell as one packed batch: FP32 PCG with the batched 3-level multigrid V-cycle "
+                        "(FP64 dots) under FP64 refinement, FP64 box-KKT damage",
             "dtype": "f32 mechanics (f64 dots, f64 refinement), f64 damage",
-            "value": n_cells * increments / (total_ms / 1e3), "unit": "cell increments/s",
+            "value": rate(total_ms), "unit": "cell increments/s",
             "ms_per_batch_increment": total_ms / increments,
             "dof_updates_per_s": dof_updates / (total_ms / 1e3),
             "mech_iters_per_cell_increment": mech_its / (n_cells * increments),
             "damage_pcg_iters_per_cell_increment": pf_its / (n_cells * increments),
+            "batched_jacobi": {"value": rate(jac_ms), "ms_per_batch_increment": jac_ms / increments,
+                               "mech_iters_per_cell_increment":
+                                   sum(r.pcg_iters_mech for rr in jac_recs for r in rr) / (n_cells * increments)},
             "batched_action": {"kernel": "h8_tile_batch_kernel<float> (every cell in one launch)",
                                "launch_ms": act_ms, "algorithmic_bytes": act_bytes,
                                "achieved_GBps": act_bytes / (act_ms / 1e3) / 1e9,
                                "hbm_frac": act_bytes / (act_ms / 1e3) / 1e9 / peak,
                                "l2": "working set beyond the 126 MB L2"}}
     if per_cell:
-        # the same cells one at a time (single-cell solver, same algorithm: FP32 Jacobi PCG under refinement)
-        form = MechForm(mixed=True)
-        one_ms, worst = 0.0, 0.0
-        for c, op in enumerate(ops):
-            sv = StaggeredSolver(op, cfg=cfg, form=form)
-            st1 = sv.initial_state()
-            sv.advance(st1, load.targets[0])  # warm-up of this cell's workspaces
-            st1 = sv.initial_state()
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for k in range(increments):
-                st1, r1 = sv.advance(st1, load.targets[k])
-            e1.record()
-            torch.cuda.synchronize()
-            one_ms += e0.elapsed_time(e1)
-            a, b = np.asarray(recs[-1][c].macro_stress), np.asarray(r1.macro_stress)
-            worst = max(worst, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
-        line["one_cell_at_a_time"] = {"value": n_cells * increments / (one_ms / 1e3), "unit": "cell increments/s",
+        one_ms, one_last = _one_cell_at_a_time(ops, load, cfg, gmg, increments)
+        plain_ms, plain_last = _one_cell_at_a_time(ops, load, cfg, PLAIN, increments)
+        line["one_cell_at_a_time"] = {"form": "the same multigrid form, single-cell solver", "value": rate(one_ms),
                                       "ms_per_batch_increment": one_ms / increments}
+        line["plain_fp64_one_cell_at_a_time"] = {"form": "plain FP64 (Jacobi PCG), single-cell solver",
+                                                 "value": rate(plain_ms), "ms_per_batch_increment": plain_ms / increments}
         line["speedup_vs_one_cell_at_a_time"] = one_ms / total_ms
-        line["rel_err_macro_stress_vs_one_cell_at_a_time"] = worst
+        line["speedup_vs_plain_fp64"] = plain_ms / total_ms
+        line["rel_err_macro_stress_vs_plain_fp64"] = worst_err(recs[-1], plain_last)
+        line["rel_err_macro_stress_jacobi_vs_plain_fp64"] = worst_err(jac_recs[-1], plain_last)
     return line
 
 

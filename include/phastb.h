@@ -590,6 +590,19 @@ int phastb_batch_mech_solve(const phastb_batch* batch, const phastb_voxel_materi
                             int max_refine, const int* live_host, double* x_out, int* info, double* rinfo,
                             void* workspace, size_t workspace_bytes, void* stream);
 
+/* phastb_batch_mech_solve with the options of phastb_h8_mech_solve_ex: precond = 1 (with mixed = 1
+ * and levels = 3) preconditions every cell's FP32 inner PCG with the voxel multigrid V-cycle of
+ * phastb_h8_mech_solve_ex, all cells in the same launches (every cell's edges divisible by 4 and at
+ * least 32, periodic).  reuse_lmax = 1 keeps the per-cell lambda_max estimates of the previous
+ * call with the same workspace.  The voxel multigrid has no counterpart in PhAST's 3D code (its 2D
+ * GMG semantics: multigrid.py:534-576, 996-1089). */
+size_t phastb_batch_mech_solve_ex_workspace_bytes(const phastb_batch* batch, const phastb_mech_opts* o);
+int phastb_batch_mech_solve_ex(const phastb_batch* batch, const phastb_voxel_material* m, const uint8_t* slot,
+                               const double* d, const uint8_t* fixed, const double* fixed_values, const double* x0,
+                               double rtol, double atol, int maxiter, int check_every, const phastb_mech_opts* o,
+                               int reuse_lmax, const int* live_host, double* x_out, int* info, double* rinfo,
+                               void* workspace, size_t workspace_bytes, void* stream);
+
 /* Box-constrained damage solve of every cell's scaled system (solve_h8_scalar_box_kkt,
  * solvers/box_kkt_h8.py:256-778).  tol_rule = 1 sets each cell's linear tolerance as the
  * staggered solver does, max(min(lin_tol, 0.1 kkt_tol / max(r0, 1)), min_tol) with r0 the

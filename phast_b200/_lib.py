@@ -155,6 +155,9 @@ SIGNATURES = {
     "phastb_batch_mech_solve_workspace_bytes": (sz, [vp, C.c_int]),
     "phastb_batch_mech_solve": (C.c_int, [vp, VM, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_int,
                                           C.c_int, C.c_double, C.c_int, ip, vp, ip, dp, vp, sz, vp]),
+    "phastb_batch_mech_solve_ex_workspace_bytes": (sz, [vp, MO]),
+    "phastb_batch_mech_solve_ex": (C.c_int, [vp, VM, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_int,
+                                             MO, C.c_int, ip, vp, ip, dp, vp, sz, vp]),
     "phastb_batch_box_kkt_workspace_bytes": (sz, [vp]),
     "phastb_batch_damage_box_kkt": (C.c_int, [vp, VM, vp, vp, vp, C.c_double, vp, C.c_double, C.c_double,
                                               C.c_double, C.c_int, C.c_int, C.c_int, ip, vp, ip, dp, vp, sz, vp]),

@@ -71,7 +71,20 @@ struct phastb_batch {
   int* d_node_nchunk = nullptr;
   int* d_mech_nchunk = nullptr;
   bool bound = false;
-  size_t table_bytes = 0;
+  size_t table_bytes = 0;     // this level's tables
+  // coarse multigrid levels (cells of edge n/2 and n/4 with 8 x 8 x 4 bricks), when every cell
+  // is periodic with edges divisible by 4 and at least 32
+  phastb_batch* lev[2] = {nullptr, nullptr};
+  int nlev = 1;
+  ~phastb_batch() {
+    delete lev[0];
+    delete lev[1];
+  }
+  size_t all_table_bytes() const {
+    size_t t = table_bytes;
+    for (int l = 0; l < nlev - 1; ++l) t += lev[l]->table_bytes;
+    return t;
+  }
 };
 
 namespace phastb {
@@ -739,6 +752,390 @@ __global__ void __launch_bounds__(kThreads) b_change_damage_kernel(BVec V, const
   }
 }
 
+// ------------------------------------------------------------ batched multigrid
+//
+// The V-cycle of gmg.cu (Chebyshev smoothing in D^-1 A, trilinear transfers,
+// coarse-level mean removal, a Jacobi step on the fine E rows) on every cell of a
+// packed batch at once, FP32.  Each level is a packed plan of its own (coarse
+// vectors use the mechanics layout with six unused, zero entries per cell); the
+// Chebyshev interval and therefore 1/theta and 1/delta differ per cell (one
+// lambda_max per cell and level), the step coefficients c1 and the 2 rho of c2 do
+// not.  Every kernel is guarded per cell by the Krylov engine's `active` flag.
+
+__device__ __forceinline__ bool cell_live(const int* guard, int stride, int c) {
+  return !guard || guard[(size_t)c * stride] != 0;
+}
+
+// res = b (less the cell's pending per-component mean when bsum_red is given, stored back
+// into b); d = invd b / theta_c; x = d  (gmg_cheb_first_b)
+__global__ void bg_first_b_kernel(BVec V, const BatchCell* cells, float* __restrict__ b,
+                                  const float* __restrict__ invd, const double* __restrict__ inv_theta,
+                                  float* __restrict__ res, float* __restrict__ d, float* __restrict__ x,
+                                  const char* bsum_red, const int* guard, int gstride) {
+  const BChunk ck = V.chunks[blockIdx.x];
+  const int c = ck.cell;
+  if (!cell_live(guard, gstride, c)) return;
+  const BatchCell& cl = cells[c];
+  const float it = float(inv_theta[c]);
+  float m[3] = {0.f, 0.f, 0.f};
+  if (bsum_red) {
+    const double* o = cell_out(bsum_red, c);
+    for (int k = 0; k < 3; ++k) m[k] = float(o[k] / cl.g.n_red);
+  }
+  const long long nu = cl.mech_off + 3LL * cl.g.n_red;
+  for (int i = ck.begin + threadIdx.x; i < ck.end; i += blockDim.x) {
+    float bi = b[i];
+    if (bsum_red && i < nu) {
+      bi -= m[(i - cl.mech_off) % 3];
+      b[i] = bi;
+    }
+    res[i] = bi;
+    const float di = invd[i] * bi * it;
+    d[i] = di;
+    x[i] = di;
+  }
+}
+
+// res = b - Ax; d = invd res / theta_c; x += d; on the fine level (e_rows) the E rows of x get
+// the Jacobi step of the macro-strain block, x_E = fixed ? 0 : b_E / diag_E  (gmg_cheb_first_res)
+__global__ void bg_first_res_kernel(BVec V, const BatchCell* cells, const float* __restrict__ b,
+                                    const float* __restrict__ Ax, const float* __restrict__ invd,
+                                    const double* __restrict__ inv_theta, float* __restrict__ res,
+                                    float* __restrict__ d, float* __restrict__ x, int e_rows,
+                                    const float* __restrict__ diag, const uint8_t* __restrict__ fixed,
+                                    const int* guard, int gstride) {
+  const BChunk ck = V.chunks[blockIdx.x];
+  const int c = ck.cell;
+  if (!cell_live(guard, gstride, c)) return;
+  const BatchCell& cl = cells[c];
+  const float it = float(inv_theta[c]);
+  const long long nu = cl.mech_off + 3LL * cl.g.n_red;
+  for (int i = ck.begin + threadIdx.x; i < ck.end; i += blockDim.x) {
+    const float r = b[i] - Ax[i];
+    res[i] = r;
+    const float di = invd[i] * r * it;
+    d[i] = di;
+    if (e_rows && i >= nu)
+      x[i] = fixed[i] ? 0.f : b[i] / diag[i];
+    else
+      x[i] = x[i] + di;
+  }
+}
+
+__device__ __forceinline__ int bg_wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+// r_c = P^T r_f per coarse node (full weighting, fine rows in `mask` read as zero), and each
+// cell's three component sums of r_c (its mean, removed by the first coarse smoothing step).
+__global__ void __launch_bounds__(kThreads) bg_restrict_kernel(BVec Vc, const BatchCell* fcells,
+                                                               const BatchCell* ccells, const float* __restrict__ rf,
+                                                               const uint8_t* __restrict__ mask,
+                                                               float* __restrict__ rc, char* sum_red,
+                                                               const int* guard, int gstride) {
+  const BChunk ck = Vc.chunks[blockIdx.x];
+  const int c = ck.cell;
+  if (!cell_live(guard, gstride, c)) return;
+  const VoxGeom& f = fcells[c].g;
+  const VoxGeom& cg = ccells[c].g;
+  const long long fo = fcells[c].mech_off, co = ccells[c].mech_off, no = ccells[c].node_off;
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int n = ck.begin + threadIdx.x; n < ck.end; n += blockDim.x) {
+    const int ln = (int)(n - no);
+    const int I = ln % cg.rx, rem = ln / cg.rx, J = rem % cg.ry, K = rem / cg.ry;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    for (int oz = -1; oz <= 1; ++oz) {
+      const int k = bg_wrap(2 * K + oz, f.nz);
+      const float wz = oz == 0 ? 1.f : 0.5f;
+      for (int oy = -1; oy <= 1; ++oy) {
+        const int j = bg_wrap(2 * J + oy, f.ny);
+        const float wy = oy == 0 ? 1.f : 0.5f;
+        for (int ox = -1; ox <= 1; ++ox) {
+          const int i = bg_wrap(2 * I + ox, f.nx);
+          const float wgt = (ox == 0 ? 1.f : 0.5f) * wy * wz;
+          const long long fn = fo + 3LL * ((long long)i + (long long)f.rx * ((long long)j + (long long)f.ry * k));
+          a0 += wgt * ((mask && mask[fn + 0]) ? 0.f : rf[fn + 0]);
+          a1 += wgt * ((mask && mask[fn + 1]) ? 0.f : rf[fn + 1]);
+          a2 += wgt * ((mask && mask[fn + 2]) ? 0.f : rf[fn + 2]);
+        }
+      }
+    }
+    const long long cn = co + 3LL * ln;
+    rc[cn + 0] = a0;
+    rc[cn + 1] = a1;
+    rc[cn + 2] = a2;
+    v[0] += double(a0);
+    v[1] += double(a1);
+    v[2] += double(a2);
+  }
+  seg_fold<3>(v, sum_red, ck, Vc.nchunk[c], [&](const double* f3, RedWs& w) {
+    for (int k = 0; k < 3; ++k) w.out[k] = f3[k];
+  });
+}
+
+// x_f += P (x_c - mean_c) per fine node, rows in `mask` untouched  (gmg_prolong_add)
+__global__ void bg_prolong_kernel(BVec Vf, const BatchCell* fcells, const BatchCell* ccells,
+                                  const float* __restrict__ xc, const uint8_t* __restrict__ mask,
+                                  float* __restrict__ xf, const char* csum_red, const int* guard, int gstride) {
+  const BChunk ck = Vf.chunks[blockIdx.x];
+  const int c = ck.cell;
+  if (!cell_live(guard, gstride, c)) return;
+  const VoxGeom& f = fcells[c].g;
+  const VoxGeom& cg = ccells[c].g;
+  const long long fo = fcells[c].mech_off, co = ccells[c].mech_off, no = fcells[c].node_off;
+  float m0 = 0.f, m1 = 0.f, m2 = 0.f;
+  if (csum_red) {
+    const double* o = cell_out(csum_red, c);
+    m0 = float(o[0] / cg.n_red);
+    m1 = float(o[1] / cg.n_red);
+    m2 = float(o[2] / cg.n_red);
+  }
+  for (int n = ck.begin + threadIdx.x; n < ck.end; n += blockDim.x) {
+    const int ln = (int)(n - no);
+    const int i = ln % f.rx, rem = ln / f.rx, j = rem % f.ry, k = rem / f.ry;
+    int I[2] = {i >> 1, 0}, J[2] = {j >> 1, 0}, K[2] = {k >> 1, 0};
+    float wx[2] = {1.f, 0.f}, wy[2] = {1.f, 0.f}, wz[2] = {1.f, 0.f};
+    int cx = 1, cy = 1, cz = 1;
+    if (i & 1) { I[1] = bg_wrap(I[0] + 1, cg.nx); wx[0] = wx[1] = 0.5f; cx = 2; }
+    if (j & 1) { J[1] = bg_wrap(J[0] + 1, cg.ny); wy[0] = wy[1] = 0.5f; cy = 2; }
+    if (k & 1) { K[1] = bg_wrap(K[0] + 1, cg.nz); wz[0] = wz[1] = 0.5f; cz = 2; }
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    for (int z = 0; z < cz; ++z)
+      for (int yy = 0; yy < cy; ++yy)
+        for (int xx = 0; xx < cx; ++xx) {
+          const long long cn = co + 3LL * ((long long)I[xx] + (long long)cg.rx * ((long long)J[yy] + (long long)cg.ry * K[z]));
+          const float wgt = wx[xx] * wy[yy] * wz[z];
+          a0 += wgt * (xc[cn + 0] - m0);
+          a1 += wgt * (xc[cn + 1] - m1);
+          a2 += wgt * (xc[cn + 2] - m2);
+        }
+    const long long fn = fo + 3LL * ln;
+    if (!(mask && mask[fn + 0])) xf[fn + 0] += a0;
+    if (!(mask && mask[fn + 1])) xf[fn + 1] += a1;
+    if (!(mask && mask[fn + 2])) xf[fn + 2] += a2;
+  }
+}
+
+// each cell's three component sums of a level vector (gmg_mean3), over the level's node chunks
+__global__ void __launch_bounds__(kThreads) bg_mean3_kernel(BVec Vn, const BatchCell* cells,
+                                                            const float* __restrict__ x, char* red, const int* guard,
+                                                            int gstride) {
+  const BChunk ck = Vn.chunks[blockIdx.x];
+  const int c = ck.cell;
+  if (!cell_live(guard, gstride, c)) return;
+  const long long mo = cells[c].mech_off, no = cells[c].node_off;
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int n = ck.begin + threadIdx.x; n < ck.end; n += blockDim.x) {
+    const long long i = mo + 3LL * (n - no);
+    v[0] += double(x[i]);
+    v[1] += double(x[i + 1]);
+    v[2] += double(x[i + 2]);
+  }
+  seg_fold<3>(v, red, ck, Vn.nchunk[c], [&](const double* f3, RedWs& w) {
+    for (int k = 0; k < 3; ++k) w.out[k] = f3[k];
+  });
+}
+
+// power iteration for lambda_max(D^-1 A) per cell: a deterministic non-smooth start ...
+__global__ void bg_power_init_kernel(BVec V, const BatchCell* cells, const uint8_t* __restrict__ mask,
+                                     float* __restrict__ v) {
+  const BChunk ck = V.chunks[blockIdx.x];
+  const BatchCell& cl = cells[ck.cell];
+  const long long nu = cl.mech_off + 3LL * cl.g.n_red;
+  for (int i = ck.begin + threadIdx.x; i < ck.end; i += blockDim.x) {
+    unsigned h = (unsigned)(i - cl.mech_off) * 2654435761u;
+    h ^= h >> 13;
+    h *= 0x5bd1e995u;
+    h ^= h >> 15;
+    v[i] = (i >= nu || (mask && mask[i])) ? 0.f : float(0.5 + (h & 0xffff) / 65536.0);
+  }
+}
+
+// ... v <- D^-1 A v with its D-norm squared per cell (out[0]) ...
+__global__ void __launch_bounds__(kThreads) bg_power_next_kernel(BVec V, const float* __restrict__ Av,
+                                                                 const float* __restrict__ invd,
+                                                                 const float* __restrict__ diag,
+                                                                 float* __restrict__ v, char* red) {
+  const BChunk ck = V.chunks[blockIdx.x];
+  double acc[1] = {0.0};
+  for (int i = ck.begin + threadIdx.x; i < ck.end; i += blockDim.x) {
+    const float z = invd[i] * Av[i];
+    v[i] = z;
+    acc[0] += double(z) * double(diag[i]) * double(z);
+  }
+  seg_fold<1>(acc, red, ck, V.nchunk[ck.cell], [&](const double* f, RedWs& w) { w.out[0] = f[0]; });
+}
+
+// ... normalised by that norm ...
+__global__ void bg_power_scale_kernel(BVec V, const char* red, float* __restrict__ v) {
+  const BChunk ck = V.chunks[blockIdx.x];
+  const double sm = cell_out(red, ck.cell)[0];
+  const double sc = sm > 0 ? 1.0 / sqrt(sm) : 0.0;
+  for (int i = ck.begin + threadIdx.x; i < ck.end; i += blockDim.x) v[i] = float(double(v[i]) * sc);
+}
+
+// ... and the Rayleigh quotient v.Av / v.Dv over the free rows at the last step
+__global__ void __launch_bounds__(kThreads) bg_power_dots_kernel(BVec V, const float* __restrict__ v,
+                                                                 const float* __restrict__ Av,
+                                                                 const float* __restrict__ diag,
+                                                                 const uint8_t* __restrict__ mask, char* red) {
+  const BChunk ck = V.chunks[blockIdx.x];
+  double acc[2] = {0.0, 0.0};
+  for (int i = ck.begin + threadIdx.x; i < ck.end; i += blockDim.x) {
+    if (mask && mask[i]) continue;
+    acc[0] += double(v[i]) * double(Av[i]);
+    acc[1] += double(v[i]) * double(diag[i]) * double(v[i]);
+  }
+  seg_fold<2>(acc, red, ck, V.nchunk[ck.cell], [&](const double* f, RedWs& w) {
+    w.out[0] = f[0];
+    w.out[1] = f[1];
+  });
+}
+
+// per cell: lambda_max from the Rayleigh quotient (or the cached value), and the Chebyshev
+// factors 1/theta and 1/delta of the interval [lmax/30, safety lmax]
+__global__ void bg_cheb_factors_kernel(int n_cells, const char* red, int from_red, double* lmax, double safety,
+                                       double* inv_theta, double* inv_delta) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cells; c += gridDim.x * blockDim.x) {
+    if (from_red) {
+      const double* o = cell_out(red, c);
+      lmax[c] = o[1] > 0 ? o[0] / o[1] : 1.0;
+    }
+    const double bmax = safety * lmax[c], amin = lmax[c] / 30.0;
+    inv_theta[c] = 1.0 / (0.5 * (bmax + amin));
+    inv_delta[c] = 1.0 / (0.5 * (bmax - amin));
+  }
+}
+
+// fine-level mask of the multigrid: the solve's fixed rows and every E row
+__global__ void bg_fine_mask_kernel(BVec V, const BatchCell* cells, const uint8_t* __restrict__ fixed,
+                                    uint8_t* __restrict__ mask) {
+  const BChunk ck = V.chunks[blockIdx.x];
+  const BatchCell& cl = cells[ck.cell];
+  const long long nu = cl.mech_off + 3LL * cl.g.n_red;
+  for (int i = ck.begin + threadIdx.x; i < ck.end; i += blockDim.x) mask[i] = fixed[i] || i >= nu;
+}
+
+// inv = mask ? 0 : 1/diag; on coarse levels the six unused entries per cell are 0 too
+__global__ void bg_invert_kernel(BVec V, const BatchCell* cells, const float* __restrict__ diag,
+                                 const uint8_t* __restrict__ mask, float* __restrict__ inv) {
+  const BChunk ck = V.chunks[blockIdx.x];
+  const BatchCell& cl = cells[ck.cell];
+  const long long nu = cl.mech_off + 3LL * cl.g.n_red;
+  for (int i = ck.begin + threadIdx.x; i < ck.end; i += blockDim.x)
+    inv[i] = ((mask && mask[i]) || (!mask && i >= nu)) ? 0.f : 1.f / diag[i];
+}
+
+// ---- batched PCG with a preconditioner (pcg_run with M): r, rr; then z = M r; rz; p = z
+
+// r = b - Ap; rr; the start-of-solve decisions without z (rz follows once M has run)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) bpcg_start_pre_kernel(BVec V, BPcg<T> w, const T* __restrict__ b,
+                                                                  const double* abs_sq, double rel,
+                                                                  const char* outer_red, const double* outer_thr_sq,
+                                                                  const int* live) {
+  const BChunk ck = V.chunks[blockIdx.x];
+  if (live && !live[ck.cell]) {
+    if (ck.j == 0 && threadIdx.x == 0) w.st[ck.cell] = PcgState{};
+    return;
+  }
+  double v[1] = {0.0};
+  for (int i = ck.begin + threadIdx.x; i < ck.end; i += blockDim.x) {
+    const T r = b[i] - w.Ap[i];
+    w.r[i] = r;
+    v[0] += double(r) * double(r);
+  }
+  const int c = ck.cell;
+  seg_fold<1>(v, w.red, ck, V.nchunk[c], [&](const double* f, RedWs&) {
+    PcgState& st = w.st[c];
+    const double RR = f[0];
+    st = PcgState{};
+    st.rr = RR;
+    st.rr0 = RR;
+    const double t = rel > 0.0 ? rel * sqrt(RR) : 0.0;
+    st.thr_sq = fmax(abs_sq ? abs_sq[c] : 0.0, t * t);
+    st.active = 1;
+    if (outer_red) st.outer_rr = cell_out(outer_red, c)[0];
+    if (outer_red && isfinite(st.outer_rr) && !(st.outer_rr > outer_thr_sq[c])) {
+      st.outer_done = 1;
+      st.active = 0;
+    } else if (!isfinite(RR) || (outer_red && !isfinite(st.outer_rr))) {
+      st.nonfinite = 1;
+      st.active = 0;
+    } else if (!(RR > st.thr_sq)) {
+      st.converged = 1;
+      st.active = 0;
+    }
+  });
+}
+
+// rz per cell after z = M r: at the start rz itself, later beta = rz_new / rz (pcg_rz_kernel)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) bpcg_rz_kernel(BVec V, BPcg<T> w, int start) {
+  const BChunk ck = V.chunks[blockIdx.x];
+  const int c = ck.cell;
+  PcgState* S = w.st + c;
+  if (!S->active) return;
+  double v[1] = {0.0};
+  for (int i = ck.begin + threadIdx.x; i < ck.end; i += blockDim.x) {
+    v[0] += double(w.r[i]) * double(w.z[i]);
+    if (start) w.p[i] = w.z[i];
+  }
+  seg_fold<1>(v, w.red, ck, V.nchunk[c], [&](const double* f, RedWs&) {
+    PcgState& st = *S;
+    const double RZ = f[0];
+    if (!isfinite(RZ)) st.nonfinite = 1;
+    if (start) {
+      st.rz = RZ;
+    } else {
+      st.beta = st.rz > 0.0 ? RZ / st.rz : 0.0;
+      st.rz = RZ;
+    }
+    if (st.nonfinite) st.active = 0;
+  });
+}
+
+// alpha from the action's p.Ap; x += alpha p; r -= alpha Ap; rr and the convergence test
+template <typename T>
+__global__ void __launch_bounds__(kThreads) bpcg_update_pre_kernel(BVec V, BPcg<T> w, T* __restrict__ x,
+                                                                   const char* dot_red) {
+  const BChunk ck = V.chunks[blockIdx.x];
+  const int c = ck.cell;
+  PcgState* S = w.st + c;
+  if (!S->active) return;
+  const double PAP = cell_out(dot_red, c)[kOutDot];
+  const bool ok = isfinite(PAP) && PAP > 0.0;
+  const double alpha = S->rz / PAP;
+  const T a = T(alpha);
+  double v[1] = {0.0};
+  if (ok) {
+    for (int i = ck.begin + threadIdx.x; i < ck.end; i += blockDim.x) {
+      x[i] = x[i] + a * w.p[i];
+      const T r = w.r[i] - a * w.Ap[i];
+      w.r[i] = r;
+      v[0] += double(r) * double(r);
+    }
+  }
+  seg_fold<1>(v, w.red, ck, V.nchunk[c], [&](const double* f, RedWs&) {
+    PcgState& st = *S;
+    const double RR = f[0];
+    st.iter += 1;
+    if (!ok) {
+      if (!isfinite(PAP)) st.nonfinite = 1;
+      if (!(PAP > 0.0)) st.breakdown = 1;
+      st.active = 0;
+      return;
+    }
+    st.alpha = alpha;
+    st.steps += 1;
+    if (!isfinite(RR)) st.nonfinite = 1;
+    st.rr = RR;
+    if (!(RR > st.thr_sq)) {
+      st.converged = 1;
+      st.active = 0;
+    }
+    if (st.nonfinite) st.active = 0;
+  });
+}
+
 // ------------------------------------------------------------ workspace layout
 
 struct Carve {
@@ -802,6 +1199,325 @@ int batch_damage_op(const phastb_batch* B, const VoxMat<double>& m, const uint8_
   return h8_dtile_batch_launch<double>(a, m, dot, B->ox, B->oy, s);
 }
 
+int gmg_level_coefs_f32(const VoxGeom& f, const VoxGeom& c, const VoxMat<float>& m, const uint8_t* slot,
+                        const float* d, const float* lam_f, const float* mu_f, float* lam_c, float* mu_c,
+                        cudaStream_t s);
+int gmg_coarse_diag_f32(const VoxGeom& c, const float* lam, const float* mu, float* scratch, float* diag,
+                        cudaStream_t s);
+
+namespace {
+
+// One level of the batch's multigrid hierarchy (FP32 vectors in the level plan's layout).
+struct BLevel {
+  const phastb_batch* P;
+  float *diag, *invd, *x, *b, *res, *dvec, *Ad, *lam, *mu;
+  double *lmax, *inv_theta, *inv_delta;  // per cell
+  char* red;                             // per-cell reductions of the level (means, power iteration)
+  char* ared;                            // per-cell workspaces of the level's tile launches
+};
+
+struct BGmg {
+  int nlev;
+  BLevel L[3];
+  VoxMat<float> m;
+  const uint8_t* slot;
+  const float* d32;
+  uint8_t* mask;         // fine level: the solve's fixed rows and the E rows
+  const uint8_t* fixed;  // fine level: the solve's fixed rows
+  double safety;
+  int deg, deg_coarse;
+  const int* guard;      // the Krylov engine's per-cell active flags
+  int gstride;
+};
+
+size_t bgmg_bytes(const phastb_batch* B) {
+  Carve cv{nullptr};
+  for (int l = 0; l < B->nlev; ++l) {
+    const phastb_batch* P = l == 0 ? B : B->lev[l - 1];
+    for (int k = 0; k < 7; ++k) cv.take<float>((size_t)P->n_mech);
+    if (l > 0) {
+      cv.take<float>(8 * (size_t)P->n_elem);
+      cv.take<float>(8 * (size_t)P->n_elem);
+    }
+    for (int k = 0; k < 3; ++k) cv.take<double>((size_t)P->n_cells);
+    cv.take<char>(n_red_ws(P));
+    cv.take<char>(n_red_ws(P));
+  }
+  cv.take<uint8_t>((size_t)B->n_mech);
+  return cv.used;
+}
+
+void bgmg_carve(BGmg& M, const phastb_batch* B, char* base) {
+  Carve cv{base};
+  M.nlev = B->nlev;
+  for (int l = 0; l < B->nlev; ++l) {
+    BLevel& L = M.L[l];
+    L.P = l == 0 ? B : B->lev[l - 1];
+    float** v[7] = {&L.diag, &L.invd, &L.x, &L.b, &L.res, &L.dvec, &L.Ad};
+    for (auto q : v) *q = cv.take<float>((size_t)L.P->n_mech);
+    L.lam = L.mu = nullptr;
+    if (l > 0) {
+      L.lam = cv.take<float>(8 * (size_t)L.P->n_elem);
+      L.mu = cv.take<float>(8 * (size_t)L.P->n_elem);
+    }
+    L.lmax = cv.take<double>((size_t)L.P->n_cells);
+    L.inv_theta = cv.take<double>((size_t)L.P->n_cells);
+    L.inv_delta = cv.take<double>((size_t)L.P->n_cells);
+    L.red = cv.take<char>(n_red_ws(L.P));
+    L.ared = cv.take<char>(n_red_ws(L.P));
+  }
+  M.mask = cv.take<uint8_t>((size_t)B->n_mech);
+}
+
+TileBatchArgs<float> bg_args(const BGmg& M, int l, const float* x) {
+  const BLevel& L = M.L[l];
+  TileBatchArgs<float> a{};
+  a.cells = L.P->d_cells;
+  a.work = L.P->d_work;
+  a.n_blocks = (int)L.P->work.size();
+  a.guard = M.guard;
+  a.guard_stride = M.gstride;
+  a.x = x;
+  a.ws = L.ared;
+  if (l == 0) {
+    a.slot = M.slot;
+    a.d = M.d32;
+    a.mask = M.mask;
+  } else {
+    a.lam_q = L.lam;
+    a.mu_q = L.mu;
+  }
+  return a;
+}
+
+// y = A x on level l (the fine level's nodal block only: its smoother leaves the E rows alone)
+int bg_level_apply(const BGmg& M, int l, const float* x, float* y, cudaStream_t s) {
+  TileBatchArgs<float> a = bg_args(M, l, x);
+  a.y = y;
+  return h8_tile_batch_level_launch(a, M.m, l == 0 ? kCoefIso : kCoefQP, l == 0 ? kModeNodal : kModeApply,
+                                    M.L[l].P->ox, M.L[l].P->oy, s);
+}
+
+// one fused Chebyshev step: res -= A din; dout = c1 din + c2 s_c invd res; x += dout
+int bg_level_cheb(const BGmg& M, int l, const float* din, float* dout, double c1, double c2, bool scaled,
+                  cudaStream_t s) {
+  const BLevel& L = M.L[l];
+  TileBatchArgs<float> a = bg_args(M, l, din);
+  a.res = L.res;
+  a.invd = L.invd;
+  a.xs = L.x;
+  a.d_out = dout;
+  a.c1 = c1;
+  a.c2 = c2;
+  a.c2_scale = scaled ? L.inv_delta : nullptr;
+  return h8_tile_batch_level_launch(a, M.m, l == 0 ? kCoefIso : kCoefQP, kModeCheb, L.P->ox, L.P->oy, s);
+}
+
+BVec level_mech_vec(const phastb_batch* P) { return mech_vec(P); }
+BVec level_node_vec(const phastb_batch* P) { return node_vec(P); }
+
+// Chebyshev smoothing of A x = b on level l (gmg.cu's chebyshev, per-cell interval)
+int bg_chebyshev(const BGmg& M, int l, int deg, bool from_zero, bool need_res, const char* bsum_red,
+                 cudaStream_t s) {
+  const BLevel& L = M.L[l];
+  const BVec V = level_mech_vec(L.P);
+  int st;
+  const double a = 1.0 / 30.0, bm = M.safety;  // interval [lmax/30, safety lmax] relative to lmax
+  const double sigma = (bm + a) / (bm - a);
+  if (from_zero) {
+    { note_launch(); bg_first_b_kernel<<<V.n_chunks, kThreads, 0, s>>>(V, L.P->d_cells, L.b, L.invd, L.inv_theta, L.res, L.dvec, L.x, bsum_red, M.guard, M.gstride); }
+  } else {
+    if ((st = bg_level_apply(M, l, L.x, L.Ad, s))) return st;
+    { note_launch(); bg_first_res_kernel<<<V.n_chunks, kThreads, 0, s>>>(V, L.P->d_cells, L.b, L.Ad, L.invd, L.inv_theta, L.res, L.dvec, L.x, l == 0, L.diag, M.fixed, M.guard, M.gstride); }
+  }
+  float* cur = L.dvec;
+  float* oth = L.Ad;
+  double rho_old = 1.0 / sigma;
+  for (int k = 1; k < deg; ++k) {
+    const double rho = 1.0 / (2.0 * sigma - rho_old);
+    if ((st = bg_level_cheb(M, l, cur, oth, rho * rho_old, 2.0 * rho, true, s))) return st;
+    std::swap(cur, oth);
+    rho_old = rho;
+  }
+  if (need_res && (st = bg_level_cheb(M, l, cur, oth, 0.0, 0.0, false, s))) return st;
+  return last_launch_status();
+}
+
+// V-cycle from level l; bsum_red: the pending mean of L.b summed by the parent's restriction;
+// on coarse levels the mean of the result is left pending in L.red for the parent's prolongation
+int bg_vcycle(const BGmg& M, int l, const char* bsum_red, const char** xsum_red, cudaStream_t s) {
+  const BLevel& L = M.L[l];
+  int st;
+  *xsum_red = nullptr;
+  if (l == M.nlev - 1) {
+    if ((st = bg_chebyshev(M, l, M.deg_coarse, true, false, bsum_red, s))) return st;
+    const BVec Vn = level_node_vec(L.P);
+    { note_launch(); bg_mean3_kernel<<<Vn.n_chunks, kThreads, 0, s>>>(Vn, L.P->d_cells, L.x, L.red, M.guard, M.gstride); }
+    *xsum_red = L.red;
+    return last_launch_status();
+  }
+  if ((st = bg_chebyshev(M, l, M.deg, true, true, bsum_red, s))) return st;
+  const BLevel& C = M.L[l + 1];
+  const BVec Vcn = level_node_vec(C.P);
+  { note_launch(); bg_restrict_kernel<<<Vcn.n_chunks, kThreads, 0, s>>>(Vcn, L.P->d_cells, C.P->d_cells, L.res, l == 0 ? M.mask : nullptr, C.b, C.red, M.guard, M.gstride); }
+  const char* csum = nullptr;
+  if ((st = bg_vcycle(M, l + 1, C.red, &csum, s))) return st;
+  const BVec Vfn = level_node_vec(L.P);
+  { note_launch(); bg_prolong_kernel<<<Vfn.n_chunks, kThreads, 0, s>>>(Vfn, L.P->d_cells, C.P->d_cells, C.x, l == 0 ? M.mask : nullptr, L.x, csum, M.guard, M.gstride); }
+  if ((st = bg_chebyshev(M, l, M.deg, false, false, nullptr, s))) return st;
+  if (l > 0) {
+    const BVec Vn = level_node_vec(L.P);
+    { note_launch(); bg_mean3_kernel<<<Vn.n_chunks, kThreads, 0, s>>>(Vn, L.P->d_cells, L.x, L.red, M.guard, M.gstride); }
+    *xsum_red = L.red;
+  }
+  return last_launch_status();
+}
+
+// z = M^-1 r for every live cell: the fine level reads r and builds z in place
+int bg_precond(const BGmg& M0, const float* r, float* z, cudaStream_t s) {
+  BGmg M = M0;
+  M.L[0].b = const_cast<float*>(r);
+  M.L[0].x = z;
+  const char* xs = nullptr;
+  return bg_vcycle(M, 0, nullptr, &xs, s);
+}
+
+// Hierarchy for the current damage field: fine mask and diagonal, coarse moduli and diagonals
+// (per-cell setup launches), and, unless reused, lambda_max of every level and cell by power
+// iteration.  Chebyshev factors per cell from lambda_max.
+int bg_setup(BGmg& M, const phastb_batch* B, char* scratch, int power_iters, bool reuse_lmax, cudaStream_t s) {
+  int st;
+  M.guard = nullptr;
+  M.gstride = 0;
+  for (int l = 0; l < M.nlev; ++l) {
+    const BLevel& L = M.L[l];
+    float* v[7] = {L.diag, L.invd, L.x, L.b, L.res, L.dvec, L.Ad};
+    for (float* q : v)
+      if ((st = cuda_status(cudaMemsetAsync(q, 0, sizeof(float) * (size_t)L.P->n_mech, s)))) return st;
+    for (char* r : {L.red, L.ared})
+      { note_launch(); b_reset_tickets_kernel<<<(L.P->n_cells + 255) / 256, 256, 0, s>>>(L.P->n_cells, r); }
+  }
+  const BVec V0 = mech_vec(B);
+  { note_launch(); bg_fine_mask_kernel<<<V0.n_chunks, kThreads, 0, s>>>(V0, B->d_cells, M.fixed, M.mask); }
+  for (int c = 0; c < B->n_cells; ++c) {
+    const BatchCell& cl = B->cells[c];
+    if ((st = h8_mech_diag_t<float>(cl.g, M.m, M.slot + cl.elem_off, nullptr, M.d32 + cl.node_off,
+                                    M.L[0].diag + cl.mech_off, scratch, s)))
+      return st;
+  }
+  { note_launch(); bg_invert_kernel<<<V0.n_chunks, kThreads, 0, s>>>(V0, B->d_cells, M.L[0].diag, M.mask, M.L[0].invd); }
+  for (int l = 1; l < M.nlev; ++l) {
+    const BLevel& F = M.L[l - 1];
+    const BLevel& Cl = M.L[l];
+    for (int c = 0; c < B->n_cells; ++c) {
+      const BatchCell& fc = F.P->cells[c];
+      const BatchCell& cc = Cl.P->cells[c];
+      if (l == 1) {
+        if ((st = gmg_level_coefs_f32(fc.g, cc.g, M.m, M.slot + fc.elem_off, M.d32 + fc.node_off, nullptr, nullptr,
+                                      Cl.lam + 8 * cc.elem_off, Cl.mu + 8 * cc.elem_off, s)))
+          return st;
+      } else if ((st = gmg_level_coefs_f32(fc.g, cc.g, M.m, nullptr, nullptr, F.lam + 8 * fc.elem_off,
+                                           F.mu + 8 * fc.elem_off, Cl.lam + 8 * cc.elem_off,
+                                           Cl.mu + 8 * cc.elem_off, s))) {
+        return st;
+      }
+      if ((st = gmg_coarse_diag_f32(cc.g, Cl.lam + 8 * cc.elem_off, Cl.mu + 8 * cc.elem_off,
+                                    reinterpret_cast<float*>(scratch), Cl.diag + cc.mech_off, s)))
+        return st;
+    }
+    const BVec Vl = mech_vec(Cl.P);
+    { note_launch(); bg_invert_kernel<<<Vl.n_chunks, kThreads, 0, s>>>(Vl, Cl.P->d_cells, Cl.diag, nullptr, Cl.invd); }
+  }
+  for (int l = 0; l < M.nlev; ++l) {
+    const BLevel& L = M.L[l];
+    const BVec V = mech_vec(L.P);
+    const int C = L.P->n_cells;
+    if (!reuse_lmax) {
+      const uint8_t* mk = l == 0 ? M.mask : nullptr;
+      { note_launch(); bg_power_init_kernel<<<V.n_chunks, kThreads, 0, s>>>(V, L.P->d_cells, mk, L.dvec); }
+      for (int k = 0; k < power_iters; ++k) {
+        if ((st = bg_level_apply(M, l, L.dvec, L.Ad, s))) return st;
+        if (k == power_iters - 1) {
+          { note_launch(); bg_power_dots_kernel<<<V.n_chunks, kThreads, 0, s>>>(V, L.dvec, L.Ad, L.diag, mk, L.red); }
+        } else {
+          { note_launch(); bg_power_next_kernel<<<V.n_chunks, kThreads, 0, s>>>(V, L.Ad, L.invd, L.diag, L.dvec, L.red); }
+          { note_launch(); bg_power_scale_kernel<<<V.n_chunks, kThreads, 0, s>>>(V, L.red, L.dvec); }
+        }
+      }
+    }
+    { note_launch(); bg_cheb_factors_kernel<<<(C + 255) / 256, 256, 0, s>>>(C, L.red, reuse_lmax ? 0 : 1, L.lmax, M.safety, L.inv_theta, L.inv_delta); }
+    if ((st = last_launch_status())) return st;
+  }
+  return PHASTB_OK;
+}
+
+// The batched PCG of bpcg_run with the multigrid V-cycle as preconditioner (pcg_run with M):
+// start r = b - A x, z = M r, rz, p = z; per iteration A p (with p.Ap), x and r, z = M r, beta,
+// p = z + beta p.  Chunks of check_every iterations are captured as one graph.
+int bpcg_run_pre(const phastb_batch* B, const BatchOp<float>& A, const GraphKey& op_key, const BVec& V,
+                 const BPcg<float>& w, const float* b, float* x, const BpcgThr& thr, const BGmg& M0, int maxiter,
+                 int check_every, const char* dot_red, int* d_count, int* h_count, cudaStream_t s) {
+  int st;
+  if ((st = A(x, w.Ap, thr.live, 1, false, s))) return st;
+  { note_launch(); bpcg_start_pre_kernel<float><<<V.n_chunks, kThreads, 0, s>>>(V, w, b, thr.abs_sq, thr.rel, thr.outer_red, thr.outer_thr_sq, thr.live); }
+  if ((st = last_launch_status())) return st;
+  BGmg M = M0;
+  M.guard = &w.st[0].active;
+  M.gstride = kStateInts;
+  if ((st = bg_precond(M, w.r, w.z, s))) return st;
+  { note_launch(); bpcg_rz_kernel<float><<<V.n_chunks, kThreads, 0, s>>>(V, w, 1); }
+  if ((st = last_launch_status())) return st;
+  const int* guard = &w.st[0].active;
+  auto iterate = [&](int k_iters) -> int {
+    int e;
+    for (int k = 0; k < k_iters; ++k) {
+      if ((e = A(w.p, w.Ap, guard, kStateInts, true, s))) return e;
+      { note_launch(); bpcg_update_pre_kernel<float><<<V.n_chunks, kThreads, 0, s>>>(V, w, x, dot_red); }
+      if ((e = bg_precond(M, w.r, w.z, s))) return e;
+      { note_launch(); bpcg_rz_kernel<float><<<V.n_chunks, kThreads, 0, s>>>(V, w, 0); }
+      { note_launch(); bpcg_dir_kernel<float><<<V.n_chunks, kThreads, 0, s>>>(V, w); }
+    }
+    { note_launch(); bpcg_count_kernel<<<1, 256, 0, s>>>(B->n_cells, w.st, d_count); }
+    return last_launch_status();
+  };
+  GraphKey key = op_key;
+  key_val(key, w);
+  key_val(key, x);
+  key_val(key, V);
+  key_val(key, check_every);
+  key_val(key, dot_red);
+  key_val(key, d_count);
+  // the hierarchy lives in the workspace: its first array, the options and the fine inputs identify it
+  key_val(key, M.nlev);
+  key_val(key, M.L[0].diag);
+  key_val(key, M.mask);
+  key_val(key, M.d32);
+  key_val(key, M.slot);
+  key_val(key, M.deg);
+  key_val(key, M.deg_coarse);
+  key_val(key, M.safety);
+  long long glaunch = 0;
+  cudaGraphExec_t gexec =
+      maxiter >= check_every ? graph_for(key, s, [&] { return iterate(check_every); }, &glaunch) : nullptr;
+  int it = 0;
+  while (it < maxiter) {
+    const int chunk = std::min(check_every, maxiter - it);
+    if (gexec && chunk == check_every) {
+      note_launch(glaunch);
+      if ((st = cuda_status(cudaGraphLaunch(gexec, s)))) return st;
+    } else if ((st = iterate(chunk))) {
+      return st;
+    }
+    it += chunk;
+    if ((st = cuda_status(cudaMemcpyAsync(h_count, d_count, sizeof(int), cudaMemcpyDeviceToHost, s)))) return st;
+    if ((st = cuda_status(cudaStreamSynchronize(s)))) return st;
+    if (*h_count == 0) break;
+  }
+  return PHASTB_OK;
+}
+
+}  // namespace
+
 }  // namespace phastb
 
 using namespace phastb;
@@ -825,10 +1541,11 @@ struct MechLayout {
   double* invd64;
   char *ared, *rred, *scratch;
   int *count, *live, *live0;
+  char* gmg;  // multigrid hierarchy (bgmg_bytes), when the inner solves use the V-cycle
   size_t bytes;
 };
 
-MechLayout mech_layout(const phastb_batch* B, int mixed, char* base) {
+MechLayout mech_layout(const phastb_batch* B, int mixed, char* base, bool gmg = false) {
   Carve cv{base};
   MechLayout L{};
   const size_t n = (size_t)B->n_mech, C = (size_t)B->n_cells;
@@ -868,6 +1585,7 @@ MechLayout mech_layout(const phastb_batch* B, int mixed, char* base) {
     L.w32.st = cv.take<PcgState>(C);
     L.w32.red = cv.take<char>(n_red_ws(B));
   }
+  L.gmg = gmg ? cv.take<char>(bgmg_bytes(B)) : nullptr;
   L.bytes = cv.used;
   return L;
 }
@@ -1012,6 +1730,42 @@ phastb_batch* phastb_batch_create(int n_cells, const phastb_voxel_grid* grids, c
   t += align_up(sizeof(BChunk) * B->mech_chunks.size());
   t += align_up(sizeof(int) * n_cells) * 2;
   B->table_bytes = t;
+  // the multigrid hierarchy of the batch: rediscretised cells of twice and four times the voxel size
+  bool gmg = true;
+  for (int c = 0; c < n_cells && gmg; ++c) {
+    const phastb_voxel_grid& g = grids[c];
+    gmg = g.px && g.py && g.pz && g.nx % 4 == 0 && g.ny % 4 == 0 && g.nz % 4 == 0 && g.nx >= 32 && g.ny >= 32 &&
+          g.nz >= 32;
+  }
+  if (gmg && ox == B->ox) {
+    std::vector<phastb_voxel_grid> cg(grids, grids + n_cells);
+    for (int l = 0; l < 2 && gmg; ++l) {
+      for (auto& g : cg) {
+        g.nx /= 2;
+        g.ny /= 2;
+        g.nz /= 2;
+        g.hx *= 2;
+        g.hy *= 2;
+        g.hz *= 2;
+      }
+      B->lev[l] = phastb_batch_create(n_cells, cg.data(), ell, dscale, 8, 8, 4);
+      gmg = B->lev[l] != nullptr;
+    }
+    if (gmg) {
+      // a coarse plan has no levels of its own
+      for (int l = 0; l < 2; ++l) {
+        B->lev[l]->nlev = 1;
+        delete B->lev[l]->lev[0];
+        delete B->lev[l]->lev[1];
+        B->lev[l]->lev[0] = B->lev[l]->lev[1] = nullptr;
+      }
+      B->nlev = 3;
+    } else {
+      delete B->lev[0];
+      delete B->lev[1];
+      B->lev[0] = B->lev[1] = nullptr;
+    }
+  }
   return B;
 }
 
@@ -1023,7 +1777,7 @@ int phastb_batch_sizes(const phastb_batch* B, long long* out) {
   out[1] = B->n_mech;
   out[2] = B->n_elem;
   out[3] = (long long)B->work.size();
-  out[4] = (long long)B->table_bytes;
+  out[4] = (long long)B->all_table_bytes();
   out[5] = (long long)B->mech_chunks.size();
   out[6] = (long long)B->node_chunks.size();
   for (int c = 0; c < B->n_cells; ++c) {
@@ -1036,10 +1790,8 @@ int phastb_batch_sizes(const phastb_batch* B, long long* out) {
   return PHASTB_OK;
 }
 
-int phastb_batch_bind(phastb_batch* B, void* tables, size_t bytes, void* stream) {
-  if (!B || !tables || bytes < B->table_bytes) return PHASTB_ERR_ARG;
-  cudaStream_t s = (cudaStream_t)stream;
-  Carve cv{static_cast<char*>(tables)};
+static int bind_level(phastb_batch* B, char* tables, cudaStream_t s) {
+  Carve cv{tables};
   B->d_cells = cv.take<BatchCell>(B->cells.size());
   B->d_work = cv.take<int2>(B->work.size());
   B->d_node_chunks = cv.take<BChunk>(B->node_chunks.size());
@@ -1056,9 +1808,22 @@ int phastb_batch_bind(phastb_batch* B, void* tables, size_t bytes, void* stream)
   if ((st = put(B->d_mech_chunks, B->mech_chunks.data(), sizeof(BChunk) * B->mech_chunks.size()))) return st;
   if ((st = put(B->d_node_nchunk, B->node_nchunk.data(), sizeof(int) * B->n_cells))) return st;
   if ((st = put(B->d_mech_nchunk, B->mech_nchunk.data(), sizeof(int) * B->n_cells))) return st;
-  if ((st = cuda_status(cudaStreamSynchronize(s)))) return st;
   B->bound = true;
   return PHASTB_OK;
+}
+
+int phastb_batch_bind(phastb_batch* B, void* tables, size_t bytes, void* stream) {
+  if (!B || !tables || bytes < B->all_table_bytes()) return PHASTB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  char* p = static_cast<char*>(tables);
+  int st = bind_level(B, p, s);
+  p += B->table_bytes;
+  for (int l = 0; l < B->nlev - 1 && !st; ++l) {
+    st = bind_level(B->lev[l], p, s);
+    p += B->lev[l]->table_bytes;
+  }
+  if (st) return st;
+  return cuda_status(cudaStreamSynchronize(s));
 }
 
 size_t phastb_batch_apply_workspace_bytes(const phastb_batch* B) { return B ? n_red_ws(B) : 0; }
@@ -1107,17 +1872,28 @@ size_t phastb_batch_mech_solve_workspace_bytes(const phastb_batch* B, int mixed)
   return mech_layout(B, mixed, nullptr).bytes;
 }
 
-int phastb_batch_mech_solve(const phastb_batch* B, const phastb_voxel_material* m, const uint8_t* slot,
-                            const double* d, const uint8_t* fixed, const double* fixed_values, const double* x0,
-                            double rtol, double atol, int maxiter, int check_every, int mixed, double inner_rtol,
-                            int max_refine, const int* live_host, double* x_out, int* info, double* rinfo,
-                            void* workspace, size_t workspace_bytes, void* stream) {
+}  // extern "C"
+
+namespace {
+
+// Multigrid options of the batched inner solves (null: Jacobi).
+struct BGmgOpts {
+  int smooth_degree, coarse_degree, power_iters, reuse_lmax;
+  double lmax_safety;
+};
+
+int batch_mech_solve_impl(const phastb_batch* B, const phastb_voxel_material* m, const uint8_t* slot,
+                          const double* d, const uint8_t* fixed, const double* fixed_values, const double* x0,
+                          double rtol, double atol, int maxiter, int check_every, int mixed, double inner_rtol,
+                          int max_refine, const int* live_host, double* x_out, int* info, double* rinfo,
+                          void* workspace, size_t workspace_bytes, void* stream, const BGmgOpts* go) {
   if (!batch_ready(B) || !valid_mat(m) || !slot || !d || !fixed || !fixed_values || !x_out || !info || !rinfo ||
       maxiter < 1 || check_every < 1 || !(rtol >= 0) || !(atol >= 0) || (rtol == 0 && atol == 0) ||
       (mixed != 0 && mixed != 1) || (mixed && (!(inner_rtol > 0) || max_refine < 1)))
     return PHASTB_ERR_ARG;
   if (!m->isotropic) return PHASTB_UNSUPPORTED;
-  MechLayout L = mech_layout(B, mixed, static_cast<char*>(workspace));
+  if (go && (!mixed || B->nlev < 3)) return PHASTB_UNSUPPORTED;
+  MechLayout L = mech_layout(B, mixed, static_cast<char*>(workspace), go != nullptr);
   if (!workspace || workspace_bytes < L.bytes) return PHASTB_ERR_WORKSPACE;
   ScopedStream scope((cudaStream_t)stream);
   if (scope.status()) return scope.status();
@@ -1211,6 +1987,19 @@ int phastb_batch_mech_solve(const phastb_batch* B, const phastb_voxel_material* 
   BatchOp<float> A32 = [&](const float* x, float* y, const int* guard, int gs, bool dot, cudaStream_t ss) {
     return batch_mech_op<float>(B, m32, slot, L.d32, fixed, x, y, L.ared, guard, gs, dot, ss);
   };
+  // the V-cycle hierarchy for this damage field (the FP32 moduli of every level)
+  BGmg G{};
+  if (go) {
+    bgmg_carve(G, B, L.gmg);
+    G.m = m32;
+    G.slot = slot;
+    G.d32 = L.d32;
+    G.fixed = fixed;
+    G.safety = go->lmax_safety;
+    G.deg = go->smooth_degree;
+    G.deg_coarse = go->coarse_degree;
+    if ((st = bg_setup(G, B, L.scratch, go->power_iters, go->reuse_lmax != 0, s))) return st;
+  }
   std::vector<int> iters(C, 0), done(C, 0), bad(C, 0), live(live0);
   std::vector<double> rn(C, 0.0);
   for (int k = 0; k < max_refine; ++k) {
@@ -1230,9 +2019,13 @@ int phastb_batch_mech_solve(const phastb_batch* B, const phastb_voxel_material* 
     thr.outer_red = L.rred;
     thr.outer_thr_sq = L.outer_thr_sq;
     thr.live = L.live;
-    if ((st = bpcg_run<float>(B, A32, key, V, L.w32, L.r32, L.inv32, L.dx32, thr, budget, check_every, PCG_FREEZE,
-                              L.ared, L.count, &h_count, s)))
+    if (G.nlev > 0) {
+      if ((st = bpcg_run_pre(B, A32, key, V, L.w32, L.r32, L.dx32, thr, G, budget, 2, L.ared, L.count, &h_count, s)))
+        return st;
+    } else if ((st = bpcg_run<float>(B, A32, key, V, L.w32, L.r32, L.inv32, L.dx32, thr, budget, check_every,
+                                     PCG_FREEZE, L.ared, L.count, &h_count, s))) {
       return st;
+    }
     if ((st = fetch_states(B, L.w32.st, &hs, s))) return st;
     int n_live = 0;
     for (int c = 0; c < C; ++c) {
@@ -1289,6 +2082,40 @@ int phastb_batch_mech_solve(const phastb_batch* B, const phastb_voxel_material* 
     if (cs != PHASTB_OK && worst == PHASTB_OK) worst = cs;
   }
   return worst;
+}
+
+}  // namespace
+
+extern "C" {
+
+int phastb_batch_mech_solve(const phastb_batch* B, const phastb_voxel_material* m, const uint8_t* slot,
+                            const double* d, const uint8_t* fixed, const double* fixed_values, const double* x0,
+                            double rtol, double atol, int maxiter, int check_every, int mixed, double inner_rtol,
+                            int max_refine, const int* live_host, double* x_out, int* info, double* rinfo,
+                            void* workspace, size_t workspace_bytes, void* stream) {
+  return batch_mech_solve_impl(B, m, slot, d, fixed, fixed_values, x0, rtol, atol, maxiter, check_every, mixed,
+                               inner_rtol, max_refine, live_host, x_out, info, rinfo, workspace, workspace_bytes,
+                               stream, nullptr);
+}
+
+size_t phastb_batch_mech_solve_ex_workspace_bytes(const phastb_batch* B, const phastb_mech_opts* o) {
+  if (!B || !o || (o->mixed != 0 && o->mixed != 1)) return 0;
+  if (o->precond && (!o->mixed || B->nlev < 3 || o->levels != 3)) return 0;
+  return mech_layout(B, o->mixed, nullptr, o->precond != 0).bytes;
+}
+
+int phastb_batch_mech_solve_ex(const phastb_batch* B, const phastb_voxel_material* m, const uint8_t* slot,
+                               const double* d, const uint8_t* fixed, const double* fixed_values, const double* x0,
+                               double rtol, double atol, int maxiter, int check_every, const phastb_mech_opts* o,
+                               int reuse_lmax, const int* live_host, double* x_out, int* info, double* rinfo,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+  if (!o || (o->precond && (o->levels != 3 || o->smooth_degree < 1 || o->coarse_degree < 1 || o->power_iters < 1 ||
+                            !(o->lmax_safety > 1.0 / 30.0))))
+    return PHASTB_ERR_ARG;
+  BGmgOpts go{o->smooth_degree, o->coarse_degree, o->power_iters, reuse_lmax, o->lmax_safety};
+  return batch_mech_solve_impl(B, m, slot, d, fixed, fixed_values, x0, rtol, atol, maxiter, check_every, o->mixed,
+                               o->inner_rtol, o->max_refine, live_host, x_out, info, rinfo, workspace,
+                               workspace_bytes, stream, o->precond ? &go : nullptr);
 }
 
 size_t phastb_batch_box_kkt_workspace_bytes(const phastb_batch* B) { return B ? kkt_layout(B, nullptr).bytes : 0; }

@@ -800,6 +800,26 @@ static int gmg_precond_apply(const void* ctx, const T* r, T* z, const int* guard
 template size_t gmg_hier_bytes<double>(const VoxGeom&, int);
 template size_t gmg_hier_bytes<float>(const VoxGeom&, int);
 
+// Per-cell setup pieces of the packed batch's multigrid (FP32): the Gauss-point moduli of a
+// coarse level from the fine level's slots and damage (lam_f == nullptr) or from the next
+// finer coarse level, and a coarse level's Jacobi diagonal (24-word element scratch).
+int gmg_level_coefs_f32(const VoxGeom& f, const VoxGeom& c, const VoxMat<float>& m, const uint8_t* slot,
+                        const float* d, const float* lam_f, const float* mu_f, float* lam_c, float* mu_c,
+                        cudaStream_t s) {
+  if (!lam_f)
+    { note_launch(); gmg_coef_from_fine<float><<<grid_for(f.n_elem), kThreads, 0, s>>>(f, c, m, slot, d, lam_c, mu_c); }
+  else
+    { note_launch(); gmg_coef_from_coarse<float><<<grid_for(f.n_elem), kThreads, 0, s>>>(f, c, lam_f, mu_f, lam_c, mu_c); }
+  return last_launch_status();
+}
+
+int gmg_coarse_diag_f32(const VoxGeom& c, const float* lam, const float* mu, float* scratch, float* diag,
+                        cudaStream_t s) {
+  { note_launch(); gmg_coarse_elem<float, 1><<<grid_for(c.n_elem), kThreads, 0, s>>>(c, lam, mu, nullptr, scratch, nullptr); }
+  { note_launch(); gmg_gather3<float><<<grid_for(c.n_red), kThreads, 0, s>>>(c, scratch, diag, nullptr); }
+  return last_launch_status();
+}
+
 }  // namespace phastb
 
 // ======================================================================= solve

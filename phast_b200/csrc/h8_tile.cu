@@ -1870,7 +1870,7 @@ __device__ __forceinline__ TileK<T> batch_k(const BatchCell& c) {
 
 // One brick of one cell per block: the block builds its cell's arguments in shared
 // memory and runs the single-grid tile body with its brick index inside the cell.
-template <typename T, int MODE, int OX, int OY>
+template <typename T, int MODE, int OX, int OY, int COEF = kCoefIso>
 __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
     h8_tile_batch_kernel(TileBatchArgs<T> b, VoxMat<T> m) {
   __shared__ TileArgs<T> sa;
@@ -1881,27 +1881,27 @@ __global__ void __launch_bounds__(kTileMaxThreads, sizeof(T) == 4 ? 2 : 1)
     a.g = c.g;
     a.ts = c.ts;
     a.pad_ = 0;
-    a.slot = b.slot + c.elem_off;
+    a.slot = b.slot ? b.slot + c.elem_off : nullptr;
     a.gq = nullptr;
     a.d = b.d ? b.d + c.node_off : nullptr;
-    a.lam_q = nullptr;
-    a.mu_q = nullptr;
+    a.lam_q = b.lam_q ? b.lam_q + 8 * c.elem_off : nullptr;
+    a.mu_q = b.mu_q ? b.mu_q + 8 * c.elem_off : nullptr;
     a.x = b.x + c.mech_off;
     a.y = b.y ? b.y + c.mech_off : nullptr;
     a.mask = b.mask ? b.mask + c.mech_off : nullptr;
-    a.res = nullptr;
-    a.invd = nullptr;
-    a.xs = nullptr;
-    a.d_out = nullptr;
-    a.c1 = 0.0;
-    a.c2 = 0.0;
+    a.res = b.res ? b.res + c.mech_off : nullptr;
+    a.invd = b.invd ? b.invd + c.mech_off : nullptr;
+    a.xs = b.xs ? b.xs + c.mech_off : nullptr;
+    a.d_out = b.d_out ? b.d_out + c.mech_off : nullptr;
+    a.c1 = b.c1;
+    a.c2 = b.c2 * (b.c2_scale ? b.c2_scale[wk.x] : 1.0);
     a.ws = red_ws(b.ws + (size_t)wk.x * red_ws_bytes());
     a.guard = b.guard ? b.guard + (size_t)wk.x * b.guard_stride : nullptr;
     a.k = batch_k<T>(c);
     sa = a;
   }
   __syncthreads();
-  tile_body<T, kCoefIso, MODE, OX, OY, false>(sa, m, nullptr, nullptr, wk.y, c.nvb);
+  tile_body<T, COEF, MODE, OX, OY, false>(sa, m, nullptr, nullptr, wk.y, c.nvb);
 }
 
 template <typename T, int MODE, int OX, int OY>
@@ -1967,6 +1967,18 @@ int tile_batch_variant(const TileBatchArgs<T>& b, const VoxMat<T>& m, cudaStream
   return last_launch_status();
 }
 
+template <int COEF, int MODE, int OX, int OY>
+int tile_batch_level_variant(const TileBatchArgs<float>& b, const VoxMat<float>& m, cudaStream_t s) {
+  auto kern = h8_tile_batch_kernel<float, MODE, OX, OY, COEF>;
+  size_t oq = 0, oc = 0;
+  const size_t smem = tile_layout<float>(OX, OY, COEF == kCoefQP, MODE == kModeCheb, &oq, &oc);
+  int st = batch_smem_attr(kern, smem);
+  if (st) return st;
+  const int threads = ((OX + 1) * (OY + 1) + 31) / 32 * 32;
+  { note_launch(); kern<<<b.n_blocks, threads, smem, s>>>(b, m); }
+  return last_launch_status();
+}
+
 template <typename T, int MODE, int OX, int OY>
 int dtile_batch_variant(const TileBatchArgs<T>& b, const VoxMat<T>& m, cudaStream_t s) {
   auto kern = h8_dtile_batch_kernel<T, MODE, OX, OY>;
@@ -1991,6 +2003,25 @@ int h8_tile_batch_launch(const TileBatchArgs<T>& b, const VoxMat<T>& m, int mode
     return dot ? tile_batch_variant<T, kModeDot, 16, 8>(b, m, s) : tile_batch_variant<T, kModeApply, 16, 8>(b, m, s);
   if (ox == 8 && oy == 8)
     return dot ? tile_batch_variant<T, kModeDot, 8, 8>(b, m, s) : tile_batch_variant<T, kModeApply, 8, 8>(b, m, s);
+  return PHASTB_ERR_ARG;
+}
+
+int h8_tile_batch_level_launch(const TileBatchArgs<float>& b, const VoxMat<float>& m, int coef, int mode, int ox,
+                               int oy, cudaStream_t s) {
+  if (b.n_blocks < 1) return PHASTB_OK;
+  if (coef == kCoefIso && !m.iso) return PHASTB_UNSUPPORTED;
+  if (coef == kCoefIso && ox == 16 && oy == 8) {
+    if (mode == kModeCheb) return tile_batch_level_variant<kCoefIso, kModeCheb, 16, 8>(b, m, s);
+    if (mode == kModeNodal) return tile_batch_level_variant<kCoefIso, kModeNodal, 16, 8>(b, m, s);
+  }
+  if (coef == kCoefIso && ox == 8 && oy == 8) {
+    if (mode == kModeCheb) return tile_batch_level_variant<kCoefIso, kModeCheb, 8, 8>(b, m, s);
+    if (mode == kModeNodal) return tile_batch_level_variant<kCoefIso, kModeNodal, 8, 8>(b, m, s);
+  }
+  if (coef == kCoefQP && ox == 8 && oy == 8) {
+    if (mode == kModeCheb) return tile_batch_level_variant<kCoefQP, kModeCheb, 8, 8>(b, m, s);
+    if (mode == kModeApply) return tile_batch_level_variant<kCoefQP, kModeApply, 8, 8>(b, m, s);
+  }
   return PHASTB_ERR_ARG;
 }
 

@@ -253,7 +253,23 @@ struct TileBatchArgs {
   double kappa;         // damage action
   int dscale;           // damage action: 1 scales it by each cell's damage-system scale
   int pad_;
+  // multigrid levels (kCoefQP: per-Gauss-point moduli, 8 per element, at 8 * elem_off) and the
+  // Chebyshev step (kModeCheb: res -= A x; d_out = c1 x + c2 s_c invd res; xs += d_out, with the
+  // per-cell factor s_c = c2_scale[c] or 1), vectors laid out like x
+  const T* lam_q;
+  const T* mu_q;
+  T* res;
+  const T* invd;
+  T* xs;
+  T* d_out;
+  double c1, c2;
+  const double* c2_scale;
 };
+
+// One multigrid-level launch of the batch: kCoefIso (the fine level: slots and g(d)) or kCoefQP
+// (coarse levels) in mode kModeApply, kModeNodal or kModeCheb.  FP32, bricks 16 x 8 or 8 x 8.
+int h8_tile_batch_level_launch(const TileBatchArgs<float>& b, const VoxMat<float>& m, int coef, int mode, int ox,
+                               int oy, cudaStream_t s);
 
 // y = A(d) x on every cell of the batch (MODE kModeApply or kModeDot: also
 // x . y per cell at ws_c.out[kOutDot]; the E-row sums at ws_c.out[0..5]).

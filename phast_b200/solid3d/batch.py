@@ -360,11 +360,17 @@ class PackedCellBatch:
         return y
 
     def mech_solve(self, d, fixed_values, *, x0=None, rtol=1e-8, atol=0.0, maxiter=20000, check_every=10,
-                   mixed=False, inner_rtol=1e-4, max_refine=30, live=None):
+                   mixed=False, inner_rtol=1e-4, max_refine=30, live=None, form=None, reuse_lmax=False):
         """Constrained mechanics solve of every cell (``live``: the cells to solve, others keep ``x0``).
 
+        ``form``: a ``MechForm``; with ``precond='gmg'`` (and ``mixed=True``) every cell's FP32 inner
+        PCG is preconditioned by the voxel multigrid V-cycle, all cells in the same launches
+        (``reuse_lmax``: keep the per-cell lambda_max estimates of the previous multigrid solve).
         Returns ``(x, status, iterations (C,), converged (C,), rhs_norm (C,), residual_norm (C,))``.
         """
+        if form is not None and form.precond == "gmg":
+            return self._mech_solve_gmg(d, fixed_values, x0, rtol, atol, maxiter, check_every, form, live,
+                                        reuse_lmax)
         import ctypes as C
 
         import numpy as np
@@ -384,6 +390,36 @@ class PackedCellBatch:
                       _lib.ptr(x), info, rinfo, wp, wn, _lib.stream(self.device))
         if st not in (_lib.OK, _lib.NONCONVERGED, _lib.BREAKDOWN, _lib.NONFINITE):
             _lib.check(st, "phastb_batch_mech_solve")
+        inf = np.array(info[:]).reshape(n, 2)
+        rin = np.array(rinfo[:]).reshape(n, 2)
+        return x, st, inf[:, 0], inf[:, 1].astype(bool), rin[:, 0], rin[:, 1]
+
+    def _mech_solve_gmg(self, d, fixed_values, x0, rtol, atol, maxiter, check_every, form, live, reuse_lmax):
+        import ctypes as C
+
+        import numpy as np
+        import torch
+
+        from .. import _lib
+        if not form.mixed:
+            raise NotImplementedError("the batched multigrid runs in the mixed form (FP32 V-cycle, FP64 refinement)")
+        n = self.n_cells
+        opts = form.struct()
+        nbytes = self._lib.phastb_batch_mech_solve_ex_workspace_bytes(self._h, opts)
+        if nbytes == 0:
+            raise NotImplementedError("the batched multigrid needs periodic cells with edges divisible by 4 and at "
+                                      "least 32 (three levels)")
+        x = torch.empty(self.n_mech, dtype=torch.float64, device=self.device)
+        info = (C.c_int * (2 * n))()
+        rinfo = (C.c_double * (2 * n))()
+        lv = None if live is None else (C.c_int * n)(*[int(bool(v)) for v in live])
+        wp, wn = self.workspace("mech_gmg", nbytes)
+        st = _lib.raw("phastb_batch_mech_solve_ex", self._h, self.mat, _lib.ptr(self.slot), _lib.ptr(d),
+                      _lib.ptr(self.fixed), _lib.ptr(fixed_values), _lib.ptr(x0), float(rtol), float(atol),
+                      int(maxiter), int(check_every), opts, int(bool(reuse_lmax)), lv, _lib.ptr(x), info, rinfo,
+                      wp, wn, _lib.stream(self.device))
+        if st not in (_lib.OK, _lib.NONCONVERGED, _lib.BREAKDOWN, _lib.NONFINITE):
+            _lib.check(st, "phastb_batch_mech_solve_ex")
         inf = np.array(info[:]).reshape(n, 2)
         rin = np.array(rinfo[:]).reshape(n, 2)
         return x, st, inf[:, 0], inf[:, 1].astype(bool), rin[:, 0], rin[:, 1]
@@ -452,8 +488,10 @@ class BatchStaggeredSolver:
     same load path (``load``).
     """
 
-    def __init__(self, batch, load, cfg=None, *, mixed=True, inner_rtol=1e-4, max_refine=30):
-        import torch
+    def __init__(self, batch, load, cfg=None, *, mixed=True, inner_rtol=1e-4, max_refine=30, form=None):
+        self.form = form
+        self.lmax_every = 10
+        self._gmg_solves = 0
         self.batch = batch
         self.load = load
         self.cfg = cfg or SolverConfig(kappa=batch.ops[0].kappa)
@@ -465,6 +503,19 @@ class BatchStaggeredSolver:
         self._max_abs_target = max(abs(float(t)) for t in load.targets)
         self._u_floor = np.array([min(op.h) * math.sqrt(3 * op.n_red) for op in batch.ops])
         self.n_attempts = 0
+        self._increments = 0
+
+    def _mech(self, d, values, x0, live, first):
+        """One batched mechanics solve of the configured form.  The multigrid's per-cell lambda_max
+        estimates are refreshed at the first solve of every ``lmax_every``-th increment."""
+        cfg = self.cfg
+        reuse = False
+        if self.form is not None and self.form.precond == "gmg":
+            reuse = self._gmg_solves > 0 and not (first and self._increments % self.lmax_every == 0)
+            self._gmg_solves += 1
+        return self.batch.mech_solve(d, values, x0=x0, rtol=cfg.pcg_rtol_mech, maxiter=cfg.pcg_maxit_mech,
+                                     check_every=cfg.check_every, mixed=self.mixed, inner_rtol=self.inner_rtol,
+                                     max_refine=self.max_refine, live=live, form=self.form, reuse_lmax=reuse)
 
     def initial_state(self):
         import torch
@@ -536,10 +587,7 @@ class BatchStaggeredSolver:
                                           reason=reason)
 
         for k in range(1, cfg.max_stagger + 1):
-            x_new, st, its, conv, _, _ = b.mech_solve(d_old, values, x0=x_old, rtol=cfg.pcg_rtol_mech,
-                                                      maxiter=cfg.pcg_maxit_mech, check_every=cfg.check_every,
-                                                      mixed=self.mixed, inner_rtol=self.inner_rtol,
-                                                      max_refine=self.max_refine, live=live)
+            x_new, st, its, conv, _, _ = self._mech(d_old, values, x_old, live, first=(k == 1))
             pm += np.where(live, its, 0)
             bad = np.flatnonzero(live & ~conv)
             if bad.size:
@@ -578,10 +626,7 @@ class BatchStaggeredSolver:
         d = d_old
         rel = np.zeros(C_)
         if cfg.final_mechanics_resolve:
-            x, st, its, conv, bn, rn = b.mech_solve(d, values, x0=x_old, rtol=cfg.pcg_rtol_mech,
-                                                    maxiter=cfg.pcg_maxit_mech, check_every=cfg.check_every,
-                                                    mixed=self.mixed, inner_rtol=self.inner_rtol,
-                                                    max_refine=self.max_refine)
+            x, st, its, conv, bn, rn = self._mech(d, values, x_old, None, first=False)
             pm += its
             if not conv.all():
                 fail(f"mechanics PCG did not converge in cells {np.flatnonzero(~conv).tolist()}")
@@ -626,4 +671,5 @@ class BatchStaggeredSolver:
                 stagger_change=float(change_done[c]), mech_relative_residual=float(rel[c]),
                 hill_mandel_rel=float(hill_rel), wall_s=wall, mean_strain=tuple(float(v) for v in E)))
         new_state = BatchState(state.step + 1, x, d, H, E_all, S_all, W, increment)
+        self._increments += 1
         return new_state, records
