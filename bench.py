@@ -503,7 +503,7 @@ def run_cfg3_action(device, flush, n_cells=16, brick=(16, 8, 8)):
             "blocks": B.n_blocks}
 
 
-def _batch_increments(B, load, cfg, flush, increments, mixed, form):
+def _batch_increments(B, load, cfg, flush, increments, mixed, form, profile=False):
     """Timed load increments 1..K of every cell of a packed batch, after one warm-up increment from a
     separate initial state; returns (ms, records per increment)."""
     from phast_b200.solid3d import batch as bt
@@ -513,6 +513,8 @@ def _batch_increments(B, load, cfg, flush, increments, mixed, form):
     solver = bt.BatchStaggeredSolver(B, load, cfg, mixed=mixed, form=form)
     state = solver.initial_state()
     total_ms, recs = 0.0, []
+    if profile:  # brackets the timed increments for a profiler started with --profile-from-start off
+        torch.cuda.profiler.start()
     for k in range(increments):
         flush_l2(flush)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -522,6 +524,8 @@ def _batch_increments(B, load, cfg, flush, increments, mixed, form):
         torch.cuda.synchronize()
         total_ms += e0.elapsed_time(e1)
         recs.append(r)
+    if profile:
+        torch.cuda.profiler.stop()
     return total_ms, recs, state
 
 
@@ -563,7 +567,7 @@ def run_cfg3(device, flush, n_cells=128, increments=CFG3_INCREMENTS, per_cell=Tr
     B = bt.PackedCellBatch(ops, brick=(16, 8, 8))
     cfg = SolverConfig(kappa=ops[0].kappa)
     gmg = forms()["mixed-gmg"]
-    total_ms, recs, state = _batch_increments(B, load, cfg, flush, increments, True, gmg)
+    total_ms, recs, state = _batch_increments(B, load, cfg, flush, increments, True, gmg, profile=True)
     jac_ms, jac_recs, _ = _batch_increments(B, load, cfg, flush, increments, True, None)
     voxels = sum(op.n_elements for op in ops)
     mech_its = sum(r.pcg_iters_mech for rr in recs for r in rr)
