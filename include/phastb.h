@@ -485,6 +485,80 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
                              int max_lin, int max_active, double* d_out, int* info, void* workspace,
                              size_t workspace_bytes, void* stream);
 
+/* ---- PF-CZM damage law (SolverConfig.damage_law = 'pfczm') ----
+ * Wu's rational degradation g = (1 - kappa) A/(A + Q) + kappa, A = (1 - d)^p,
+ * Q = a1 d (1 + a2 d + a2 a3 d^2) (physics/pfczm.py:79-125) with a1 per material slot,
+ * a1 = 4 E_ref Gc / (pi ell f_t^2 (1 - kappa)) (pfczm.py:16-31, operator.py:326-392), and the
+ * softening constants of pfczm_softening_parameters (pfczm.py:57-65).  Gc, ell and kappa
+ * come from the phastb_voxel_material. */
+typedef struct {
+  double a1[PHASTB_MAX_SLOTS];
+  double a2, a3;  /* softening: linear (-1/2, 0), exponential (2^(5/3) - 3, 0) */
+  double p;       /* exponent of A, >= 2 */
+} phastb_pfczm_law;
+
+/* gq (E,8) = g(d_q), the degradation the elastic action and solve take as gq.
+ * degradation, operator.py:939-946 */
+int phastb_h8_pfczm_degradation(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                                const phastb_pfczm_law* law, const uint8_t* slot, const double* d,
+                                double* gq, void* stream);
+
+/* Workspace of the PF-CZM energy, gradient, tangent action and diagonal. */
+size_t phastb_h8_pfczm_workspace_bytes(const phastb_voxel_grid* g);
+
+/* out_host[0] = the damage energy sum_q w H_q g(d_q) + Gc/(pi ell) int (2d - d^2)
+ * + Gc ell/pi int |grad d|^2 (H NULL: no history term), [1] the history term, [2] the local
+ * surface part, [3] the gradient surface part, [4..4+PHASTB_MAX_SLOTS) the surface energy by
+ * slot.  pfczm_damage_energy operator.py:465-489, _pfczm_fracture_energy :608-631 */
+#define PHASTB_PFCZM_ENERGY_WORDS (4 + PHASTB_MAX_SLOTS)
+int phastb_h8_pfczm_energy(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                           const phastb_pfczm_law* law, const uint8_t* slot, const double* d, const double* H,
+                           double* out_host, void* workspace, size_t workspace_bytes, void* stream);
+
+/* grad = scale * d(energy)/dd.  pfczm_damage_gradient, operator.py:491-513 */
+int phastb_h8_pfczm_gradient(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                             const phastb_pfczm_law* law, const uint8_t* slot, const double* d, const double* H,
+                             double scale, double* grad, void* workspace, size_t workspace_bytes, void* stream);
+
+/* W (E,8) = max(H g''(d_q) - 2 Gc/(pi ell), 0.25 * 2 Gc/(pi ell)), the Gauss-point curvatures
+ * of the Newton tangent.  pfczm_tangent_weights, operator.py:515-539 */
+int phastb_h8_pfczm_tangent_weights(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                                    const phastb_pfczm_law* law, const uint8_t* slot, const double* d,
+                                    const double* H, double* W, void* stream);
+
+/* y = scale * [Gc (2 ell/pi) L f + sum_q w W_q N_q N_q^T f], and its Jacobi diagonal.
+ * pfczm_tangent_action / pfczm_tangent_diagonal, operator.py:541-566 */
+int phastb_h8_pfczm_tangent_apply(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                                  const uint8_t* slot, const double* W, const double* f, double scale, double* y,
+                                  void* workspace, size_t workspace_bytes, void* stream);
+int phastb_h8_pfczm_tangent_diagonal(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                                     const uint8_t* slot, const double* W, double scale, double* diag,
+                                     void* workspace, size_t workspace_bytes, void* stream);
+
+/* Projected Newton solve of the PF-CZM damage energy over lower <= d <= 1 from `initial`,
+ * each step a box-QP of the tangent (the box-KKT solve above, at kkt_tol / 10) with an
+ * Armijo line search and projected step doubling, stopped when the projected scaled gradient
+ * is at most kkt_tol in the max norm.  lin_tol is SolverConfig.damage_linear_tol.
+ * info[0] PCG iterations, info[1] active-set iterations, info[2] Newton iterations,
+ * info[3] failure reason (0 none, 1 non-finite energy, 2 non-finite gradient, 3 box-QP
+ * failed, 4 line search failed, 5 Newton limit); rinfo[0] final projected gradient,
+ * rinfo[1] final energy.  StaggeredSolver._damage_pfczm, solid3d/staggered.py:843-1096 */
+size_t phastb_h8_pfczm_solve_workspace_bytes(const phastb_voxel_grid* g);
+int phastb_h8_pfczm_damage_solve(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                                 const phastb_pfczm_law* law, const uint8_t* slot, const double* H, double scale,
+                                 const double* lower, const double* initial, double kkt_tol, double lin_tol,
+                                 int max_lin, int max_active, int max_newton, double* d_out, int* info,
+                                 double* rinfo, void* workspace, size_t workspace_bytes, void* stream);
+
+/* The increment record (phastb_h8_increment_record) with the elastic part at the given
+ * degradation gq (NULL: g(d) of AT2) and, with law non-NULL, the PF-CZM surface energy
+ * Gc/(pi ell) int (2d - d^2) + Gc ell/pi int |grad d|^2 in [13:23).  _pfczm_fracture_energy,
+ * operator.py:608-631 */
+int phastb_h8_increment_record_ex(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                                  const uint8_t* slot, const double* x, const double* gq, const double* d,
+                                  const double* H, double threshold, const phastb_pfczm_law* law,
+                                  double* out_host, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Staggered change parts out[0..4] = ||du~||, ||u~||, max|dE|, max|E|, max|dd| (FP64, host).
  * StaggeredSolver._change, solid3d/staggered.py:1097-1124 */
 int phastb_h8_stagger_change(int n_u, const double* x_new, const double* x_old, int n_d,

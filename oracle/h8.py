@@ -459,8 +459,26 @@ class Cfg3D:
     damage_max_active_set: int = 64
 
 
-def increment(op: VoxelOperator, cfg: Cfg3D, x, d, H_prev, previous, target):
-    """One _attempt: returns (x, d, H, stagger_iters, pcg_mech, pcg_pf, macro_stress)."""
+def _damage_at2(op, cfg, H, lower, initial):
+    """The box-KKT AT2 damage solve of one staggered iteration (staggered.py:753-800)."""
+    s = op.damage_scale
+    rhs = s * op.damage_rhs(H)
+    dg = s * op.damage_diagonal(H)
+    act = lambda v: s * op.damage_action(v, H)  # noqa: E731
+    r0 = float(np.linalg.norm(rhs - act(initial)))
+    tol = min(cfg.damage_linear_tol, 0.1 * cfg.damage_kkt_tol / max(r0, 1.0))
+    tol = max(tol, 4.0 * float(np.finfo(np.float64).eps))
+    d_new, its, _, _ = box_kkt(act, rhs, dg, lower, 1.0, initial, tol, cfg.damage_kkt_tol, cfg.damage_maxit,
+                               cfg.damage_max_active_set)
+    return d_new, its
+
+
+def increment(op: VoxelOperator, cfg: Cfg3D, x, d, H_prev, previous, target, degradation=None, damage=None):
+    """One _attempt: returns (x, d, H, stagger_iters, pcg_mech, pcg_pf, macro_stress).
+
+    ``degradation(d)`` and ``damage(H, lower, initial) -> (d, pcg iterations)`` replace the
+    AT2 law when given (the PF-CZM law of ``pfczm.py``)."""
+    degradation = op.degradation if degradation is None else degradation
     nu = 3 * op.n_red
     if previous != 0.0:
         x_old = x * (target / previous)
@@ -476,7 +494,7 @@ def increment(op: VoxelOperator, cfg: Cfg3D, x, d, H_prev, previous, target):
     pm = pp = 0
     H = H_prev
     for k in range(1, cfg.max_stagger + 1):
-        g = op.degradation(d_old)
+        g = degradation(d_old)
         x_new, its, conv, _, _ = solve_constrained(lambda v: op.mech_action(v, g), op.mech_diagonal(g), mask, values,
                                                    x0=x_old, rtol=cfg.pcg_rtol_mech, maxiter=cfg.pcg_maxit_mech,
                                                    check_every=cfg.check_every)
@@ -485,15 +503,10 @@ def increment(op: VoxelOperator, cfg: Cfg3D, x, d, H_prev, previous, target):
         pm += its
         Y = op.driving_force(x_new)
         H = np.maximum(H_prev, Y)
-        s = op.damage_scale
-        rhs = s * op.damage_rhs(H)
-        dg = s * op.damage_diagonal(H)
-        act = lambda v: s * op.damage_action(v, H)
-        r0 = float(np.linalg.norm(rhs - act(d_old)))
-        tol = min(cfg.damage_linear_tol, 0.1 * cfg.damage_kkt_tol / max(r0, 1.0))
-        tol = max(tol, 4.0 * float(np.finfo(np.float64).eps))
-        d_new, its, _, _ = box_kkt(act, rhs, dg, lower, 1.0, d_old, tol, cfg.damage_kkt_tol, cfg.damage_maxit,
-                                   cfg.damage_max_active_set)
+        if damage is None:
+            d_new, its = _damage_at2(op, cfg, H, lower, d_old)
+        else:
+            d_new, its = damage(H, lower, d_old)
         pp += its
         du = float(np.linalg.norm(x_new[:nu] - x_old[:nu]))
         un = float(np.linalg.norm(x_new[:nu]))
@@ -508,7 +521,7 @@ def increment(op: VoxelOperator, cfg: Cfg3D, x, d, H_prev, previous, target):
             break
     else:
         raise RuntimeError("stagger did not converge")
-    g = op.degradation(d_old)
+    g = degradation(d_old)
     x_fin, its, conv, _, _ = solve_constrained(lambda v: op.mech_action(v, g), op.mech_diagonal(g), mask, values,
                                                x0=x_old, rtol=cfg.pcg_rtol_mech, maxiter=cfg.pcg_maxit_mech,
                                                check_every=cfg.check_every)

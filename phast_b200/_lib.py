@@ -45,6 +45,10 @@ class VoxelMaterial(C.Structure):
                 ("driver", C.c_int * MAX_SLOTS), ("kappa", C.c_double), ("ell", C.c_double)]
 
 
+class PfczmLaw(C.Structure):
+    _fields_ = [("a1", C.c_double * MAX_SLOTS), ("a2", C.c_double), ("a3", C.c_double), ("p", C.c_double)]
+
+
 class MechOpts(C.Structure):
     _fields_ = [("precond", C.c_int), ("mixed", C.c_int), ("levels", C.c_int), ("smooth_degree", C.c_int),
                 ("coarse_degree", C.c_int), ("power_iters", C.c_int), ("lmax_safety", C.c_double),
@@ -68,6 +72,7 @@ Q4G, Q4M, VG, VM = C.POINTER(Q4Grid), C.POINTER(Q4Material), C.POINTER(VoxelGrid
 T3DM = C.POINTER(T3DamageModel)
 T3M = C.POINTER(T3Mesh)
 MO = C.POINTER(MechOpts)
+PL = C.POINTER(PfczmLaw)
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -140,6 +145,17 @@ SIGNATURES = {
     "phastb_h8_stagger_change": (C.c_int, [C.c_int, vp, vp, C.c_int, vp, vp, dp, vp, sz, vp]),
     "phastb_h8_record_workspace_bytes": (sz, [VG]),
     "phastb_h8_increment_record": (C.c_int, [VG, VM, vp, vp, vp, vp, C.c_double, dp, vp, sz, vp]),
+    "phastb_h8_increment_record_ex": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, C.c_double, PL, dp, vp, sz, vp]),
+    "phastb_h8_pfczm_degradation": (C.c_int, [VG, VM, PL, vp, vp, vp, vp]),
+    "phastb_h8_pfczm_workspace_bytes": (sz, [VG]),
+    "phastb_h8_pfczm_energy": (C.c_int, [VG, VM, PL, vp, vp, vp, dp, vp, sz, vp]),
+    "phastb_h8_pfczm_gradient": (C.c_int, [VG, VM, PL, vp, vp, vp, C.c_double, vp, vp, sz, vp]),
+    "phastb_h8_pfczm_tangent_weights": (C.c_int, [VG, VM, PL, vp, vp, vp, vp, vp]),
+    "phastb_h8_pfczm_tangent_apply": (C.c_int, [VG, VM, vp, vp, vp, C.c_double, vp, vp, sz, vp]),
+    "phastb_h8_pfczm_tangent_diagonal": (C.c_int, [VG, VM, vp, vp, C.c_double, vp, vp, sz, vp]),
+    "phastb_h8_pfczm_solve_workspace_bytes": (sz, [VG]),
+    "phastb_h8_pfczm_damage_solve": (C.c_int, [VG, VM, PL, vp, vp, C.c_double, vp, vp, C.c_double, C.c_double,
+                                               C.c_int, C.c_int, C.c_int, vp, ip, dp, vp, sz, vp]),
     "phastb_h8_damage_residual_workspace_bytes": (sz, [VG]),
     "phastb_h8_damage_residual_norm": (C.c_int, [VG, VM, vp, vp, C.c_double, vp, dp, vp, sz, vp]),
     "phastb_scale_set": (C.c_int, [C.c_int, vp, C.c_double, C.c_int, C.c_double, vp, vp]),
@@ -171,6 +187,7 @@ SIGNATURES = {
     "phastb_batch_stagger_change": (C.c_int, [vp, vp, vp, vp, vp, dp, vp, sz, vp]),
 }
 RECORD_WORDS = 27
+PFCZM_ENERGY_WORDS = 4 + MAX_SLOTS
 
 _lock = threading.Lock()
 _lib = None

@@ -708,8 +708,9 @@ __global__ void __launch_bounds__(kThreads) h8_record_kernel(VoxGeom g, VoxMat<d
                                                              const uint8_t* __restrict__ slot,
                                                              const double* __restrict__ d,
                                                              const double* __restrict__ H, double threshold,
-                                                             RedWs ws) {
+                                                             int pfczm, RedWs ws) {
   const double ihx = 1.0 / g.hx, ihy = 1.0 / g.hy, ihz = 1.0 / g.hz, w = g.w, ell = m.ell;
+  constexpr double kPi = 3.14159265358979323846;
   double acc[kRecSums];
 #pragma unroll
   for (int k = 0; k < kRecSums; ++k) acc[k] = 0.0;
@@ -723,9 +724,15 @@ __global__ void __launch_bounds__(kThreads) h8_record_kernel(VoxGeom g, VoxMat<d
 #pragma unroll
     for (int L = 0; L < 8; ++L) dd[L] = __ldg(d + nd[L]);
     interp_sf(dd, dq);
+    // AT2: int d^2; PF-CZM: int alpha(d) = int (2 d - d^2)
     double mloc = 0.0;
+    if (pfczm) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) mloc += dq[q] * dq[q];
+      for (int q = 0; q < 8; ++q) mloc += 2.0 * dq[q] - dq[q] * dq[q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) mloc += dq[q] * dq[q];
+    }
     double Dx[2][2], Dy[2][2], Dz[2][2];
     grad_sf(dd, ihx, ihy, ihz, Dx, Dy, Dz);
     double gl = 0.0;
@@ -736,8 +743,8 @@ __global__ void __launch_bounds__(kThreads) h8_record_kernel(VoxGeom g, VoxMat<d
     // each face-difference gradient value holds at the two Gauss points along its own axis
     const int s = slot[e];
     const double Gc = m.Gc[s];
-    const double local = Gc / (2.0 * ell) * (w * mloc);
-    const double grad = 0.5 * Gc * ell * (2.0 * w * gl);
+    const double local = pfczm ? Gc / (kPi * ell) * (w * mloc) : Gc / (2.0 * ell) * (w * mloc);
+    const double grad = pfczm ? Gc * ell / kPi * (2.0 * w * gl) : 0.5 * Gc * ell * (2.0 * w * gl);
 #pragma unroll
     for (int k = 0; k < PHASTB_MAX_SLOTS; ++k) acc[k] += (k == s) ? local + grad : 0.0;
     acc[PHASTB_MAX_SLOTS] += local;
@@ -812,6 +819,14 @@ size_t phastb_h8_record_workspace_bytes(const phastb_voxel_grid* g) {
 int phastb_h8_increment_record(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
                                const double* x, const double* d, const double* H, double threshold,
                                double* out_host, void* workspace, size_t workspace_bytes, void* stream) {
+  return phastb_h8_increment_record_ex(g, m, slot, x, nullptr, d, H, threshold, nullptr, out_host, workspace,
+                                       workspace_bytes, stream);
+}
+
+int phastb_h8_increment_record_ex(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                                  const double* x, const double* gq, const double* d, const double* H,
+                                  double threshold, const phastb_pfczm_law* law, double* out_host,
+                                  void* workspace, size_t workspace_bytes, void* stream) {
   if (!valid_vox(g) || !valid_mat(m) || !slot || !d || !out_host) return PHASTB_ERR_ARG;
   if (!workspace || workspace_bytes < phastb_h8_record_workspace_bytes(g)) return PHASTB_ERR_WORKSPACE;
   const VoxGeom v = make_vox_geom(*g);
@@ -822,11 +837,11 @@ int phastb_h8_increment_record(const phastb_voxel_grid* g, const phastb_voxel_ma
   if ((st = red_ws_reset(ws_s, s)) || (st = red_ws_reset(ws_d, s))) return st;
   if (x) {
     { note_launch(); h8_mech_elem_kernel<double, true><<<grid_for(v.n_elem), kThreads, 0, s>>>(
-        v, make_vox_mat<double>(*m), slot, x, nullptr, d, nullptr, nullptr, nullptr, ws_s, nullptr); }
+        v, make_vox_mat<double>(*m), slot, x, gq, d, nullptr, nullptr, nullptr, ws_s, nullptr); }
     if ((st = last_launch_status())) return st;
   }
   { note_launch(); h8_record_kernel<<<grid_for(v.n_elem), kThreads, 0, s>>>(v, make_vox_mat<double>(*m), slot, d, H,
-                                                                             threshold, ws_d); }
+                                                                             threshold, law ? 1 : 0, ws_d); }
   if ((st = last_launch_status())) return st;
   if (x) {
     if ((st = cuda_status(cudaMemcpyAsync(out_host, x + 3 * (size_t)v.n_red, 6 * sizeof(double),

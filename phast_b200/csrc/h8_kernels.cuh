@@ -51,7 +51,11 @@ struct VoxMat {
   T lam[PHASTB_MAX_SLOTS], mu[PHASTB_MAX_SLOTS], Gc[PHASTB_MAX_SLOTS];
   int driver[PHASTB_MAX_SLOTS];
   int iso;
-  int pad_;  // no implicit padding (hashed as bytes)
+  // Form of the scalar damage operator (no implicit padding: hashed as bytes):
+  // 0 AT2, Gc (M/ell + ell L) + 2 (1 - kappa) H-mass; 1 the PF-CZM Newton tangent,
+  // Gc (2 ell/pi) L + the mass of the Gauss-point weights passed as the history
+  // (built with kappa = 1/2, so that 2 (1 - kappa) = 1).
+  int dform;
   T kappa, ell;
 };
 static_assert(sizeof(VoxMat<double>) == 8 * (PHASTB_MAX_SLOTS * 24 + 2) + 4 * (PHASTB_MAX_SLOTS + 2), "padding");
@@ -76,6 +80,24 @@ VoxMat<T> make_vox_mat(const phastb_voxel_material& m) {
   r.iso = m.isotropic;
   r.kappa = T(m.kappa);
   r.ell = T(m.ell);
+  return r;
+}
+
+// The same material in another word size (field by field).
+template <typename U, typename T>
+VoxMat<U> vox_mat_cast(const VoxMat<T>& a) {
+  VoxMat<U> r{};
+  for (int s = 0; s < PHASTB_MAX_SLOTS; ++s) {
+    for (int k = 0; k < 21; ++k) r.C[s][k] = U(a.C[s][k]);
+    r.lam[s] = U(a.lam[s]);
+    r.mu[s] = U(a.mu[s]);
+    r.Gc[s] = U(a.Gc[s]);
+    r.driver[s] = a.driver[s];
+  }
+  r.iso = a.iso;
+  r.dform = a.dform;
+  r.kappa = U(a.kappa);
+  r.ell = U(a.ell);
   return r;
 }
 

@@ -974,10 +974,12 @@ __device__ __forceinline__ double dtile_pass(const DTileArgs<T>& a, unsigned cha
 template <typename T>
 void damage_slot_coefs(DTileArgs<T>& a, const VoxMat<T>& m) {
   const T w = T(a.g.w), ell = T(a.ell);
+  // PF-CZM tangent: no mass term of its own, Gc (2 ell / pi) L
+  const T lt = T(2.0 * a.ell / 3.14159265358979323846);
   for (int i = 0; i < PHASTB_MAX_SLOTS; ++i) {
     const T gc = m.Gc[i];
-    a.gc_ell[i] = gc / ell;
-    a.gc_k2[i] = T(2) * w * gc * ell;
+    a.gc_ell[i] = m.dform == 1 ? T(0) : gc / ell;
+    a.gc_k2[i] = m.dform == 1 ? T(2) * w * gc * lt : T(2) * w * gc * ell;
   }
 }
 

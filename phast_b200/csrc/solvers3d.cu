@@ -145,15 +145,16 @@ __global__ void where_kernel(int n, const uint8_t* __restrict__ fixed, const dou
 // fixed = la | ua | peq; known = where(fixed, (ua ? upper : lower), 0);
 // x0f = where(free, initial, 0); invd = 1/where(free, diag, 1)
 __global__ void kkt_setup_kernel(int n, const uint8_t* __restrict__ la, const uint8_t* __restrict__ ua,
-                                 const double* __restrict__ lower, double upper, const double* __restrict__ initial,
-                                 const double* __restrict__ diag, uint8_t* __restrict__ fixed,
-                                 double* __restrict__ known, double* __restrict__ x0f,
+                                 const double* __restrict__ lower, const double* __restrict__ upv, double upper,
+                                 const double* __restrict__ initial, const double* __restrict__ diag,
+                                 uint8_t* __restrict__ fixed, double* __restrict__ known, double* __restrict__ x0f,
                                  double* __restrict__ invd) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const bool peq = lower[i] == upper;
+    const double ub = upv ? upv[i] : upper;
+    const bool peq = lower[i] == ub;
     const bool f = la[i] || ua[i] || peq;
     fixed[i] = f;
-    known[i] = f ? (ua[i] ? upper : lower[i]) : 0.0;
+    known[i] = f ? (ua[i] ? ub : lower[i]) : 0.0;
     x0f[i] = f ? 0.0 : (initial ? initial[i] : 0.0);
     invd[i] = 1.0 / (f ? 1.0 : diag[i]);
   }
@@ -164,7 +165,8 @@ __global__ void __launch_bounds__(kThreads) kkt_update_kernel(int n, const uint8
                                                               const double* __restrict__ cand,
                                                               const double* __restrict__ Acand,
                                                               const double* __restrict__ rhs,
-                                                              const double* __restrict__ lower, double upper,
+                                                              const double* __restrict__ lower,
+                                                              const double* __restrict__ upv, double upper,
                                                               double kkt_tol, uint8_t* __restrict__ la,
                                                               uint8_t* __restrict__ ua, double* __restrict__ grad,
                                                               RedWs ws) {
@@ -174,7 +176,7 @@ __global__ void __launch_bounds__(kThreads) kkt_update_kernel(int n, const uint8
     grad[i] = gr;
     const bool fr = !fixed[i];
     const bool add_l = fr && (cand[i] < lower[i]);
-    const bool add_u = fr && (cand[i] > upper);
+    const bool add_u = fr && (cand[i] > (upv ? upv[i] : upper));
     const bool rel_l = la[i] && (gr < -kkt_tol);
     const bool rel_u = ua[i] && (gr > kkt_tol);
     if (add_l || add_u || rel_l || rel_u) acc[0] += 1.0;
@@ -187,17 +189,18 @@ __global__ void __launch_bounds__(kThreads) kkt_update_kernel(int n, const uint8
 // KKT audit (box_kkt_h8._kkt_diagnostics): returns violation count and maxima.
 __global__ void __launch_bounds__(kThreads) kkt_audit_kernel(int n, const double* __restrict__ sol,
                                                              const double* __restrict__ grad,
-                                                             const double* __restrict__ lower, double upper,
+                                                             const double* __restrict__ lower,
+                                                             const double* __restrict__ upv, double upper,
                                                              const uint8_t* __restrict__ la,
                                                              const uint8_t* __restrict__ ua, double tol, RedWs ws) {
   // acc: [violations count, max|free grad|, max|projected grad|, max|complementarity|]
   double cnt = 0, fs = 0, pg = 0, cm = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double s = sol[i], g = grad[i], lo = lower[i];
-    const bool peq = lo == upper;
+    const double s = sol[i], g = grad[i], lo = lower[i], up = upv ? upv[i] : upper;
+    const bool peq = lo == up;
     const bool l = la[i], u = ua[i];
     const bool fixed = l || u || peq;
-    if (s < lo || s > upper) cnt += 1.0;
+    if (s < lo || s > up) cnt += 1.0;
     if (l && g < -tol) cnt += 1.0;
     if (u && -g < -tol) cnt += 1.0;
     if (!fixed) {
@@ -210,7 +213,7 @@ __global__ void __launch_bounds__(kThreads) kkt_audit_kernel(int n, const double
     }
     if (u) {
       pg = fmax(pg, fabs(fmax(g, 0.0)));
-      cm = fmax(cm, fabs(fmax(-g, 0.0) * (upper - s)));
+      cm = fmax(cm, fabs(fmax(-g, 0.0) * (up - s)));
     }
   }
   __shared__ double sh[32];
@@ -380,19 +383,20 @@ size_t phastb_h8_box_kkt_workspace_bytes(const phastb_voxel_grid* g) {
          align_up(sizeof(float) * 8 * (size_t)v.n_elem) + red_ws_bytes();
 }
 
-int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
-                             const double* H, double scale, const double* lower, double upper,
-                             const double* initial, double lin_tol, double kkt_tol, int max_lin, int max_active,
-                             double* d_out, int* info, void* workspace, size_t workspace_bytes, void* stream) {
-  if (!valid_vox(g) || !valid_mat(m) || !slot || !lower || !d_out || max_lin < 1 || max_active < 1 ||
-      !(lin_tol > 0) || !(kkt_tol >= 0))
-    return PHASTB_ERR_ARG;
-  if (!workspace || workspace_bytes < phastb_h8_box_kkt_workspace_bytes(g)) return PHASTB_ERR_WORKSPACE;
-  ScopedStream scope((cudaStream_t)stream);
-  if (scope.status()) return scope.status();
-  cudaStream_t s = scope.get();
-  const VoxGeom v = make_vox_geom(*g);
-  const VoxMat<double> mm = make_vox_mat<double>(*m);
+}  // extern "C"
+
+namespace phastb {
+
+// The primal active-set box solve behind phastb_h8_damage_box_kkt.  With rhs_in / diag_in
+// NULL the system is the AT2 damage system of history H (its right-hand side and Jacobi
+// diagonal formed here); otherwise the caller gives them and H holds the Gauss-point
+// weights of the operator mm describes (the PF-CZM Newton tangent).  upper_v (NULL: the
+// scalar upper) is the upper bound per node.  The workspace is
+// phastb_h8_box_kkt_workspace_bytes.
+int box_kkt_run(const VoxGeom& v, const VoxMat<double>& mm, const uint8_t* slot, const double* H, double scale,
+                const double* rhs_in, const double* diag_in, const double* lower, const double* upper_v,
+                double upper, const double* initial, double lin_tol, double kkt_tol, int max_lin, int max_active,
+                bool allow_mixed, double* d_out, int* info, void* workspace, cudaStream_t s) {
   const int n = v.n_red;
   char* p = static_cast<char*>(workspace);
   PcgWs<double> w = pcg_ws<double>(p, n);
@@ -431,7 +435,7 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
   float* palt32 = reinterpret_cast<float*>(q32 + 3 * fb);
   float* H32 = H ? reinterpret_cast<float*>(q32 + 4 * fb) : nullptr;
   RedWs dw32 = red_ws(q32 + 4 * fb + align_up(sizeof(float) * 8 * (size_t)v.n_elem));
-  const bool mixed = damage_mixed_enabled();
+  const bool mixed = allow_mixed && damage_mixed_enabled();
   const int G = grid_for(n);
   int st;
   if ((st = red_ws_reset(rw, s))) return st;
@@ -441,7 +445,7 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
   if (H && (st = cuda_status(cudaMemcpyAsync(Hw, H, sizeof(double) * 8 * (size_t)v.n_elem,
                                               cudaMemcpyDeviceToDevice, s))))
     return st;
-  const VoxMat<float> m32 = make_vox_mat<float>(*m);
+  const VoxMat<float> m32 = vox_mat_cast<float>(mm);
   if (mixed && H) {
     const size_t ne = 8 * (size_t)v.n_elem;
     { note_launch(); to_f32_kernel<<<grid_for((long long)ne), kThreads, 0, s>>>(ne, Hw, H32); }
@@ -451,15 +455,24 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
     const int e = cuda_status(cudaMemcpyAsync(d_out, xd, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     return e ? e : code;
   };
-  if ((st = h8_damage_launch(v, mm, slot, 1, nullptr, Hw, scale, rhs, nullptr, scratch, nullptr, s))) return st;
-  if (!H && (st = cuda_status(cudaMemsetAsync(rhs, 0, sizeof(double) * n, s)))) return st;
-  if ((st = h8_damage_launch(v, mm, slot, 2, nullptr, Hw, scale, diag, nullptr, scratch, nullptr, s))) return st;
+  if (rhs_in) {
+    if ((st = cuda_status(cudaMemcpyAsync(rhs, rhs_in, sizeof(double) * n, cudaMemcpyDeviceToDevice, s)))) return st;
+  } else {
+    if ((st = h8_damage_launch(v, mm, slot, 1, nullptr, Hw, scale, rhs, nullptr, scratch, nullptr, s))) return st;
+    if (!H && (st = cuda_status(cudaMemsetAsync(rhs, 0, sizeof(double) * n, s)))) return st;
+  }
+  if (diag_in) {
+    if ((st = cuda_status(cudaMemcpyAsync(diag, diag_in, sizeof(double) * n, cudaMemcpyDeviceToDevice, s))))
+      return st;
+  } else if ((st = h8_damage_launch(v, mm, slot, 2, nullptr, Hw, scale, diag, nullptr, scratch, nullptr, s))) {
+    return st;
+  }
   if ((st = cuda_status(cudaMemsetAsync(la, 0, 2 * ub, s)))) return st;
   DamageCtx full{v, mm, slot, Hw, scale, nullptr, scratch};
   int total = 0;
   const double* cinit = initial;
   for (int ai = 1; ai <= max_active; ++ai) {
-    { note_launch(); kkt_setup_kernel<<<G, kThreads, 0, s>>>(n, la, ua, lower, upper, cinit, diag, fixed, known, xd, invd); }
+    { note_launch(); kkt_setup_kernel<<<G, kThreads, 0, s>>>(n, la, ua, lower, upper_v, upper, cinit, diag, fixed, known, xd, invd); }
     // b_f = where(free, rhs - A known, 0)
     if ((st = damage_op(&full, known, w.Ap, nullptr, s))) return st;
     { note_launch(); constrained_rhs_kernel<<<G, kThreads, 0, s>>>(n, fixed, rhs, w.Ap, bf, rw); }
@@ -535,10 +548,10 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
     if (pr.breakdown) return finish(PHASTB_BREAKDOWN);
     // gradient, active-set change
     if ((st = damage_op(&full, xd, w.Ap, nullptr, s))) return st;
-    { note_launch(); kkt_update_kernel<<<G, kThreads, 0, s>>>(n, fixed, xd, w.Ap, rhs, lower, upper, kkt_tol, la, ua, grad, rw); }
+    { note_launch(); kkt_update_kernel<<<G, kThreads, 0, s>>>(n, fixed, xd, w.Ap, rhs, lower, upper_v, upper, kkt_tol, la, ua, grad, rw); }
     // the audit of the updated sets is only read when nothing changed, but running
     // it now lets one synchronisation fetch both results
-    { note_launch(); kkt_audit_kernel<<<G, kThreads, 0, s>>>(n, xd, grad, lower, upper, la, ua, kkt_tol, kw); }
+    { note_launch(); kkt_audit_kernel<<<G, kThreads, 0, s>>>(n, xd, grad, lower, upper_v, upper, la, ua, kkt_tol, kw); }
     if ((st = last_launch_status())) return st;
     double changes, a[4];
     if ((st = cuda_status(cudaMemcpyAsync(&changes, rw.out, sizeof(double), cudaMemcpyDeviceToHost, s)))) return st;
@@ -556,6 +569,25 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
     cinit = grad;
   }
   return finish(PHASTB_NONCONVERGED);
+}
+
+}  // namespace phastb
+
+extern "C" {
+
+int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                             const double* H, double scale, const double* lower, double upper,
+                             const double* initial, double lin_tol, double kkt_tol, int max_lin, int max_active,
+                             double* d_out, int* info, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !lower || !d_out || max_lin < 1 || max_active < 1 ||
+      !(lin_tol > 0) || !(kkt_tol >= 0))
+    return PHASTB_ERR_ARG;
+  if (!workspace || workspace_bytes < phastb_h8_box_kkt_workspace_bytes(g)) return PHASTB_ERR_WORKSPACE;
+  ScopedStream scope((cudaStream_t)stream);
+  if (scope.status()) return scope.status();
+  return box_kkt_run(make_vox_geom(*g), make_vox_mat<double>(*m), slot, H, scale, nullptr, nullptr, lower, nullptr,
+                     upper, initial, lin_tol, kkt_tol, max_lin, max_active, true, d_out, info, workspace,
+                     scope.get());
 }
 
 int phastb_h8_stagger_change(int n_u, const double* x_new, const double* x_old, int n_d, const double* d_new,

@@ -5,9 +5,9 @@ and ``build_element_arrays`` (src/phast/solid3d/materials.py:474-547) with the s
 names, fields, defaults and validation errors, so a caller written against the
 reference builds the same objects here.  Objects of the reference package with
 the same fields are accepted wherever these are (the operator reads attributes
-only).  Options of the reference that this backend does not run (PF-CZM damage,
-crack closure, Anderson mixing, smeared-laminate phases, the interface driver,
-``history_only`` irreversibility) are accepted by the data classes and refused
+only).  Options of the reference that this backend does not run (crack closure,
+Anderson mixing, smeared-laminate phases, the interface driver, ``history_only``
+irreversibility) are accepted by the data classes and refused
 with ``NotImplementedError`` when an operator or solver is built from them.
 """
 from __future__ import annotations
@@ -318,7 +318,7 @@ class SolverConfig:
     """Numerical settings of the staggered solve (model.py:706-897); defaults are PhAST's.
 
     The GPU backend runs ``dtype='float64'`` results (the chosen mechanics form may compute
-    in FP32 under FP64 refinement; see ``StaggeredSolver(form=...)``), ``damage_law='at2'``,
+    in FP32 under FP64 refinement; see ``StaggeredSolver(form=...)``), ``damage_law`` 'at2' or 'pfczm',
     ``irreversibility='box_kkt'``, ``history`` 'max' or 'current', ``crack_closure='none'`` and
     ``anderson_depth=0``; ``device`` names the CUDA device.
     """
@@ -353,7 +353,7 @@ class SolverConfig:
     damage_law: str = "at2"
     pfczm_softening: str = "linear"
     pfczm_p: float = 2
-    pfczm_max_newton: int = 50
+    pfczm_max_newton: int = 100
 
     def __post_init__(self):
         for key in ("batch_size", "max_stagger", "pcg_maxit_mech", "check_every", "damage_maxit",
@@ -393,8 +393,6 @@ class SolverConfig:
 def unsupported_options(cfg):
     """Names of ``cfg`` settings this backend does not run (empty when it runs them all)."""
     out = []
-    if getattr(cfg, "damage_law", "at2") != "at2":
-        out.append(f"damage_law={cfg.damage_law!r}")
     if getattr(cfg, "crack_closure", "none") != "none":
         out.append(f"crack_closure={cfg.crack_closure!r}")
     if getattr(cfg, "anderson_depth", 0) != 0:
@@ -497,13 +495,17 @@ def build_element_arrays(model, cfg, *, device=None):
         tangent=torch.as_tensor(np.asarray(model.tangent).reshape(-1, 3), dtype=torch.float64, device=target))
 
 
-def sphere_pore_model(shape, radius_fraction, *, E=3000.0, nu=0.35, Gc=0.5, ell_voxels=2.0, pore_stiffness=1e-6):
-    """A cubic-voxel cell of ``mi_matrix`` with one central spherical ``pore`` (E x ``pore_stiffness``)."""
+def sphere_pore_model(shape, radius_fraction, *, E=3000.0, nu=0.35, Gc=0.5, ell_voxels=2.0, pore_stiffness=1e-6,
+                      tensile_strength=None, pore_tensile_strength=None):
+    """A cubic-voxel cell of ``mi_matrix`` with one central spherical ``pore`` (E x ``pore_stiffness``);
+    the tensile strengths (MPa) are those of the PF-CZM law."""
     nx, ny, nz = shape
     h = 1.0 / nz
     phase = sphere_pore_phase(shape, radius_fraction, PHASE_ID["mi_matrix"], PHASE_ID["pore"])
-    phases = {"mi_matrix": PhaseMaterial("mi_matrix", "isotropic", Gc, "spectral", E, nu),
-              "pore": PhaseMaterial("pore", "isotropic", Gc, "spectral", E * pore_stiffness, nu)}
+    phases = {"mi_matrix": PhaseMaterial("mi_matrix", "isotropic", Gc, "spectral", E, nu,
+                                         tensile_strength=tensile_strength),
+              "pore": PhaseMaterial("pore", "isotropic", Gc, "spectral", E * pore_stiffness, nu,
+                                    tensile_strength=pore_tensile_strength)}
     tangent = np.zeros((nz, ny, nx, 3))
     tangent[..., 2] = 1.0
     return VoxelModel(VoxelGrid(shape, (h, h, h)), phase, tangent, MaterialTable(phases, ell_voxels * h, "micro"))

@@ -9,6 +9,7 @@ one launch each of ``libphastb.so``'s tiled z-marching kernels.
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import numpy as np
 import torch
@@ -18,6 +19,15 @@ from .._lib import call, ptr, stream
 from .model import SolverConfig, build_element_arrays, isotropic_C, unsupported_options
 
 PORE = "pore"
+
+
+def pfczm_softening_parameters(softening):
+    """``(a2, a3)`` of Wu's softening laws (pfczm.py:57-65)."""
+    if softening == "linear":
+        return -0.5, 0.0
+    if softening == "exponential":
+        return 2.0 ** (5.0 / 3.0) - 3.0, 0.0
+    raise ValueError(f"PF-CZM softening must be one of ('linear', 'exponential'), got {softening!r}")
 
 
 def _driver_code(phase, split_isotropic):
@@ -45,7 +55,7 @@ class PeriodicVoxelPhaseFieldOperator:
         bad = unsupported_options(cfg)
         if bad:
             raise NotImplementedError(f"the B200 backend does not run {', '.join(bad)}")
-        if pfczm_strengths is not None:
+        if pfczm_strengths is not None and getattr(cfg, "damage_law", "at2") != "pfczm":
             raise ValueError("pfczm_strengths applies to damage_law 'pfczm' only")
         model.validate()
         if materials is None:
@@ -64,6 +74,8 @@ class PeriodicVoxelPhaseFieldOperator:
         self.mat_arrays = materials
         self._setup(model.grid, slot, phases, float(model.materials.length_scale), float(cfg.kappa), load,
                     cfg.energy_split_isotropic, pinned_node, materials.stiffness_index.device)
+        if getattr(cfg, "damage_law", "at2") == "pfczm":
+            self._build_pfczm(cfg, pfczm_strengths)
 
     @classmethod
     def from_slots(cls, grid, slot, phases, ell, kappa, load, *, split_isotropic="spectral", pinned_node=None,
@@ -137,6 +149,11 @@ class PeriodicVoxelPhaseFieldOperator:
         self._red = _lib.Workspace(self.device)
         self._rec = _lib.Workspace(self.device)
         self._resid = _lib.Workspace(self.device)
+        self._pf = None
+        self._pfws = _lib.Workspace(self.device)
+        self.pfczm_bound = None
+        self.pfczm_phases = {}
+        self.pfczm_strengths = {}
 
     # -- construction helpers -----------------------------------------------------------
     def _choose_pinned_node(self):
@@ -163,6 +180,64 @@ class PeriodicVoxelPhaseFieldOperator:
             nodes = i + rx * (j + ry * k)
             np.add.at(count, nodes[pore], 1)
         return int(np.argmin(count))
+
+    def _build_pfczm(self, cfg, strengths):
+        """Per-slot ``a1`` of the PF-CZM law and the onset check (operator.py:326-439).
+
+        ``a1 = 4 E Gc / (pi ell f_t^2 (1 - kappa))`` (pfczm.py:16-31) with ``f_t`` the phase's
+        ``tensile_strength`` or its ``pfczm_strengths`` override; raises ``ValueError`` when a present
+        phase has no strength, or when ``a1 < p + a2`` (``g''(0) < 0``) in a phase with a damage driver.
+        """
+        a2, a3 = pfczm_softening_parameters(cfg.pfczm_softening)
+        p = float(cfg.pfczm_p)
+        bound = p + a2
+        scale = max(1.0 - self.kappa, 1.0e-30)
+        law = _lib.PfczmLaw()
+        law.a2, law.a3, law.p = a2, a3, p
+        strengths = dict(strengths or {})
+        names = {ph.name for ph in self.phases}
+        for name, value in strengths.items():
+            if name not in names:
+                raise ValueError(f"pfczm_strengths phase {name!r} is not present in the cell")
+            f = float(value)
+            if not (math.isfinite(f) and f > 0.0):
+                raise ValueError(f"pfczm_strengths[{name!r}] must be finite and positive")
+            self.pfczm_strengths[name] = f
+        missing, violations = [], []
+        for s, ph in enumerate(self.phases):
+            f = self.pfczm_strengths.get(ph.name, getattr(ph, "tensile_strength", None))
+            if f is None:
+                missing.append(ph.name)
+                continue
+            E, Gc, f = float(ph.E), float(ph.Gc), float(f)
+            a1 = 4.0 * E * Gc / (math.pi * self.ell * f ** 2 * scale)
+            law.a1[s] = a1
+            checked = int(self.mat.driver[s]) != _lib.DRIVER_NONE
+            f_max = (4.0 * E * Gc / (math.pi * self.ell * scale) / bound) ** 0.5
+            ell_max = 4.0 * E * Gc / (math.pi * f ** 2 * scale) / bound
+            ok = (not checked) or a1 >= bound
+            if not ok:
+                violations.append(f"{ph.name}: a1 = {a1:.4g} < {bound:g} (f_t = {f:g} MPa; largest admissible f_t "
+                                  f"{f_max:.4g} MPa at this ell, largest admissible ell {ell_max:.4g} mm at this f_t)")
+            self.pfczm_phases[ph.name] = {"f_t": f, "E_ref_min": E, "E_ref_max": E, "Gc_min": Gc, "Gc_max": Gc,
+                                          "a1_min": a1, "a1_max": a1, "a1_bound": bound, "f_t_max": f_max,
+                                          "ell_max": ell_max, "onset_checked": checked, "onset_ok": ok}
+        if missing:
+            raise ValueError("damage_law 'pfczm' needs a tensile strength for every phase of the cell "
+                             f"(material.tensile_strength); missing: {', '.join(missing)}")
+        if violations:
+            raise ValueError(f"damage_law 'pfczm': the onset condition a1 >= p + a2 = {bound:g} (g''(0) >= 0, i.e. "
+                             "ell <= 4 E Gc / (pi f_t^2 (1 - kappa)(p + a2)), 8 l_ch / (3 pi) for linear softening) "
+                             f"fails at ell = {self.ell:g} mm in: " + "; ".join(violations))
+        self._pf = law
+        self.pfczm_bound = bound
+        self._a1 = torch.as_tensor(np.array([law.a1[s] for s in range(len(self.phases))])[self.slot_np],
+                                   dtype=torch.float64, device=self.device)
+
+    @property
+    def is_pfczm(self):
+        """Whether the damage law is the PF-CZM law (``damage_law = 'pfczm'``)."""
+        return self._pf is not None
 
     def scratch(self, dtype=torch.float64):
         code = _lib.F64 if dtype == torch.float64 else _lib.F32
@@ -215,11 +290,24 @@ class PeriodicVoxelPhaseFieldOperator:
 
     # -- mechanics -------------------------------------------------------------------------
     def degradation(self, d):
-        """g (E, 8) = (1-kappa)(1-d_q)^2 + kappa (operator.py:939-946)."""
+        """Gauss-point degradation g (E, 8) with d_q = d_e N^T (operator.py:939-946): AT2
+        (1-kappa)(1-d_q)^2 + kappa, or the PF-CZM rational law (FP64) with ``damage_law='pfczm'``."""
         d = self._check("d", d, (self.n_red,))
+        if self._pf is not None:
+            dd = d.to(torch.float64).contiguous()
+            g = torch.empty(self.n_elements, 8, dtype=torch.float64, device=self.device)
+            call("phastb_h8_pfczm_degradation", self.vgrid, self.mat, C.byref(self._pf), ptr(self.slot), ptr(dd),
+                 ptr(g), stream())
+            return g.to(d.dtype)
         g = torch.empty(self.n_elements, 8, dtype=d.dtype, device=self.device)
         call("phastb_h8_degradation", self.vgrid, self._dt(d), ptr(d), self.kappa, ptr(g), stream())
         return g
+
+    def _law_g(self, g, d, dtype):
+        """``(g, d)`` for the kernels: the PF-CZM law cannot be fused from ``d``, so it becomes ``g``."""
+        if self._pf is not None and g is None and d is not None:
+            return self.degradation(d).to(dtype), None
+        return g, d
 
     @staticmethod
     def _no_closure(opening=None, closure=None):
@@ -231,6 +319,7 @@ class PeriodicVoxelPhaseFieldOperator:
         the degradation into the action; ``mask`` zeroes rows; ``out`` receives the result."""
         self._no_closure(opening, closure)
         x = self._check("x", x, (self.n_mech,))
+        g, d = self._law_g(g, d, x.dtype)
         gq = None if g is None else self._check("g", g, (self.n_elements, 8), x.dtype)
         dd = None if d is None else self._check("d", d, (self.n_red,)).to(x.dtype)
         mk = None if mask is None else mask.to(torch.uint8).contiguous()
@@ -246,6 +335,7 @@ class PeriodicVoxelPhaseFieldOperator:
 
     def mech_operator(self, g=None, *, d=None):
         """The action ``v -> A(g) v`` as a callable that ``solve_constrained`` recognises."""
+        g, d = self._law_g(g, d, torch.float64)
         return MechOperator(self, g, d)
 
     def tile_shape(self, dtype=torch.float64, shape=None):
@@ -275,6 +365,7 @@ class PeriodicVoxelPhaseFieldOperator:
         """Jacobi diagonal of A(g) (operator.py:1196-1254)."""
         self._no_closure(opening, closure)
         dtype = g.dtype if g is not None else (d.dtype if d is not None else torch.float64)
+        g, d = self._law_g(g, d, dtype)
         gq = None if g is None else self._check("g", g, (self.n_elements, 8), dtype)
         dd = None if d is None else self._check("d", d, (self.n_red,), dtype)
         y = torch.empty(self.n_mech, dtype=dtype, device=self.device)
@@ -284,6 +375,7 @@ class PeriodicVoxelPhaseFieldOperator:
 
     def _stress_energy(self, x, g=None, d=None):
         x = self._check("x", x, (self.n_mech,), torch.float64)
+        g, d = self._law_g(g, d, torch.float64)
         gq = None if g is None else self._check("g", g, (self.n_elements, 8), torch.float64)
         dd = None if d is None else self._check("d", d, (self.n_red,), torch.float64)
         rE = (C.c_double * 6)()
@@ -362,7 +454,9 @@ class PeriodicVoxelPhaseFieldOperator:
 
     def fracture_energy(self, d):
         """Fracture energy in mJ (operator.py:1511-1545): per element Gc/(2 ell) d.M d ('local') plus
-        Gc ell/2 d.L d ('gradient'), and 'by_phase' over the present phases (pores included)."""
+        Gc ell/2 d.L d ('gradient'), and 'by_phase' over the present phases (pores included).  With
+        the PF-CZM law the functional is Gc/(pi ell) int (2d - d^2) + Gc ell/pi int |grad d|^2
+        (_pfczm_fracture_energy, operator.py:608-631)."""
         out = self.increment_record(None, d, None, 1.0)
         return {"total": out["local"] + out["gradient"], "local": out["local"], "gradient": out["gradient"],
                 "by_phase": out["by_phase"]}
@@ -376,8 +470,14 @@ class PeriodicVoxelPhaseFieldOperator:
         Hq = None if H is None else self._check("H", H, (self.n_elements, 8), torch.float64)
         out = (C.c_double * _lib.RECORD_WORDS)()
         wp, wn = self._rec.get(_lib.load().phastb_h8_record_workspace_bytes(self.vgrid))
-        call("phastb_h8_increment_record", self.vgrid, self.mat, ptr(self.slot), ptr(xx), ptr(d), ptr(Hq),
-             float(threshold), out, wp, wn, stream())
+        if self._pf is not None:
+            # elastic part at the PF-CZM degradation, surface energy of the PF-CZM functional
+            gq = None if xx is None else self.degradation(d)
+            call("phastb_h8_increment_record_ex", self.vgrid, self.mat, ptr(self.slot), ptr(xx), ptr(gq), ptr(d),
+                 ptr(Hq), float(threshold), C.byref(self._pf), out, wp, wn, stream())
+        else:
+            call("phastb_h8_increment_record", self.vgrid, self.mat, ptr(self.slot), ptr(xx), ptr(d), ptr(Hq),
+                 float(threshold), out, wp, wn, stream())
         v = list(out)
         S = _lib.MAX_SLOTS
         return {"E": np.array(v[0:6]), "rE": np.array(v[6:12]), "energy": v[12],
@@ -394,6 +494,82 @@ class PeriodicVoxelPhaseFieldOperator:
         call("phastb_h8_damage_residual_norm", self.vgrid, self.mat, ptr(self.slot), ptr(Hq), self.damage_scale,
              ptr(d), C.byref(r), wp, wn, stream())
         return float(r.value)
+
+    # -- PF-CZM damage law ------------------------------------------------------------------
+    def _pf_law(self):
+        if self._pf is None:
+            raise ValueError("the PF-CZM damage operators need damage_law 'pfczm'")
+        return C.byref(self._pf)
+
+    def _pf_ws(self):
+        return self._pfws.get(_lib.load().phastb_h8_pfczm_workspace_bytes(self.vgrid))
+
+    def _pf_H(self, H):
+        return None if H is None else self._check("H", H, (self.n_elements, 8), torch.float64)
+
+    def pfczm_damage_energy(self, d, H):
+        """PF-CZM damage energy in mJ as a 0-dim tensor (operator.py:465-489):
+        ``sum_q w H_q g(d_q) + Gc/(pi ell) int (2d - d^2) + Gc ell/pi int |grad d|^2``; ``H=None``
+        drops the history term."""
+        law = self._pf_law()
+        d = self._check("d", d, (self.n_red,), torch.float64)
+        out = (C.c_double * _lib.PFCZM_ENERGY_WORDS)()
+        wp, wn = self._pf_ws()
+        call("phastb_h8_pfczm_energy", self.vgrid, self.mat, law, ptr(self.slot), ptr(d), ptr(self._pf_H(H)), out,
+             wp, wn, stream())
+        return torch.tensor(float(out[0]), dtype=torch.float64, device=self.device)
+
+    def pfczm_damage_gradient(self, d, H, *, scale=1.0):
+        """Unscaled gradient (n_red,) of :meth:`pfczm_damage_energy` (operator.py:491-513)."""
+        law = self._pf_law()
+        d = self._check("d", d, (self.n_red,), torch.float64)
+        y = torch.empty(self.n_red, dtype=torch.float64, device=self.device)
+        wp, wn = self._pf_ws()
+        call("phastb_h8_pfczm_gradient", self.vgrid, self.mat, law, ptr(self.slot), ptr(d), ptr(self._pf_H(H)),
+             float(scale), ptr(y), wp, wn, stream())
+        return y
+
+    def pfczm_tangent_weights(self, d, H):
+        """Gauss-point curvatures (E, 8) of the Newton tangent (operator.py:515-539):
+        ``max(H g''(d_q) - 2 Gc/(pi ell), 0.25 * 2 Gc/(pi ell))``."""
+        law = self._pf_law()
+        d = self._check("d", d, (self.n_red,), torch.float64)
+        W = torch.empty(self.n_elements, 8, dtype=torch.float64, device=self.device)
+        call("phastb_h8_pfczm_tangent_weights", self.vgrid, self.mat, law, ptr(self.slot), ptr(d),
+             ptr(self._pf_H(H)), ptr(W), stream())
+        return W
+
+    def pfczm_tangent_action(self, field, weights, *, scale=1.0):
+        """Unscaled tangent action ``Gc (2 ell/pi) L f + sum_q w c_q N_q N_q^T f`` (operator.py:541-553)."""
+        self._pf_law()
+        f = self._check("field", field, (self.n_red,), torch.float64)
+        W = self._check("weights", weights, (self.n_elements, 8), torch.float64)
+        y = torch.empty(self.n_red, dtype=torch.float64, device=self.device)
+        wp, wn = self._pf_ws()
+        call("phastb_h8_pfczm_tangent_apply", self.vgrid, self.mat, ptr(self.slot), ptr(W), ptr(f), float(scale),
+             ptr(y), wp, wn, stream())
+        return y
+
+    def pfczm_tangent_diagonal(self, weights, *, scale=1.0):
+        """Unscaled Jacobi diagonal of :meth:`pfczm_tangent_action` (operator.py:555-566)."""
+        self._pf_law()
+        W = self._check("weights", weights, (self.n_elements, 8), torch.float64)
+        y = torch.empty(self.n_red, dtype=torch.float64, device=self.device)
+        wp, wn = self._pf_ws()
+        call("phastb_h8_pfczm_tangent_diagonal", self.vgrid, self.mat, ptr(self.slot), ptr(W), float(scale), ptr(y),
+             wp, wn, stream())
+        return y
+
+    def pfczm_newton_system(self, d, H, *, scaled=True, correction=False):
+        """SPD Newton subproblem at ``d`` and the gradient there, both times ``damage_scale`` when
+        ``scaled`` (operator.py:568-606): the tangent ``K`` of the curvature weights and the
+        right-hand side ``K d - gradient`` (``-gradient`` with ``correction=True``)."""
+        scale = self.damage_scale if scaled else 1.0
+        W = self.pfczm_tangent_weights(d, H)
+        gradient = self.pfczm_damage_gradient(d, H, scale=scale)
+        system = PfczmNewtonSystem(self, W, scale)
+        system.rhs = -gradient if correction else system.apply(d) - gradient
+        return system, gradient
 
     def damage_system(self, H, *, scaled=True):
         """The scaled damage system; solved by ``solve_h8_scalar_box_kkt`` (operator.py:1495-1509)."""
@@ -436,3 +612,26 @@ class H8DamageSystem:
     @property
     def diagonal(self):
         return self.op.damage_diagonal(self.H, scale=self.scale)
+
+
+class PfczmNewtonSystem:
+    """The SPD Newton subproblem of the PF-CZM damage solve (operator.py:568-606): ``apply``,
+    ``rhs`` and ``diagonal`` like PhAST's ``H8ScalarSPDSystem``; ``weights`` are the tangent's
+    Gauss-point curvatures."""
+
+    def __init__(self, op, weights, scale):
+        self.op, self.weights, self.scale = op, weights, float(scale)
+        self.rhs = None
+
+    @property
+    def n_dofs(self):
+        return self.op.n_red
+
+    def apply(self, field):
+        return self.op.pfczm_tangent_action(field, self.weights, scale=self.scale)
+
+    action = apply
+
+    @property
+    def diagonal(self):
+        return self.op.pfczm_tangent_diagonal(self.weights, scale=self.scale)

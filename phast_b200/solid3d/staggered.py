@@ -303,7 +303,14 @@ def solve_constrained_form(op, form, *, fixed_mask, fixed_values, d=None, x0=Non
     ``lmax_cache`` (a ctypes array of 3 doubles, zero to estimate) carries the multigrid's
     lambda_max estimates from one solve to the next.
     """
-    if form.precond == "jacobi" and not form.mixed:
+    plain = form.precond == "jacobi" and not form.mixed
+    if getattr(op, "is_pfczm", False) and d is not None:
+        # the PF-CZM degradation enters the elastic action as g (E, 8)
+        if not plain:
+            raise NotImplementedError("damage_law 'pfczm' runs the plain FP64 mechanics form only")
+        return _solve_fused(op, fixed_mask=fixed_mask, fixed_values=fixed_values, g=op.degradation(d), x0=x0,
+                            rtol=rtol, atol=atol, maxiter=maxiter, check_every=check_every)
+    if plain:
         return _solve_fused(op, fixed_mask=fixed_mask, fixed_values=fixed_values, d=d, x0=x0, rtol=rtol,
                             atol=atol, maxiter=maxiter, check_every=check_every)
     n = op.n_mech
@@ -506,6 +513,8 @@ class StaggeredSolver:
         bad = unsupported_options(cfg)
         if bad:
             raise NotImplementedError(f"the B200 backend does not run {', '.join(bad)}")
+        if op.is_pfczm and (form.precond != "jacobi" or form.mixed):
+            raise NotImplementedError("damage_law 'pfczm' runs the plain FP64 mechanics form only")
         self.op = op
         self.load = load
         self.cfg = cfg
@@ -525,6 +534,9 @@ class StaggeredSolver:
         self._mask_u8 = self._mask.to(torch.uint8).contiguous()
         self._zeros = torch.zeros(op.n_mech, dtype=torch.float64, device=op.device)
         self._red = _lib.Workspace(op.device)
+        self._pfws = _lib.Workspace(op.device)
+        self._newton_count = 0
+        self.last_newton_iters = None
         lengths = tuple(n * h for n, h in zip(op.shape, op.h))
         axis = self._c if self._c < 3 else 0
         others = tuple(lengths[a] for a in range(3) if a != axis)
@@ -583,6 +595,8 @@ class StaggeredSolver:
 
     def _damage(self, H, lower, initial):
         """(d, PCG iterations, active-set iterations, kkt_ok) of the box-KKT damage solve (staggered.py:753-800)."""
+        if self.op.is_pfczm:
+            return self._damage_pfczm(H, lower, initial)
         cfg, op = self.cfg, self.op
         r0 = op.damage_residual_norm(H, initial)
         if not math.isfinite(r0):
@@ -602,6 +616,45 @@ class StaggeredSolver:
         except RuntimeError as exc:
             raise _AttemptFailure(f"damage PCG breakdown: {exc}") from exc
         return res.solution, res.total_pcg_iterations, res.active_set_iterations, res.satisfies_kkt
+
+    def _damage_pfczm(self, H, lower, initial):
+        """Projected Newton solve of the PF-CZM damage energy over ``lower <= d <= 1``
+        (StaggeredSolver._damage_pfczm, staggered.py:843-1096), the whole loop in one C-ABI call:
+        box-QP of the tangent per step (the box-KKT engine at damage_kkt_tol / 10), Armijo line
+        search with step halving, projected step doubling after a full step.  Returns
+        ``(d, pcg iterations, active-set iterations, True)``; failures raise ``_AttemptFailure``."""
+        op, cfg = self.op, self.cfg
+        out = torch.empty(op.n_red, dtype=torch.float64, device=op.device)
+        info = (C.c_int * 4)()
+        rinfo = (C.c_double * 2)()
+        wp, wn = self._pfws.get(_lib.load().phastb_h8_pfczm_solve_workspace_bytes(op.vgrid))
+        st = raw("phastb_h8_pfczm_damage_solve", op.vgrid, op.mat, C.byref(op._pf), ptr(op.slot), ptr(H),
+                 float(op.damage_scale), ptr(lower), ptr(initial), float(cfg.damage_kkt_tol),
+                 float(cfg.damage_linear_tol), int(cfg.damage_maxit), int(cfg.damage_max_active_set),
+                 int(cfg.pfczm_max_newton), ptr(out), info, rinfo, wp, wn, stream())
+        pcg, sets, its, reason = (int(v) for v in info)
+        if st not in (_lib.OK, _lib.NONCONVERGED, _lib.BREAKDOWN, _lib.NONFINITE):
+            _lib.check(st, "phastb_h8_pfczm_damage_solve")
+        if st != _lib.OK:
+            if reason == 1:
+                msg = "damage PF-CZM energy is not finite"
+            elif reason == 2:
+                msg = "damage PF-CZM gradient is not finite"
+            elif reason == 3 and st in (_lib.BREAKDOWN, _lib.NONFINITE):
+                msg = f"damage PF-CZM Newton subproblem PCG breakdown (status {st})"
+            elif reason == 3:
+                msg = (f"damage PF-CZM Newton subproblem failed at Newton iteration {its + 1}: H8 scalar box-KKT "
+                       f"failed ({pcg} PCG iterations, {sets} active-set iterations in total)")
+            elif reason == 4:
+                msg = (f"damage PF-CZM line search failed at Newton iteration {its + 1} "
+                       "(no decrease after 30 halvings)")
+            else:
+                msg = (f"damage PF-CZM Newton did not converge in {cfg.pfczm_max_newton} iterations "
+                       f"(projected gradient {rinfo[0]:.3e} > damage_kkt_tol {cfg.damage_kkt_tol:.3e})")
+            raise _AttemptFailure(msg)
+        self.last_newton_iters = its
+        self._newton_count += its
+        return out, pcg, sets, True
 
     def _predictor(self, state, previous, target):
         """x * (target / previous) with E[c] = target; zero start from an unloaded state (staggered.py:1207-1213)."""
@@ -642,6 +695,7 @@ class StaggeredSolver:
 
     def _attempt(self, state, target, previous, increment, cutbacks, t0):
         op, cfg = self.op, self.cfg
+        self._newton_count = 0
         # mech_fixed_values(target) as one kernel: zero except E[controlled] = target
         values = torch.empty(op.n_mech, dtype=torch.float64, device=op.device)
         _lib.call("phastb_scale_set", op.n_mech, ptr(self._zeros), 0.0, self._n_u + self._c, float(target), ptr(values),
@@ -711,7 +765,8 @@ class StaggeredSolver:
             stagger_iters=k, pcg_iters_mech=pm, pcg_iters_pf=pp, active_set_iters=sets, cutbacks=int(cutbacks),
             converged=True, kkt_ok=bool(kkt), stagger_change=float(change),
             mech_relative_residual=float(info.relative_residual), hill_mandel_rel=float(hill_rel),
-            wall_s=perf_counter() - t0, mean_strain=macro_strain)
+            wall_s=perf_counter() - t0, mean_strain=macro_strain,
+            newton_iters_pf=self._newton_count if op.is_pfczm else None)
         return new_state, record
 
     # -- increments with cutback, and the load path -------------------------------------------

@@ -45,6 +45,12 @@ FUNCTIONS = [
     ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.pack_mech"),
     ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.mech_fixed_mask"),
     ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.mech_fixed_values"),
+    ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.pfczm_damage_energy"),
+    ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.pfczm_damage_gradient"),
+    ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.pfczm_tangent_weights"),
+    ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.pfczm_tangent_action"),
+    ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.pfczm_tangent_diagonal"),
+    ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.pfczm_newton_system"),
     ("phast.solid3d.linalg", "pcg"),
     ("phast.solid3d.linalg", "solve_constrained"),
     ("phast.solvers.box_kkt_h8", "solve_h8_scalar_box_kkt"),

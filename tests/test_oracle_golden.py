@@ -230,3 +230,63 @@ def test_t3_at1_and_nodal_history_oracle():
     assert rel(act(g["x"]), g["nodal_Ax"]) < 1e-13
     d, it = solvers2d.projected_cg(act, bn, mn, g["d_prev"], g["d_prev"], 1e-10, 3000)
     assert rel(d, g["nodal_d_solve"]) < 1e-12 and it == int(g["nodal_iters"][0])
+
+
+def _pfczm_op(g, shape_key="shape", phase_key="phase", pinned_key="pinned", softening="linear"):
+    from oracle import pfczm
+    base = _h8_op({"phase": g[phase_key], "shape": g[shape_key], "h": g["h"], "pinned": g[pinned_key]})
+    E = float(g["E"])
+    return pfczm.PfczmOperator(base, [E, E * float(g["pore_ratio"])], [float(g["f_matrix"]), float(g["f_pore"])],
+                               softening=softening, p=2 if softening == "linear" else 2.5)
+
+
+@pytest.mark.parametrize("softening", ["linear", "exponential"])
+def test_pfczm_operators(softening):
+    """PF-CZM degradation, energy, gradient and Newton tangent against the reference."""
+    g = golden("pfczm")
+    op = _pfczm_op(g, softening=softening)
+    tag = softening[:3]
+    d, H, f = g[f"{tag}_d"], g[f"{tag}_H"], g[f"{tag}_f"]
+    assert np.allclose(op.a1, g[f"{tag}_a1"], rtol=1e-14, atol=0)
+    assert rel(op.degradation(d), g[f"{tag}_g"]) < 1e-13
+    assert abs(op.energy(d, H) - g[f"{tag}_energy"][0]) <= 1e-12 * abs(g[f"{tag}_energy"][0])
+    assert abs(op.energy(d, None) - g[f"{tag}_energy"][1]) <= 1e-12 * abs(g[f"{tag}_energy"][1])
+    assert abs(op.fracture_energy(d) - g[f"{tag}_frac"][0]) <= 1e-12 * abs(g[f"{tag}_frac"][0])
+    assert rel(op.gradient(d, H), g[f"{tag}_grad"]) < 1e-12
+    W = op.tangent_weights(d, H)
+    assert rel(W, g[f"{tag}_W"]) < 1e-12
+    assert rel(op.tangent_action(f, W), g[f"{tag}_Kf"]) < 1e-12
+    assert rel(op.tangent_diagonal(W), g[f"{tag}_Kdiag"]) < 1e-12
+    _, rhs, _, grad = op.newton_system(d, H)
+    assert rel(rhs, g[f"{tag}_rhs"]) < 1e-12 and rel(grad, g[f"{tag}_sgrad"]) < 1e-12
+
+
+def test_pfczm_newton_solve():
+    """One projected Newton damage solve: iterate, counts and the energy sequence."""
+    from oracle import pfczm
+    g = golden("pfczm")
+    op = _pfczm_op(g)
+    dn, pcg, sets, nw, energies = pfczm.damage_pfczm(op, h8.Cfg3D(), g["newton_H"], g["newton_lower"],
+                                                     g["newton_lower"])
+    assert [pcg, sets, nw] == [int(v) for v in g["newton_counts"]]
+    assert rel(dn, g["newton_d"]) < 1e-10
+    assert rel(np.array(energies), g["newton_energies"]) < 1e-12
+
+
+def test_pfczm_staggered_increments():
+    """Four staggered increments of the 6^3 pore cell with the PF-CZM law (two of them cracking)."""
+    from oracle import pfczm
+    g = golden("pfczm")
+    op = _pfczm_op(g, "st_shape", "st_phase", "st_pinned")
+    cfg = h8.Cfg3D()
+    x, d, H = np.zeros(op.base.n_mech), np.zeros(op.base.n_red), np.zeros((op.base.n_elements, 8))
+    prev = 0.0
+    for k, target in enumerate(g["st_targets"]):
+        x, d, H, stag, pm, pp, sets, nw, sig = pfczm.increment(op, cfg, x, d, H, prev, float(target))
+        prev = float(target)
+        assert stag == int(g["st_stag"][k]) and nw == int(g["st_newton"][k])
+        assert pm == int(g["st_pcg_mech"][k]) and pp == int(g["st_pcg_pf"][k]) and sets == int(g["st_sets"][k])
+        assert rel(sig, g["st_sigma"][k]) < 1e-9
+        assert rel(d, g["st_d"][k]) < 1e-8 if g["st_d"][k].any() else not d.any()
+        assert rel(x, g["st_x"][k]) < 1e-8
+        assert abs(op.fracture_energy(d) - g["st_frac"][k]) <= 1e-8 * max(abs(g["st_frac"][k]), 1e-300)
