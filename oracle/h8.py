@@ -473,12 +473,25 @@ def _damage_at2(op, cfg, H, lower, initial):
     return d_new, its
 
 
-def increment(op: VoxelOperator, cfg: Cfg3D, x, d, H_prev, previous, target, degradation=None, damage=None):
+def increment(op: VoxelOperator, cfg: Cfg3D, x, d, H_prev, previous, target, degradation=None, damage=None,
+              mechanics=None):
     """One _attempt: returns (x, d, H, stagger_iters, pcg_mech, pcg_pf, macro_stress).
 
     ``degradation(d)`` and ``damage(H, lower, initial) -> (d, pcg iterations)`` replace the
-    AT2 law when given (the PF-CZM law of ``pfczm.py``)."""
+    AT2 law when given (the PF-CZM law of ``pfczm.py``); ``mechanics(g, values, x0) ->
+    (x, pcg iterations)`` replaces the linear mechanics solve (the closure of ``closure.py``)."""
     degradation = op.degradation if degradation is None else degradation
+    mask = op.fixed_mask()
+
+    def _linear(g, values, x0):
+        xs, its, conv, _, _ = solve_constrained(lambda v: op.mech_action(v, g), op.mech_diagonal(g), mask, values,
+                                                x0=x0, rtol=cfg.pcg_rtol_mech, maxiter=cfg.pcg_maxit_mech,
+                                                check_every=cfg.check_every)
+        if not conv:
+            raise RuntimeError("mechanics PCG did not converge")
+        return xs, its
+
+    mechanics = _linear if mechanics is None else mechanics
     nu = 3 * op.n_red
     if previous != 0.0:
         x_old = x * (target / previous)
@@ -495,11 +508,7 @@ def increment(op: VoxelOperator, cfg: Cfg3D, x, d, H_prev, previous, target, deg
     H = H_prev
     for k in range(1, cfg.max_stagger + 1):
         g = degradation(d_old)
-        x_new, its, conv, _, _ = solve_constrained(lambda v: op.mech_action(v, g), op.mech_diagonal(g), mask, values,
-                                                   x0=x_old, rtol=cfg.pcg_rtol_mech, maxiter=cfg.pcg_maxit_mech,
-                                                   check_every=cfg.check_every)
-        if not conv:
-            raise RuntimeError("mechanics PCG did not converge")
+        x_new, its = mechanics(g, values, x_old)
         pm += its
         Y = op.driving_force(x_new)
         H = np.maximum(H_prev, Y)
@@ -522,8 +531,6 @@ def increment(op: VoxelOperator, cfg: Cfg3D, x, d, H_prev, previous, target, deg
     else:
         raise RuntimeError("stagger did not converge")
     g = degradation(d_old)
-    x_fin, its, conv, _, _ = solve_constrained(lambda v: op.mech_action(v, g), op.mech_diagonal(g), mask, values,
-                                               x0=x_old, rtol=cfg.pcg_rtol_mech, maxiter=cfg.pcg_maxit_mech,
-                                               check_every=cfg.check_every)
+    x_fin, its = mechanics(g, values, x_old)
     pm += its
     return x_fin, d_old, H, k, pm, pp, op.macro_stress(x_fin, g)

@@ -290,3 +290,46 @@ def test_pfczm_staggered_increments():
         assert rel(d, g["st_d"][k]) < 1e-8 if g["st_d"][k].any() else not d.any()
         assert rel(x, g["st_x"][k]) < 1e-8
         assert abs(op.fracture_energy(d) - g["st_frac"][k]) <= 1e-8 * max(abs(g["st_frac"][k]), 1e-300)
+
+
+def test_closure_operators():
+    """Crack closure (isotropic group): pattern, fixed- and own-pattern action, diagonal, energy,
+    stress, pattern change and the kinematic guard against the reference."""
+    from oracle import closure
+    g = golden("closure")
+    cl = closure.ClosureOperator(_h8_op(g))
+    x, x2, d = g["x"], g["x2"], g["d"]
+    gq = cl.base.degradation(d)
+    assert np.array_equal(cl.pattern(x), g["pattern"]) and np.array_equal(cl.pattern(x2), g["pattern2"])
+    assert rel(cl.mech_action(x, gq, g["pattern2"]), g["act_fixed"]) < 1e-12
+    assert rel(cl.mech_action(x, gq), g["act_own"]) < 1e-12
+    assert rel(cl.mech_diagonal(gq, g["pattern2"]), g["diag_fixed"]) < 1e-12
+    assert rel(cl.mech_diagonal(gq), g["diag_all"]) < 1e-12
+    assert abs(cl.elastic_energy(x, gq) - float(g["energy"][0])) <= 1e-12 * abs(float(g["energy"][0]))
+    assert rel(cl.macro_stress(x, gq), g["sigma"]) < 1e-12
+    new, changed = cl.pattern_change(x, g["pattern2"], gq)
+    assert np.array_equal(new, g["change_pattern"]) and changed == bool(g["changed"][0])
+    assert cl.pattern_change(x, g["pattern"], gq)[1] == bool(g["unchanged"][0])
+    assert rel(np.array(cl.kinematic_guard(x)), g["guard"]) < 1e-12
+
+
+def test_closure_staggered_increments():
+    """Four staggered increments of the 6^3 pore cell with the crack closure (AT2)."""
+    from oracle import closure
+    g = golden("closure")
+    op = _h8_op({"phase": g["st_phase"], "shape": g["st_shape"], "h": g["h"], "pinned": g["st_pinned"]})
+    cl = closure.ClosureOperator(op)
+    cfg = h8.Cfg3D()
+    x, d, H = np.zeros(op.n_mech), np.zeros(op.n_red), np.zeros((op.n_elements, 8))
+    prev = 0.0
+    for k, target in enumerate(g["st_targets"]):
+        x, d, H, stag, pm, pp, solves, sig, guard = closure.increment(cl, cfg, x, d, H, prev, float(target))
+        prev = float(target)
+        assert (stag, solves) == (int(g["st_stag"][k]), int(g["st_closure_solves"][k])), k
+        # the mechanics solves stop at PhAST's relative residual 1e-8: the summation order moves a
+        # stopping point by an iteration, and on the nearly broken cell of increment 4 (max d 0.98)
+        # the soft modes carry the solve tolerance into x
+        assert abs(pm - int(g["st_pcg_mech"][k])) <= 2 and pp == int(g["st_pcg_pf"][k]), k
+        assert rel(sig, g["st_sigma"][k]) < 1e-8
+        assert rel(d, g["st_d"][k]) < 1e-6 and rel(x, g["st_x"][k]) < (1e-8 if k < 3 else 1e-5)
+        assert rel(np.array(guard), g["st_guard"][k]) < 1e-6
