@@ -559,6 +559,60 @@ int phastb_h8_increment_record_ex(const phastb_voxel_grid* g, const phastb_voxel
                                   const double* H, double threshold, const phastb_pfczm_law* law,
                                   double* out_host, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- crack closure (SolverConfig.crack_closure = 'axes'), isotropic group ----
+ * Elements with a damage driver add back (1 - g) of psi_c = sum_k k_k/2 <v_k . eps>-^2 with
+ * the rows v = (trace, e_x, e_y, e_z) and moduli (lam, 2 mu, 2 mu, 2 mu) of their slot
+ * (splits.py:486-503).  A sign pattern is one byte per Gauss point, (E,8): bit k set where
+ * v_k . eps < 0 (ClosurePattern.iso, model.py:1200-1223); a fixed pattern makes the
+ * add-back linear.  Workspace of the calls below: phastb_h8_closure_workspace_bytes. */
+size_t phastb_h8_closure_workspace_bytes(const phastb_voxel_grid* g);
+
+/* pattern (E,8) of state x.  closure_pattern, operator.py:821-834 */
+int phastb_h8_closure_pattern(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                              const double* x, uint8_t* pattern, void* stream);
+
+/* New pattern of x and *changed_host = whether a flipped bit's stress jump (1 - g) k |v . eps|
+ * exceeds tolerance x the largest k |v . eps|.  closure_pattern_change, operator.py:836-873 */
+int phastb_h8_closure_pattern_change(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                                     const uint8_t* slot, const double* x, const double* gq,
+                                     const uint8_t* pattern_old, double tolerance, uint8_t* pattern_new,
+                                     int* changed_host, void* workspace, size_t workspace_bytes, void* stream);
+
+/* y += the add-back's internal force at x (pattern NULL: each point's own signs); rows with
+ * mask set are left alone.  The closure terms of _stress_pass_closure, operator.py:1039-1108 */
+int phastb_h8_closure_apply_add(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                                const double* x, const double* gq, const uint8_t* pattern, const uint8_t* mask,
+                                double* y, void* workspace, size_t workspace_bytes, void* stream);
+
+/* diag += the add-back's Jacobi-diagonal terms (pattern NULL: every bit).  _closure_diagonal,
+ * operator.py:1274-1302 */
+int phastb_h8_closure_diagonal_add(const phastb_voxel_grid* g, const phastb_voxel_material* m,
+                                   const uint8_t* slot, const double* gq, const uint8_t* pattern, double* diag,
+                                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* out_host[0] = the add-back's energy sum w (1 - g) psi_c, [1..3] its r_E rows xx, yy, zz
+ * (pattern NULL: each point's own signs), to add to phastb_h8_stress_energy.
+ * operator.py:1039-1108 */
+int phastb_h8_closure_energy(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                             const double* x, const double* gq, const uint8_t* pattern, double* out_host,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/* out_host = [smallest element-mean normal strain, smallest principal value of the element-mean
+ * strains, smallest Gauss-point det(I + grad u)].  kinematic_guard, operator.py:1713-1770;
+ * workspace phastb_reduce_workspace_bytes. */
+int phastb_h8_kinematic_guard(const phastb_voxel_grid* g, const double* x, double* out_host, void* workspace,
+                              size_t workspace_bytes, void* stream);
+
+/* The constrained mechanics solve of phastb_h8_mech_solve with the closure add-back of a fixed
+ * pattern in the operator and in its Jacobi diagonal (the linear solve of each closure pattern
+ * iteration, StaggeredSolver._linear_mechanics, staggered.py:550-587). */
+size_t phastb_h8_mech_solve_closure_workspace_bytes(const phastb_voxel_grid* g);
+int phastb_h8_mech_solve_closure(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                                 const double* gq, const uint8_t* pattern, const uint8_t* fixed,
+                                 const double* fixed_values, const double* x0, double rtol, double atol,
+                                 int maxiter, int check_every, double* x_out, int* info, double* rinfo,
+                                 void* workspace, size_t workspace_bytes, void* stream);
+
 /* Staggered change parts out[0..4] = ||du~||, ||u~||, max|dE|, max|E|, max|dd| (FP64, host).
  * StaggeredSolver._change, solid3d/staggered.py:1097-1124 */
 int phastb_h8_stagger_change(int n_u, const double* x_new, const double* x_old, int n_d,

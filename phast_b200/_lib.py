@@ -146,6 +146,16 @@ SIGNATURES = {
     "phastb_h8_record_workspace_bytes": (sz, [VG]),
     "phastb_h8_increment_record": (C.c_int, [VG, VM, vp, vp, vp, vp, C.c_double, dp, vp, sz, vp]),
     "phastb_h8_increment_record_ex": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, C.c_double, PL, dp, vp, sz, vp]),
+    "phastb_h8_closure_workspace_bytes": (sz, [VG]),
+    "phastb_h8_closure_pattern": (C.c_int, [VG, VM, vp, vp, vp, vp]),
+    "phastb_h8_closure_pattern_change": (C.c_int, [VG, VM, vp, vp, vp, vp, C.c_double, vp, ip, vp, sz, vp]),
+    "phastb_h8_closure_apply_add": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
+    "phastb_h8_closure_diagonal_add": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, sz, vp]),
+    "phastb_h8_closure_energy": (C.c_int, [VG, VM, vp, vp, vp, vp, dp, vp, sz, vp]),
+    "phastb_h8_kinematic_guard": (C.c_int, [VG, vp, dp, vp, sz, vp]),
+    "phastb_h8_mech_solve_closure_workspace_bytes": (sz, [VG]),
+    "phastb_h8_mech_solve_closure": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int,
+                                               C.c_int, vp, ip, dp, vp, sz, vp]),
     "phastb_h8_pfczm_degradation": (C.c_int, [VG, VM, PL, vp, vp, vp, vp]),
     "phastb_h8_pfczm_workspace_bytes": (sz, [VG]),
     "phastb_h8_pfczm_energy": (C.c_int, [VG, VM, PL, vp, vp, vp, dp, vp, sz, vp]),

@@ -101,6 +101,30 @@ VoxMat<U> vox_mat_cast(const VoxMat<T>& a) {
   return r;
 }
 
+// Ascending eigenvalues of a symmetric 3x3 tensor by the trigonometric
+// solution of the characteristic cubic (Smith 1961), as symmetric_eigvalsh_3x3
+// (solid3d/splits.py:93-125).
+__device__ __forceinline__ void eig3(double a11, double a22, double a33, double a12, double a13, double a23,
+                                     double* ev) {
+  const double q = (a11 + a22 + a33) / 3.0;
+  const double b11 = a11 - q, b22 = a22 - q, b33 = a33 - q;
+  const double p1 = a12 * a12 + a13 * a13 + a23 * a23;
+  const double p = sqrt((b11 * b11 + b22 * b22 + b33 * b33 + 2.0 * p1) / 6.0);
+  if (!(p > 2.2250738585072014e-308)) {
+    ev[0] = ev[1] = ev[2] = q;
+    return;
+  }
+  const double det = b11 * (b22 * b33 - a23 * a23) - a12 * (a12 * b33 - a23 * a13) + a13 * (a12 * a23 - b22 * a13);
+  double r = det / (2.0 * p * p * p);
+  r = fmin(fmax(r, -1.0), 1.0);
+  const double phi = acos(r) / 3.0;
+  const double big = q + 2.0 * p * cos(phi);
+  const double small = q + 2.0 * p * cos(phi + 2.0943951023931954923);  // 2 pi / 3
+  ev[0] = small;
+  ev[1] = 3.0 * q - big - small;
+  ev[2] = big;
+}
+
 __device__ __forceinline__ int wrap(int i, int n, int periodic) { return periodic ? (i >= n ? i - n : i) : i; }
 
 // Reduced node ids of the 8 corners of element (ie, je, ke), lexicographic.

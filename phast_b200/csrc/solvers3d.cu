@@ -26,6 +26,14 @@ int h8_damage_launch(const VoxGeom& v, const VoxMat<double>& mm, const uint8_t* 
                      const double* H, double scale, double* y, const uint8_t* mask, void* scratch,
                      const int* guard, cudaStream_t s);
 
+int closure_add_launch(const VoxGeom& v, const VoxMat<double>& m, const uint8_t* slot, const double* x,
+                       const double* gq, const uint8_t* pattern, const uint8_t* mask, double* y, void* sc,
+                       cudaStream_t s);
+int closure_diag_launch(const VoxGeom& v, const VoxMat<double>& m, const uint8_t* slot, const double* gq,
+                        const uint8_t* pattern, double* diag, void* sc, cudaStream_t s);
+int closure_reset(void* sc, const VoxGeom& v, cudaStream_t s);
+size_t closure_scratch_bytes(const VoxGeom& v);
+
 struct MechCtx {
   VoxGeom v;
   VoxMat<double> m;
@@ -34,11 +42,17 @@ struct MechCtx {
   const double* d;
   const uint8_t* mask;
   void* scratch;
+  // crack closure with a fixed sign pattern (closure != 0): the add-back joins the action
+  const uint8_t* pattern;
+  void* clsc;
+  long long closure;  // 64-bit: no tail padding in the bytes that key a captured graph
 };
 
 static int mech_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
   const MechCtx* k = static_cast<const MechCtx*>(c);
-  return h8_mech_apply_t<double>(k->v, k->m, k->slot, x, k->gq, k->d, k->mask, y, k->scratch, guard, s);
+  int st = h8_mech_apply_t<double>(k->v, k->m, k->slot, x, k->gq, k->d, k->mask, y, k->scratch, guard, s);
+  if (st || !k->closure) return st;
+  return closure_add_launch(k->v, k->m, k->slot, x, k->gq, k->pattern, k->mask, y, k->clsc, s);
 }
 
 static int mech_op_dot(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
@@ -294,15 +308,14 @@ size_t phastb_h8_mech_solve_workspace_bytes(const phastb_voxel_grid* g, int dtyp
          align_up(sizeof(double) * 8 * (size_t)v.n_elem);
 }
 
-int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
-                         const double* gq, const double* d, const uint8_t* fixed, const double* fixed_values,
-                         const double* x0, double rtol, double atol, int maxiter, int check_every, double* x_out,
-                         int* info, double* rinfo, void* workspace, size_t workspace_bytes, void* stream) {
-  if (!valid_vox(g) || !valid_mat(m) || !slot || !fixed || !fixed_values || !x_out || maxiter < 1 ||
-      check_every < 1 || !(rtol >= 0) || !(atol >= 0) || (rtol == 0 && atol == 0))
-    return PHASTB_ERR_ARG;
-  if (!workspace || workspace_bytes < phastb_h8_mech_solve_workspace_bytes(g, PHASTB_F64))
-    return PHASTB_ERR_WORKSPACE;
+// The constrained Jacobi PCG of phastb_h8_mech_solve; with closure != 0 the operator and its
+// diagonal carry the crack-closure add-back of the sign pattern (copied into cl_ws, which
+// holds closure_scratch_bytes + 8 E bytes).
+static int mech_solve_impl(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                           const double* gq, const double* d, const uint8_t* pattern, int closure, void* cl_ws,
+                           const uint8_t* fixed, const double* fixed_values, const double* x0, double rtol,
+                           double atol, int maxiter, int check_every, double* x_out, int* info, double* rinfo,
+                           void* workspace, void* stream) {
   ScopedStream scope((cudaStream_t)stream);
   if (scope.status()) return scope.status();
   cudaStream_t s = scope.get();
@@ -337,10 +350,21 @@ int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material
     return st;
   d = d ? dw : nullptr;
   gq = gq ? gw : nullptr;
+  const uint8_t* patw = nullptr;
+  if (closure) {
+    if ((st = closure_reset(cl_ws, v, s))) return st;
+    if (pattern) {
+      uint8_t* pw = static_cast<uint8_t*>(cl_ws) + closure_scratch_bytes(v);
+      if ((st = cuda_status(cudaMemcpyAsync(pw, pattern, 8 * (size_t)v.n_elem, cudaMemcpyDeviceToDevice, s))))
+        return st;
+      patw = pw;
+    }
+  }
   // diagonal of A(g) into invd, then the constrained setup
   if ((st = h8_mech_diag_t<double>(v, mm, slot, gq, d, invd, scratch, s))) return st;
+  if (closure && (st = closure_diag_launch(v, mm, slot, gq, patw, invd, cl_ws, s))) return st;
   { note_launch(); constrained_setup_kernel<<<G, kThreads, 0, s>>>(n, fixed, fixed_values, x0, xc, x_out, invd); }
-  MechCtx full{v, mm, slot, gq, d, nullptr, scratch};
+  MechCtx full{v, mm, slot, gq, d, nullptr, scratch, patw, cl_ws, closure};
   if ((st = mech_op(&full, xc, w.Ap, nullptr, s))) return st;
   { note_launch(); constrained_rhs_kernel<<<G, kThreads, 0, s>>>(n, fixed, nullptr, w.Ap, bf, rw); }
   if ((st = last_launch_status())) return st;
@@ -356,8 +380,9 @@ int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material
     return last_launch_status();
   }
   const double thr = std::max(rtol * bn, atol);
-  MechCtx free_ctx{v, mm, slot, gq, d, fixed, scratch};
-  LinOp<double> A{mech_op, &free_ctx, sizeof(free_ctx), mech_op_dot, h8_apply_dot_slot(v, 8, scratch)};
+  MechCtx free_ctx{v, mm, slot, gq, d, fixed, scratch, patw, cl_ws, closure};
+  LinOp<double> A{mech_op, &free_ctx, sizeof(free_ctx), closure ? nullptr : mech_op_dot,
+                  closure ? nullptr : h8_apply_dot_slot(v, 8, scratch)};
   PcgResult pr{};
   if ((st = cuda_status(cudaMemcpyAsync(xw, x_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, s)))) return st;
   if ((st = pcg_run<double>(A, n, w, bf, invd, nullptr, xw, thr, maxiter, check_every, PCG_FREEZE, 0.0, &pr, s)))
@@ -369,6 +394,40 @@ int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material
   if (pr.nonfinite) return PHASTB_NONFINITE;
   if (pr.breakdown) return PHASTB_BREAKDOWN;
   return pr.converged ? PHASTB_OK : PHASTB_NONCONVERGED;
+}
+
+int phastb_h8_mech_solve(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                         const double* gq, const double* d, const uint8_t* fixed, const double* fixed_values,
+                         const double* x0, double rtol, double atol, int maxiter, int check_every, double* x_out,
+                         int* info, double* rinfo, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !fixed || !fixed_values || !x_out || maxiter < 1 ||
+      check_every < 1 || !(rtol >= 0) || !(atol >= 0) || (rtol == 0 && atol == 0))
+    return PHASTB_ERR_ARG;
+  if (!workspace || workspace_bytes < phastb_h8_mech_solve_workspace_bytes(g, PHASTB_F64))
+    return PHASTB_ERR_WORKSPACE;
+  return mech_solve_impl(g, m, slot, gq, d, nullptr, 0, nullptr, fixed, fixed_values, x0, rtol, atol, maxiter,
+                         check_every, x_out, info, rinfo, workspace, stream);
+}
+
+size_t phastb_h8_mech_solve_closure_workspace_bytes(const phastb_voxel_grid* g) {
+  if (!valid_vox(g)) return 0;
+  const VoxGeom v = make_vox_geom(*g);
+  return phastb_h8_mech_solve_workspace_bytes(g, PHASTB_F64) + closure_scratch_bytes(v) +
+         align_up(8 * (size_t)v.n_elem);
+}
+
+int phastb_h8_mech_solve_closure(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                                 const double* gq, const uint8_t* pattern, const uint8_t* fixed,
+                                 const double* fixed_values, const double* x0, double rtol, double atol,
+                                 int maxiter, int check_every, double* x_out, int* info, double* rinfo,
+                                 void* workspace, size_t workspace_bytes, void* stream) {
+  if (!valid_vox(g) || !valid_mat(m) || !slot || !gq || !pattern || !fixed || !fixed_values || !x_out ||
+      maxiter < 1 || check_every < 1 || !(rtol >= 0) || !(atol >= 0) || (rtol == 0 && atol == 0))
+    return PHASTB_ERR_ARG;
+  if (!workspace || workspace_bytes < phastb_h8_mech_solve_closure_workspace_bytes(g)) return PHASTB_ERR_WORKSPACE;
+  void* cl_ws = static_cast<char*>(workspace) + phastb_h8_mech_solve_workspace_bytes(g, PHASTB_F64);
+  return mech_solve_impl(g, m, slot, gq, nullptr, pattern, 1, cl_ws, fixed, fixed_values, x0, rtol, atol, maxiter,
+                         check_every, x_out, info, rinfo, workspace, stream);
 }
 
 size_t phastb_h8_box_kkt_workspace_bytes(const phastb_voxel_grid* g) {

@@ -5,9 +5,9 @@ and ``build_element_arrays`` (src/phast/solid3d/materials.py:474-547) with the s
 names, fields, defaults and validation errors, so a caller written against the
 reference builds the same objects here.  Objects of the reference package with
 the same fields are accepted wherever these are (the operator reads attributes
-only).  Options of the reference that this backend does not run (crack closure,
-Anderson mixing, smeared-laminate phases, the interface driver, ``history_only``
-irreversibility) are accepted by the data classes and refused
+only).  Options of the reference that this backend does not run (Anderson mixing,
+smeared-laminate phases with their band closure, the interface driver,
+``history_only`` irreversibility) are accepted by the data classes and refused
 with ``NotImplementedError`` when an operator or solver is built from them.
 """
 from __future__ import annotations
@@ -319,7 +319,7 @@ class SolverConfig:
 
     The GPU backend runs ``dtype='float64'`` results (the chosen mechanics form may compute
     in FP32 under FP64 refinement; see ``StaggeredSolver(form=...)``), ``damage_law`` 'at2' or 'pfczm',
-    ``irreversibility='box_kkt'``, ``history`` 'max' or 'current', ``crack_closure='none'`` and
+    ``irreversibility='box_kkt'``, ``history`` 'max' or 'current', ``crack_closure`` 'none' or 'axes' and
     ``anderson_depth=0``; ``device`` names the CUDA device.
     """
     device: str = "cuda"
@@ -393,8 +393,6 @@ class SolverConfig:
 def unsupported_options(cfg):
     """Names of ``cfg`` settings this backend does not run (empty when it runs them all)."""
     out = []
-    if getattr(cfg, "crack_closure", "none") != "none":
-        out.append(f"crack_closure={cfg.crack_closure!r}")
     if getattr(cfg, "anderson_depth", 0) != 0:
         out.append(f"anderson_depth={cfg.anderson_depth!r}")
     if getattr(cfg, "irreversibility", "box_kkt") != "box_kkt":
@@ -519,3 +517,28 @@ def sphere_pore_phase(shape, radius_fraction, matrix_id=PHASE_ID["mi_matrix"], p
     phase = np.full((nz, ny, nx), matrix_id, dtype=np.uint8)
     phase[np.linalg.norm(c, axis=-1) < radius_fraction] = pore_id
     return phase
+
+
+@dataclass
+class ClosurePattern:
+    """Sign pattern of the crack-closure terms at every quadrature point (model.py:1200-1223).
+
+    ``iso`` ``(E, 8, 4)`` bool holds the bits ``[tr eps < 0], [eps_xx < 0], [eps_yy < 0],
+    [eps_zz < 0]`` of the isotropic closure (False outside the group); ``band`` is the
+    smeared-laminate group, ``None`` here (laminate phases are not run by this backend).  For a
+    fixed pattern the closure stress is linear in the strain.
+    """
+    iso: torch.Tensor | None = None
+    band: torch.Tensor | None = None
+
+    def groups(self):
+        return (self.iso, self.band)
+
+    def equals(self, other):
+        """Whether both patterns hold the same bits in every group."""
+        for mine, theirs in zip(self.groups(), other.groups()):
+            if (mine is None) != (theirs is None):
+                return False
+            if mine is not None and not torch.equal(mine, theirs):
+                return False
+        return True

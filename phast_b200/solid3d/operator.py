@@ -76,6 +76,8 @@ class PeriodicVoxelPhaseFieldOperator:
                     cfg.energy_split_isotropic, pinned_node, materials.stiffness_index.device)
         if getattr(cfg, "damage_law", "at2") == "pfczm":
             self._build_pfczm(cfg, pfczm_strengths)
+        if getattr(cfg, "crack_closure", "none") == "axes":
+            self._build_closure()
 
     @classmethod
     def from_slots(cls, grid, slot, phases, ell, kappa, load, *, split_isotropic="spectral", pinned_node=None,
@@ -151,6 +153,9 @@ class PeriodicVoxelPhaseFieldOperator:
         self._resid = _lib.Workspace(self.device)
         self._pf = None
         self._pfws = _lib.Workspace(self.device)
+        self._closure = False
+        self._clws = _lib.Workspace(self.device)
+        self._kgws = _lib.Workspace(self.device)
         self.pfczm_bound = None
         self.pfczm_phases = {}
         self.pfczm_strengths = {}
@@ -304,20 +309,27 @@ class PeriodicVoxelPhaseFieldOperator:
         return g
 
     def _law_g(self, g, d, dtype):
-        """``(g, d)`` for the kernels: the PF-CZM law cannot be fused from ``d``, so it becomes ``g``."""
-        if self._pf is not None and g is None and d is not None:
+        """``(g, d)`` for the kernels: the PF-CZM law and the closure add-back need ``g`` itself."""
+        if (self._pf is not None or self._closure) and g is None and d is not None:
             return self.degradation(d).to(dtype), None
         return g, d
 
-    @staticmethod
-    def _no_closure(opening=None, closure=None):
-        if opening is not None or closure is not None:
-            raise NotImplementedError("interface opening and crack closure are not supported by the GPU backend")
+    def _no_closure(self, opening=None, closure=None):
+        """The packed (E, 8) sign pattern of ``closure`` (None: each point's own signs)."""
+        if opening is not None:
+            raise NotImplementedError("interface opening patterns are not supported by the GPU backend")
+        if closure is None:
+            return None
+        if not self._closure:
+            raise ValueError("closure applies with crack_closure 'axes' only; this operator has none")
+        return self._packed(closure)
 
     def mech_action(self, x, g=None, *, opening=None, closure=None, d=None, mask=None, out=None):
         """A(g) x (operator.py:1171-1194); ``g=None`` means undamaged.  ``d`` instead of ``g`` fuses
-        the degradation into the action; ``mask`` zeroes rows; ``out`` receives the result."""
-        self._no_closure(opening, closure)
+        the degradation into the action; ``mask`` zeroes rows; ``out`` receives the result.  With the
+        crack closure the (1 - g) add-back of ``closure``'s pattern joins (each point's own signs when
+        ``closure`` is None)."""
+        pattern = self._no_closure(opening, closure)
         x = self._check("x", x, (self.n_mech,))
         g, d = self._law_g(g, d, x.dtype)
         gq = None if g is None else self._check("g", g, (self.n_elements, 8), x.dtype)
@@ -331,6 +343,11 @@ class PeriodicVoxelPhaseFieldOperator:
                 raise ValueError("out must be a distinct contiguous tensor like x")
         call("phastb_h8_mech_apply", self.vgrid, self.mat, ptr(self.slot), self._dt(x), ptr(x), ptr(gq), ptr(dd),
              ptr(mk), ptr(y), self.scratch(x.dtype), stream())
+        if self._closure and gq is not None:
+            self._fp64_closure(x)
+            wp, wn = self._cl_ws()
+            call("phastb_h8_closure_apply_add", self.vgrid, self.mat, ptr(self.slot), ptr(x), ptr(gq), ptr(pattern),
+                 ptr(mk), ptr(y), wp, wn, stream())
         return y
 
     def mech_operator(self, g=None, *, d=None):
@@ -362,8 +379,9 @@ class PeriodicVoxelPhaseFieldOperator:
         return tuple(shape), float(ms.value)
 
     def mech_diagonal(self, g=None, *, opening=None, closure=None, d=None):
-        """Jacobi diagonal of A(g) (operator.py:1196-1254)."""
-        self._no_closure(opening, closure)
+        """Jacobi diagonal of A(g) (operator.py:1196-1302); with the crack closure the add-back's terms
+        of ``closure``'s bits (every bit when None)."""
+        pattern = self._no_closure(opening, closure)
         dtype = g.dtype if g is not None else (d.dtype if d is not None else torch.float64)
         g, d = self._law_g(g, d, dtype)
         gq = None if g is None else self._check("g", g, (self.n_elements, 8), dtype)
@@ -371,9 +389,14 @@ class PeriodicVoxelPhaseFieldOperator:
         y = torch.empty(self.n_mech, dtype=dtype, device=self.device)
         call("phastb_h8_mech_diagonal", self.vgrid, self.mat, ptr(self.slot), self._dt(y), ptr(gq), ptr(dd), ptr(y),
              self.scratch(dtype), stream())
+        if self._closure and gq is not None:
+            self._fp64_closure(y)
+            wp, wn = self._cl_ws()
+            call("phastb_h8_closure_diagonal_add", self.vgrid, self.mat, ptr(self.slot), ptr(gq), ptr(pattern), ptr(y),
+                 wp, wn, stream())
         return y
 
-    def _stress_energy(self, x, g=None, d=None):
+    def _stress_energy(self, x, g=None, d=None, pattern=None):
         x = self._check("x", x, (self.n_mech,), torch.float64)
         g, d = self._law_g(g, d, torch.float64)
         gq = None if g is None else self._check("g", g, (self.n_elements, 8), torch.float64)
@@ -382,18 +405,30 @@ class PeriodicVoxelPhaseFieldOperator:
         en = C.c_double(0.0)
         call("phastb_h8_stress_energy", self.vgrid, self.mat, ptr(self.slot), ptr(x), ptr(gq), ptr(dd), rE,
              C.byref(en), self.scratch(torch.float64), stream())
-        return np.array(list(rE)), float(en.value)
+        rE, en = np.array(list(rE)), float(en.value)
+        if self._closure and gq is not None:
+            out = self._closure_energy(x, gq, pattern)
+            rE[:3] += out[1:4]
+            en += out[0]
+        return rE, en
+
+    def _closure_energy(self, x, gq, pattern=None):
+        out = (C.c_double * 4)()
+        wp, wn = self._cl_ws()
+        call("phastb_h8_closure_energy", self.vgrid, self.mat, ptr(self.slot), ptr(x), ptr(gq), ptr(pattern), out,
+             wp, wn, stream())
+        return np.array(list(out))
 
     def macro_stress(self, x, g=None, *, opening=None, closure=None, d=None):
         """Sigma = r_E / V (operator.py:1303-1316)."""
-        self._no_closure(opening, closure)
-        rE, _ = self._stress_energy(x, g, d)
+        pattern = self._no_closure(opening, closure)
+        rE, _ = self._stress_energy(x, g, d, pattern)
         return torch.as_tensor(rE / self.volume, dtype=torch.float64, device=self.device)
 
     def elastic_energy(self, x, g=None, *, opening=None, closure=None, d=None):
         """0.5 x . A(g) x in mJ, a 0-dim tensor (operator.py:1318-1340)."""
-        self._no_closure(opening, closure)
-        _, en = self._stress_energy(x, g, d)
+        pattern = self._no_closure(opening, closure)
+        _, en = self._stress_energy(x, g, d, pattern)
         return torch.tensor(en, dtype=torch.float64, device=self.device)
 
     def mean_strain(self, x):
@@ -405,13 +440,103 @@ class PeriodicVoxelPhaseFieldOperator:
 
     def hill_mandel(self, x, g=None, *, closure=None):
         """``mean_work = 2 E_el / V``, ``macro_work = Sigma . E`` and their relative gap (operator.py:1390-1413)."""
-        self._no_closure(None, closure)
-        rE, en = self._stress_energy(x, g)
+        pattern = self._no_closure(None, closure)
+        rE, en = self._stress_energy(x, g, None, pattern)
         E = self.split_mech(x)[1].detach().cpu().numpy()
         mean = 2.0 * en / self.volume
         macro = float(np.dot(rE / self.volume, E))
         scale = max(abs(mean), abs(macro))
         return {"mean_work": mean, "macro_work": macro, "relative": abs(mean - macro) / scale if scale > 0 else 0.0}
+
+    # -- crack closure ('axes', isotropic group) ---------------------------------------------
+    def _build_closure(self):
+        """The isotropic closure group (operator.py:673-727): every element with a damage driver, rows
+        (trace, e_x, e_y, e_z), moduli (lam, 2 mu, 2 mu, 2 mu) of its slot."""
+        for s, ph in enumerate(self.phases):
+            if int(self.mat.driver[s]) != _lib.DRIVER_NONE and self._lam[s] < 0.0:
+                raise ValueError("crack_closure 'axes' needs lam >= 0 in every isotropic phase")
+        self._closure = True
+
+    @property
+    def has_closure(self):
+        """Whether the crack closure is on (``crack_closure != 'none'``)."""
+        return self._closure
+
+    @property
+    def n_closure_band(self):
+        """Number of smeared-laminate band elements with the band closure (none here)."""
+        return 0
+
+    def _cl_ws(self):
+        return self._clws.get(_lib.load().phastb_h8_closure_workspace_bytes(self.vgrid))
+
+    @staticmethod
+    def _fp64_closure(t):
+        if t.dtype != torch.float64:
+            raise NotImplementedError("the crack closure runs in FP64")
+
+    def _packed(self, closure):
+        """(E, 8) uint8 bits of a ClosurePattern (bit k: row k active)."""
+        packed = getattr(closure, "_packed", None)
+        if packed is not None:
+            return packed
+        iso = getattr(closure, "iso", None)
+        if getattr(closure, "band", None) is not None:
+            raise ValueError("closure.band must be None: the model has no band closure group")
+        if not isinstance(iso, torch.Tensor) or iso.dtype != torch.bool:
+            raise TypeError("closure.iso must be a torch.bool tensor")
+        if tuple(iso.shape) != (self.n_elements, 8, 4) or iso.device != self.device:
+            raise ValueError(f"closure.iso must have shape {(self.n_elements, 8, 4)} on {self.device}")
+        weights = torch.tensor([1, 2, 4, 8], dtype=torch.uint8, device=self.device)
+        return (iso.to(torch.uint8) * weights).sum(-1).to(torch.uint8).contiguous()
+
+    def _pattern_object(self, packed):
+        from .model import ClosurePattern
+        bits = torch.tensor([1, 2, 4, 8], dtype=torch.uint8, device=self.device)
+        out = ClosurePattern(iso=(packed.unsqueeze(-1) & bits) != 0, band=None)
+        out._packed = packed
+        return out
+
+    def _closure_pattern_packed(self, x):
+        x = self._check("x", x, (self.n_mech,), torch.float64)
+        out = torch.empty(self.n_elements, 8, dtype=torch.uint8, device=self.device)
+        call("phastb_h8_closure_pattern", self.vgrid, self.mat, ptr(self.slot), ptr(x), ptr(out), stream())
+        return out
+
+    def _closure_change_packed(self, x, old, g, tolerance):
+        x = self._check("x", x, (self.n_mech,), torch.float64)
+        g = self._check("g", g, (self.n_elements, 8), torch.float64)
+        new = torch.empty_like(old)
+        changed = (C.c_int * 1)()
+        wp, wn = self._cl_ws()
+        call("phastb_h8_closure_pattern_change", self.vgrid, self.mat, ptr(self.slot), ptr(x), ptr(g), ptr(old),
+             float(tolerance), ptr(new), changed, wp, wn, stream())
+        return new, bool(changed[0])
+
+    def closure_pattern(self, x):
+        """Sign pattern ``v . eps < 0`` of every closure term at state ``x`` (operator.py:821-834)."""
+        if not self._closure:
+            raise ValueError("closure_pattern needs crack_closure 'axes'")
+        return self._pattern_object(self._closure_pattern_packed(x))
+
+    def closure_pattern_change(self, x, pattern, g, *, tolerance=1.0e-8):
+        """New closure pattern of state ``x`` and whether it changed materially (operator.py:836-873):
+        a flipped bit counts where its stress jump ``(1 - g) k |v . eps|`` exceeds ``tolerance`` times
+        the largest ``k |v . eps|``."""
+        old = self._no_closure(None, pattern)
+        if old is None:
+            raise ValueError("closure_pattern_change needs a pattern")
+        new, changed = self._closure_change_packed(x, old, g, tolerance)
+        return self._pattern_object(new), changed
+
+    def kinematic_guard(self, x, d):
+        """Smallest element-mean normal strain, principal strain of the element-mean strain and
+        Gauss-point ``det(I + grad u)`` of state ``x`` (operator.py:1713-1770)."""
+        x = self._check("x", x, (self.n_mech,), torch.float64)
+        out = (C.c_double * 3)()
+        wp, wn = self._kgws.get(_lib.load().phastb_reduce_workspace_bytes())
+        call("phastb_h8_kinematic_guard", self.vgrid, ptr(x), out, wp, wn, stream())
+        return {"min_normal_strain": float(out[0]), "min_principal_strain": float(out[1]), "min_det_F": float(out[2])}
 
     def driving_force(self, x):
         """Undamaged driving energy Y (E, 8) (operator.py:1415-1444)."""
@@ -479,6 +604,11 @@ class PeriodicVoxelPhaseFieldOperator:
             call("phastb_h8_increment_record", self.vgrid, self.mat, ptr(self.slot), ptr(xx), ptr(d), ptr(Hq),
                  float(threshold), out, wp, wn, stream())
         v = list(out)
+        if self._closure and xx is not None:
+            # the closure add-back at each point's own signs joins r_E and the elastic energy
+            extra = self._closure_energy(xx, self.degradation(d))
+            v[6:9] = [a + b for a, b in zip(v[6:9], extra[1:4])]
+            v[12] += extra[0]
         S = _lib.MAX_SLOTS
         return {"E": np.array(v[0:6]), "rE": np.array(v[6:12]), "energy": v[12],
                 "by_phase": {p.name: v[13 + s] for s, p in enumerate(self.phases)},

@@ -485,6 +485,11 @@ class _AttemptFailure(Exception):
 
 _TINY = 1.0e-300
 _MIN_LINEAR_TOLERANCE = 4.0 * float(np.finfo(np.float64).eps)
+_CLOSURE_MAX_SOLVES = 50            # INTERFACE_MAX_SOLVES, staggered.py:99
+_CLOSURE_PATTERN_TOLERANCE = 1.0e-8  # staggered.py:105
+_LS_ARMIJO = 1.0e-4                 # LINE_SEARCH_ARMIJO, staggered.py:109
+_LS_ENERGY_RTOL = 1.0e-12           # staggered.py:112
+_LS_MAX_HALVINGS = 30               # staggered.py:115
 
 
 class StaggeredSolver:
@@ -515,6 +520,8 @@ class StaggeredSolver:
             raise NotImplementedError(f"the B200 backend does not run {', '.join(bad)}")
         if op.is_pfczm and (form.precond != "jacobi" or form.mixed):
             raise NotImplementedError("damage_law 'pfczm' runs the plain FP64 mechanics form only")
+        if op.has_closure and (form.precond != "jacobi" or form.mixed):
+            raise NotImplementedError("crack_closure 'axes' runs the plain FP64 mechanics form only")
         self.op = op
         self.load = load
         self.cfg = cfg
@@ -535,6 +542,9 @@ class StaggeredSolver:
         self._zeros = torch.zeros(op.n_mech, dtype=torch.float64, device=op.device)
         self._red = _lib.Workspace(op.device)
         self._pfws = _lib.Workspace(op.device)
+        self._clws = _lib.Workspace(op.device)
+        self.last_interface_solves = 0
+        self.last_line_search_steps = 0
         self._newton_count = 0
         self.last_newton_iters = None
         lengths = tuple(n * h for n, h in zip(op.shape, op.h))
@@ -582,6 +592,8 @@ class StaggeredSolver:
         return max(du_rel, dE_rel, dd)
 
     def _mechanics(self, d, values, x0):
+        if self.op.has_closure:
+            return self._closure_mechanics(d, values, x0)
         cfg = self.cfg
         try:
             x, info = solve_constrained_form(self.op, self.form, fixed_mask=self._mask_u8, fixed_values=values, d=d,
@@ -592,6 +604,75 @@ class StaggeredSolver:
         if not info.converged:
             raise _AttemptFailure(f"mechanics PCG did not converge in {cfg.pcg_maxit_mech} iterations")
         return x, info
+
+    def _linear_closure(self, g, pattern, values, x0):
+        """The mechanics solve of one closure pattern (StaggeredSolver._linear_mechanics,
+        staggered.py:550-587): the constrained Jacobi PCG with the add-back of ``pattern``."""
+        op, cfg = self.op, self.cfg
+        out = torch.empty(op.n_mech, dtype=torch.float64, device=op.device)
+        info = (C.c_int * 2)()
+        rinfo = (C.c_double * 2)()
+        wp, wn = self._clws.get(_lib.load().phastb_h8_mech_solve_closure_workspace_bytes(op.vgrid))
+        st = raw("phastb_h8_mech_solve_closure", op.vgrid, op.mat, ptr(op.slot), ptr(g), ptr(pattern),
+                 ptr(self._mask_u8), ptr(values), ptr(x0), float(cfg.pcg_rtol_mech), 0.0, int(cfg.pcg_maxit_mech),
+                 int(cfg.check_every), ptr(out), info, rinfo, wp, wn, stream())
+        if st in (_lib.BREAKDOWN, _lib.NONFINITE):
+            raise _AttemptFailure(f"mechanics PCG breakdown: PCG breakdown (status {st})")
+        if st not in (_lib.OK, _lib.NONCONVERGED):
+            _lib.check(st, "phastb_h8_mech_solve_closure")
+        bn, rn = float(rinfo[0]), float(rinfo[1])
+        pinfo = PCGInfo(int(info[0]), bool(info[1]), bn, rn, rn / bn if bn > 0 else 0.0)
+        if not pinfo.converged:
+            raise _AttemptFailure(f"mechanics PCG did not converge in {cfg.pcg_maxit_mech} iterations "
+                                  f"(relative residual {pinfo.relative_residual:.3e} > {cfg.pcg_rtol_mech:.3e})")
+        return out, pinfo
+
+    def _energy_line_search(self, x, y, g):
+        """Damped step from ``x`` towards the pattern solution ``y`` (staggered.py:589-626): alpha halved
+        from 1 until the degraded energy (each point at its own signs) meets the Armijo test with the
+        round-off allowance of ``|energy(x)|``; ``alpha = 1`` returns ``y`` itself."""
+        op = self.op
+        p = y - x
+        energy0 = float(op.elastic_energy(x, g))
+        force = op.mech_action(x, g)
+        free = ~self._mask
+        slope = min(float(torch.dot(force[free], p[free])), 0.0)
+        allowance = _LS_ENERGY_RTOL * abs(energy0)
+        alpha = 1.0
+        for _ in range(_LS_MAX_HALVINGS + 1):
+            trial = y if alpha == 1.0 else x + alpha * p
+            energy = float(op.elastic_energy(trial, g))
+            if not math.isfinite(energy):
+                raise _AttemptFailure("mechanics energy is not finite in the line search")
+            if energy <= energy0 + _LS_ARMIJO * alpha * slope + allowance:
+                return trial, alpha
+            alpha *= 0.5
+        raise _AttemptFailure(f"the energy line search of the closure mechanics solve found no decrease in "
+                              f"{_LS_MAX_HALVINGS} halvings")
+
+    def _closure_mechanics(self, d, values, x0):
+        """Line-searched active-set mechanics solve over the closure pattern (staggered.py:698-751):
+        start from the pattern of ``x0``, solve the linear system of the pattern, take the energy line
+        search towards it, and stop when no bit flips materially after a full step (at most
+        50 solves).  ``last_interface_solves`` records the solves."""
+        op = self.op
+        g = op.degradation(d)
+        pattern = op._closure_pattern_packed(x0)
+        iterations = 0
+        damped = 0
+        for solve in range(1, _CLOSURE_MAX_SOLVES + 1):
+            y, info = self._linear_closure(g, pattern, values, x0)
+            iterations += info.iterations
+            x, alpha = self._energy_line_search(x0, y, g)
+            damped += int(alpha < 1.0)
+            pattern, changed = op._closure_change_packed(x, pattern, g, _CLOSURE_PATTERN_TOLERANCE)
+            if not changed and alpha == 1.0:
+                self.last_interface_solves = solve
+                self.last_line_search_steps = damped
+                return x, dataclasses.replace(info, iterations=iterations)
+            x0 = x
+        raise _AttemptFailure("the closure pattern (crack_closure 'axes'), with the opening pattern of the interface "
+                              f"elements where present, did not settle in {_CLOSURE_MAX_SOLVES} mechanics solves")
 
     def _damage(self, H, lower, initial):
         """(d, PCG iterations, active-set iterations, kkt_ok) of the box-KKT damage solve (staggered.py:753-800)."""
@@ -710,9 +791,13 @@ class StaggeredSolver:
         change = math.inf
         converged = False
         info = None
+        closure = op.has_closure
+        closure_solves = 0
         for k in range(1, cfg.max_stagger + 1):
             x_new, info = self._mechanics(d_old, values, x_old)
             pm += info.iterations
+            if closure:
+                closure_solves += self.last_interface_solves
             H = op.driving_history(x_new, state.H if cfg.history == "max" else None)[1]
             d_new, its, s, kkt = self._damage(H, lower, d_old)
             pp += its
@@ -729,6 +814,8 @@ class StaggeredSolver:
         if cfg.final_mechanics_resolve:
             x, info = self._mechanics(d, values, x_old)
             pm += info.iterations
+            if closure:
+                closure_solves += self.last_interface_solves
         else:
             x = x_old
         # every scalar of the record in one kernel pair and one host read
@@ -740,6 +827,13 @@ class StaggeredSolver:
         scalars = np.concatenate([E, sigma, [elastic, fracture, rec["max_d"], rec["max_H"]]])
         if not np.isfinite(scalars).all():
             raise _AttemptFailure("accepted state has non-finite stress, strain or energy")
+        closure_record = {}
+        if closure:
+            # the closure solves of the increment and the kinematic guard of the accepted state
+            guard = op.kinematic_guard(x, d)
+            closure_record = {"closure_solves": int(closure_solves), "min_normal_strain": guard["min_normal_strain"],
+                              "min_principal_strain": guard["min_principal_strain"],
+                              "min_det_F": guard["min_det_F"]}
         mean_work = 2.0 * elastic / op.volume
         macro_work = float(np.dot(sigma, E))
         scale = max(abs(mean_work), abs(macro_work))
@@ -766,7 +860,7 @@ class StaggeredSolver:
             converged=True, kkt_ok=bool(kkt), stagger_change=float(change),
             mech_relative_residual=float(info.relative_residual), hill_mandel_rel=float(hill_rel),
             wall_s=perf_counter() - t0, mean_strain=macro_strain,
-            newton_iters_pf=self._newton_count if op.is_pfczm else None)
+            newton_iters_pf=self._newton_count if op.is_pfczm else None, **closure_record)
         return new_state, record
 
     # -- increments with cutback, and the load path -------------------------------------------

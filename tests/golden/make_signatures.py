@@ -51,6 +51,9 @@ FUNCTIONS = [
     ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.pfczm_tangent_action"),
     ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.pfczm_tangent_diagonal"),
     ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.pfczm_newton_system"),
+    ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.closure_pattern"),
+    ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.closure_pattern_change"),
+    ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.kinematic_guard"),
     ("phast.solid3d.linalg", "pcg"),
     ("phast.solid3d.linalg", "solve_constrained"),
     ("phast.solvers.box_kkt_h8", "solve_h8_scalar_box_kkt"),
@@ -88,6 +91,7 @@ DATACLASSES = [
     ("phast.solid3d.model", "IncrementRecord"),
     ("phast.solid3d.staggered", "SolverState"),
     ("phast.solid3d.linalg", "PCGInfo"),
+    ("phast.solid3d.model", "ClosurePattern"),
 ]
 
 PLAIN = (int, float, str, bool, type(None), tuple)
