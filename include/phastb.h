@@ -485,6 +485,21 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
                              int max_lin, int max_active, double* d_out, int* info, void* workspace,
                              size_t workspace_bytes, void* stream);
 
+/* ---- Anderson mixing of the staggered damage fixed point ----
+ * Type II Anderson mixing of d = G(d) with the last depth + 1 pairs
+ * (_AndersonAccelerator.step, solvers/staggered_solver.py:165-255).  hist holds
+ * 2 (depth + 1) n doubles owned by the caller: rows 0..depth the residuals G(d) - d, rows
+ * depth+1.. the outputs G(d), used as a ring.  `count` is the number of pairs already stored
+ * (0 after a reset) and `head` the row the new pair (d_in, d_out) goes to; the caller advances
+ * head = (head + 1) mod (depth + 1) and count = min(count + 1, depth + 1) after each call.
+ * d_mix = G(d) when there is no history, the normal equations (+ reg I) are singular or the
+ * mix's residual is above 1.5x that of G(d) (*used_host = 0); otherwise the mix clamped to
+ * [floor, 1] (floor NULL: 0), *used_host = 1.  depth <= 6. */
+size_t phastb_anderson_workspace_bytes(int depth);
+int phastb_anderson_step(int n, int depth, int count, int head, double* hist, const double* d_in,
+                         const double* d_out, const double* floor, double reg, double* d_mix, int* used_host,
+                         void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- PF-CZM damage law (SolverConfig.damage_law = 'pfczm') ----
  * Wu's rational degradation g = (1 - kappa) A/(A + Q) + kappa, A = (1 - d)^p,
  * Q = a1 d (1 + a2 d + a2 a3 d^2) (physics/pfczm.py:79-125) with a1 per material slot,

@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libphastb.so")
 SOURCES = ["capi.cu", "q4.cu", "h8.cu", "h8_tile.cu", "engine.cu", "solvers2d.cu", "solvers3d.cu", "gmg.cu", "t3.cu",
-           "batch3d.cu", "pfczm.cu", "closure.cu"]
+           "batch3d.cu", "pfczm.cu", "closure.cu", "anderson.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

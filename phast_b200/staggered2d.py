@@ -9,11 +9,14 @@ solve, relative-L2 convergence on u and d with ``min_stag = 2``).
 """
 from __future__ import annotations
 
+import ctypes as C
 from dataclasses import dataclass
 from typing import Optional
 
 import torch
 
+from . import _lib
+from ._lib import call, ptr, stream
 from .damage2d import PhaseFieldDamageSolver
 from .fem2d import FEMOperators
 from .mechanics2d import ExplicitDynamics, QuasiStaticSolver
@@ -96,15 +99,48 @@ class BoundaryConditions:
         return mask.to(self.device), vals.to(self.device)
 
 
+class AndersonAccelerator:
+    """Type II Anderson mixing of the damage fixed point (_AndersonAccelerator,
+    staggered_solver.py:165-255): the last ``m + 1`` pairs in a device ring, one C-ABI call per
+    staggered pass (``phastb_anderson_step``)."""
+
+    def __init__(self, n, m=5, device="cuda", reg=1e-10):
+        self.n, self.m, self.reg = int(n), int(m), float(reg)
+        self.hist = torch.empty(2 * (self.m + 1) * self.n, dtype=torch.float64, device=device)
+        self._ws = _lib.Workspace(torch.device(device))
+        self.count = self.head = 0
+        self.used = 0
+
+    def reset(self):
+        """Clear the history (each new load step)."""
+        self.count = self.head = 0
+
+    def step(self, d_in, d_out, d_prev_step=None):
+        """The next iterate: the mix clamped to [d_prev_step, 1], or ``d_out`` when there is no
+        history, the least-squares system is singular or the mix fails the residual safeguard."""
+        mix = torch.empty_like(d_out)
+        used = (C.c_int * 1)()
+        wp, wn = self._ws.get(_lib.load().phastb_anderson_workspace_bytes(self.m))
+        call("phastb_anderson_step", self.n, self.m, self.count, self.head, ptr(self.hist), ptr(d_in.contiguous()),
+             ptr(d_out.contiguous()), ptr(None if d_prev_step is None else d_prev_step.contiguous()), self.reg,
+             ptr(mix), used, wp, wn, stream())
+        self.head = (self.head + 1) % (self.m + 1)
+        self.count = min(self.count + 1, self.m + 1)
+        self.used += int(used[0])
+        return mix
+
+
 class StaggeredSolver:
     """GPU staggered phase-field step (staggered_solver.py:269-1344)."""
 
     def __init__(self, mesh, material, bcs, config=None, ctx=None):
         self.config = config or SolverConfig()
         cfg = self.config
-        if cfg.anderson_depth or cfg.damage_viscosity or cfg.H_cap is not None or cfg.H_update_method != "hard_max":
-            raise NotImplementedError("Anderson mixing, damage viscosity and non-hard-max H updates are not "
-                                      "implemented by the B200 backend")
+        if cfg.damage_viscosity or cfg.H_cap is not None or cfg.H_update_method != "hard_max":
+            raise NotImplementedError("damage viscosity and non-hard-max H updates are not implemented by the B200 "
+                                      "backend")
+        if cfg.anderson_depth and not 1 <= int(cfg.anderson_depth) <= 6:
+            raise NotImplementedError("the B200 backend runs Anderson mixing of depth 1 to 6")
         if cfg.stagger_criterion != "relative" or cfg.stagger_norm != "l2":
             raise NotImplementedError("only the relative-L2 stagger criterion is implemented")
         self.mesh, self.material, self.bcs = mesh, material, bcs
@@ -203,14 +239,24 @@ class StaggeredSolver:
             return self.H_elem
         tol = cfg.stagger_tol
         d_prev_step = self.d.clone()
+        aa = None
+        if cfg.anderson_depth > 0:
+            if getattr(self, "_aa", None) is None:
+                self._aa = AndersonAccelerator(self.d.numel(), int(cfg.anderson_depth), self.device)
+            else:
+                self._aa.reset()
+            aa = self._aa
         stag = 0
         for stag in range(cfg.max_stagger):
             need = stag >= 1
-            d_old = self.d.clone() if need else self.d
+            d_old = self.d.clone() if (need or aa is not None) else self.d
             u_old = self.u.clone() if need else self.u
             self.step_mechanics()
             self.step_compute_driving_force()
             self.step_solve_damage(d_prev_step=d_prev_step)
+            if aa is not None:
+                # the mixed field is the next iterate and the one the convergence test measures
+                self.d = aa.step(d_old, self.d, d_prev_step)
             if self.stagger_trace is not None:
                 self.stagger_trace.append((self.u.clone(), self.d.clone(), self.H_elem.clone()))
             if need:

@@ -1,0 +1,52 @@
+"""Anderson mixing of the 2D staggered damage fixed point on the GPU against fixtures the
+reference wrote (``tests/golden/make_golden_anderson.py``): the accelerator alone on a seeded
+sequence, and quasi-static SENT load steps with ``anderson_depth = 3`` (needs a B200)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden, rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("tag", ["floor", "nofloor"])
+def test_anderson_accelerator(tag):
+    from phast_b200.staggered2d import AndersonAccelerator
+    g = golden("anderson")
+    ins, outs, mixes = g[f"acc_{tag}_in"], g[f"acc_{tag}_out"], g[f"acc_{tag}_mix"]
+    aa = AndersonAccelerator(ins.shape[1], 3, "cuda")
+    floor = torch.as_tensor(g["acc_floor"], device="cuda") if tag == "floor" else None
+    for k in range(ins.shape[0]):
+        out = aa.step(torch.as_tensor(ins[k], device="cuda"), torch.as_tensor(outs[k], device="cuda"), floor)
+        assert rel(out.cpu(), mixes[k]) < 1e-12, k
+    assert aa.used > 0
+
+
+def test_anderson_staggered_sent():
+    """Four SENT load steps with depth-3 mixing: stagger counts, fields and reactions."""
+    import phast_b200 as pb
+    g = golden("anderson")
+    nx = int(g["nx"])
+    sm = pb.structured_q4_mesh(1.0, 1.0, nx, nx)
+    mesh = pb.FEMMesh.from_tensors(sm.nodes, sm.quads, element_type="Q4", device="cuda")
+    bcs = pb.BoundaryConditions(mesh.n_nodes, device="cuda")
+    mat = pb.Material(E=210000.0, nu=0.3, Gc=2.7, l0=0.1, eta_residual=1e-8, energy_split="isotropic", rho=7.8e-9)
+    bcs.fix(sm.node_sets["bottom"], 0)
+    bcs.fix(sm.node_sets["bottom"], 1)
+    bcs.add(sm.node_sets["top"], 1, 1.0)
+    bcs.add_pf_dirichlet(torch.as_tensor(g["notch"]), 1.0)
+    cfg = pb.SolverConfig(solver_type="quasi_static", backend="cg", static_tol=1e-10, damage_tol=1e-10,
+                          bounds_method="projected_cg", use_multigrid=False, stagger_tol=1e-6, max_stagger=100,
+                          anderson_depth=3)
+    s = pb.StaggeredSolver(mesh, mat, bcs, cfg)
+    s._apply_pf_dirichlet()
+    for k, lf in enumerate(g["loads"]):
+        bcs.load_factor = float(lf)
+        s.step_full()
+        assert s._last_stagger_iter == int(g["sent_stag"][k]), k
+        assert rel(s.u.cpu(), g["sent_u"][k]) < 1e-7, k
+        assert rel(s.d.cpu(), g["sent_d"][k]) < 1e-7, k
+        rf = s.fem.compute_reaction_force(s.u, s.d, sm.node_sets["top"], component=1)
+        assert abs(rf - g["sent_rf"][k]) <= 1e-6 * abs(g["sent_rf"][k]), k
+    assert ((s.d.cpu().numpy() > 0.9) == (g["sent_d"][-1] > 0.9)).all()

@@ -333,3 +333,14 @@ def test_closure_staggered_increments():
         assert rel(sig, g["st_sigma"][k]) < 1e-8
         assert rel(d, g["st_d"][k]) < 1e-6 and rel(x, g["st_x"][k]) < (1e-8 if k < 3 else 1e-5)
         assert rel(np.array(guard), g["st_guard"][k]) < 1e-6
+
+
+@pytest.mark.parametrize("tag", ["floor", "nofloor"])
+def test_anderson_accelerator(tag):
+    """Anderson mixing of the 2D staggered fixed point, eight steps of depth 3, against the reference."""
+    from oracle.anderson import AndersonAccelerator
+    g = golden("anderson")
+    aa = AndersonAccelerator(m=3)
+    for k in range(g[f"acc_{tag}_in"].shape[0]):
+        out = aa.step(g[f"acc_{tag}_in"][k], g[f"acc_{tag}_out"][k], g["acc_floor"] if tag == "floor" else None)
+        assert rel(out, g[f"acc_{tag}_mix"][k]) < 1e-12, k
