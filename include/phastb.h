@@ -500,6 +500,17 @@ int phastb_anderson_step(int n, int depth, int count, int head, double* hist, co
                          const double* d_out, const double* floor, double reg, double* d_mix, int* used_host,
                          void* workspace, size_t workspace_bytes, void* stream);
 
+/* Projected Anderson mixing of the 3D staggered damage fixed point (ProjectedAnderson,
+ * solid3d/staggered.py:290-376) on the same ring: push (d_in, d_out) into row `head`; with
+ * want_mix and at least two pairs, d_mix = clamp(d_out - dG gamma, lower, upper) where gamma
+ * solves the normal equations of the unit-norm residual differences (zero columns dropped)
+ * with `reg` on the diagonal.  *status_host: 0 no mix (too few pairs, every difference zero, a
+ * singular system or a non-finite mix), 1 a mix that differs from d_out, 2 a mix equal to it. */
+int phastb_anderson_projected(int n, int depth, int count, int head, double* hist, const double* d_in,
+                              const double* d_out, int want_mix, const double* lower, double upper, double reg,
+                              double* d_mix, int* status_host, void* workspace, size_t workspace_bytes,
+                              void* stream);
+
 /* ---- PF-CZM damage law (SolverConfig.damage_law = 'pfczm') ----
  * Wu's rational degradation g = (1 - kappa) A/(A + Q) + kappa, A = (1 - d)^p,
  * Q = a1 d (1 + a2 d + a2 a3 d^2) (physics/pfczm.py:79-125) with a1 per material slot,

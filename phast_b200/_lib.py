@@ -149,6 +149,8 @@ SIGNATURES = {
     "phastb_anderson_workspace_bytes": (sz, [C.c_int]),
     "phastb_anderson_step": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, C.c_double, vp, ip, vp,
                                        sz, vp]),
+    "phastb_anderson_projected": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_int, vp, C.c_double,
+                                            C.c_double, vp, ip, vp, sz, vp]),
     "phastb_h8_closure_workspace_bytes": (sz, [VG]),
     "phastb_h8_closure_pattern": (C.c_int, [VG, VM, vp, vp, vp, vp]),
     "phastb_h8_closure_pattern_change": (C.c_int, [VG, VM, vp, vp, vp, vp, C.c_double, vp, ip, vp, sz, vp]),

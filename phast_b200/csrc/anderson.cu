@@ -110,6 +110,31 @@ __global__ void __launch_bounds__(kThreads) aa_mix_kernel(int n, int depth, Ring
   reduce_multi<2>(acc, ws);
 }
 
+// Projected mix: mix = clamp(d_out - sum_i (G_{i+1} - G_i) gamma_i, lower, upper);
+// ws.out = [entries not finite before the clamp, entries that differ from d_out].
+__global__ void __launch_bounds__(kThreads) aa_pmix_kernel(int n, int depth, Ring r, Gamma gm,
+                                                           const double* __restrict__ hist,
+                                                           const double* __restrict__ d_out,
+                                                           const double* __restrict__ lower, double upper,
+                                                           double* __restrict__ mix, RedWs ws) {
+  const int mk = r.c - 1;
+  const size_t N = (size_t)n;
+  const double* G = hist + (size_t)(depth + 1) * N;
+  double acc[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+#pragma unroll
+    for (int a = 0; a < kMaxDepth; ++a)
+      if (a < mk) s += (G[(size_t)r.rows[a + 1] * N + i] - G[(size_t)r.rows[a] * N + i]) * gm.g[a];
+    double v = d_out[i] - s;
+    if (!isfinite(v)) acc[0] += 1.0;
+    v = fmin(fmax(v, lower[i]), upper);
+    mix[i] = v;
+    if (v != d_out[i]) acc[1] += 1.0;
+  }
+  reduce_multi<2>(acc, ws);
+}
+
 __global__ void aa_clamp_kernel(int n, const double* __restrict__ floor, double* __restrict__ mix) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double lo = floor ? floor[i] : 0.0;
@@ -212,6 +237,76 @@ int phastb_anderson_step(int n, int depth, int count, int head, double* hist, co
   { note_launch(); aa_clamp_kernel<<<G, kThreads, 0, s>>>(n, floor, d_mix); }
   if ((st = last_launch_status())) return st;
   if (used_host) *used_host = 1;
+  return PHASTB_OK;
+}
+
+int phastb_anderson_projected(int n, int depth, int count, int head, double* hist, const double* d_in,
+                              const double* d_out, int want_mix, const double* lower, double upper, double reg,
+                              double* d_mix, int* status_host, void* workspace, size_t workspace_bytes,
+                              void* stream) {
+  if (n < 1 || depth < 1 || depth > kMaxDepth || count < 0 || count > depth + 1 || head < 0 || head > depth ||
+      !hist || !d_in || !d_out || !status_host || !(reg >= 0.0) || (want_mix && (!lower || !d_mix)))
+    return PHASTB_ERR_ARG;
+  if (!workspace || workspace_bytes < phastb_anderson_workspace_bytes(depth)) return PHASTB_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  char* p = static_cast<char*>(workspace);
+  double* part = reinterpret_cast<double*>(p);
+  unsigned* counter = reinterpret_cast<unsigned*>(p + gram_part_bytes());
+  double* gout = reinterpret_cast<double*>(p + gram_part_bytes() + 256);
+  RedWs mw = red_ws(p + gram_ws_bytes());
+  Ring r{};
+  r.c = std::min(count + 1, depth + 1);
+  const int R = depth + 1;
+  for (int i = 0; i < r.c; ++i) r.rows[i] = ((head - (r.c - 1) + i) % R + R) % R;
+  *status_host = 0;
+  int st;
+  if ((st = cuda_status(cudaMemsetAsync(counter, 0, sizeof(unsigned), s)))) return st;
+  if ((st = red_ws_reset(mw, s))) return st;
+  const int G = grid_for(n);
+  // the push, with the products of the normal equations when a mix is wanted
+  Ring rp = r;
+  if (!want_mix || r.c < 2) {
+    rp.c = 1;
+    rp.rows[0] = r.rows[r.c - 1];  // the new pair's row, no products
+  }
+  { note_launch(); aa_gram_kernel<<<G, kThreads, 0, s>>>(n, depth, rp, hist, d_in, d_out, part, counter, gout); }
+  if ((st = last_launch_status())) return st;
+  if (!want_mix || r.c < 2) return cuda_status(cudaStreamSynchronize(s));
+  const int mk = r.c - 1;
+  const int K = mk * (mk + 1) / 2 + mk;
+  double prod[kMaxProducts];
+  if ((st = cuda_status(cudaMemcpyAsync(prod, gout, sizeof(double) * K, cudaMemcpyDeviceToHost, s)))) return st;
+  if ((st = cuda_status(cudaStreamSynchronize(s)))) return st;
+  // unit-norm columns of dF (zero columns dropped), relative regularisation on the normal equations
+  double P[kMaxDepth][kMaxDepth], pf[kMaxDepth], sc[kMaxDepth];
+  int k = 0;
+  for (int a = 0; a < mk; ++a)
+    for (int c = a; c < mk; ++c) {
+      P[a][c] = P[c][a] = prod[k];
+      ++k;
+    }
+  for (int a = 0; a < mk; ++a) pf[a] = prod[k + a];
+  int keep[kMaxDepth], nk = 0;
+  for (int a = 0; a < mk; ++a) {
+    sc[a] = std::sqrt(std::max(P[a][a], 0.0));
+    if (sc[a] > 0.0) keep[nk++] = a;
+  }
+  if (nk == 0) return PHASTB_OK;
+  double A[kMaxDepth * kMaxDepth], b[kMaxDepth], x[kMaxDepth];
+  for (int i = 0; i < nk; ++i) {
+    for (int j = 0; j < nk; ++j) A[i * nk + j] = P[keep[i]][keep[j]] / (sc[keep[i]] * sc[keep[j]]);
+    A[i * nk + i] += reg;
+    b[i] = pf[keep[i]] / sc[keep[i]];
+  }
+  if (!solve_small(nk, A, b, x)) return PHASTB_OK;
+  Gamma gm{};
+  for (int i = 0; i < nk; ++i) gm.g[keep[i]] = x[i] / sc[keep[i]];
+  { note_launch(); aa_pmix_kernel<<<G, kThreads, 0, s>>>(n, depth, r, gm, hist, d_out, lower, upper, d_mix, mw); }
+  if ((st = last_launch_status())) return st;
+  double cnt[2];
+  if ((st = red_ws_fetch(mw, cnt, 2, s))) return st;
+  if (cnt[0] > 0.0) return PHASTB_OK;  // a non-finite mix is no mix
+  *status_host = cnt[1] > 0.0 ? 1 : 2;
   return PHASTB_OK;
 }
 

@@ -9,6 +9,6 @@ from .model import (DRIVER_FULL, DRIVER_NONE, DRIVER_SPECTRAL, PHASE_ID, PHASE_N
                     isotropic_C, lame, resolve_driver, sphere_pore_model, sphere_pore_phase)
 from .operator import H8DamageSystem, MechOperator, PeriodicVoxelPhaseFieldOperator, PfczmNewtonSystem
 from .staggered import (PLAIN, BoxKKTFailureEvidence, BoxKKTResult, H8ScalarBoxKKTConvergenceError, IncrementRecord,
-                        MechForm, PCGBreakdownError, PCGConvergenceError, PCGInfo, SolverState,
+                        MechForm, PCGBreakdownError, PCGConvergenceError, PCGInfo, ProjectedAnderson, SolverState,
                         StaggerConvergenceError, StaggeredSolver, pcg, solve_constrained, solve_constrained_form,
                         solve_h8_scalar_box_kkt)

@@ -320,7 +320,7 @@ class SolverConfig:
     The GPU backend runs ``dtype='float64'`` results (the chosen mechanics form may compute
     in FP32 under FP64 refinement; see ``StaggeredSolver(form=...)``), ``damage_law`` 'at2' or 'pfczm',
     ``irreversibility='box_kkt'``, ``history`` 'max' or 'current', ``crack_closure`` 'none' or 'axes' and
-    ``anderson_depth=0``; ``device`` names the CUDA device.
+    ``anderson_depth`` 0-6; ``device`` names the CUDA device.
     """
     device: str = "cuda"
     dtype: str = "float64"
@@ -393,8 +393,8 @@ class SolverConfig:
 def unsupported_options(cfg):
     """Names of ``cfg`` settings this backend does not run (empty when it runs them all)."""
     out = []
-    if getattr(cfg, "anderson_depth", 0) != 0:
-        out.append(f"anderson_depth={cfg.anderson_depth!r}")
+    if getattr(cfg, "anderson_depth", 0) > 6:
+        out.append(f"anderson_depth={cfg.anderson_depth!r} (the B200 backend mixes at most 6 pairs)")
     if getattr(cfg, "irreversibility", "box_kkt") != "box_kkt":
         out.append(f"irreversibility={cfg.irreversibility!r}")
     if getattr(cfg, "energy_split_band", "isotropic") != "isotropic":

@@ -490,6 +490,92 @@ _CLOSURE_PATTERN_TOLERANCE = 1.0e-8  # staggered.py:105
 _LS_ARMIJO = 1.0e-4                 # LINE_SEARCH_ARMIJO, staggered.py:109
 _LS_ENERGY_RTOL = 1.0e-12           # staggered.py:112
 _LS_MAX_HALVINGS = 30               # staggered.py:115
+ANDERSON_REGULARISATION = 1.0e-10   # staggered.py:133
+_ANDERSON_ENERGY_RTOL = 1.0e-12     # staggered.py:136
+
+
+class ProjectedAnderson:
+    """Type II Anderson mixing of the damage fixed point with a box projection (staggered.py:290-376):
+    the last ``depth + 1`` pairs ``(d, G(d))`` in a device ring; a mix solves the regularised normal
+    equations of the unit-norm residual differences and is clamped to ``[lower, upper]``.
+
+    ``push(d_in, d_out)`` stores a pair, ``mix(lower, upper=1.0)`` returns the projected mix or
+    ``None``; ``push_mix`` does both in one C-ABI call and also returns ``None`` for a mix equal
+    to ``d_out``.
+    """
+
+    def __init__(self, depth, *, regularisation=ANDERSON_REGULARISATION, n=None, device="cuda"):
+        if isinstance(depth, bool) or int(depth) != depth or not 1 <= int(depth) <= 6:
+            raise ValueError(f"depth must be an integer in 1..6, got {depth!r}")
+        if not (math.isfinite(regularisation) and regularisation >= 0.0):
+            raise ValueError(f"regularisation must be finite and >= 0, got {regularisation!r}")
+        self.depth = int(depth)
+        self.regularisation = float(regularisation)
+        self.device = torch.device(device)
+        self._n = None if n is None else int(n)
+        self._hist = None
+        self._ws = _lib.Workspace(self.device)
+        self.count = self.head = 0
+        self._pending = None
+        self._last_mix = None
+
+    def __len__(self):
+        return min(self.count + (self._pending is not None), self.depth + 1)
+
+    def reset(self):
+        """Forget every stored pair."""
+        self.count = self.head = 0
+        self._pending = None
+        self._last_mix = None
+
+    def _call(self, d_in, d_out, want, lower, upper):
+        d_in = d_in.to(torch.float64).contiguous()
+        d_out = d_out.to(torch.float64).contiguous()
+        if self._hist is None:
+            self._n = d_in.numel() if self._n is None else self._n
+            self._hist = torch.empty(2 * (self.depth + 1) * self._n, dtype=torch.float64, device=self.device)
+        if d_in.numel() != self._n or d_out.shape != d_in.shape:
+            raise ValueError("d_in and d_out must be vectors of the cell's length")
+        low = None
+        if want:
+            low = lower.to(torch.float64).contiguous() if isinstance(lower, torch.Tensor) else \
+                torch.full((self._n,), float(lower), dtype=torch.float64, device=self.device)
+        mixed = torch.empty_like(d_out) if want else None
+        status = (C.c_int * 1)()
+        wp, wn = self._ws.get(_lib.load().phastb_anderson_workspace_bytes(self.depth))
+        _lib.call("phastb_anderson_projected", self._n, self.depth, self.count, self.head, ptr(self._hist),
+                  ptr(d_in), ptr(d_out), int(bool(want)), ptr(low), float(upper), self.regularisation, ptr(mixed),
+                  status, wp, wn, stream())
+        self.head = (self.head + 1) % (self.depth + 1)
+        self.count = min(self.count + 1, self.depth + 1)
+        return mixed, int(status[0])
+
+    def _flush(self):
+        if self._pending is not None:
+            self._call(*self._pending, False, None, 1.0)
+            self._pending = None
+
+    def push(self, d_in, d_out):
+        """Store the pair ``(d_in, G(d_in))`` (copies; the oldest pair drops out at ``depth + 1``).
+        The pair enters the device ring with the next ``mix`` or ``push``."""
+        self._flush()
+        self._pending = (d_in.detach().clone(), d_out.detach().clone())
+
+    def mix(self, lower, upper=1.0):
+        """Projected mixed iterate of the stored pairs, or ``None`` when no mix is defined (fewer than two
+        pairs, every residual difference zero, a singular system or a non-finite mix)."""
+        if self._pending is None:
+            return self._last_mix
+        mixed, status = self._call(*self._pending, True, lower, upper)
+        self._pending = None
+        self._last_mix = mixed if status in (1, 2) else None
+        return self._last_mix
+
+    def push_mix(self, d_in, d_out, lower, upper=1.0, *, mix=True):
+        """Store the pair and return the projected mix, or ``None`` (no mix defined, or equal to d_out)."""
+        self._flush()
+        mixed, status = self._call(d_in, d_out, mix, lower, upper)
+        return mixed if status == 1 else None
 
 
 class StaggeredSolver:
@@ -520,6 +606,8 @@ class StaggeredSolver:
             raise NotImplementedError(f"the B200 backend does not run {', '.join(bad)}")
         if op.is_pfczm and (form.precond != "jacobi" or form.mixed):
             raise NotImplementedError("damage_law 'pfczm' runs the plain FP64 mechanics form only")
+        if op.has_closure and cfg.anderson_depth > 0:
+            raise ValueError("Anderson mixing (anderson_depth > 0) is not available with crack_closure 'axes'")
         if op.has_closure and (form.precond != "jacobi" or form.mixed):
             raise NotImplementedError("crack_closure 'axes' runs the plain FP64 mechanics form only")
         self.op = op
@@ -793,20 +881,67 @@ class StaggeredSolver:
         info = None
         closure = op.has_closure
         closure_solves = 0
+        # Anderson mixing: a fresh history for every attempt; a mixed input is judged by its own
+        # iteration against the plain iterate it replaced (staggered.py:1282-1400)
+        anderson = ProjectedAnderson(cfg.anderson_depth, n=op.n_red, device=op.device) \
+            if cfg.anderson_depth > 0 else None
+        best_energy = math.inf
+        n_accepted = n_rejected = 0
+        fallback = None
         for k in range(1, cfg.max_stagger + 1):
-            x_new, info = self._mechanics(d_old, values, x_old)
-            pm += info.iterations
-            if closure:
-                closure_solves += self.last_interface_solves
-            H = op.driving_history(x_new, state.H if cfg.history == "max" else None)[1]
-            d_new, its, s, kkt = self._damage(H, lower, d_old)
-            pp += its
-            sets += s
-            change = self._change(x_new, x_old, d_new, d_old, step_size)
-            x_old, d_old = x_new, d_new
+            try:
+                x_new, info = self._mechanics(d_old, values, x_old)
+                pm += info.iterations
+                if closure:
+                    closure_solves += self.last_interface_solves
+                H = op.driving_history(x_new, state.H if cfg.history == "max" else None)[1]
+                d_new, its, s, kkt = self._damage(H, lower, d_old)
+                pp += its
+                sets += s
+                change = self._change(x_new, x_old, d_new, d_old, step_size)
+            except _AttemptFailure:
+                if fallback is None:
+                    raise
+                # the iteration from a mixed input failed: return to the plain iterate
+                n_rejected += 1
+                x_old, d_old = fallback[1], fallback[0]
+                fallback = None
+                anderson.reset()
+                continue
+            rejected = False
+            residual = None
+            if anderson is not None:
+                residual = float(torch.linalg.vector_norm(d_new - d_old))
+                rec = op.increment_record(x_new, d_new, None, cfg.damaged_threshold)
+                total = rec["energy"] + rec["local"] + rec["gradient"]
+                if fallback is not None:
+                    # the end-of-iteration total energy must not rise above the lowest of the
+                    # attempt, and the fixed-point residual not above the replaced iteration's
+                    rejected = (total > best_energy + _ANDERSON_ENERGY_RTOL * abs(best_energy)) or \
+                        (residual > fallback[2])
+                    if rejected:
+                        n_rejected += 1
+                    else:
+                        n_accepted += 1
+                if not rejected:
+                    best_energy = min(best_energy, total)
+            if rejected:
+                x_old, d_old = fallback[1], fallback[0]
+                fallback = None
+                anderson.reset()
+                continue
+            fallback = None
             if change <= cfg.stagger_tol and k >= cfg.min_stagger:
+                x_old, d_old = x_new, d_new
                 converged = True
                 break
+            if anderson is not None:
+                mixed = anderson.push_mix(d_old, d_new, lower, mix=k >= cfg.anderson_start)
+                if mixed is not None:
+                    fallback = (d_new, x_new, residual)
+                    x_old, d_old = x_new, mixed
+                    continue
+            x_old, d_old = x_new, d_new
         if not converged:
             raise _AttemptFailure(f"staggered iteration did not converge in {cfg.max_stagger} iterations "
                                   f"(change {change:.3e} > stagger_tol {cfg.stagger_tol:.3e})")
@@ -860,7 +995,9 @@ class StaggeredSolver:
             converged=True, kkt_ok=bool(kkt), stagger_change=float(change),
             mech_relative_residual=float(info.relative_residual), hill_mandel_rel=float(hill_rel),
             wall_s=perf_counter() - t0, mean_strain=macro_strain,
-            newton_iters_pf=self._newton_count if op.is_pfczm else None, **closure_record)
+            newton_iters_pf=self._newton_count if op.is_pfczm else None,
+            anderson_accepted=n_accepted if anderson is not None else None,
+            anderson_rejected=n_rejected if anderson is not None else None, **closure_record)
         return new_state, record
 
     # -- increments with cutback, and the load path -------------------------------------------

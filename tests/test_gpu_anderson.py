@@ -50,3 +50,41 @@ def test_anderson_staggered_sent():
         rf = s.fem.compute_reaction_force(s.u, s.d, sm.node_sets["top"], component=1)
         assert abs(rf - g["sent_rf"][k]) <= 1e-6 * abs(g["sent_rf"][k]), k
     assert ((s.d.cpu().numpy() > 0.9) == (g["sent_d"][-1] > 0.9)).all()
+
+
+def test_projected_anderson_mixer():
+    """ProjectedAnderson's push/mix (3D) against the reference on a seeded sequence."""
+    from phast_b200.solid3d import ProjectedAnderson
+    g = golden("anderson3d")
+    pa = ProjectedAnderson(3)
+    lower = torch.as_tensor(g["mix_lower"], device="cuda")
+    for k in range(g["mix_in"].shape[0]):
+        pa.push(torch.as_tensor(g["mix_in"][k], device="cuda"), torch.as_tensor(g["mix_out"][k], device="cuda"))
+        m = pa.mix(lower)
+        assert (m is not None) == bool(g["mix_has"][k]), k
+        if m is not None:
+            assert rel(m.cpu(), g["mix_mix"][k]) < 1e-12, k
+
+
+def test_projected_anderson_staggered_increments():
+    """Four increments of the 6^3 pore cell with anderson_depth = 3 through PhAST's solver API:
+    stagger passes, accepted and rejected mixes and damage PCG counts equal to the reference's."""
+    from phast_b200.solid3d import LoadCase, PeriodicVoxelPhaseFieldOperator, SolverConfig, StaggeredSolver
+    from phast_b200.solid3d import sphere_pore_model
+    g = golden("anderson3d")
+    targets = tuple(float(v) for v in g["st_targets"])
+    op = PeriodicVoxelPhaseFieldOperator(
+        sphere_pore_model((6, 6, 6), 0.2),
+        LoadCase(name="zz", controlled=2, targets=targets, free=(), fixed_zero=(0, 1, 3, 4, 5)),
+        SolverConfig(device="cuda", kappa=1e-6, energy_split_isotropic="spectral", anderson_depth=3))
+    solver = StaggeredSolver(op)
+    state = solver.initial_state()
+    for k, target in enumerate(targets):
+        state, rec = solver.advance(state, target)
+        assert rec.stagger_iters == int(g["st_stag"][k]), k
+        assert (rec.anderson_accepted, rec.anderson_rejected) == (int(g["st_acc"][k]), int(g["st_rej"][k])), k
+        assert rec.pcg_iters_pf == int(g["st_pcg_pf"][k]), k
+        assert abs(rec.pcg_iters_mech - int(g["st_pcg_mech"][k])) <= 2, k
+        assert rel(np.array(rec.macro_stress), g["st_sigma"][k]) < 1e-8
+        assert rel(state.d.cpu(), g["st_d"][k]) < 1e-6
+        assert rel(state.x.cpu(), g["st_x"][k]) < (1e-8 if k < 3 else 1e-5)
