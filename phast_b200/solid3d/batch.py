@@ -495,6 +495,12 @@ class BatchStaggeredSolver:
         self.batch = batch
         self.load = load
         self.cfg = cfg or SolverConfig(kappa=batch.ops[0].kappa)
+        c = self.cfg
+        if (getattr(c, "irreversibility", "box_kkt") != "box_kkt" or getattr(c, "anderson_depth", 0)
+                or getattr(c, "crack_closure", "none") != "none" or getattr(c, "damage_law", "at2") != "at2"
+                or any(op.is_pfczm or op.has_closure for op in batch.ops)):
+            raise NotImplementedError("the packed batch runs the AT2 law with box-KKT irreversibility, without "
+                                      "crack closure or Anderson mixing")
         self.mixed = bool(mixed)
         self.inner_rtol = float(inner_rtol)
         self.max_refine = int(max_refine)

@@ -5,9 +5,8 @@ and ``build_element_arrays`` (src/phast/solid3d/materials.py:474-547) with the s
 names, fields, defaults and validation errors, so a caller written against the
 reference builds the same objects here.  Objects of the reference package with
 the same fields are accepted wherever these are (the operator reads attributes
-only).  Options of the reference that this backend does not run (Anderson mixing,
-smeared-laminate phases with their band closure, the interface driver,
-``history_only`` irreversibility) are accepted by the data classes and refused
+only).  Options of the reference that this backend does not run (smeared-laminate
+phases with their band closure, the interface driver) are accepted by the data classes and refused
 with ``NotImplementedError`` when an operator or solver is built from them.
 """
 from __future__ import annotations
@@ -319,7 +318,7 @@ class SolverConfig:
 
     The GPU backend runs ``dtype='float64'`` results (the chosen mechanics form may compute
     in FP32 under FP64 refinement; see ``StaggeredSolver(form=...)``), ``damage_law`` 'at2' or 'pfczm',
-    ``irreversibility='box_kkt'``, ``history`` 'max' or 'current', ``crack_closure`` 'none' or 'axes' and
+    ``irreversibility`` 'box_kkt' or 'history_only', ``history`` 'max' or 'current', ``crack_closure`` 'none' or 'axes' and
     ``anderson_depth`` 0-6; ``device`` names the CUDA device.
     """
     device: str = "cuda"
@@ -395,8 +394,6 @@ def unsupported_options(cfg):
     out = []
     if getattr(cfg, "anderson_depth", 0) > 6:
         out.append(f"anderson_depth={cfg.anderson_depth!r} (the B200 backend mixes at most 6 pairs)")
-    if getattr(cfg, "irreversibility", "box_kkt") != "box_kkt":
-        out.append(f"irreversibility={cfg.irreversibility!r}")
     if getattr(cfg, "energy_split_band", "isotropic") != "isotropic":
         out.append(f"energy_split_band={cfg.energy_split_band!r}")
     if getattr(cfg, "dtype", "float64") != "float64":

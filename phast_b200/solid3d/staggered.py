@@ -631,6 +631,8 @@ class StaggeredSolver:
         self._red = _lib.Workspace(op.device)
         self._pfws = _lib.Workspace(op.device)
         self._clws = _lib.Workspace(op.device)
+        self._neg_inf = None
+        self.last_bound_violations = None
         self.last_interface_solves = 0
         self.last_line_search_steps = 0
         self._newton_count = 0
@@ -763,7 +765,8 @@ class StaggeredSolver:
                               f"elements where present, did not settle in {_CLOSURE_MAX_SOLVES} mechanics solves")
 
     def _damage(self, H, lower, initial):
-        """(d, PCG iterations, active-set iterations, kkt_ok) of the box-KKT damage solve (staggered.py:753-800)."""
+        """(d, PCG iterations, active-set iterations, kkt_ok) of the box-KKT damage solve, or of the
+        unbounded Dirichlet PCG with ``irreversibility='history_only'`` (staggered.py:753-841)."""
         if self.op.is_pfczm:
             return self._damage_pfczm(H, lower, initial)
         cfg, op = self.cfg, self.op
@@ -772,6 +775,8 @@ class StaggeredSolver:
             raise _AttemptFailure("damage residual is not finite")
         # the PCG stops at tol * max(||r0||, 1) while the KKT audit is absolute
         tol = max(min(cfg.damage_linear_tol, 0.1 * cfg.damage_kkt_tol / max(r0, 1.0)), _MIN_LINEAR_TOLERANCE)
+        if cfg.irreversibility == "history_only":
+            return self._damage_history_only(H, lower, initial, tol)
         # the bounds hold by construction: lower is the accepted damage of the last
         # increment (in [0, 1]) and initial is lower itself or a box-KKT solution
         try:
@@ -785,6 +790,31 @@ class StaggeredSolver:
         except RuntimeError as exc:
             raise _AttemptFailure(f"damage PCG breakdown: {exc}") from exc
         return res.solution, res.total_pcg_iterations, res.active_set_iterations, res.satisfies_kkt
+
+    def _damage_history_only(self, H, lower, initial, tol):
+        """The damage system solved without bounds (one Dirichlet PCG with nothing fixed: the box
+        solve with infinite bounds), then the bound-violation statistics (staggered.py:801-841)."""
+        cfg, op = self.cfg, self.op
+        if self._neg_inf is None:
+            self._neg_inf = torch.full((op.n_red,), -math.inf, dtype=torch.float64, device=op.device)
+        try:
+            res = solve_h8_scalar_box_kkt(op.damage_system(H), lower_bound=self._neg_inf, upper_bound=math.inf,
+                                          initial=initial, linear_tolerance=tol, kkt_tolerance=math.inf,
+                                          max_linear_iterations=cfg.damage_maxit, max_active_set_iterations=1,
+                                          check_bounds=False)
+        except H8ScalarBoxKKTConvergenceError as exc:
+            raise _AttemptFailure(f"damage PCG did not converge in {cfg.damage_maxit} iterations") from exc
+        except RuntimeError as exc:
+            raise _AttemptFailure(f"damage PCG breakdown: {exc}") from exc
+        d = res.solution
+        stats = torch.stack(((d < lower).sum().to(torch.float64), (d < 0.0).sum().to(torch.float64),
+                             (d > 1.0).sum().to(torch.float64), torch.clamp_min(lower - d, 0.0).max(),
+                             torch.clamp_min(d - 1.0, 0.0).max())).cpu()
+        self.last_bound_violations = {"below_previous": int(stats[0]), "below_zero": int(stats[1]),
+                                      "above_one": int(stats[2]), "max_decrease": float(stats[3]),
+                                      "max_excess_over_one": float(stats[4])}
+        kkt_ok = int(stats[0]) == 0 and int(stats[1]) == 0 and int(stats[2]) == 0
+        return d, res.total_pcg_iterations, 0, kkt_ok
 
     def _damage_pfczm(self, H, lower, initial):
         """Projected Newton solve of the PF-CZM damage energy over ``lower <= d <= 1``

@@ -88,3 +88,28 @@ def test_projected_anderson_staggered_increments():
         assert rel(np.array(rec.macro_stress), g["st_sigma"][k]) < 1e-8
         assert rel(state.d.cpu(), g["st_d"][k]) < 1e-6
         assert rel(state.x.cpu(), g["st_x"][k]) < (1e-8 if k < 3 else 1e-5)
+
+
+def test_history_only_staggered_increments():
+    """irreversibility='history_only': the damage step without bounds and its violation statistics,
+    three increments of the 6^3 pore cell against the reference."""
+    from phast_b200.solid3d import LoadCase, PeriodicVoxelPhaseFieldOperator, SolverConfig, StaggeredSolver
+    from phast_b200.solid3d import sphere_pore_model
+    g = golden("history_only")
+    targets = tuple(float(v) for v in g["st_targets"])
+    op = PeriodicVoxelPhaseFieldOperator(
+        sphere_pore_model((6, 6, 6), 0.2),
+        LoadCase(name="zz", controlled=2, targets=targets, free=(), fixed_zero=(0, 1, 3, 4, 5)),
+        SolverConfig(device="cuda", kappa=1e-6, energy_split_isotropic="spectral", irreversibility="history_only"))
+    solver = StaggeredSolver(op)
+    state = solver.initial_state()
+    for k, target in enumerate(targets):
+        state, rec = solver.advance(state, target)
+        assert rec.stagger_iters == int(g["st_stag"][k]), k
+        assert (rec.pcg_iters_pf, rec.active_set_iters) == (int(g["st_pcg_pf"][k]), int(g["st_sets"][k])), k
+        assert abs(rec.pcg_iters_mech - int(g["st_pcg_mech"][k])) <= 2, k
+        assert rec.kkt_ok == bool(g["st_kkt"][k])
+        v = solver.last_bound_violations
+        assert [v["below_previous"], v["below_zero"], v["above_one"]] == [int(a) for a in g["st_viol"][k][:3]]
+        assert rel(np.array(rec.macro_stress), g["st_sigma"][k]) < 1e-8
+        assert rel(state.d.cpu(), g["st_d"][k]) < 1e-7 and rel(state.x.cpu(), g["st_x"][k]) < 1e-7
