@@ -469,8 +469,12 @@ PFCZM_F_PORE = PFCZM_F_MATRIX * 1e-3        # keeps the pore's a1 equal to the m
 PFCZM_CPU_BUDGET_S = 30.0
 
 
-def reference_pfczm_solver(n=PFCZM_N):
-    """The PF-CZM pore cell built with the reference's own classes (phast.solid3d)."""
+CLOSURE_TARGETS = (0.006, 0.012)
+
+
+def reference_law_solver(n, targets, *, pfczm=False, closure=False):
+    """The pore cell built with the reference's own classes (phast.solid3d), with the PF-CZM law
+    or the crack closure."""
     from phast.solid3d.model import (PHASE_ID, LoadCase, MaterialTable, PhaseMaterial, SolverConfig, VoxelGrid,
                                      VoxelModel)
     from phast.solid3d.operator import PeriodicVoxelPhaseFieldOperator
@@ -480,45 +484,56 @@ def reference_pfczm_solver(n=PFCZM_N):
     c = np.stack([(i + 0.5) / n - 0.5, (j + 0.5) / n - 0.5, (k + 0.5) / n - 0.5], -1)
     phase = np.full((n, n, n), PHASE_ID["mi_matrix"], dtype=np.uint8)
     phase[np.linalg.norm(c, axis=-1) < 0.2] = PHASE_ID["pore"]
+    fm, fp = (PFCZM_F_MATRIX, PFCZM_F_PORE) if pfczm else (None, None)
     phases = {"mi_matrix": PhaseMaterial(name="mi_matrix", kind="isotropic", Gc=0.5, driver="spectral", E=3000.0,
-                                         nu=0.35, tensile_strength=PFCZM_F_MATRIX),
+                                         nu=0.35, tensile_strength=fm),
               "pore": PhaseMaterial(name="pore", kind="isotropic", Gc=0.5, driver="spectral", E=3000.0 * 1e-6,
-                                    nu=0.35, tensile_strength=PFCZM_F_PORE)}
+                                    nu=0.35, tensile_strength=fp)}
     tangent = np.zeros((n, n, n, 3))
     tangent[..., 2] = 1.0
     model = VoxelModel(grid=VoxelGrid(shape=(n, n, n), h=(h, h, h)), phase_id=phase, tangent=tangent,
                        materials=MaterialTable(phases=phases, length_scale=2 * h, scale="micro"))
-    load = LoadCase(name="zz", controlled=2, targets=PFCZM_TARGETS, free=(), fixed_zero=(0, 1, 3, 4, 5))
-    cfg = SolverConfig(device="cpu", kappa=1e-6, energy_split_isotropic="spectral", damage_law="pfczm")
+    load = LoadCase(name="zz", controlled=2, targets=targets, free=(), fixed_zero=(0, 1, 3, 4, 5))
+    cfg = SolverConfig(device="cpu", kappa=1e-6, energy_split_isotropic="spectral",
+                       damage_law="pfczm" if pfczm else "at2", crack_closure="axes" if closure else "none")
     op = PeriodicVoxelPhaseFieldOperator(model, load, cfg)
     return op, StaggeredSolver(op)
 
 
-def run_pfczm(device, with_cpu, n=PFCZM_N):
-    """Bench line of the PF-CZM law: whole staggered increments 1-4 of the pore cell (plain FP64
-    mechanics, projected Newton damage solve), and the reference's increments on the host cores
-    with the fields compared where both ran."""
+_COUNT_FIELDS = ("stagger_iters", "newton_iters_pf", "closure_solves", "pcg_iters_mech", "pcg_iters_pf",
+                 "active_set_iters")
+
+
+def _counts(rec):
+    return {f: getattr(rec, f) for f in _COUNT_FIELDS if getattr(rec, f, None) is not None}
+
+
+def _run_law_line(device, with_cpu, n, targets, workload, form, *, pfczm=False, closure=False):
+    """Whole staggered increments of the pore cell with the PF-CZM law or the crack closure (plain
+    FP64 mechanics), and the reference's increments on the host cores with the fields compared where
+    both ran."""
     from phast_b200.solid3d import LoadCase, PeriodicVoxelPhaseFieldOperator, SolverConfig, StaggeredSolver
     from phast_b200.solid3d import sphere_pore_model
 
     def build():
-        model = sphere_pore_model((n, n, n), 0.2, tensile_strength=PFCZM_F_MATRIX,
-                                  pore_tensile_strength=PFCZM_F_PORE)
-        load = LoadCase(name="zz", controlled=2, targets=PFCZM_TARGETS, free=(), fixed_zero=(0, 1, 3, 4, 5))
-        cfg = SolverConfig(device=str(device), kappa=1e-6, energy_split_isotropic="spectral", damage_law="pfczm")
+        model = sphere_pore_model((n, n, n), 0.2, tensile_strength=PFCZM_F_MATRIX if pfczm else None,
+                                  pore_tensile_strength=PFCZM_F_PORE if pfczm else None)
+        load = LoadCase(name="zz", controlled=2, targets=targets, free=(), fixed_zero=(0, 1, 3, 4, 5))
+        cfg = SolverConfig(device=str(device), kappa=1e-6, energy_split_isotropic="spectral",
+                           damage_law="pfczm" if pfczm else "at2", crack_closure="axes" if closure else "none")
         op = PeriodicVoxelPhaseFieldOperator(model, load, cfg)
         return op, StaggeredSolver(op)
 
-    # warm-up: the first two increments on a separate solver (workspaces, library init)
+    # warm-up on a separate solver (workspaces, library init)
     op, solver = build()
     st = solver.initial_state()
-    for t in PFCZM_TARGETS[:2]:
+    for t in targets[:2]:
         st, _ = solver.advance(st, t)
     op, solver = build()
     state = solver.initial_state()
     states, recs, ms = [], [], []
     launches0 = _lib_launches()
-    for t in PFCZM_TARGETS:
+    for t in targets:
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -529,26 +544,19 @@ def run_pfczm(device, with_cpu, n=PFCZM_N):
         states.append(state)
         recs.append(rec)
     launches = _lib_launches() - launches0
-    line = {"workload": f"3D periodic pore cell {n}^3 (E 3000, nu 0.35, Gc 0.5, ell 2h, pore E x 1e-6), "
-                        f"damage_law 'pfczm' (linear softening, f_t {PFCZM_F_MATRIX:g} MPa), spectral split, "
-                        f"uniaxial zz strain increments {PFCZM_TARGETS}",
-            "dtype": "f64", "form": "plain FP64 mechanics (Jacobi PCG, PF-CZM g per Gauss point) + projected "
-                                    "Newton damage solve (box-KKT QP per step)",
-            "value": len(ms) / (sum(ms) / 1e3), "unit": "staggered increments/s", "ms_per_increment": ms,
-            "gpu_launches": int(launches),
-            "per_increment": [{"stagger": r.stagger_iters, "newton": r.newton_iters_pf, "pcg_mech": r.pcg_iters_mech,
-                               "pcg_pf": r.pcg_iters_pf, "active_sets": r.active_set_iters,
-                               "max_d": r.max_damage} for r in recs]}
+    line = {"workload": workload, "dtype": "f64", "form": form, "value": len(ms) / (sum(ms) / 1e3),
+            "unit": "staggered increments/s", "ms_per_increment": ms, "gpu_launches": int(launches),
+            "per_increment": [dict(_counts(r), max_d=r.max_damage) for r in recs]}
     if with_cpu:
         try:
             import torch as th
             import_reference()
             threads = os.cpu_count() or 1
             th.set_num_threads(threads)
-            rop, rsolver = reference_pfczm_solver(n)
+            rop, rsolver = reference_law_solver(n, targets, pfczm=pfczm, closure=closure)
             rstate = rsolver.initial_state()
             secs, rrecs = [], []
-            for k, t in enumerate(PFCZM_TARGETS):
+            for t in targets:
                 t0 = time.perf_counter()
                 rstate, rrec = rsolver.advance(rstate, t)
                 secs.append(time.perf_counter() - t0)
@@ -567,13 +575,8 @@ def run_pfczm(device, with_cpu, n=PFCZM_N):
             line["speedup_vs_reference_same_increments"] = sum(secs) / (ours_ms / 1e3)
             line["parity_vs_reference"] = {
                 "increments": len(secs),
-                "reference_per_increment": [{"stagger": r.stagger_iters, "newton": r.newton_iters_pf,
-                                             "pcg_mech": r.pcg_iters_mech, "pcg_pf": r.pcg_iters_pf,
-                                             "active_sets": r.active_set_iters} for r in rrecs],
-                "same_counts": all((a.stagger_iters, a.newton_iters_pf, a.pcg_iters_mech, a.pcg_iters_pf,
-                                    a.active_set_iters) == (b.stagger_iters, b.newton_iters_pf, b.pcg_iters_mech,
-                                                            b.pcg_iters_pf, b.active_set_iters)
-                                   for a, b in zip(recs, rrecs)),
+                "reference_per_increment": [_counts(r) for r in rrecs],
+                "same_counts": all(_counts(a) == _counts(b) for a, b in zip(recs, rrecs)),
                 "rel_err_x": rel(states[k].x.cpu().numpy(), rstate.x.numpy()),
                 "rel_err_d": rel(states[k].d.cpu().numpy(), rstate.d.numpy()) if float(rstate.d.abs().max()) > 0
                 else float(states[k].d.abs().max()),
@@ -581,6 +584,27 @@ def run_pfczm(device, with_cpu, n=PFCZM_N):
         except Exception as exc:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "sample": f"unavailable: {type(exc).__name__}: {exc}"}
     return line
+
+
+def run_pfczm(device, with_cpu, n=PFCZM_N):
+    """Bench line of the PF-CZM law: increments 1-4 of the pore cell through the onset of cracking."""
+    return _run_law_line(
+        device, with_cpu, n, PFCZM_TARGETS,
+        f"3D periodic pore cell {n}^3 (E 3000, nu 0.35, Gc 0.5, ell 2h, pore E x 1e-6), damage_law 'pfczm' "
+        f"(linear softening, f_t {PFCZM_F_MATRIX:g} MPa), spectral split, uniaxial zz strain increments "
+        f"{PFCZM_TARGETS}",
+        "plain FP64 mechanics (Jacobi PCG, PF-CZM g per Gauss point) + projected Newton damage solve (box-KKT QP "
+        "per step)", pfczm=True)
+
+
+def run_closure(device, with_cpu, n=PFCZM_N):
+    """Bench line of the crack closure: AT2 increments of the pore cell with crack_closure 'axes'."""
+    return _run_law_line(
+        device, with_cpu, n, CLOSURE_TARGETS,
+        f"3D periodic pore cell {n}^3 (E 3000, nu 0.35, Gc 0.5, ell 2h, pore E x 1e-6), AT2, spectral split, "
+        f"crack_closure 'axes', uniaxial zz strain increments {CLOSURE_TARGETS}",
+        "plain FP64 mechanics with the closure add-back (line-searched pattern iteration) + box-KKT damage",
+        closure=True)
 
 
 def _lib_launches():
@@ -947,10 +971,11 @@ def run_ours(args, rank, world, device):
         except Exception as exc:  # noqa: BLE001
             out.setdefault("configs", {})["cfg4"] = {"error": f"{type(exc).__name__}: {exc}"}
     if not args.no_2d:
-        try:
-            out.setdefault("configs", {})["pfczm"] = run_pfczm(device, world == 1 and rank == 0 and not args.no_cpu)
-        except Exception as exc:  # noqa: BLE001
-            out.setdefault("configs", {})["pfczm"] = {"error": f"{type(exc).__name__}: {exc}"}
+        for key, fn in (("pfczm", run_pfczm), ("closure", run_closure)):
+            try:
+                out.setdefault("configs", {})[key] = fn(device, world == 1 and rank == 0 and not args.no_cpu)
+            except Exception as exc:  # noqa: BLE001
+                out.setdefault("configs", {})[key] = {"error": f"{type(exc).__name__}: {exc}"}
     if world == 1 and rank == 0 and not args.no_cpu:
         try:
             secs, threads, recs = time_reference(args.steps, CPU_BASELINE_BUDGET_S)
@@ -1095,6 +1120,7 @@ def main():
     ap.add_argument("--cfg3-action", action="store_true", help="time the packed batch's elastic action alone")
     ap.add_argument("--cfg4-only", action="store_true", help="print the gradient line (cfg4) alone")
     ap.add_argument("--pfczm-only", action="store_true", help="print the PF-CZM line alone")
+    ap.add_argument("--closure-only", action="store_true", help="print the crack-closure line alone")
     ap.add_argument("--brick", default="16,8,8", help="brick ox,oy,kz of --cfg3-action")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -1112,6 +1138,9 @@ def main():
     torch.cuda.set_device(device)
     if args.pfczm_only:
         print(json.dumps(run_pfczm(device, not args.no_cpu)), flush=True)
+        return
+    if args.closure_only:
+        print(json.dumps(run_closure(device, not args.no_cpu)), flush=True)
         return
     if args.cfg4_only:
         print(json.dumps(run_cfg4(device)), flush=True)
