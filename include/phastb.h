@@ -485,6 +485,12 @@ int phastb_h8_damage_box_kkt(const phastb_voxel_grid* g, const phastb_voxel_mate
                              int max_lin, int max_active, double* d_out, int* info, void* workspace,
                              size_t workspace_bytes, void* stream);
 
+/* f = dF/du . du on T3: the consistent tangent of the split-aware internal force at u, the
+ * autograd JVP QuasiStaticSolver takes as its CG operator (mechanics_solver.py:1705-1733); the
+ * T3 counterpart of phastb_q4_tangent_apply.  d NULL means g = 1. */
+int phastb_t3_tangent_apply(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u,
+                            const double* du, const double* d, double* f, void* stream);
+
 /* ---- Anderson mixing of the staggered damage fixed point ----
  * Type II Anderson mixing of d = G(d) with the last depth + 1 pairs
  * (_AndersonAccelerator.step, solvers/staggered_solver.py:165-255).  hist holds

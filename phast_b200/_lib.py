@@ -146,6 +146,7 @@ SIGNATURES = {
     "phastb_h8_record_workspace_bytes": (sz, [VG]),
     "phastb_h8_increment_record": (C.c_int, [VG, VM, vp, vp, vp, vp, C.c_double, dp, vp, sz, vp]),
     "phastb_h8_increment_record_ex": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, C.c_double, PL, dp, vp, sz, vp]),
+    "phastb_t3_tangent_apply": (C.c_int, [T3M, Q4M, vp, vp, vp, vp, vp]),
     "phastb_anderson_workspace_bytes": (sz, [C.c_int]),
     "phastb_anderson_step": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, C.c_double, vp, ip, vp,
                                        sz, vp]),

@@ -125,6 +125,23 @@ static int t3_force_op(const void* c, const double* x, double* y, const int* gua
   return t3_force_launch(k->mesh, k->m, x, k->d, y, k->mask, guard, s);
 }
 
+int t3_tangent_launch(const phastb_t3_mesh& mesh, const phastb_q4_material& m, const double* u, const double* du,
+                      const double* d, double* f, const uint8_t* mask, const int* guard, cudaStream_t s);
+
+// The consistent tangent at the Newton iterate `u` on T3 (as Q4TangentCtx).
+struct T3TangentCtx {
+  phastb_t3_mesh mesh;
+  phastb_q4_material m;
+  const double* d;
+  const uint8_t* mask;
+  const double* u;
+};
+
+static int t3_tangent_op(const void* c, const double* x, double* y, const int* guard, cudaStream_t s) {
+  const T3TangentCtx* k = static_cast<const T3TangentCtx*>(c);
+  return t3_tangent_launch(k->mesh, k->m, k->u, x, k->d, y, k->mask, guard, s);
+}
+
 static int t3_force_eval(const void* c, const double* u, double* f, cudaStream_t s) {
   const T3ForceCtx* k = static_cast<const T3ForceCtx*>(c);
   return t3_force_launch(k->mesh, k->m, u, k->d, f, nullptr, nullptr, s);
@@ -394,8 +411,6 @@ int phastb_t3_qs_solve(const phastb_t3_mesh* mesh, const phastb_q4_material* m, 
                        double ls_c, int* info, void* workspace, size_t workspace_bytes, void* stream) {
   if (!t3_valid_mesh(mesh) || !m || !d || !bc_mask || !bc_vals || !u || cg_max_iter < 1 || max_iter < 0)
     return PHASTB_ERR_ARG;
-  if (m->stress_split != PHASTB_SPLIT_ISOTROPIC && m->stress_split != PHASTB_SPLIT_LINEAR)
-    return PHASTB_UNSUPPORTED;
   const int n2 = 2 * mesh->n_nodes;
   if (!workspace || workspace_bytes < phastb_t3_qs_workspace_bytes(mesh->n_nodes)) return PHASTB_ERR_WORKSPACE;
   ScopedStream scope((cudaStream_t)stream);
@@ -406,7 +421,18 @@ int phastb_t3_qs_solve(const phastb_t3_mesh* mesh, const phastb_q4_material* m, 
   std::memcpy(&kctx.m, m, offsetof(phastb_q4_material, psi_split) + sizeof(int));
   kctx.d = d;
   kctx.mask = bc_mask;
-  LinOp<double> K{t3_force_op, &kctx, sizeof(kctx)};
+  // the splits whose stress is not linear in the strain take the consistent tangent (as on Q4)
+  const int sp = m->stress_split;
+  const bool tangent = sp == PHASTB_SPLIT_AMOR || sp == PHASTB_SPLIT_SPECTRAL || sp == PHASTB_SPLIT_STAR_CONVEX;
+  T3TangentCtx tctx;
+  std::memset(&tctx, 0, sizeof(tctx));
+  tctx.mesh = *mesh;
+  std::memcpy(&tctx.m, m, offsetof(phastb_q4_material, psi_split) + sizeof(int));
+  tctx.d = d;
+  tctx.mask = bc_mask;
+  tctx.u = u;
+  LinOp<double> K = tangent ? LinOp<double>{t3_tangent_op, &tctx, sizeof(tctx)}
+                            : LinOp<double>{t3_force_op, &kctx, sizeof(kctx)};
   return qs_newton(n2, K, t3_force_eval, &kctx, f_ext, bc_mask, bc_vals, u, tol, cg_tol, cg_max_iter, max_iter,
                    line_search, ls_max_steps, ls_min_alpha, ls_c, info, workspace, scope.get());
 }

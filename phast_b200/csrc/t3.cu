@@ -72,6 +72,41 @@ __global__ void __launch_bounds__(kThreads) t3_force_colour(T3Dev t, Mat2<double
   }
 }
 
+// Consistent tangent: f_a += A (dsigma(eps(u); eps(du)) . grad phi_a) for the elements of one
+// colour, the directional derivative of the split stress at the iterate u (dstress2), at the
+// element-mean degradation of the force kernel.  The autograd JVP of internal_force that
+// QuasiStaticSolver takes as its CG operator (mechanics_solver.py:1705-1733), on T3.
+__global__ void __launch_bounds__(kThreads) t3_tangent_colour(T3Dev t, Mat2<double> m, int split,
+                                                              const double* __restrict__ u,
+                                                              const double* __restrict__ du,
+                                                              const double* __restrict__ d, double* f, int k0,
+                                                              int k1, const int* guard) {
+  if (guard && *guard == 0) return;
+  const int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= k1) return;
+  const int e = __ldg(t.order + k);
+  int n[3];
+  double gp[3][2], exx, eyy, gxy;
+  t3_strain(t, e, u, exx, eyy, gxy, n, gp);
+  double vxx = 0.0, vyy = 0.0, vxy = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double vx = du[2 * n[a]], vy = du[2 * n[a] + 1];
+    vxx += gp[a][0] * vx;
+    vyy += gp[a][1] * vy;
+    vxy += gp[a][1] * vx + gp[a][0] * vy;
+  }
+  const double g = d ? degr(m, (__ldg(d + n[0]) + __ldg(d + n[1]) + __ldg(d + n[2])) / 3.0) : 1.0;
+  double sxx, syy, sxy;
+  dstress2(m, split, exx, eyy, gxy, vxx, vyy, vxy, g, sxx, syy, sxy);
+  const double A = __ldg(t.areas + e);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    f[2 * n[a]] += A * (sxx * gp[a][0] + sxy * gp[a][1]);
+    f[2 * n[a] + 1] += A * (sxy * gp[a][0] + syy * gp[a][1]);
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) t3_psi_kernel(T3Dev t, Mat2<double> m, const double* __restrict__ u,
                                                           const double* __restrict__ Hin, double* __restrict__ Hout,
                                                           double* __restrict__ psi, int ne) {
@@ -406,6 +441,21 @@ int t3_force_launch(const phastb_t3_mesh& mesh, const phastb_q4_material& m, con
   return last_launch_status();
 }
 
+int t3_tangent_launch(const phastb_t3_mesh& mesh, const phastb_q4_material& m, const double* u, const double* du,
+                      const double* d, double* f, const uint8_t* mask, const int* guard, cudaStream_t s) {
+  const int n2 = 2 * mesh.n_nodes;
+  { note_launch(); t3_zero_kernel<<<grid_for(n2), kThreads, 0, s>>>(n2, f, guard); }
+  const T3Dev t = t3_dev(mesh);
+  const Mat2<double> mm = make_mat2<double>(m);
+  for (int c = 0; c < mesh.n_colors; ++c) {
+    const int k0 = mesh.color_off[c], k1 = mesh.color_off[c + 1];
+    if (k1 <= k0) continue;
+    { note_launch(); t3_tangent_colour<<<grid_full(k1 - k0), kThreads, 0, s>>>(t, mm, m.stress_split, u, du, d, f, k0, k1, guard); }
+  }
+  if (mask) { note_launch(); t3_mask_rows_kernel<<<grid_for(n2), kThreads, 0, s>>>(n2, mask, f, guard); }
+  return last_launch_status();
+}
+
 namespace {
 
 // Damage operator context for the Krylov engines.  The mesh is held by value;
@@ -629,6 +679,12 @@ int phastb_t3_damage_adjoint_grads(const phastb_t3_mesh* mesh, const double* lam
   { note_launch(); t3_damage_adjoint_kernel<<<grid_full(ne), kThreads, 0, (cudaStream_t)stream>>>(
       t3_dev(*mesh), lam, d, l0, grad_gc_e, grad_H, lam_K_d_e, lam_M_d_e, ne); }
   return last_launch_status();
+}
+
+int phastb_t3_tangent_apply(const phastb_t3_mesh* mesh, const phastb_q4_material* m, const double* u,
+                            const double* du, const double* d, double* f, void* stream) {
+  if (!t3_valid_mesh(mesh) || !m || !u || !du || !f) return PHASTB_ERR_ARG;
+  return t3_tangent_launch(*mesh, *m, u, du, d, f, nullptr, nullptr, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -122,10 +122,6 @@ class QuasiStaticSolver:
         if tol_rel is not None:
             raise NotImplementedError("relative Newton tolerance is not implemented by the B200 backend")
         split = stress_split_of(fem.material)
-        if split != "isotropic" and getattr(fem, "t3", None) is not None:
-            raise NotImplementedError(
-                f"quasi-static mechanics on T3 meshes with the {split!r} split is not implemented by the B200 "
-                "backend (the consistent-tangent kernel is structured-Q4); use energy_split='isotropic'")
         if consistent_tangent is False and split in ("spectral", "amor", "star_convex"):
             raise NotImplementedError("the secant (frozen-state) linearisation is not implemented by the B200 "
                                       "backend; the consistent tangent is used")
