@@ -515,38 +515,55 @@ def _run_law_line(device, with_cpu, n, targets, workload, form, *, pfczm=False, 
     from phast_b200.solid3d import LoadCase, PeriodicVoxelPhaseFieldOperator, SolverConfig, StaggeredSolver
     from phast_b200.solid3d import sphere_pore_model
 
-    def build():
+    from phast_b200.solid3d.staggered import PLAIN
+
+    def build(mech_form=PLAIN):
         model = sphere_pore_model((n, n, n), 0.2, tensile_strength=PFCZM_F_MATRIX if pfczm else None,
                                   pore_tensile_strength=PFCZM_F_PORE if pfczm else None)
         load = LoadCase(name="zz", controlled=2, targets=targets, free=(), fixed_zero=(0, 1, 3, 4, 5))
         cfg = SolverConfig(device=str(device), kappa=1e-6, energy_split_isotropic="spectral",
                            damage_law="pfczm" if pfczm else "at2", crack_closure="axes" if closure else "none")
         op = PeriodicVoxelPhaseFieldOperator(model, load, cfg)
-        return op, StaggeredSolver(op)
+        return op, StaggeredSolver(op, form=mech_form)
 
-    # warm-up on a separate solver (workspaces, library init)
-    op, solver = build()
-    st = solver.initial_state()
-    for t in targets[:2]:
-        st, _ = solver.advance(st, t)
-    op, solver = build()
-    state = solver.initial_state()
-    states, recs, ms = [], [], []
-    launches0 = _lib_launches()
-    for t in targets:
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        state, rec = solver.advance(state, t)
-        e1.record()
-        torch.cuda.synchronize()
-        ms.append(e0.elapsed_time(e1))
-        states.append(state)
-        recs.append(rec)
-    launches = _lib_launches() - launches0
+    def timed(mech_form=PLAIN):
+        # warm-up on a separate solver (workspaces, library init), then the timed increments
+        op, solver = build(mech_form)
+        st = solver.initial_state()
+        for t in targets[:2]:
+            st, _ = solver.advance(st, t)
+        op, solver = build(mech_form)
+        state = solver.initial_state()
+        states, recs, ms = [], [], []
+        launches0 = _lib_launches()
+        for t in targets:
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            state, rec = solver.advance(state, t)
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            states.append(state)
+            recs.append(rec)
+        return states, recs, ms, _lib_launches() - launches0
+
+    states, recs, ms, launches = timed()
     line = {"workload": workload, "dtype": "f64", "form": form, "value": len(ms) / (sum(ms) / 1e3),
             "unit": "staggered increments/s", "ms_per_increment": ms, "gpu_launches": int(launches),
             "per_increment": [dict(_counts(r), max_d=r.max_damage) for r in recs]}
+    if pfczm:
+        # the multigrid and FP32 forms take the PF-CZM g as a Gauss-point field
+        chosen = forms()["mixed-gmg"]
+        c_states, c_recs, c_ms, c_launches = timed(chosen)
+        rel_ = lambda a, b: float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))  # noqa: E731
+        line["chosen_form"] = {
+            "form": "FP32 PCG + FP32 3-level multigrid under FP64 refinement (PF-CZM g per Gauss point in every "
+                    "level), projected Newton damage solve",
+            "value": len(c_ms) / (sum(c_ms) / 1e3), "ms_per_increment": c_ms, "gpu_launches": int(c_launches),
+            "speedup_vs_plain_fp64": sum(ms) / sum(c_ms),
+            "rel_err_vs_plain_fp64": {"x": rel_(c_states[-1].x, states[-1].x), "d": rel_(c_states[-1].d, states[-1].d)},
+            "per_increment": [_counts(r) for r in c_recs]}
     if with_cpu:
         try:
             import torch as th

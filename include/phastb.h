@@ -474,6 +474,16 @@ int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_mater
                             double* x_out, int* info, double* rinfo, void* workspace,
                             size_t workspace_bytes, void* stream);
 
+/* phastb_h8_mech_solve_ex with a Gauss-point degradation gq (E,8) in every operator (the fine
+ * action, the smoother, the Jacobi diagonal and the coarse moduli) in place of g(d): the
+ * multigrid and FP32 forms for the PF-CZM law, whose g is not the AT2 g(d). */
+size_t phastb_h8_mech_solve_ex_g_workspace_bytes(const phastb_voxel_grid* g, const phastb_mech_opts* o);
+int phastb_h8_mech_solve_ex_g(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                              const double* gq, const uint8_t* fixed, const double* fixed_values, const double* x0,
+                              double rtol, double atol, int maxiter, int check_every, const phastb_mech_opts* o,
+                              double* lmax_io, double* x_out, int* info, double* rinfo, void* workspace,
+                              size_t workspace_bytes, void* stream);
+
 /* Box-constrained damage solve lower <= d <= upper by the primal active-set method
  * with a Dirichlet PCG per set (scale applied to the system).
  * solve_h8_scalar_box_kkt + solve_h8_scalar_dirichlet_pcg, solvers/box_kkt_h8.py:256-778.

@@ -139,6 +139,9 @@ SIGNATURES = {
     "phastb_h8_mech_solve_ex_workspace_bytes": (sz, [VG, MO]),
     "phastb_h8_mech_solve_ex": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_int, MO,
                                           dp, vp, ip, dp, vp, sz, vp]),
+    "phastb_h8_mech_solve_ex_g_workspace_bytes": (sz, [VG, MO]),
+    "phastb_h8_mech_solve_ex_g": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_int,
+                                            MO, dp, vp, ip, dp, vp, sz, vp]),
     "phastb_h8_box_kkt_workspace_bytes": (sz, [VG]),
     "phastb_h8_damage_box_kkt": (C.c_int, [VG, VM, vp, vp, C.c_double, vp, C.c_double, vp, C.c_double, C.c_double,
                                            C.c_int, C.c_int, vp, ip, vp, sz, vp]),

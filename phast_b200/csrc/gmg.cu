@@ -58,13 +58,20 @@ __device__ __forceinline__ void elem_ijk2(const VoxGeom& g, int e, int& ie, int&
 // fine voxel, stored at the coarse Gauss point that voxel hosts.
 template <typename T>
 __global__ void gmg_coef_from_fine(VoxGeom f, VoxGeom c, VoxMat<T> m, const uint8_t* __restrict__ slot,
-                                   const T* __restrict__ d, T* __restrict__ lam_c, T* __restrict__ mu_c) {
+                                   const T* __restrict__ d, const T* __restrict__ gq, T* __restrict__ lam_c,
+                                   T* __restrict__ mu_c) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < f.n_elem; e += gridDim.x * blockDim.x) {
     int ie, je, ke;
     elem_ijk2(f, e, ie, je, ke);
     const int s = slot[e];
     T gm = T(1);
-    if (d) {
+    if (gq) {
+      // the mean of the given Gauss-point degradation
+      gm = T(0);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) gm += __ldg(gq + 8 * (size_t)e + q);
+      gm *= T(0.125);
+    } else if (d) {
       int nd[8];
       vox_corners(f, ie, je, ke, nd);
       T dd[8], dq[8];
@@ -501,6 +508,7 @@ struct Gmg {
   VoxMat<T> mat;
   const uint8_t* slot;
   const T* dfield;       // fine-level damage (T) for g(d), may be null
+  const T* gfield;       // fine-level Gauss-point degradation (E,8), used instead of g(d) when set
   const uint8_t* mask;   // fine-level mask: fixed dofs + E rows
   const uint8_t* fmask;  // the solve's own fixed mask (for the E block)
   void* scratch;         // element scratch (fine size)
@@ -538,6 +546,7 @@ static int level_cheb(const Gmg<T>& M, int l, const T* din, T* dout, double c1, 
   if (l == 0) {
     a.slot = M.slot;
     a.d = M.dfield;
+    a.gq = M.gfield;
     a.mask = M.mask;
     return h8_tile_launch<T>(a, M.mat, M.mat.iso ? kCoefIso : kCoefAniso, kModeCheb, s);
   }
@@ -554,6 +563,7 @@ static int level_apply(const Gmg<T>& M, int l, const T* x, T* y, cudaStream_t s)
     TileArgs<T> a = tile_args<T>(M.lv[0].g, 0);
     a.slot = M.slot;
     a.d = M.dfield;
+    a.gq = M.gfield;
     a.x = x;
     a.y = y;
     a.mask = M.mask;
@@ -733,12 +743,14 @@ static char* gmg_carve(Gmg<T>& M, const VoxGeom& f, int levels, char* p) {
 // Chebyshev bounds).  `fixed` is the solve's mask over the n_mech rows.
 template <typename T>
 static int gmg_setup(Gmg<T>& M, const VoxMat<T>& mat, const uint8_t* slot, const T* dfield, const uint8_t* fixed,
-                     int deg, int deg_coarse, int power_iters, double safety, double* lmax_io, cudaStream_t s) {
+                     int deg, int deg_coarse, int power_iters, double safety, double* lmax_io, cudaStream_t s,
+                     const T* gfield = nullptr) {
   int st;
   M.safety = safety;
   M.mat = mat;
   M.slot = slot;
   M.dfield = dfield;
+  M.gfield = gfield;
   M.fmask = fixed;
   M.deg = deg;
   M.deg_coarse = deg_coarse;
@@ -750,14 +762,15 @@ static int gmg_setup(Gmg<T>& M, const VoxMat<T>& mat, const uint8_t* slot, const
   RedWs sw = red_ws(static_cast<char*>(M.scratch) + (h8_scratch_bytes(f, sizeof(T) == 4 ? PHASTB_F32 : PHASTB_F64) -
                                                       red_ws_bytes()));
   if ((st = cuda_status(cudaMemsetAsync(sw.counter, 0, sizeof(unsigned), s)))) return st;
-  if ((st = h8_mech_diag_t<T>(f, mat, slot, nullptr, dfield, M.lv[0].diag, M.scratch, s))) return st;
+  if ((st = h8_mech_diag_t<T>(f, mat, slot, gfield, dfield, M.lv[0].diag, M.scratch, s))) return st;
   { note_launch(); gmg_invert<T><<<grid_for(nm), kThreads, 0, s>>>(nm, M.lv[0].diag, M.mask, M.lv[0].invd); }
   for (int l = 1; l < M.nlev; ++l) {
     const GmgLevel<T>& F = M.lv[l - 1];
     GmgLevel<T>& C = M.lv[l];
     if (l == 1) {
       note_launch();
-      gmg_coef_from_fine<T><<<grid_for(F.g.n_elem), kThreads, 0, s>>>(F.g, C.g, mat, slot, dfield, C.lam, C.mu);
+      gmg_coef_from_fine<T><<<grid_for(F.g.n_elem), kThreads, 0, s>>>(F.g, C.g, mat, slot, dfield, gfield, C.lam,
+                                                                         C.mu);
     } else {
       note_launch();
       gmg_coef_from_coarse<T><<<grid_for(F.g.n_elem), kThreads, 0, s>>>(F.g, C.g, F.lam, F.mu, C.lam, C.mu);
@@ -807,7 +820,7 @@ int gmg_level_coefs_f32(const VoxGeom& f, const VoxGeom& c, const VoxMat<float>&
                         const float* d, const float* lam_f, const float* mu_f, float* lam_c, float* mu_c,
                         cudaStream_t s) {
   if (!lam_f)
-    { note_launch(); gmg_coef_from_fine<float><<<grid_for(f.n_elem), kThreads, 0, s>>>(f, c, m, slot, d, lam_c, mu_c); }
+    { note_launch(); gmg_coef_from_fine<float><<<grid_for(f.n_elem), kThreads, 0, s>>>(f, c, m, slot, d, nullptr, lam_c, mu_c); }
   else
     { note_launch(); gmg_coef_from_coarse<float><<<grid_for(f.n_elem), kThreads, 0, s>>>(f, c, lam_f, mu_f, lam_c, mu_c); }
   return last_launch_status();
@@ -849,18 +862,19 @@ struct MechOpT {
   const T* d;
   const uint8_t* mask;
   void* scratch;
+  const T* gq;  // Gauss-point degradation (E,8) used instead of g(d) when set
 };
 
 template <typename T>
 static int mech_op_t(const void* c, const T* x, T* y, const int* guard, cudaStream_t s) {
   const MechOpT<T>* k = static_cast<const MechOpT<T>*>(c);
-  return h8_mech_apply_t<T>(k->v, k->m, k->slot, x, nullptr, k->d, k->mask, y, k->scratch, guard, s);
+  return h8_mech_apply_t<T>(k->v, k->m, k->slot, x, k->gq, k->d, k->mask, y, k->scratch, guard, s);
 }
 
 template <typename T>
 static int mech_op_dot_t(const void* c, const T* x, T* y, const int* guard, cudaStream_t s) {
   const MechOpT<T>* k = static_cast<const MechOpT<T>*>(c);
-  return h8_mech_apply_dot_t<T>(k->v, k->m, k->slot, x, nullptr, k->d, k->mask, y, k->scratch, guard, s);
+  return h8_mech_apply_dot_t<T>(k->v, k->m, k->slot, x, k->gq, k->d, k->mask, y, k->scratch, guard, s);
 }
 
 __global__ void ex_setup_kernel(int n, const uint8_t* __restrict__ fixed, const double* __restrict__ vals,
@@ -906,7 +920,8 @@ struct ExLayout {
   PcgWs<float> w32;
   double *xc, *bf, *r64;
   double *d64, *x64;  // workspace copies of the damage field and the FP64 iterate (stable graph pointers)
-  float *d32, *r32, *dx32, *inv32;
+  double* gq64;       // workspace copy of a Gauss-point degradation (E,8), when one is given
+  float *d32, *r32, *dx32, *inv32, *gq32;
   void* scratch64;
   RedWs rw;
   Gmg<double> g64;
@@ -914,7 +929,7 @@ struct ExLayout {
   size_t bytes;
 };
 
-static ExLayout ex_layout(const VoxGeom& v, const phastb_mech_opts& o, char* base) {
+static ExLayout ex_layout(const VoxGeom& v, const phastb_mech_opts& o, char* base, bool with_gq = false) {
   ExLayout L{};
   char* p = base;
   const int n = 3 * v.n_red + 6;
@@ -930,6 +945,10 @@ static ExLayout ex_layout(const VoxGeom& v, const phastb_mech_opts& o, char* bas
   L.x64 = reinterpret_cast<double*>(take(sizeof(double) * n));
   L.scratch64 = take(h8_scratch_bytes(v, PHASTB_F64));
   L.rw = red_ws(take(red_ws_bytes()));
+  if (with_gq) {
+    L.gq64 = reinterpret_cast<double*>(take(sizeof(double) * 8 * (size_t)v.n_elem));
+    if (o.mixed) L.gq32 = reinterpret_cast<float*>(take(sizeof(float) * 8 * (size_t)v.n_elem));
+  }
   if (!o.mixed) {
     L.w64 = pcg_ws<double>(p, n);
     p += align_up(pcg_ws_bytes<double>(n));
@@ -981,17 +1000,21 @@ size_t phastb_h8_mech_solve_ex_workspace_bytes(const phastb_voxel_grid* g, const
   return ex_layout(v, *o, nullptr).bytes;
 }
 
-int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
-                            const double* d, const uint8_t* fixed, const double* fixed_values, const double* x0,
-                            double rtol, double atol, int maxiter, int check_every, const phastb_mech_opts* o,
-                            double* lmax_io, double* x_out, int* info, double* rinfo, void* workspace,
-                            size_t workspace_bytes, void* stream) {
+}  // extern "C"
+
+// The extended solve with the damage field d (g(d) of AT2 in every operator) or, when gq is
+// given, a Gauss-point degradation (E,8) in its place (the PF-CZM law's g).
+static int mech_solve_ex_impl(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                              const double* d, const double* gq, const uint8_t* fixed, const double* fixed_values,
+                              const double* x0, double rtol, double atol, int maxiter, int check_every,
+                              const phastb_mech_opts* o, double* lmax_io, double* x_out, int* info, double* rinfo,
+                              void* workspace, size_t workspace_bytes, void* stream) {
   if (!valid_vox(g) || !valid_mat(m) || !slot || !fixed || !fixed_values || !x_out || maxiter < 1 ||
       check_every < 1 || !(rtol >= 0) || !(atol >= 0) || (rtol == 0 && atol == 0))
     return PHASTB_ERR_ARG;
   const VoxGeom v = make_vox_geom(*g);
   if (!opts_ok(o, v)) return PHASTB_ERR_ARG;
-  ExLayout L = ex_layout(v, *o, static_cast<char*>(workspace));
+  ExLayout L = ex_layout(v, *o, static_cast<char*>(workspace), gq != nullptr);
   if (!workspace || workspace_bytes < L.bytes) return PHASTB_ERR_WORKSPACE;
   ScopedStream scope((cudaStream_t)stream);
   if (scope.status()) return scope.status();
@@ -1007,8 +1030,12 @@ int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_mater
   if (d && (st = cuda_status(cudaMemcpyAsync(L.d64, d, sizeof(double) * v.n_red, cudaMemcpyDeviceToDevice, s))))
     return st;
   const double* dd = d ? L.d64 : nullptr;
-  MechOpT<double> full{v, m64, slot, dd, nullptr, L.scratch64};
-  MechOpT<double> freeop{v, m64, slot, dd, fixed, L.scratch64};
+  if (gq && (st = cuda_status(cudaMemcpyAsync(L.gq64, gq, sizeof(double) * 8 * (size_t)v.n_elem,
+                                               cudaMemcpyDeviceToDevice, s))))
+    return st;
+  const double* gg = gq ? L.gq64 : nullptr;
+  MechOpT<double> full{v, m64, slot, dd, nullptr, L.scratch64, gg};
+  MechOpT<double> freeop{v, m64, slot, dd, fixed, L.scratch64, gg};
   if ((st = mech_op_t<double>(&full, L.xc, L.r64, nullptr, s))) return st;
   { note_launch(); ex_rhs_kernel<<<G, kThreads, 0, s>>>(n, fixed, nullptr, L.r64, L.bf, L.rw); }
   if ((st = last_launch_status())) return st;
@@ -1032,7 +1059,7 @@ int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_mater
     PcgResult pr{};
     if (o->precond) {
       if ((st = gmg_setup<double>(L.g64, m64, slot, dd, fixed, o->smooth_degree, o->coarse_degree, o->power_iters,
-                                  o->lmax_safety, lmax_io, s)))
+                                  o->lmax_safety, lmax_io, s, gg)))
         return st;
       Precond<double> M{gmg_precond_apply<double>, &L.g64, sizeof(L.g64)};
       if ((st = cuda_status(cudaMemcpyAsync(L.x64, x_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, s))))
@@ -1041,7 +1068,7 @@ int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_mater
                                 &pr, s)))
         return st;
     } else {
-      if ((st = h8_mech_diag_t<double>(v, m64, slot, nullptr, dd, L.r64, L.scratch64, s))) return st;
+      if ((st = h8_mech_diag_t<double>(v, m64, slot, gg, dd, L.r64, L.scratch64, s))) return st;
       { note_launch(); gmg_invert<double><<<G, kThreads, 0, s>>>(n, L.r64, fixed, L.r64); }
       if ((st = cuda_status(cudaMemcpyAsync(L.x64, x_out, sizeof(double) * n, cudaMemcpyDeviceToDevice, s))))
         return st;
@@ -1061,19 +1088,25 @@ int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_mater
   }
   // FP32 inner PCG (FP64 dot products) + FP64 iterative refinement
   const VoxMat<float> m32 = make_vox_mat<float>(*m);
-  { note_launch(); gmg_convert<double, float><<<grid_for(v.n_red), kThreads, 0, s>>>(v.n_red, dd, L.d32); }
+  if (dd) { note_launch(); gmg_convert<double, float><<<grid_for(v.n_red), kThreads, 0, s>>>(v.n_red, dd, L.d32); }
+  const float* d32 = dd ? L.d32 : nullptr;
+  if (gg) {
+    const long long ne8 = 8LL * v.n_elem;
+    { note_launch(); gmg_convert<double, float><<<grid_for(ne8), kThreads, 0, s>>>((int)ne8, gg, L.gq32); }
+  }
+  const float* g32 = gg ? L.gq32 : nullptr;
   void* scratch32 = L.g32.scratch;
   if (o->precond) {
-    if ((st = gmg_setup<float>(L.g32, m32, slot, L.d32, fixed, o->smooth_degree, o->coarse_degree, o->power_iters,
-                                 o->lmax_safety, lmax_io, s)))
+    if ((st = gmg_setup<float>(L.g32, m32, slot, d32, fixed, o->smooth_degree, o->coarse_degree, o->power_iters,
+                                 o->lmax_safety, lmax_io, s, g32)))
       return st;
   } else {
     RedWs s32 = red_ws(static_cast<char*>(scratch32) + h8_scratch_bytes(v, PHASTB_F32) - red_ws_bytes());
     if ((st = red_ws_reset(s32, s))) return st;
-    if ((st = h8_mech_diag_t<float>(v, m32, slot, nullptr, L.d32, L.inv32, scratch32, s))) return st;
+    if ((st = h8_mech_diag_t<float>(v, m32, slot, g32, d32, L.inv32, scratch32, s))) return st;
     { note_launch(); ex_invert_f<<<G, kThreads, 0, s>>>(n, L.inv32, fixed, L.inv32); }
   }
-  MechOpT<float> free32{v, m32, slot, L.d32, fixed, scratch32};
+  MechOpT<float> free32{v, m32, slot, d32, fixed, scratch32, g32};
   LinOp<float> A32{mech_op_t<float>, &free32, sizeof(free32), mech_op_dot_t<float>,
                    h8_apply_dot_slot(v, 4, scratch32)};
   Precond<float> M32{gmg_precond_apply<float>, &L.g32, sizeof(L.g32)};
@@ -1121,6 +1154,34 @@ int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_mater
   if (info) { info[0] = total; info[1] = converged; }
   if (rinfo) rinfo[1] = rn;
   return converged ? PHASTB_OK : PHASTB_NONCONVERGED;
+}
+
+extern "C" {
+
+int phastb_h8_mech_solve_ex(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                            const double* d, const uint8_t* fixed, const double* fixed_values, const double* x0,
+                            double rtol, double atol, int maxiter, int check_every, const phastb_mech_opts* o,
+                            double* lmax_io, double* x_out, int* info, double* rinfo, void* workspace,
+                            size_t workspace_bytes, void* stream) {
+  return mech_solve_ex_impl(g, m, slot, d, nullptr, fixed, fixed_values, x0, rtol, atol, maxiter, check_every, o,
+                            lmax_io, x_out, info, rinfo, workspace, workspace_bytes, stream);
+}
+
+size_t phastb_h8_mech_solve_ex_g_workspace_bytes(const phastb_voxel_grid* g, const phastb_mech_opts* o) {
+  if (!valid_vox(g)) return 0;
+  const VoxGeom v = make_vox_geom(*g);
+  if (!opts_ok(o, v)) return 0;
+  return ex_layout(v, *o, nullptr, true).bytes;
+}
+
+int phastb_h8_mech_solve_ex_g(const phastb_voxel_grid* g, const phastb_voxel_material* m, const uint8_t* slot,
+                              const double* gq, const uint8_t* fixed, const double* fixed_values, const double* x0,
+                              double rtol, double atol, int maxiter, int check_every, const phastb_mech_opts* o,
+                              double* lmax_io, double* x_out, int* info, double* rinfo, void* workspace,
+                              size_t workspace_bytes, void* stream) {
+  if (!gq) return PHASTB_ERR_ARG;
+  return mech_solve_ex_impl(g, m, slot, nullptr, gq, fixed, fixed_values, x0, rtol, atol, maxiter, check_every, o,
+                            lmax_io, x_out, info, rinfo, workspace, workspace_bytes, stream);
 }
 
 }  // extern "C"

@@ -304,18 +304,21 @@ def solve_constrained_form(op, form, *, fixed_mask, fixed_values, d=None, x0=Non
     lambda_max estimates from one solve to the next.
     """
     plain = form.precond == "jacobi" and not form.mixed
+    gq = None
     if getattr(op, "is_pfczm", False) and d is not None:
-        # the PF-CZM degradation enters the elastic action as g (E, 8)
-        if not plain:
-            raise NotImplementedError("damage_law 'pfczm' runs the plain FP64 mechanics form only")
-        return _solve_fused(op, fixed_mask=fixed_mask, fixed_values=fixed_values, g=op.degradation(d), x0=x0,
-                            rtol=rtol, atol=atol, maxiter=maxiter, check_every=check_every)
+        # the PF-CZM degradation enters every operator as g (E, 8)
+        gq = op.degradation(d).contiguous()
+        if plain:
+            return _solve_fused(op, fixed_mask=fixed_mask, fixed_values=fixed_values, g=gq, x0=x0, rtol=rtol,
+                                atol=atol, maxiter=maxiter, check_every=check_every)
     if plain:
         return _solve_fused(op, fixed_mask=fixed_mask, fixed_values=fixed_values, d=d, x0=x0, rtol=rtol,
                             atol=atol, maxiter=maxiter, check_every=check_every)
     n = op.n_mech
     opts = form.struct()
-    nbytes = _lib.load().phastb_h8_mech_solve_ex_workspace_bytes(op.vgrid, opts)
+    lib = _lib.load()
+    nbytes = (lib.phastb_h8_mech_solve_ex_workspace_bytes(op.vgrid, opts) if gq is None
+              else lib.phastb_h8_mech_solve_ex_g_workspace_bytes(op.vgrid, opts))
     if nbytes == 0:
         raise NotImplementedError(f"mechanics form {form} is not available for a {op.shape} grid "
                                   "(multigrid needs edges divisible by 2^(levels-1))")
@@ -328,9 +331,14 @@ def solve_constrained_form(op, form, *, fixed_mask, fixed_values, d=None, x0=Non
     info = (C.c_int * 2)()
     rinfo = (C.c_double * 2)()
     wp, wn = op._ws.get(nbytes)
-    st = raw("phastb_h8_mech_solve_ex", op.vgrid, op.mat, ptr(op.slot), ptr(dd), ptr(mask), ptr(vals), ptr(x0c),
-             float(rtol), float(atol), int(maxiter), int(check_every), opts, lmax_cache, ptr(out), info, rinfo, wp, wn,
-             stream())
+    if gq is None:
+        st = raw("phastb_h8_mech_solve_ex", op.vgrid, op.mat, ptr(op.slot), ptr(dd), ptr(mask), ptr(vals), ptr(x0c),
+                 float(rtol), float(atol), int(maxiter), int(check_every), opts, lmax_cache, ptr(out), info, rinfo,
+                 wp, wn, stream())
+    else:
+        st = raw("phastb_h8_mech_solve_ex_g", op.vgrid, op.mat, ptr(op.slot), ptr(gq), ptr(mask), ptr(vals),
+                 ptr(x0c), float(rtol), float(atol), int(maxiter), int(check_every), opts, lmax_cache, ptr(out), info,
+                 rinfo, wp, wn, stream())
     if st in (_lib.BREAKDOWN, _lib.NONFINITE):
         raise PCGBreakdownError(f"PCG breakdown (status {st})")
     if st not in (_lib.OK, _lib.NONCONVERGED):
@@ -604,8 +612,6 @@ class StaggeredSolver:
         bad = unsupported_options(cfg)
         if bad:
             raise NotImplementedError(f"the B200 backend does not run {', '.join(bad)}")
-        if op.is_pfczm and (form.precond != "jacobi" or form.mixed):
-            raise NotImplementedError("damage_law 'pfczm' runs the plain FP64 mechanics form only")
         if op.has_closure and cfg.anderson_depth > 0:
             raise ValueError("Anderson mixing (anderson_depth > 0) is not available with crack_closure 'axes'")
         if op.has_closure and (form.precond != "jacobi" or form.mixed):

@@ -106,15 +106,62 @@ def test_pfczm_staggered_increments():
 
 
 def test_pfczm_refuses_what_it_does_not_run():
-    from phast_b200.solid3d import StaggeredSolver
-    from phast_b200.solid3d.staggered import MechForm
-    g = golden("pfczm")
-    op, _ = _op(g)
-    with pytest.raises(NotImplementedError):
-        StaggeredSolver(op, form=MechForm(precond="gmg"))
     with pytest.raises(ValueError, match="onset condition"):
         from phast_b200.solid3d import LoadCase, PeriodicVoxelPhaseFieldOperator, SolverConfig, sphere_pore_model
         model = sphere_pore_model((6, 6, 6), 0.2, tensile_strength=200.0, pore_tensile_strength=0.03)
         PeriodicVoxelPhaseFieldOperator(model, LoadCase(name="zz", controlled=2, targets=(0.01,), free=(),
                                                         fixed_zero=(0, 1, 3, 4, 5)),
                                         SolverConfig(device="cuda", damage_law="pfczm"))
+
+
+def _cell16():
+    from phast_b200.solid3d import LoadCase, PeriodicVoxelPhaseFieldOperator, SolverConfig, sphere_pore_model
+    model = sphere_pore_model((16, 16, 16), 0.2, tensile_strength=30.0, pore_tensile_strength=0.03)
+    targets = (0.004, 0.007, 0.009)
+    load = LoadCase(name="zz", controlled=2, targets=targets, free=(), fixed_zero=(0, 1, 3, 4, 5))
+    cfg = SolverConfig(device="cuda", kappa=1e-6, energy_split_isotropic="spectral", damage_law="pfczm",
+                       pcg_rtol_mech=1e-12, damage_linear_tol=1e-12)
+    return PeriodicVoxelPhaseFieldOperator(model, load, cfg), cfg, targets
+
+
+def test_pfczm_multigrid_and_fp32_forms_match_plain():
+    """The multigrid and FP32 forms take the PF-CZM g in every operator (fine action, smoother,
+    diagonal, coarse moduli): the same FP64 solution as the plain Jacobi solve."""
+    from phast_b200.solid3d.staggered import MechForm, _solve_fused, solve_constrained_form
+    op, _, _ = _cell16()
+    rng = np.random.default_rng(5)
+    d = _t(np.clip(rng.uniform(-0.3, 0.9, size=op.n_red), 0, 1))
+    mask = op.mech_fixed_mask().to(torch.uint8).contiguous()
+    vals = op.mech_fixed_values(0.004)
+    x1, info = _solve_fused(op, fixed_mask=mask, fixed_values=vals, g=op.degradation(d), rtol=1e-12, maxiter=20000)
+    assert info.converged
+    for form in (MechForm(precond="gmg", mixed=True, smooth_degree=1, coarse_degree=6, inner_rtol=1e-5),
+                 MechForm(precond="gmg"), MechForm(mixed=True)):
+        x, inf = solve_constrained_form(op, form, fixed_mask=mask, fixed_values=vals, d=d, rtol=1e-10, maxiter=20000)
+        assert inf.converged and inf.relative_residual <= 1e-10, form
+        assert rel(x.cpu(), x1.cpu()) < 1e-7, form
+        if form.precond == "gmg":
+            assert inf.iterations * 4 < info.iterations, (form, inf.iterations, info.iterations)
+
+
+def test_pfczm_staggered_chosen_form_matches_plain():
+    """Three PF-CZM increments of a 16^3 cell with FP32 + multigrid mechanics under FP64 refinement
+    take the plain FP64 solver's decisions with the same fields (tight solver tolerances)."""
+    from phast_b200.solid3d import StaggeredSolver
+    from phast_b200.solid3d.staggered import PLAIN, MechForm
+    op, cfg, targets = _cell16()
+    runs = []
+    for form in (PLAIN, MechForm(precond="gmg", mixed=True, smooth_degree=1, coarse_degree=6, inner_rtol=1e-5)):
+        solver = StaggeredSolver(op, cfg=cfg, form=form)
+        state = solver.initial_state()
+        recs = []
+        for t in targets:
+            state, rec = solver.advance(state, t)
+            recs.append(rec)
+        runs.append((state, recs))
+    (s0, r0), (s1, r1) = runs
+    assert float(s0.d.max()) > 0.0
+    for a, b in zip(r0, r1):
+        assert (a.stagger_iters, a.newton_iters_pf) == (b.stagger_iters, b.newton_iters_pf)
+        assert rel(np.array(b.macro_stress), np.array(a.macro_stress)) < 1e-7
+    assert rel(s1.d.cpu(), s0.d.cpu()) < 1e-6 and rel(s1.x.cpu(), s0.x.cpu()) < 1e-6
