@@ -639,11 +639,12 @@ int phastb_h8_closure_energy(const phastb_voxel_grid* g, const phastb_voxel_mate
                              const double* x, const double* gq, const uint8_t* pattern, double* out_host,
                              void* workspace, size_t workspace_bytes, void* stream);
 
-/* out_host = [smallest element-mean normal strain, smallest principal value of the element-mean
- * strains, smallest Gauss-point det(I + grad u)].  kinematic_guard, operator.py:1713-1770;
- * workspace phastb_reduce_workspace_bytes. */
-int phastb_h8_kinematic_guard(const phastb_voxel_grid* g, const double* x, double* out_host, void* workspace,
-                              size_t workspace_bytes, void* stream);
+/* out_host[0..2] = [smallest element-mean normal strain, smallest principal value of the
+ * element-mean strains, smallest Gauss-point det(I + grad u)], out_host[3..5] the same over the
+ * elements whose mean nodal damage exceeds threshold (+inf when there are none or d is NULL).
+ * kinematic_guard, operator.py:1713-1770; workspace phastb_reduce_workspace_bytes. */
+int phastb_h8_kinematic_guard(const phastb_voxel_grid* g, const double* x, const double* d, double threshold,
+                              double* out_host, void* workspace, size_t workspace_bytes, void* stream);
 
 /* The constrained mechanics solve of phastb_h8_mech_solve with the closure add-back of a fixed
  * pattern in the operator and in its Jacobi diagonal (the linear solve of each closure pattern

@@ -161,7 +161,7 @@ SIGNATURES = {
     "phastb_h8_closure_apply_add": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
     "phastb_h8_closure_diagonal_add": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, sz, vp]),
     "phastb_h8_closure_energy": (C.c_int, [VG, VM, vp, vp, vp, vp, dp, vp, sz, vp]),
-    "phastb_h8_kinematic_guard": (C.c_int, [VG, vp, dp, vp, sz, vp]),
+    "phastb_h8_kinematic_guard": (C.c_int, [VG, vp, vp, C.c_double, dp, vp, sz, vp]),
     "phastb_h8_mech_solve_closure_workspace_bytes": (sz, [VG]),
     "phastb_h8_mech_solve_closure": (C.c_int, [VG, VM, vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int,
                                                C.c_int, vp, ip, dp, vp, sz, vp]),

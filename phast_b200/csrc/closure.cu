@@ -255,8 +255,11 @@ __global__ void __launch_bounds__(kThreads) cl_gather_add_kernel(VoxGeom g, cons
 }
 
 // ws.out = [min element-mean normal strain, min principal value of the element-mean strain,
-// min Gauss-point det(I + E + grad u~)] (kinematic_guard, operator.py:1713-1770).
-__global__ void __launch_bounds__(kThreads) kin_guard_kernel(VoxGeom g, const double* __restrict__ x, RedWs ws) {
+// min Gauss-point det(I + E + grad u~), the same three over the damaged elements (mean nodal
+// damage > threshold; +inf when there are none)] (kinematic_guard, operator.py:1713-1770).
+__global__ void __launch_bounds__(kThreads) kin_guard_kernel(VoxGeom g, const double* __restrict__ x,
+                                                             const double* __restrict__ d, double threshold,
+                                                             RedWs ws) {
   const double* Ex = x + 3 * (size_t)g.n_red;
   double E6[6];
 #pragma unroll
@@ -265,7 +268,7 @@ __global__ void __launch_bounds__(kThreads) kin_guard_kernel(VoxGeom g, const do
   const double Em[3][3] = {{E6[0], 0.5 * E6[5], 0.5 * E6[4]},
                            {0.5 * E6[5], E6[1], 0.5 * E6[3]},
                            {0.5 * E6[4], 0.5 * E6[3], E6[2]}};
-  double mn = INFINITY, mp = INFINITY, md = INFINITY;
+  double mn = INFINITY, mp = INFINITY, md = INFINITY, dn = INFINITY, dp = INFINITY, dd = INFINITY;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.n_elem; e += gridDim.x * blockDim.x) {
     int ie, je, ke;
     elem_ijk(g, e, ie, je, ke);
@@ -274,6 +277,7 @@ __global__ void __launch_bounds__(kThreads) kin_guard_kernel(VoxGeom g, const do
     ElemGrad G;
     elem_grad(g, x, nd, G);
     double eps[6] = {0, 0, 0, 0, 0, 0};
+    double emin_det = INFINITY;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       double F[3][3];
@@ -284,7 +288,7 @@ __global__ void __launch_bounds__(kThreads) kin_guard_kernel(VoxGeom g, const do
       const double det = F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) -
                          F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
                          F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
-      md = fmin(md, det);
+      emin_det = fmin(emin_det, det);
       eps[0] += G.at(0, 0, q) + E6[0];
       eps[1] += G.at(1, 1, q) + E6[1];
       eps[2] += G.at(2, 2, q) + E6[2];
@@ -294,28 +298,37 @@ __global__ void __launch_bounds__(kThreads) kin_guard_kernel(VoxGeom g, const do
     }
 #pragma unroll
     for (int i = 0; i < 6; ++i) eps[i] *= 0.125;
-    mn = fmin(mn, fmin(eps[0], fmin(eps[1], eps[2])));
+    const double en = fmin(eps[0], fmin(eps[1], eps[2]));
     double ev[3];
     eig3(eps[0], eps[1], eps[2], 0.5 * eps[5], 0.5 * eps[4], 0.5 * eps[3], ev);
+    mn = fmin(mn, en);
     mp = fmin(mp, ev[0]);
+    md = fmin(md, emin_det);
+    if (d) {
+      double dm = 0.0;
+#pragma unroll
+      for (int L = 0; L < 8; ++L) dm += __ldg(d + nd[L]);
+      if (dm / 8.0 > threshold) {
+        dn = fmin(dn, en);
+        dp = fmin(dp, ev[0]);
+        dd = fmin(dd, emin_det);
+      }
+    }
   }
   __shared__ double sh[32];
-  const double b0 = block_min(mn, sh), b1 = block_min(mp, sh), b2 = block_min(md, sh);
-  if (threadIdx.x == 0) {
-    ws.part[blockIdx.x] = b0;
-    ws.part[kMaxPartials + blockIdx.x] = b1;
-    ws.part[2 * kMaxPartials + blockIdx.x] = b2;
+  const double v[6] = {mn, mp, md, dn, dp, dd};
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const double b = block_min(v[k], sh);
+    if (threadIdx.x == 0) ws.part[k * kMaxPartials + blockIdx.x] = b;
   }
   if (arrive_last(ws.counter)) {
-    const double t0 = fold_min(ws.part, gridDim.x, sh);
-    const double t1 = fold_min(ws.part + kMaxPartials, gridDim.x, sh);
-    const double t2 = fold_min(ws.part + 2 * kMaxPartials, gridDim.x, sh);
-    if (threadIdx.x == 0) {
-      ws.out[0] = t0;
-      ws.out[1] = t1;
-      ws.out[2] = t2;
-      *ws.counter = 0u;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const double t = fold_min(ws.part + k * kMaxPartials, gridDim.x, sh);
+      if (threadIdx.x == 0) ws.out[k] = t;
     }
+    if (threadIdx.x == 0) *ws.counter = 0u;
   }
 }
 
@@ -436,8 +449,8 @@ int phastb_h8_closure_energy(const phastb_voxel_grid* g, const phastb_voxel_mate
   return red_ws_fetch(ws, out_host, 4, s);
 }
 
-int phastb_h8_kinematic_guard(const phastb_voxel_grid* g, const double* x, double* out_host, void* workspace,
-                              size_t workspace_bytes, void* stream) {
+int phastb_h8_kinematic_guard(const phastb_voxel_grid* g, const double* x, const double* d, double threshold,
+                              double* out_host, void* workspace, size_t workspace_bytes, void* stream) {
   if (!valid_vox(g) || !x || !out_host) return PHASTB_ERR_ARG;
   if (!workspace || workspace_bytes < red_ws_bytes()) return PHASTB_ERR_WORKSPACE;
   const VoxGeom v = make_vox_geom(*g);
@@ -445,9 +458,9 @@ int phastb_h8_kinematic_guard(const phastb_voxel_grid* g, const double* x, doubl
   RedWs ws = red_ws(workspace);
   int st = red_ws_reset(ws, s);
   if (st) return st;
-  { note_launch(); kin_guard_kernel<<<grid_for(v.n_elem), kThreads, 0, s>>>(v, x, ws); }
+  { note_launch(); kin_guard_kernel<<<grid_for(v.n_elem), kThreads, 0, s>>>(v, x, d, threshold, ws); }
   if ((st = last_launch_status())) return st;
-  return red_ws_fetch(ws, out_host, 3, s);
+  return red_ws_fetch(ws, out_host, 6, s);
 }
 
 }  // extern "C"

@@ -531,12 +531,21 @@ class PeriodicVoxelPhaseFieldOperator:
 
     def kinematic_guard(self, x, d):
         """Smallest element-mean normal strain, principal strain of the element-mean strain and
-        Gauss-point ``det(I + grad u)`` of state ``x`` (operator.py:1713-1770)."""
+        Gauss-point ``det(I + grad u)`` of state ``x``, and the same over the elements whose mean nodal
+        damage exceeds ``cfg.damaged_threshold`` (``damaged_*``, None when there are none)
+        (operator.py:1713-1770)."""
         x = self._check("x", x, (self.n_mech,), torch.float64)
-        out = (C.c_double * 3)()
+        d = self._check("d", d, (self.n_red,), torch.float64)
+        out = (C.c_double * 6)()
         wp, wn = self._kgws.get(_lib.load().phastb_reduce_workspace_bytes())
-        call("phastb_h8_kinematic_guard", self.vgrid, ptr(x), out, wp, wn, stream())
-        return {"min_normal_strain": float(out[0]), "min_principal_strain": float(out[1]), "min_det_F": float(out[2])}
+        call("phastb_h8_kinematic_guard", self.vgrid, ptr(x), ptr(d), float(self.cfg.damaged_threshold), out, wp, wn,
+             stream())
+        v = [float(a) for a in out]
+        damaged = math.isfinite(v[3])
+        return {"min_normal_strain": v[0], "min_principal_strain": v[1], "min_det_F": v[2],
+                "damaged_min_normal_strain": v[3] if damaged else None,
+                "damaged_min_principal_strain": v[4] if damaged else None,
+                "damaged_min_det_F": v[5] if damaged else None}
 
     def driving_force(self, x):
         """Undamaged driving energy Y (E, 8) (operator.py:1415-1444)."""

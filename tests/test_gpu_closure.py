@@ -46,6 +46,12 @@ def test_closure_operators():
     guard = op.kinematic_guard(x, d)
     assert rel(np.array([guard["min_normal_strain"], guard["min_principal_strain"], guard["min_det_F"]]),
                g["guard"]) < 1e-12
+    # the damaged_* minima: none without damage, the overall minima when every element is damaged
+    none = op.kinematic_guard(x, torch.zeros_like(d))
+    assert none["damaged_min_det_F"] is None and none["damaged_min_normal_strain"] is None
+    full = op.kinematic_guard(x, torch.ones_like(d))
+    for key in ("min_normal_strain", "min_principal_strain", "min_det_F"):
+        assert full["damaged_" + key] == full[key]
     # a pattern is refused without the closure
     from phast_b200.solid3d import LoadCase, PeriodicVoxelPhaseFieldOperator, SolverConfig, sphere_pore_model
     plain = PeriodicVoxelPhaseFieldOperator(sphere_pore_model((5, 4, 6), 0.3),
