@@ -418,7 +418,7 @@ def lognormal_gc(nx, ny, mean=2.7, cov=0.2, corr=4.0, seed=0):
     return np.exp(np.log(mean) - 0.5 * s2 + np.sqrt(s2) * g).reshape(-1)
 
 
-def run_cfg4(device, steps=CFG4_STEPS):
+def run_cfg4(device, steps=CFG4_STEPS, with_cpu=False):
     """Bench line of cfg4: d(peak reaction)/d(Gc field) of the 256 x 256 SENT run through the
     hand-written reverse pass (checkpoint every 10 load steps), on load steps 1..steps of 50."""
     import phast_b200 as pb
@@ -454,7 +454,24 @@ def run_cfg4(device, steps=CFG4_STEPS):
             "objective": float(res.objective), "peak_step": int(res.peak_step),
             "staggered_passes": [int(v) for v in res.passes][:steps],
             "grad_norm": float(torch.linalg.vector_norm(g)), "grad_finite": bool(torch.isfinite(g).all()),
-            "check": "central differences (1e-4 relative) and PhAST's autograd gradient in tests/test_gpu_adjoint_qs.py"}
+            "check": "central differences (1e-4 relative) and PhAST's autograd gradient in tests/test_gpu_adjoint_qs.py",
+            **(_cfg4_reference(load, steps, fwd_ms) if with_cpu else {})}
+
+
+def _cfg4_reference(load, steps, fwd_ms):
+    """The reference's forward quasi-static steps on the same 256 x 256 SENT (uniform Gc, the field's
+    mean; its autograd gradient is not timed), load steps 1-2, beside this forward."""
+    try:
+        secs, threads = _time_reference_2d(CFG4, 2, load)
+        ours = steps / (fwd_ms / 1e3)
+        return {"cpu_baseline": {
+                    "value": len(secs) / sum(secs), "unit": "load steps/s (forward only)", "cores": threads,
+                    "kind": "reference",
+                    "sample": f"PhAST {PHAST_VERSION} StaggeredSolver.step_full (FP64, torch CPU) on the same mesh "
+                              f"with Gc uniform at 2.7, load steps 1-2 ({', '.join(f'{x:.1f}' for x in secs)} s)"},
+                "forward_speedup_vs_reference": ours / (len(secs) / sum(secs))}
+    except Exception as exc:  # noqa: BLE001
+        return {"cpu_baseline": {"value": None, "sample": f"unavailable: {type(exc).__name__}: {exc}"}}
 
 
 # ---------------------------------------------------------------------------
@@ -723,7 +740,50 @@ def _one_cell_at_a_time(ops, load, cfg, form, increments):
     return ms, last
 
 
-def run_cfg3(device, flush, n_cells=128, increments=CFG3_INCREMENTS, per_cell=True):
+CFG3_CPU_BUDGET_S = 40.0
+
+
+def reference_cfg3_cells(cells, load, increments, budget_s):
+    """The reference's solid3d solver on one batch cell per edge size (smallest first), whole
+    increments 1..K, until the budget is spent.  Returns [(N, seconds per increment)]."""
+    import torch as th
+    import_reference()
+    from phast.solid3d.model import (PHASE_ID, LoadCase, MaterialTable, PhaseMaterial, SolverConfig, VoxelGrid,
+                                     VoxelModel)
+    from phast.solid3d.operator import PeriodicVoxelPhaseFieldOperator
+    from phast.solid3d.staggered import StaggeredSolver
+    from phast_b200.solid3d import batch as bt
+    th.set_num_threads(os.cpu_count() or 1)
+    names = [p.name for p in bt.BATCH_PHASES]
+    ids = np.array([PHASE_ID[nm] for nm in names], dtype=np.uint8)
+    phases = {p.name: PhaseMaterial(name=p.name, kind="isotropic", Gc=p.Gc, driver="spectral", E=p.E, nu=p.nu)
+              for p in bt.BATCH_PHASES}
+    ref_load = LoadCase(name=load.name, controlled=load.controlled, targets=tuple(load.targets),
+                        free=tuple(load.free), fixed_zero=tuple(load.fixed_zero))
+    out, spent = [], 0.0
+    for n in sorted({c.n for c in cells}):
+        cell = next(c for c in cells if c.n == n)
+        h = 1.0 / n
+        tangent = np.zeros((n, n, n, 3))
+        tangent[..., 2] = 1.0
+        model = VoxelModel(grid=VoxelGrid(shape=(n, n, n), h=(h, h, h)), phase_id=ids[cell.phase], tangent=tangent,
+                           materials=MaterialTable(phases=phases, length_scale=2 * h, scale="micro"))
+        cfg = SolverConfig(device="cpu", kappa=1e-6, energy_split_isotropic="spectral")
+        solver = StaggeredSolver(PeriodicVoxelPhaseFieldOperator(model, ref_load, cfg))
+        state = solver.initial_state()
+        secs = []
+        for k in range(increments):
+            t0 = time.perf_counter()
+            state, _ = solver.advance(state, ref_load.targets[k])
+            secs.append(time.perf_counter() - t0)
+        out.append((n, sum(secs) / len(secs)))
+        spent += sum(secs)
+        if spent + 8.0 * out[-1][1] * increments > budget_s:  # the next size takes about twice as long
+            break
+    return out, th.get_num_threads()
+
+
+def run_cfg3(device, flush, n_cells=128, increments=CFG3_INCREMENTS, per_cell=True, with_cpu=False):
     """Bench line of cfg3: the seeded particle-in-cube batch advanced as one packed batch (every
     cell in one launch per operator apply, per multigrid step and per Krylov vector step), load
     increments 1..K of every cell from the initial state; beside the batch with Jacobi PCG and
@@ -800,6 +860,19 @@ def run_cfg3(device, flush, n_cells=128, increments=CFG3_INCREMENTS, per_cell=Tr
         line["speedup_vs_plain_fp64"] = plain_ms / total_ms
         line["rel_err_macro_stress_vs_plain_fp64"] = worst_err(recs[-1], plain_last)
         line["rel_err_macro_stress_jacobi_vs_plain_fp64"] = worst_err(jac_recs[-1], plain_last)
+    if with_cpu:
+        try:
+            per_size, threads = reference_cfg3_cells(cells, load, increments, CFG3_CPU_BUDGET_S)
+            ref_rate = len(per_size) / sum(t for _, t in per_size)  # cell increments/s over the sampled cells
+            line["cpu_baseline"] = {
+                "value": ref_rate, "unit": "cell increments/s", "cores": threads, "kind": "reference",
+                "sample": f"PhAST {PHAST_VERSION} phast.solid3d.StaggeredSolver.advance (FP64, torch CPU) on one "
+                          f"batch cell per edge size, smallest first, increments 1-{increments}: "
+                          + ", ".join(f"N={n}: {t:.1f} s per increment" for n, t in per_size)
+                          + " (the larger cells are slower, so the batch's true reference rate is lower)"}
+            line["speedup_vs_reference_lower_bound"] = line["value"] / ref_rate
+        except Exception as exc:  # noqa: BLE001
+            line["cpu_baseline"] = {"value": None, "sample": f"unavailable: {type(exc).__name__}: {exc}"}
     return line
 
 
@@ -979,12 +1052,13 @@ def run_ours(args, rank, world, device):
     # and does not cost the headline
     if args.cfg3_cells > 0:
         try:
-            out.setdefault("configs", {})["cfg3"] = run_cfg3(device, flush, n_cells=args.cfg3_cells)
+            out.setdefault("configs", {})["cfg3"] = run_cfg3(device, flush, n_cells=args.cfg3_cells,
+                                                             with_cpu=world == 1 and rank == 0 and not args.no_cpu)
         except Exception as exc:  # noqa: BLE001
             out.setdefault("configs", {})["cfg3"] = {"error": f"{type(exc).__name__}: {exc}"}
     if not args.no_2d:
         try:
-            out.setdefault("configs", {})["cfg4"] = run_cfg4(device)
+            out.setdefault("configs", {})["cfg4"] = run_cfg4(device, with_cpu=world == 1 and rank == 0 and not args.no_cpu)
         except Exception as exc:  # noqa: BLE001
             out.setdefault("configs", {})["cfg4"] = {"error": f"{type(exc).__name__}: {exc}"}
     if not args.no_2d:
@@ -1160,7 +1234,7 @@ def main():
         print(json.dumps(run_closure(device, not args.no_cpu)), flush=True)
         return
     if args.cfg4_only:
-        print(json.dumps(run_cfg4(device)), flush=True)
+        print(json.dumps(run_cfg4(device, with_cpu=not args.no_cpu)), flush=True)
         return
     if args.cfg3_action:
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
@@ -1169,7 +1243,7 @@ def main():
         return
     if args.cfg3_only:
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
-        print(json.dumps(run_cfg3(device, flush, n_cells=args.cfg3_cells)), flush=True)
+        print(json.dumps(run_cfg3(device, flush, n_cells=args.cfg3_cells, with_cpu=not args.no_cpu)), flush=True)
         return
     if args.kernel_only:
         if args.damage_cg:
