@@ -25,6 +25,7 @@ DRIVER_NONE, DRIVER_FULL, DRIVER_SPECTRAL = 0, 1, 2  # model.py:52
 DRIVER_INTERFACE = 3
 MATERIAL_KINDS = ("isotropic", "smeared_laminate")
 DRIVER_NAMES = ("spectral", "full", "none", "interface")
+_PFCZM_EXPONENTS = {"linear": 2, "exponential": 2.5}  # Wu's softening exponents (physics/pfczm.py:12)
 
 
 def _set(obj, name, value):
@@ -387,6 +388,40 @@ class SolverConfig:
         if isinstance(self.anderson_depth, bool) or int(self.anderson_depth) != self.anderson_depth or \
                 self.anderson_depth < 0:
             raise ValueError(f"anderson_depth must be an integer >= 0, got {self.anderson_depth!r}")
+        _set(self, "anderson_depth", int(self.anderson_depth))
+        _set(self, "damaged_threshold", threshold)
+        # the cross-option rules of solid3d/model.py:840-895: a mix needs two residuals, the
+        # closure's line-searched mechanics is not covered by the mixing safeguard, the
+        # variational band stress is the derivative of the interface split, and the PF-CZM
+        # settings belong to that law (its exponent fixed by the softening curve)
+        start = self.anderson_start
+        if isinstance(start, bool) or int(start) != start or start < 2:
+            raise ValueError(f"anderson_start must be an integer >= 2 (a mix needs two staggered residuals), "
+                             f"got {start!r}")
+        _set(self, "anderson_start", int(start))
+        if self.band_stress == "variational" and self.energy_split_band != "interface":
+            raise ValueError("band_stress 'variational' needs energy_split_band 'interface'")
+        if self.crack_closure != "none" and self.anderson_depth > 0:
+            raise ValueError("crack_closure 'axes' is not available with Anderson mixing (anderson_depth > 0)")
+        p = self.pfczm_p
+        if isinstance(p, bool) or not isinstance(p, (int, float)) or not math.isfinite(p) or p < 2:
+            raise ValueError(f"pfczm_p must be a number >= 2, got {p!r}")
+        p = int(p) if float(p).is_integer() else float(p)
+        _set(self, "pfczm_p", p)
+        _set(self, "pfczm_max_newton", _positive_int("pfczm_max_newton", self.pfczm_max_newton))
+        if self.damage_law == "at2":
+            changed = [k for k in ("pfczm_softening", "pfczm_p", "pfczm_max_newton")
+                       if getattr(self, k) != getattr(SolverConfig, k)]
+            if changed:
+                raise ValueError(f"{', '.join(changed)} apply to damage_law 'pfczm' only")
+        else:
+            if self.irreversibility != "box_kkt":
+                raise ValueError("damage_law 'pfczm' needs irreversibility 'box_kkt' (the crack function "
+                                 "2d - d^2 is unbounded below for d < 0)")
+            wu_p = _PFCZM_EXPONENTS[self.pfczm_softening]
+            if p != wu_p:
+                raise ValueError(f"pfczm_softening {self.pfczm_softening!r} is Wu's law with pfczm_p = {wu_p}, "
+                                 f"got {p!r}")
 
 
 def unsupported_options(cfg):

@@ -30,3 +30,27 @@ def test_pfczm_softening_parameters():
     assert abs(a2 - (2.0 ** (5.0 / 3.0) - 3.0)) < 1e-15 and a3 == 0.0
     with pytest.raises(ValueError):
         pfczm_softening_parameters("cubic")
+
+
+@pytest.mark.parametrize("kw", [dict(anderson_start=1), dict(anderson_start=True),
+                                dict(crack_closure="axes", anderson_depth=2),
+                                dict(band_stress="variational"),
+                                dict(pfczm_p=1.5, damage_law="pfczm"), dict(pfczm_p=float("nan"), damage_law="pfczm"),
+                                dict(pfczm_p=2.5), dict(pfczm_softening="exponential"), dict(pfczm_max_newton=50),
+                                dict(damage_law="pfczm", pfczm_max_newton=0),
+                                dict(damage_law="pfczm", irreversibility="history_only"),
+                                dict(damage_law="pfczm", pfczm_p=2.5),
+                                dict(damage_law="pfczm", pfczm_softening="exponential")])
+def test_invalid_combinations_raise(kw):
+    # the reference's SolverConfig refuses the same settings (solid3d/model.py:840-895)
+    with pytest.raises(ValueError):
+        SolverConfig(**kw)
+
+
+def test_valid_combinations_normalise():
+    cfg = SolverConfig(damage_law="pfczm", pfczm_softening="exponential", pfczm_p=2.5, pfczm_max_newton=40)
+    assert cfg.pfczm_p == 2.5 and cfg.pfczm_max_newton == 40
+    cfg = SolverConfig(damage_law="pfczm", pfczm_p=2.0)
+    assert cfg.pfczm_p == 2 and isinstance(cfg.pfczm_p, int)
+    cfg = SolverConfig(energy_split_band="interface", band_stress="variational", anderson_depth=2.0, anderson_start=3.0)
+    assert cfg.anderson_depth == 2 and isinstance(cfg.anderson_start, int)
