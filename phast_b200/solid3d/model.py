@@ -317,10 +317,12 @@ class LoadCase:
 class SolverConfig:
     """Numerical settings of the staggered solve (model.py:706-897); defaults are PhAST's.
 
-    The GPU backend runs ``dtype='float64'`` results (the chosen mechanics form may compute
-    in FP32 under FP64 refinement; see ``StaggeredSolver(form=...)``), ``damage_law`` 'at2' or 'pfczm',
-    ``irreversibility`` 'box_kkt' or 'history_only', ``history`` 'max' or 'current', ``crack_closure`` 'none' or 'axes' and
-    ``anderson_depth`` 0-6; ``device`` names the CUDA device.
+    ``dtype`` is 'float64' only, as in the reference (the chosen mechanics form may compute in
+    FP32 under FP64 refinement; see ``StaggeredSolver(form=...)``).  The GPU backend runs
+    ``damage_law`` 'at2' or 'pfczm', ``irreversibility`` 'box_kkt' or 'history_only', ``history``
+    'max' or 'current', ``crack_closure`` 'none' or 'axes' and ``anderson_depth`` 0-6; ``device``
+    names the CUDA device (the default here, where the reference's is 'cpu').  Invalid settings
+    and combinations raise the reference's ``ValueError`` at construction.
     """
     device: str = "cuda"
     dtype: str = "float64"
@@ -374,7 +376,18 @@ class SolverConfig:
         threshold = _finite("damaged_threshold", self.damaged_threshold)
         if not 0.0 < threshold <= 1.0:
             raise ValueError("damaged_threshold must lie in (0, 1]")
-        _choice("dtype", self.dtype, ("float64", "float32"))
+        # the reference refuses every dtype but float64 and every device but cpu/cuda at
+        # construction (model.py:806-809, 683-700, 1441-1446)
+        if not (self.dtype == "float64" or self.dtype is torch.float64):
+            raise ValueError(f"only float64 is supported, got {self.dtype!r}")
+        try:
+            dev = torch.device(self.device)
+        except (RuntimeError, TypeError) as exc:
+            raise ValueError(f"device must be cpu or cuda, got {self.device!r}") from exc
+        if dev.type not in ("cpu", "cuda"):
+            raise ValueError(f"device must be cpu or cuda, got {self.device!r}")
+        if self.num_threads is not None:
+            _positive_int("num_threads", self.num_threads)
         _choice("preconditioner", self.preconditioner, ("jacobi",))
         _choice("irreversibility", self.irreversibility, ("box_kkt", "history_only"))
         _choice("history", self.history, ("max", "current"))
@@ -431,8 +444,6 @@ def unsupported_options(cfg):
         out.append(f"anderson_depth={cfg.anderson_depth!r} (the B200 backend mixes at most 6 pairs)")
     if getattr(cfg, "energy_split_band", "isotropic") != "isotropic":
         out.append(f"energy_split_band={cfg.energy_split_band!r}")
-    if getattr(cfg, "dtype", "float64") != "float64":
-        out.append(f"dtype={cfg.dtype!r}")
     return out
 
 

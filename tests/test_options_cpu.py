@@ -16,8 +16,7 @@ def test_run_options_are_accepted(kw):
 
 
 @pytest.mark.parametrize("kw,name", [(dict(anderson_depth=7), "anderson_depth"),
-                                     (dict(energy_split_band="interface"), "energy_split_band"),
-                                     (dict(dtype="float32"), "dtype")])
+                                     (dict(energy_split_band="interface"), "energy_split_band")])
 def test_other_options_are_named(kw, name):
     bad = unsupported_options(SolverConfig(**kw))
     assert len(bad) == 1 and bad[0].startswith(name)
@@ -32,7 +31,8 @@ def test_pfczm_softening_parameters():
         pfczm_softening_parameters("cubic")
 
 
-@pytest.mark.parametrize("kw", [dict(anderson_start=1), dict(anderson_start=True),
+@pytest.mark.parametrize("kw", [dict(anderson_start=1), dict(anderson_start=True), dict(dtype="float32"),
+                                dict(device="mps"), dict(device="tpu:0"), dict(num_threads=0),
                                 dict(crack_closure="axes", anderson_depth=2),
                                 dict(band_stress="variational"),
                                 dict(pfczm_p=1.5, damage_law="pfczm"), dict(pfczm_p=float("nan"), damage_law="pfczm"),
