@@ -152,9 +152,20 @@ class PhaseMaterial:
         _choice(f"{self.name}: driver", self.driver, DRIVER_NAMES)
         _set(self, "Gc", _positive(f"{self.name}: Gc", self.Gc))
         if self.kind == "smeared_laminate":
-            if not self.layers:
+            if self.layers is None or len(self.layers) < 1:
                 raise ValueError(f"{self.name}: smeared_laminate phases need layers")
-            _set(self, "layers", tuple(tuple(float(v) for v in layer) for layer in self.layers))
+            layers = []
+            for i, layer in enumerate(self.layers):
+                if len(layer) != 3:
+                    raise ValueError(f"{self.name}: layer {i} must be (fraction, E, nu)")
+                nu_i = _finite(f"{self.name}: layer {i} nu", layer[2])
+                if not -1.0 < nu_i < 0.5:
+                    raise ValueError(f"{self.name}: layer {i} nu must lie in (-1, 0.5)")
+                layers.append((_positive(f"{self.name}: layer {i} fraction", layer[0]),
+                               _positive(f"{self.name}: layer {i} E", layer[1]), nu_i))
+            if abs(sum(f for f, _, _ in layers) - 1.0) > 1.0e-12:
+                raise ValueError(f"{self.name}: layer fractions must sum to 1")
+            _set(self, "layers", tuple(layers))
         elif self.layers is not None:
             raise ValueError(f"{self.name}: layers apply to smeared_laminate phases only")
         if self.E is None or self.nu is None:
@@ -230,9 +241,20 @@ class VoxelModel:
         if not np.isfinite(tangent).all():
             raise ValueError("tangent contains non-finite values")
         self.tangent = np.ascontiguousarray(tangent)
-        missing = [name for name in self.phases_present() if name not in self.materials.phases]
+        present = self.phases_present()
+        missing = [name for name in present if name not in self.materials.phases]
         if missing:
             raise ValueError(f"phases {missing} are present but have no material")
+        for name in present:
+            if self.materials.phases[name].kind == "isotropic":
+                continue
+            norms = np.linalg.norm(self.tangent[self.phase_id == PHASE_ID[name]], axis=-1)
+            if norms.size and float(np.abs(norms - 1.0).max()) > 1.0e-8:
+                raise ValueError(f"phase {name!r}: tangents must be unit vectors")
+        if "interface_nodes" in self.aux:
+            mask = np.asarray(self.aux["interface_nodes"])
+            if mask.shape != (self.grid.n_nodes_full,) or mask.dtype != np.bool_:
+                raise ValueError(f"aux['interface_nodes'] must be a bool array of shape ({self.grid.n_nodes_full},)")
 
     def phases_present(self):
         return tuple(PHASE_NAMES[int(i)] for i in np.unique(np.asarray(self.phase_id)))
