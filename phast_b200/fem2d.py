@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import math
 from dataclasses import dataclass, field
+from typing import Optional
 
 import numpy as np
 import torch
@@ -23,7 +24,12 @@ from ._lib import call, ptr, stream
 
 @dataclass
 class Material:
-    """The fields of ``phast.physics.material.Material`` the hot path reads (material.py:379-529)."""
+    """``phast.physics.material.Material`` (physics/material.py:80-257): the same fields in the
+    same order with the same defaults, and the same construction checks and normalisation
+    (``eta_residual <= 0`` becomes 1e-7, ``pf_model`` upper-cased).  The GPU kernels read the
+    elastic, fracture and split fields; the solvers refuse, with ``NotImplementedError``, the
+    laws and couplings they do not run (PF-CZM, Allen-Cahn, non-standard degradation,
+    plasticity, the principal-stress driver, the ``sigma_ts`` nucleation scaling)."""
     E: float = 210000.0
     nu: float = 0.3
     Gc: float = 2.7
@@ -32,12 +38,73 @@ class Material:
     eta_residual: float = 1e-7
     energy_split: str = "amor"
     pf_model: str = "AT2"
-    at1_threshold: object = "auto"
     gamma_correction: bool = False
     degradation_type: str = "standard"
     stress_degradation: str = "split"
+    cubic_s: float = 1.0
+    sigma_ts: float = 0.0
+    pfczm_p: int = 2
+    pfczm_softening: str = "linear"
     driving_force: str = "strain_energy"
     plane_stress: bool = False
+    at1_threshold: object = "auto"
+    plasticity_model: str = "none"
+    yield_stress: float = 0.0
+    hardening_modulus: float = 0.0
+    hardening_type: str = "none"
+    voce_q_inf: Optional[float] = None
+    voce_b: Optional[float] = None
+    swift_K: Optional[float] = None
+    swift_n: Optional[float] = None
+    swift_eps0: Optional[float] = None
+
+    def __post_init__(self):
+        # the reference's rules (material.py:176-257), restated
+        if self.eta_residual <= 0.0:
+            self.eta_residual = 1e-7
+        model = str(self.pf_model)
+        self.pf_model = "allencahn" if model.lower() == "allencahn" else model.upper()
+        if self.pf_model not in ("AT1", "AT2", "PFCZM", "allencahn"):
+            raise ValueError(f"pf_model must be 'AT1', 'AT2', 'PFCZM', or 'allencahn', got {self.pf_model!r}")
+        if self.stress_degradation not in ("split", "full"):
+            raise ValueError(f"stress_degradation must be 'split' or 'full', got {self.stress_degradation!r}")
+        if self.degradation_type == "rational_at2" and self.pf_model != "AT2":
+            raise ValueError(f"degradation_type='rational_at2' is defined for pf_model='AT2', got {self.pf_model!r}")
+        if isinstance(self.pfczm_p, bool) or not isinstance(self.pfczm_p, int) or self.pfczm_p < 2:
+            raise ValueError(f"pfczm_p must be an integer >= 2, got {self.pfczm_p!r}")
+        if self.pfczm_softening not in ("linear", "exponential"):
+            raise ValueError(f"pfczm_softening must be 'linear' or 'exponential', got {self.pfczm_softening!r}")
+        if self.energy_split == "spectral_plane_stress_condensed" and not self.plane_stress:
+            raise ValueError("energy_split='spectral_plane_stress_condensed' requires plane_stress=True")
+        if self.pf_model == "PFCZM" and self.sigma_ts <= 0.0:
+            raise ValueError("pf_model='PFCZM' requires sigma_ts > 0")
+        if self.pf_model == "PFCZM" and self.degradation_type != "standard":
+            raise ValueError("pf_model='PFCZM' requires degradation_type='standard'")
+        t = self.at1_threshold
+        if isinstance(t, str):
+            if t != "auto":
+                raise ValueError(f"at1_threshold must be 'auto' or a float, got {t!r}")
+        elif not isinstance(t, (int, float)):
+            raise ValueError(f"at1_threshold must be 'auto' or a float, got type {type(t).__name__}")
+        elif t < 0.0:
+            raise ValueError(f"at1_threshold must be non-negative, got {t}")
+        if self.cubic_s < 0.0:
+            raise ValueError(f"cubic_s must be non-negative, got {self.cubic_s}")
+        if self.plasticity_model != "none":
+            if self.yield_stress <= 0.0:
+                raise ValueError(f"plasticity_model={self.plasticity_model!r} requires yield_stress > 0")
+            if self.hardening_modulus < 0.0:
+                raise ValueError(f"hardening_modulus must be non-negative, got {self.hardening_modulus}")
+            if self.hardening_type == "voce":
+                if self.voce_q_inf is None or self.voce_b is None:
+                    raise ValueError("hardening_type='voce' requires voce_q_inf and voce_b to be set")
+                if self.voce_b <= 0.0:
+                    raise ValueError(f"voce_b must be > 0, got {self.voce_b}")
+            if self.hardening_type == "swift":
+                if self.swift_K is None or self.swift_n is None:
+                    raise ValueError("hardening_type='swift' requires swift_K and swift_n to be set")
+                if self.swift_K <= 0.0 or self.swift_n <= 0.0:
+                    raise ValueError(f"swift_K and swift_n must be > 0, got K={self.swift_K}, n={self.swift_n}")
 
     @property
     def lam(self):

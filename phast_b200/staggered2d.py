@@ -143,6 +143,13 @@ class StaggeredSolver:
             raise NotImplementedError("the B200 backend runs Anderson mixing of depth 1 to 6")
         if cfg.stagger_criterion != "relative" or cfg.stagger_norm != "l2":
             raise NotImplementedError("only the relative-L2 stagger criterion is implemented")
+        if getattr(material, "plasticity_model", "none") != "none":
+            raise NotImplementedError("plasticity coupling is not implemented by the B200 backend")
+        if getattr(material, "driving_force", "strain_energy") != "strain_energy":
+            raise NotImplementedError("only the strain-energy driving force is implemented")
+        if (getattr(material, "sigma_ts", None) or 0.0) > 0.0:
+            raise NotImplementedError("the sigma_ts nucleation scaling of the driving force is not implemented by the "
+                                      "B200 backend")
         self.mesh, self.material, self.bcs = mesh, material, bcs
         self.fem = FEMOperators(mesh, material)
         fem = self.fem

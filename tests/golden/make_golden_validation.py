@@ -1,11 +1,13 @@
 """Writes tests/golden/validation.json: which constructor arguments the reference's 3D data
 classes (VoxelGrid, PhaseMaterial, MaterialTable, VoxelModel, LoadCase, SolverConfig;
-src/phast/solid3d/model.py:183-897) accept and which they refuse, with the exception class.
+src/phast/solid3d/model.py:183-897) and its 2D ``Material`` (src/phast/physics/material.py:80-257)
+accept and which they refuse, with the exception class (and, for an accepted 2D material, the
+fields it normalises).
 
 Usage: python tests/golden/make_golden_validation.py <path to the reference's src directory>
 
 Each case is plain JSON data; ``build(mod, case)`` turns it into a constructor call on the
-classes of ``mod`` (the reference's module here, ``phast_b200.solid3d.model`` in the test),
+classes of ``mod`` (the reference's classes here, ``phast_b200``'s in the test),
 so the test replays the same calls on this backend's classes.
 """
 from __future__ import annotations
@@ -150,8 +152,38 @@ for kw in [dict(), dict(kappa=0.0), dict(kappa=1.0), dict(kappa=-1e-3), dict(kap
     _case("SolverConfig", **({"device": "cuda"} | kw))
 
 
+# 2D Material (physics/material.py:80-257)
+MAT = dict(E=210000.0, nu=0.3, Gc=2.7, l0=0.05)
+for kw in [dict(), dict(pf_model="at1"), dict(pf_model="AllenCahn"), dict(pf_model="at3"), dict(pf_model="pfczm"),
+           dict(pf_model="PFCZM", sigma_ts=3.0), dict(pf_model="PFCZM", sigma_ts=3.0, degradation_type="cubic"),
+           dict(eta_residual=0.0), dict(eta_residual=-1.0), dict(stress_degradation="partial"),
+           dict(stress_degradation="full"), dict(degradation_type="rational_at2"),
+           dict(degradation_type="rational_at2", pf_model="AT1"), dict(pfczm_p=1), dict(pfczm_p=2.5),
+           dict(pfczm_p=True), dict(pfczm_p=3), dict(pfczm_softening="cubic"), dict(pfczm_softening="exponential"),
+           dict(energy_split="spectral_plane_stress_condensed"),
+           dict(energy_split="spectral_plane_stress_condensed", plane_stress=True),
+           dict(at1_threshold="manual"), dict(at1_threshold=-1.0), dict(at1_threshold=2.5), dict(at1_threshold=0),
+           dict(at1_threshold=[1.0]), dict(cubic_s=-0.5), dict(plasticity_model="j2_isotropic"),
+           dict(plasticity_model="j2_isotropic", yield_stress=300.0),
+           dict(plasticity_model="j2_isotropic", yield_stress=300.0, hardening_modulus=-1.0),
+           dict(plasticity_model="j2_isotropic", yield_stress=300.0, hardening_type="voce"),
+           dict(plasticity_model="j2_isotropic", yield_stress=300.0, hardening_type="voce", voce_q_inf=100.0,
+                voce_b=0.0),
+           dict(plasticity_model="j2_isotropic", yield_stress=300.0, hardening_type="voce", voce_q_inf=100.0,
+                voce_b=5.0),
+           dict(plasticity_model="j2_isotropic", yield_stress=300.0, hardening_type="swift", swift_K=500.0),
+           dict(plasticity_model="j2_isotropic", yield_stress=300.0, hardening_type="swift", swift_K=500.0,
+                swift_n=-0.2),
+           dict(hardening_type="swift")]:
+    _case("Material2D", **(MAT | kw))
+
+NORMALISED = ("pf_model", "eta_residual", "at1_threshold", "pfczm_p")
+"""Fields of an accepted 2D Material whose stored value the fixture records."""
+
+
 def build(mod, case):
-    """Run the constructor call of ``case`` on the classes of module ``mod``."""
+    """Run the constructor call of ``case`` on the classes of namespace ``mod`` (the 3D data
+    classes and ``Material``, the 2D material)."""
     cls, kw = case["cls"], dict(case["kw"])
 
     def phase(args):
@@ -190,14 +222,19 @@ def build(mod, case):
         return mod.LoadCase(**{k: tuple(v) if isinstance(v, list) else v for k, v in kw.items()})
     if cls == "SolverConfig":
         return mod.SolverConfig(**kw)
+    if cls == "Material2D":
+        return mod.Material(**kw)
     raise KeyError(cls)
 
 
 def outcome(mod, case):
+    """``'ok'`` (with the normalised fields of a 2D material) or the exception class name."""
     try:
-        build(mod, case)
+        obj = build(mod, case)
     except (ValueError, TypeError) as exc:
         return type(exc).__name__
+    if case["cls"] == "Material2D":
+        return "ok " + json.dumps({k: getattr(obj, k) for k in NORMALISED})
     return "ok"
 
 
@@ -205,11 +242,15 @@ def main(src):
     sys.path.insert(0, HERE)
     from make_golden import _import_reference
     _import_reference(src)
-    import phast.solid3d.model as ref
+    import types
+    import phast.solid3d.model as ref3d
+    from phast.physics.material import Material
+    ref = types.SimpleNamespace(**vars(ref3d))
+    ref.Material = Material
     out = [dict(case, outcome=outcome(ref, case)) for case in CASES]
     with open(os.path.join(HERE, "validation.json"), "w") as f:
         json.dump(out, f, indent=0)
-    print(f"{len(out)} cases, {sum(c['outcome'] != 'ok' for c in out)} refused")
+    print(f"{len(out)} cases, {sum(not c['outcome'].startswith('ok') for c in out)} refused")
 
 
 if __name__ == "__main__":

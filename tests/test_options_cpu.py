@@ -54,3 +54,13 @@ def test_valid_combinations_normalise():
     assert cfg.pfczm_p == 2 and isinstance(cfg.pfczm_p, int)
     cfg = SolverConfig(energy_split_band="interface", band_stress="variational", anderson_depth=2.0, anderson_start=3.0)
     assert cfg.anderson_depth == 2 and isinstance(cfg.anderson_start, int)
+
+
+@pytest.mark.parametrize("kw", [dict(plasticity_model="j2_isotropic", yield_stress=300.0),
+                                dict(driving_force="principal_stress"), dict(sigma_ts=3.0)])
+def test_2d_solver_refuses_couplings_it_does_not_run(kw):
+    # refused before any mesh or device work, so this runs without a GPU
+    from phast_b200.fem2d import Material
+    from phast_b200.staggered2d import StaggeredSolver, SolverConfig as Config2D
+    with pytest.raises(NotImplementedError):
+        StaggeredSolver(None, Material(**kw), None, Config2D(solver_type="quasi_static"))

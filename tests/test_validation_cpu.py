@@ -1,6 +1,7 @@
-"""The 3D data classes accept and refuse the same constructor arguments as the reference's
-(src/phast/solid3d/model.py:183-897), with the same exception class: 135 cases recorded from
-the reference's own classes by ``tests/golden/make_golden_validation.py``."""
+"""The 3D data classes and the 2D ``Material`` accept and refuse the same constructor
+arguments as the reference's (src/phast/solid3d/model.py:183-897, src/phast/physics/material.py:
+80-257), with the same exception class and the same normalised fields: cases recorded from the
+reference's own classes by ``tests/golden/make_golden_validation.py``."""
 import importlib.util
 import json
 import os
@@ -8,7 +9,13 @@ import os
 import pytest
 
 from conftest import GOLDEN
-import phast_b200.solid3d.model as ours
+import types
+
+import phast_b200.solid3d.model as _model3d
+from phast_b200.fem2d import Material
+
+ours = types.SimpleNamespace(**vars(_model3d))
+ours.Material = Material
 
 _spec = importlib.util.spec_from_file_location("make_golden_validation",
                                                os.path.join(GOLDEN, "make_golden_validation.py"))
