@@ -24,9 +24,15 @@ from .mechanics2d import ExplicitDynamics, QuasiStaticSolver
 
 @dataclass
 class SolverConfig:
-    """The ``SolverConfig`` fields the hot path reads (staggered_solver.py:45-162)."""
+    """``phast.solvers.staggered_solver.SolverConfig`` (staggered_solver.py:45-162): the same
+    fields in the same order with the same defaults, and its rule that the quasi-static solver
+    types default to the Jacobi preconditioner.  ``dtype`` (last, this backend's own) selects
+    FP32 state for the explicit step.  Options the GPU path does not run (generalized-alpha,
+    adaptive time steps, mesh refinement or stagger tolerance, smooth-max history updates, the
+    fresh-damage corrector) are refused by ``StaggeredSolver`` with ``NotImplementedError``."""
     solver_type: str = "explicit"
     time_integrator: str = "central_difference"
+    rho_inf: float = 0.5
     dt: Optional[float] = None
     dt_safety: float = 1.0
     num_steps: int = 200
@@ -35,7 +41,9 @@ class SolverConfig:
     static_tol: float = 1e-8
     static_max_iter: int = 5000
     H_cap: Optional[float] = None
+    softmax_H_beta: Optional[float] = None
     H_update_method: str = "hard_max"
+    H_update_scale: Optional[float] = None
     stagger_tol: float = 1e-6
     max_stagger: int = 500
     stagger_criterion: str = "relative"
@@ -43,7 +51,12 @@ class SolverConfig:
     use_multigrid: bool = True
     bounds_method: str = "post_clamp"
     preconditioner: Optional[str] = None
+    adaptive_refine: bool = False
+    refine_every: int = 10
+    refine_d_threshold: float = 0.5
+    refine_grad_d_threshold: float = 0.3
     anderson_depth: int = 0
+    adaptive_stagger_tol: bool = False
     differentiable: bool = False
     fail_on_mechanics_nonconvergence: bool = True
     fail_on_stagger_nonconvergence: bool = True
@@ -55,8 +68,25 @@ class SolverConfig:
     line_search_max_steps: int = 8
     line_search_min_alpha: float = 1e-4
     line_search_c: float = 1e-4
+    adaptive_dt: bool = False
+    adaptive_dt_d_threshold: float = 0.01
+    adaptive_dt_min_factor: float = 0.1
+    adaptive_dt_grow_rate: float = 1.1
+    dt_growth_threshold: float = 0.001
+    dt_cutback_threshold: float = 0.01
+    dt_floor: float = 1e-12
     damage_every: int = 3
+    fresh_d_in_corrector: bool = False
+    dump_every: int = 10
+    h5_every: int = 1
+    viz_format: str = "vtu"
+    print_every: int = 10
     dtype: torch.dtype = torch.float64
+
+    def __post_init__(self):
+        if self.preconditioner is None and self.solver_type in ("static", "quasi_static", "quasi_static_legacy",
+                                                                "lbfgs", "monolithic"):
+            self.preconditioner = "jacobi"
 
 
 class BoundaryConditions:
@@ -143,6 +173,15 @@ class StaggeredSolver:
             raise NotImplementedError("the B200 backend runs Anderson mixing of depth 1 to 6")
         if cfg.stagger_criterion != "relative" or cfg.stagger_norm != "l2":
             raise NotImplementedError("only the relative-L2 stagger criterion is implemented")
+        if cfg.softmax_H_beta is not None:
+            raise NotImplementedError("the smooth-max history update (softmax_H_beta) is not implemented by the B200 "
+                                      "backend")
+        if cfg.solver_type == "explicit" and cfg.time_integrator not in ("central_difference", "verlet", "newmark"):
+            raise NotImplementedError(f"time_integrator {cfg.time_integrator!r}: the B200 backend runs the central "
+                                      "difference step")
+        for name in ("adaptive_refine", "adaptive_stagger_tol", "adaptive_dt", "fresh_d_in_corrector"):
+            if getattr(cfg, name):
+                raise NotImplementedError(f"{name}=True is not implemented by the B200 backend")
         if getattr(material, "plasticity_model", "none") != "none":
             raise NotImplementedError("plasticity coupling is not implemented by the B200 backend")
         if getattr(material, "driving_force", "strain_energy") != "strain_energy":

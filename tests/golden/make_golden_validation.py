@@ -1,7 +1,7 @@
 """Writes tests/golden/validation.json: which constructor arguments the reference's 3D data
 classes (VoxelGrid, PhaseMaterial, MaterialTable, VoxelModel, LoadCase, SolverConfig;
-src/phast/solid3d/model.py:183-897) and its 2D ``Material`` (src/phast/physics/material.py:80-257)
-accept and which they refuse, with the exception class (and, for an accepted 2D material, the
+src/phast/solid3d/model.py:183-897), its 2D ``Material`` (src/phast/physics/material.py:80-257)
+and 2D ``SolverConfig`` (src/phast/solvers/staggered_solver.py:45-162) accept and which they refuse, with the exception class (and, for an accepted 2D material, the
 fields it normalises).
 
 Usage: python tests/golden/make_golden_validation.py <path to the reference's src directory>
@@ -177,13 +177,21 @@ for kw in [dict(), dict(pf_model="at1"), dict(pf_model="AllenCahn"), dict(pf_mod
            dict(hardening_type="swift")]:
     _case("Material2D", **(MAT | kw))
 
-NORMALISED = ("pf_model", "eta_residual", "at1_threshold", "pfczm_p")
-"""Fields of an accepted 2D Material whose stored value the fixture records."""
+# 2D SolverConfig (solvers/staggered_solver.py:45-162): no checks, one normalisation
+for kw in [dict(), dict(solver_type="quasi_static"), dict(solver_type="static"), dict(solver_type="monolithic"),
+           dict(solver_type="quasi_static", preconditioner="gmg"), dict(solver_type="explicit", preconditioner="gmg"),
+           dict(adaptive_dt=True, print_every=0, h5_every=0, viz_format="pv", dump_every=0),
+           dict(time_integrator="verlet", rho_inf=0.8, softmax_H_beta=10.0, H_update_scale=0.5)]:
+    _case("Config2D", **kw)
+
+NORMALISED = {"Material2D": ("pf_model", "eta_residual", "at1_threshold", "pfczm_p"),
+              "Config2D": ("preconditioner", "solver_type", "time_integrator")}
+"""Fields of an accepted 2D object whose stored value the fixture records."""
 
 
 def build(mod, case):
     """Run the constructor call of ``case`` on the classes of namespace ``mod`` (the 3D data
-    classes and ``Material``, the 2D material)."""
+    classes, ``Material`` and ``Config2D``, the 2D material and solver settings)."""
     cls, kw = case["cls"], dict(case["kw"])
 
     def phase(args):
@@ -224,6 +232,8 @@ def build(mod, case):
         return mod.SolverConfig(**kw)
     if cls == "Material2D":
         return mod.Material(**kw)
+    if cls == "Config2D":
+        return mod.Config2D(**kw)
     raise KeyError(cls)
 
 
@@ -233,8 +243,8 @@ def outcome(mod, case):
         obj = build(mod, case)
     except (ValueError, TypeError) as exc:
         return type(exc).__name__
-    if case["cls"] == "Material2D":
-        return "ok " + json.dumps({k: getattr(obj, k) for k in NORMALISED})
+    if case["cls"] in NORMALISED:
+        return "ok " + json.dumps({k: getattr(obj, k) for k in NORMALISED[case["cls"]]})
     return "ok"
 
 
@@ -245,8 +255,9 @@ def main(src):
     import types
     import phast.solid3d.model as ref3d
     from phast.physics.material import Material
+    from phast.solvers.staggered_solver import SolverConfig as Config2D
     ref = types.SimpleNamespace(**vars(ref3d))
-    ref.Material = Material
+    ref.Material, ref.Config2D = Material, Config2D
     out = [dict(case, outcome=outcome(ref, case)) for case in CASES]
     with open(os.path.join(HERE, "validation.json"), "w") as f:
         json.dump(out, f, indent=0)

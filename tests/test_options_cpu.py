@@ -64,3 +64,14 @@ def test_2d_solver_refuses_couplings_it_does_not_run(kw):
     from phast_b200.staggered2d import StaggeredSolver, SolverConfig as Config2D
     with pytest.raises(NotImplementedError):
         StaggeredSolver(None, Material(**kw), None, Config2D(solver_type="quasi_static"))
+
+
+@pytest.mark.parametrize("kw", [dict(softmax_H_beta=10.0), dict(time_integrator="generalized_alpha"),
+                                dict(time_integrator="gen_alpha"), dict(adaptive_refine=True),
+                                dict(adaptive_stagger_tol=True), dict(adaptive_dt=True),
+                                dict(fresh_d_in_corrector=True)])
+def test_2d_solver_refuses_options_it_does_not_run(kw):
+    from phast_b200.fem2d import Material
+    from phast_b200.staggered2d import StaggeredSolver, SolverConfig as Config2D
+    with pytest.raises(NotImplementedError):
+        StaggeredSolver(None, Material(), None, Config2D(**kw))

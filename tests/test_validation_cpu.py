@@ -1,4 +1,4 @@
-"""The 3D data classes and the 2D ``Material`` accept and refuse the same constructor
+"""The 3D data classes, the 2D ``Material`` and the 2D ``SolverConfig`` accept and refuse the same constructor
 arguments as the reference's (src/phast/solid3d/model.py:183-897, src/phast/physics/material.py:
 80-257), with the same exception class and the same normalised fields: cases recorded from the
 reference's own classes by ``tests/golden/make_golden_validation.py``."""
@@ -13,9 +13,10 @@ import types
 
 import phast_b200.solid3d.model as _model3d
 from phast_b200.fem2d import Material
+from phast_b200.staggered2d import SolverConfig as Config2D
 
 ours = types.SimpleNamespace(**vars(_model3d))
-ours.Material = Material
+ours.Material, ours.Config2D = Material, Config2D
 
 _spec = importlib.util.spec_from_file_location("make_golden_validation",
                                                os.path.join(GOLDEN, "make_golden_validation.py"))
