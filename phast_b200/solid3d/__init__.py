@@ -10,5 +10,5 @@ from .model import (DRIVER_FULL, DRIVER_NONE, DRIVER_SPECTRAL, PHASE_ID, PHASE_N
 from .operator import H8DamageSystem, MechOperator, PeriodicVoxelPhaseFieldOperator, PfczmNewtonSystem
 from .staggered import (PLAIN, BoxKKTFailureEvidence, BoxKKTResult, H8ScalarBoxKKTConvergenceError, IncrementRecord,
                         MechForm, PCGBreakdownError, PCGConvergenceError, PCGInfo, ProjectedAnderson, SolverState,
-                        StaggerConvergenceError, StaggeredSolver, pcg, solve_constrained, solve_constrained_form,
-                        solve_h8_scalar_box_kkt)
+                        StaggerConvergenceError, StaggeredSolver, load_checkpoint, pcg, save_checkpoint,
+                        solve_constrained, solve_constrained_form, solve_h8_scalar_box_kkt)

@@ -467,6 +467,51 @@ class PeriodicVoxelPhaseFieldOperator:
         """Number of smeared-laminate band elements with the band closure (none here)."""
         return 0
 
+    # -- the interface driver (operator.py:634-655, 991-1008): this backend refuses the
+    # interface driver, so there are no interface elements and the queries say so
+    @property
+    def has_interface(self):
+        """Whether any element uses the directional interface driver (never here)."""
+        return False
+
+    @property
+    def n_interface(self):
+        """Number of interface-driver elements (0 here)."""
+        return 0
+
+    @property
+    def has_interface_stress(self):
+        """Whether interface elements carry the variational band stress (never here)."""
+        return False
+
+    def interface_normal_traction(self, x):
+        """Normal interface traction ``(n_interface, 8)`` of the interface elements: empty here."""
+        self._check("x", x, (self.n_mech,))
+        return torch.empty((0, 8), dtype=self.dtype, device=self.device)
+
+    def interface_opening(self, x):
+        """Normal-opening pattern ``(n_interface, 8)`` bool: empty here."""
+        return self.interface_normal_traction(x) > 0.0
+
+    def reduced_of_full(self):
+        """Reduced node of every full grid node ``(N_full,)`` (periodic.py:40-123): full node
+        ``i + (nx+1)(j + (ny+1) k)`` maps to ``i' + rx (j' + ry k')`` with periodic axes wrapped."""
+        if getattr(self, "_rof", None) is None:
+            nx, ny, nz = self.shape
+            rx, ry, _ = self.reduced_shape
+            px, py, pz = bool(self.vgrid.px), bool(self.vgrid.py), bool(self.vgrid.pz)
+            i = np.arange(nx + 1) % nx if px else np.arange(nx + 1)
+            j = np.arange(ny + 1) % ny if py else np.arange(ny + 1)
+            k = np.arange(nz + 1) % nz if pz else np.arange(nz + 1)
+            idx = i[None, None, :] + rx * (j[None, :, None] + ry * k[:, None, None])
+            self._rof = torch.as_tensor(idx.reshape(-1), dtype=torch.long, device=self.device)
+        return self._rof
+
+    def expand_damage(self, d):
+        """Full nodal damage ``P d`` ``(N_full,)`` (operator.py:1546-1550)."""
+        d = self._check("d", d, (self.n_red,))
+        return d[self.reduced_of_full()]
+
     def _cl_ws(self):
         return self._clws.get(_lib.load().phastb_h8_closure_workspace_bytes(self.vgrid))
 

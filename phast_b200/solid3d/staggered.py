@@ -439,6 +439,61 @@ class SolverState:
                            self.d_prev_step.to(device), int(self.increment))
 
 
+CHECKPOINT_FORMAT = "phast.solid3d.checkpoint"
+CHECKPOINT_VERSION = 1
+_STATE_TENSORS = ("x", "d", "H", "macro_strain", "macro_stress", "d_prev_step")
+
+
+def save_checkpoint(path, state, *, meta=None):
+    """Write ``state`` and JSON-serialisable ``meta`` (solid3d/staggered.py:1638-1663).
+
+    The file is the reference's checkpoint format, so either package resumes the other's
+    runs: a ``torch.save`` dict with ``format``, ``version``, the state's scalars and its
+    tensors on the CPU, and ``meta`` as a sorted JSON string; it is written beside the
+    target and moved over it, so a crash never leaves a half-written checkpoint.
+    """
+    import json
+    import os
+    from pathlib import Path
+    if not isinstance(state, SolverState):
+        raise TypeError("state must be a SolverState")
+    path = Path(path)
+    path.parent.mkdir(parents=True, exist_ok=True)
+    body = {"step": int(state.step), "increment": int(state.increment), "external_work": float(state.external_work)}
+    for name in _STATE_TENSORS:
+        body[name] = getattr(state, name).detach().to("cpu", copy=True)
+    payload = {"format": CHECKPOINT_FORMAT, "version": CHECKPOINT_VERSION, "state": body,
+               "meta_json": json.dumps(dict(meta or {}), sort_keys=True)}
+    tmp = path.with_name(path.name + ".tmp")
+    torch.save(payload, tmp)
+    os.replace(tmp, path)
+    return path
+
+
+def load_checkpoint(path, device="cpu"):
+    """``(state, meta)`` from a checkpoint file (solid3d/staggered.py:1666-1690); the fields
+    the solver keeps on the device go to ``device``, the macro strain and stress stay on the
+    host as this package's states hold them."""
+    import json
+    from pathlib import Path
+    target = torch.device(device)
+    payload = torch.load(Path(path), map_location="cpu", weights_only=True)
+    if not isinstance(payload, dict) or payload.get("format") != CHECKPOINT_FORMAT:
+        raise ValueError(f"{path} is not a {CHECKPOINT_FORMAT} file")
+    if payload.get("version") != CHECKPOINT_VERSION:
+        raise ValueError(f"unsupported checkpoint version {payload.get('version')!r}")
+    body = payload["state"]
+    for name in _STATE_TENSORS:
+        t = body.get(name)
+        if not isinstance(t, torch.Tensor) or t.dtype != torch.float64:
+            raise ValueError(f"checkpoint field {name!r} must be a float64 tensor")
+    state = SolverState(step=int(body["step"]), x=body["x"].to(target), d=body["d"].to(target),
+                        H=body["H"].to(target), macro_strain=body["macro_strain"].clone(),
+                        macro_stress=body["macro_stress"].clone(), external_work=float(body["external_work"]),
+                        d_prev_step=body["d_prev_step"].to(target), increment=int(body["increment"]))
+    return state, json.loads(payload["meta_json"])
+
+
 @dataclass(frozen=True)
 class IncrementRecord:
     """Scalar record of one accepted load increment (solid3d/model.py:1234-1300), same fields.

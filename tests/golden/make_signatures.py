@@ -54,6 +54,11 @@ FUNCTIONS = [
     ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.closure_pattern"),
     ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.closure_pattern_change"),
     ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.kinematic_guard"),
+    ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.expand_damage"),
+    ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.interface_normal_traction"),
+    ("phast.solid3d.operator", "PeriodicVoxelPhaseFieldOperator.interface_opening"),
+    ("phast.solid3d.staggered", "save_checkpoint"),
+    ("phast.solid3d.staggered", "load_checkpoint"),
     ("phast.solid3d.linalg", "pcg"),
     ("phast.solid3d.linalg", "solve_constrained"),
     ("phast.solvers.box_kkt_h8", "solve_h8_scalar_box_kkt"),
@@ -92,6 +97,8 @@ DATACLASSES = [
     ("phast.solid3d.staggered", "SolverState"),
     ("phast.solid3d.linalg", "PCGInfo"),
     ("phast.solid3d.model", "ClosurePattern"),
+    ("phast.physics.material", "Material"),
+    ("phast.solvers.staggered_solver", "SolverConfig"),
 ]
 
 PLAIN = (int, float, str, bool, type(None), tuple)

@@ -75,3 +75,19 @@ def test_2d_solver_refuses_options_it_does_not_run(kw):
     from phast_b200.staggered2d import StaggeredSolver, SolverConfig as Config2D
     with pytest.raises(NotImplementedError):
         StaggeredSolver(None, Material(), None, Config2D(**kw))
+
+
+def test_reduced_of_full_matches_reference_map():
+    # the full-to-reduced node map behind expand_damage, against the reference's own map
+    # (tests/golden/make_golden_periodic_map.py); the index arithmetic runs on the host
+    import types
+    from conftest import golden
+    from phast_b200.solid3d.operator import PeriodicVoxelPhaseFieldOperator as Op
+    g = golden("periodic_map")
+    for n in range(int(g["n"][0])):
+        shape, per = tuple(int(v) for v in g[f"shape_{n}"]), tuple(bool(v) for v in g[f"periodic_{n}"])
+        red = tuple(s if p else s + 1 for s, p in zip(shape, per))
+        assert red == tuple(int(v) for v in g[f"reduced_shape_{n}"])
+        fake = types.SimpleNamespace(shape=shape, reduced_shape=red, device="cpu", _rof=None,
+                                     vgrid=types.SimpleNamespace(px=int(per[0]), py=int(per[1]), pz=int(per[2])))
+        assert (Op.reduced_of_full(fake).numpy() == g[f"rof_{n}"]).all(), n

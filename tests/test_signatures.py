@@ -6,7 +6,7 @@ every mirrored function or method, every reference parameter must exist here
 under the same name, of the same kind, in the same order and (for constant
 defaults) with the same default; parameters this package adds must come after
 them and have defaults.  For every mirrored data class the field names must be
-the reference's, in order.
+the reference's, in order (followed by the few fields this package adds, listed below).
 """
 import dataclasses
 import inspect
@@ -21,6 +21,8 @@ with open(os.path.join(ROOT, "tests", "golden", "reference_signatures.json")) as
 
 # defaults that differ on purpose: the device of a GPU backend
 DEFAULT_EXCEPTIONS = set()
+# fields this package adds after the reference's: the FP32 state of the 2D explicit step
+EXTRA_FIELDS = {"phast.solvers.staggered_solver:SolverConfig": ["dtype"]}
 
 
 def _ours(module, qualname):
@@ -57,4 +59,4 @@ def test_signature_matches_reference(key):
 def test_dataclass_fields_match_reference(key):
     module, qualname = key.split(":")
     cls = _ours(module, qualname)
-    assert [f.name for f in dataclasses.fields(cls)] == REF["dataclasses"][key]
+    assert [f.name for f in dataclasses.fields(cls)] == REF["dataclasses"][key] + EXTRA_FIELDS.get(key, [])
