@@ -252,6 +252,15 @@ class StaggeredSolver:
         self.H_elem = H_new
         return H_new
 
+    def set_damage(self, d_new):
+        """Replace the damage field with a copy of ``d_new`` (staggered_solver.py:1409-1411); the
+        kernels read it through raw pointers, so its shape, dtype and device are checked."""
+        if not isinstance(d_new, torch.Tensor) or tuple(d_new.shape) != tuple(self.d.shape):
+            raise ValueError(f"d_new must be a tensor of shape {tuple(self.d.shape)}")
+        if d_new.device != self.d.device:
+            raise ValueError(f"d_new must be on {self.d.device}")
+        self.d = d_new.to(self.d.dtype).clone().contiguous()
+
     def step_solve_damage(self, d_prev_step=None):
         pf_mask, pf_vals = self._pf()
         d_prev_arg = d_prev_step if d_prev_step is not None else self.d

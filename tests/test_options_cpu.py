@@ -91,3 +91,18 @@ def test_reduced_of_full_matches_reference_map():
         fake = types.SimpleNamespace(shape=shape, reduced_shape=red, device="cpu", _rof=None,
                                      vgrid=types.SimpleNamespace(px=int(per[0]), py=int(per[1]), pz=int(per[2])))
         assert (Op.reduced_of_full(fake).numpy() == g[f"rof_{n}"]).all(), n
+
+
+def test_2d_set_damage_checks_and_copies():
+    # the method only touches self.d, so a stand-in object with CPU tensors exercises it
+    import types
+    import torch
+    from phast_b200.staggered2d import StaggeredSolver
+    fake = types.SimpleNamespace(d=torch.zeros(5, dtype=torch.float64))
+    new = torch.linspace(0, 1, 5, dtype=torch.float32)
+    StaggeredSolver.set_damage(fake, new)
+    assert fake.d.dtype == torch.float64 and torch.equal(fake.d, new.double()) and fake.d.data_ptr() != new.data_ptr()
+    with pytest.raises(ValueError):
+        StaggeredSolver.set_damage(fake, torch.zeros(4, dtype=torch.float64))
+    with pytest.raises(ValueError):
+        StaggeredSolver.set_damage(fake, [0.0] * 5)
